@@ -1,0 +1,260 @@
+/*
+ * h264_oracle_par.c -- whole-clip driver of the CPU oracle (test
+ * infrastructure and the timed CPU baseline only).
+ *
+ * It runs, per P frame f (reference = source frame f-1, the source-domain
+ * reference the mb-tree lookahead also uses, mbtree.rs:431-434):
+ *   planes  = build_hpel_planes(Y[f-1])                       inter.rs:816
+ *   picks   = plain-ME frame model (best_part per MB)         mb16.rs:4921
+ *   coeffs  = MC of each pick + luma T/Q at qp                mb16.rs:3436-3450
+ * and, over the whole clip, the HalfRes lookahead
+ *   half    = downsample2x(Y[f]);  costs = frame_costs(...)   mbtree.rs:61, 208
+ * Frames are independent, so the driver shards them over threads the
+ * way encode_all shards GOPs over std::thread (lib.rs:745-805), on POSIX
+ * threads.
+ */
+#include "h264_oracle.h"
+
+#include <pthread.h>
+#include <stdlib.h>
+#include <string.h>
+#include <unistd.h>
+
+/* A minimal dynamic parallel-for over [0, n) on POSIX threads. */
+typedef struct {
+    void (*fn)(void *arg, int i, int tid);
+    void *arg;
+    int n, tid;
+    volatile int *next;
+    pthread_mutex_t *mu;
+} par_worker;
+
+static void *par_main(void *p) {
+    par_worker *w = (par_worker *)p;
+    for (;;) {
+        pthread_mutex_lock(w->mu);
+        int i = (*w->next)++;
+        pthread_mutex_unlock(w->mu);
+        if (i >= w->n) break;
+        w->fn(w->arg, i, w->tid);
+    }
+    return NULL;
+}
+
+static void par_for(int n, int nthreads, void (*fn)(void *, int, int), void *arg) {
+    if (nthreads < 1) nthreads = 1;
+    if (nthreads > n) nthreads = n > 0 ? n : 1;
+    volatile int next = 0;
+    pthread_mutex_t mu = PTHREAD_MUTEX_INITIALIZER;
+    pthread_t th[256];
+    par_worker w[256];
+    if (nthreads > 256) nthreads = 256;
+    for (int t = 0; t < nthreads; t++) {
+        w[t].fn = fn; w[t].arg = arg; w[t].n = n; w[t].tid = t; w[t].next = &next; w[t].mu = &mu;
+    }
+    for (int t = 1; t < nthreads; t++) pthread_create(&th[t], NULL, par_main, &w[t]);
+    par_main(&w[0]);
+    for (int t = 1; t < nthreads; t++) pthread_join(th[t], NULL);
+}
+
+typedef struct {
+    int32_t fast, mb_use_satd, sadfp, mv_cost_kind;
+    double sadfp_lambda;
+    int32_t me_snap, me_fc;
+    uint32_t dia_mask, dia_sub_mask;
+    int32_t subpel, subpel_pat, sp_single_pass, sub_pat, me_subpel_iter, sp_maxit, sp_fc;
+} or_me_params_flat;
+
+static void unflatten(const or_me_params_flat *f, const uint16_t *tab, or_me_params *p) {
+    p->fast = f->fast; p->mb_use_satd = f->mb_use_satd; p->sadfp = f->sadfp; p->mv_cost_kind = f->mv_cost_kind;
+    p->mv_cost_tab = tab; p->sadfp_lambda = f->sadfp_lambda; p->me_snap = f->me_snap; p->me_fc = f->me_fc;
+    p->dia_mask = f->dia_mask; p->dia_sub_mask = f->dia_sub_mask; p->subpel = f->subpel;
+    p->subpel_pat = f->subpel_pat; p->sp_single_pass = f->sp_single_pass; p->sub_pat = f->sub_pat;
+    p->me_subpel_iter = f->me_subpel_iter; p->sp_maxit = f->sp_maxit; p->sp_fc = f->sp_fc;
+}
+
+int or_num_threads(void) {
+    long n = sysconf(_SC_NPROCESSORS_ONLN);
+    return n > 0 ? (int)n : 1;
+}
+
+/* ctypes-friendly motion_search entry (the params struct passed flat). */
+void or_motion_search_flat(const uint8_t *src, const uint8_t *ref, const uint8_t *planes4, int cw, int ch, int pad,
+                           const or_me_params_flat *pf, const uint16_t *tab, int lx, int ly, int rw, int rh,
+                           const int32_t *preds, int npred, double lambda_me, const int32_t *start, int32_t *out_mv,
+                           int64_t *out_cost, int32_t *out_evals) {
+    int pw = cw + 2 * pad, ph = ch + 2 * pad;
+    size_t ps = (size_t)pw * ph;
+    or_me_frame fr;
+    fr.src = src; fr.ref = ref; fr.cw = cw; fr.ch = ch;
+    fr.planes.f = planes4; fr.planes.h = planes4 + ps; fr.planes.v = planes4 + 2 * ps; fr.planes.c = planes4 + 3 * ps;
+    fr.planes.pw = pw; fr.planes.ph = ph; fr.planes.pad = pad; fr.planes.cw = cw; fr.planes.ch = ch;
+    or_me_params p;
+    unflatten(pf, tab, &p);
+    or_me_result r;
+    or_motion_search(&fr, &p, lx, ly, rw, rh, preds, npred, lambda_me, start, &r);
+    out_mv[0] = r.mvx; out_mv[1] = r.mvy;
+    *out_cost = r.cost;
+    if (out_evals) *out_evals = r.evals;
+}
+
+/* ctypes-friendly distortion of one candidate: kind 0 = SATD (mc_satd_hp), 1 = SAD. */
+int64_t or_candidate_dist(const uint8_t *src, const uint8_t *ref, const uint8_t *planes4, int cw, int ch, int pad,
+                          int kind, int lx, int ly, int rw, int rh, int mvx, int mvy) {
+    int pw = cw + 2 * pad, ph = ch + 2 * pad;
+    size_t ps = (size_t)pw * ph;
+    or_me_frame fr;
+    fr.src = src; fr.ref = ref; fr.cw = cw; fr.ch = ch;
+    fr.planes.f = planes4; fr.planes.h = planes4 + ps; fr.planes.v = planes4 + 2 * ps; fr.planes.c = planes4 + 3 * ps;
+    fr.planes.pw = pw; fr.planes.ph = ph; fr.planes.pad = pad; fr.planes.cw = cw; fr.planes.ch = ch;
+    return kind == 0 ? or_mc_satd_hp(&fr, 1, lx, ly, rw, rh, mvx, mvy) : or_mc_sad_hp(&fr, 1, lx, ly, rw, rh, mvx, mvy);
+}
+
+/* Builds pad + H/V/C into one buffer laid out F|H|V|C (each pw*ph). */
+void or_build_planes4(const uint8_t *ref, int cw, int ch, int pad, uint8_t *planes4) {
+    int pw = cw + 2 * pad, ph = ch + 2 * pad;
+    size_t ps = (size_t)pw * ph;
+    or_build_hpel_planes(ref, cw, ch, pad, planes4, planes4 + ps, planes4 + 2 * ps, planes4 + 3 * ps);
+}
+
+/* Plain-ME frame model over one (src, ref) pair; picks written flat:
+ * per MB {shape, mv0x, mv0y, mv1x, mv1y, cost_lo, cost_hi, evals-unused}. */
+void or_me_frame_flat(const uint8_t *src, const uint8_t *ref, const uint8_t *planes4, int cw, int ch, int pad,
+                      const or_me_params_flat *pf, const uint16_t *tab, double lambda_me, int64_t split_gate,
+                      int32_t *picks /* 6 per MB */, int64_t *costs /* 2 per MB: pick, 16x16 */) {
+    int pw = cw + 2 * pad, ph = ch + 2 * pad;
+    size_t ps = (size_t)pw * ph;
+    or_me_frame fr;
+    fr.src = src; fr.ref = ref; fr.cw = cw; fr.ch = ch;
+    fr.planes.f = planes4; fr.planes.h = planes4 + ps; fr.planes.v = planes4 + 2 * ps; fr.planes.c = planes4 + 3 * ps;
+    fr.planes.pw = pw; fr.planes.ph = ph; fr.planes.pad = pad; fr.planes.cw = cw; fr.planes.ch = ch;
+    or_me_params p;
+    unflatten(pf, tab, &p);
+    int nmb = (cw / 16) * (ch / 16);
+    or_mb_pick *pk = (or_mb_pick *)malloc(sizeof(or_mb_pick) * nmb);
+    or_me_frame_plain(&fr, &p, lambda_me, split_gate, pk);
+    for (int i = 0; i < nmb; i++) {
+        picks[6 * i + 0] = pk[i].shape;
+        picks[6 * i + 1] = pk[i].mv[0][0];
+        picks[6 * i + 2] = pk[i].mv[0][1];
+        picks[6 * i + 3] = pk[i].mv[1][0];
+        picks[6 * i + 4] = pk[i].mv[1][1];
+        picks[6 * i + 5] = 0;
+        costs[2 * i] = pk[i].cost;
+        costs[2 * i + 1] = pk[i].cost16;
+    }
+    free(pk);
+}
+
+/* Motion-compensated luma prediction of one MB for a pick (16x16 or the two
+ * 16x8 / 8x16 partitions), through mc_luma (inter.rs:1193). */
+static void mb_pred_for_pick(const uint8_t *ref, int cw, int ch, int mbx, int mby, const int32_t *pick, uint8_t pred[256]) {
+    int shape = pick[0];
+    uint8_t part[256];
+    if (shape == 0) {
+        or_mc_luma(ref, cw, ch, mbx * 16, mby * 16, 16, 16, pick[1], pick[2], pred);
+        return;
+    }
+    for (int k = 0; k < 2; k++) {
+        int ox = shape == 2 ? 8 * k : 0, oy = shape == 1 ? 8 * k : 0;
+        int bw = shape == 2 ? 8 : 16, bh = shape == 1 ? 8 : 16;
+        or_mc_luma(ref, cw, ch, mbx * 16 + ox, mby * 16 + oy, bw, bh, pick[1 + 2 * k], pick[2 + 2 * k], part);
+        for (int r = 0; r < bh; r++) memcpy(pred + (oy + r) * 16 + ox, part + r * bw, bw);
+    }
+}
+
+/* MC + luma T/Q of every MB of one frame from its picks. */
+void or_mc_tq_frame(const uint8_t *src, const uint8_t *ref, int cw, int ch, const int32_t *picks, int qp, int dz_div,
+                    int16_t *coeffs /* 256 per MB */) {
+    int mb_w = cw / 16, mb_h = ch / 16;
+    for (int mby = 0; mby < mb_h; mby++)
+        for (int mbx = 0; mbx < mb_w; mbx++) {
+            int m = mby * mb_w + mbx;
+            uint8_t pred[256];
+            mb_pred_for_pick(ref, cw, ch, mbx, mby, picks + 6 * m, pred);
+            or_mb_luma_tq(src + (int64_t)mby * 16 * cw + mbx * 16, cw, pred, qp, dz_div, coeffs + (int64_t)m * 256);
+        }
+}
+
+typedef struct {
+    const uint8_t *frames;
+    uint8_t *half;
+    int cw, ch, cwh, chh, mb_w, mb_h, nmb;
+    size_t fs, hs;
+    int mode;
+    int32_t *intra, *inter, *mvs;
+} la_args;
+
+static void la_down(void *p, int f, int tid) {
+    la_args *a = (la_args *)p;
+    (void)tid;
+    or_downsample2x(a->frames + a->fs * f, a->cw, a->ch, a->half + a->hs * f);
+}
+
+static void la_costs(void *p, int f, int tid) {
+    la_args *a = (la_args *)p;
+    (void)tid;
+    or_frame_costs(a->frames + a->fs * f, a->cw, a->ch, a->half + a->hs * f, a->cwh, a->chh, a->mb_w, a->mb_h,
+                   f > 0 ? a->frames + a->fs * (f - 1) : NULL, f > 0 ? a->half + a->hs * (f - 1) : NULL, a->mode,
+                   a->intra + (size_t)a->nmb * f, a->inter + (size_t)a->nmb * f, a->mvs + (size_t)2 * a->nmb * f);
+}
+
+/* HalfRes lookahead of a whole clip (mbtree.rs:413-436 for mode HalfRes). */
+void or_lookahead_clip(const uint8_t *frames, int nframes, int cw, int ch, int mode, int32_t *intra, int32_t *inter,
+                       int32_t *mvs, int nthreads) {
+    int mb_w = cw / 16, mb_h = ch / 16, nmb = mb_w * mb_h;
+    int cwh = cw / 2, chh = ch / 2;
+    size_t fs = (size_t)cw * ch, hs = (size_t)cwh * chh;
+    uint8_t *half = (uint8_t *)malloc(hs * nframes);
+    la_args a = {frames, half, cw, ch, cwh, chh, mb_w, mb_h, nmb, fs, hs, mode, intra, inter, mvs};
+    par_for(nframes, nthreads, la_down, &a);
+    par_for(nframes, nthreads, la_costs, &a);
+    free(half);
+}
+
+typedef struct {
+    const uint8_t *frames;
+    int cw, ch, pad;
+    const or_me_params_flat *pf;
+    const uint16_t *tab;
+    double lambda_me;
+    int64_t split_gate;
+    int qp, dz_div;
+    int32_t *picks;
+    int64_t *costs;
+    int16_t *coeffs;
+    int nmb;
+    size_t fs, p4;
+} pp_args;
+
+static void pp_frame(void *p, int i, int tid) {
+    pp_args *a = (pp_args *)p;
+    (void)tid;
+    int f = i + 1;
+    uint8_t *planes = (uint8_t *)malloc(a->p4);
+    const uint8_t *ref = a->frames + a->fs * (f - 1), *src = a->frames + a->fs * f;
+    or_build_planes4(ref, a->cw, a->ch, a->pad, planes);
+    or_me_frame_flat(src, ref, planes, a->cw, a->ch, a->pad, a->pf, a->tab, a->lambda_me, a->split_gate,
+                     a->picks + (size_t)6 * a->nmb * f, a->costs + (size_t)2 * a->nmb * f);
+    or_mc_tq_frame(src, ref, a->cw, a->ch, a->picks + (size_t)6 * a->nmb * f, a->qp, a->dz_div,
+                   a->coeffs + (size_t)256 * a->nmb * f);
+    free(planes);
+}
+
+/* The whole pixel path over a clip: planes, ME, MC+T/Q (frames 1..n-1) and the
+ * lookahead (all frames).  Outputs are per frame; frame 0 rows are zero. */
+void or_pixel_path_clip(const uint8_t *frames, int nframes, int cw, int ch, int pad, const or_me_params_flat *pf,
+                        const uint16_t *tab, double lambda_me, int64_t split_gate, int qp, int dz_div,
+                        int32_t *picks, int64_t *costs, int16_t *coeffs, int32_t *la_intra, int32_t *la_inter,
+                        int32_t *la_mvs, int nthreads) {
+    int nmb = (cw / 16) * (ch / 16);
+    size_t fs = (size_t)cw * ch;
+    int pw = cw + 2 * pad, ph = ch + 2 * pad;
+    size_t p4 = (size_t)4 * pw * ph;
+    memset(picks, 0, sizeof(int32_t) * 6 * nmb);
+    memset(costs, 0, sizeof(int64_t) * 2 * nmb);
+    memset(coeffs, 0, sizeof(int16_t) * 256 * nmb);
+    pp_args a = {frames, cw, ch, pad, pf, tab, lambda_me, split_gate, qp, dz_div, picks, costs, coeffs, nmb, fs, p4};
+    par_for(nframes - 1, nthreads, pp_frame, &a);
+    or_lookahead_clip(frames, nframes, cw, ch, 2, la_intra, la_inter, la_mvs, nthreads);
+}

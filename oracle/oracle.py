@@ -1,0 +1,217 @@
+"""ctypes wrapper of the CPU oracle (oracle/liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: tests/, __graft_entry__.smoke() and bench.py's
+CPU-baseline leg are the only callers.  The product (rusty_h264_b200) never
+imports this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+
+u8p = C.POINTER(C.c_uint8)
+i16p = C.POINTER(C.c_int16)
+i32p = C.POINTER(C.c_int32)
+i64p = C.POINTER(C.c_int64)
+u16p = C.POINTER(C.c_uint16)
+
+
+class MeParamsFlat(C.Structure):
+    """Mirror of or_me_params_flat (oracle/h264_oracle_par.c)."""
+
+    _fields_ = [
+        ("fast", C.c_int32), ("mb_use_satd", C.c_int32), ("sadfp", C.c_int32), ("mv_cost_kind", C.c_int32),
+        ("sadfp_lambda", C.c_double),
+        ("me_snap", C.c_int32), ("me_fc", C.c_int32),
+        ("dia_mask", C.c_uint32), ("dia_sub_mask", C.c_uint32),
+        ("subpel", C.c_int32), ("subpel_pat", C.c_int32), ("sp_single_pass", C.c_int32), ("sub_pat", C.c_int32),
+        ("me_subpel_iter", C.c_int32), ("sp_maxit", C.c_int32), ("sp_fc", C.c_int32),
+    ]
+
+
+def balanced_params(**kw) -> MeParamsFlat:
+    """The Balanced-preset motion_search settings (config.rs:448-571 defaults)."""
+    p = MeParamsFlat(fast=0, mb_use_satd=0, sadfp=0, mv_cost_kind=0, sadfp_lambda=0.5, me_snap=1, me_fc=1,
+                     dia_mask=0b11100, dia_sub_mask=0b10000, subpel=1, subpel_pat=-1, sp_single_pass=1, sub_pat=2,
+                     me_subpel_iter=1, sp_maxit=0, sp_fc=0)
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def build() -> str:
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB_PATH
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = C.CDLL(LIB_PATH)
+        L.or_satd4x4_wels.restype = C.c_int32
+        L.or_satd_region_wels.restype = C.c_int32
+        L.or_sad.restype = C.c_int32
+        L.or_satd_px.restype = C.c_int64
+        L.or_satd_avg.restype = C.c_uint32
+        L.or_sad_avg.restype = C.c_int64
+        L.or_median3.restype = C.c_int32
+        L.or_luma_sample.restype = C.c_int32
+        L.or_mvbits.restype = C.c_uint32
+        L.or_mc_satd_hp.restype = C.c_int64
+        L.or_mc_sad_hp.restype = C.c_int64
+        L.or_intra_cost.restype = C.c_int32
+        L.or_la_mc_satd.restype = C.c_int64
+        L.or_candidate_dist.restype = C.c_int64
+        L.or_num_threads.restype = C.c_int
+        L.or_motion_search_flat.argtypes = [u8p, u8p, u8p, C.c_int, C.c_int, C.c_int, C.POINTER(MeParamsFlat), u16p,
+                                            C.c_int, C.c_int, C.c_int, C.c_int, i32p, C.c_int, C.c_double, i32p,
+                                            i32p, i64p, i32p]
+        L.or_me_frame_flat.argtypes = [u8p, u8p, u8p, C.c_int, C.c_int, C.c_int, C.POINTER(MeParamsFlat), u16p,
+                                       C.c_double, C.c_int64, i32p, i64p]
+        L.or_pixel_path_clip.argtypes = [u8p, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(MeParamsFlat), u16p,
+                                         C.c_double, C.c_int64, C.c_int, C.c_int, i32p, i64p, i16p, i32p, i32p, i32p,
+                                         C.c_int]
+        _lib = L
+    return _lib
+
+
+def ptr(a: np.ndarray, t=u8p):
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(t)
+
+
+# ---- convenience wrappers ---------------------------------------------------
+
+def satd_px(src, ss, pred, ps, w, h) -> int:
+    return lib().or_satd_px(ptr(src), ss, ptr(pred), ps, w, h)
+
+
+def pad_plane(y: np.ndarray, pad: int) -> np.ndarray:
+    h, w = y.shape
+    f = np.empty((h + 2 * pad, w + 2 * pad), np.uint8)
+    lib().or_pad_plane(ptr(np.ascontiguousarray(y)), w, h, pad, ptr(f))
+    return f
+
+
+def hpel_fused(f: np.ndarray):
+    ph, pw = f.shape
+    h, v, c = (np.empty_like(f) for _ in range(3))
+    lib().or_hpel_fused(ptr(f), pw, ph, ptr(h), ptr(v), ptr(c))
+    return h, v, c
+
+
+def hpel_tiles(f: np.ndarray):
+    ph, pw = f.shape
+    h, v, c = (np.empty_like(f) for _ in range(3))
+    lib().or_hpel_tiles(ptr(f), pw, ph, ptr(h), ptr(v), ptr(c))
+    return h, v, c
+
+
+def build_planes4(y: np.ndarray, pad: int = 32) -> np.ndarray:
+    """F|H|V|C padded planes of a luma frame, shape (4, ph, pw)."""
+    ch, cw = y.shape
+    out = np.empty((4, ch + 2 * pad, cw + 2 * pad), np.uint8)
+    lib().or_build_planes4(ptr(np.ascontiguousarray(y)), cw, ch, pad, ptr(out))
+    return out
+
+
+def mc_luma(ref: np.ndarray, x0, y0, bw, bh, mvx, mvy) -> np.ndarray:
+    ch, cw = ref.shape
+    out = np.empty((bh, bw), np.uint8)
+    lib().or_mc_luma(ptr(ref), cw, ch, x0, y0, bw, bh, mvx, mvy, ptr(out))
+    return out
+
+
+def luma_sample(ref: np.ndarray, ix, iy, fx, fy) -> int:
+    ch, cw = ref.shape
+    return lib().or_luma_sample(ptr(ref), cw, ch, ix, iy, fx, fy)
+
+
+def mv_cost_table() -> np.ndarray:
+    t = np.empty(4096, np.uint16)
+    lib().or_build_mv_cost(ptr(t, u16p))
+    return t
+
+
+def motion_search(src, ref, planes4, params, lx, ly, rw, rh, preds, lambda_me, start=None, tab=None, pad=32):
+    ch, cw = src.shape
+    pr = np.ascontiguousarray(np.asarray(preds, np.int32).reshape(-1))
+    mv = np.zeros(2, np.int32)
+    cost = np.zeros(1, np.int64)
+    ev = np.zeros(1, np.int32)
+    st = None if start is None else np.asarray(start, np.int32)
+    tab = mv_cost_table() if tab is None else tab
+    lib().or_motion_search_flat(ptr(src), ptr(ref), ptr(planes4), cw, ch, pad, C.byref(params), ptr(tab, u16p),
+                                lx, ly, rw, rh, ptr(pr, i32p), len(pr) // 2, float(lambda_me),
+                                None if st is None else ptr(st, i32p), ptr(mv, i32p), ptr(cost, i64p), ptr(ev, i32p))
+    return (int(mv[0]), int(mv[1])), int(cost[0]), int(ev[0])
+
+
+def candidate_dist(src, ref, planes4, kind, lx, ly, rw, rh, mvx, mvy, pad=32) -> int:
+    ch, cw = src.shape
+    return lib().or_candidate_dist(ptr(src), ptr(ref), ptr(planes4), cw, ch, pad, kind, lx, ly, rw, rh, mvx, mvy)
+
+
+def me_frame(src, ref, planes4, params, lambda_me, split_gate=-1, tab=None, pad=32):
+    ch, cw = src.shape
+    nmb = (cw // 16) * (ch // 16)
+    picks = np.zeros((nmb, 6), np.int32)
+    costs = np.zeros((nmb, 2), np.int64)
+    tab = mv_cost_table() if tab is None else tab
+    lib().or_me_frame_flat(ptr(src), ptr(ref), ptr(planes4), cw, ch, pad, C.byref(params), ptr(tab, u16p),
+                           float(lambda_me), int(split_gate), ptr(picks, i32p), ptr(costs, i64p))
+    return picks, costs
+
+
+def mc_tq_frame(src, ref, picks, qp, dz_div=6):
+    ch, cw = src.shape
+    nmb = (cw // 16) * (ch // 16)
+    out = np.zeros((nmb, 256), np.int16)
+    lib().or_mc_tq_frame(ptr(src), ptr(ref), cw, ch, ptr(np.ascontiguousarray(picks), i32p), qp, dz_div,
+                         ptr(out, i16p))
+    return out
+
+
+def downsample2x(y):
+    ch, cw = y.shape
+    out = np.empty((ch // 2, cw // 2), np.uint8)
+    lib().or_downsample2x(ptr(np.ascontiguousarray(y)), cw, ch, ptr(out))
+    return out
+
+
+def lookahead_clip(frames: np.ndarray, mode=2, nthreads=1):
+    n, ch, cw = frames.shape
+    nmb = (cw // 16) * (ch // 16)
+    intra = np.zeros((n, nmb), np.int32)
+    inter = np.zeros((n, nmb), np.int32)
+    mvs = np.zeros((n, nmb, 2), np.int32)
+    lib().or_lookahead_clip(ptr(np.ascontiguousarray(frames)), n, cw, ch, mode, ptr(intra, i32p), ptr(inter, i32p),
+                            ptr(mvs, i32p), nthreads)
+    return intra, inter, mvs
+
+
+def pixel_path_clip(frames: np.ndarray, params, lambda_me, split_gate, qp, dz_div=6, pad=32, nthreads=1, tab=None):
+    n, ch, cw = frames.shape
+    nmb = (cw // 16) * (ch // 16)
+    picks = np.zeros((n, nmb, 6), np.int32)
+    costs = np.zeros((n, nmb, 2), np.int64)
+    coeffs = np.zeros((n, nmb, 256), np.int16)
+    intra = np.zeros((n, nmb), np.int32)
+    inter = np.zeros((n, nmb), np.int32)
+    mvs = np.zeros((n, nmb, 2), np.int32)
+    tab = mv_cost_table() if tab is None else tab
+    lib().or_pixel_path_clip(ptr(np.ascontiguousarray(frames)), n, cw, ch, pad, C.byref(params), ptr(tab, u16p),
+                             float(lambda_me), int(split_gate), qp, dz_div, ptr(picks, i32p), ptr(costs, i64p),
+                             ptr(coeffs, i16p), ptr(intra, i32p), ptr(inter, i32p), ptr(mvs, i32p), nthreads)
+    return dict(picks=picks, costs=costs, coeffs=coeffs, la_intra=intra, la_inter=inter, la_mvs=mvs)

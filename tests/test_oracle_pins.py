@@ -1,0 +1,379 @@
+"""Pins the CPU oracle to the reference's own tests (CPU only, no GPU).
+
+Each test ports one reference test (file:line in its docstring) with the same
+corpus or LCG stream, checking the oracle against either the reference's
+literal expected values (tests/golden/reference_known_answers.json) or an
+independent numpy restatement of the formula that reference test spells out.
+Where the reference loops tens of thousands of times, the first part of the
+identical stream is used so the CPU suite stays fast.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests._lcg import Lcg32, Lcg64
+
+GOLD = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "reference_known_answers.json")))
+
+H4 = np.array([[1, 1, 1, 1], [1, 1, -1, -1], [1, -1, -1, 1], [1, -1, 1, -1]], np.int64)
+CF = np.array([[1, 1, 1, 1], [2, 1, -1, -2], [1, -1, -1, 1], [1, -2, 2, -1]], np.int64)
+
+
+def np_satd_sum(src, pred):
+    """Σ|H·d·Hᵀ| over the 4x4 blocks of (src - pred): the scalar satd_px."""
+    d = src.astype(np.int64) - pred.astype(np.int64)
+    h, w = d.shape
+    tot = 0
+    for by in range(0, h, 4):
+        for bx in range(0, w, 4):
+            tot += int(np.abs(H4 @ d[by:by + 4, bx:bx + 4] @ H4.T).sum())
+    return tot
+
+
+def np_wels(src, pred):
+    """openh264's region SATD: Σ_4x4 ((Σ|H·d|+1)>>1) (x86_asm.rs satd_region_ref)."""
+    d = src.astype(np.int64) - pred.astype(np.int64)
+    h, w = d.shape
+    tot = 0
+    for by in range(0, h, 4):
+        for bx in range(0, w, 4):
+            tot += (int(np.abs(H4 @ d[by:by + 4, bx:bx + 4] @ H4.T).sum()) + 1) >> 1
+    return tot
+
+
+def corpus(seed):
+    """satd_sad.rs:389-400 / x86_asm.rs:306-314 structured corpus."""
+    i = np.arange(16)[:, None]
+    j = np.arange(16)[None, :]
+    a = ((i * 37 + j * 101 + seed * 3) & 0xFF).astype(np.uint8)
+    b = ((i * 53 + j * 17 + seed * 29 + 7) & 0xFF).astype(np.uint8)
+    return np.ascontiguousarray(a), np.ascontiguousarray(b)
+
+
+def test_satd_sad_family_matches_openh264_formula():
+    """satd_sad.rs:403-427, x86_asm.rs:303-323: every shape vs the openh264-C formula."""
+    L = O.lib()
+    for seed in range(96):
+        a, b = corpus(seed)
+        for w, h in [(16, 16), (16, 8), (8, 16), (8, 8), (4, 4)]:
+            got = L.or_satd_region_wels(O.ptr(a), 16, O.ptr(b), 16, w, h)
+            assert got == np_wels(a[:h, :w], b[:h, :w]), (seed, w, h)
+        for w, h in [(16, 16), (16, 8), (8, 16)]:
+            got = L.or_sad(O.ptr(a), 16, O.ptr(b), 16, w, h)
+            assert got == int(np.abs(a[:h, :w].astype(int) - b[:h, :w].astype(int)).sum())
+
+
+def test_satd_extremes():
+    """satd_sad.rs:430-452: saturated and alternating blocks."""
+    L = O.lib()
+    for va, vb in [(0, 255), (255, 0), (0, 0), (255, 255)]:
+        a = np.full((16, 16), va, np.uint8)
+        b = np.full((16, 16), vb, np.uint8)
+        assert L.or_satd_region_wels(O.ptr(a), 16, O.ptr(b), 16, 16, 16) == np_wels(a, b)
+    i = np.arange(16)[:, None]
+    j = np.arange(16)[None, :]
+    a = np.ascontiguousarray(np.where((i + j) % 2 == 0, 255, 0).astype(np.uint8))
+    b = np.ascontiguousarray(np.broadcast_to(np.where(i % 2 == 0, 0, 255), (16, 16)).astype(np.uint8))
+    assert L.or_satd_region_wels(O.ptr(a), 16, O.ptr(b), 16, 16, 16) == np_wels(a, b)
+    assert L.or_satd_region_wels(O.ptr(a), 16, O.ptr(b), 16, 8, 8) == np_wels(a[:8, :8], b[:8, :8])
+
+
+def test_satd_px_is_exactly_twice_wels():
+    """encoder tests/satd_asm_compare.rs:38-75: 2·Wels == Σ|H·d| (seed 0x1234_5678_9abc_def0)."""
+    st = Lcg64(0x1234_5678_9ABC_DEF0)
+    L = O.lib()
+    for n in (4, 8, 16):
+        for _ in range(600):
+            src = st.bytes(n * n).reshape(n, n).copy()
+            pred = st.bytes(n * n).reshape(n, n).copy()
+            rust = np_satd_sum(src, pred)
+            wels = L.or_satd_region_wels(O.ptr(src), n, O.ptr(pred), n, n, n)
+            assert 2 * wels == rust
+            assert O.satd_px(src, n, pred, n, n, n) == rust
+
+
+def test_satd_avg_matches_materialized():
+    """encoder tests/satd_avg_compare.rs:129-170 (seed 0xabcd_ef01_2345_6789), every x4 shape."""
+    st = Lcg64(0xABCD_EF01_2345_6789)
+    L = O.lib()
+    for _ in range(150):
+        ss = 16 + int(st.next()) % 32
+        rs = 16 + int(st.next()) % 32
+        src = st.bytes(15 * ss + 16 + 8)
+        planes = [st.bytes(15 * rs + 16 + 4 * rs + 64) for _ in range(3)]
+        idx = [(int(st.next()) % 3, (int(st.next()) % 4) * rs + int(st.next()) % 32,
+                int(st.next()) % 3, (int(st.next()) % 4) * rs + int(st.next()) % 32) for _ in range(4)]
+        for (pa, oa, pb, ob) in idx:
+            for w, h in [(16, 16), (16, 8), (8, 16), (8, 8)]:
+                A = planes[pa][oa:]
+                B = planes[pb][ob:]
+                got = L.or_satd_avg(O.ptr(src), ss, O.ptr(np.ascontiguousarray(A)), O.ptr(np.ascontiguousarray(B)),
+                                    rs, w, h)
+                s2 = np.lib.stride_tricks.as_strided(src, (h, w), (ss, 1))
+                a2 = np.lib.stride_tricks.as_strided(A, (h, w), (rs, 1)).astype(np.int32)
+                b2 = np.lib.stride_tricks.as_strided(B, (h, w), (rs, 1)).astype(np.int32)
+                avg = ((a2 + b2 + 1) >> 1).astype(np.uint8)
+                assert got == np_satd_sum(s2, avg)
+
+
+def test_quant_mf_oh_table_matches_reference_rows():
+    """transform.rs:1447-1500: derived MF table == the reference's literal 52 rows."""
+    L = O.lib()
+    rows = GOLD["quant_mf_oh"]["rows"]
+    for qp in range(52):
+        mf = np.zeros(8, np.int16)
+        L.or_quant_mf_oh(qp, O.ptr(mf, O.i16p))
+        assert mf.tolist() == rows[qp], qp
+
+
+def test_quant_four_matches_wels_new_quant():
+    """transform_quant.rs:199-222 and x86_asm.rs:325-352 with the fixed FF/MF vectors."""
+    g = GOLD["quant_four_fixed"]
+    ff = np.array(g["ff"], np.int16)
+    mf = np.array(g["mf"], np.int16)
+    L = O.lib()
+    for seed in range(64):
+        k = np.arange(64)
+        inp = (((k * 37 + seed * 53) % 2000) - 1000).astype(np.int16)
+        got = inp.copy()
+        L.or_quant_four_4x4(O.ptr(got, O.i16p), O.ptr(ff, O.i16p), O.ptr(mf, O.i16p))
+        row = (k % 16) // 4
+        col = k % 4
+        pos = (row & 1) * 4 + col
+        c = inp.astype(np.int64)
+        lvl = ((np.abs(c) + ff[pos]) * mf[pos]) >> 16
+        want = np.where(c < 0, -lvl, lvl).astype(np.int16)
+        assert np.array_equal(got, want), seed
+
+
+def test_quant_four_full_range_lcg():
+    """transform_quant.rs:591-617 (seed 0x1234): full i16 range incl. i16::MIN."""
+    st = Lcg64(0x1234)
+    L = O.lib()
+    for rnd in range(300):
+        ffmf = (st.bulk(16) % np.uint64(32768)).astype(np.int16)
+        ff = np.ascontiguousarray(ffmf[0::2])
+        mf = np.ascontiguousarray(ffmf[1::2])
+        inp = (st.bulk(64) & np.uint64(0xFFFF)).astype(np.uint16).view(np.int16).copy()
+        if rnd == 0:
+            inp[0], inp[1], inp[2] = -32768, 32767, 0
+        got = inp.copy()
+        L.or_quant_four_4x4(O.ptr(got, O.i16p), O.ptr(ff, O.i16p), O.ptr(mf, O.i16p))
+        k = np.arange(64)
+        pos = (((k % 16) // 4) & 1) * 4 + k % 4
+        c = inp.astype(np.int64)
+        lvl = (((np.abs(c) + ff[pos].astype(np.int64)) * mf[pos].astype(np.int64)) >> 16).astype(np.int64)
+        want = np.where(c < 0, -lvl, lvl).astype(np.int64).astype(np.int16)
+        assert np.array_equal(got, want), rnd
+
+
+def test_dct_four_t4_matches_forward_core_formula():
+    """transform_quant.rs:141-166: dct_four_t4 == Cf·X·Cfᵀ per sub-block, openh264 order."""
+    L = O.lib()
+    y = np.arange(8)[:, None]
+    x = np.arange(8)[None, :]
+    for seed in range(128):
+        src = np.ascontiguousarray(((y * 31 + x * 17 + seed * 7) & 0xFF).astype(np.uint8))
+        pred = np.ascontiguousarray(((y * 13 + x * 41 + seed * 5 + 9) & 0xFF).astype(np.uint8))
+        dct = np.zeros(64, np.int16)
+        L.or_dct_four_t4(O.ptr(dct, O.i16p), O.ptr(src), 8, O.ptr(pred), 8)
+        for k, (ox, oy) in enumerate([(0, 0), (4, 0), (0, 4), (4, 4)]):
+            d = src[oy:oy + 4, ox:ox + 4].astype(np.int64) - pred[oy:oy + 4, ox:ox + 4]
+            want = (CF @ d @ CF.T).reshape(-1)
+            assert np.array_equal(dct[k * 16:(k + 1) * 16], want.astype(np.int16)), (seed, k)
+
+
+def test_dct_lcg_stream_and_saturated_round():
+    """transform_quant.rs:620-640 (seed 0xbeef): random src/pred incl. the 255-vs-0 round."""
+    st = Lcg64(0xBEEF)
+    L = O.lib()
+    for rnd in range(300):
+        sp = st.bytes(128)
+        src = np.ascontiguousarray(sp[0::2].reshape(8, 8))
+        pred = np.ascontiguousarray(sp[1::2].reshape(8, 8))
+        if rnd == 0:
+            src[:] = 255
+            pred[:] = 0
+        dct = np.zeros(64, np.int16)
+        L.or_dct_four_t4(O.ptr(dct, O.i16p), O.ptr(src), 8, O.ptr(pred), 8)
+        for k, (ox, oy) in enumerate([(0, 0), (4, 0), (0, 4), (4, 4)]):
+            d = src[oy:oy + 4, ox:ox + 4].astype(np.int64) - pred[oy:oy + 4, ox:ox + 4]
+            assert np.array_equal(dct[k * 16:(k + 1) * 16], (CF @ d @ CF.T).reshape(-1).astype(np.int16))
+
+
+def test_forward_transforms_flat_known_answers():
+    """transform.rs:1167-1188: flat 4x4 -> DC 64, flat 8x8 -> DC 256, AC zero."""
+    L = O.lib()
+    g4 = GOLD["forward_core_flat"]
+    out = np.zeros(16, np.int32)
+    L.or_forward_core(O.ptr(np.array(g4["input"], np.int32), O.i32p), O.ptr(out, O.i32p))
+    assert out[0] == g4["dc"] and not out[1:].any()
+    g8 = GOLD["forward_core_8x8_flat"]
+    out8 = np.zeros(64, np.int32)
+    L.or_forward_core_8x8(O.ptr(np.array(g8["input"], np.int32), O.i32p), O.ptr(out8, O.i32p))
+    assert out8[0] == g8["dc"] and not out8[1:].any()
+
+
+def test_quantize_structure_matches_quant_four():
+    """transform.rs:121-139: quantize == quant_four_4x4 with quant_dz_ff + QUANT_MF_OH."""
+    L = O.lib()
+    rng = np.random.default_rng(7)
+    for qp in range(52):
+        c = rng.integers(-4080, 4081, 16).astype(np.int32)
+        out = np.zeros(16, np.int32)
+        L.or_quantize(O.ptr(c, O.i32p), qp, 6, O.ptr(out, O.i32p))
+        ff = np.zeros(8, np.int16)
+        mf = np.zeros(8, np.int16)
+        L.or_quant_dz_ff(qp, 6, O.ptr(ff, O.i16p))
+        L.or_quant_mf_oh(qp, O.ptr(mf, O.i16p))
+        d = np.zeros(64, np.int16)
+        d[:16] = c
+        L.or_quant_four_4x4(O.ptr(d, O.i16p), O.ptr(ff, O.i16p), O.ptr(mf, O.i16p))
+        assert np.array_equal(out, d[:16].astype(np.int32))
+
+
+def test_median_and_mv_prediction_known_answers():
+    """inter.rs:1994-2034."""
+    L = O.lib()
+    for a, b, c, want in GOLD["median3"]["cases"]:
+        assert L.or_median3(a, b, c) == want
+    for case in GOLD["predict_mv"]["cases"]:
+        arrs = [np.array(case[k], np.int32) for k in ("a", "b", "c")]
+        out = np.zeros(2, np.int32)
+        L.or_predict_mv(*[O.ptr(x, O.i32p) for x in arrs], case["cur_ref"], O.ptr(out, O.i32p))
+        assert out.tolist() == case["want"], case
+
+
+def test_mc_luma_known_answers():
+    """inter.rs:2037-2063: zero-MV copy, edge clamp, flat stays flat."""
+    for case in GOLD["mc_luma"]["cases"]:
+        ref = np.array(case["ref"], np.uint8).reshape(case["ch"], case["cw"])
+        got = O.mc_luma(ref, case["x0"], case["y0"], case["bw"], case["bh"], case["mvx"], case["mvy"])
+        assert got.reshape(-1).tolist() == case["want"]
+    fl = GOLD["mc_luma"]["flat"]
+    ref = np.full((fl["ch"], fl["cw"]), fl["value"], np.uint8)
+    for fx, fy in fl["phases"]:
+        got = O.mc_luma(ref, fl["x0"], fl["y0"], fl["bw"], fl["bh"], fx, fy)
+        assert (got == fl["value"]).all()
+
+
+def np_luma_sample_block(ref, x0, y0, bw, bh, mvx, mvy):
+    """luma_sample (inter.rs:134-176) vectorised over a block: the spec §8.4.2.2.1 oracle."""
+    ch, cw = ref.shape
+    ix0, iy0 = x0 + (mvx >> 2), y0 + (mvy >> 2)
+    fx, fy = mvx & 3, mvy & 3
+    yy = iy0 + np.arange(bh)[:, None]
+    xx = ix0 + np.arange(bw)[None, :]
+    R = ref.astype(np.int64)
+
+    def g(dx, dy):
+        return R[np.clip(yy + dy, 0, ch - 1), np.clip(xx + dx, 0, cw - 1)]
+
+    def hor6(dy):
+        return g(-2, dy) - 5 * g(-1, dy) + 20 * g(0, dy) + 20 * g(1, dy) - 5 * g(2, dy) + g(3, dy)
+
+    def ver6(dx):
+        return g(dx, -2) - 5 * g(dx, -1) + 20 * g(dx, 0) + 20 * g(dx, 1) - 5 * g(dx, 2) + g(dx, 3)
+
+    clip = lambda v: np.clip(v, 0, 255)
+    if fx == 0 and fy == 0:
+        return g(0, 0)
+    b = clip((hor6(0) + 16) >> 5)
+    h = clip((ver6(0) + 16) >> 5)
+    m = clip((ver6(1) + 16) >> 5)
+    s = clip((hor6(1) + 16) >> 5)
+    j = clip((hor6(-2) - 5 * hor6(-1) + 20 * hor6(0) + 20 * hor6(1) - 5 * hor6(2) + hor6(3) + 512) >> 10)
+    av = lambda p, q: (p + q + 1) >> 1
+    return {
+        (1, 0): av(g(0, 0), b), (2, 0): b, (3, 0): av(g(1, 0), b),
+        (0, 1): av(g(0, 0), h), (1, 1): av(b, h), (2, 1): av(b, j), (3, 1): av(b, m),
+        (0, 2): h, (1, 2): av(h, j), (2, 2): j, (3, 2): av(j, m),
+        (0, 3): av(g(0, 1), h), (1, 3): av(h, s), (2, 3): av(j, s), (3, 3): av(m, s),
+    }[(fx, fy)]
+
+
+def test_mc_luma_block_kernels_match_per_pixel_spec():
+    """inter.rs:1914-1947 (40x32, LCG32 0x1357_9bdf): mc_luma == luma_sample, interior and edge."""
+    st = Lcg32(0x1357_9BDF)
+    cw, ch = 40, 32
+    ref = np.array([(st.next() >> 24) & 0xFF for _ in range(cw * ch)], np.uint8).reshape(ch, cw)
+    for bw, bh in [(16, 16), (8, 8), (4, 4), (8, 16), (16, 8)]:
+        for x0, y0 in [(8, 8), (0, 0), (cw - bw, ch - bh)]:
+            for mvx in range(-9, 10):
+                for mvy in range(-9, 10):
+                    got = O.mc_luma(ref, x0, y0, bw, bh, mvx, mvy)
+                    want = np_luma_sample_block(ref, x0, y0, bw, bh, mvx, mvy)
+                    assert np.array_equal(got, want), (bw, bh, x0, y0, mvx, mvy)
+
+
+def test_luma_sample_oracle_matches_numpy_spec():
+    """The C luma_sample restatement agrees with the vectorised spec form."""
+    rng = np.random.default_rng(3)
+    ref = rng.integers(0, 256, (24, 20), dtype=np.uint8)
+    for fx in range(4):
+        for fy in range(4):
+            for ix, iy in [(-5, -5), (0, 0), (7, 9), (19, 23), (25, 30)]:
+                want = np_luma_sample_block(ref, ix, iy, 1, 1, fx, fy)[0, 0]
+                assert O.luma_sample(ref, ix, iy, fx, fy) == want
+
+
+def np_hpel_planes(f):
+    """H/V/C from the padded plane with taps clamped to the plane (inter.rs:908-991)."""
+    ph, pw = f.shape
+    F = f.astype(np.int64)
+    ys = np.arange(ph)[:, None]
+    xs = np.arange(pw)[None, :]
+    tap = [1, -5, 20, 20, -5, 1]
+
+    def at(dy, dx):
+        return F[np.clip(ys + dy, 0, ph - 1), np.clip(xs + dx, 0, pw - 1)]
+
+    Hs = sum(t * at(0, k - 2) for k, t in enumerate(tap))
+    Vs = sum(t * at(k - 2, 0) for k, t in enumerate(tap))
+    # centre: horizontal 6-tap over the clamped-column vertical intermediates
+    vt = sum(t * F[np.clip(np.arange(ph) + k - 2, 0, ph - 1)] for k, t in enumerate(tap))  # ph x pw
+    Cs = sum(t * vt[:, np.clip(np.arange(pw) + k - 2, 0, pw - 1)] for k, t in enumerate(tap))
+    clip = lambda v: np.clip(v, 0, 255).astype(np.uint8)
+    return clip((Hs + 16) >> 5), clip((Vs + 16) >> 5), clip((Cs + 512) >> 10)
+
+
+def test_fused_hpel_builder_matches_tiles():
+    """inter.rs:1824-1868 (LCG64 0x5eed_f00d_dead_beef): fused == tiles == spec, 3 geometries."""
+    st = Lcg64(0x5EED_F00D_DEAD_BEEF)
+    for cw, ch, pad in [(64, 48, 16), (80, 64, 12), (176, 144, 32)]:
+        ref = st.bytes(cw * ch).reshape(ch, cw).copy()
+        f = O.pad_plane(ref, pad)
+        h1, v1, c1 = O.hpel_tiles(f)
+        h2, v2, c2 = O.hpel_fused(f)
+        assert np.array_equal(h1, h2) and np.array_equal(v1, v2) and np.array_equal(c1, c2)
+        h3, v3, c3 = np_hpel_planes(f)
+        assert np.array_equal(h2, h3) and np.array_equal(v2, v3) and np.array_equal(c2, c3)
+
+
+def test_hpel_block_matches_mc_luma():
+    """inter.rs:1871-1911 (96x64, LCG32 0x9E37_79B9): plane reads == mc_luma (strided sample)."""
+    st = Lcg32(0x9E37_79B9)
+    cw, ch = 96, 64
+    ref = np.array([(st.next() >> 24) & 0xFF for _ in range(cw * ch)], np.uint8).reshape(ch, cw)
+    planes = O.build_planes4(ref, 32)
+    src = ref.copy()
+    checked = 0
+    for bw, bh in [(16, 16), (16, 8), (8, 16), (8, 8), (8, 4), (4, 8), (4, 4)]:
+        for fy in range(4):
+            for fx in range(4):
+                if fx == 0 and fy == 0:
+                    continue
+                for y0 in range(0, ch - bh, 21):
+                    for x0 in range(0, cw - bw, 25):
+                        for dx, dy in [(0, 0), (4, 0), (-4, -4), (8, 8), (-64, -64), (96, 40), (40, -96)]:
+                            mvx, mvy = dx + fx, dy + fy
+                            # mc_satd_hp takes the plane arms where they apply and mc_luma
+                            # elsewhere; its SATD must equal SATD against mc_luma's block.
+                            want = O.mc_luma(ref, x0, y0, bw, bh, mvx, mvy)
+                            d = O.candidate_dist(src, ref, planes, 0, x0, y0, bw, bh, mvx, mvy)
+                            assert d == np_satd_sum(src[y0:y0 + bh, x0:x0 + bw], want)
+                            checked += 1
+    assert checked > 2000
