@@ -1,0 +1,373 @@
+"""Benchmark of the encoder pixel hot path on B200.
+
+Workload (one step): the 1080p synthetic clip (1920x1080 coded as 1920x1088,
+60 frames, the seeded generator in rusty_h264_b200/synth.py) through the whole
+path: half-pel planes of the 59 reference pictures, plain-ME of the 59 P
+frames (best_part 16x16 + 16x8/8x16 per MB, Balanced preset, QP 27, lme =
+sqrt(lambda)*1.25), MC + luma T/Q of every chosen MB, and the HalfRes mb-tree
+lookahead (downsample + frame costs) of all 60 frames.
+
+* value: Mpx/s of displayed luma (60 x 1920 x 1080 per step) with the clip
+  resident in HBM, CUDA-event timed on the launching stream.  The clip, planes
+  and coefficients (~1 GB) exceed the 126 MB L2, so no flush is needed.
+* e2e: the same work through h264a_pixel_path_host from pinned host memory,
+  host->device copy of the frames and device->host copy of every result
+  inside the timed region (the call synchronises; wall-clock timed).
+* roofline: the dominant kernel (the persistent ME kernel) against the INT32
+  issue rate measured on this device by h264a_measure_int32_peak; the
+  algorithmic work is 112 integer ops per 4x4 Hadamard-SATD evaluation the
+  reference performs (the kernel reports the count per MB).
+* cpu_baseline: the C restatement of the reference path (oracle/) on one host
+  core over a 3-frame sample of the same clip.
+
+--impl reference times that CPU restatement with all host threads instead.
+With --gpus N (torchrun) every rank runs an independent replica on its own
+clip (distinct seed): replicas only, no collective on the data path.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "1080p encode Mpx/s: plain GPU ME vs learned-proposal ME at ≤0.5% BD-rate"
+W, H, FRAMES, QP = 1920, 1080, 60, 27
+SATD_OPS_PER_4X4 = 112
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--frames", type=int, default=FRAMES)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        backend = "nccl"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    return ws, rank, local
+
+
+def clip(seed: int, frames: int):
+    from rusty_h264_b200 import synth
+
+    cache = os.path.join("/tmp", f"h264a_hd_clip_s{seed}_f{frames}.npy")
+    if os.path.exists(cache):
+        return np.load(cache)
+    y, _, _ = synth.hd_clip(frames, seed)
+    f = synth.coded_luma(y)
+    try:
+        np.save(cache, f)
+    except OSError:
+        pass
+    return f
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax.append(float(p[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(frames: np.ndarray, nthreads: int, lam: float, gate: int):
+    """The CPU restatement of the reference path on a bounded sample."""
+    from oracle import oracle as O
+
+    t0 = time.perf_counter()
+    O.pixel_path_clip(frames, O.balanced_params(), lam, gate, QP, nthreads=nthreads)
+    dt = time.perf_counter() - t0
+    return frames.shape[0] * W * H / dt / 1e6, dt
+
+
+def run_reference(args, ws, rank):
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    from rusty_h264_b200.accel import frame_lambda, split_gate_for_qp
+
+    nthreads = O.lib().or_num_threads()
+    lam = float(np.sqrt(frame_lambda(QP)) * 1.25)
+    gate = split_gate_for_qp(QP)
+    f = clip(1, args.frames)
+    sample = min(args.frames, max(3, nthreads + 1))
+    frames = np.ascontiguousarray(f[:sample])
+    for _ in range(args.warmup):
+        cpu_baseline(frames[:3], nthreads, lam, gate)
+    times = []
+    for _ in range(args.steps):
+        _, dt = cpu_baseline(frames, nthreads, lam, gate)
+        times.append(dt)
+    ms = float(np.mean(times)) * 1e3
+    value = sample * W * H / (ms * 1e-3) / 1e6
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": "Mpx/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u8/i32", "data": "synthetic (seeded 1080p generator)", "impl": "reference",
+        "config": {"workload": "1080p 60-frame clip, pixel path (planes, plain-ME, MC+T/Q, HalfRes lookahead)",
+                   "sample_frames_per_step": sample, "qp": QP},
+        "cpu_baseline": {"value": round(value, 3), "unit": "Mpx/s", "cores": nthreads, "kind": "port",
+                         "sample": f"{sample} frames of the 1080p clip per step"},
+        "e2e": {"value": round(value, 3), "unit": "Mpx/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, ws, rank, local):
+    import torch
+
+    from rusty_h264_b200 import accel as A
+
+    torch.cuda.set_device(local)
+    acc = A.Accel(local)
+    n = args.frames
+    f = clip(1 + rank, n)
+    ch, cw = f.shape[1:]
+    pad = 32
+    pw, ph = cw + 2 * pad, ch + 2 * pad
+    nmb = (cw // 16) * (ch // 16)
+    qp = QP
+    lam = float(np.sqrt(A.frame_lambda(qp)) * 1.25)
+    gate = A.split_gate_for_qp(qp)
+    params = A.default_me_params()
+    dev = f"cuda:{local}"
+    d_frames = torch.from_numpy(f).to(dev)
+    planes = torch.empty((n - 1, 4, ph, pw), dtype=torch.uint8, device=dev)
+    picks = torch.zeros((n, nmb, 6), dtype=torch.int32, device=dev)
+    costs = torch.zeros((n, nmb, 2), dtype=torch.int64, device=dev)
+    coeffs = torch.zeros((n, nmb, 256), dtype=torch.int16, device=dev)
+    half = torch.empty((n, ch // 2, cw // 2), dtype=torch.uint8, device=dev)
+    la_intra = torch.empty((n, nmb), dtype=torch.int32, device=dev)
+    la_inter = torch.empty((n, nmb), dtype=torch.int32, device=dev)
+    la_mvs = torch.empty((n, nmb, 2), dtype=torch.int32, device=dev)
+    me_frames, tq_frames = [], []
+    for i in range(1, n):
+        pic = A.Picture(d_frames[i].data_ptr(), planes[i - 1].data_ptr(), cw, ch, pad)
+        me_frames.append(A.MeFrame(pic, lam, gate, picks[i].data_ptr(), costs[i].data_ptr()))
+        tq_frames.append(A.TqFrame(pic, picks[i].data_ptr(), qp, 6, coeffs[i].data_ptr()))
+    stream = torch.cuda.current_stream()
+    ev = {k: (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for k in ("hpel", "me", "tq", "la")}
+    stage_ms = {k: [] for k in ev}
+
+    def step(record=False):
+        e = ev
+        if record:
+            e["hpel"][0].record(stream)
+        acc.hpel_build(d_frames[: n - 1], pad, out=planes)
+        if record:
+            e["hpel"][1].record(stream)
+            e["me"][0].record(stream)
+        acc.me_frames(me_frames, params)
+        if record:
+            e["me"][1].record(stream)
+            e["tq"][0].record(stream)
+        acc.mc_tq_frames(tq_frames)
+        if record:
+            e["tq"][1].record(stream)
+            e["la"][0].record(stream)
+        h = acc.L.h264a_downsample2x(acc.ctx, d_frames.data_ptr(), cw, ch, n, cw * ch, half.data_ptr(),
+                                     acc._stream())
+        acc._check(h)
+        acc._check(acc.L.h264a_lookahead_costs(acc.ctx, d_frames.data_ptr(), half.data_ptr(), cw, ch, n, 2,
+                                               la_intra.data_ptr(), la_inter.data_ptr(), la_mvs.data_ptr(),
+                                               acc._stream()))
+        if record:
+            e["la"][1].record(stream)
+
+    kernels_per_step = 1 + ((n - 1 + 95) // 96) + ((n - 1 + 95) // 96) + 1 + 3
+
+    def barrier():
+        if ws > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        step()
+    acc.sync()
+    barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for _ in range(args.steps):
+        step()
+    t1.record(stream)
+    torch.cuda.synchronize()
+    acc.sync()
+    clk = clocks.stop()
+    barrier()
+    ms = t0.elapsed_time(t1) / args.steps
+    if ws > 1:
+        import torch.distributed as dist
+
+        tt = torch.tensor([ms], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    value = ws * n * W * H / (ms * 1e-3) / 1e6
+
+    # per-stage device times (a separate pass with events between the stages)
+    for _ in range(max(3, args.steps // 2)):
+        step(record=True)
+        torch.cuda.synchronize()
+        for k, (a, b) in ev.items():
+            stage_ms[k].append(a.elapsed_time(b))
+    acc.sync()
+    stage = {k: float(np.mean(v)) for k, v in stage_ms.items()}
+    work4x4 = int(picks[1:, :, 5].sum().item())
+    int32_peak = acc.measure_int32_peak()
+    me_ops = work4x4 * SATD_OPS_PER_4X4
+    achieved = me_ops / (stage["me"] * 1e-3) / 1e9
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    hpel_bytes = (n - 1) * (cw * ch + 4 * pw * ph)
+    roofline = {
+        "kernel": "me_frames_kernel (persistent plain-ME)", "bound": "int32", "achieved": round(achieved, 1),
+        "peak": round(int32_peak, 1), "unit": "Gop/s", "frac": round(achieved / int32_peak, 4),
+        "peak_source": "measured live by h264a_measure_int32_peak (INT32 is not in MEASURED_PEAKS.json)",
+        "traffic": None,
+        "work": {"satd_4x4_evals_per_step": work4x4, "ops_per_4x4": SATD_OPS_PER_4X4},
+        "hpel_kernel": {"bound": "hbm", "achieved_gbs": round(hpel_bytes / (stage["hpel"] * 1e-3) / 1e9, 1),
+                        "peak_gbs": hbm_peak, "frac": round(hpel_bytes / (stage["hpel"] * 1e-3) / 1e9 / hbm_peak, 4),
+                        "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback 6650"},
+    }
+    line = {
+        "metric": METRIC, "value": round(value, 2), "unit": "Mpx/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u8/i32", "data": "synthetic (seeded 1080p generator, per-rank seed)",
+        "config": {"workload": "1080p 60-frame clip, pixel path (planes, plain-ME, MC+T/Q, HalfRes lookahead)",
+                   "frames_per_step": n, "qp": qp, "preset": "balanced", "split_partitions": True,
+                   "l2": "inputs and outputs (~1 GB) exceed L2; no flush", "parallelism": f"replicas x{ws}"},
+        "stage_ms": {k: round(v, 4) for k, v in stage.items()},
+        "roofline": roofline,
+        "clocks": clk,
+        "gpu_launches": kernels_per_step * args.steps,
+    }
+    if not args.no_e2e:
+        host_frames = torch.from_numpy(f).pin_memory()
+        outs = dict(picks=torch.zeros((n, nmb, 6), dtype=torch.int32).pin_memory(),
+                    costs=torch.zeros((n, nmb, 2), dtype=torch.int64).pin_memory(),
+                    coeffs=torch.zeros((n, nmb, 256), dtype=torch.int16).pin_memory(),
+                    la_intra=torch.zeros((n, nmb), dtype=torch.int32).pin_memory(),
+                    la_inter=torch.zeros((n, nmb), dtype=torch.int32).pin_memory(),
+                    la_mvs=torch.zeros((n, nmb, 2), dtype=torch.int32).pin_memory())
+        outs_np = {k: v.numpy() for k, v in outs.items()}
+        fr_np = host_frames.numpy()
+        for _ in range(args.warmup):
+            acc.pixel_path_host(fr_np, params, lam, gate, qp, out=outs_np)
+        barrier()
+        ts = []
+        for _ in range(args.steps):
+            s0 = time.perf_counter()
+            acc.pixel_path_host(fr_np, params, lam, gate, qp, out=outs_np)
+            ts.append(time.perf_counter() - s0)
+        e2e_ms = float(np.mean(ts)) * 1e3
+        if ws > 1:
+            import torch.distributed as dist
+
+            tt = torch.tensor([e2e_ms], device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            e2e_ms = float(tt.item())
+        d2h = sum(v.numel() * v.element_size() for v in outs.values())
+        line["e2e"] = {"value": round(ws * n * W * H / (e2e_ms * 1e-3) / 1e6, 2), "unit": "Mpx/s",
+                       "h2d_bytes_per_step": int(f.nbytes), "d2h_bytes_per_step": int(d2h),
+                       "ms_per_step": round(e2e_ms, 3), "timing": "wall clock around the synchronous C-ABI call"}
+        # the host path and the device-resident path must agree
+        assert np.array_equal(outs_np["coeffs"], coeffs.cpu().numpy())
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        v, dt = cpu_baseline(np.ascontiguousarray(f[:3]), 1, lam, gate)
+        line["cpu_baseline"] = {"value": round(v, 3), "unit": "Mpx/s", "cores": 1, "kind": "port",
+                                "sample": "3 frames of the 1080p clip (2 P frames + lookahead), one thread"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    acc.close()
+
+
+def main():
+    args = parse()
+    ws, rank, local = dist_init()
+    if args.impl == "reference":
+        run_reference(args, ws, rank)
+    else:
+        run_ours(args, ws, rank, local)
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

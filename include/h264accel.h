@@ -1,0 +1,246 @@
+/*
+ * h264accel.h -- C ABI of libh264accel_cuda.so, the B200 (sm_100a) encoder
+ * pixel hot path of rusty_h264.
+ *
+ * The reference's boundary is the free-function surface of the
+ * `rusty_h264-accel` crate (crates/rusty_h264-accel/src/lib.rs:33-58), called
+ * per block (~17 ns of work each).  A GPU launch costs ~100x that, so every
+ * entry point here keeps the value contract of one reference function but
+ * takes a whole batch (or a whole frame) per call.  Each declaration names the
+ * reference function it replaces.
+ *
+ * Conventions
+ *  - Every call returns H264A_OK (0) or a negative H264A_E_* code; the message
+ *    is in h264a_last_error() (per thread).  Nothing aborts across the ABI.
+ *  - Pointers named d_* are device pointers (CUDA global memory of the
+ *    context's device); h_* are host pointers.  Callers own every buffer.
+ *  - `stream` is a cudaStream_t (NULL = the context's own stream).  Calls only
+ *    enqueue work; results are ready when the stream is synchronised
+ *    (h264a_sync).  Calls on one context from several threads must use
+ *    different streams.
+ *  - Planes: a reference picture's cached planes are one buffer F|H|V|C, each
+ *    pw*ph bytes with pw = cw + 2*pad, ph = ch + 2*pad, stride pw: the
+ *    HpelPlanes layout of crates/rusty_h264-common/src/inter.rs:707-730.
+ *  - Motion vectors are quarter-pel (i32, x then y), as in the reference.
+ */
+#ifndef H264ACCEL_H
+#define H264ACCEL_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define H264A_API __attribute__((visibility("default")))
+#else
+#define H264A_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define H264A_OK 0
+#define H264A_E_ARG (-1)       /* invalid argument (size, stride, pointer) */
+#define H264A_E_CUDA (-2)      /* a CUDA runtime call failed */
+#define H264A_E_TIMEOUT (-3)   /* a bounded device wait ran out (see h264a_last_error) */
+#define H264A_E_NOMEM (-4)     /* device allocation failed */
+#define H264A_E_NODEV (-5)     /* no usable sm_100 device */
+
+typedef struct h264a_ctx h264a_ctx;
+
+/* ---- context ----------------------------------------------------------- */
+H264A_API const char *h264a_version(void);
+H264A_API const char *h264a_last_error(void);
+H264A_API int h264a_ctx_create(int device, h264a_ctx **out);
+H264A_API int h264a_ctx_destroy(h264a_ctx *ctx);
+H264A_API int h264a_sync(h264a_ctx *ctx, void *stream);
+/* convenience device memory for callers without the CUDA runtime (FFI) */
+H264A_API int h264a_dev_alloc(h264a_ctx *ctx, size_t bytes, void **d_out);
+H264A_API int h264a_dev_free(h264a_ctx *ctx, void *d_ptr);
+H264A_API int h264a_memcpy_h2d(h264a_ctx *ctx, void *d_dst, const void *h_src, size_t bytes, void *stream);
+H264A_API int h264a_memcpy_d2h(h264a_ctx *ctx, void *h_dst, const void *d_src, size_t bytes, void *stream);
+
+/* ---- a1/a2: half-pel planes -------------------------------------------- */
+/* pad_plane_into + hpel_fused / build_hpel_planes
+ * (common/src/inter.rs:798-849, accel/src/hpel.rs:34-203) for n pictures:
+ * picture i is d_ref + i*ref_frame_stride (cw x ch, row stride cw), its planes
+ * go to d_planes + i*4*pw*ph.  pad >= 3 (the reference default is 32). */
+H264A_API int h264a_hpel_build(h264a_ctx *ctx, const uint8_t *d_ref, int cw, int ch, int pad, int n,
+                     size_t ref_frame_stride, uint8_t *d_planes, void *stream);
+
+/* ---- a6/a7/a8: block metrics -------------------------------------------- */
+#define H264A_METRIC_SATD_WELS 0 /* Σ_4x4((Σ|H·d|+1)>>1): satd_16x16..satd_4x4 (satd_sad.rs:309-340) */
+#define H264A_METRIC_SATD 1      /* Σ|H·d|: satd_x4 / satd_x4p (satd_avg.rs:350-420), satd_px (mb16.rs:6027) */
+#define H264A_METRIC_SAD 2       /* Σ|a−b|: sad_16x16.. / sad_x4 (satd_sad.rs:342-363, satd_avg.rs:462) */
+#define H264A_METRIC_SATD_AVG 3  /* Σ|H·(a−(b+c+1)>>1)|: satd_avg / satd_avg_x4 (satd_avg.rs:536-602) */
+#define H264A_METRIC_SAD_AVG 4   /* Σ|a−(b+c+1)>>1|: sad_avg_strided (mb16.rs:6104) */
+/* out[i] = metric of the w×h blocks at d_a+a_off[i] (stride sa) vs d_b+b_off[i]
+ * (stride sb) [and d_c+c_off[i] for the *_AVG metrics, stride sb].
+ * (w,h) in {16x16,16x8,8x16,8x8,8x4,4x8,4x4}.  The x4 calls are this with n=4k. */
+H264A_API int h264a_block_metric(h264a_ctx *ctx, int metric, int w, int h, const uint8_t *d_a, const int64_t *d_a_off, int sa,
+                       const uint8_t *d_b, const int64_t *d_b_off, const uint8_t *d_c, const int64_t *d_c_off, int sb,
+                       int n, int32_t *d_out, void *stream);
+
+/* ---- a3/a4/a5/a9: candidate distortion ---------------------------------- */
+typedef struct {
+    const uint8_t *d_src;    /* coded source luma, stride cw */
+    const uint8_t *d_planes; /* the reference's F|H|V|C planes */
+    int32_t cw, ch, pad;
+} h264a_picture;
+
+typedef struct {
+    int32_t pic;             /* index into the picture array */
+    int32_t x, y, w, h;      /* block in the source */
+    int32_t mvx, mvy;        /* quarter-pel candidate */
+} h264a_candidate;
+
+/* Distortion of arbitrary candidates, exactly the values of MeCtx::eval
+ * (accel/src/mectx.rs:112-166) / mc_satd_hp (metric SATD, mb16.rs:1930) and
+ * mc_sad_hp (metric SAD, mb16.rs:2018), including candidates off the planes,
+ * where the reference falls back to mc_luma (inter.rs:1193).  A candidate
+ * whose picture index, shape or block position is out of range gets -1. */
+H264A_API int h264a_candidate_dist(h264a_ctx *ctx, const h264a_picture *d_pics, int npics, const h264a_candidate *d_cands, int n,
+                         int metric, int32_t *d_out, void *stream);
+
+/* ---- a10/a11/a12: motion search ------------------------------------------ */
+typedef struct {
+    int32_t fast;            /* Preset::Fast: SAD cost, [16,4] ladder (config.rs:8-38) */
+    int32_t mb_use_satd;     /* fast preset's SATD override (mb16.rs:2507) */
+    int32_t sadfp;           /* B2: SAD-domain full-pel phase (mb16.rs:616-643) */
+    int32_t mv_cost_kind;    /* 0 Exp-Golomb, 1 smooth table, 2 measured table (mb16.rs:563) */
+    const uint16_t *d_mv_cost_tab; /* device, 4096 u16 (kinds 1, 2; see h264a_build_mv_cost_table) */
+    double sadfp_lambda;     /* RFF_ME_SADL, 0.5 (mb16.rs:756) */
+    int32_t me_snap;         /* tune_me_snap, 1 */
+    int32_t me_fc;           /* fixed-centre diamond of the accel build, 1 (mb16.rs:700) */
+    uint32_t dia_mask;       /* rungs of [64,32,16,8,4] qpel, 0b11100 (mb16.rs:828) */
+    uint32_t dia_sub_mask;   /* sub-8x8 rungs, 0b10000 (mb16.rs:851) */
+    int32_t subpel;          /* run the [2,1] sub-pel steps (mb16.rs:2956) */
+    int32_t subpel_pat;      /* -1 = preset default, else RFF_SUBPEL_PAT 0..3 */
+    int32_t sp_single_pass;  /* Balanced (mb16.rs:1664) */
+    int32_t sub_pat;         /* RFF_SUBPEL_SUB, 2 */
+    int32_t me_subpel_iter;  /* tune_me_subpel_iter, 1 */
+    int32_t sp_maxit;        /* RFF_SP_MAXIT, 0 = unlimited */
+    int32_t sp_fc;           /* RFF_SP_FC batched rings, 0 */
+} h264a_me_params;
+
+/* Fills *p with the Balanced-preset defaults the reference encoder runs. */
+H264A_API void h264a_me_params_default(h264a_me_params *p);
+/* The smooth mvd-cost table of mb16.rs:508-519 (kind 1), 4096 entries, host. */
+H264A_API void h264a_build_mv_cost_table(uint16_t *h_out);
+
+typedef struct {
+    int32_t pic;
+    int32_t x, y, w, h;      /* partition in the source, w,h in {16,8,4} */
+    int32_t npred;           /* 1..4 seeds; preds[0] is the mvd centre */
+    int32_t preds[8];
+    int32_t has_start;       /* refine-only search from start (mb16.rs:2445) */
+    int32_t start[2];
+    double lambda_me;
+} h264a_me_job;
+
+typedef struct {
+    int32_t mvx, mvy;
+    int64_t cost;            /* J = D + (λ·bits) as i64, the search's own domain */
+    int32_t evals;           /* distortion evaluations performed */
+    int32_t status;          /* 0 ok */
+} h264a_me_result;
+
+/* n independent motion_search calls (mb16.rs:2433-3302), one warp each.  A
+ * job with an out-of-range picture, shape, position or npred gets status -1. */
+H264A_API int h264a_me_search(h264a_ctx *ctx, const h264a_picture *d_pics, int npics, const h264a_me_params *params,
+                    const h264a_me_job *d_jobs, int n, h264a_me_result *d_out, void *stream);
+
+/* Plain-ME frames: every MB of every frame runs best_part (mb16.rs:4921) for
+ * 16x16 and, when its J exceeds split_gate (>= 0), the 16x8/8x16 partitions
+ * with the MB's neighbours feeding predict_mv (inter.rs:36, mv_neighbors_block
+ * mb16.rs:1871) in raster dependency order, every MB assumed coded inter with
+ * ref 0.  One persistent launch drains a work queue over all frames (MBs of
+ * different frames interleave); each MB waits (bounded) for its left and
+ * top-right neighbours.  Picks: 6 i32 per MB {shape 0/1/2, mv0x, mv0y, mv1x,
+ * mv1y, work} where work counts the 4x4-block distortion evaluations the
+ * reference performs for the MB; costs: 2 i64 per MB {pick J, 16x16 J}. */
+typedef struct {
+    h264a_picture pic;
+    double lambda_me;
+    int64_t split_gate;
+    int32_t *d_picks;
+    int64_t *d_costs;
+} h264a_me_frame;
+
+H264A_API int h264a_me_frames(h264a_ctx *ctx, const h264a_me_frame *h_frames, int nframes, const h264a_me_params *params,
+                    void *stream);
+
+/* Exhaustive full-pel 16x16 grid (±R around each MB's centre MV) with SAD and
+ * SATD values as the ME cost functions return them (mc_sad_hp / mc_satd_hp at
+ * full-pel MVs), and the per-MB argmin of dist + (λ·bits(mv − pmv)) in raster
+ * order with first-wins ties (the exhaustive probe of mb16.rs:2889-2900).
+ * d_centers/d_pmv: 2 i32 per MB (NULL = zero).  Grids (optional, NULL to
+ * skip): (2R+1)^2 i32 per MB, row-major in dy.  d_best: 4 i32 per MB
+ * {mvx, mvy, cost, dist} for metric (0 = SAD, 1 = SATD).  1 <= R <= 64. */
+H264A_API int h264a_fullpel_grid(h264a_ctx *ctx, const h264a_picture *h_pic, int R, const int32_t *d_centers,
+                       const int32_t *d_pmv, int metric, int mv_cost_kind, const uint16_t *d_mv_cost_tab,
+                       double lambda, int32_t *d_sad_grid, int32_t *d_satd_grid, int32_t *d_best, void *stream);
+
+/* ---- a13/a14/a15: forward transform + quant ------------------------------ */
+/* dct_four_t4 + quant_four_4x4 (accel/src/transform_quant.rs:76, 122) over n
+ * 8x8 regions: region i is at (xy[2i], xy[2i+1]) in both planes; 64 i16 out
+ * per region in the reference's sub-block order; ff/mf from quant_dz_ff(qp,dz)
+ * and QUANT_MF_OH[qp] (transform.rs:145, 1447), qp per region. */
+H264A_API int h264a_dct_quant_4x4(h264a_ctx *ctx, const uint8_t *d_src, int ss, const uint8_t *d_pred, int ps,
+                        const int32_t *d_xy, const uint8_t *d_qp, int dz_div, int n, int16_t *d_out, void *stream);
+/* forward_core_8x8 + quantize_8x8 (transform.rs:548, 613), flat or given
+ * scaling-list weights (host array of 64 i32, raster; NULL = flat 16):
+ * 64 i32 levels per region, raster order. */
+H264A_API int h264a_dct_quant_8x8(h264a_ctx *ctx, const uint8_t *d_src, int ss, const uint8_t *d_pred, int ps,
+                        const int32_t *d_xy, const uint8_t *d_qp, const int32_t *h_weight, int dz_div, int n,
+                        int32_t *d_out, void *stream);
+/* MC of each MB's pick (the planes' quarter-pel prediction = mc_luma) then the
+ * luma T/Q of mb16.rs:3436-3450: 256 i16 per MB, for n frames. */
+typedef struct {
+    h264a_picture pic;
+    const int32_t *d_picks;  /* 6 i32 per MB, as h264a_me_frames writes */
+    int32_t qp, dz_div;
+    int16_t *d_coeffs;       /* 256 i16 per MB */
+} h264a_tq_frame;
+H264A_API int h264a_mc_tq_frames(h264a_ctx *ctx, const h264a_tq_frame *h_frames, int nframes, void *stream);
+
+/* ---- a16-a19: mb-tree lookahead ------------------------------------------ */
+/* downsample2x (encoder/src/mbtree.rs:61-74) of n frames cw x ch -> cw/2 x ch/2. */
+H264A_API int h264a_downsample2x(h264a_ctx *ctx, const uint8_t *d_frames, int cw, int ch, int n, size_t frame_stride,
+                       uint8_t *d_half, void *stream);
+/* frame_costs (mbtree.rs:208-263) of n consecutive frames, frame f against
+ * frame f-1 (frame 0 is the IDR: intra only).  mode 0 FullRes, 1 Hybrid,
+ * 2 HalfRes (the default, config.rs:568).  d_full: n frames cw x ch;
+ * d_half: their downsample2x (needed for modes 1, 2).  Out per MB: intra,
+ * inter (i32) and the full-res quarter-pel MV (2 i32). */
+H264A_API int h264a_lookahead_costs(h264a_ctx *ctx, const uint8_t *d_full, const uint8_t *d_half, int cw, int ch, int n,
+                          int mode, int32_t *d_intra, int32_t *d_inter, int32_t *d_mvs, void *stream);
+
+/* ---- the whole pixel path from host memory -------------------------------- */
+/* Copies n coded luma frames (cw x ch, contiguous) to the device, builds the
+ * planes of frames 0..n-2, runs plain-ME + MC + T/Q for frames 1..n-1 (each
+ * against the previous source frame) and the HalfRes lookahead for all n
+ * frames, and copies the results back.  Output arrays are per frame (frame 0
+ * rows are zero for picks/costs/coeffs): h_picks 6 i32/MB, h_costs 2 i64/MB,
+ * h_coeffs 256 i16/MB, h_la_intra/h_la_inter 1 i32/MB, h_la_mvs 2 i32/MB.
+ * Device buffers are cached in the context between calls of the same shape. */
+H264A_API int h264a_pixel_path_host(h264a_ctx *ctx, const uint8_t *h_frames, int n, int cw, int ch, const h264a_me_params *params,
+                          const uint16_t *h_mv_cost_tab, double lambda_me, int64_t split_gate, int qp, int dz_div,
+                          int32_t *h_picks, int64_t *h_costs, int16_t *h_coeffs, int32_t *h_la_intra,
+                          int32_t *h_la_inter, int32_t *h_la_mvs);
+
+/* ---- diagnostics ----------------------------------------------------------- */
+/* Failure-detection self-test: one warp runs the persistent kernel's bounded
+ * wait on a flag that nothing sets, giving up after spin_limit polls.  The next
+ * h264a_sync on `stream` then returns H264A_E_TIMEOUT and the context stays
+ * usable.  No counterpart in the reference (it has no device waits). */
+H264A_API int h264a_selftest_bounded_wait(h264a_ctx *ctx, int spin_limit, void *stream);
+/* Measures the device's INT32 issue rate (three-input adds, lane instructions
+ * per second / 1e9) with a short independent-chain kernel: the roofline
+ * denominator of the SAD/SATD kernels.  Synchronous; no reference counterpart. */
+H264A_API int h264a_measure_int32_peak(h264a_ctx *ctx, double *gops_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* H264ACCEL_H */

@@ -1,0 +1,296 @@
+// capi.cu -- context, error reporting, parameter mirrors and the host-buffer
+// pipeline entry of libh264accel_cuda.so.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "h264accel_internal.h"
+
+namespace h264a {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+int fail(int code, const std::string& msg) {
+    set_error(msg);
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+    return fail(H264A_E_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+int check_launch(const char* what) {
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, what);
+    return H264A_OK;
+}
+
+MeParamsDev to_dev(const h264a_me_params& p) {
+    MeParamsDev d;
+    d.fast = p.fast;
+    d.use_sad = p.fast && !p.mb_use_satd;
+    d.sadfp = p.sadfp;
+    d.kind = p.mv_cost_kind;
+    d.tab = p.d_mv_cost_tab;
+    d.sadfp_lambda = p.sadfp_lambda;
+    d.me_snap = p.me_snap;
+    d.fc = p.me_fc;
+    d.dia_mask = p.dia_mask;
+    d.dia_sub_mask = p.dia_sub_mask;
+    d.subpel = p.subpel;
+    d.subpel_pat = p.subpel_pat;
+    d.sp_single_pass = p.sp_single_pass;
+    d.sub_pat = p.sub_pat;
+    d.me_subpel_iter = p.me_subpel_iter;
+    d.sp_maxit = p.sp_maxit;
+    d.sp_fc = p.sp_fc;
+    return d;
+}
+
+int ensure_me_scratch(h264a_ctx* ctx, size_t n) {
+    if (n <= ctx->flags_cap) return H264A_OK;
+    if (ctx->d_flags) cudaFree(ctx->d_flags);
+    ctx->d_flags = nullptr;
+    ctx->flags_cap = 0;
+    size_t cap = n < 4096 ? 4096 : n + n / 4;
+    if (cudaMalloc(&ctx->d_flags, cap * sizeof(int32_t)) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(H264A_E_NOMEM, "persistent-kernel flags: cudaMalloc failed");
+    }
+    H264A_CUDA(cudaMemset(ctx->d_flags, 0, cap * sizeof(int32_t)));
+    ctx->flags_cap = cap;
+    ctx->epoch = 0;
+    return H264A_OK;
+}
+
+int next_epoch(h264a_ctx* ctx, cudaStream_t st) {
+    if (ctx->epoch >= 0x7ffffff0) {  // wrap: clear the flags so stale values never match
+        if (cudaMemsetAsync(ctx->d_flags, 0, ctx->flags_cap * sizeof(int32_t), st) != cudaSuccess) {
+            cudaGetLastError();
+            set_error("persistent-kernel flags: reset failed");
+            return -1;
+        }
+        ctx->epoch = 0;
+    }
+    return ++ctx->epoch;
+}
+
+}  // namespace h264a
+
+using namespace h264a;
+
+extern "C" const char* h264a_version(void) { return "h264accel_cuda 0.1.0 (sm_100a)"; }
+
+extern "C" const char* h264a_last_error(void) { return g_last_error.c_str(); }
+
+extern "C" int h264a_ctx_create(int device, h264a_ctx** out) {
+    if (!out) return fail(H264A_E_ARG, "ctx_create: null out");
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        return fail(H264A_E_NODEV, "ctx_create: no CUDA device");
+    }
+    if (device < 0 || device >= count) return fail(H264A_E_ARG, "ctx_create: device index out of range");
+    cudaDeviceProp prop;
+    H264A_CUDA(cudaGetDeviceProperties(&prop, device));
+    if (prop.major != 10) return fail(H264A_E_NODEV, std::string("ctx_create: built for sm_100a, device is ") + prop.name);
+    H264A_CUDA(cudaSetDevice(device));
+    h264a_ctx* c = new h264a_ctx();
+    c->device = device;
+    c->num_sms = prop.multiProcessorCount;
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMalloc(&c->d_counter, sizeof(int32_t)) != cudaSuccess ||
+        cudaMalloc(&c->d_status, sizeof(int32_t)) != cudaSuccess ||
+        cudaMemset(c->d_status, 0, sizeof(int32_t)) != cudaSuccess) {
+        const cudaError_t e = cudaGetLastError();
+        h264a_ctx_destroy(c);
+        return cuda_fail(e, "ctx_create");
+    }
+    *out = c;
+    return H264A_OK;
+}
+
+extern "C" int h264a_ctx_destroy(h264a_ctx* ctx) {
+    if (!ctx) return H264A_OK;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (ctx->d_counter) cudaFree(ctx->d_counter);
+    if (ctx->d_status) cudaFree(ctx->d_status);
+    if (ctx->d_flags) cudaFree(ctx->d_flags);
+    if (ctx->pp_buf) cudaFree(ctx->pp_buf);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return H264A_OK;
+}
+
+// Synchronises `stream` and reports a bounded-wait timeout recorded by a
+// persistent kernel since the last sync (the status word is then cleared).
+extern "C" int h264a_sync(h264a_ctx* ctx, void* stream) {
+    if (!ctx) return fail(H264A_E_ARG, "sync: null ctx");
+    cudaStream_t st = pick_stream(ctx, stream);
+    H264A_CUDA(cudaStreamSynchronize(st));
+    int32_t status = 0;
+    H264A_CUDA(cudaMemcpy(&status, ctx->d_status, sizeof status, cudaMemcpyDeviceToHost));
+    if (status != 0) {
+        H264A_CUDA(cudaMemset(ctx->d_status, 0, sizeof(int32_t)));
+        return fail(H264A_E_TIMEOUT, "a bounded wait for a neighbouring macroblock ran out (status " +
+                                         std::to_string(status) + ")");
+    }
+    return H264A_OK;
+}
+
+extern "C" int h264a_dev_alloc(h264a_ctx* ctx, size_t bytes, void** d_out) {
+    if (!ctx || !d_out) return fail(H264A_E_ARG, "dev_alloc: null pointer");
+    if (cudaMalloc(d_out, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        *d_out = nullptr;
+        return fail(H264A_E_NOMEM, "dev_alloc: cudaMalloc failed");
+    }
+    return H264A_OK;
+}
+
+extern "C" int h264a_dev_free(h264a_ctx* ctx, void* d_ptr) {
+    if (!ctx) return fail(H264A_E_ARG, "dev_free: null ctx");
+    H264A_CUDA(cudaFree(d_ptr));
+    return H264A_OK;
+}
+
+extern "C" int h264a_memcpy_h2d(h264a_ctx* ctx, void* d_dst, const void* h_src, size_t bytes, void* stream) {
+    if (!ctx || (!d_dst && bytes) || (!h_src && bytes)) return fail(H264A_E_ARG, "memcpy_h2d: null pointer");
+    H264A_CUDA(cudaMemcpyAsync(d_dst, h_src, bytes, cudaMemcpyHostToDevice, pick_stream(ctx, stream)));
+    return H264A_OK;
+}
+
+extern "C" int h264a_memcpy_d2h(h264a_ctx* ctx, void* h_dst, const void* d_src, size_t bytes, void* stream) {
+    if (!ctx || (!d_src && bytes) || (!h_dst && bytes)) return fail(H264A_E_ARG, "memcpy_d2h: null pointer");
+    H264A_CUDA(cudaMemcpyAsync(h_dst, d_src, bytes, cudaMemcpyDeviceToHost, pick_stream(ctx, stream)));
+    return H264A_OK;
+}
+
+extern "C" void h264a_me_params_default(h264a_me_params* p) {
+    if (!p) return;
+    memset(p, 0, sizeof *p);
+    // Balanced preset (config.rs:8-38, mb16.rs:1620-1745 defaults)
+    p->fast = 0;
+    p->mb_use_satd = 0;
+    p->sadfp = 0;
+    p->mv_cost_kind = 0;
+    p->d_mv_cost_tab = nullptr;
+    p->sadfp_lambda = 0.5;
+    p->me_snap = 1;
+    p->me_fc = 1;
+    p->dia_mask = 0x1c;      // [16,8,4] quarter-pel
+    p->dia_sub_mask = 0x10;  // [4]
+    p->subpel = 1;
+    p->subpel_pat = -1;
+    p->sp_single_pass = 1;
+    p->sub_pat = 2;
+    p->me_subpel_iter = 1;
+    p->sp_maxit = 0;
+    p->sp_fc = 0;
+}
+
+// build_mv_cost (mb16.rs:508-519): round(4·(2·log2(a+1) + 0.718 + [a≠0])).
+extern "C" void h264a_build_mv_cost_table(uint16_t* h_out) {
+    if (!h_out) return;
+    for (uint32_t a = 0; a < 4096; a++) {
+        const double c = 2.0 * std::log2(double(a + 1)) + 0.718 + (a != 0 ? 1.0 : 0.0);
+        h_out[a] = uint16_t(std::round(c * 4.0));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// The whole pixel path from host buffers
+// ---------------------------------------------------------------------------
+
+static size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
+
+extern "C" int h264a_pixel_path_host(h264a_ctx* ctx, const uint8_t* h_frames, int n, int cw, int ch,
+                                     const h264a_me_params* params, const uint16_t* h_mv_cost_tab, double lambda_me,
+                                     int64_t split_gate, int qp, int dz_div, int32_t* h_picks, int64_t* h_costs,
+                                     int16_t* h_coeffs, int32_t* h_la_intra, int32_t* h_la_inter, int32_t* h_la_mvs) {
+    if (!ctx || !h_frames || !params || !h_picks || !h_costs || !h_coeffs || !h_la_intra || !h_la_inter || !h_la_mvs)
+        return fail(H264A_E_ARG, "pixel_path_host: null pointer");
+    if (n < 1 || cw < 16 || ch < 16 || cw % 16 || ch % 16) return fail(H264A_E_ARG, "pixel_path_host: bad geometry");
+    if ((params->mv_cost_kind == 1 || params->mv_cost_kind == 2) && !h_mv_cost_tab)
+        return fail(H264A_E_ARG, "pixel_path_host: mv cost kinds 1 and 2 need a table");
+    const int pad = 32;
+    const int pw = cw + 2 * pad, ph = ch + 2 * pad;
+    const size_t nmb = size_t(cw / 16) * (ch / 16);
+    const size_t fs = size_t(cw) * ch, hs = fs / 4, p4 = size_t(4) * pw * ph;
+    // one cached device arena
+    size_t off = 0;
+    const size_t o_frames = off; off = align256(off + fs * n);
+    const size_t o_planes = off; off = align256(off + p4 * (n > 1 ? n - 1 : 1));
+    const size_t o_half = off; off = align256(off + hs * n);
+    const size_t o_picks = off; off = align256(off + sizeof(int32_t) * 6 * nmb * n);
+    const size_t o_costs = off; off = align256(off + sizeof(int64_t) * 2 * nmb * n);
+    const size_t o_coeffs = off; off = align256(off + sizeof(int16_t) * 256 * nmb * n);
+    const size_t o_intra = off; off = align256(off + sizeof(int32_t) * nmb * n);
+    const size_t o_inter = off; off = align256(off + sizeof(int32_t) * nmb * n);
+    const size_t o_mvs = off; off = align256(off + sizeof(int32_t) * 2 * nmb * n);
+    const size_t o_tab = off; off = align256(off + sizeof(uint16_t) * 4096);
+    if (off > ctx->pp_bytes) {
+        if (ctx->pp_buf) cudaFree(ctx->pp_buf);
+        ctx->pp_buf = nullptr;
+        ctx->pp_bytes = 0;
+        if (cudaMalloc(&ctx->pp_buf, off) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(H264A_E_NOMEM, "pixel_path_host: device arena allocation failed");
+        }
+        ctx->pp_bytes = off;
+    }
+    char* base = reinterpret_cast<char*>(ctx->pp_buf);
+    uint8_t* d_frames = reinterpret_cast<uint8_t*>(base + o_frames);
+    uint8_t* d_planes = reinterpret_cast<uint8_t*>(base + o_planes);
+    uint8_t* d_half = reinterpret_cast<uint8_t*>(base + o_half);
+    int32_t* d_picks = reinterpret_cast<int32_t*>(base + o_picks);
+    int64_t* d_costs = reinterpret_cast<int64_t*>(base + o_costs);
+    int16_t* d_coeffs = reinterpret_cast<int16_t*>(base + o_coeffs);
+    int32_t* d_intra = reinterpret_cast<int32_t*>(base + o_intra);
+    int32_t* d_inter = reinterpret_cast<int32_t*>(base + o_inter);
+    int32_t* d_mvs = reinterpret_cast<int32_t*>(base + o_mvs);
+    uint16_t* d_tab = reinterpret_cast<uint16_t*>(base + o_tab);
+    cudaStream_t st = ctx->stream;
+    H264A_CUDA(cudaMemcpyAsync(d_frames, h_frames, fs * n, cudaMemcpyHostToDevice, st));
+    h264a_me_params prm = *params;
+    if (prm.mv_cost_kind == 1 || prm.mv_cost_kind == 2) {
+        H264A_CUDA(cudaMemcpyAsync(d_tab, h_mv_cost_tab, sizeof(uint16_t) * 4096, cudaMemcpyHostToDevice, st));
+        prm.d_mv_cost_tab = d_tab;
+    }
+    H264A_CUDA(cudaMemsetAsync(d_picks, 0, sizeof(int32_t) * 6 * nmb, st));
+    H264A_CUDA(cudaMemsetAsync(d_costs, 0, sizeof(int64_t) * 2 * nmb, st));
+    H264A_CUDA(cudaMemsetAsync(d_coeffs, 0, sizeof(int16_t) * 256 * nmb, st));
+    int rc;
+    if (n > 1) {
+        rc = h264a_hpel_build(ctx, d_frames, cw, ch, pad, n - 1, fs, d_planes, st);
+        if (rc) return rc;
+        std::vector<h264a_me_frame> mf(n - 1);
+        std::vector<h264a_tq_frame> tf(n - 1);
+        for (int f = 1; f < n; f++) {
+            h264a_picture pic{d_frames + fs * f, d_planes + p4 * (f - 1), cw, ch, pad};
+            mf[f - 1] = {pic, lambda_me, split_gate, d_picks + 6 * nmb * f, d_costs + 2 * nmb * f};
+            tf[f - 1] = {pic, d_picks + 6 * nmb * f, qp, dz_div, d_coeffs + 256 * nmb * f};
+        }
+        rc = h264a_me_frames(ctx, mf.data(), n - 1, &prm, st);
+        if (rc) return rc;
+        rc = h264a_mc_tq_frames(ctx, tf.data(), n - 1, st);
+        if (rc) return rc;
+    }
+    rc = h264a_downsample2x(ctx, d_frames, cw, ch, n, fs, d_half, st);
+    if (rc) return rc;
+    rc = h264a_lookahead_costs(ctx, d_frames, d_half, cw, ch, n, 2, d_intra, d_inter, d_mvs, st);
+    if (rc) return rc;
+    H264A_CUDA(cudaMemcpyAsync(h_picks, d_picks, sizeof(int32_t) * 6 * nmb * n, cudaMemcpyDeviceToHost, st));
+    H264A_CUDA(cudaMemcpyAsync(h_costs, d_costs, sizeof(int64_t) * 2 * nmb * n, cudaMemcpyDeviceToHost, st));
+    H264A_CUDA(cudaMemcpyAsync(h_coeffs, d_coeffs, sizeof(int16_t) * 256 * nmb * n, cudaMemcpyDeviceToHost, st));
+    H264A_CUDA(cudaMemcpyAsync(h_la_intra, d_intra, sizeof(int32_t) * nmb * n, cudaMemcpyDeviceToHost, st));
+    H264A_CUDA(cudaMemcpyAsync(h_la_inter, d_inter, sizeof(int32_t) * nmb * n, cudaMemcpyDeviceToHost, st));
+    H264A_CUDA(cudaMemcpyAsync(h_la_mvs, d_mvs, sizeof(int32_t) * 2 * nmb * n, cudaMemcpyDeviceToHost, st));
+    return h264a_sync(ctx, st);
+}

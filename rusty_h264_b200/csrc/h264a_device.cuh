@@ -1,0 +1,199 @@
+// h264a_device.cuh -- device building blocks shared by the sm_100a kernels.
+//
+// All codec arithmetic is integer and bit-exact with the reference
+// (Remade-With-Rust/rusty_h264); each helper names the reference function
+// whose value it reproduces.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "h264accel_internal.h"
+
+namespace h264a {
+
+// ---------------------------------------------------------------------------
+// Byte access
+// ---------------------------------------------------------------------------
+
+// Four consecutive bytes at any alignment, little-endian, from read-only global
+// memory: two aligned 32-bit loads and a funnel shift.  Reads stay inside the
+// 4-byte words that hold p[0..3].
+__device__ __forceinline__ uint32_t ld4u(const uint8_t* p) {
+    const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+    const uint32_t* w = reinterpret_cast<const uint32_t*>(a & ~uintptr_t(3));
+    const uint32_t sh = uint32_t(a & 3) * 8u;
+    const uint32_t lo = __ldg(w);
+    if (sh == 0) return lo;
+    const uint32_t hi = __ldg(w + 1);
+    return __funnelshift_r(lo, hi, sh);
+}
+
+__device__ __forceinline__ int byte_of(uint32_t w, int k) { return int((w >> (8 * k)) & 0xffu); }
+
+__device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+// ---------------------------------------------------------------------------
+// 4x4 Hadamard SATD
+// ---------------------------------------------------------------------------
+
+// Σ|H·(s−p)·Hᵀ| of one 4x4 block given as four packed rows: the unrounded
+// value of satd_4x4_sum (transform.rs:701); the openh264 per-block SATD
+// (satd_sad.rs:39) is (this + 1) >> 1.  Butterfly order as satd4x4_scalar.
+__device__ __forceinline__ int satd4x4_rows(const uint32_t s[4], const uint32_t p[4]) {
+    int m[4][4];
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+        const int d0 = byte_of(s[r], 0) - byte_of(p[r], 0);
+        const int d1 = byte_of(s[r], 1) - byte_of(p[r], 1);
+        const int d2 = byte_of(s[r], 2) - byte_of(p[r], 2);
+        const int d3 = byte_of(s[r], 3) - byte_of(p[r], 3);
+        const int s0 = d0 + d2, s1 = d1 + d3, s2 = d0 - d2, s3 = d1 - d3;
+        m[r][0] = s0 + s1; m[r][1] = s2 + s3; m[r][2] = s2 - s3; m[r][3] = s0 - s1;
+    }
+    int sum = 0;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        const int s0 = m[0][j] + m[2][j], s1 = m[1][j] + m[3][j];
+        const int s2 = m[0][j] - m[2][j], s3 = m[1][j] - m[3][j];
+        sum += abs(s0 + s1) + abs(s2 + s3) + abs(s2 - s3) + abs(s0 - s1);
+    }
+    return sum;
+}
+
+// Σ|s−p| of one 4x4 block (sad_scalar, satd_sad.rs:74).
+__device__ __forceinline__ int sad4x4_rows(const uint32_t s[4], const uint32_t p[4]) {
+    return int(__vsadu4(s[0], p[0]) + __vsadu4(s[1], p[1]) + __vsadu4(s[2], p[2]) + __vsadu4(s[3], p[3]));
+}
+
+// ---------------------------------------------------------------------------
+// Quarter-pel prediction from the cached planes
+// ---------------------------------------------------------------------------
+
+// Plane set of one reference picture: F|H|V|C, each pw×ph, stride pw, the
+// layout HpelPlanes holds (inter.rs:707).
+struct Planes {
+    const uint8_t* base;  // F at base, H at +ps, V at +2ps, C at +3ps
+    int pw, ph, pad;
+    long long ps;
+    __device__ __forceinline__ const uint8_t* plane(int i) const { return base + ps * i; }
+};
+
+// Operand table of the quarter phases (inter.rs:1086-1099, mectx.rs:143-156):
+// plane a at (+dxa,+dya), plane b at (+dxb,+dyb); planes 0=F 1=H 2=V 3=C.
+// Half/full phases use one plane (inter.rs:1024-1035).
+struct PhaseOps { int8_t pa, dxa, dya, pb, dxb, dyb; };
+
+__device__ __forceinline__ PhaseOps phase_ops(int fx, int fy) {
+    switch (fx * 4 + fy) {
+        case 0 * 4 + 0: return {0, 0, 0, -1, 0, 0};
+        case 2 * 4 + 0: return {1, 0, 0, -1, 0, 0};
+        case 0 * 4 + 2: return {2, 0, 0, -1, 0, 0};
+        case 2 * 4 + 2: return {3, 0, 0, -1, 0, 0};
+        case 1 * 4 + 0: return {0, 0, 0, 1, 0, 0};
+        case 3 * 4 + 0: return {0, 1, 0, 1, 0, 0};
+        case 0 * 4 + 1: return {0, 0, 0, 2, 0, 0};
+        case 0 * 4 + 3: return {0, 0, 1, 2, 0, 0};
+        case 1 * 4 + 1: return {1, 0, 0, 2, 0, 0};
+        case 3 * 4 + 1: return {1, 0, 0, 2, 1, 0};
+        case 1 * 4 + 3: return {1, 0, 1, 2, 0, 0};
+        case 3 * 4 + 3: return {1, 0, 1, 2, 1, 0};
+        case 2 * 4 + 1: return {1, 0, 0, 3, 0, 0};
+        case 2 * 4 + 3: return {1, 0, 1, 3, 0, 0};
+        case 1 * 4 + 2: return {2, 0, 0, 3, 0, 0};
+        default:        return {2, 1, 0, 3, 0, 0};  // (3,2)
+    }
+}
+
+// The four packed prediction rows of the 4x4 block whose top-left full-pel
+// sample is (ix, iy) in picture coordinates, at phase (fx, fy).  Equal to
+// mc_luma (inter.rs:1193) for every position: inside the padded planes the rows
+// are plane reads (and the (a+b+1)>>1 average, which __vavgu4 computes per
+// byte); outside, every operand coordinate is clamped to the plane, which
+// reproduces mc_luma's per-tap clamping because the planes are built from the
+// edge-replicated picture with a pad of at least 3.
+__device__ __forceinline__ void pred_rows(const Planes& P, int ix, int iy, int fx, int fy, uint32_t out[4]) {
+    const PhaseOps op = phase_ops(fx, fy);
+    const int px = ix + P.pad, py = iy + P.pad;
+    const bool inside = px >= 0 && py >= 0 && px + 5 <= P.pw && py + 5 <= P.ph;
+    if (inside) {
+        const uint8_t* a = P.plane(op.pa) + (long long)(py + op.dya) * P.pw + px + op.dxa;
+        if (op.pb < 0) {
+#pragma unroll
+            for (int r = 0; r < 4; r++) out[r] = ld4u(a + (long long)r * P.pw);
+        } else {
+            const uint8_t* b = P.plane(op.pb) + (long long)(py + op.dyb) * P.pw + px + op.dxb;
+#pragma unroll
+            for (int r = 0; r < 4; r++) out[r] = __vavgu4(ld4u(a + (long long)r * P.pw), ld4u(b + (long long)r * P.pw));
+        }
+        return;
+    }
+    const uint8_t* A = P.plane(op.pa);
+    const uint8_t* B = P.plane(op.pb < 0 ? op.pa : op.pb);
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+        uint32_t w = 0;
+        const int ya = clampi(py + r + op.dya, 0, P.ph - 1);
+        const int yb = clampi(py + r + op.dyb, 0, P.ph - 1);
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            int v = __ldg(A + (long long)ya * P.pw + clampi(px + c + op.dxa, 0, P.pw - 1));
+            if (op.pb >= 0) {
+                const int u = __ldg(B + (long long)yb * P.pw + clampi(px + c + op.dxb, 0, P.pw - 1));
+                v = (v + u + 1) >> 1;
+            }
+            w |= uint32_t(v) << (8 * c);
+        }
+        out[r] = w;
+    }
+}
+
+// Packed rows of a full-pel 4x4 block read from a plain picture with clamped
+// coordinates (mc_luma's full-pel arm, inter.rs:1213-1243).
+__device__ __forceinline__ void fullpel_rows_clamped(const uint8_t* pic, int w, int h, int x, int y, uint32_t out[4]) {
+    if (x >= 0 && y >= 0 && x + 4 <= w && y + 4 <= h) {
+#pragma unroll
+        for (int r = 0; r < 4; r++) out[r] = ld4u(pic + (long long)(y + r) * w + x);
+        return;
+    }
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+        const int yy = clampi(y + r, 0, h - 1);
+        uint32_t v = 0;
+#pragma unroll
+        for (int c = 0; c < 4; c++) v |= uint32_t(__ldg(pic + (long long)yy * w + clampi(x + c, 0, w - 1))) << (8 * c);
+        out[r] = v;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Rate model and λ pricing (mb16.rs:2454-2482, 2540-2578)
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ uint32_t mvbits(int kind, const uint16_t* tab, int d) {
+    if (kind == 1 || kind == 2) {
+        unsigned a = unsigned(d < 0 ? -d : d);
+        if (a > 4095u) a = 4095u;
+        return __ldg(tab + a);
+    }
+    const uint32_t codenum = d > 0 ? uint32_t(2 * d - 1) : uint32_t(-2 * d);
+    return 1u + 2u * (31u - uint32_t(__clz(int(codenum + 1u))));
+}
+
+// (λ·rate as f64) as i64: one IEEE double multiply rounded to nearest, then
+// truncation toward zero, the same two steps the reference performs.
+__device__ __forceinline__ long long lam_cost(double lam, uint32_t rate) {
+    return __double2ll_rz(__dmul_rn(lam, double(rate)));
+}
+
+// ---------------------------------------------------------------------------
+// Warp helpers
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ int warp_seg_sum(int v, int seg) {
+    // sum over aligned groups of `seg` lanes (seg a power of two <= 32)
+    for (int o = seg >> 1; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+}  // namespace h264a

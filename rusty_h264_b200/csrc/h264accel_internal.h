@@ -1,0 +1,59 @@
+// h264accel_internal.h -- host-side plumbing shared by the .cu files of
+// libh264accel_cuda.so (context, error reporting, launch helpers).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+#include "../../include/h264accel.h"
+
+struct h264a_ctx {
+    int device = 0;
+    int num_sms = 0;
+    cudaStream_t stream = nullptr;
+    // device scratch of the persistent ME kernel: work-queue counter, per-MB
+    // done flags, and a status word (error code + where it happened)
+    int32_t *d_counter = nullptr;
+    int32_t *d_flags = nullptr;
+    size_t flags_cap = 0;      // number of int32 flags allocated
+    int32_t *d_status = nullptr;
+    int32_t epoch = 0;         // value a finished MB writes into its flag
+    // cached buffers of h264a_pixel_path_host
+    void *pp_buf = nullptr;
+    size_t pp_bytes = 0;
+};
+
+namespace h264a {
+
+void set_error(const std::string &msg);
+int fail(int code, const std::string &msg);
+int cuda_fail(cudaError_t e, const char *what);
+inline cudaStream_t pick_stream(h264a_ctx *ctx, void *s) {
+    return s ? reinterpret_cast<cudaStream_t>(s) : ctx->stream;
+}
+int check_launch(const char *what);
+// grows the per-MB done flags to at least n entries (zeroed, epoch reset)
+int ensure_me_scratch(h264a_ctx *ctx, size_t n);
+// the flag value of the next persistent launch on `st`
+int next_epoch(h264a_ctx *ctx, cudaStream_t st);
+
+// Device-side mirror of h264a_me_params with only the fields the kernels read.
+struct MeParamsDev {
+    int32_t fast, use_sad, sadfp, kind;
+    const uint16_t *tab;
+    double sadfp_lambda;
+    int32_t me_snap, fc;
+    uint32_t dia_mask, dia_sub_mask;
+    int32_t subpel, subpel_pat, sp_single_pass, sub_pat, me_subpel_iter, sp_maxit, sp_fc;
+};
+MeParamsDev to_dev(const h264a_me_params &p);
+
+}  // namespace h264a
+
+#define H264A_CUDA(call)                                              \
+    do {                                                              \
+        cudaError_t e_ = (call);                                      \
+        if (e_ != cudaSuccess) return ::h264a::cuda_fail(e_, #call); \
+    } while (0)

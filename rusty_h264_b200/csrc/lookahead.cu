@@ -1,0 +1,295 @@
+// lookahead.cu -- a16-a19: the mb-tree lookahead's per-frame costs
+// (crates/rusty_h264-encoder/src/mbtree.rs:61-263).
+//
+//  * downsample2x: one thread per four output pixels, 8-byte loads.
+//  * intra_cost: one lane per 4x4 sub-block, Σ|Hadamard AC| reduced per MB.
+//  * inter_cost + frame_costs: the seeded full-pel diamond.  The seed chain
+//    (left MV, else top MV; mbtree.rs:225-231) makes every row a sequential
+//    chain that starts from column 0, and column 0 a chain down the frame.
+//    Frames are independent (source domain, f against f-1), so one warp walks
+//    the column-0 chain of each frame, then one warp per (frame, row) walks
+//    the rest of the row.  Inside a search the warp prices the four ring
+//    points of the cascading diamond together and takes the first improvement,
+//    re-pricing the rest of the ring around the moved centre (the reference's
+//    evaluation order).
+#include "h264a_device.cuh"
+
+namespace h264a {
+
+__global__ void downsample2x_kernel(const uint8_t* __restrict__ in, int cw, int ch, size_t fstride,
+                                    uint8_t* __restrict__ out) {
+    const int hw = cw / 2, hh = ch / 2;
+    const int f = blockIdx.z;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;  // group of 4 outputs
+    const int groups_per_row = hw / 4;
+    if (t >= (long long)groups_per_row * hh) return;
+    const int j = int(t / groups_per_row), i4 = int(t % groups_per_row) * 4;
+    const uint8_t* a = in + fstride * f + (long long)(2 * j) * cw + 2 * i4;
+    const uint2 r0 = *reinterpret_cast<const uint2*>(a);
+    const uint2 r1 = *reinterpret_cast<const uint2*>(a + cw);
+    uint32_t o = 0;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const uint32_t w0 = k < 2 ? r0.x : r0.y, w1 = k < 2 ? r1.x : r1.y;
+        const int sh = (k & 1) * 16;
+        const uint32_t s = ((w0 >> sh) & 255) + ((w0 >> (sh + 8)) & 255) + ((w1 >> sh) & 255) + ((w1 >> (sh + 8)) & 255);
+        o |= ((s + 2) / 4) << (8 * k);
+    }
+    *reinterpret_cast<uint32_t*>(out + (size_t)hw * hh * f + (long long)j * hw + i4) = o;
+}
+
+// Scoring-resolution geometry of one lookahead mode.
+struct LaGeom {
+    int bs;        // block size at the scoring resolution (8 HalfRes, 16 otherwise)
+    int sw, sh;    // scoring picture size
+};
+
+// intra_cost (mbtree.rs:78-93) of every MB of every frame; frame 0 (IDR) also
+// gets inter = intra, mv = 0 (mbtree.rs:257).
+__global__ void la_intra_kernel(const uint8_t* __restrict__ pics, size_t fstride, LaGeom g, int mb_w, int mb_h, int n,
+                                int32_t* __restrict__ intra, int32_t* __restrict__ inter, int32_t* __restrict__ mvs) {
+    const int lg = g.bs == 16 ? 4 : 2;  // sub-blocks per MB: 16 or 4
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long gm = t >> lg;  // global MB index
+    const long long nmb = (long long)mb_w * mb_h;
+    const int sb = int(t & ((1 << lg) - 1));
+    int v = 0;
+    const bool live = gm < nmb * n;
+    if (live) {
+        const int f = int(gm / nmb), m = int(gm % nmb);
+        const int mbx = m % mb_w, mby = m / mb_w;
+        const int nbx = g.bs / 4;
+        const int x = mbx * g.bs + (sb % nbx) * 4, y = mby * g.bs + (sb / nbx) * 4;
+        const uint8_t* p = pics + fstride * f + (long long)y * g.sw + x;
+        uint32_t s[4];
+        const uint32_t z[4] = {0, 0, 0, 0};
+#pragma unroll
+        for (int r = 0; r < 4; r++) s[r] = ld4u(p + (long long)r * g.sw);
+        const int dc = int(__vsadu4(s[0], 0) + __vsadu4(s[1], 0) + __vsadu4(s[2], 0) + __vsadu4(s[3], 0));
+        v = satd4x4_rows(s, z) - dc;  // Σ|AC|: the DC coefficient is the (non-negative) block sum
+    }
+    v = warp_seg_sum(v, 1 << lg);
+    if (live && sb == 0) {
+        const int c = v < 1 ? 1 : v;
+        intra[gm] = c;
+        if (gm < nmb) {  // frame 0: the IDR, no reference
+            inter[gm] = c;
+            mvs[2 * gm] = 0;
+            mvs[2 * gm + 1] = 0;
+        }
+    }
+}
+
+// One warp's view of a full-pel SATD search of a bs x bs block.
+struct LaSearch {
+    const uint8_t* cur;
+    const uint8_t* ref;
+    int w, h, bs, lg_nb, lane, bxo, byo, x0, y0;
+    uint32_t srow[4];
+    int2* cand;
+    int* dist;
+
+    __device__ void init(const uint8_t* c, const uint8_t* r, int pw, int ph, int b, int bx0, int by0, int2* cs,
+                         int* ds) {
+        cur = c; ref = r; w = pw; h = ph; bs = b; x0 = bx0; y0 = by0; cand = cs; dist = ds;
+        lane = threadIdx.x & 31;
+        lg_nb = b == 16 ? 4 : 2;
+        const int nbx = b / 4;
+        const int sb = lane & ((1 << lg_nb) - 1);
+        bxo = (sb % nbx) * 4;
+        byo = (sb / nbx) * 4;
+#pragma unroll
+        for (int r = 0; r < 4; r++) srow[r] = ld4u(cur + (long long)(y0 + byo + r) * w + x0 + bxo);
+    }
+
+    // SATD of cand[0..n) (full-pel MVs, quarter-pel units) into dist.
+    __device__ void eval(int n) {
+        const int nb = 1 << lg_nb;
+        for (int base = 0; base < (n << lg_nb); base += 32) {
+            const int c = (base + lane) >> lg_nb;
+            int d = 0;
+            if (c < n) {
+                const int2 mv = cand[c];
+                uint32_t p[4];
+                fullpel_rows_clamped(ref, w, h, x0 + bxo + (mv.x >> 2), y0 + byo + (mv.y >> 2), p);
+                d = satd4x4_rows(srow, p);
+            }
+            d = warp_seg_sum(d, nb);
+            if (c < n && (lane & (nb - 1)) == 0) dist[c] = d;
+        }
+        __syncwarp();
+    }
+};
+
+// inter_cost (mbtree.rs:154-197): returns cost (capped to i32) and MV.
+__device__ void la_inter_cost(LaSearch& s, int seedx, int seedy, int max_step, int& cost, int& mvx, int& mvy) {
+    if (s.lane == 0) {
+        s.cand[0] = make_int2(0, 0);
+        s.cand[1] = make_int2(seedx, seedy);
+    }
+    __syncwarp();
+    s.eval(2);
+    long long best = s.dist[0];
+    int bx = 0, by = 0;
+    if (best != 0) {
+        if ((seedx != 0 || seedy != 0) && s.dist[1] < best) {
+            best = s.dist[1];
+            bx = seedx;
+            by = seedy;
+        }
+        __syncwarp();
+        const int rx[4] = {1, -1, 0, 0}, ry[4] = {0, 0, 1, -1};
+        for (int step = max_step; step >= 1; step >>= 1) {
+            for (int guard = 0; guard < (1 << 20); guard++) {
+                bool moved = false;
+                int i = 0;
+                while (i < 4) {
+                    const int n = 4 - i;
+                    if (s.lane < n) s.cand[s.lane] = make_int2(bx + rx[i + s.lane] * step * 4, by + ry[i + s.lane] * step * 4);
+                    __syncwarp();
+                    s.eval(n);
+                    const int d = s.lane < n ? s.dist[s.lane] : 0;
+                    const unsigned hit = __ballot_sync(0xffffffffu, s.lane < n && (long long)d < best);
+                    if (hit == 0) {
+                        __syncwarp();
+                        break;
+                    }
+                    const int j = __ffs(hit) - 1;
+                    best = __shfl_sync(0xffffffffu, d, j);
+                    bx = s.cand[j].x;
+                    by = s.cand[j].y;
+                    moved = true;
+                    i += j + 1;
+                    __syncwarp();
+                }
+                if (!moved) break;
+            }
+        }
+    }
+    __syncwarp();
+    cost = best > 0x7fffffffLL ? 0x7fffffff : int(best);
+    mvx = bx;
+    mvy = by;
+}
+
+struct LaBufs {
+    const uint8_t* full;  // n frames cw x ch
+    const uint8_t* half;  // n frames cw/2 x ch/2 (modes 1, 2)
+    int cw, ch, mb_w, mb_h, n, mode;
+    int32_t* intra;
+    int32_t* inter;
+    int32_t* mvs;
+};
+
+// frame_costs for MB (mbx, mby) of frame f >= 1 given the full-res seed.
+__device__ void la_mb(const LaBufs& b, int f, int mbx, int mby, int sfx, int sfy, int2* cs, int* ds, int& outx,
+                      int& outy) {
+    const long long nmb = (long long)b.mb_w * b.mb_h;
+    const long long gm = nmb * f + (long long)mby * b.mb_w + mbx;
+    const int cwh = b.cw / 2, chh = b.ch / 2;
+    const size_t fs = (size_t)b.cw * b.ch, hs = (size_t)cwh * chh;
+    LaSearch s;
+    int cost, mx, my;
+    if (b.mode == 0) {  // FullRes
+        s.init(b.full + fs * f, b.full + fs * (f - 1), b.cw, b.ch, 16, mbx * 16, mby * 16, cs, ds);
+        la_inter_cost(s, sfx, sfy, 8, cost, mx, my);
+    } else {
+        s.init(b.half + hs * f, b.half + hs * (f - 1), cwh, chh, 8, mbx * 8, mby * 8, cs, ds);
+        int hx, hy;
+        la_inter_cost(s, sfx / 2, sfy / 2, 8, cost, hx, hy);
+        if (b.mode == 2) {  // HalfRes
+            mx = hx * 2;
+            my = hy * 2;
+        } else {  // Hybrid: refine at full-res from the coarse MV
+            s.init(b.full + fs * f, b.full + fs * (f - 1), b.cw, b.ch, 16, mbx * 16, mby * 16, cs, ds);
+            la_inter_cost(s, hx * 2, hy * 2, 2, cost, mx, my);
+        }
+    }
+    if (s.lane == 0) {
+        const int ic = b.intra[gm];
+        b.inter[gm] = cost < ic ? cost : ic;
+        b.mvs[2 * gm] = mx;
+        b.mvs[2 * gm + 1] = my;
+    }
+    outx = mx;
+    outy = my;
+}
+
+constexpr int LA_WARPS = 4;
+
+// Column 0 of every frame f >= 1 (one warp per frame).
+__global__ void __launch_bounds__(32 * LA_WARPS) la_col0_kernel(LaBufs b) {
+    __shared__ int2 cs[LA_WARPS][32];
+    __shared__ int ds[LA_WARPS][32];
+    const int w = threadIdx.x >> 5;
+    const int f = 1 + blockIdx.x * LA_WARPS + w;
+    if (f >= b.n) return;
+    int sx = 0, sy = 0;
+    for (int mby = 0; mby < b.mb_h; mby++) {
+        int mx, my;
+        la_mb(b, f, 0, mby, sx, sy, cs[w], ds[w], mx, my);
+        sx = mx;
+        sy = my;
+    }
+}
+
+// Columns 1.. of every row of every frame f >= 1 (one warp per row), seeded by
+// the left neighbour (column 0 comes from la_col0_kernel).
+__global__ void __launch_bounds__(32 * LA_WARPS) la_rows_kernel(LaBufs b) {
+    __shared__ int2 cs[LA_WARPS][32];
+    __shared__ int ds[LA_WARPS][32];
+    const int w = threadIdx.x >> 5;
+    const long long r = (long long)blockIdx.x * LA_WARPS + w;  // (frame-1) * mb_h + row
+    if (r >= (long long)(b.n - 1) * b.mb_h) return;
+    const int f = 1 + int(r / b.mb_h), mby = int(r % b.mb_h);
+    const long long gm0 = (long long)b.mb_w * b.mb_h * f + (long long)mby * b.mb_w;
+    int sx = b.mvs[2 * gm0], sy = b.mvs[2 * gm0 + 1];
+    for (int mbx = 1; mbx < b.mb_w; mbx++) {
+        int mx, my;
+        la_mb(b, f, mbx, mby, sx, sy, cs[w], ds[w], mx, my);
+        sx = mx;
+        sy = my;
+    }
+}
+
+}  // namespace h264a
+
+using namespace h264a;
+
+extern "C" int h264a_downsample2x(h264a_ctx* ctx, const uint8_t* d_frames, int cw, int ch, int n, size_t frame_stride,
+                                  uint8_t* d_half, void* stream) {
+    if (!ctx || !d_frames || !d_half) return fail(H264A_E_ARG, "downsample2x: null pointer");
+    if (cw < 16 || ch < 16 || cw % 16 || ch % 16 || n < 1 || n > 65535)
+        return fail(H264A_E_ARG, "downsample2x: frames must be MB-aligned, 1 <= n <= 65535");
+    if (frame_stride % 8 || (n > 1 && frame_stride < (size_t)cw * ch) ||
+        (reinterpret_cast<uintptr_t>(d_frames) & 7) || (reinterpret_cast<uintptr_t>(d_half) & 3))
+        return fail(H264A_E_ARG, "downsample2x: misaligned frames");
+    const long long groups = (long long)(cw / 8) * (ch / 2);
+    dim3 grid(unsigned((groups + 255) / 256), 1, n);
+    downsample2x_kernel<<<grid, 256, 0, pick_stream(ctx, stream)>>>(d_frames, cw, ch, frame_stride, d_half);
+    return check_launch("downsample2x_kernel");
+}
+
+extern "C" int h264a_lookahead_costs(h264a_ctx* ctx, const uint8_t* d_full, const uint8_t* d_half, int cw, int ch, int n,
+                                     int mode, int32_t* d_intra, int32_t* d_inter, int32_t* d_mvs, void* stream) {
+    if (!ctx || !d_full || !d_intra || !d_inter || !d_mvs) return fail(H264A_E_ARG, "lookahead_costs: null pointer");
+    if (mode < 0 || mode > 2) return fail(H264A_E_ARG, "lookahead_costs: mode must be 0 (full), 1 (hybrid) or 2 (half)");
+    if (mode != 0 && !d_half) return fail(H264A_E_ARG, "lookahead_costs: modes 1 and 2 need the half-res frames");
+    if (cw < 16 || ch < 16 || cw % 16 || ch % 16 || n < 1) return fail(H264A_E_ARG, "lookahead_costs: bad geometry");
+    cudaStream_t st = pick_stream(ctx, stream);
+    LaBufs b{d_full, d_half, cw, ch, cw / 16, ch / 16, n, mode, d_intra, d_inter, d_mvs};
+    const LaGeom g = mode == 2 ? LaGeom{8, cw / 2, ch / 2} : LaGeom{16, cw, ch};
+    const size_t fstride = mode == 2 ? (size_t)(cw / 2) * (ch / 2) : (size_t)cw * ch;
+    const long long nmb = (long long)(cw / 16) * (ch / 16);
+    const long long threads = nmb * n * (g.bs == 16 ? 16 : 4);
+    la_intra_kernel<<<unsigned((threads + 255) / 256), 256, 0, st>>>(mode == 2 ? d_half : d_full, fstride, g, cw / 16,
+                                                                    ch / 16, n, d_intra, d_inter, d_mvs);
+    int rc = check_launch("la_intra_kernel");
+    if (rc || n < 2) return rc;
+    la_col0_kernel<<<unsigned((n - 1 + LA_WARPS - 1) / LA_WARPS), 32 * LA_WARPS, 0, st>>>(b);
+    rc = check_launch("la_col0_kernel");
+    if (rc) return rc;
+    const long long rows = (long long)(n - 1) * (ch / 16);
+    la_rows_kernel<<<unsigned((rows + LA_WARPS - 1) / LA_WARPS), 32 * LA_WARPS, 0, st>>>(b);
+    return check_launch("la_rows_kernel");
+}

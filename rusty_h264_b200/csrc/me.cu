@@ -1,0 +1,631 @@
+// me.cu -- a10/a11/a12: motion_search (crates/rusty_h264-encoder/src/mb16.rs:
+// 2433-3302), best_part (:4921) and the plain-ME frame pass.
+//
+// One warp runs one search.  Each lane owns one 4x4 sub-block of the
+// partition (its source rows stay in registers for the whole search), so a
+// pass over 32 lanes prices 32/nb candidates at once (nb = sub-blocks per
+// partition).  Control flow is warp-uniform and replays the reference exactly:
+//  * fixed-centre diamond passes and batched rings price their 4/8 candidates
+//    together, then take the first strict-minimum like the reference's argmin;
+//  * cascading rings (the centre moves mid-ring) are priced speculatively
+//    against the current centre; the first improving point is taken and the
+//    remaining points are re-priced around the new centre, which is exactly
+//    the order in which the reference evaluates them.
+// λ·rate is computed as an IEEE double product truncated toward zero, the
+// same arithmetic as `(λ·rate as f64) as i64`.
+#include <algorithm>
+#include <climits>
+#include <cstring>
+#include <vector>
+
+#include "h264a_device.cuh"
+
+namespace h264a {
+
+constexpr int MET_SATD = 0;
+constexpr int MET_SAD = 1;
+
+struct MePic {
+    Planes P;
+    const uint8_t* src;
+    int cw, ch;
+};
+
+__device__ __forceinline__ MePic make_pic(const h264a_picture& pc) {
+    MePic m;
+    m.P.base = pc.d_planes;
+    m.P.pad = pc.pad;
+    m.P.pw = pc.cw + 2 * pc.pad;
+    m.P.ph = pc.ch + 2 * pc.pad;
+    m.P.ps = (long long)m.P.pw * m.P.ph;
+    m.src = pc.d_src;
+    m.cw = pc.cw;
+    m.ch = pc.ch;
+    return m;
+}
+
+// Per-warp shared scratch: candidate MVs and their distortions.
+struct WarpScratch {
+    int2 cand[32];
+    int dist[32];
+};
+
+struct Search {
+    MePic pic;
+    const MeParamsDev* pr;
+    int lx, ly, rw, rh, lg_nb, lane;
+    int bxo, byo;  // this lane's sub-block offset inside the partition
+    uint32_t srow[4];
+    int cx, cy;    // mvd centre (predictors[0])
+    double lam_r, lam_fp, lam_me;
+    bool sadfp;
+    int m_main;    // metric of `cost`
+    int evals_ref, evals_done;
+    WarpScratch* ws;
+
+    __device__ void init(const MePic& p, const MeParamsDev* prm, int x, int y, int w, int h, int centre_x,
+                         int centre_y, double lambda_me, bool refine_only, WarpScratch* scratch) {
+        pic = p;
+        pr = prm;
+        lx = x; ly = y; rw = w; rh = h;
+        lane = threadIdx.x & 31;
+        lg_nb = (w == 16 ? 2 : (w == 8 ? 1 : 0)) + (h == 16 ? 2 : (h == 8 ? 1 : 0));
+        const int nbx = w >> 2;
+        const int blk = lane & ((1 << lg_nb) - 1);
+        bxo = (blk % nbx) * 4;
+        byo = (blk / nbx) * 4;
+#pragma unroll
+        for (int r = 0; r < 4; r++) srow[r] = ld4u(p.src + (long long)(y + byo + r) * p.cw + x + bxo);
+        cx = centre_x; cy = centre_y;
+        lam_me = lambda_me;
+        lam_r = prm->kind != 0 ? lambda_me * 0.25 : lambda_me;
+        sadfp = !prm->fast && !refine_only && prm->sadfp;
+        lam_fp = lambda_me * (sadfp ? prm->sadfp_lambda : 1.0);
+        m_main = prm->use_sad ? MET_SAD : MET_SATD;
+        evals_ref = 0;
+        evals_done = 0;
+        ws = scratch;
+    }
+
+    __device__ __forceinline__ uint32_t rate(int mvx, int mvy) const {
+        return mvbits(pr->kind, pr->tab, mvx - cx) + mvbits(pr->kind, pr->tab, mvy - cy);
+    }
+
+    // Distortions of ws->cand[0..n) under `metric` into ws->dist.
+    __device__ void eval(int n, int metric) {
+        const int nb = 1 << lg_nb;
+        const int total = n << lg_nb;
+        for (int base = 0; base < total; base += 32) {
+            const int p = base + lane;
+            const int c = p >> lg_nb;
+            int d = 0;
+            if (c < n) {
+                const int2 mv = ws->cand[c];
+                uint32_t pr4[4];
+                pred_rows(pic.P, lx + bxo + (mv.x >> 2), ly + byo + (mv.y >> 2), mv.x & 3, mv.y & 3, pr4);
+                d = metric == MET_SAD ? sad4x4_rows(srow, pr4) : satd4x4_rows(srow, pr4);
+            }
+            d = warp_seg_sum(d, nb);
+            if (c < n && (lane & (nb - 1)) == 0) ws->dist[c] = d;
+        }
+        __syncwarp();
+        evals_done += n;
+    }
+
+    // Price candidate `lane` (if lane < n): dist + (lam·rate) as i64.
+    __device__ __forceinline__ long long lane_cost(int n, double lam) const {
+        if (lane >= n) return LLONG_MAX;
+        const int2 mv = ws->cand[lane];
+        return (long long)ws->dist[lane] + lam_cost(lam, rate(mv.x, mv.y));
+    }
+
+    // First-wins argmin over lanes < n; returns index or -1 if none beats best_c.
+    __device__ int argmin_below(long long cc, long long best_c, long long& out_c) const {
+        long long v = cc;
+        int idx = lane;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const long long ov = __shfl_xor_sync(0xffffffffu, v, o);
+            const int oi = __shfl_xor_sync(0xffffffffu, idx, o);
+            if (ov < v || (ov == v && oi < idx)) { v = ov; idx = oi; }
+        }
+        out_c = v;
+        return v < best_c ? idx : -1;
+    }
+
+    // Fixed-centre batch of n candidates already in ws->cand: the first strict
+    // minimum below best_c (or -1).  Prices with `lam`; counts n reference evals.
+    __device__ int fixed_batch(int n, int metric, double lam, long long best_c, long long& bc) {
+        eval(n, metric);
+        const long long cc = lane_cost(n, lam);
+        const int bi = argmin_below(cc, best_c, bc);
+        evals_ref += n;
+        __syncwarp();
+        return bi;
+    }
+
+    // Cascading ring around a moving centre (the reference's first-improver
+    // walk).  ring offsets (dx,dy)*step; returns whether any point improved.
+    __device__ bool cascade_ring(const int8_t* rx, const int8_t* ry, int nring, int step, int metric, double lam,
+                                 long long& best_c, int& bx, int& by) {
+        bool improved = false;
+        int i = 0;
+        while (i < nring) {
+            const int n = nring - i;
+            if (lane < n) ws->cand[lane] = make_int2(bx + rx[i + lane] * step, by + ry[i + lane] * step);
+            __syncwarp();
+            eval(n, metric);
+            const long long cc = lane_cost(n, lam);
+            const unsigned hit = __ballot_sync(0xffffffffu, lane < n && cc < best_c);
+            if (hit == 0) {
+                evals_ref += n;
+                __syncwarp();
+                break;
+            }
+            const int j = __ffs(hit) - 1;
+            const long long cj = __shfl_sync(0xffffffffu, cc, j);
+            const int2 mv = ws->cand[j];
+            evals_ref += j + 1;
+            best_c = cj;
+            bx = mv.x;
+            by = mv.y;
+            improved = true;
+            i += j + 1;
+            __syncwarp();
+        }
+        return improved;
+    }
+
+    __device__ bool in_plane_window(int mvx, int mvy) const {
+        const int px = lx + (mvx >> 2) + pic.P.pad, py = ly + (mvy >> 2) + pic.P.pad;
+        return px >= 0 && py >= 0 && px + rw + 1 <= pic.P.pw && py + rh + 1 <= pic.P.ph;
+    }
+};
+
+__constant__ int8_t kRingX[8] = {1, -1, 0, 0, 1, -1, 1, -1};
+__constant__ int8_t kRingY[8] = {0, 0, 1, -1, 1, -1, -1, 1};
+
+// motion_search for one partition (warp-cooperative, uniform control flow).
+__device__ void motion_search_warp(Search& s, const int* preds, int npred, const int* start, int& out_x, int& out_y,
+                                   long long& out_c) {
+    const MeParamsDev& pr = *s.pr;
+    const bool refine_only = start != nullptr;
+    const int m_fp = s.sadfp ? MET_SAD : s.m_main;
+    const double l_fp = s.sadfp ? s.lam_fp : s.lam_r;  // cost_fp's λ (cost's λ when B2 is off)
+    int bx = 0, by = 0;
+    long long best_c;
+    long long bc;
+    // ---- seeds (mb16.rs:2580-2596) ----
+    if (refine_only) {
+        bx = start[0]; by = start[1];
+        if (s.lane == 0) s.ws->cand[0] = make_int2(bx, by);
+        __syncwarp();
+        s.eval(1, s.m_main);
+        best_c = (long long)s.ws->dist[0] + lam_cost(s.lam_r, s.rate(bx, by));
+        s.evals_ref += 1;
+        __syncwarp();
+    } else {
+        if (s.lane == 0) s.ws->cand[0] = make_int2(0, 0);
+        if (s.lane >= 1 && s.lane <= npred) s.ws->cand[s.lane] = make_int2(preds[2 * (s.lane - 1)], preds[2 * (s.lane - 1) + 1]);
+        __syncwarp();
+        s.eval(npred + 1, m_fp);
+        const long long cc = s.lane_cost(npred + 1, l_fp);
+        // sequential strict-< scan: (0,0) first, then predictors in order
+        best_c = __shfl_sync(0xffffffffu, cc, 0);
+        for (int i = 1; i <= npred; i++) {
+            const long long ci = __shfl_sync(0xffffffffu, cc, i);
+            if (ci < best_c) {
+                best_c = ci;
+                bx = s.ws->cand[i].x;
+                by = s.ws->cand[i].y;
+            }
+        }
+        s.evals_ref += npred + 1;
+        __syncwarp();
+    }
+    const int seed_x = bx, seed_y = by;
+    long long seed_c = best_c;
+    // ---- integer snap (mb16.rs:2597-2607) ----
+    if (!refine_only && pr.me_snap && ((bx & 3) != 0 || (by & 3) != 0)) {
+        const int sx = ((bx + 2) >> 2) * 4, sy = ((by + 2) >> 2) * 4;
+        if (s.lane == 0) s.ws->cand[0] = make_int2(sx, sy);
+        __syncwarp();
+        s.eval(1, m_fp);
+        best_c = (long long)s.ws->dist[0] + lam_cost(l_fp, s.rate(sx, sy));
+        s.evals_ref += 1;
+        bx = sx; by = sy;
+        __syncwarp();
+    }
+    // ---- diamond ladder (mb16.rs:2616-2727) ----
+    if (!refine_only) {
+        int steps[5];
+        int nsteps = 0;
+        if (pr.fast) {
+            steps[0] = 16; steps[1] = 4; nsteps = 2;
+        } else {
+            const uint32_t mask = (s.rw < 8 || s.rh < 8) ? pr.dia_sub_mask : pr.dia_mask;
+            const int rungs[5] = {64, 32, 16, 8, 4};
+#pragma unroll
+            for (int i = 0; i < 5; i++)
+                if (mask & (1u << i)) steps[nsteps++] = rungs[i];
+        }
+        const bool x4shape = (s.rw == 16 || s.rw == 8) && (s.rh == 16 || s.rh == 8);
+        const bool fc = !pr.fast && pr.fc && x4shape;
+        for (int si = 0; si < nsteps; si++) {
+            const int step = steps[si];
+            for (int guard = 0; guard < (1 << 20); guard++) {
+                if (fc && (bx & 3) == 0 && (by & 3) == 0) {
+                    const int st = step >> 2;
+                    const int px = s.lx + (bx >> 2), py = s.ly + (by >> 2);
+                    if (px - st >= 0 && py - st >= 0 && px + st + s.rw <= s.pic.cw && py + st + s.rh <= s.pic.ch) {
+                        if (s.lane < 4) s.ws->cand[s.lane] = make_int2(bx + kRingX[s.lane] * step, by + kRingY[s.lane] * step);
+                        __syncwarp();
+                        int bi;
+                        if (s.rw == 16) {
+                            // sad_x4 / satd_x4 batch priced with lam_fp (mb16.rs:2676-2690)
+                            bi = s.fixed_batch(4, s.sadfp ? MET_SAD : MET_SATD, s.lam_fp, best_c, bc);
+                        } else {
+                            // 8-wide shapes price each point with cost_fp (mb16.rs:2691)
+                            bi = s.fixed_batch(4, m_fp, l_fp, best_c, bc);
+                        }
+                        if (bi < 0) break;
+                        best_c = bc;
+                        bx += kRingX[bi] * step;
+                        by += kRingY[bi] * step;
+                        continue;
+                    }
+                }
+                if (!s.cascade_ring(kRingX, kRingY, 4, step, m_fp, l_fp, best_c, bx, by)) break;
+            }
+        }
+    }
+    // ---- B2 reprice into the SATD domain (mb16.rs:2744-2747) ----
+    if (s.sadfp) {
+        if (s.lane == 0) {
+            s.ws->cand[0] = make_int2(bx, by);
+            s.ws->cand[1] = make_int2(seed_x, seed_y);
+        }
+        __syncwarp();
+        s.eval(2, s.m_main);
+        best_c = (long long)s.ws->dist[0] + lam_cost(s.lam_r, s.rate(bx, by));
+        seed_c = (long long)s.ws->dist[1] + lam_cost(s.lam_r, s.rate(seed_x, seed_y));
+        s.evals_ref += 2;
+        __syncwarp();
+    }
+    // ---- sub-pel rings (mb16.rs:2956-3283) ----
+    if (pr.subpel) {
+        const bool sub_shape = s.rw < 8 || s.rh < 8;
+        const int pat = pr.subpel_pat >= 0 ? pr.subpel_pat : (sub_shape ? pr.sub_pat : (pr.sp_single_pass ? 2 : 0));
+        const bool x4shape = (s.rw == 16 || s.rw == 8) && (s.rh == 16 || s.rh == 8);
+        const bool sp_fc = pr.sp_fc && !pr.fast && x4shape;
+        const int nring = (pat & 1) ? 4 : 8;
+        for (int k = 0; k < 2; k++) {
+            const int step = k == 0 ? 2 : 1;
+            int iter = 0;
+            for (int guard = 0; guard < (1 << 20); guard++) {
+                if (sp_fc && (pat & 1) == 0 && (step == 1 || ((bx & 3) == 0 && (by & 3) == 0))) {
+                    iter++;
+                    bool all = true;
+                    for (int i = 0; i < 8; i++) all = all && s.in_plane_window(bx + kRingX[i] * step, by + kRingY[i] * step);
+                    if (all) {
+                        if (s.lane < 8) s.ws->cand[s.lane] = make_int2(bx + kRingX[s.lane] * step, by + kRingY[s.lane] * step);
+                        __syncwarp();
+                        // 16-wide: satd_avg_x4 / satd_x4p priced with lambda_me; 8-wide: cost()
+                        const int bi = s.rw == 16 ? s.fixed_batch(8, MET_SATD, s.lam_me, best_c, bc)
+                                                  : s.fixed_batch(8, s.m_main, s.lam_r, best_c, bc);
+                        const bool stop = bi < 0 || !pr.me_subpel_iter || (pat & 2) || (pr.sp_maxit != 0 && iter >= pr.sp_maxit);
+                        if (bi >= 0) {
+                            best_c = bc;
+                            bx += kRingX[bi] * step;
+                            by += kRingY[bi] * step;
+                        }
+                        if (stop) break;
+                        continue;
+                    }
+                    iter--;
+                }
+                iter++;
+                const bool improved = s.cascade_ring(kRingX, kRingY, nring, step, s.m_main, s.lam_r, best_c, bx, by);
+                if (!improved || !pr.me_subpel_iter || (pat & 2) || (pr.sp_maxit != 0 && iter >= pr.sp_maxit)) break;
+            }
+        }
+    }
+    // ---- seed restore (mb16.rs:3297-3300) ----
+    if (pr.me_snap && seed_c < best_c) {
+        bx = seed_x; by = seed_y; best_c = seed_c;
+    }
+    out_x = bx; out_y = by; out_c = best_c;
+}
+
+__device__ __forceinline__ bool job_shape_ok(int w, int h) {
+    return (w == 16 && (h == 16 || h == 8)) || (w == 8 && (h == 16 || h == 8 || h == 4)) ||
+           (w == 4 && (h == 8 || h == 4));
+}
+
+constexpr int ME_WARPS = 4;
+
+__global__ void __launch_bounds__(32 * ME_WARPS) me_search_kernel(const h264a_picture* __restrict__ pics, int npics,
+                                                                 MeParamsDev prm, const h264a_me_job* __restrict__ jobs,
+                                                                 int n, h264a_me_result* __restrict__ out) {
+    __shared__ WarpScratch scratch[ME_WARPS];
+    const int w = threadIdx.x >> 5;
+    const long long j = (long long)blockIdx.x * ME_WARPS + w;
+    if (j >= n) return;
+    const h264a_me_job job = jobs[j];
+    h264a_me_result res{};
+    const bool ok = job.pic >= 0 && job.pic < npics && job_shape_ok(job.w, job.h) && job.npred >= 1 && job.npred <= 4;
+    h264a_picture pc{};
+    bool inside = false;
+    if (ok) {
+        pc = pics[job.pic];
+        inside = job.x >= 0 && job.y >= 0 && job.x + job.w <= pc.cw && job.y + job.h <= pc.ch;
+    }
+    if (!ok || !inside) {
+        res.status = -1;
+        if ((threadIdx.x & 31) == 0) out[j] = res;
+        return;
+    }
+    Search s;
+    s.init(make_pic(pc), &prm, job.x, job.y, job.w, job.h, job.preds[0], job.preds[1], job.lambda_me,
+           job.has_start != 0, &scratch[w]);
+    int mx, my;
+    long long c;
+    motion_search_warp(s, job.preds, job.npred, job.has_start ? job.start : nullptr, mx, my, c);
+    if ((threadIdx.x & 31) == 0) {
+        res.mvx = mx; res.mvy = my; res.cost = c; res.evals = s.evals_ref; res.status = 0;
+        out[j] = res;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Plain-ME frames: persistent work-queue kernel
+// ---------------------------------------------------------------------------
+
+struct FrameDesc {
+    h264a_picture pic;
+    double lambda_me;
+    long long split_gate;
+    int32_t* picks;
+    int64_t* costs;
+    int flag_base;
+    int mb_w, mb_h;
+};
+
+// One launch's frames, passed by value.  Frames are sorted by MB count
+// (descending) and the work queue deals MB m of every frame that has one
+// before MB m+1 of any frame: segment j covers MB indices
+// [nmb[j+1], nmb[j]) of frames 0..j, so its tickets are (nmb[j]-nmb[j+1])*(j+1).
+constexpr int ME_MAXF = 96;
+struct FrameBatch {
+    FrameDesc f[ME_MAXF];
+    long long seg_start[ME_MAXF + 1];
+    int n;
+};
+
+constexpr int SPIN_LIMIT = 1000 * 1000;  // ~0.5 s of polling (a 200 ns sleep per poll)
+
+__device__ __forceinline__ int ld_acquire(const int* p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release(int* p, int v) {
+    asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Waits (bounded) until flag == epoch; on timeout records `code` in status.
+__device__ void wait_flag(const int* flag, int epoch, int* status, int code, int limit) {
+    for (int it = 0;; it++) {
+        if (ld_acquire(flag) == epoch) return;
+        if (it >= limit) {
+            atomicCAS(status, 0, code);
+            return;
+        }
+        __nanosleep(200);
+    }
+}
+
+// The MV of neighbour MB `m`'s 4x4 block at (bx4, by4) under its pick.
+__device__ __forceinline__ int2 pick_mv_at(const int32_t* picks, int m, int bx4, int by4) {
+    const int32_t* p = picks + 6 * m;
+    const int shape = __ldcg(p);
+    const int part = shape == 1 ? (by4 >= 2) : (shape == 2 ? (bx4 >= 2) : 0);
+    return make_int2(__ldcg(p + 1 + 2 * part), __ldcg(p + 2 + 2 * part));
+}
+
+// predict_mv (inter.rs:36-69) with every available neighbour inter, ref 0.
+__device__ __forceinline__ int2 predict_mv_ref0(bool aa, int2 a, bool ba, int2 b, bool ca, int2 c) {
+    int2 mva = aa ? a : make_int2(0, 0);
+    int2 mvb = ba ? b : make_int2(0, 0);
+    int2 mvc = ca ? c : make_int2(0, 0);
+    int ra = aa ? 0 : -1, rb = ba ? 0 : -1, rc = ca ? 0 : -1;
+    if (!ba && !ca && aa) { mvb = mva; rb = ra; mvc = mva; rc = ra; }
+    const int matches = (ra == 0) + (rb == 0) + (rc == 0);
+    if (matches == 1) return ra == 0 ? mva : (rb == 0 ? mvb : mvc);
+    auto med = [](int x, int y, int z) { return x + y + z - min(min(x, y), z) - max(max(x, y), z); };
+    return make_int2(med(mva.x, mvb.x, mvc.x), med(mva.y, mvb.y, mvc.y));
+}
+
+__global__ void __launch_bounds__(32 * ME_WARPS) me_frames_kernel(const __grid_constant__ FrameBatch batch,
+                                                                 long long total, MeParamsDev prm,
+                                                                 int* __restrict__ counter, int* __restrict__ flags,
+                                                                 int epoch, int* __restrict__ status, int spin_limit) {
+    __shared__ WarpScratch scratch[ME_WARPS];
+    const int w = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        int t = 0;
+        if (lane == 0) t = atomicAdd(counter, 1);
+        t = __shfl_sync(0xffffffffu, t, 0);
+        if (t >= total) return;
+        int j = 0;
+        while (j + 1 < batch.n && batch.seg_start[j + 1] <= t) j++;
+        const long long u = t - batch.seg_start[j];
+        const int nxt = j + 1 < batch.n ? batch.f[j + 1].mb_w * batch.f[j + 1].mb_h : 0;
+        const FrameDesc& fd = batch.f[int(u % (j + 1))];
+        const int m = nxt + int(u / (j + 1));
+        const int mbx = m % fd.mb_w, mby = m / fd.mb_w;
+        int* fl = flags + fd.flag_base;
+        // dependencies: left, and top-right (or top at the right edge)
+        if (lane == 0) {
+            if (mbx > 0) wait_flag(fl + m - 1, epoch, status, 1, spin_limit);
+            if (mby > 0) wait_flag(fl + m - fd.mb_w + (mbx < fd.mb_w - 1 ? 1 : 0), epoch, status, 1, spin_limit);
+        }
+        __syncwarp();
+        // neighbours of the MB's top-left 4x4 block (mv_neighbors_block, mb16.rs:1871)
+        const bool aa = mbx > 0, ba = mby > 0, ca = mby > 0 && mbx < fd.mb_w - 1, da = mbx > 0 && mby > 0;
+        const int2 a = aa ? pick_mv_at(fd.picks, m - 1, 3, 0) : make_int2(0, 0);
+        const int2 b = ba ? pick_mv_at(fd.picks, m - fd.mb_w, 0, 3) : make_int2(0, 0);
+        int2 c = ca ? pick_mv_at(fd.picks, m - fd.mb_w + 1, 0, 3) : make_int2(0, 0);
+        bool cav = ca;
+        if (!ca) {
+            cav = da;
+            c = da ? pick_mv_at(fd.picks, m - fd.mb_w - 1, 3, 3) : make_int2(0, 0);
+        }
+        const int2 pmv = predict_mv_ref0(aa, a, ba, b, cav, c);
+        const MePic pic = make_pic(fd.pic);
+        const int lx = mbx * 16, ly = mby * 16;
+        int preds[4] = {pmv.x, pmv.y, 0, 0};
+        Search s;
+        int x16, y16;
+        long long c16;
+        s.init(pic, &prm, lx, ly, 16, 16, pmv.x, pmv.y, fd.lambda_me, false, &scratch[w]);
+        motion_search_warp(s, preds, 1, nullptr, x16, y16, c16);
+        int evals = s.evals_ref << s.lg_nb;  // 4x4-block evaluations
+        int shape = 0;
+        int mv0x = x16, mv0y = y16, mv1x = x16, mv1y = y16;
+        long long best = c16;
+        if (fd.split_gate >= 0 && c16 > fd.split_gate) {
+            preds[2] = x16; preds[3] = y16;
+            int px[4], py[4];
+            long long pc[4];
+            const int ox[4] = {0, 0, 0, 8}, oy[4] = {0, 8, 0, 0};
+            const int ww[4] = {16, 16, 8, 8}, hh[4] = {8, 8, 16, 16};
+            for (int k = 0; k < 4; k++) {
+                s.init(pic, &prm, lx + ox[k], ly + oy[k], ww[k], hh[k], pmv.x, pmv.y, fd.lambda_me, false, &scratch[w]);
+                motion_search_warp(s, preds, 2, nullptr, px[k], py[k], pc[k]);
+                evals += s.evals_ref << s.lg_nb;
+            }
+            if (pc[0] + pc[1] < best) {
+                best = pc[0] + pc[1]; shape = 1;
+                mv0x = px[0]; mv0y = py[0]; mv1x = px[1]; mv1y = py[1];
+            }
+            if (pc[2] + pc[3] < best) {
+                best = pc[2] + pc[3]; shape = 2;
+                mv0x = px[2]; mv0y = py[2]; mv1x = px[3]; mv1y = py[3];
+            }
+        }
+        if (lane == 0) {
+            int32_t* p = fd.picks + 6 * m;
+            p[0] = shape; p[1] = mv0x; p[2] = mv0y; p[3] = mv1x; p[4] = mv1y; p[5] = evals;
+            fd.costs[2 * m] = best;
+            fd.costs[2 * m + 1] = c16;
+            __threadfence();
+            st_release(fl + m, epoch);
+        }
+        __syncwarp();
+    }
+}
+
+// One warp waits on a flag that nothing sets; the bounded wait must give up
+// after `limit` polls and record status code 2.
+__global__ void bounded_wait_selftest_kernel(const int* flag, int* status, int limit) {
+    if (threadIdx.x == 0) wait_flag(flag, 1, status, 2, limit);
+}
+
+}  // namespace h264a
+
+using namespace h264a;
+
+extern "C" int h264a_selftest_bounded_wait(h264a_ctx* ctx, int spin_limit, void* stream) {
+    if (!ctx || spin_limit < 0 || spin_limit > SPIN_LIMIT) return fail(H264A_E_ARG, "selftest_bounded_wait: bad limit");
+    int rc = ensure_me_scratch(ctx, 1);
+    if (rc) return rc;
+    cudaStream_t st = pick_stream(ctx, stream);
+    // the counter word is zero-initialised scratch that no kernel of this call writes
+    H264A_CUDA(cudaMemsetAsync(ctx->d_counter, 0, sizeof(int32_t), st));
+    bounded_wait_selftest_kernel<<<1, 32, 0, st>>>(ctx->d_counter, ctx->d_status, spin_limit);
+    return check_launch("bounded_wait_selftest_kernel");
+}
+
+extern "C" int h264a_me_search(h264a_ctx* ctx, const h264a_picture* d_pics, int npics, const h264a_me_params* params,
+                               const h264a_me_job* d_jobs, int n, h264a_me_result* d_out, void* stream) {
+    if (!ctx || !d_pics || !params || !d_jobs || !d_out) return fail(H264A_E_ARG, "me_search: null pointer");
+    if (n < 0 || npics < 1) return fail(H264A_E_ARG, "me_search: bad count");
+    if ((params->mv_cost_kind == 1 || params->mv_cost_kind == 2) && !params->d_mv_cost_tab)
+        return fail(H264A_E_ARG, "me_search: mv cost kinds 1 and 2 need d_mv_cost_tab");
+    if (n == 0) return H264A_OK;
+    const MeParamsDev prm = to_dev(*params);
+    me_search_kernel<<<unsigned((n + ME_WARPS - 1) / ME_WARPS), 32 * ME_WARPS, 0, pick_stream(ctx, stream)>>>(
+        d_pics, npics, prm, d_jobs, n, d_out);
+    return check_launch("me_search_kernel");
+}
+
+extern "C" int h264a_me_frames(h264a_ctx* ctx, const h264a_me_frame* h_frames, int nframes,
+                               const h264a_me_params* params, void* stream) {
+    if (!ctx || !h_frames || !params) return fail(H264A_E_ARG, "me_frames: null pointer");
+    if (nframes < 1) return fail(H264A_E_ARG, "me_frames: need at least one frame");
+    if ((params->mv_cost_kind == 1 || params->mv_cost_kind == 2) && !params->d_mv_cost_tab)
+        return fail(H264A_E_ARG, "me_frames: mv cost kinds 1 and 2 need d_mv_cost_tab");
+    for (int i = 0; i < nframes; i++) {
+        const h264a_me_frame& f = h_frames[i];
+        if (!f.pic.d_src || !f.pic.d_planes || !f.d_picks || !f.d_costs)
+            return fail(H264A_E_ARG, "me_frames: null frame pointer");
+        if (f.pic.cw < 16 || f.pic.ch < 16 || f.pic.cw % 16 || f.pic.ch % 16 || f.pic.pad < 3 || f.pic.pad > 128)
+            return fail(H264A_E_ARG, "me_frames: frames must be MB-aligned with 3 <= pad <= 128");
+        if ((long long)(f.pic.cw / 16) * (f.pic.ch / 16) > (1 << 24))
+            return fail(H264A_E_ARG, "me_frames: frame too large");
+    }
+    cudaStream_t st = pick_stream(ctx, stream);
+    const MeParamsDev prm = to_dev(*params);
+    int per_sm = 0;
+    H264A_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, me_frames_kernel, 32 * ME_WARPS, 0));
+    // frames are launched in groups of up to ME_MAXF, largest first
+    std::vector<int> order(nframes);
+    for (int i = 0; i < nframes; i++) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        return (long long)h_frames[a].pic.cw * h_frames[a].pic.ch > (long long)h_frames[b].pic.cw * h_frames[b].pic.ch;
+    });
+    for (int g0 = 0; g0 < nframes; g0 += ME_MAXF) {
+        const int gn = nframes - g0 < ME_MAXF ? nframes - g0 : ME_MAXF;
+        FrameBatch fb;
+        memset(&fb, 0, sizeof fb);
+        fb.n = gn;
+        long long total = 0;
+        for (int k = 0; k < gn; k++) {
+            const h264a_me_frame& f = h_frames[order[g0 + k]];
+            FrameDesc& d = fb.f[k];
+            d.pic = f.pic;
+            d.lambda_me = f.lambda_me;
+            d.split_gate = f.split_gate;
+            d.picks = f.d_picks;
+            d.costs = f.d_costs;
+            d.mb_w = f.pic.cw / 16;
+            d.mb_h = f.pic.ch / 16;
+            d.flag_base = int(total);
+            total += (long long)d.mb_w * d.mb_h;
+        }
+        long long acc = 0;
+        for (int j = 0; j < gn; j++) {
+            fb.seg_start[j] = acc;
+            const long long nj = (long long)fb.f[j].mb_w * fb.f[j].mb_h;
+            const long long nn = j + 1 < gn ? (long long)fb.f[j + 1].mb_w * fb.f[j + 1].mb_h : 0;
+            acc += (nj - nn) * (j + 1);
+        }
+        fb.seg_start[gn] = acc;
+        if (acc != total) return fail(H264A_E_ARG, "me_frames: internal queue layout error");
+        int rc = ensure_me_scratch(ctx, size_t(total));
+        if (rc) return rc;
+        H264A_CUDA(cudaMemsetAsync(ctx->d_counter, 0, sizeof(int32_t), st));
+        const int epoch = next_epoch(ctx, st);
+        if (epoch < 0) return H264A_E_CUDA;
+        long long blocks = (long long)ctx->num_sms * (per_sm > 0 ? per_sm : 1);
+        const long long need = (total + ME_WARPS - 1) / ME_WARPS;
+        if (blocks > need) blocks = need;
+        me_frames_kernel<<<unsigned(blocks), 32 * ME_WARPS, 0, st>>>(fb, total, prm, ctx->d_counter, ctx->d_flags,
+                                                                     epoch, ctx->d_status, SPIN_LIMIT);
+        rc = check_launch("me_frames_kernel");
+        if (rc) return rc;
+    }
+    return H264A_OK;
+}

@@ -1,0 +1,320 @@
+// tq.cu -- a13/a14/a15: forward integer transforms and quantisation.
+//
+//  * dct_four_t4 + quant_four_4x4 (crates/rusty_h264-accel/src/transform_quant.rs:
+//    71-135) with FF = quant_dz_ff(qp, dz) and MF = QUANT_MF_OH[qp]
+//    (crates/rusty_h264-common/src/transform.rs:145-159, 1447-1500);
+//  * forward_core_8x8 + quantize_8x8 (transform.rs:492-629);
+//  * the fused MC + luma T/Q of chosen MBs (mb16.rs:3436-3450).
+// All in registers, one thread per 4x4 block (one row/column per thread for
+// 8x8); HBM traffic is the source and prediction bytes in and the
+// coefficients out.
+#include <cstring>
+#include <vector>
+
+#include "h264a_device.cuh"
+
+namespace h264a {
+
+struct QuantTables4 {
+    int16_t ff[52][8];
+    int16_t mf[52][8];
+};
+
+// QUANT_MF (transform.rs:25-32) and openh264's slot -> position group map.
+static const int kQuantMf[6][3] = {{13107, 5243, 8066}, {11916, 4660, 7490}, {10082, 4194, 6554},
+                                   {9362, 3647, 5825},  {8192, 3355, 5243},  {7282, 2893, 4559}};
+static const int kGroup8[8] = {0, 2, 0, 2, 2, 1, 2, 1};
+
+// quant_dz_ff (transform.rs:145-159) and QUANT_MF_OH[qp] (transform.rs:1447):
+// the openh264 table is round-half-up(MF << 16 >> qbits), qbits = 15 + qp/6.
+static QuantTables4 make_tables4(int dz_div) {
+    QuantTables4 t;
+    for (int qp = 0; qp < 52; qp++) {
+        const int m = qp % 6;
+        const long long qbits = 15 + qp / 6;
+        const long long f = (1LL << qbits) / dz_div;
+        for (int i = 0; i < 8; i++) {
+            const long long mfg = kQuantMf[m][kGroup8[i]];
+            t.ff[qp][i] = int16_t((f + mfg / 2) / mfg);
+            const int sh = int(qbits) - 16;
+            const long long r = sh < 0 ? mfg << 1 : (sh == 0 ? mfg : (mfg + (1LL << (sh - 1))) >> sh);
+            t.mf[qp][i] = int16_t(r);
+        }
+    }
+    return t;
+}
+
+// fwd_1d + forward_core (transform.rs:72-119), rows then columns, in place.
+__device__ __forceinline__ void forward_core4(int m[16]) {
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+        const int x0 = m[r * 4], x1 = m[r * 4 + 1], x2 = m[r * 4 + 2], x3 = m[r * 4 + 3];
+        const int t0 = x0 + x3, t1 = x1 + x2, t2 = x1 - x2, t3 = x0 - x3;
+        m[r * 4] = t0 + t1; m[r * 4 + 1] = 2 * t3 + t2; m[r * 4 + 2] = t0 - t1; m[r * 4 + 3] = t3 - 2 * t2;
+    }
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+        const int x0 = m[c], x1 = m[4 + c], x2 = m[8 + c], x3 = m[12 + c];
+        const int t0 = x0 + x3, t1 = x1 + x2, t2 = x1 - x2, t3 = x0 - x3;
+        m[c] = t0 + t1; m[4 + c] = 2 * t3 + t2; m[8 + c] = t0 - t1; m[12 + c] = t3 - 2 * t2;
+    }
+}
+
+// Residual -> dct_four_t4's i16 cast -> quant_four_4x4 (pos = (row&1)*4+col),
+// written as 16 consecutive i16 (two 16-byte stores).
+__device__ __forceinline__ void tq4x4_store(const uint32_t s[4], const uint32_t p[4], const int16_t* ff,
+                                            const int16_t* mf, int16_t* out) {
+    int m[16];
+#pragma unroll
+    for (int r = 0; r < 4; r++)
+#pragma unroll
+        for (int c = 0; c < 4; c++) m[r * 4 + c] = byte_of(s[r], c) - byte_of(p[r], c);
+    forward_core4(m);
+    uint32_t w[8];
+#pragma unroll
+    for (int i = 0; i < 16; i += 2) {
+        int v2[2];
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            const int idx = i + k;
+            const int pos = ((idx >> 2) & 1) * 4 + (idx & 3);
+            const int c = int(int16_t(m[idx]));
+            const int lvl = ((abs(c) + int(ff[pos])) * int(mf[pos])) >> 16;
+            v2[k] = int(int16_t(c < 0 ? -lvl : lvl));
+        }
+        w[i >> 1] = (uint32_t(uint16_t(v2[0]))) | (uint32_t(uint16_t(v2[1])) << 16);
+    }
+    uint4* o = reinterpret_cast<uint4*>(out);
+    o[0] = make_uint4(w[0], w[1], w[2], w[3]);
+    o[1] = make_uint4(w[4], w[5], w[6], w[7]);
+}
+
+__global__ void dct_quant_4x4_kernel(const uint8_t* __restrict__ src, int ss, const uint8_t* __restrict__ pred, int ps,
+                                     const int32_t* __restrict__ xy, const uint8_t* __restrict__ qp, QuantTables4 qt,
+                                     int n, int16_t* __restrict__ out) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long r = t >> 2;
+    if (r >= n) return;
+    const int k = int(t & 3);
+    const int ox = (k & 1) * 4, oy = (k >> 1) * 4;  // sub-block order (0,0),(4,0),(0,4),(4,4)
+    const int x = xy[2 * r] + ox, y = xy[2 * r + 1] + oy;
+    uint32_t s[4], p[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        s[i] = ld4u(src + (long long)(y + i) * ss + x);
+        p[i] = ld4u(pred + (long long)(y + i) * ps + x);
+    }
+    const int q = qp[r] > 51 ? 51 : qp[r];
+    tq4x4_store(s, p, qt.ff[q], qt.mf[q], out + r * 64 + k * 16);
+}
+
+// ---- 8x8 -------------------------------------------------------------------
+
+struct QuantTables8 {
+    int32_t mf[6][64];   // QUANT_MF_8X8[qp%6][group] * 16 / weight
+    long long ff[52];    // (1 << (16 + qp/6)) / dz
+};
+
+static const int kQuantMf8[6][6] = {
+    {13107, 14564, 8192, 13797, 10486, 10923}, {11916, 13797, 7490, 12483, 9362, 10083},
+    {10083, 11398, 6242, 10923, 7944, 8456},   {9362, 10486, 5825, 10083, 7490, 7944},
+    {8192, 9362, 5140, 8738, 6554, 6899},      {7282, 8192, 4520, 7710, 5699, 6096},
+};
+
+static int pos_group_8x8(int i, int j) {
+    const int i4 = i % 4, j4 = j % 4;
+    if (i4 == 0 && j4 == 0) return 0;
+    if (i % 2 == 1 && j % 2 == 1) return 1;
+    if (i4 == 2 && j4 == 2) return 2;
+    if ((i4 == 0 && j % 2 == 1) || (i % 2 == 1 && j4 == 0)) return 3;
+    if ((i4 == 0 && j4 == 2) || (i4 == 2 && j4 == 0)) return 4;
+    return 5;
+}
+
+// fwd_1d_8x8 (transform.rs:492-524).
+__device__ __forceinline__ void fwd8(const int s[8], int y[8]) {
+    const int a0 = s[0] + s[7], a1 = s[1] + s[6], a2 = s[2] + s[5], a3 = s[3] + s[4];
+    const int a4 = s[0] - s[7], a5 = s[1] - s[6], a6 = s[2] - s[5], a7 = s[3] - s[4];
+    const int b0 = a0 + a3, b1 = a1 + a2, b2 = a0 - a3, b3 = a1 - a2;
+    y[0] = b0 + b1;
+    y[2] = b2 + (b3 >> 1);
+    y[4] = b0 - b1;
+    y[6] = (b2 >> 1) - b3;
+    const int b4 = a5 + a6 + ((a4 >> 1) + a4);
+    const int b5 = a4 - a7 - ((a6 >> 1) + a6);
+    const int b6 = a4 + a7 - ((a5 >> 1) + a5);
+    const int b7 = a5 - a6 + ((a7 >> 1) + a7);
+    y[1] = b4 + (b7 >> 2);
+    y[3] = b5 + (b6 >> 2);
+    y[5] = b6 - (b5 >> 2);
+    y[7] = (b4 >> 2) - b7;
+}
+
+// 8 threads per region: thread r transforms row r, then column r (through
+// shared memory), then quantises that column.
+__global__ void __launch_bounds__(256) dct_quant_8x8_kernel(const uint8_t* __restrict__ src, int ss,
+                                                           const uint8_t* __restrict__ pred, int ps,
+                                                           const int32_t* __restrict__ xy,
+                                                           const uint8_t* __restrict__ qp, QuantTables8 qt, int n,
+                                                           int32_t* __restrict__ out) {
+    __shared__ int tile[32][65];
+    const int local = threadIdx.x >> 3;  // region within the block
+    const int row = threadIdx.x & 7;
+    const long long r = (long long)blockIdx.x * 32 + local;
+    const bool live = r < n;
+    if (live) {
+        const int x = xy[2 * r], y = xy[2 * r + 1] + row;
+        const uint32_t s0 = ld4u(src + (long long)y * ss + x), s1 = ld4u(src + (long long)y * ss + x + 4);
+        const uint32_t p0 = ld4u(pred + (long long)y * ps + x), p1 = ld4u(pred + (long long)y * ps + x + 4);
+        int v[8], o[8];
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            v[c] = byte_of(s0, c) - byte_of(p0, c);
+            v[c + 4] = byte_of(s1, c) - byte_of(p1, c);
+        }
+        fwd8(v, o);
+#pragma unroll
+        for (int c = 0; c < 8; c++) tile[local][row * 8 + c] = o[c];
+    }
+    __syncthreads();
+    if (!live) return;
+    int v[8], o[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) v[k] = tile[local][k * 8 + row];
+    fwd8(v, o);
+    const int q = qp[r] > 51 ? 51 : qp[r];
+    const int m = q % 6;
+    const int qbits = 16 + q / 6;
+    const long long ff = qt.ff[q];
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        const int idx = k * 8 + row;
+        const long long a = o[k] < 0 ? -(long long)o[k] : (long long)o[k];
+        const int lvl = int((a * qt.mf[m][idx] + ff) >> qbits);
+        out[r * 64 + idx] = o[k] < 0 ? -lvl : lvl;
+    }
+}
+
+// ---- fused MC + luma T/Q of whole frames ---------------------------------------
+
+struct TqFrameDesc {
+    h264a_picture pic;
+    const int32_t* picks;
+    int qp;
+    int16_t* coeffs;
+    int mb_w;
+    int nmb;
+};
+
+constexpr int TQ_MAXF = 96;
+struct TqBatch {
+    TqFrameDesc f[TQ_MAXF];
+    int mb_base[TQ_MAXF];
+    int n;
+};
+
+__global__ void mc_tq_frames_kernel(const __grid_constant__ TqBatch batch, long long total_mb, QuantTables4 qt) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long g = t >> 4;  // MB index across the batch
+    if (g >= total_mb) return;
+    int lo = 0, hi = batch.n - 1;  // last frame whose base <= g
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (batch.mb_base[mid] <= g) lo = mid; else hi = mid - 1;
+    }
+    const TqFrameDesc& fd = batch.f[lo];
+    const int m = int(g - batch.mb_base[lo]);
+    const int blk = int(t & 15);
+    const int bx = (blk & 3) * 4, by = (blk >> 2) * 4;  // 4x4 block inside the MB
+    const int mbx = m % fd.mb_w, mby = m / fd.mb_w;
+    const int32_t* pk = fd.picks + 6 * m;
+    const int shape = pk[0];
+    const int part = shape == 1 ? (by >= 8) : (shape == 2 ? (bx >= 8) : 0);
+    const int mvx = pk[1 + 2 * part], mvy = pk[2 + 2 * part];
+    Planes P{fd.pic.d_planes, fd.pic.cw + 2 * fd.pic.pad, fd.pic.ch + 2 * fd.pic.pad, fd.pic.pad, 0};
+    P.ps = (long long)P.pw * P.ph;
+    const int x = mbx * 16 + bx, y = mby * 16 + by;
+    uint32_t s[4], p[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) s[i] = ld4u(fd.pic.d_src + (long long)(y + i) * fd.pic.cw + x);
+    pred_rows(P, x + (mvx >> 2), y + (mvy >> 2), mvx & 3, mvy & 3, p);
+    // reference layout: region qi (0,0),(8,0),(0,8),(8,8); sub-block k (0,0),(4,0),(0,4),(4,4)
+    const int qi = (by >= 8 ? 2 : 0) + (bx >= 8 ? 1 : 0);
+    const int k = ((by & 4) ? 2 : 0) + ((bx & 4) ? 1 : 0);
+    const int q = fd.qp > 51 ? 51 : (fd.qp < 0 ? 0 : fd.qp);
+    tq4x4_store(s, p, qt.ff[q], qt.mf[q], fd.coeffs + (long long)m * 256 + qi * 64 + k * 16);
+}
+
+}  // namespace h264a
+
+using namespace h264a;
+
+extern "C" int h264a_dct_quant_4x4(h264a_ctx* ctx, const uint8_t* d_src, int ss, const uint8_t* d_pred, int ps,
+                                   const int32_t* d_xy, const uint8_t* d_qp, int dz_div, int n, int16_t* d_out,
+                                   void* stream) {
+    if (!ctx || !d_src || !d_pred || !d_xy || !d_qp || !d_out) return fail(H264A_E_ARG, "dct_quant_4x4: null pointer");
+    if (n < 0 || dz_div < 1 || ss < 8 || ps < 8) return fail(H264A_E_ARG, "dct_quant_4x4: bad count, stride or dz");
+    if ((reinterpret_cast<uintptr_t>(d_out) & 15) != 0) return fail(H264A_E_ARG, "dct_quant_4x4: out must be 16-byte aligned");
+    if (n == 0) return H264A_OK;
+    const QuantTables4 qt = make_tables4(dz_div);
+    const long long threads = (long long)n * 4;
+    dct_quant_4x4_kernel<<<unsigned((threads + 255) / 256), 256, 0, pick_stream(ctx, stream)>>>(d_src, ss, d_pred, ps,
+                                                                                                d_xy, d_qp, qt, n, d_out);
+    return check_launch("dct_quant_4x4_kernel");
+}
+
+extern "C" int h264a_dct_quant_8x8(h264a_ctx* ctx, const uint8_t* d_src, int ss, const uint8_t* d_pred, int ps,
+                                   const int32_t* d_xy, const uint8_t* d_qp, const int32_t* h_weight, int dz_div,
+                                   int n, int32_t* d_out, void* stream) {
+    if (!ctx || !d_src || !d_pred || !d_xy || !d_qp || !d_out) return fail(H264A_E_ARG, "dct_quant_8x8: null pointer");
+    if (n < 0 || dz_div < 1 || ss < 8 || ps < 8) return fail(H264A_E_ARG, "dct_quant_8x8: bad count, stride or dz");
+    if (n == 0) return H264A_OK;
+    QuantTables8 qt;
+    for (int m = 0; m < 6; m++)
+        for (int idx = 0; idx < 64; idx++) {
+            const int w = h_weight ? h_weight[idx] : 16;
+            if (w <= 0) return fail(H264A_E_ARG, "dct_quant_8x8: weights must be positive");
+            qt.mf[m][idx] = int32_t((long long)kQuantMf8[m][pos_group_8x8(idx / 8, idx % 8)] * 16 / w);
+        }
+    for (int q = 0; q < 52; q++) qt.ff[q] = (1LL << (16 + q / 6)) / dz_div;
+    dct_quant_8x8_kernel<<<unsigned((n + 31) / 32), 256, 0, pick_stream(ctx, stream)>>>(d_src, ss, d_pred, ps, d_xy,
+                                                                                        d_qp, qt, n, d_out);
+    return check_launch("dct_quant_8x8_kernel");
+}
+
+extern "C" int h264a_mc_tq_frames(h264a_ctx* ctx, const h264a_tq_frame* h_frames, int nframes, void* stream) {
+    if (!ctx || !h_frames || nframes < 1) return fail(H264A_E_ARG, "mc_tq_frames: bad arguments");
+    const int dz = h_frames[0].dz_div;
+    for (int i = 0; i < nframes; i++) {
+        const h264a_tq_frame& f = h_frames[i];
+        if (!f.pic.d_src || !f.pic.d_planes || !f.d_picks || !f.d_coeffs)
+            return fail(H264A_E_ARG, "mc_tq_frames: null frame pointer");
+        if (f.pic.cw < 16 || f.pic.ch < 16 || f.pic.cw % 16 || f.pic.ch % 16 || f.pic.pad < 3 || f.pic.pad > 128)
+            return fail(H264A_E_ARG, "mc_tq_frames: frames must be MB-aligned with 3 <= pad <= 128");
+        if (f.dz_div != dz || dz < 1) return fail(H264A_E_ARG, "mc_tq_frames: one dz_div >= 1 per call");
+        if ((reinterpret_cast<uintptr_t>(f.d_coeffs) & 15) != 0)
+            return fail(H264A_E_ARG, "mc_tq_frames: coefficients must be 16-byte aligned");
+        if ((long long)(f.pic.cw / 16) * (f.pic.ch / 16) > (1 << 24))
+            return fail(H264A_E_ARG, "mc_tq_frames: frame too large");
+    }
+    cudaStream_t st = pick_stream(ctx, stream);
+    const QuantTables4 qt = make_tables4(dz);
+    for (int g0 = 0; g0 < nframes; g0 += TQ_MAXF) {
+        const int gn = nframes - g0 < TQ_MAXF ? nframes - g0 : TQ_MAXF;
+        TqBatch b;
+        memset(&b, 0, sizeof b);
+        b.n = gn;
+        long long total = 0;
+        for (int k = 0; k < gn; k++) {
+            const h264a_tq_frame& f = h_frames[g0 + k];
+            b.f[k] = {f.pic, f.d_picks, f.qp, f.d_coeffs, f.pic.cw / 16, (f.pic.cw / 16) * (f.pic.ch / 16)};
+            b.mb_base[k] = int(total);
+            total += b.f[k].nmb;
+        }
+        const long long threads = total * 16;
+        mc_tq_frames_kernel<<<unsigned((threads + 255) / 256), 256, 0, st>>>(b, total, qt);
+        const int rc = check_launch("mc_tq_frames_kernel");
+        if (rc) return rc;
+    }
+    return H264A_OK;
+}

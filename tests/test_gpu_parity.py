@@ -1,0 +1,519 @@
+"""GPU parity: every CUDA entry point against the CPU oracle, bit-exact.
+
+All calls go through the C ABI (rusty_h264_b200.accel -> libh264accel_cuda.so).
+Inputs are seeded synthetic clips (rusty_h264_b200.synth) and the reference
+tests' LCG streams; the oracle is oracle/liboracle.so.  Integer work, so the
+tolerance is zero everywhere.
+"""
+import ctypes as C
+import zlib
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from rusty_h264_b200 import accel as A
+from rusty_h264_b200 import synth
+from tests._lcg import Lcg64
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def acc():
+    a = A.Accel(0)
+    yield a
+    a.close()
+
+
+@pytest.fixture(scope="module")
+def cif():
+    y, _, _ = synth.cif_clip(5, 0)
+    return synth.coded_luma(y)
+
+
+def dev(acc, a):
+    return acc.to_dev(np.ascontiguousarray(a))
+
+
+# ---------------------------------------------------------------------------
+# a1/a2 planes
+# ---------------------------------------------------------------------------
+
+@pytest.mark.parametrize("cw,ch,pad", [(64, 48, 16), (80, 64, 12), (176, 144, 32), (352, 288, 32), (48, 32, 3),
+                                       (16, 16, 32)])
+def test_hpel_planes_match_oracle(acc, cw, ch, pad):
+    st = Lcg64(0x5EED_F00D_DEAD_BEEF + cw)
+    frames = st.bytes(2 * cw * ch).reshape(2, ch, cw).copy()
+    got = acc.hpel_build(dev(acc, frames), pad=pad)
+    acc.sync()
+    got = got.cpu().numpy()
+    for i in range(2):
+        want = O.build_planes4(frames[i], pad)
+        assert np.array_equal(got[i], want), (cw, ch, pad, i)
+
+
+def test_hpel_planes_1080p(acc):
+    y, _, _ = synth.hd_clip(2, 7)
+    f = synth.coded_luma(y)
+    got = acc.hpel_build(dev(acc, f), pad=32)
+    acc.sync()
+    got = got.cpu().numpy()
+    for i in range(2):
+        assert np.array_equal(got[i], O.build_planes4(f[i], 32))
+
+
+# ---------------------------------------------------------------------------
+# a6/a7/a8 block metrics (encoder tests/satd_avg_compare.rs streams)
+# ---------------------------------------------------------------------------
+
+def test_block_metrics_match_oracle(acc):
+    st = Lcg64(0x0DD0_C0DE_1234_5678)
+    L = O.lib()
+    ss, rs = 40, 56
+    src_rows, pl_rows = 64, 96
+    src = st.bytes(src_rows * ss)
+    planes = st.bytes(pl_rows * rs)
+    d_src, d_pl = dev(acc, src), dev(acc, planes)
+    for (w, h) in [(16, 16), (16, 8), (8, 16), (8, 8), (8, 4), (4, 8), (4, 4)]:
+        n = 96
+        rnd = lambda m: int(st.next()) % m
+        a_off = np.array([rnd(src_rows - h) * ss + rnd(ss - w + 1) for _ in range(n)], np.int64)
+        b_off = np.array([rnd(pl_rows - h) * rs + rnd(rs - w + 1) for _ in range(n)], np.int64)
+        c_off = np.array([rnd(pl_rows - h) * rs + rnd(rs - w + 1) for _ in range(n)], np.int64)
+        da, db, dc = dev(acc, a_off), dev(acc, b_off), dev(acc, c_off)
+        for metric in (A.METRIC_SATD_WELS, A.METRIC_SATD, A.METRIC_SAD, A.METRIC_SATD_AVG, A.METRIC_SAD_AVG):
+            avg = metric in (A.METRIC_SATD_AVG, A.METRIC_SAD_AVG)
+            got = acc.block_metric(metric, w, h, d_src, da, ss, d_pl, db, rs, d_pl if avg else None,
+                                   dc if avg else None)
+            acc.sync()
+            got = got.cpu().numpy()
+            for i in range(n):
+                a = np.ascontiguousarray(src[a_off[i]:])
+                b = np.ascontiguousarray(planes[b_off[i]:])
+                c = np.ascontiguousarray(planes[c_off[i]:])
+                if metric == A.METRIC_SATD_WELS:
+                    want = L.or_satd_region_wels(O.ptr(a), ss, O.ptr(b), rs, w, h)
+                elif metric == A.METRIC_SATD:
+                    want = L.or_satd_px(O.ptr(a), ss, O.ptr(b), rs, w, h)
+                elif metric == A.METRIC_SAD:
+                    want = L.or_sad(O.ptr(a), ss, O.ptr(b), rs, w, h)
+                elif metric == A.METRIC_SATD_AVG:
+                    want = L.or_satd_avg(O.ptr(a), ss, O.ptr(b), O.ptr(c), rs, w, h)
+                else:
+                    want = L.or_sad_avg(O.ptr(a), ss, O.ptr(b), O.ptr(c), rs, w, h)
+                assert got[i] == want, (w, h, metric, i)
+
+
+# ---------------------------------------------------------------------------
+# a3/a4/a5/a9 candidate distortion
+# ---------------------------------------------------------------------------
+
+SHAPES = [(16, 16), (16, 8), (8, 16), (8, 8), (8, 4), (4, 8), (4, 4)]
+
+
+def test_candidate_dist_matches_oracle_everywhere(acc, cif):
+    src, ref = cif[1], cif[0]
+    planes = O.build_planes4(ref, 32)
+    d_src, d_pl = dev(acc, src), dev(acc, planes)
+    d_pics, _ = acc.pictures([d_src], [d_pl])
+    rng = np.random.default_rng(11)
+    ch, cw = src.shape
+    cands = []
+    for _ in range(1500):
+        w, h = SHAPES[rng.integers(len(SHAPES))]
+        x = int(rng.integers(0, cw - w + 1))
+        y = int(rng.integers(0, ch - h + 1))
+        r = int(rng.choice([16, 200, 2000]))  # interior, beyond the pad, far off the planes
+        cands.append(A.Candidate(0, x, y, w, h, int(rng.integers(-r, r + 1)), int(rng.integers(-r, r + 1))))
+    for metric, kind in ((A.METRIC_SATD, 0), (A.METRIC_SAD, 1)):
+        got = acc.candidate_dist(d_pics, 1, cands, metric)
+        acc.sync()
+        got = got.cpu().numpy()
+        for i, c in enumerate(cands):
+            want = O.candidate_dist(src, ref, planes, kind, c.x, c.y, c.w, c.h, c.mvx, c.mvy)
+            assert got[i] == want, (metric, c.x, c.y, c.w, c.h, c.mvx, c.mvy)
+
+
+def test_candidate_dist_rejects_out_of_range(acc, cif):
+    d_src, d_pl = dev(acc, cif[1]), dev(acc, O.build_planes4(cif[0], 32))
+    d_pics, _ = acc.pictures([d_src], [d_pl])
+    bad = [A.Candidate(1, 0, 0, 16, 16, 0, 0), A.Candidate(0, 340, 0, 16, 16, 0, 0), A.Candidate(0, 0, 0, 32, 16, 0, 0),
+           A.Candidate(0, -4, 0, 8, 8, 0, 0)]
+    got = acc.candidate_dist(d_pics, 1, bad, A.METRIC_SATD)
+    acc.sync()
+    assert (got.cpu().numpy() == -1).all()
+
+
+# ---------------------------------------------------------------------------
+# a10/a11/a12 motion search
+# ---------------------------------------------------------------------------
+
+def me_variants():
+    tab_smooth = O.mv_cost_table()
+    rng = np.random.default_rng(5)
+    tab_true = np.sort(rng.integers(4, 300, 4096)).astype(np.uint16)  # stand-in measured table
+    tab_true[0] = 4
+    return [
+        ("balanced", {}, None),
+        ("sadfp", {"sadfp": 1}, None),
+        ("smooth_cost", {"mv_cost_kind": 1}, tab_smooth),
+        ("sadfp_smooth", {"sadfp": 1, "mv_cost_kind": 1}, tab_smooth),
+        ("true_cost", {"mv_cost_kind": 2}, tab_true),
+        ("fast", {"fast": 1, "subpel": 0, "sp_single_pass": 0}, None),
+        ("fast_subpel", {"fast": 1, "sp_single_pass": 0}, None),
+        ("fast_satd", {"fast": 1, "mb_use_satd": 1, "subpel": 0, "sp_single_pass": 0}, None),
+        ("sp_fc", {"sp_fc": 1}, None),
+        ("sp_fc_walk", {"sp_fc": 1, "sp_single_pass": 0}, None),
+        ("walk_to_convergence", {"sp_single_pass": 0}, None),
+        ("ring4_walk", {"subpel_pat": 1}, None),
+        ("ring4_single", {"subpel_pat": 3}, None),
+        ("cascade_diamond", {"me_fc": 0}, None),
+        ("no_snap", {"me_snap": 0}, None),
+        ("sp_maxit1", {"sp_single_pass": 0, "sp_maxit": 1}, None),
+        ("full_ladder", {"dia_mask": 0x1F, "dia_sub_mask": 0x1C}, None),
+    ]
+
+
+def oracle_params(ov):
+    p = O.balanced_params()
+    for k, v in ov.items():
+        setattr(p, k, v)
+    return p
+
+
+def make_jobs(rng, cw, ch, n, refine_frac=0.1):
+    jobs = []
+    for _ in range(n):
+        w, h = SHAPES[rng.integers(len(SHAPES))]
+        x = int(rng.integers(0, cw // w)) * w
+        y = int(rng.integers(0, ch // h)) * h
+        npred = int(rng.integers(1, 5))
+        preds = [int(v) for v in rng.integers(-40, 41, 2 * npred)]
+        if rng.random() < 0.3:
+            preds[0] = (preds[0] >> 2) * 4
+            preds[1] = (preds[1] >> 2) * 4
+        qp = int(rng.integers(22, 38))
+        lam = np.sqrt(A.frame_lambda(qp)) * float(rng.choice([1.0, 1.25, 1.6]))
+        j = A.MeJob()
+        j.pic, j.x, j.y, j.w, j.h, j.npred = 0, x, y, w, h, npred
+        for k, v in enumerate(preds):
+            j.preds[k] = v
+        if rng.random() < refine_frac:
+            j.has_start = 1
+            j.start[0], j.start[1] = int(rng.integers(-30, 31)), int(rng.integers(-30, 31))
+        j.lambda_me = lam
+        jobs.append(j)
+    return jobs
+
+
+@pytest.mark.parametrize("name,ov,tab", me_variants(), ids=[v[0] for v in me_variants()])
+def test_me_search_matches_oracle(acc, cif, name, ov, tab):
+    src, ref = cif[2], cif[1]
+    planes = O.build_planes4(ref, 32)
+    d_src, d_pl = dev(acc, src), dev(acc, planes)
+    d_pics, _ = acc.pictures([d_src], [d_pl])
+    d_tab = dev(acc, tab) if tab is not None else None
+    params = A.default_me_params(**ov)
+    if d_tab is not None:
+        params.d_mv_cost_tab = d_tab.data_ptr()
+    rng = np.random.default_rng(zlib.crc32(name.encode()))
+    ch, cw = src.shape
+    jobs = make_jobs(rng, cw, ch, 300)
+    raw = acc.me_search(d_pics, 1, params, jobs)
+    acc.sync()
+    got = acc.me_results(raw)
+    op = oracle_params(ov)
+    for i, j in enumerate(jobs):
+        preds = list(j.preds)[:2 * j.npred]
+        start = (j.start[0], j.start[1]) if j.has_start else None
+        (mx, my), cost, _ = O.motion_search(src, ref, planes, op, j.x, j.y, j.w, j.h, preds, j.lambda_me, start=start,
+                                            tab=tab if tab is not None else O.mv_cost_table())
+        assert got[i, 4] == 0
+        assert (got[i, 0], got[i, 1], got[i, 2]) == (mx, my, cost), (name, i, j.x, j.y, j.w, j.h, preds, start)
+
+
+def test_me_search_rejects_bad_jobs(acc, cif):
+    d_src, d_pl = dev(acc, cif[1]), dev(acc, O.build_planes4(cif[0], 32))
+    d_pics, _ = acc.pictures([d_src], [d_pl])
+    bad = []
+    for (pic, x, w, npred) in [(3, 0, 16, 1), (0, 344, 16, 1), (0, 0, 12, 1), (0, 0, 16, 0), (0, 0, 16, 5)]:
+        j = A.MeJob()
+        j.pic, j.x, j.y, j.w, j.h, j.npred, j.lambda_me = pic, x, 0, w, 16, npred, 4.0
+        bad.append(j)
+    raw = acc.me_search(d_pics, 1, A.default_me_params(), bad)
+    acc.sync()
+    assert (acc.me_results(raw)[:, 4] == -1).all()
+
+
+def run_me_frames(acc, pairs, params, lam, split_gate, tab=None):
+    """pairs: list of (src, ref) luma frames; returns [(picks, costs)] from the GPU."""
+    frames, keep, outs = [], [], []
+    for src, ref in pairs:
+        ch, cw = src.shape
+        nmb = (cw // 16) * (ch // 16)
+        d_src, d_pl = dev(acc, src), acc.hpel_build(dev(acc, ref[None]), 32)[0]
+        picks = acc.zeros((nmb, 6), acc.torch.int32)
+        costs = acc.zeros((nmb, 2), acc.torch.int64)
+        keep += [d_src, d_pl]
+        outs.append((picks, costs))
+        frames.append(A.MeFrame(A.Picture(d_src.data_ptr(), d_pl.data_ptr(), cw, ch, 32), lam, split_gate,
+                                picks.data_ptr(), costs.data_ptr()))
+    acc.me_frames(frames, params)
+    acc.sync()
+    return [(p.cpu().numpy(), c.cpu().numpy()) for p, c in outs]
+
+
+@pytest.mark.parametrize("split", [False, True])
+@pytest.mark.parametrize("variant", ["balanced", "sadfp_smooth"])
+def test_me_frames_matches_oracle(acc, cif, split, variant):
+    ov = {} if variant == "balanced" else {"sadfp": 1, "mv_cost_kind": 1}
+    tab = O.mv_cost_table()
+    params = A.default_me_params(**ov)
+    d_tab = dev(acc, tab)
+    params.d_mv_cost_tab = d_tab.data_ptr()
+    qp = 26
+    lam = float(np.sqrt(A.frame_lambda(qp)))
+    gate = A.split_gate_for_qp(qp) if split else -1
+    # a mixed-resolution batch: four CIF frame pairs plus a small 160x96 pair
+    small = np.ascontiguousarray(cif[:, 32:128, 48:208])
+    pairs = [(cif[f], cif[f - 1]) for f in range(1, 5)] + [(small[1], small[0])]
+    got = run_me_frames(acc, pairs, params, lam, gate)
+    op = oracle_params(ov)
+    for (src, ref), (picks, costs) in zip(pairs, got):
+        wp, wc = O.me_frame(src, ref, O.build_planes4(ref, 32), op, lam, gate, tab=tab)
+        assert np.array_equal(picks[:, :5], wp[:, :5]), variant
+        assert np.array_equal(costs, wc), variant
+
+
+def test_me_frames_single_mb_and_flat(acc):
+    flat = np.full((2, 16, 16), 90, np.uint8)
+    rng = np.random.default_rng(3)
+    tiny = rng.integers(0, 256, (2, 32, 48)).astype(np.uint8)
+    params = A.default_me_params()
+    pairs = [(flat[1], flat[0]), (tiny[1], tiny[0])]
+    got = run_me_frames(acc, pairs, params, 5.0, 0)
+    op = O.balanced_params()
+    for (src, ref), (picks, costs) in zip(pairs, got):
+        wp, wc = O.me_frame(src, ref, O.build_planes4(ref, 32), op, 5.0, 0)
+        assert np.array_equal(picks[:, :5], wp[:, :5]) and np.array_equal(costs, wc)
+
+
+def test_fullpel_grid_matches_oracle(acc, cif):
+    src, ref = cif[3], cif[2]
+    planes = O.build_planes4(ref, 32)
+    d_src, d_pl = dev(acc, src), dev(acc, planes)
+    pic = A.Picture(d_src.data_ptr(), d_pl.data_ptr(), 352, 288, 32)
+    R = 8
+    nmb = 22 * 18
+    rng = np.random.default_rng(9)
+    centers = rng.integers(-64, 65, (nmb, 2)).astype(np.int32)
+    pmv = rng.integers(-64, 65, (nmb, 2)).astype(np.int32)
+    tab = O.mv_cost_table()
+    lam = 6.5
+    n = 2 * R + 1
+    checked = range(0, nmb, 7)
+    oracle_grids = {}
+    for m in checked:
+        mbx, mby = m % 22, m // 22
+        cx, cy = (centers[m] + 2) >> 2
+        ws = np.zeros(n * n, np.int32)
+        wt = np.zeros(n * n, np.int32)
+        for dy in range(-R, R + 1):
+            for dx in range(-R, R + 1):
+                i = (dy + R) * n + dx + R
+                mvx, mvy = int(cx + dx) * 4, int(cy + dy) * 4
+                ws[i] = O.candidate_dist(src, ref, planes, 1, mbx * 16, mby * 16, 16, 16, mvx, mvy)
+                wt[i] = O.candidate_dist(src, ref, planes, 0, mbx * 16, mby * 16, 16, 16, mvx, mvy)
+        oracle_grids[m] = (ws, wt)
+    for metric in (0, 1):
+        for kind in (0, 1):
+            sad, satd, best = acc.fullpel_grid(pic, R, dev(acc, centers), dev(acc, pmv), metric, kind, dev(acc, tab),
+                                               lam)
+            acc.sync()
+            sad, satd, best = sad.cpu().numpy(), satd.cpu().numpy(), best.cpu().numpy()
+            for m in checked:
+                cx, cy = (centers[m] + 2) >> 2
+                ws, wt = oracle_grids[m]
+                assert np.array_equal(sad[m], ws) and np.array_equal(satd[m], wt), m
+                dist = ws if metric == 0 else wt
+                bc, bi = None, None
+                for i in range(n * n):  # raster order, strict <
+                    dy, dx = i // n - R, i % n - R
+                    mvx, mvy = int(cx + dx) * 4, int(cy + dy) * 4
+                    rate = O.lib().or_mvbits(kind, O.ptr(tab, O.u16p), mvx - int(pmv[m, 0])) + \
+                        O.lib().or_mvbits(kind, O.ptr(tab, O.u16p), mvy - int(pmv[m, 1]))
+                    c = int(dist[i]) + int(lam * rate)
+                    if bc is None or c < bc:
+                        bc, bi = c, i
+                dy, dx = bi // n - R, bi % n - R
+                assert best[m].tolist() == [int(cx + dx) * 4, int(cy + dy) * 4, bc, int(dist[bi])], (m, metric, kind)
+
+
+# ---------------------------------------------------------------------------
+# a13/a14/a15 transform + quant
+# ---------------------------------------------------------------------------
+
+def test_dct_quant_4x4_matches_oracle(acc):
+    rng = np.random.default_rng(21)
+    src = rng.integers(0, 256, (64, 96)).astype(np.uint8)
+    pred = rng.integers(0, 256, (64, 96)).astype(np.uint8)
+    pred[:8, :8] = 0
+    src[:8, :8] = 255
+    n = 200
+    xy = np.stack([rng.integers(0, 96 - 8, n), rng.integers(0, 64 - 8, n)], 1).astype(np.int32)
+    xy[0] = (0, 0)
+    qp = rng.integers(0, 52, n).astype(np.uint8)
+    for dz in (6, 3, 2):
+        got = acc.dct_quant_4x4(dev(acc, src), 96, dev(acc, pred), 96, dev(acc, xy), dev(acc, qp), dz)
+        acc.sync()
+        got = got.cpu().numpy()
+        L = O.lib()
+        for i in range(n):
+            x, y = xy[i]
+            d = np.zeros(64, np.int16)
+            s = np.ascontiguousarray(src[y:, x:])
+            p = np.ascontiguousarray(pred[y:, x:])
+            L.or_dct_four_t4(O.ptr(d, O.i16p), O.ptr(s), 96, O.ptr(p), 96)
+            ff, mf = np.zeros(8, np.int16), np.zeros(8, np.int16)
+            L.or_quant_dz_ff(int(qp[i]), dz, O.ptr(ff, O.i16p))
+            L.or_quant_mf_oh(int(qp[i]), O.ptr(mf, O.i16p))
+            L.or_quant_four_4x4(O.ptr(d, O.i16p), O.ptr(ff, O.i16p), O.ptr(mf, O.i16p))
+            assert np.array_equal(got[i], d), (i, dz)
+
+
+def test_dct_quant_8x8_matches_oracle(acc):
+    rng = np.random.default_rng(22)
+    src = rng.integers(0, 256, (64, 96)).astype(np.uint8)
+    pred = rng.integers(0, 256, (64, 96)).astype(np.uint8)
+    n = 100
+    xy = np.stack([rng.integers(0, 96 - 8, n), rng.integers(0, 64 - 8, n)], 1).astype(np.int32)
+    qp = rng.integers(0, 52, n).astype(np.uint8)
+    weights = [None, rng.integers(6, 40, 64).astype(np.int32)]
+    L = O.lib()
+    for wgt in weights:
+        got = acc.dct_quant_8x8(dev(acc, src), 96, dev(acc, pred), 96, dev(acc, xy), dev(acc, qp), wgt, 6)
+        acc.sync()
+        got = got.cpu().numpy()
+        w = np.full(64, 16, np.int32) if wgt is None else wgt
+        for i in range(n):
+            x, y = xy[i]
+            res = (src[y:y + 8, x:x + 8].astype(np.int32) - pred[y:y + 8, x:x + 8]).reshape(-1).copy()
+            c = np.zeros(64, np.int32)
+            lv = np.zeros(64, np.int32)
+            L.or_forward_core_8x8(O.ptr(res, O.i32p), O.ptr(c, O.i32p))
+            L.or_quantize_8x8(O.ptr(c, O.i32p), int(qp[i]), O.ptr(w, O.i32p), 6, O.ptr(lv, O.i32p))
+            assert np.array_equal(got[i], lv), i
+
+
+def test_mc_tq_frames_matches_oracle(acc, cif):
+    params = O.balanced_params()
+    qp = 26
+    lam = float(np.sqrt(A.frame_lambda(qp)))
+    frames, keep, outs = [], [], []
+    for f in (1, 2, 3):
+        src, ref = cif[f], cif[f - 1]
+        picks, _ = O.me_frame(src, ref, O.build_planes4(ref, 32), params, lam, A.split_gate_for_qp(qp))
+        d_src, d_pl = dev(acc, src), acc.hpel_build(dev(acc, ref[None]), 32)[0]
+        d_pk = dev(acc, picks)
+        co = acc.zeros((picks.shape[0], 256), acc.torch.int16)
+        keep += [d_src, d_pl, d_pk]
+        outs.append((co, src, ref, picks, qp + f))
+        frames.append(A.TqFrame(A.Picture(d_src.data_ptr(), d_pl.data_ptr(), 352, 288, 32), d_pk.data_ptr(), qp + f, 6,
+                                co.data_ptr()))
+    acc.mc_tq_frames(frames)
+    acc.sync()
+    for co, src, ref, picks, q in outs:
+        assert np.array_equal(co.cpu().numpy(), O.mc_tq_frame(src, ref, picks, q, 6))
+
+
+# ---------------------------------------------------------------------------
+# a16-a19 lookahead
+# ---------------------------------------------------------------------------
+
+@pytest.mark.parametrize("mode", [2, 1, 0])
+def test_lookahead_matches_oracle(acc, cif, mode):
+    full = dev(acc, cif)
+    half = acc.downsample2x(full)
+    acc.sync()
+    assert np.array_equal(half.cpu().numpy(), np.stack([O.downsample2x(f) for f in cif]))
+    intra, inter, mvs = acc.lookahead_costs(full, half, mode)
+    acc.sync()
+    wi, wn, wm = O.lookahead_clip(cif, mode)
+    assert np.array_equal(intra.cpu().numpy(), wi)
+    assert np.array_equal(inter.cpu().numpy(), wn)
+    assert np.array_equal(mvs.cpu().numpy(), wm)
+
+
+def test_lookahead_flat_and_static(acc):
+    flat = np.full((3, 32, 32), 77, np.uint8)
+    full = dev(acc, flat)
+    half = acc.downsample2x(full)
+    intra, inter, mvs = acc.lookahead_costs(full, half, 2)
+    acc.sync()
+    wi, wn, wm = O.lookahead_clip(flat, 2)
+    assert np.array_equal(intra.cpu().numpy(), wi) and (wi == 1).all()
+    assert np.array_equal(inter.cpu().numpy(), wn) and np.array_equal(mvs.cpu().numpy(), wm)
+
+
+# ---------------------------------------------------------------------------
+# The whole path through the host-buffer entry point
+# ---------------------------------------------------------------------------
+
+def compare_pixel_path(got, want):
+    for k in ("picks", "costs", "coeffs", "la_intra", "la_inter", "la_mvs"):
+        g, w = got[k], want[k]
+        if k == "picks":
+            g, w = g[..., :5], w[..., :5]
+        assert np.array_equal(g, w), k
+
+
+def test_pixel_path_host_cif_matches_oracle(acc, cif):
+    params = A.default_me_params()
+    qp = 26
+    lam = float(np.sqrt(A.frame_lambda(qp)))
+    gate = A.split_gate_for_qp(qp)
+    got = acc.pixel_path_host(cif, params, lam, gate, qp)
+    want = O.pixel_path_clip(cif, O.balanced_params(), lam, gate, qp, nthreads=4)
+    compare_pixel_path(got, want)
+
+
+def test_pixel_path_host_1080p_matches_oracle(acc):
+    y, _, _ = synth.hd_clip(3, 1)
+    frames = synth.coded_luma(y)
+    params = A.default_me_params()
+    qp = 27
+    lam = float(np.sqrt(A.frame_lambda(qp)) * 1.25)
+    gate = A.split_gate_for_qp(qp)
+    got = acc.pixel_path_host(frames, params, lam, gate, qp)
+    want = O.pixel_path_clip(frames, O.balanced_params(), lam, gate, qp, nthreads=8)
+    compare_pixel_path(got, want)
+    # size-independent properties of the full-size output
+    assert (got["picks"][1:, :, 0] <= 2).all()
+    assert (got["la_inter"] <= got["la_intra"]).all() and (got["la_intra"] >= 1).all()
+
+
+# ---------------------------------------------------------------------------
+# Failure handling
+# ---------------------------------------------------------------------------
+
+def test_bounded_wait_times_out_and_context_survives(acc, cif):
+    assert acc.selftest_bounded_wait(2000) == A.H264A_E_TIMEOUT
+    assert b"bounded wait" in acc.L.h264a_last_error()
+    # the context and device still work afterwards
+    got = acc.hpel_build(dev(acc, cif[:1]), 32)
+    acc.sync()
+    assert np.array_equal(got.cpu().numpy()[0], O.build_planes4(cif[0], 32))
+
+
+def test_invalid_arguments_rejected_before_launch(acc, cif):
+    d = dev(acc, cif[:1])
+    out = acc.empty((1, 4, 288 + 4, 352 + 4), acc.torch.uint8)
+    rc = acc.L.h264a_hpel_build(acc.ctx, d.data_ptr(), 352, 288, 2, 1, 352 * 288, out.data_ptr(), None)
+    assert rc == -1 and b"pad" in acc.L.h264a_last_error()
+    rc = acc.L.h264a_fullpel_grid(acc.ctx, C.byref(A.Picture(d.data_ptr(), out.data_ptr(), 352, 288, 32)), 65, None,
+                                  None, 0, 0, None, 1.0, None, None, None, None)
+    assert rc == -1
+    rc = acc.L.h264a_block_metric(acc.ctx, 0, 12, 16, d.data_ptr(), d.data_ptr(), 16, d.data_ptr(), d.data_ptr(),
+                                  None, None, 16, 1, d.data_ptr(), None)
+    assert rc == -1
