@@ -14,10 +14,10 @@
  *    is in h264a_last_error() (per thread).  Nothing aborts across the ABI.
  *  - Pointers named d_* are device pointers (CUDA global memory of the
  *    context's device); h_* are host pointers.  Callers own every buffer.
- *  - `stream` is a cudaStream_t (NULL = the context's own stream).  Calls only
- *    enqueue work; results are ready when the stream is synchronised
- *    (h264a_sync).  Calls on one context from several threads must use
- *    different streams.
+ *  - `stream` is a cudaStream_t (NULL = the device's default stream, as in the
+ *    CUDA runtime).  Calls only enqueue work; results are ready when the
+ *    stream is synchronised (h264a_sync).  h264a_me_frames serialises on the
+ *    context's work-queue scratch: one context per concurrent stream.
  *  - Planes: a reference picture's cached planes are one buffer F|H|V|C, each
  *    pw*ph bytes with pw = cw + 2*pad, ph = ch + 2*pad, stride pw: the
  *    HpelPlanes layout of crates/rusty_h264-common/src/inter.rs:707-730.

@@ -166,6 +166,51 @@ __device__ __forceinline__ void fullpel_rows_clamped(const uint8_t* pic, int w, 
     }
 }
 
+// Quarter-pel prediction rows of a 4x4 block straight from a plain picture
+// (no cached planes), every tap clamped: luma_sample (inter.rs:134-176), the
+// value mc_luma returns.  Used where the reference interpolates a picture it
+// keeps no planes for (the lookahead's sub-pel seed probes).
+__device__ __forceinline__ int pic_at(const uint8_t* pic, int w, int h, int x, int y) {
+    return __ldg(pic + (long long)clampi(y, 0, h - 1) * w + clampi(x, 0, w - 1));
+}
+__device__ __forceinline__ int clip255d(int v) { return v < 0 ? 0 : (v > 255 ? 255 : v); }
+// value of plane `pl` (0 full-pel, 1 horizontal half, 2 vertical half, 3 centre) at (x, y)
+__device__ __forceinline__ int half_sample(const uint8_t* pic, int w, int h, int pl, int x, int y) {
+    if (pl == 0) return pic_at(pic, w, h, x, y);
+    if (pl == 1) {
+        const int s = pic_at(pic, w, h, x - 2, y) - 5 * pic_at(pic, w, h, x - 1, y) + 20 * pic_at(pic, w, h, x, y) +
+                      20 * pic_at(pic, w, h, x + 1, y) - 5 * pic_at(pic, w, h, x + 2, y) + pic_at(pic, w, h, x + 3, y);
+        return clip255d((s + 16) >> 5);
+    }
+    if (pl == 2) {
+        const int s = pic_at(pic, w, h, x, y - 2) - 5 * pic_at(pic, w, h, x, y - 1) + 20 * pic_at(pic, w, h, x, y) +
+                      20 * pic_at(pic, w, h, x, y + 1) - 5 * pic_at(pic, w, h, x, y + 2) + pic_at(pic, w, h, x, y + 3);
+        return clip255d((s + 16) >> 5);
+    }
+    const int tap[6] = {1, -5, 20, 20, -5, 1};
+    int acc = 0;
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+        int v = 0;
+#pragma unroll
+        for (int j = 0; j < 6; j++) v += tap[j] * pic_at(pic, w, h, x - 2 + k, y - 2 + j);
+        acc += tap[k] * v;
+    }
+    return clip255d((acc + 512) >> 10);
+}
+__device__ __noinline__ static void subpel_rows_clamped(const uint8_t* pic, int w, int h, int x, int y, int fx, int fy, uint32_t out[4]) {
+    const PhaseOps op = phase_ops(fx, fy);
+    for (int r = 0; r < 4; r++) {
+        uint32_t wd = 0;
+        for (int c = 0; c < 4; c++) {
+            int v = half_sample(pic, w, h, op.pa, x + c + op.dxa, y + r + op.dya);
+            if (op.pb >= 0) v = (v + half_sample(pic, w, h, op.pb, x + c + op.dxb, y + r + op.dyb) + 1) >> 1;
+            wd |= uint32_t(v) << (8 * c);
+        }
+        out[r] = wd;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Rate model and λ pricing (mb16.rs:2454-2482, 2540-2578)
 // ---------------------------------------------------------------------------

@@ -30,9 +30,8 @@ namespace h264a {
 void set_error(const std::string &msg);
 int fail(int code, const std::string &msg);
 int cuda_fail(cudaError_t e, const char *what);
-inline cudaStream_t pick_stream(h264a_ctx *ctx, void *s) {
-    return s ? reinterpret_cast<cudaStream_t>(s) : ctx->stream;
-}
+// `stream` follows the CUDA convention: NULL is the device's default stream.
+inline cudaStream_t pick_stream(h264a_ctx *, void *s) { return reinterpret_cast<cudaStream_t>(s); }
 int check_launch(const char *what);
 // grows the per-MB done flags to at least n entries (zeroed, epoch reset)
 int ensure_me_scratch(h264a_ctx *ctx, size_t n);

@@ -80,7 +80,8 @@ __global__ void la_intra_kernel(const uint8_t* __restrict__ pics, size_t fstride
     }
 }
 
-// One warp's view of a full-pel SATD search of a bs x bs block.
+// One warp's view of the SATD search of a bs x bs block (full-pel steps around
+// a seed that may carry a sub-pel fraction).
 struct LaSearch {
     const uint8_t* cur;
     const uint8_t* ref;
@@ -111,7 +112,10 @@ struct LaSearch {
             if (c < n) {
                 const int2 mv = cand[c];
                 uint32_t p[4];
-                fullpel_rows_clamped(ref, w, h, x0 + bxo + (mv.x >> 2), y0 + byo + (mv.y >> 2), p);
+                if (((mv.x | mv.y) & 3) == 0)
+                    fullpel_rows_clamped(ref, w, h, x0 + bxo + (mv.x >> 2), y0 + byo + (mv.y >> 2), p);
+                else  // a sub-pel seed (Hybrid mode halves a full-res MV): mc_luma on the plain picture
+                    subpel_rows_clamped(ref, w, h, x0 + bxo + (mv.x >> 2), y0 + byo + (mv.y >> 2), mv.x & 3, mv.y & 3, p);
                 d = satd4x4_rows(srow, p);
             }
             d = warp_seg_sum(d, nb);

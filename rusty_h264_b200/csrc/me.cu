@@ -305,8 +305,13 @@ __device__ void motion_search_warp(Search& s, const int* preds, int npred, const
             for (int guard = 0; guard < (1 << 20); guard++) {
                 if (sp_fc && (pat & 1) == 0 && (step == 1 || ((bx & 3) == 0 && (by & 3) == 0))) {
                     iter++;
+                    // hpel_qpel_refs / hpel_ref resolve every ring point (inter.rs:1015, 1060):
+                    // inside the +1-slack window, and at step 1 a quarter phase
                     bool all = true;
-                    for (int i = 0; i < 8; i++) all = all && s.in_plane_window(bx + kRingX[i] * step, by + kRingY[i] * step);
+                    for (int i = 0; i < 8; i++) {
+                        const int qx = bx + kRingX[i] * step, qy = by + kRingY[i] * step;
+                        all = all && s.in_plane_window(qx, qy) && (step == 2 || ((qx | qy) & 1));
+                    }
                     if (all) {
                         if (s.lane < 8) s.ws->cand[s.lane] = make_int2(bx + kRingX[s.lane] * step, by + kRingY[s.lane] * step);
                         __syncwarp();

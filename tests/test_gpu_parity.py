@@ -372,8 +372,8 @@ def test_dct_quant_4x4_matches_oracle(acc):
         for i in range(n):
             x, y = xy[i]
             d = np.zeros(64, np.int16)
-            s = np.ascontiguousarray(src[y:, x:])
-            p = np.ascontiguousarray(pred[y:, x:])
+            s = src.reshape(-1)[y * 96 + x:]
+            p = pred.reshape(-1)[y * 96 + x:]
             L.or_dct_four_t4(O.ptr(d, O.i16p), O.ptr(s), 96, O.ptr(p), 96)
             ff, mf = np.zeros(8, np.int16), np.zeros(8, np.int16)
             L.or_quant_dz_ff(int(qp[i]), dz, O.ptr(ff, O.i16p))
