@@ -29,6 +29,14 @@ __device__ __forceinline__ uint32_t ld4u(const uint8_t* p) {
     return __funnelshift_r(lo, hi, sh);
 }
 
+// Branch-free form of ld4u for reads whose following aligned word is known to
+// lie inside the buffer (plane reads inside the padded window).
+__device__ __forceinline__ uint32_t ld4u_nb(const uint8_t* p) {
+    const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+    const uint32_t* w = reinterpret_cast<const uint32_t*>(a & ~uintptr_t(3));
+    return __funnelshift_r(__ldg(w), __ldg(w + 1), uint32_t(a & 3) * 8u);
+}
+
 __device__ __forceinline__ int byte_of(uint32_t w, int k) { return int((w >> (8 * k)) & 0xffu); }
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
@@ -59,6 +67,54 @@ __device__ __forceinline__ int satd4x4_rows(const uint32_t s[4], const uint32_t 
         sum += abs(s0 + s1) + abs(s2 + s3) + abs(s2 - s3) + abs(s0 - s1);
     }
     return sum;
+}
+
+// Per-byte (a+b+1)>>1 (what pavgb and the reference's avg_rows compute):
+// (a|b) − ((a^b)>>1) per byte, which never borrows across bytes.
+__device__ __forceinline__ uint32_t avg_up4(uint32_t a, uint32_t b) {
+    return (a | b) - (((a ^ b) >> 1) & 0x7f7f7f7fu);
+}
+
+// Source rows of a 4x4 block split into column pairs (c0|c2) and (c1|c3) in
+// 16-bit halves, the operand form of satd4x4_packed.
+__device__ __forceinline__ void split_pairs(const uint32_t s[4], uint32_t a[4], uint32_t b[4]) {
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+        a[r] = __byte_perm(s[r], 0u, 0x4240);
+        b[r] = __byte_perm(s[r], 0u, 0x4341);
+    }
+}
+
+// Low 16 bits, sign-extended (the low half of a packed pair).
+__device__ __forceinline__ int sext16(int v) { return int(int16_t(uint16_t(uint32_t(v) & 0xffffu))); }
+
+// Σ|H·(s−p)·Hᵀ| of a 4x4 block with the source pre-split (split_pairs): the
+// same value as satd4x4_rows.  Each 32-bit register carries two columns as
+// hi·2^16 + lo; the butterflies are linear, so plain 32-bit adds keep both
+// halves exact (|half| <= 2040 here).  The last butterfly of every row is
+// folded into |x+y| + |x−y| = 2·max(|x|,|y|).
+__device__ __forceinline__ int satd4x4_packed(const uint32_t sa[4], const uint32_t sb[4], const uint32_t p[4]) {
+    int A[4], B[4];
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+        A[r] = int(sa[r]) - int(__byte_perm(p[r], 0u, 0x4240));
+        B[r] = int(sb[r]) - int(__byte_perm(p[r], 0u, 0x4341));
+    }
+    {
+        const int t0 = A[0] + A[1], t1 = A[0] - A[1], t2 = A[2] + A[3], t3 = A[2] - A[3];
+        A[0] = t0 + t2; A[1] = t1 + t3; A[2] = t0 - t2; A[3] = t1 - t3;
+        const int u0 = B[0] + B[1], u1 = B[0] - B[1], u2 = B[2] + B[3], u3 = B[2] - B[3];
+        B[0] = u0 + u2; B[1] = u1 + u3; B[2] = u0 - u2; B[3] = u1 - u3;
+    }
+    int sum = 0;
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+        const int pp = A[r] + B[r], qq = A[r] - B[r];
+        const int pl = sext16(pp), ph = (pp - pl) >> 16;
+        const int ql = sext16(qq), qh = (qq - ql) >> 16;
+        sum += max(abs(pl), abs(ph)) + max(abs(ql), abs(qh));
+    }
+    return 2 * sum;
 }
 
 // Σ|s−p| of one 4x4 block (sad_scalar, satd_sad.rs:74).
@@ -105,29 +161,59 @@ __device__ __forceinline__ PhaseOps phase_ops(int fx, int fy) {
     }
 }
 
+// The same table packed into two 64-bit words, one byte per phase fx*4+fy:
+// bits 0-1 plane a, bits 2-3 plane b (0 = single plane; b is never F),
+// bit 4 dx_a, bit 5 dy_a, bit 6 dx_b, bit 7 dy_b.  A byte extract replaces the
+// divergent switch when the lanes of a warp hold different phases.
+__host__ __device__ constexpr uint32_t phase_byte(int pa, int pb, int dxa, int dya, int dxb, int dyb) {
+    return uint32_t(pa | (pb << 2) | (dxa << 4) | (dya << 5) | (dxb << 6) | (dyb << 7));
+}
+constexpr unsigned long long kPhaseLo =
+    (unsigned long long)phase_byte(0, 0, 0, 0, 0, 0) | ((unsigned long long)phase_byte(0, 2, 0, 0, 0, 0) << 8) |
+    ((unsigned long long)phase_byte(2, 0, 0, 0, 0, 0) << 16) | ((unsigned long long)phase_byte(0, 2, 0, 1, 0, 0) << 24) |
+    ((unsigned long long)phase_byte(0, 1, 0, 0, 0, 0) << 32) | ((unsigned long long)phase_byte(1, 2, 0, 0, 0, 0) << 40) |
+    ((unsigned long long)phase_byte(2, 3, 0, 0, 0, 0) << 48) | ((unsigned long long)phase_byte(1, 2, 0, 1, 0, 0) << 56);
+constexpr unsigned long long kPhaseHi =
+    (unsigned long long)phase_byte(1, 0, 0, 0, 0, 0) | ((unsigned long long)phase_byte(1, 3, 0, 0, 0, 0) << 8) |
+    ((unsigned long long)phase_byte(3, 0, 0, 0, 0, 0) << 16) | ((unsigned long long)phase_byte(1, 3, 0, 1, 0, 0) << 24) |
+    ((unsigned long long)phase_byte(0, 1, 1, 0, 0, 0) << 32) | ((unsigned long long)phase_byte(1, 2, 0, 0, 1, 0) << 40) |
+    ((unsigned long long)phase_byte(2, 3, 1, 0, 0, 0) << 48) | ((unsigned long long)phase_byte(1, 2, 0, 1, 1, 0) << 56);
+
+__device__ __forceinline__ uint32_t phase_bits(int fx, int fy) {
+    const int idx = fx * 4 + fy;
+    const unsigned long long w = idx < 8 ? kPhaseLo : kPhaseHi;
+    return uint32_t(w >> ((idx & 7) * 8)) & 0xffu;
+}
+
 // The four packed prediction rows of the 4x4 block whose top-left full-pel
 // sample is (ix, iy) in picture coordinates, at phase (fx, fy).  Equal to
 // mc_luma (inter.rs:1193) for every position: inside the padded planes the rows
-// are plane reads (and the (a+b+1)>>1 average, which __vavgu4 computes per
-// byte); outside, every operand coordinate is clamped to the plane, which
+// are plane reads (and the (a+b+1)>>1 average, computed per byte by
+// avg_up4); outside, every operand coordinate is clamped to the plane, which
 // reproduces mc_luma's per-tap clamping because the planes are built from the
 // edge-replicated picture with a pad of at least 3.
 __device__ __forceinline__ void pred_rows(const Planes& P, int ix, int iy, int fx, int fy, uint32_t out[4]) {
-    const PhaseOps op = phase_ops(fx, fy);
     const int px = ix + P.pad, py = iy + P.pad;
-    const bool inside = px >= 0 && py >= 0 && px + 5 <= P.pw && py + 5 <= P.ph;
+    // inside: both aligned words ld4u_nb touches for an operand starting at
+    // px+dx (dx <= 1) end by px+8, so they stay in the operand's row
+    const bool inside = px >= 0 && py >= 0 && px + 9 <= P.pw && py + 5 <= P.ph;
     if (inside) {
-        const uint8_t* a = P.plane(op.pa) + (long long)(py + op.dya) * P.pw + px + op.dxa;
-        if (op.pb < 0) {
+        const uint32_t pb = phase_bits(fx, fy);
+        const int pa = int(pb & 3), pbb = int((pb >> 2) & 3);
+        const uint8_t* a = P.base + P.ps * pa + (long long)(py + int((pb >> 5) & 1)) * P.pw + px + int((pb >> 4) & 1);
+        if (pbb == 0) {
 #pragma unroll
-            for (int r = 0; r < 4; r++) out[r] = ld4u(a + (long long)r * P.pw);
+            for (int r = 0; r < 4; r++) out[r] = ld4u_nb(a + (long long)r * P.pw);
         } else {
-            const uint8_t* b = P.plane(op.pb) + (long long)(py + op.dyb) * P.pw + px + op.dxb;
+            const uint8_t* b =
+                P.base + P.ps * pbb + (long long)(py + int((pb >> 7) & 1)) * P.pw + px + int((pb >> 6) & 1);
 #pragma unroll
-            for (int r = 0; r < 4; r++) out[r] = __vavgu4(ld4u(a + (long long)r * P.pw), ld4u(b + (long long)r * P.pw));
+            for (int r = 0; r < 4; r++)
+                out[r] = avg_up4(ld4u_nb(a + (long long)r * P.pw), ld4u_nb(b + (long long)r * P.pw));
         }
         return;
     }
+    const PhaseOps op = phase_ops(fx, fy);
     const uint8_t* A = P.plane(op.pa);
     const uint8_t* B = P.plane(op.pb < 0 ? op.pa : op.pb);
 #pragma unroll

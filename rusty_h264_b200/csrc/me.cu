@@ -50,12 +50,17 @@ struct WarpScratch {
     int dist[32];
 };
 
+// Candidates per round: rings have 4 or 8 points and seeds at most 5, so a
+// 16x16 round needs at most four 32-lane passes.
+constexpr int ME_MAX_PASS = 4;
+
 struct Search {
     MePic pic;
     const MeParamsDev* pr;
     int lx, ly, rw, rh, lg_nb, lane;
     int bxo, byo;  // this lane's sub-block offset inside the partition
     uint32_t srow[4];
+    uint32_t spa[4], spb[4];  // srow split into column pairs for satd4x4_packed
     int cx, cy;    // mvd centre (predictors[0])
     double lam_r, lam_fp, lam_me;
     bool sadfp;
@@ -74,8 +79,11 @@ struct Search {
         const int blk = lane & ((1 << lg_nb) - 1);
         bxo = (blk % nbx) * 4;
         byo = (blk / nbx) * 4;
+        // x + bxo is a multiple of 4 and the row lies inside the picture: aligned loads
 #pragma unroll
-        for (int r = 0; r < 4; r++) srow[r] = ld4u(p.src + (long long)(y + byo + r) * p.cw + x + bxo);
+        for (int r = 0; r < 4; r++)
+            srow[r] = __ldg(reinterpret_cast<const uint32_t*>(p.src + (long long)(y + byo + r) * p.cw + x + bxo));
+        split_pairs(srow, spa, spb);
         cx = centre_x; cy = centre_y;
         lam_me = lambda_me;
         lam_r = prm->kind != 0 ? lambda_me * 0.25 : lambda_me;
@@ -91,53 +99,60 @@ struct Search {
         return mvbits(pr->kind, pr->tab, mvx - cx) + mvbits(pr->kind, pr->tab, mvy - cy);
     }
 
-    // Distortions of ws->cand[0..n) under `metric` into ws->dist.
-    __device__ void eval(int n, int metric) {
+    // Distortions of ws->cand[0..n) under `metric` into ws->dist.  All the
+    // round's plane loads are issued before any of them is consumed, so a round
+    // pays one memory latency however many passes it takes.
+    __device__ __noinline__ void eval(int n, int metric) {
         const int nb = 1 << lg_nb;
-        const int total = n << lg_nb;
-        for (int base = 0; base < total; base += 32) {
-            const int p = base + lane;
-            const int c = p >> lg_nb;
-            int d = 0;
-            if (c < n) {
+        const int npass = ((n << lg_nb) + 31) >> 5;
+        uint32_t pr4[ME_MAX_PASS][4];
+#pragma unroll
+        for (int k = 0; k < ME_MAX_PASS; k++) {
+            const int c = (32 * k + lane) >> lg_nb;
+            if (k < npass && c < n) {
                 const int2 mv = ws->cand[c];
-                uint32_t pr4[4];
-                pred_rows(pic.P, lx + bxo + (mv.x >> 2), ly + byo + (mv.y >> 2), mv.x & 3, mv.y & 3, pr4);
-                d = metric == MET_SAD ? sad4x4_rows(srow, pr4) : satd4x4_rows(srow, pr4);
+                pred_rows(pic.P, lx + bxo + (mv.x >> 2), ly + byo + (mv.y >> 2), mv.x & 3, mv.y & 3, pr4[k]);
             }
-            d = warp_seg_sum(d, nb);
-            if (c < n && (lane & (nb - 1)) == 0) ws->dist[c] = d;
+        }
+#pragma unroll
+        for (int k = 0; k < ME_MAX_PASS; k++) {
+            if (k < npass) {
+                const int c = (32 * k + lane) >> lg_nb;
+                int d = 0;
+                if (c < n) d = metric == MET_SAD ? sad4x4_rows(srow, pr4[k]) : satd4x4_packed(spa, spb, pr4[k]);
+                d = warp_seg_sum(d, nb);
+                if (c < n && (lane & (nb - 1)) == 0) ws->dist[c] = d;
+            }
         }
         __syncwarp();
         evals_done += n;
     }
 
-    // Price candidate `lane` (if lane < n): dist + (lam·rate) as i64.
-    __device__ __forceinline__ long long lane_cost(int n, double lam) const {
-        if (lane >= n) return LLONG_MAX;
+    // Price candidate `lane` (if lane < n): dist + (lam·rate) as i64, held in
+    // 32 bits.  Distortions are below 2^21 and λ·rate below 2^28 for every
+    // λ the encoder forms (sqrt of 0.85·2^13 times a scale <= 4, rates < 2^17),
+    // so the sum never saturates and comparisons match the reference's i64.
+    __device__ __forceinline__ int lane_cost(int n, double lam) const {
+        if (lane >= n) return INT_MAX;
         const int2 mv = ws->cand[lane];
-        return (long long)ws->dist[lane] + lam_cost(lam, rate(mv.x, mv.y));
+        const long long c = (long long)ws->dist[lane] + lam_cost(lam, rate(mv.x, mv.y));
+        return c > INT_MAX - 1 ? INT_MAX - 1 : int(c);
     }
 
-    // First-wins argmin over lanes < n; returns index or -1 if none beats best_c.
-    __device__ int argmin_below(long long cc, long long best_c, long long& out_c) const {
-        long long v = cc;
-        int idx = lane;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            const long long ov = __shfl_xor_sync(0xffffffffu, v, o);
-            const int oi = __shfl_xor_sync(0xffffffffu, idx, o);
-            if (ov < v || (ov == v && oi < idx)) { v = ov; idx = oi; }
-        }
-        out_c = v;
-        return v < best_c ? idx : -1;
+    // First-wins argmin over lanes < n; returns the index (or -1 if the
+    // minimum does not beat best_c) and the minimum in out_c.
+    __device__ __forceinline__ int argmin_below(int cc, long long best_c, long long& out_c) const {
+        const int m = __reduce_min_sync(0xffffffffu, cc);
+        const unsigned at = __ballot_sync(0xffffffffu, cc == m);
+        out_c = m;
+        return (long long)m < best_c ? __ffs(at) - 1 : -1;
     }
 
     // Fixed-centre batch of n candidates already in ws->cand: the first strict
     // minimum below best_c (or -1).  Prices with `lam`; counts n reference evals.
     __device__ int fixed_batch(int n, int metric, double lam, long long best_c, long long& bc) {
         eval(n, metric);
-        const long long cc = lane_cost(n, lam);
+        const int cc = lane_cost(n, lam);
         const int bi = argmin_below(cc, best_c, bc);
         evals_ref += n;
         __syncwarp();
@@ -155,15 +170,15 @@ struct Search {
             if (lane < n) ws->cand[lane] = make_int2(bx + rx[i + lane] * step, by + ry[i + lane] * step);
             __syncwarp();
             eval(n, metric);
-            const long long cc = lane_cost(n, lam);
-            const unsigned hit = __ballot_sync(0xffffffffu, lane < n && cc < best_c);
+            const int cc = lane_cost(n, lam);
+            const unsigned hit = __ballot_sync(0xffffffffu, lane < n && (long long)cc < best_c);
             if (hit == 0) {
                 evals_ref += n;
                 __syncwarp();
                 break;
             }
             const int j = __ffs(hit) - 1;
-            const long long cj = __shfl_sync(0xffffffffu, cc, j);
+            const int cj = __shfl_sync(0xffffffffu, cc, j);
             const int2 mv = ws->cand[j];
             evals_ref += j + 1;
             best_c = cj;
@@ -186,7 +201,7 @@ __constant__ int8_t kRingX[8] = {1, -1, 0, 0, 1, -1, 1, -1};
 __constant__ int8_t kRingY[8] = {0, 0, 1, -1, 1, -1, -1, 1};
 
 // motion_search for one partition (warp-cooperative, uniform control flow).
-__device__ void motion_search_warp(Search& s, const int* preds, int npred, const int* start, int& out_x, int& out_y,
+__device__ __noinline__ void motion_search_warp(Search& s, const int* preds, int npred, const int* start, int& out_x, int& out_y,
                                    long long& out_c) {
     const MeParamsDev& pr = *s.pr;
     const bool refine_only = start != nullptr;
@@ -209,7 +224,7 @@ __device__ void motion_search_warp(Search& s, const int* preds, int npred, const
         if (s.lane >= 1 && s.lane <= npred) s.ws->cand[s.lane] = make_int2(preds[2 * (s.lane - 1)], preds[2 * (s.lane - 1) + 1]);
         __syncwarp();
         s.eval(npred + 1, m_fp);
-        const long long cc = s.lane_cost(npred + 1, l_fp);
+        const int cc = s.lane_cost(npred + 1, l_fp);
         // sequential strict-< scan: (0,0) first, then predictors in order
         best_c = __shfl_sync(0xffffffffu, cc, 0);
         for (int i = 1; i <= npred; i++) {
@@ -397,9 +412,13 @@ struct FrameDesc {
 };
 
 // One launch's frames, passed by value.  Frames are sorted by MB count
-// (descending) and the work queue deals MB m of every frame that has one
-// before MB m+1 of any frame: segment j covers MB indices
+// (descending) and the work queue deals the k-th MB of every frame that has
+// one before the (k+1)-th of any frame: segment j covers positions
 // [nmb[j+1], nmb[j]) of frames 0..j, so its tickets are (nmb[j]-nmb[j+1])*(j+1).
+// Within a frame the k-th MB is taken in wavefront order (anti-diagonals
+// t = x + 2y, then y): every MB's neighbours (left, top, top-left, top-right)
+// lie on earlier diagonals, so a window of resident warps always holds MBs
+// that are ready, and no MB ever waits on a ticket dealt after its own.
 constexpr int ME_MAXF = 96;
 struct FrameBatch {
     FrameDesc f[ME_MAXF];
@@ -408,6 +427,30 @@ struct FrameBatch {
 };
 
 constexpr int SPIN_LIMIT = 1000 * 1000;  // ~0.5 s of polling (a 200 ns sleep per poll)
+
+// Number of MBs (x, y) of a W x H frame with x + 2y < t.
+__device__ __forceinline__ int wave_prefix(int W, int H, int t) {
+    int n = 0;
+    for (int y = 0; y < H; y++) {
+        const int c = t - 2 * y;
+        if (c <= 0) break;
+        n += c < W ? c : W;
+    }
+    return n;
+}
+
+// The k-th MB of a W x H frame in wavefront order.
+__device__ __forceinline__ void wave_mb(int W, int H, int k, int& x, int& y) {
+    int lo = 0, hi = (W - 1) + 2 * (H - 1);  // find the diagonal t with prefix(t) <= k < prefix(t+1)
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (wave_prefix(W, H, mid) <= k) lo = mid; else hi = mid - 1;
+    }
+    const int t = lo;
+    const int ylo = t - (W - 1) > 0 ? (t - (W - 1) + 1) >> 1 : 0;
+    y = ylo + (k - wave_prefix(W, H, t));
+    x = t - 2 * y;
+}
 
 __device__ __forceinline__ int ld_acquire(const int* p) {
     int v;
@@ -451,7 +494,7 @@ __device__ __forceinline__ int2 predict_mv_ref0(bool aa, int2 a, bool ba, int2 b
     return make_int2(med(mva.x, mvb.x, mvc.x), med(mva.y, mvb.y, mvc.y));
 }
 
-__global__ void __launch_bounds__(32 * ME_WARPS) me_frames_kernel(const __grid_constant__ FrameBatch batch,
+__global__ void __launch_bounds__(32 * ME_WARPS, 5) me_frames_kernel(const __grid_constant__ FrameBatch batch,
                                                                  long long total, MeParamsDev prm,
                                                                  int* __restrict__ counter, int* __restrict__ flags,
                                                                  int epoch, int* __restrict__ status, int spin_limit) {
@@ -468,8 +511,10 @@ __global__ void __launch_bounds__(32 * ME_WARPS) me_frames_kernel(const __grid_c
         const long long u = t - batch.seg_start[j];
         const int nxt = j + 1 < batch.n ? batch.f[j + 1].mb_w * batch.f[j + 1].mb_h : 0;
         const FrameDesc& fd = batch.f[int(u % (j + 1))];
-        const int m = nxt + int(u / (j + 1));
-        const int mbx = m % fd.mb_w, mby = m / fd.mb_w;
+        const int k = nxt + int(u / (j + 1));  // position in the frame's wavefront order
+        int mbx, mby;
+        wave_mb(fd.mb_w, fd.mb_h, k, mbx, mby);
+        const int m = mby * fd.mb_w + mbx;
         int* fl = flags + fd.flag_base;
         // dependencies: left, and top-right (or top at the right edge)
         if (lane == 0) {

@@ -30,7 +30,7 @@ __global__ void block_metric_kernel(int metric, int w, int h, const uint8_t* __r
         if (metric == H264A_METRIC_SATD_AVG || metric == H264A_METRIC_SAD_AVG) {
             const uint8_t* c = Cc + c_off[pair] + (long long)by * sb + bx;
 #pragma unroll
-            for (int r = 0; r < 4; r++) p[r] = __vavgu4(ld4u(b + (long long)r * sb), ld4u(c + (long long)r * sb));
+            for (int r = 0; r < 4; r++) p[r] = avg_up4(ld4u(b + (long long)r * sb), ld4u(c + (long long)r * sb));
         } else {
 #pragma unroll
             for (int r = 0; r < 4; r++) p[r] = ld4u(b + (long long)r * sb);
