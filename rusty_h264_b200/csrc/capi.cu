@@ -57,11 +57,13 @@ int ensure_me_scratch(h264a_ctx* ctx, size_t n) {
     ctx->d_flags = nullptr;
     ctx->flags_cap = 0;
     size_t cap = n < 4096 ? 4096 : n + n / 4;
-    if (cudaMalloc(&ctx->d_flags, cap * sizeof(int32_t)) != cudaSuccess) {
+    cap = (cap + 63) & ~size_t(63);
+    const size_t bytes = cap * sizeof(int32_t);  // one done flag per MB
+    if (cudaMalloc(&ctx->d_flags, bytes) != cudaSuccess) {
         cudaGetLastError();
-        return fail(H264A_E_NOMEM, "persistent-kernel flags: cudaMalloc failed");
+        return fail(H264A_E_NOMEM, "persistent-kernel scratch: cudaMalloc failed");
     }
-    H264A_CUDA(cudaMemset(ctx->d_flags, 0, cap * sizeof(int32_t)));
+    H264A_CUDA(cudaMemset(ctx->d_flags, 0, bytes));
     ctx->flags_cap = cap;
     ctx->epoch = 0;
     return H264A_OK;
@@ -104,7 +106,7 @@ extern "C" int h264a_ctx_create(int device, h264a_ctx** out) {
     c->device = device;
     c->num_sms = prop.multiProcessorCount;
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaMalloc(&c->d_counter, sizeof(int32_t)) != cudaSuccess ||
+        cudaMalloc(&c->d_counter, 4 * sizeof(int32_t)) != cudaSuccess ||
         cudaMalloc(&c->d_status, sizeof(int32_t)) != cudaSuccess ||
         cudaMemset(c->d_status, 0, sizeof(int32_t)) != cudaSuccess) {
         const cudaError_t e = cudaGetLastError();

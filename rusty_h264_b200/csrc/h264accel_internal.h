@@ -13,11 +13,12 @@ struct h264a_ctx {
     int device = 0;
     int num_sms = 0;
     cudaStream_t stream = nullptr;
-    // device scratch of the persistent ME kernel: work-queue counter, per-MB
-    // done flags, and a status word (error code + where it happened)
+    // device scratch of the persistent ME kernel: the work-queue counter, one
+    // done flag per MB (flags_cap MBs), and a status word (the code of a
+    // bounded wait that ran out)
     int32_t *d_counter = nullptr;
     int32_t *d_flags = nullptr;
-    size_t flags_cap = 0;      // number of int32 flags allocated
+    size_t flags_cap = 0;      // MBs the scratch holds
     int32_t *d_status = nullptr;
     int32_t epoch = 0;         // value a finished MB writes into its flag
     // cached buffers of h264a_pixel_path_host

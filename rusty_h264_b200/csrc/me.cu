@@ -25,217 +25,226 @@ namespace h264a {
 constexpr int MET_SATD = 0;
 constexpr int MET_SAD = 1;
 
-struct MePic {
-    Planes P;
-    const uint8_t* src;
-    int cw, ch;
-};
-
-__device__ __forceinline__ MePic make_pic(const h264a_picture& pc) {
-    MePic m;
-    m.P.base = pc.d_planes;
-    m.P.pad = pc.pad;
-    m.P.pw = pc.cw + 2 * pc.pad;
-    m.P.ph = pc.ch + 2 * pc.pad;
-    m.P.ps = (long long)m.P.pw * m.P.ph;
-    m.src = pc.d_src;
-    m.cw = pc.cw;
-    m.ch = pc.ch;
-    return m;
-}
-
-// Per-warp shared scratch: candidate MVs and their distortions.
+// Per-warp shared state: the round's candidates and distortions, and the
+// search's cold parameters (read a few times per round, so they live here
+// rather than in registers).
 struct WarpScratch {
     int2 cand[32];
     int dist[32];
+    const uint8_t* base;  // F|H|V|C planes
+    int pw, ph, pad, cw, ch, rw, rh;
+    int cx, cy;           // mvd centre, predictors[0]
+    double lam_r;         // cost's λ (λ/4 for the table kinds)
+    double lam_fp;        // cost_fp's λ (λ·RFF_ME_SADL under B2, else λ)
+    double lam_me;        // λ itself (the batched sub-pel arms)
 };
 
-// Candidates per round: rings have 4 or 8 points and seeds at most 5, so a
-// 16x16 round needs at most four 32-lane passes.
-constexpr int ME_MAX_PASS = 4;
+// Passes whose plane loads are in flight together (a 16x16 ring of 8 takes
+// four 32-lane passes, done as two groups).
+constexpr int ME_MAX_PASS = 2;
 
-struct Search {
-    MePic pic;
-    const MeParamsDev* pr;
-    int lx, ly, rw, rh, lg_nb, lane;
-    int bxo, byo;  // this lane's sub-block offset inside the partition
+// Register-resident part of one search (every function below is inlined, so
+// nothing of it is ever addressed in local memory); the rest is in the
+// warp's WarpScratch.
+struct SearchGeom {
+    int lx, ly, lg_nb, lane, bxo, byo;
+    uint32_t spa[4], spb[4];  // this lane's source 4x4 rows, split into column pairs
+};
+
+__device__ __forceinline__ void geom_init(SearchGeom& g, WarpScratch& ws, const h264a_picture& pc, int x, int y, int w,
+                                          int h) {
+    g.lx = x; g.ly = y;
+    g.lane = threadIdx.x & 31;
+    if (g.lane == 0) {
+        ws.base = pc.d_planes;
+        ws.pad = pc.pad;
+        ws.pw = pc.cw + 2 * pc.pad;
+        ws.ph = pc.ch + 2 * pc.pad;
+        ws.cw = pc.cw;
+        ws.ch = pc.ch;
+        ws.rw = w;
+        ws.rh = h;
+    }
+    g.lg_nb = (w == 16 ? 2 : (w == 8 ? 1 : 0)) + (h == 16 ? 2 : (h == 8 ? 1 : 0));
+    const int nbx = w >> 2;
+    const int blk = g.lane & ((1 << g.lg_nb) - 1);
+    g.bxo = (blk % nbx) * 4;
+    g.byo = (blk / nbx) * 4;
     uint32_t srow[4];
-    uint32_t spa[4], spb[4];  // srow split into column pairs for satd4x4_packed
-    int cx, cy;    // mvd centre (predictors[0])
-    double lam_r, lam_fp, lam_me;
-    bool sadfp;
-    int m_main;    // metric of `cost`
-    int evals_ref, evals_done;
-    WarpScratch* ws;
-
-    __device__ void init(const MePic& p, const MeParamsDev* prm, int x, int y, int w, int h, int centre_x,
-                         int centre_y, double lambda_me, bool refine_only, WarpScratch* scratch) {
-        pic = p;
-        pr = prm;
-        lx = x; ly = y; rw = w; rh = h;
-        lane = threadIdx.x & 31;
-        lg_nb = (w == 16 ? 2 : (w == 8 ? 1 : 0)) + (h == 16 ? 2 : (h == 8 ? 1 : 0));
-        const int nbx = w >> 2;
-        const int blk = lane & ((1 << lg_nb) - 1);
-        bxo = (blk % nbx) * 4;
-        byo = (blk / nbx) * 4;
-        // x + bxo is a multiple of 4 and the row lies inside the picture: aligned loads
+    // x + bxo is a multiple of 4 and the row lies inside the picture: aligned loads
 #pragma unroll
-        for (int r = 0; r < 4; r++)
-            srow[r] = __ldg(reinterpret_cast<const uint32_t*>(p.src + (long long)(y + byo + r) * p.cw + x + bxo));
-        split_pairs(srow, spa, spb);
-        cx = centre_x; cy = centre_y;
-        lam_me = lambda_me;
-        lam_r = prm->kind != 0 ? lambda_me * 0.25 : lambda_me;
-        sadfp = !prm->fast && !refine_only && prm->sadfp;
-        lam_fp = lambda_me * (sadfp ? prm->sadfp_lambda : 1.0);
-        m_main = prm->use_sad ? MET_SAD : MET_SATD;
-        evals_ref = 0;
-        evals_done = 0;
-        ws = scratch;
-    }
+    for (int r = 0; r < 4; r++)
+        srow[r] = __ldg(reinterpret_cast<const uint32_t*>(pc.d_src + (long long)(y + g.byo + r) * pc.cw + x + g.bxo));
+    split_pairs(srow, g.spa, g.spb);
+    __syncwarp();
+}
 
-    __device__ __forceinline__ uint32_t rate(int mvx, int mvy) const {
-        return mvbits(pr->kind, pr->tab, mvx - cx) + mvbits(pr->kind, pr->tab, mvy - cy);
-    }
-
-    // Distortions of ws->cand[0..n) under `metric` into ws->dist.  All the
-    // round's plane loads are issued before any of them is consumed, so a round
-    // pays one memory latency however many passes it takes.
-    __device__ __noinline__ void eval(int n, int metric) {
-        const int nb = 1 << lg_nb;
-        const int npass = ((n << lg_nb) + 31) >> 5;
-        uint32_t pr4[ME_MAX_PASS][4];
+// Distortions of ws.cand[0..n) under `metric` into ws.dist.  All the round's
+// plane loads are issued before any is consumed, so a round pays one memory
+// latency however many passes it takes.
+__device__ __forceinline__ void eval_round(const SearchGeom& g, WarpScratch& ws, int n, int metric) {
+    const int nb = 1 << g.lg_nb;
+    const int npass = ((n << g.lg_nb) + 31) >> 5;
+    Planes P;
+    P.base = ws.base; P.pw = ws.pw; P.ph = ws.ph; P.pad = ws.pad; P.ps = (long long)ws.pw * ws.ph;
+    for (int k0 = 0; k0 < npass; k0 += ME_MAX_PASS) {
+    uint32_t pr4[ME_MAX_PASS][4];
 #pragma unroll
-        for (int k = 0; k < ME_MAX_PASS; k++) {
-            const int c = (32 * k + lane) >> lg_nb;
-            if (k < npass && c < n) {
-                const int2 mv = ws->cand[c];
-                pred_rows(pic.P, lx + bxo + (mv.x >> 2), ly + byo + (mv.y >> 2), mv.x & 3, mv.y & 3, pr4[k]);
-            }
+    for (int kk = 0; kk < ME_MAX_PASS; kk++) {
+        const int k = k0 + kk;
+        const int c = (32 * k + g.lane) >> g.lg_nb;
+        if (k < npass && c < n) {
+            const int2 mv = ws.cand[c];
+            pred_rows(P, g.lx + g.bxo + (mv.x >> 2), g.ly + g.byo + (mv.y >> 2), mv.x & 3, mv.y & 3, pr4[kk]);
         }
+    }
 #pragma unroll
-        for (int k = 0; k < ME_MAX_PASS; k++) {
-            if (k < npass) {
-                const int c = (32 * k + lane) >> lg_nb;
-                int d = 0;
-                if (c < n) d = metric == MET_SAD ? sad4x4_rows(srow, pr4[k]) : satd4x4_packed(spa, spb, pr4[k]);
-                d = warp_seg_sum(d, nb);
-                if (c < n && (lane & (nb - 1)) == 0) ws->dist[c] = d;
+    for (int kk = 0; kk < ME_MAX_PASS; kk++) {
+        const int k = k0 + kk;
+        if (k < npass) {
+            const int c = (32 * k + g.lane) >> g.lg_nb;
+            int d = 0;
+            if (c < n) {
+                if (metric == MET_SAD) {
+                    uint32_t srow[4];
+#pragma unroll
+                    for (int r = 0; r < 4; r++) srow[r] = g.spa[r] | (g.spb[r] << 8);
+                    d = sad4x4_rows(srow, pr4[kk]);
+                } else {
+                    d = satd4x4_packed(g.spa, g.spb, pr4[kk]);
+                }
             }
+            d = warp_seg_sum(d, nb);
+            if (c < n && (g.lane & (nb - 1)) == 0) ws.dist[c] = d;
         }
-        __syncwarp();
-        evals_done += n;
     }
+    }
+    __syncwarp();
+}
 
-    // Price candidate `lane` (if lane < n): dist + (lam·rate) as i64, held in
-    // 32 bits.  Distortions are below 2^21 and λ·rate below 2^28 for every
-    // λ the encoder forms (sqrt of 0.85·2^13 times a scale <= 4, rates < 2^17),
-    // so the sum never saturates and comparisons match the reference's i64.
-    __device__ __forceinline__ int lane_cost(int n, double lam) const {
-        if (lane >= n) return INT_MAX;
-        const int2 mv = ws->cand[lane];
-        const long long c = (long long)ws->dist[lane] + lam_cost(lam, rate(mv.x, mv.y));
-        return c > INT_MAX - 1 ? INT_MAX - 1 : int(c);
-    }
+// Rate of an MV against the search's mvd centre (mb16.rs:2454-2482).
+__device__ __forceinline__ uint32_t rate_of(const MeParamsDev& pr, const WarpScratch& ws, int mvx, int mvy) {
+    return mvbits(pr.kind, pr.tab, mvx - ws.cx) + mvbits(pr.kind, pr.tab, mvy - ws.cy);
+}
 
-    // First-wins argmin over lanes < n; returns the index (or -1 if the
-    // minimum does not beat best_c) and the minimum in out_c.
-    __device__ __forceinline__ int argmin_below(int cc, long long best_c, long long& out_c) const {
-        const int m = __reduce_min_sync(0xffffffffu, cc);
-        const unsigned at = __ballot_sync(0xffffffffu, cc == m);
-        out_c = m;
-        return (long long)m < best_c ? __ffs(at) - 1 : -1;
-    }
+// dist + (lam·rate) as i64 for candidate `lane` (< n), held in 32 bits: the
+// distortions are below 2^21 and λ·rate below 2^28 for every λ the encoder
+// forms (sqrt of 0.85·2^13 times a scale <= 4, rates < 2^17), so the sum
+// never saturates and comparisons match the reference's i64.
+__device__ __forceinline__ int lane_cost(const MeParamsDev& pr, const WarpScratch& ws, int lane, int n, double lam) {
+    if (lane >= n) return INT_MAX;
+    const int2 mv = ws.cand[lane];
+    const long long c = (long long)ws.dist[lane] + lam_cost(lam, rate_of(pr, ws, mv.x, mv.y));
+    return c > INT_MAX - 1 ? INT_MAX - 1 : int(c);
+}
 
-    // Fixed-centre batch of n candidates already in ws->cand: the first strict
-    // minimum below best_c (or -1).  Prices with `lam`; counts n reference evals.
-    __device__ int fixed_batch(int n, int metric, double lam, long long best_c, long long& bc) {
-        eval(n, metric);
-        const int cc = lane_cost(n, lam);
-        const int bi = argmin_below(cc, best_c, bc);
-        evals_ref += n;
-        __syncwarp();
-        return bi;
-    }
-
-    // Cascading ring around a moving centre (the reference's first-improver
-    // walk).  ring offsets (dx,dy)*step; returns whether any point improved.
-    __device__ bool cascade_ring(const int8_t* rx, const int8_t* ry, int nring, int step, int metric, double lam,
-                                 long long& best_c, int& bx, int& by) {
-        bool improved = false;
-        int i = 0;
-        while (i < nring) {
-            const int n = nring - i;
-            if (lane < n) ws->cand[lane] = make_int2(bx + rx[i + lane] * step, by + ry[i + lane] * step);
-            __syncwarp();
-            eval(n, metric);
-            const int cc = lane_cost(n, lam);
-            const unsigned hit = __ballot_sync(0xffffffffu, lane < n && (long long)cc < best_c);
-            if (hit == 0) {
-                evals_ref += n;
-                __syncwarp();
-                break;
-            }
-            const int j = __ffs(hit) - 1;
-            const int cj = __shfl_sync(0xffffffffu, cc, j);
-            const int2 mv = ws->cand[j];
-            evals_ref += j + 1;
-            best_c = cj;
-            bx = mv.x;
-            by = mv.y;
-            improved = true;
-            i += j + 1;
-            __syncwarp();
-        }
-        return improved;
-    }
-
-    __device__ bool in_plane_window(int mvx, int mvy) const {
-        const int px = lx + (mvx >> 2) + pic.P.pad, py = ly + (mvy >> 2) + pic.P.pad;
-        return px >= 0 && py >= 0 && px + rw + 1 <= pic.P.pw && py + rh + 1 <= pic.P.ph;
-    }
-};
+// Fixed-centre batch of n candidates already in ws.cand: index of the first
+// strict minimum below best_c, or -1 (the reference's argmin loops).
+__device__ __forceinline__ int fixed_batch(const SearchGeom& g, const MeParamsDev& pr, WarpScratch& ws, int n,
+                                           int metric, double lam, long long best_c, long long& bc, int& evals) {
+    eval_round(g, ws, n, metric);
+    const int cc = lane_cost(pr, ws, g.lane, n, lam);
+    const int m = __reduce_min_sync(0xffffffffu, cc);
+    const unsigned at = __ballot_sync(0xffffffffu, cc == m);
+    evals += n;
+    __syncwarp();
+    bc = m;
+    return (long long)m < best_c ? __ffs(at) - 1 : -1;
+}
 
 __constant__ int8_t kRingX[8] = {1, -1, 0, 0, 1, -1, 1, -1};
 __constant__ int8_t kRingY[8] = {0, 0, 1, -1, 1, -1, -1, 1};
 
-// motion_search for one partition (warp-cooperative, uniform control flow).
-__device__ __noinline__ void motion_search_warp(Search& s, const int* preds, int npred, const int* start, int& out_x, int& out_y,
-                                   long long& out_c) {
-    const MeParamsDev& pr = *s.pr;
+// Cascading ring around a moving centre (the reference's first-improver
+// walk): points are priced against the current centre; at the first
+// improvement the centre moves and the remaining points are re-priced around
+// it, which is the order the reference evaluates them in.
+__device__ __forceinline__ bool cascade_ring(const SearchGeom& g, const MeParamsDev& pr, WarpScratch& ws, int nring,
+                                             int step, int metric, double lam, long long& best_c, int& bx, int& by,
+                                             int& evals) {
+    bool improved = false;
+    int i = 0;
+    while (i < nring) {
+        const int n = nring - i;
+        if (g.lane < n) ws.cand[g.lane] = make_int2(bx + kRingX[i + g.lane] * step, by + kRingY[i + g.lane] * step);
+        __syncwarp();
+        eval_round(g, ws, n, metric);
+        const int cc = lane_cost(pr, ws, g.lane, n, lam);
+        const unsigned hit = __ballot_sync(0xffffffffu, g.lane < n && (long long)cc < best_c);
+        if (hit == 0) {
+            evals += n;
+            __syncwarp();
+            break;
+        }
+        const int j = __ffs(hit) - 1;
+        const int cj = __shfl_sync(0xffffffffu, cc, j);
+        const int2 mv = ws.cand[j];
+        evals += j + 1;
+        best_c = cj;
+        bx = mv.x;
+        by = mv.y;
+        improved = true;
+        i += j + 1;
+        __syncwarp();
+    }
+    return improved;
+}
+
+__device__ __forceinline__ bool in_plane_window(const SearchGeom& g, const WarpScratch& ws, int mvx, int mvy) {
+    const int px = g.lx + (mvx >> 2) + ws.pad, py = g.ly + (mvy >> 2) + ws.pad;
+    return px >= 0 && py >= 0 && px + ws.rw + 1 <= ws.pw && py + ws.rh + 1 <= ws.ph;
+}
+
+// motion_search (mb16.rs:2433-3302) of the partition in `g` (warp-cooperative,
+// uniform control flow).  preds: npred (x,y) pairs, preds[0] the mvd centre;
+// start: refine-only start MV or nullptr.  Returns the reference's evaluation
+// count in `evals`.
+__device__ __forceinline__ void motion_search_warp(const SearchGeom& g, const MeParamsDev& pr, WarpScratch& ws,
+                                                   const int* preds, int npred, const int* start, double lambda_me,
+                                                   int& out_x, int& out_y, long long& out_c, int& evals) {
     const bool refine_only = start != nullptr;
-    const int m_fp = s.sadfp ? MET_SAD : s.m_main;
-    const double l_fp = s.sadfp ? s.lam_fp : s.lam_r;  // cost_fp's λ (cost's λ when B2 is off)
+    const bool sadfp = !pr.fast && !refine_only && pr.sadfp;
+    const int m_main = pr.use_sad ? MET_SAD : MET_SATD;
+    if (g.lane == 0) {
+        ws.cx = preds[0];
+        ws.cy = preds[1];
+        ws.lam_me = lambda_me;
+        ws.lam_r = pr.kind != 0 ? lambda_me * 0.25 : lambda_me;
+        ws.lam_fp = lambda_me * (sadfp ? pr.sadfp_lambda : 1.0);
+    }
+    __syncwarp();
+    const int m_fp = sadfp ? MET_SAD : m_main;
+#define L_FP (sadfp ? ws.lam_fp : ws.lam_r)  // cost_fp's λ (cost's λ when B2 is off)
+    evals = 0;
     int bx = 0, by = 0;
-    long long best_c;
-    long long bc;
+    long long best_c, bc;
     // ---- seeds (mb16.rs:2580-2596) ----
     if (refine_only) {
         bx = start[0]; by = start[1];
-        if (s.lane == 0) s.ws->cand[0] = make_int2(bx, by);
+        if (g.lane == 0) ws.cand[0] = make_int2(bx, by);
         __syncwarp();
-        s.eval(1, s.m_main);
-        best_c = (long long)s.ws->dist[0] + lam_cost(s.lam_r, s.rate(bx, by));
-        s.evals_ref += 1;
+        eval_round(g, ws, 1, m_main);
+        best_c = (long long)ws.dist[0] + lam_cost(ws.lam_r, rate_of(pr, ws, bx, by));
+        evals += 1;
         __syncwarp();
     } else {
-        if (s.lane == 0) s.ws->cand[0] = make_int2(0, 0);
-        if (s.lane >= 1 && s.lane <= npred) s.ws->cand[s.lane] = make_int2(preds[2 * (s.lane - 1)], preds[2 * (s.lane - 1) + 1]);
+        if (g.lane == 0) ws.cand[0] = make_int2(0, 0);
+        if (g.lane >= 1 && g.lane <= npred)
+            ws.cand[g.lane] = make_int2(preds[2 * (g.lane - 1)], preds[2 * (g.lane - 1) + 1]);
         __syncwarp();
-        s.eval(npred + 1, m_fp);
-        const int cc = s.lane_cost(npred + 1, l_fp);
-        // sequential strict-< scan: (0,0) first, then predictors in order
+        eval_round(g, ws, npred + 1, m_fp);
+        const int cc = lane_cost(pr, ws, g.lane, npred + 1, L_FP);
+        // sequential strict-< scan: (0,0) first, then the predictors in order
         best_c = __shfl_sync(0xffffffffu, cc, 0);
         for (int i = 1; i <= npred; i++) {
             const long long ci = __shfl_sync(0xffffffffu, cc, i);
             if (ci < best_c) {
                 best_c = ci;
-                bx = s.ws->cand[i].x;
-                by = s.ws->cand[i].y;
+                bx = ws.cand[i].x;
+                by = ws.cand[i].y;
             }
         }
-        s.evals_ref += npred + 1;
+        evals += npred + 1;
         __syncwarp();
     }
     const int seed_x = bx, seed_y = by;
@@ -243,46 +252,41 @@ __device__ __noinline__ void motion_search_warp(Search& s, const int* preds, int
     // ---- integer snap (mb16.rs:2597-2607) ----
     if (!refine_only && pr.me_snap && ((bx & 3) != 0 || (by & 3) != 0)) {
         const int sx = ((bx + 2) >> 2) * 4, sy = ((by + 2) >> 2) * 4;
-        if (s.lane == 0) s.ws->cand[0] = make_int2(sx, sy);
+        if (g.lane == 0) ws.cand[0] = make_int2(sx, sy);
         __syncwarp();
-        s.eval(1, m_fp);
-        best_c = (long long)s.ws->dist[0] + lam_cost(l_fp, s.rate(sx, sy));
-        s.evals_ref += 1;
+        eval_round(g, ws, 1, m_fp);
+        best_c = (long long)ws.dist[0] + lam_cost(L_FP, rate_of(pr, ws, sx, sy));
+        evals += 1;
         bx = sx; by = sy;
         __syncwarp();
     }
     // ---- diamond ladder (mb16.rs:2616-2727) ----
     if (!refine_only) {
-        int steps[5];
-        int nsteps = 0;
-        if (pr.fast) {
-            steps[0] = 16; steps[1] = 4; nsteps = 2;
-        } else {
-            const uint32_t mask = (s.rw < 8 || s.rh < 8) ? pr.dia_sub_mask : pr.dia_mask;
-            const int rungs[5] = {64, 32, 16, 8, 4};
-#pragma unroll
-            for (int i = 0; i < 5; i++)
-                if (mask & (1u << i)) steps[nsteps++] = rungs[i];
-        }
-        const bool x4shape = (s.rw == 16 || s.rw == 8) && (s.rh == 16 || s.rh == 8);
+        const int rw = ws.rw, rh = ws.rh;
+        const bool x4shape = (rw == 16 || rw == 8) && (rh == 16 || rh == 8);
         const bool fc = !pr.fast && pr.fc && x4shape;
-        for (int si = 0; si < nsteps; si++) {
-            const int step = steps[si];
+        const uint32_t mask = pr.fast ? 0u : ((rw < 8 || rh < 8) ? pr.dia_sub_mask : pr.dia_mask);
+        for (int si = 0; si < 5; si++) {
+            int step;
+            if (pr.fast) {
+                if (si >= 2) break;
+                step = si == 0 ? 16 : 4;
+            } else {
+                if (!(mask & (1u << si))) continue;
+                step = 64 >> si;  // rungs [64,32,16,8,4] quarter-pel
+            }
             for (int guard = 0; guard < (1 << 20); guard++) {
                 if (fc && (bx & 3) == 0 && (by & 3) == 0) {
                     const int st = step >> 2;
-                    const int px = s.lx + (bx >> 2), py = s.ly + (by >> 2);
-                    if (px - st >= 0 && py - st >= 0 && px + st + s.rw <= s.pic.cw && py + st + s.rh <= s.pic.ch) {
-                        if (s.lane < 4) s.ws->cand[s.lane] = make_int2(bx + kRingX[s.lane] * step, by + kRingY[s.lane] * step);
+                    const int px = g.lx + (bx >> 2), py = g.ly + (by >> 2);
+                    if (px - st >= 0 && py - st >= 0 && px + st + rw <= ws.cw && py + st + rh <= ws.ch) {
+                        if (g.lane < 4) ws.cand[g.lane] = make_int2(bx + kRingX[g.lane] * step, by + kRingY[g.lane] * step);
                         __syncwarp();
-                        int bi;
-                        if (s.rw == 16) {
-                            // sad_x4 / satd_x4 batch priced with lam_fp (mb16.rs:2676-2690)
-                            bi = s.fixed_batch(4, s.sadfp ? MET_SAD : MET_SATD, s.lam_fp, best_c, bc);
-                        } else {
-                            // 8-wide shapes price each point with cost_fp (mb16.rs:2691)
-                            bi = s.fixed_batch(4, m_fp, l_fp, best_c, bc);
-                        }
+                        // 16-wide: sad_x4 / satd_x4 batch priced with lam_fp (mb16.rs:2676-2690);
+                        // 8-wide shapes price each point with cost_fp (mb16.rs:2691)
+                        const int bi = rw == 16
+                                           ? fixed_batch(g, pr, ws, 4, sadfp ? MET_SAD : MET_SATD, ws.lam_fp, best_c, bc, evals)
+                                           : fixed_batch(g, pr, ws, 4, m_fp, L_FP, best_c, bc, evals);
                         if (bi < 0) break;
                         best_c = bc;
                         bx += kRingX[bi] * step;
@@ -290,28 +294,29 @@ __device__ __noinline__ void motion_search_warp(Search& s, const int* preds, int
                         continue;
                     }
                 }
-                if (!s.cascade_ring(kRingX, kRingY, 4, step, m_fp, l_fp, best_c, bx, by)) break;
+                if (!cascade_ring(g, pr, ws, 4, step, m_fp, L_FP, best_c, bx, by, evals)) break;
             }
         }
     }
     // ---- B2 reprice into the SATD domain (mb16.rs:2744-2747) ----
-    if (s.sadfp) {
-        if (s.lane == 0) {
-            s.ws->cand[0] = make_int2(bx, by);
-            s.ws->cand[1] = make_int2(seed_x, seed_y);
+    if (sadfp) {
+        if (g.lane == 0) {
+            ws.cand[0] = make_int2(bx, by);
+            ws.cand[1] = make_int2(seed_x, seed_y);
         }
         __syncwarp();
-        s.eval(2, s.m_main);
-        best_c = (long long)s.ws->dist[0] + lam_cost(s.lam_r, s.rate(bx, by));
-        seed_c = (long long)s.ws->dist[1] + lam_cost(s.lam_r, s.rate(seed_x, seed_y));
-        s.evals_ref += 2;
+        eval_round(g, ws, 2, m_main);
+        best_c = (long long)ws.dist[0] + lam_cost(ws.lam_r, rate_of(pr, ws, bx, by));
+        seed_c = (long long)ws.dist[1] + lam_cost(ws.lam_r, rate_of(pr, ws, seed_x, seed_y));
+        evals += 2;
         __syncwarp();
     }
     // ---- sub-pel rings (mb16.rs:2956-3283) ----
     if (pr.subpel) {
-        const bool sub_shape = s.rw < 8 || s.rh < 8;
+        const int rw = ws.rw, rh = ws.rh;
+        const bool sub_shape = rw < 8 || rh < 8;
         const int pat = pr.subpel_pat >= 0 ? pr.subpel_pat : (sub_shape ? pr.sub_pat : (pr.sp_single_pass ? 2 : 0));
-        const bool x4shape = (s.rw == 16 || s.rw == 8) && (s.rh == 16 || s.rh == 8);
+        const bool x4shape = (rw == 16 || rw == 8) && (rh == 16 || rh == 8);
         const bool sp_fc = pr.sp_fc && !pr.fast && x4shape;
         const int nring = (pat & 1) ? 4 : 8;
         for (int k = 0; k < 2; k++) {
@@ -325,15 +330,16 @@ __device__ __noinline__ void motion_search_warp(Search& s, const int* preds, int
                     bool all = true;
                     for (int i = 0; i < 8; i++) {
                         const int qx = bx + kRingX[i] * step, qy = by + kRingY[i] * step;
-                        all = all && s.in_plane_window(qx, qy) && (step == 2 || ((qx | qy) & 1));
+                        all = all && in_plane_window(g, ws, qx, qy) && (step == 2 || ((qx | qy) & 1));
                     }
                     if (all) {
-                        if (s.lane < 8) s.ws->cand[s.lane] = make_int2(bx + kRingX[s.lane] * step, by + kRingY[s.lane] * step);
+                        if (g.lane < 8) ws.cand[g.lane] = make_int2(bx + kRingX[g.lane] * step, by + kRingY[g.lane] * step);
                         __syncwarp();
                         // 16-wide: satd_avg_x4 / satd_x4p priced with lambda_me; 8-wide: cost()
-                        const int bi = s.rw == 16 ? s.fixed_batch(8, MET_SATD, s.lam_me, best_c, bc)
-                                                  : s.fixed_batch(8, s.m_main, s.lam_r, best_c, bc);
-                        const bool stop = bi < 0 || !pr.me_subpel_iter || (pat & 2) || (pr.sp_maxit != 0 && iter >= pr.sp_maxit);
+                        const int bi = rw == 16 ? fixed_batch(g, pr, ws, 8, MET_SATD, ws.lam_me, best_c, bc, evals)
+                                                : fixed_batch(g, pr, ws, 8, m_main, ws.lam_r, best_c, bc, evals);
+                        const bool stop =
+                            bi < 0 || !pr.me_subpel_iter || (pat & 2) || (pr.sp_maxit != 0 && iter >= pr.sp_maxit);
                         if (bi >= 0) {
                             best_c = bc;
                             bx += kRingX[bi] * step;
@@ -345,7 +351,7 @@ __device__ __noinline__ void motion_search_warp(Search& s, const int* preds, int
                     iter--;
                 }
                 iter++;
-                const bool improved = s.cascade_ring(kRingX, kRingY, nring, step, s.m_main, s.lam_r, best_c, bx, by);
+                const bool improved = cascade_ring(g, pr, ws, nring, step, m_main, ws.lam_r, best_c, bx, by, evals);
                 if (!improved || !pr.me_subpel_iter || (pat & 2) || (pr.sp_maxit != 0 && iter >= pr.sp_maxit)) break;
             }
         }
@@ -355,6 +361,7 @@ __device__ __noinline__ void motion_search_warp(Search& s, const int* preds, int
         bx = seed_x; by = seed_y; best_c = seed_c;
     }
     out_x = bx; out_y = by; out_c = best_c;
+#undef L_FP
 }
 
 __device__ __forceinline__ bool job_shape_ok(int w, int h) {
@@ -365,8 +372,9 @@ __device__ __forceinline__ bool job_shape_ok(int w, int h) {
 constexpr int ME_WARPS = 4;
 
 __global__ void __launch_bounds__(32 * ME_WARPS) me_search_kernel(const h264a_picture* __restrict__ pics, int npics,
-                                                                 MeParamsDev prm, const h264a_me_job* __restrict__ jobs,
-                                                                 int n, h264a_me_result* __restrict__ out) {
+                                                                 const __grid_constant__ MeParamsDev prm,
+                                                                 const h264a_me_job* __restrict__ jobs, int n,
+                                                                 h264a_me_result* __restrict__ out) {
     __shared__ WarpScratch scratch[ME_WARPS];
     const int w = threadIdx.x >> 5;
     const long long j = (long long)blockIdx.x * ME_WARPS + w;
@@ -385,14 +393,14 @@ __global__ void __launch_bounds__(32 * ME_WARPS) me_search_kernel(const h264a_pi
         if ((threadIdx.x & 31) == 0) out[j] = res;
         return;
     }
-    Search s;
-    s.init(make_pic(pc), &prm, job.x, job.y, job.w, job.h, job.preds[0], job.preds[1], job.lambda_me,
-           job.has_start != 0, &scratch[w]);
-    int mx, my;
+    SearchGeom g;
+    geom_init(g, scratch[w], pc, job.x, job.y, job.w, job.h);
+    int mx, my, evals;
     long long c;
-    motion_search_warp(s, job.preds, job.npred, job.has_start ? job.start : nullptr, mx, my, c);
+    motion_search_warp(g, prm, scratch[w], job.preds, job.npred, job.has_start ? job.start : nullptr, job.lambda_me, mx,
+                       my, c, evals);
     if ((threadIdx.x & 31) == 0) {
-        res.mvx = mx; res.mvy = my; res.cost = c; res.evals = s.evals_ref; res.status = 0;
+        res.mvx = mx; res.mvy = my; res.cost = c; res.evals = evals; res.status = 0;
         out[j] = res;
     }
 }
@@ -494,10 +502,18 @@ __device__ __forceinline__ int2 predict_mv_ref0(bool aa, int2 a, bool ba, int2 b
     return make_int2(med(mva.x, mvb.x, mvc.x), med(mva.y, mvb.y, mvc.y));
 }
 
-__global__ void __launch_bounds__(32 * ME_WARPS, 5) me_frames_kernel(const __grid_constant__ FrameBatch batch,
-                                                                 long long total, MeParamsDev prm,
-                                                                 int* __restrict__ counter, int* __restrict__ flags,
-                                                                 int epoch, int* __restrict__ status, int spin_limit) {
+// The persistent plain-ME kernel.  Each warp takes MB tickets dealt in
+// wavefront order (frames interleaved), waits (bounded, status 1) until the
+// MB's left and top-right neighbours are published, derives the median
+// predictor from their picks, runs best_part for 16x16 and, when its J exceeds
+// the gate, for the four 16x8/8x16 partitions (mb16.rs:8869-8913), and
+// publishes the pick.
+__global__ void __launch_bounds__(32 * ME_WARPS, 4) me_frames_kernel(const __grid_constant__ FrameBatch batch,
+                                                                    long long total,
+                                                                    const __grid_constant__ MeParamsDev prm,
+                                                                    int* __restrict__ counter, int* __restrict__ flags,
+                                                                    int epoch, int* __restrict__ status,
+                                                                    int spin_limit) {
     __shared__ WarpScratch scratch[ME_WARPS];
     const int w = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
@@ -525,44 +541,40 @@ __global__ void __launch_bounds__(32 * ME_WARPS, 5) me_frames_kernel(const __gri
         // neighbours of the MB's top-left 4x4 block (mv_neighbors_block, mb16.rs:1871)
         const bool aa = mbx > 0, ba = mby > 0, ca = mby > 0 && mbx < fd.mb_w - 1, da = mbx > 0 && mby > 0;
         const int2 a = aa ? pick_mv_at(fd.picks, m - 1, 3, 0) : make_int2(0, 0);
-        const int2 b = ba ? pick_mv_at(fd.picks, m - fd.mb_w, 0, 3) : make_int2(0, 0);
+        const int2 bb = ba ? pick_mv_at(fd.picks, m - fd.mb_w, 0, 3) : make_int2(0, 0);
         int2 c = ca ? pick_mv_at(fd.picks, m - fd.mb_w + 1, 0, 3) : make_int2(0, 0);
         bool cav = ca;
         if (!ca) {
             cav = da;
             c = da ? pick_mv_at(fd.picks, m - fd.mb_w - 1, 3, 3) : make_int2(0, 0);
         }
-        const int2 pmv = predict_mv_ref0(aa, a, ba, b, cav, c);
-        const MePic pic = make_pic(fd.pic);
+        const int2 pmv = predict_mv_ref0(aa, a, ba, bb, cav, c);
         const int lx = mbx * 16, ly = mby * 16;
         int preds[4] = {pmv.x, pmv.y, 0, 0};
-        Search s;
-        int x16, y16;
-        long long c16;
-        s.init(pic, &prm, lx, ly, 16, 16, pmv.x, pmv.y, fd.lambda_me, false, &scratch[w]);
-        motion_search_warp(s, preds, 1, nullptr, x16, y16, c16);
-        int evals = s.evals_ref << s.lg_nb;  // 4x4-block evaluations
-        int shape = 0;
-        int mv0x = x16, mv0y = y16, mv1x = x16, mv1y = y16;
-        long long best = c16;
-        if (fd.split_gate >= 0 && c16 > fd.split_gate) {
-            preds[2] = x16; preds[3] = y16;
-            int px[4], py[4];
-            long long pc[4];
-            const int ox[4] = {0, 0, 0, 8}, oy[4] = {0, 8, 0, 0};
-            const int ww[4] = {16, 16, 8, 8}, hh[4] = {8, 8, 16, 16};
-            for (int k = 0; k < 4; k++) {
-                s.init(pic, &prm, lx + ox[k], ly + oy[k], ww[k], hh[k], pmv.x, pmv.y, fd.lambda_me, false, &scratch[w]);
-                motion_search_warp(s, preds, 2, nullptr, px[k], py[k], pc[k]);
-                evals += s.evals_ref << s.lg_nb;
-            }
-            if (pc[0] + pc[1] < best) {
-                best = pc[0] + pc[1]; shape = 1;
-                mv0x = px[0]; mv0y = py[0]; mv1x = px[1]; mv1y = py[1];
-            }
-            if (pc[2] + pc[3] < best) {
-                best = pc[2] + pc[3]; shape = 2;
-                mv0x = px[2]; mv0y = py[2]; mv1x = px[3]; mv1y = py[3];
+        // best_part for 16x16, then (J above the gate) the four partitions
+        // seeded with [pmv, mv16]; one inlined search body.
+        int evals = 0, shape = 0, mv0x = 0, mv0y = 0, mv1x = 0, mv1y = 0;
+        long long c16 = 0, best = 0, pc0 = 0;
+        int px0 = 0, py0 = 0;
+        for (int k5 = 0; k5 < 5; k5++) {
+            if (k5 == 1 && !(fd.split_gate >= 0 && c16 > fd.split_gate)) break;
+            const int ox = k5 == 4 ? 8 : 0, oy = k5 == 2 ? 8 : 0;
+            const int ww = k5 == 0 ? 16 : (k5 <= 2 ? 16 : 8), hh = k5 == 0 ? 16 : (k5 <= 2 ? 8 : 16);
+            SearchGeom geo;
+            geom_init(geo, scratch[w], fd.pic, lx + ox, ly + oy, ww, hh);
+            int rx, ry, ev;
+            long long rc;
+            motion_search_warp(geo, prm, scratch[w], preds, k5 == 0 ? 1 : 2, nullptr, fd.lambda_me, rx, ry, rc, ev);
+            evals += ev << geo.lg_nb;  // 4x4-block evaluations
+            if (k5 == 0) {
+                c16 = rc; best = rc;
+                mv0x = mv1x = rx; mv0y = mv1y = ry;
+                preds[2] = rx; preds[3] = ry;
+            } else if (k5 == 1 || k5 == 3) {
+                px0 = rx; py0 = ry; pc0 = rc;
+            } else if (pc0 + rc < best) {  // k5 == 2: the 16x8 pair, k5 == 4: the 8x16 pair
+                best = pc0 + rc; shape = k5 == 2 ? 1 : 2;
+                mv0x = px0; mv0y = py0; mv1x = rx; mv1y = ry;
             }
         }
         if (lane == 0) {
