@@ -170,6 +170,24 @@ typedef struct {
 H264A_API int h264a_me_frames(h264a_ctx *ctx, const h264a_me_frame *h_frames, int nframes, const h264a_me_params *params,
                     void *stream);
 
+/* h264a_me_frames for callers that cannot allocate device memory when they
+ * run motion estimation (an encoder thread that must not block on the CUDA
+ * allocator, or a host that gives this library a fixed memory budget and owns
+ * every buffer).  No counterpart in the reference.  It needs no context and
+ * allocates nothing: the persistent kernel's scratch (queue counter and one
+ * flag per macroblock) is a fixed device array inside the library, so one call
+ * covers at most H264A_NOALLOC_MAX_MBS macroblocks (sum over its frames) and at
+ * most 96 frames; larger requests return H264A_E_ARG.  The array is set up
+ * (its device address looked up) on the first call on each device, so make
+ * that first call before any stream capture.  Every call on a device shares
+ * the array: calls that overlap on the GPU race and must not be issued on
+ * concurrent streams.  The caller passes a device int32 d_status, which the
+ * call zeroes and the kernel sets to non-zero if a bounded wait ran out; read
+ * it after synchronising `stream`.  Outputs as h264a_me_frames. */
+#define H264A_NOALLOC_MAX_MBS 65536
+H264A_API int h264a_me_frames_noalloc(const h264a_me_frame *h_frames, int nframes, const h264a_me_params *params,
+                                      int32_t *d_status, void *stream);
+
 /* Exhaustive full-pel 16x16 grid (±R around each MB's centre MV) with SAD and
  * SATD values as the ME cost functions return them (mc_sad_hp / mc_satd_hp at
  * full-pel MVs), and the per-MB argmin of dist + (λ·bits(mv − pmv)) in raster

@@ -79,7 +79,7 @@ EXPORTS = (
     "h264a_block_metric", "h264a_candidate_dist", "h264a_me_params_default", "h264a_build_mv_cost_table",
     "h264a_me_search", "h264a_me_frames", "h264a_fullpel_grid", "h264a_dct_quant_4x4", "h264a_dct_quant_8x8",
     "h264a_mc_tq_frames", "h264a_downsample2x", "h264a_lookahead_costs", "h264a_pixel_path_host",
-    "h264a_selftest_bounded_wait", "h264a_measure_int32_peak",
+    "h264a_selftest_bounded_wait", "h264a_measure_int32_peak", "h264a_me_frames_noalloc",
 )
 
 _lib = None
@@ -118,6 +118,7 @@ def load_library() -> C.CDLL:
                                         vp, vp, vp]
     L.h264a_selftest_bounded_wait.argtypes = [vp, i32, vp]
     L.h264a_measure_int32_peak.argtypes = [vp, C.POINTER(C.c_double)]
+    L.h264a_me_frames_noalloc.argtypes = [vp, i32, C.POINTER(MeParams), vp, vp]
     _lib = L
     return L
 

@@ -16,6 +16,8 @@
 #include <algorithm>
 #include <climits>
 #include <cstring>
+#include <mutex>
+#include <string>
 #include <vector>
 
 #include "h264a_device.cuh"
@@ -690,4 +692,132 @@ extern "C" int h264a_me_frames(h264a_ctx* ctx, const h264a_me_frame* h_frames, i
         if (rc) return rc;
     }
     return H264A_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Plain-ME frames without any allocation
+// ---------------------------------------------------------------------------
+//
+// Some callers cannot allocate device memory at the moment they run motion
+// estimation: a real-time encoder thread that must not block on the CUDA
+// allocator (cudaMalloc can synchronise the device and take a global lock),
+// or a host application that hands this library a fixed memory budget and
+// owns every buffer itself.  h264a_me_frames needs a context, and the
+// context allocates the persistent kernel's scratch (the work-queue counter
+// and one done flag per macroblock).  The entry below runs the same kernel
+// with that scratch taken from this fixed array instead: one counter word
+// plus one flag word per macroblock, for at most H264A_NOALLOC_MAX_MBS
+// macroblocks per call (256 KiB per device, held by every device that loads
+// the library until the process exits).
+
+namespace h264a {
+
+// [0] work-queue counter, [1..] per-MB done flags.
+static __device__ __align__(256) int g_noalloc_scratch[1 + H264A_NOALLOC_MAX_MBS];
+
+struct NoallocDevice {
+    int* scratch;  // device address of g_noalloc_scratch on this device (nullptr: not set up)
+    int epoch;     // flag value of the latest launch on this device
+};
+constexpr int kNoallocMaxDevices = 64;
+static NoallocDevice g_noalloc_dev[kNoallocMaxDevices];
+static std::mutex g_noalloc_mu;
+
+}  // namespace h264a
+
+extern "C" int h264a_me_frames_noalloc(const h264a_me_frame* h_frames, int nframes, const h264a_me_params* params,
+                                       int32_t* d_status, void* stream) {
+    if (!h_frames || !params || !d_status) return fail(H264A_E_ARG, "me_frames_noalloc: null pointer");
+    if (nframes < 1 || nframes > ME_MAXF)
+        return fail(H264A_E_ARG, "me_frames_noalloc: 1 to " + std::to_string(ME_MAXF) + " frames per call");
+    if ((params->mv_cost_kind == 1 || params->mv_cost_kind == 2) && !params->d_mv_cost_tab)
+        return fail(H264A_E_ARG, "me_frames_noalloc: mv cost kinds 1 and 2 need d_mv_cost_tab");
+    long long total = 0;
+    for (int i = 0; i < nframes; i++) {
+        const h264a_me_frame& f = h_frames[i];
+        if (!f.pic.d_src || !f.pic.d_planes || !f.d_picks || !f.d_costs)
+            return fail(H264A_E_ARG, "me_frames_noalloc: null frame pointer");
+        if (f.pic.cw < 16 || f.pic.ch < 16 || f.pic.cw % 16 || f.pic.ch % 16 || f.pic.pad < 3 || f.pic.pad > 128)
+            return fail(H264A_E_ARG, "me_frames_noalloc: frames must be MB-aligned with 3 <= pad <= 128");
+        total += (long long)(f.pic.cw / 16) * (f.pic.ch / 16);
+    }
+    if (total > H264A_NOALLOC_MAX_MBS)
+        return fail(H264A_E_ARG, "me_frames_noalloc: " + std::to_string(total) + " macroblocks exceed the " +
+                                     std::to_string(H264A_NOALLOC_MAX_MBS) + "-macroblock scratch of this entry point");
+    int dev = 0;
+    H264A_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kNoallocMaxDevices) return fail(H264A_E_ARG, "me_frames_noalloc: device index too large");
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    int* scratch;
+    int epoch;
+    {
+        std::lock_guard<std::mutex> lock(g_noalloc_mu);
+        NoallocDevice& nd = g_noalloc_dev[dev];
+        if (!nd.scratch) {
+            // first call on this device: the array's device address (the
+            // symbol itself is only a host-side stand-in)
+            void* p = nullptr;
+            H264A_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+            nd.scratch = static_cast<int*>(p);
+            nd.epoch = 0;
+        }
+        if (nd.epoch >= 0x7ffffff0) {  // flags from older launches must never equal the new value
+            H264A_CUDA(cudaMemsetAsync(nd.scratch + 1, 0, sizeof(int) * H264A_NOALLOC_MAX_MBS, st));
+            nd.epoch = 0;
+        }
+        epoch = ++nd.epoch;
+        scratch = nd.scratch;
+    }
+    // frames largest first, dealt round-robin in wavefront order (as h264a_me_frames)
+    int order[ME_MAXF];
+    for (int i = 0; i < nframes; i++) order[i] = i;
+    for (int i = 1; i < nframes; i++) {  // stable insertion sort by size, descending
+        const int v = order[i];
+        const long long sv = (long long)h_frames[v].pic.cw * h_frames[v].pic.ch;
+        int k = i;
+        while (k > 0 && (long long)h_frames[order[k - 1]].pic.cw * h_frames[order[k - 1]].pic.ch < sv) {
+            order[k] = order[k - 1];
+            k--;
+        }
+        order[k] = v;
+    }
+    FrameBatch fb;
+    memset(&fb, 0, sizeof fb);
+    fb.n = nframes;
+    long long acc = 0;
+    total = 0;
+    for (int k = 0; k < nframes; k++) {
+        const h264a_me_frame& f = h_frames[order[k]];
+        FrameDesc& d = fb.f[k];
+        d.pic = f.pic;
+        d.lambda_me = f.lambda_me;
+        d.split_gate = f.split_gate;
+        d.picks = f.d_picks;
+        d.costs = f.d_costs;
+        d.mb_w = f.pic.cw / 16;
+        d.mb_h = f.pic.ch / 16;
+        d.flag_base = int(total);
+        total += (long long)d.mb_w * d.mb_h;
+    }
+    for (int j = 0; j < nframes; j++) {
+        fb.seg_start[j] = acc;
+        const long long nj = (long long)fb.f[j].mb_w * fb.f[j].mb_h;
+        const long long nn = j + 1 < nframes ? (long long)fb.f[j + 1].mb_w * fb.f[j + 1].mb_h : 0;
+        acc += (nj - nn) * (j + 1);
+    }
+    fb.seg_start[nframes] = acc;
+    // the counter and the caller's status word must start at zero; the flags
+    // need no clearing because every launch waits for its own epoch value
+    H264A_CUDA(cudaMemsetAsync(scratch, 0, sizeof(int), st));
+    H264A_CUDA(cudaMemsetAsync(d_status, 0, sizeof(int32_t), st));
+    int per_sm = 0, sms = 0;
+    H264A_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, me_frames_kernel, 32 * ME_WARPS, 0));
+    H264A_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    long long blocks = (long long)sms * (per_sm > 0 ? per_sm : 1);
+    const long long need = (total + ME_WARPS - 1) / ME_WARPS;
+    if (blocks > need) blocks = need;
+    const MeParamsDev prm = to_dev(*params);
+    me_frames_kernel<<<unsigned(blocks), 32 * ME_WARPS, 0, st>>>(fb, total, prm, scratch, scratch + 1, epoch,
+                                                                 d_status, SPIN_LIMIT);
+    return check_launch("me_frames_kernel (no-alloc)");
 }
