@@ -39,7 +39,66 @@ struct WarpScratch {
     double lam_r;         // cost's λ (λ/4 for the table kinds)
     double lam_fp;        // cost_fp's λ (λ·RFF_ME_SADL under B2, else λ)
     double lam_me;        // λ itself (the batched sub-pel arms)
+    int win_ok;           // the MB's reference window is staged in shared memory
+    int wx0, wy0;         // its origin in padded-plane coordinates
 };
+
+// ---------------------------------------------------------------------------
+// Per-MB reference window in shared memory
+// ---------------------------------------------------------------------------
+// The F|H|V|C planes around the MB's predicted position, copied once per MB by
+// the bulk-copy (TMA) engine: WIN_H rows of WIN_W bytes per plane, every
+// search of the MB (16x16 and its partitions) then reads its candidates from
+// shared memory.  Candidates whose reads leave the window take the plane path
+// (pred_rows), which gives the same bytes.  32 bytes of padding follow every
+// fourth row, so the rows that one candidate's 16 lanes read together (four
+// apart) land in four different 8-bank groups.
+constexpr int WIN_W = 64, WIN_H = 44;
+constexpr int WIN_PLANE = WIN_H * WIN_W + (WIN_H / 4) * 32;  // bytes per plane (a multiple of 16)
+constexpr int WIN_BYTES = 4 * WIN_PLANE;
+constexpr int WIN_R = 12;  // the window starts this far up/left of the predicted position
+constexpr int WIN_OFF = -(1 << 30);  // window offset of a search without one: below -2^29 for any MV, so every read misses
+
+__device__ __forceinline__ int win_row(int y) { return y * WIN_W + ((y >> 2) << 5); }
+
+__device__ __forceinline__ uint32_t lds_u32(uint32_t addr) {
+    uint32_t v;
+    asm volatile("ld.shared.u32 %0, [%1];" : "=r"(v) : "r"(addr));
+    return v;
+}
+
+// Rows of the 4x4 block at window position (wx, wy) (full-pel part of the MV
+// applied) at phase (fx, fy): the same operand table and averaging as
+// pred_rows, read from the staged window at shared address `win`.
+__device__ __forceinline__ void win_rows(uint32_t win, int wx, int wy, int fx, int fy, uint32_t out[4]) {
+    const uint32_t pb = phase_bits(fx, fy);
+    const int pa = int(pb & 3), pbb = int((pb >> 2) & 3);
+    const int xa = wx + int((pb >> 4) & 1), ya = wy + int((pb >> 5) & 1);
+    const uint32_t a = win + uint32_t(pa * WIN_PLANE + (xa & ~3));
+    const uint32_t sha = uint32_t(xa & 3) * 8u;
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+        const uint32_t ar = a + uint32_t(win_row(ya + r));
+        out[r] = __funnelshift_r(lds_u32(ar), lds_u32(ar + 4), sha);
+    }
+    if (pbb != 0) {
+        const int xb = wx + int((pb >> 6) & 1), yb = wy + int((pb >> 7) & 1);
+        const uint32_t b = win + uint32_t(pbb * WIN_PLANE + (xb & ~3));
+        const uint32_t shb = uint32_t(xb & 3) * 8u;
+#pragma unroll
+        for (int r = 0; r < 4; r++) {
+            const uint32_t br = b + uint32_t(win_row(yb + r));
+            out[r] = avg_up4(out[r], __funnelshift_r(lds_u32(br), lds_u32(br + 4), shb));
+        }
+    }
+}
+
+// Both operands of a block at window position (wx, wy) lie inside the window:
+// x reads cover the aligned words from (wx + dx) & ~3 to +8, rows wy + dy ..
+// wy + dy + 3, with dx, dy <= 1.
+__device__ __forceinline__ bool win_covers(int wx, int wy) {
+    return wx >= 0 && ((wx + 1) & ~3) <= WIN_W - 8 && wy >= 0 && wy + 5 <= WIN_H;
+}
 
 // Passes whose plane loads are in flight together (a 16x16 ring of 8 takes
 // four 32-lane passes, done as two groups).
@@ -50,12 +109,15 @@ constexpr int ME_MAX_PASS = 2;
 // warp's WarpScratch.
 struct SearchGeom {
     int lx, ly, lg_nb, lane, bxo, byo;
+    int wox, woy;             // this lane's block at MV (0,0) in window coordinates (WIN_OFF: no window)
+    uint32_t win;             // shared address of the warp's window
     uint32_t spa[4], spb[4];  // this lane's source 4x4 rows, split into column pairs
 };
 
 __device__ __forceinline__ void geom_init(SearchGeom& g, WarpScratch& ws, const h264a_picture& pc, int x, int y, int w,
-                                          int h) {
+                                          int h, uint32_t win) {
     g.lx = x; g.ly = y;
+    g.win = win;
     g.lane = threadIdx.x & 31;
     if (g.lane == 0) {
         ws.base = pc.d_planes;
@@ -72,6 +134,13 @@ __device__ __forceinline__ void geom_init(SearchGeom& g, WarpScratch& ws, const 
     const int blk = g.lane & ((1 << g.lg_nb) - 1);
     g.bxo = (blk % nbx) * 4;
     g.byo = (blk / nbx) * 4;
+    if (ws.win_ok) {
+        g.wox = x + g.bxo + pc.pad - ws.wx0;
+        g.woy = y + g.byo + pc.pad - ws.wy0;
+    } else {
+        g.wox = WIN_OFF;
+        g.woy = WIN_OFF;
+    }
     uint32_t srow[4];
     // x + bxo is a multiple of 4 and the row lies inside the picture: aligned loads
 #pragma unroll
@@ -97,7 +166,12 @@ __device__ __forceinline__ void eval_round(const SearchGeom& g, WarpScratch& ws,
         const int c = (32 * k + g.lane) >> g.lg_nb;
         if (k < npass && c < n) {
             const int2 mv = ws.cand[c];
-            pred_rows(P, g.lx + g.bxo + (mv.x >> 2), g.ly + g.byo + (mv.y >> 2), mv.x & 3, mv.y & 3, pr4[kk]);
+            const int dx = mv.x >> 2, dy = mv.y >> 2;
+            const int wx = g.wox + dx, wy = g.woy + dy;
+            if (win_covers(wx, wy))
+                win_rows(g.win, wx, wy, mv.x & 3, mv.y & 3, pr4[kk]);
+            else
+                pred_rows(P, g.lx + g.bxo + dx, g.ly + g.byo + dy, mv.x & 3, mv.y & 3, pr4[kk]);
         }
     }
 #pragma unroll
@@ -372,6 +446,9 @@ __device__ __forceinline__ bool job_shape_ok(int w, int h) {
 }
 
 constexpr int ME_WARPS = 4;
+#ifndef ME_MIN_BLOCKS
+#define ME_MIN_BLOCKS 3
+#endif
 
 __global__ void __launch_bounds__(32 * ME_WARPS) me_search_kernel(const h264a_picture* __restrict__ pics, int npics,
                                                                  const __grid_constant__ MeParamsDev prm,
@@ -395,8 +472,10 @@ __global__ void __launch_bounds__(32 * ME_WARPS) me_search_kernel(const h264a_pi
         if ((threadIdx.x & 31) == 0) out[j] = res;
         return;
     }
+    if ((threadIdx.x & 31) == 0) scratch[w].win_ok = 0;
+    __syncwarp();
     SearchGeom g;
-    geom_init(g, scratch[w], pc, job.x, job.y, job.w, job.h);
+    geom_init(g, scratch[w], pc, job.x, job.y, job.w, job.h, 0u);
     int mx, my, evals;
     long long c;
     motion_search_warp(g, prm, scratch[w], job.preds, job.npred, job.has_start ? job.start : nullptr, job.lambda_me, mx,
@@ -438,15 +517,12 @@ struct FrameBatch {
 
 constexpr int SPIN_LIMIT = 1000 * 1000;  // ~0.5 s of polling (a 200 ns sleep per poll)
 
-// Number of MBs (x, y) of a W x H frame with x + 2y < t.
+// Number of MBs (x, y) of a W x H frame with x + 2y < t: rows y < a are
+// full (t - 2y >= W), rows a <= y < b hold t - 2y MBs.
 __device__ __forceinline__ int wave_prefix(int W, int H, int t) {
-    int n = 0;
-    for (int y = 0; y < H; y++) {
-        const int c = t - 2 * y;
-        if (c <= 0) break;
-        n += c < W ? c : W;
-    }
-    return n;
+    const int a = t >= W ? min((t - W) / 2 + 1, H) : 0;
+    const int b = t >= 1 ? min((t - 1) / 2 + 1, H) : 0;
+    return a * W + (b - a) * t - (b - a) * (a + b - 1);
 }
 
 // The k-th MB of a W x H frame in wavefront order.
@@ -483,6 +559,38 @@ __device__ void wait_flag(const int* flag, int epoch, int* status, int code, int
     }
 }
 
+// mbarrier and bulk-copy primitives (shared addresses are 32-bit).
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+
+// Waits (bounded) for the phase `parity` of the warp's window barrier; on
+// timeout records `code` in status and keeps waiting (again bounded) so that
+// no copy is left in flight into the window.
+__device__ __forceinline__ void wait_window(uint32_t bar, uint32_t parity, int* status, int code, int limit) {
+    for (int it = 0; !mbar_try_wait(bar, parity); it++) {
+        if (it == limit) atomicCAS(status, 0, code);
+        if (it >= 2 * limit) break;
+    }
+}
+
 // The MV of neighbour MB `m`'s 4x4 block at (bx4, by4) under its pick.
 __device__ __forceinline__ int2 pick_mv_at(const int32_t* picks, int m, int bx4, int by4) {
     const int32_t* p = picks + 6 * m;
@@ -507,18 +615,30 @@ __device__ __forceinline__ int2 predict_mv_ref0(bool aa, int2 a, bool ba, int2 b
 // The persistent plain-ME kernel.  Each warp takes MB tickets dealt in
 // wavefront order (frames interleaved), waits (bounded, status 1) until the
 // MB's left and top-right neighbours are published, derives the median
-// predictor from their picks, runs best_part for 16x16 and, when its J exceeds
-// the gate, for the four 16x8/8x16 partitions (mb16.rs:8869-8913), and
-// publishes the pick.
-__global__ void __launch_bounds__(32 * ME_WARPS, 4) me_frames_kernel(const __grid_constant__ FrameBatch batch,
+// predictor from their picks, stages the reference window around it in
+// shared memory (bulk copies; status 3 if they do not land), runs best_part
+// for 16x16 and, when its J exceeds the gate, for the four 16x8/8x16
+// partitions (mb16.rs:8869-8913), and publishes the pick.
+// Dynamic shared memory: ME_WARPS windows of WIN_BYTES.
+__global__ void __launch_bounds__(32 * ME_WARPS, ME_MIN_BLOCKS) me_frames_kernel(const __grid_constant__ FrameBatch batch,
                                                                     long long total,
                                                                     const __grid_constant__ MeParamsDev prm,
                                                                     int* __restrict__ counter, int* __restrict__ flags,
                                                                     int epoch, int* __restrict__ status,
                                                                     int spin_limit) {
     __shared__ WarpScratch scratch[ME_WARPS];
+    __shared__ __align__(8) unsigned long long win_bar[ME_WARPS];
+    extern __shared__ __align__(128) uint8_t me_win[];
     const int w = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
+    const uint32_t win = uint32_t(__cvta_generic_to_shared(me_win)) + uint32_t(w * WIN_BYTES);
+    const uint32_t bar = uint32_t(__cvta_generic_to_shared(&win_bar[w]));
+    if (lane == 0) {
+        mbar_init(bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncwarp();
+    uint32_t parity = 0;
     for (;;) {
         int t = 0;
         if (lane == 0) t = atomicAdd(counter, 1);
@@ -552,6 +672,32 @@ __global__ void __launch_bounds__(32 * ME_WARPS, 4) me_frames_kernel(const __gri
         }
         const int2 pmv = predict_mv_ref0(aa, a, ba, bb, cav, c);
         const int lx = mbx * 16, ly = mby * 16;
+        // stage the window: WIN_R rows/columns up-left of the predicted
+        // position, the x origin on a 16-byte boundary (bulk-copy alignment)
+        const h264a_picture& pc = fd.pic;
+        const int pw = pc.cw + 2 * pc.pad, ph = pc.ch + 2 * pc.pad;
+        const bool win_ok = ((reinterpret_cast<uintptr_t>(pc.d_planes) | uintptr_t(pw)) & 15) == 0 && pw >= WIN_W &&
+                            ph >= WIN_H;
+        if (win_ok) {
+            const int wx0 = min(max((lx + pc.pad + (pmv.x >> 2) - WIN_R) & ~15, 0), pw - WIN_W);
+            const int wy0 = min(max(ly + pc.pad + (pmv.y >> 2) - WIN_R, 0), ph - WIN_H);
+            if (lane == 0) {
+                scratch[w].wx0 = wx0;
+                scratch[w].wy0 = wy0;
+                // the previous MB's window reads are complete (the warp is converged here)
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                mbar_expect_tx(bar, uint32_t(4 * WIN_H * WIN_W));
+            }
+            __syncwarp();
+            const long long ps = (long long)pw * ph;
+            for (int i = lane; i < 4 * WIN_H; i += 32) {
+                const int pl = i / WIN_H, r = i - pl * WIN_H;
+                bulk_g2s(win + uint32_t(pl * WIN_PLANE + win_row(r)),
+                         pc.d_planes + ps * pl + (long long)(wy0 + r) * pw + wx0, WIN_W, bar);
+            }
+        }
+        if (lane == 0) scratch[w].win_ok = win_ok;
+        __syncwarp();
         int preds[4] = {pmv.x, pmv.y, 0, 0};
         // best_part for 16x16, then (J above the gate) the four partitions
         // seeded with [pmv, mv16]; one inlined search body.
@@ -563,7 +709,11 @@ __global__ void __launch_bounds__(32 * ME_WARPS, 4) me_frames_kernel(const __gri
             const int ox = k5 == 4 ? 8 : 0, oy = k5 == 2 ? 8 : 0;
             const int ww = k5 == 0 ? 16 : (k5 <= 2 ? 16 : 8), hh = k5 == 0 ? 16 : (k5 <= 2 ? 8 : 16);
             SearchGeom geo;
-            geom_init(geo, scratch[w], fd.pic, lx + ox, ly + oy, ww, hh);
+            geom_init(geo, scratch[w], pc, lx + ox, ly + oy, ww, hh, win);
+            if (k5 == 0 && win_ok) {
+                wait_window(bar, parity, status, 3, spin_limit);
+                parity ^= 1u;
+            }
             int rx, ry, ev;
             long long rc;
             motion_search_warp(geo, prm, scratch[w], preds, k5 == 0 ? 1 : 2, nullptr, fd.lambda_me, rx, ry, rc, ev);
@@ -600,6 +750,17 @@ __global__ void bounded_wait_selftest_kernel(const int* flag, int* status, int l
 }  // namespace h264a
 
 using namespace h264a;
+
+// Dynamic shared memory of me_frames_kernel, its opt-in above 48 KB, and the
+// CTAs per SM it reaches.
+static int me_frames_setup(int& per_sm) {
+    const int smem = ME_WARPS * WIN_BYTES;
+    H264A_CUDA(cudaFuncSetAttribute(me_frames_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    per_sm = 0;
+    H264A_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, me_frames_kernel, 32 * ME_WARPS, smem));
+    if (per_sm < 1) per_sm = 1;
+    return H264A_OK;
+}
 
 extern "C" int h264a_selftest_bounded_wait(h264a_ctx* ctx, int spin_limit, void* stream) {
     if (!ctx || spin_limit < 0 || spin_limit > SPIN_LIMIT) return fail(H264A_E_ARG, "selftest_bounded_wait: bad limit");
@@ -643,7 +804,8 @@ extern "C" int h264a_me_frames(h264a_ctx* ctx, const h264a_me_frame* h_frames, i
     cudaStream_t st = pick_stream(ctx, stream);
     const MeParamsDev prm = to_dev(*params);
     int per_sm = 0;
-    H264A_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, me_frames_kernel, 32 * ME_WARPS, 0));
+    int rc0 = me_frames_setup(per_sm);
+    if (rc0) return rc0;
     // frames are launched in groups of up to ME_MAXF, largest first
     std::vector<int> order(nframes);
     for (int i = 0; i < nframes; i++) order[i] = i;
@@ -683,10 +845,10 @@ extern "C" int h264a_me_frames(h264a_ctx* ctx, const h264a_me_frame* h_frames, i
         H264A_CUDA(cudaMemsetAsync(ctx->d_counter, 0, sizeof(int32_t), st));
         const int epoch = next_epoch(ctx, st);
         if (epoch < 0) return H264A_E_CUDA;
-        long long blocks = (long long)ctx->num_sms * (per_sm > 0 ? per_sm : 1);
+        long long blocks = (long long)ctx->num_sms * per_sm;
         const long long need = (total + ME_WARPS - 1) / ME_WARPS;
         if (blocks > need) blocks = need;
-        me_frames_kernel<<<unsigned(blocks), 32 * ME_WARPS, 0, st>>>(fb, total, prm, ctx->d_counter, ctx->d_flags,
+        me_frames_kernel<<<unsigned(blocks), 32 * ME_WARPS, ME_WARPS * WIN_BYTES, st>>>(fb, total, prm, ctx->d_counter, ctx->d_flags,
                                                                      epoch, ctx->d_status, SPIN_LIMIT);
         rc = check_launch("me_frames_kernel");
         if (rc) return rc;
@@ -811,13 +973,14 @@ extern "C" int h264a_me_frames_noalloc(const h264a_me_frame* h_frames, int nfram
     H264A_CUDA(cudaMemsetAsync(scratch, 0, sizeof(int), st));
     H264A_CUDA(cudaMemsetAsync(d_status, 0, sizeof(int32_t), st));
     int per_sm = 0, sms = 0;
-    H264A_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, me_frames_kernel, 32 * ME_WARPS, 0));
+    const int rc0 = me_frames_setup(per_sm);
+    if (rc0) return rc0;
     H264A_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    long long blocks = (long long)sms * (per_sm > 0 ? per_sm : 1);
+    long long blocks = (long long)sms * per_sm;
     const long long need = (total + ME_WARPS - 1) / ME_WARPS;
     if (blocks > need) blocks = need;
     const MeParamsDev prm = to_dev(*params);
-    me_frames_kernel<<<unsigned(blocks), 32 * ME_WARPS, 0, st>>>(fb, total, prm, scratch, scratch + 1, epoch,
+    me_frames_kernel<<<unsigned(blocks), 32 * ME_WARPS, ME_WARPS * WIN_BYTES, st>>>(fb, total, prm, scratch, scratch + 1, epoch,
                                                                  d_status, SPIN_LIMIT);
     return check_launch("me_frames_kernel (no-alloc)");
 }

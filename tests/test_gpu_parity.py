@@ -246,18 +246,18 @@ def test_me_search_rejects_bad_jobs(acc, cif):
     assert (acc.me_results(raw)[:, 4] == -1).all()
 
 
-def run_me_frames(acc, pairs, params, lam, split_gate, tab=None):
+def run_me_frames(acc, pairs, params, lam, split_gate, tab=None, pad=32):
     """pairs: list of (src, ref) luma frames; returns [(picks, costs)] from the GPU."""
     frames, keep, outs = [], [], []
     for src, ref in pairs:
         ch, cw = src.shape
         nmb = (cw // 16) * (ch // 16)
-        d_src, d_pl = dev(acc, src), acc.hpel_build(dev(acc, ref[None]), 32)[0]
+        d_src, d_pl = dev(acc, src), acc.hpel_build(dev(acc, ref[None]), pad)[0]
         picks = acc.zeros((nmb, 6), acc.torch.int32)
         costs = acc.zeros((nmb, 2), acc.torch.int64)
         keep += [d_src, d_pl]
         outs.append((picks, costs))
-        frames.append(A.MeFrame(A.Picture(d_src.data_ptr(), d_pl.data_ptr(), cw, ch, 32), lam, split_gate,
+        frames.append(A.MeFrame(A.Picture(d_src.data_ptr(), d_pl.data_ptr(), cw, ch, pad), lam, split_gate,
                                 picks.data_ptr(), costs.data_ptr()))
     acc.me_frames(frames, params)
     acc.sync()
@@ -297,6 +297,25 @@ def test_me_frames_single_mb_and_flat(acc):
     for (src, ref), (picks, costs) in zip(pairs, got):
         wp, wc = O.me_frame(src, ref, O.build_planes4(ref, 32), op, 5.0, 0)
         assert np.array_equal(picks[:, :5], wp[:, :5]) and np.array_equal(costs, wc)
+
+
+@pytest.mark.parametrize("pad", [32, 35, 16])
+def test_me_frames_window_edges(acc, cif, pad):
+    """The per-MB shared-memory window and the plane path it falls back to:
+    a large global shift puts seeds and ring points outside the window, a pad
+    of 35 leaves plane rows off the 16-byte grid (no window at all), and a pad
+    of 16 on a 16x16 frame makes the planes narrower than the window."""
+    shifted = np.ascontiguousarray(np.roll(cif[2], (-17, 21), (0, 1)))
+    tiny = np.ascontiguousarray(cif[2, 100:116, 200:216])
+    tiny_ref = np.ascontiguousarray(cif[1, 100:116, 200:216])
+    pairs = [(shifted, cif[2]), (cif[3], cif[2]), (tiny, tiny_ref)]
+    lam = float(np.sqrt(A.frame_lambda(30)))
+    gate = A.split_gate_for_qp(30)
+    got = run_me_frames(acc, pairs, A.default_me_params(), lam, gate, pad=pad)
+    op = O.balanced_params()
+    for (src, ref), (picks, costs) in zip(pairs, got):
+        wp, wc = O.me_frame(src, ref, O.build_planes4(ref, pad), op, lam, gate, pad=pad)
+        assert np.array_equal(picks[:, :5], wp[:, :5]) and np.array_equal(costs, wc), pad
 
 
 def test_fullpel_grid_matches_oracle(acc, cif):
