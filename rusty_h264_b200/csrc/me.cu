@@ -214,67 +214,45 @@ __device__ __forceinline__ int lane_cost(const MeParamsDev& pr, const WarpScratc
     return c > INT_MAX - 1 ? INT_MAX - 1 : int(c);
 }
 
-// Fixed-centre batch of n candidates already in ws.cand: index of the first
-// strict minimum below best_c, or -1 (the reference's argmin loops).
-__device__ __forceinline__ int fixed_batch(const SearchGeom& g, const MeParamsDev& pr, WarpScratch& ws, int n,
-                                           int metric, double lam, long long best_c, long long& bc, int& evals) {
-    eval_round(g, ws, n, metric);
-    const int cc = lane_cost(pr, ws, g.lane, n, lam);
-    const int m = __reduce_min_sync(0xffffffffu, cc);
-    const unsigned at = __ballot_sync(0xffffffffu, cc == m);
-    evals += n;
-    __syncwarp();
-    bc = m;
-    return (long long)m < best_c ? __ffs(at) - 1 : -1;
-}
-
-__constant__ int8_t kRingX[8] = {1, -1, 0, 0, 1, -1, 1, -1};
-__constant__ int8_t kRingY[8] = {0, 0, 1, -1, 1, -1, -1, 1};
-
-// Cascading ring around a moving centre (the reference's first-improver
-// walk): points are priced against the current centre; at the first
-// improvement the centre moves and the remaining points are re-priced around
-// it, which is the order the reference evaluates them in.
-__device__ __forceinline__ bool cascade_ring(const SearchGeom& g, const MeParamsDev& pr, WarpScratch& ws, int nring,
-                                             int step, int metric, double lam, long long& best_c, int& bx, int& by,
-                                             int& evals) {
-    bool improved = false;
-    int i = 0;
-    while (i < nring) {
-        const int n = nring - i;
-        if (g.lane < n) ws.cand[g.lane] = make_int2(bx + kRingX[i + g.lane] * step, by + kRingY[i + g.lane] * step);
-        __syncwarp();
-        eval_round(g, ws, n, metric);
-        const int cc = lane_cost(pr, ws, g.lane, n, lam);
-        const unsigned hit = __ballot_sync(0xffffffffu, g.lane < n && (long long)cc < best_c);
-        if (hit == 0) {
-            evals += n;
-            __syncwarp();
-            break;
-        }
-        const int j = __ffs(hit) - 1;
-        const int cj = __shfl_sync(0xffffffffu, cc, j);
-        const int2 mv = ws.cand[j];
-        evals += j + 1;
-        best_c = cj;
-        bx = mv.x;
-        by = mv.y;
-        improved = true;
-        i += j + 1;
-        __syncwarp();
-    }
-    return improved;
-}
+// The eight ring points (dx, dy) in the reference's order: (1,0) (-1,0) (0,1)
+// (0,-1) (1,1) (-1,-1) (1,-1) (-1,1); the four-point diamond is the first four.
+// Packed two bits per point as d+1, so a lane computes its point without a
+// memory lookup.
+constexpr uint32_t kRingXP = 0x2252u, kRingYP = 0x8225u;
+__device__ __forceinline__ int ring_dx(int i) { return int((kRingXP >> (2 * i)) & 3u) - 1; }
+__device__ __forceinline__ int ring_dy(int i) { return int((kRingYP >> (2 * i)) & 3u) - 1; }
 
 __device__ __forceinline__ bool in_plane_window(const SearchGeom& g, const WarpScratch& ws, int mvx, int mvy) {
     const int px = g.lx + (mvx >> 2) + ws.pad, py = g.ly + (mvy >> 2) + ws.pad;
     return px >= 0 && py >= 0 && px + ws.rw + 1 <= ws.pw && py + ws.rh + 1 <= ws.ph;
 }
 
+// dist + λ·rate of candidate i as the reference's i64 (every lane the same value).
+__device__ __forceinline__ long long cand_cost64(const MeParamsDev& pr, const WarpScratch& ws, int i, double lam) {
+    const int2 mv = ws.cand[i];
+    return (long long)ws.dist[i] + lam_cost(lam, rate_of(pr, ws, mv.x, mv.y));
+}
+
+// Search phases and what an evaluation round's results are for.
+constexpr int PH_SEEDS = 0, PH_SNAP = 1, PH_DIA = 2, PH_REPRICE = 3, PH_SUB = 4, PH_DONE = 5;
+constexpr int EV_START = 0, EV_SEEDS = 1, EV_SNAP = 2, EV_FIXED = 3, EV_RING = 4, EV_REPRICE = 5;
+constexpr int LOOP_GUARD = 1 << 20;  // iterations of one rung / sub-pel step
+
 // motion_search (mb16.rs:2433-3302) of the partition in `g` (warp-cooperative,
 // uniform control flow).  preds: npred (x,y) pairs, preds[0] the mvd centre;
 // start: refine-only start MV or nullptr.  Returns the reference's evaluation
 // count in `evals`.
+//
+// The search is written as one loop around a single evaluation round, so the
+// round's code exists once per kernel: each iteration plans the next batch of
+// candidates from the phase state (seeds, integer snap, diamond ladder, B2
+// reprice, sub-pel rings), prices it, and folds the result back into the state.
+//  * fixed-centre batches (the FC diamond, sp_fc rings) price all points and
+//    take the first strict minimum, like the reference's argmin loops;
+//  * cascading rings (the centre moves mid-ring) price the remaining points
+//    against the current centre; at the first improvement the centre moves and
+//    the points after it are priced again around the new centre, which is the
+//    order in which the reference evaluates them.
 __device__ __forceinline__ void motion_search_warp(const SearchGeom& g, const MeParamsDev& pr, WarpScratch& ws,
                                                    const int* preds, int npred, const int* start, double lambda_me,
                                                    int& out_x, int& out_y, long long& out_c, int& evals) {
@@ -288,156 +266,237 @@ __device__ __forceinline__ void motion_search_warp(const SearchGeom& g, const Me
         ws.lam_r = pr.kind != 0 ? lambda_me * 0.25 : lambda_me;
         ws.lam_fp = lambda_me * (sadfp ? pr.sadfp_lambda : 1.0);
     }
+    if (g.lane >= 1 && g.lane <= npred && !refine_only)
+        ws.cand[g.lane] = make_int2(preds[2 * (g.lane - 1)], preds[2 * (g.lane - 1) + 1]);
     __syncwarp();
     const int m_fp = sadfp ? MET_SAD : m_main;
-#define L_FP (sadfp ? ws.lam_fp : ws.lam_r)  // cost_fp's λ (cost's λ when B2 is off)
+    const double l_fp = sadfp ? ws.lam_fp : ws.lam_r;  // cost_fp's λ (cost's λ when B2 is off)
+    const int rw = ws.rw, rh = ws.rh;
+    const bool x4shape = (rw == 16 || rw == 8) && (rh == 16 || rh == 8);
+    const bool fc = !pr.fast && pr.fc && x4shape;
+    const uint32_t dmask = pr.fast ? 0u : ((rw < 8 || rh < 8) ? pr.dia_sub_mask : pr.dia_mask);
+    const int spat = pr.subpel_pat >= 0 ? pr.subpel_pat : ((rw < 8 || rh < 8) ? pr.sub_pat : (pr.sp_single_pass ? 2 : 0));
+    const bool sp_fc = pr.sp_fc && !pr.fast && x4shape;
+    const int sp_nring = (spat & 1) ? 4 : 8;
+
     evals = 0;
-    int bx = 0, by = 0;
-    long long best_c, bc;
-    // ---- seeds (mb16.rs:2580-2596) ----
-    if (refine_only) {
-        bx = start[0]; by = start[1];
-        if (g.lane == 0) ws.cand[0] = make_int2(bx, by);
-        __syncwarp();
-        eval_round(g, ws, 1, m_main);
-        best_c = (long long)ws.dist[0] + lam_cost(ws.lam_r, rate_of(pr, ws, bx, by));
-        evals += 1;
-        __syncwarp();
-    } else {
-        if (g.lane == 0) ws.cand[0] = make_int2(0, 0);
-        if (g.lane >= 1 && g.lane <= npred)
-            ws.cand[g.lane] = make_int2(preds[2 * (g.lane - 1)], preds[2 * (g.lane - 1) + 1]);
-        __syncwarp();
-        eval_round(g, ws, npred + 1, m_fp);
-        const int cc = lane_cost(pr, ws, g.lane, npred + 1, L_FP);
-        // sequential strict-< scan: (0,0) first, then the predictors in order
-        best_c = __shfl_sync(0xffffffffu, cc, 0);
-        for (int i = 1; i <= npred; i++) {
-            const long long ci = __shfl_sync(0xffffffffu, cc, i);
-            if (ci < best_c) {
-                best_c = ci;
-                bx = ws.cand[i].x;
-                by = ws.cand[i].y;
-            }
-        }
-        evals += npred + 1;
-        __syncwarp();
-    }
-    const int seed_x = bx, seed_y = by;
-    long long seed_c = best_c;
-    // ---- integer snap (mb16.rs:2597-2607) ----
-    if (!refine_only && pr.me_snap && ((bx & 3) != 0 || (by & 3) != 0)) {
-        const int sx = ((bx + 2) >> 2) * 4, sy = ((by + 2) >> 2) * 4;
-        if (g.lane == 0) ws.cand[0] = make_int2(sx, sy);
-        __syncwarp();
-        eval_round(g, ws, 1, m_fp);
-        best_c = (long long)ws.dist[0] + lam_cost(L_FP, rate_of(pr, ws, sx, sy));
-        evals += 1;
-        bx = sx; by = sy;
-        __syncwarp();
-    }
-    // ---- diamond ladder (mb16.rs:2616-2727) ----
-    if (!refine_only) {
-        const int rw = ws.rw, rh = ws.rh;
-        const bool x4shape = (rw == 16 || rw == 8) && (rh == 16 || rh == 8);
-        const bool fc = !pr.fast && pr.fc && x4shape;
-        const uint32_t mask = pr.fast ? 0u : ((rw < 8 || rh < 8) ? pr.dia_sub_mask : pr.dia_mask);
-        for (int si = 0; si < 5; si++) {
-            int step;
-            if (pr.fast) {
-                if (si >= 2) break;
-                step = si == 0 ? 16 : 4;
-            } else {
-                if (!(mask & (1u << si))) continue;
-                step = 64 >> si;  // rungs [64,32,16,8,4] quarter-pel
-            }
-            for (int guard = 0; guard < (1 << 20); guard++) {
+    int bx = 0, by = 0, seed_x = 0, seed_y = 0;
+    long long best_c = 0, seed_c = 0;
+    int phase = PH_SEEDS;
+    int si = -1;        // diamond rung, -1 before the first
+    int sk = -1;        // sub-pel step index (0: step 2, 1: step 1), -1 before the first
+    int loops = 0;      // iterations of the current rung / sub-pel step
+    int iter = 0;       // sub-pel iterations of the current step
+    int step = 0;
+    bool ring_open = false, ring_improved = false;  // a cascading ring in progress
+    int ring_i = 0, ring_n = 0;
+    for (;;) {
+        // ---------- plan the next round ----------
+        int kind = -1, n = 0, metric = m_main;
+        double lam = ws.lam_r;
+        while (kind < 0 && phase != PH_DONE) {
+            if (phase == PH_SEEDS) {
+                // seeds (mb16.rs:2580-2596): the start MV, or (0,0) then the predictors
+                if (refine_only) {
+                    bx = start[0]; by = start[1];
+                    if (g.lane == 0) ws.cand[0] = make_int2(bx, by);
+                    kind = EV_START; n = 1; metric = m_main; lam = ws.lam_r;
+                } else {
+                    if (g.lane == 0) ws.cand[0] = make_int2(0, 0);
+                    kind = EV_SEEDS; n = npred + 1; metric = m_fp; lam = l_fp;
+                }
+            } else if (phase == PH_SNAP) {
+                // integer snap (mb16.rs:2597-2607)
+                if (!refine_only && pr.me_snap && ((bx & 3) != 0 || (by & 3) != 0)) {
+                    if (g.lane == 0) ws.cand[0] = make_int2(((bx + 2) >> 2) * 4, ((by + 2) >> 2) * 4);
+                    kind = EV_SNAP; n = 1; metric = m_fp; lam = l_fp;
+                } else {
+                    phase = PH_DIA;
+                }
+            } else if (phase == PH_DIA) {
+                // diamond ladder (mb16.rs:2616-2727)
+                if (ring_open) {
+                    kind = EV_RING; n = ring_n - ring_i; metric = m_fp; lam = l_fp;
+                    if (g.lane < n)
+                        ws.cand[g.lane] = make_int2(bx + ring_dx(ring_i + g.lane) * step, by + ring_dy(ring_i + g.lane) * step);
+                    break;
+                }
+                if (si < 0 || loops >= LOOP_GUARD) {
+                    // next enabled rung
+                    int nsi = si + 1;
+                    if (pr.fast) nsi = nsi >= 2 ? 5 : nsi;
+                    else
+                        while (nsi < 5 && !(dmask & (1u << nsi))) nsi++;
+                    if (nsi >= 5) {
+                        phase = PH_REPRICE;
+                        continue;
+                    }
+                    si = nsi;
+                    step = pr.fast ? (si == 0 ? 16 : 4) : (64 >> si);  // rungs [64,32,16,8,4] quarter-pel
+                    loops = 0;
+                }
+                loops++;
+                bool fixed = false;
                 if (fc && (bx & 3) == 0 && (by & 3) == 0) {
                     const int st = step >> 2;
                     const int px = g.lx + (bx >> 2), py = g.ly + (by >> 2);
-                    if (px - st >= 0 && py - st >= 0 && px + st + rw <= ws.cw && py + st + rh <= ws.ch) {
-                        if (g.lane < 4) ws.cand[g.lane] = make_int2(bx + kRingX[g.lane] * step, by + kRingY[g.lane] * step);
-                        __syncwarp();
-                        // 16-wide: sad_x4 / satd_x4 batch priced with lam_fp (mb16.rs:2676-2690);
-                        // 8-wide shapes price each point with cost_fp (mb16.rs:2691)
-                        const int bi = rw == 16
-                                           ? fixed_batch(g, pr, ws, 4, sadfp ? MET_SAD : MET_SATD, ws.lam_fp, best_c, bc, evals)
-                                           : fixed_batch(g, pr, ws, 4, m_fp, L_FP, best_c, bc, evals);
-                        if (bi < 0) break;
-                        best_c = bc;
-                        bx += kRingX[bi] * step;
-                        by += kRingY[bi] * step;
+                    fixed = px - st >= 0 && py - st >= 0 && px + st + rw <= ws.cw && py + st + rh <= ws.ch;
+                }
+                if (g.lane < 4) ws.cand[g.lane] = make_int2(bx + ring_dx(g.lane) * step, by + ring_dy(g.lane) * step);
+                if (fixed) {
+                    // 16-wide: sad_x4 / satd_x4 batch priced with lam_fp (mb16.rs:2676-2690);
+                    // 8-wide shapes price each point with cost_fp (mb16.rs:2691)
+                    kind = EV_FIXED; n = 4;
+                    metric = rw == 16 ? (sadfp ? MET_SAD : MET_SATD) : m_fp;
+                    lam = rw == 16 ? ws.lam_fp : l_fp;
+                } else {
+                    ring_open = true; ring_improved = false; ring_i = 0; ring_n = 4;
+                    kind = EV_RING; n = 4; metric = m_fp; lam = l_fp;
+                }
+            } else if (phase == PH_REPRICE) {
+                // B2 reprice into the SATD domain (mb16.rs:2744-2747)
+                if (sadfp) {
+                    if (g.lane == 0) {
+                        ws.cand[0] = make_int2(bx, by);
+                        ws.cand[1] = make_int2(seed_x, seed_y);
+                    }
+                    kind = EV_REPRICE; n = 2; metric = m_main; lam = ws.lam_r;
+                } else {
+                    phase = PH_SUB;
+                }
+            } else {  // PH_SUB: sub-pel rings (mb16.rs:2956-3283)
+                if (ring_open) {
+                    kind = EV_RING; n = ring_n - ring_i; metric = m_main; lam = ws.lam_r;
+                    if (g.lane < n)
+                        ws.cand[g.lane] = make_int2(bx + ring_dx(ring_i + g.lane) * step, by + ring_dy(ring_i + g.lane) * step);
+                    break;
+                }
+                if (!pr.subpel) {
+                    phase = PH_DONE;
+                    continue;
+                }
+                if (sk < 0 || loops >= LOOP_GUARD) {
+                    if (++sk >= 2) {
+                        phase = PH_DONE;
                         continue;
                     }
+                    step = sk == 0 ? 2 : 1;
+                    loops = 0;
+                    iter = 0;
                 }
-                if (!cascade_ring(g, pr, ws, 4, step, m_fp, L_FP, best_c, bx, by, evals)) break;
-            }
-        }
-    }
-    // ---- B2 reprice into the SATD domain (mb16.rs:2744-2747) ----
-    if (sadfp) {
-        if (g.lane == 0) {
-            ws.cand[0] = make_int2(bx, by);
-            ws.cand[1] = make_int2(seed_x, seed_y);
-        }
-        __syncwarp();
-        eval_round(g, ws, 2, m_main);
-        best_c = (long long)ws.dist[0] + lam_cost(ws.lam_r, rate_of(pr, ws, bx, by));
-        seed_c = (long long)ws.dist[1] + lam_cost(ws.lam_r, rate_of(pr, ws, seed_x, seed_y));
-        evals += 2;
-        __syncwarp();
-    }
-    // ---- sub-pel rings (mb16.rs:2956-3283) ----
-    if (pr.subpel) {
-        const int rw = ws.rw, rh = ws.rh;
-        const bool sub_shape = rw < 8 || rh < 8;
-        const int pat = pr.subpel_pat >= 0 ? pr.subpel_pat : (sub_shape ? pr.sub_pat : (pr.sp_single_pass ? 2 : 0));
-        const bool x4shape = (rw == 16 || rw == 8) && (rh == 16 || rh == 8);
-        const bool sp_fc = pr.sp_fc && !pr.fast && x4shape;
-        const int nring = (pat & 1) ? 4 : 8;
-        for (int k = 0; k < 2; k++) {
-            const int step = k == 0 ? 2 : 1;
-            int iter = 0;
-            for (int guard = 0; guard < (1 << 20); guard++) {
-                if (sp_fc && (pat & 1) == 0 && (step == 1 || ((bx & 3) == 0 && (by & 3) == 0))) {
-                    iter++;
+                loops++;
+                if (sp_fc && (spat & 1) == 0 && (step == 1 || ((bx & 3) == 0 && (by & 3) == 0))) {
                     // hpel_qpel_refs / hpel_ref resolve every ring point (inter.rs:1015, 1060):
                     // inside the +1-slack window, and at step 1 a quarter phase
                     bool all = true;
                     for (int i = 0; i < 8; i++) {
-                        const int qx = bx + kRingX[i] * step, qy = by + kRingY[i] * step;
+                        const int qx = bx + ring_dx(i) * step, qy = by + ring_dy(i) * step;
                         all = all && in_plane_window(g, ws, qx, qy) && (step == 2 || ((qx | qy) & 1));
                     }
                     if (all) {
-                        if (g.lane < 8) ws.cand[g.lane] = make_int2(bx + kRingX[g.lane] * step, by + kRingY[g.lane] * step);
-                        __syncwarp();
+                        iter++;
+                        if (g.lane < 8)
+                            ws.cand[g.lane] = make_int2(bx + ring_dx(g.lane) * step, by + ring_dy(g.lane) * step);
                         // 16-wide: satd_avg_x4 / satd_x4p priced with lambda_me; 8-wide: cost()
-                        const int bi = rw == 16 ? fixed_batch(g, pr, ws, 8, MET_SATD, ws.lam_me, best_c, bc, evals)
-                                                : fixed_batch(g, pr, ws, 8, m_main, ws.lam_r, best_c, bc, evals);
-                        const bool stop =
-                            bi < 0 || !pr.me_subpel_iter || (pat & 2) || (pr.sp_maxit != 0 && iter >= pr.sp_maxit);
-                        if (bi >= 0) {
-                            best_c = bc;
-                            bx += kRingX[bi] * step;
-                            by += kRingY[bi] * step;
-                        }
-                        if (stop) break;
-                        continue;
+                        kind = EV_FIXED; n = 8;
+                        metric = rw == 16 ? MET_SATD : m_main;
+                        lam = rw == 16 ? ws.lam_me : ws.lam_r;
+                        break;
                     }
-                    iter--;
                 }
                 iter++;
-                const bool improved = cascade_ring(g, pr, ws, nring, step, m_main, ws.lam_r, best_c, bx, by, evals);
-                if (!improved || !pr.me_subpel_iter || (pat & 2) || (pr.sp_maxit != 0 && iter >= pr.sp_maxit)) break;
+                if (g.lane < sp_nring)
+                    ws.cand[g.lane] = make_int2(bx + ring_dx(g.lane) * step, by + ring_dy(g.lane) * step);
+                ring_open = true; ring_improved = false; ring_i = 0; ring_n = sp_nring;
+                kind = EV_RING; n = sp_nring; metric = m_main; lam = ws.lam_r;
             }
         }
+        if (kind < 0) break;
+        __syncwarp();
+
+        // ---------- price the round ----------
+        eval_round(g, ws, n, metric);
+        const int cc = lane_cost(pr, ws, g.lane, n, lam);
+
+        // ---------- fold the result into the state ----------
+        if (kind == EV_START) {
+            best_c = cand_cost64(pr, ws, 0, lam);
+            evals += 1;
+            seed_x = bx; seed_y = by; seed_c = best_c;
+            phase = PH_REPRICE;  // refine-only: no snap, no ladder, no B2 reprice; on to the sub-pel rings
+        } else if (kind == EV_SEEDS) {
+            // sequential strict-< scan: (0,0) first, then the predictors in order
+            best_c = __shfl_sync(0xffffffffu, cc, 0);
+            bx = 0; by = 0;
+            for (int i = 1; i < n; i++) {
+                const long long ci = __shfl_sync(0xffffffffu, cc, i);
+                if (ci < best_c) {
+                    best_c = ci;
+                    bx = ws.cand[i].x;
+                    by = ws.cand[i].y;
+                }
+            }
+            evals += n;
+            seed_x = bx; seed_y = by; seed_c = best_c;
+            phase = PH_SNAP;
+        } else if (kind == EV_SNAP) {
+            bx = ws.cand[0].x; by = ws.cand[0].y;
+            best_c = cand_cost64(pr, ws, 0, lam);
+            evals += 1;
+            phase = PH_DIA;
+        } else if (kind == EV_REPRICE) {
+            best_c = cand_cost64(pr, ws, 0, lam);
+            seed_c = cand_cost64(pr, ws, 1, lam);
+            evals += 2;
+            phase = PH_SUB;
+        } else if (kind == EV_FIXED) {
+            const int m = __reduce_min_sync(0xffffffffu, cc);
+            const unsigned at = __ballot_sync(0xffffffffu, cc == m);
+            evals += n;
+            const int bi = (long long)m < best_c ? __ffs(at) - 1 : -1;
+            if (bi >= 0) {
+                best_c = m;
+                bx += ring_dx(bi) * step;
+                by += ring_dy(bi) * step;
+            }
+            if (phase == PH_DIA) {
+                if (bi < 0) loops = LOOP_GUARD;  // rung done
+            } else {
+                const bool stop = bi < 0 || !pr.me_subpel_iter || (spat & 2) || (pr.sp_maxit != 0 && iter >= pr.sp_maxit);
+                if (stop) loops = LOOP_GUARD;  // step done
+            }
+        } else {  // EV_RING
+            const unsigned hit = __ballot_sync(0xffffffffu, g.lane < n && (long long)cc < best_c);
+            if (hit == 0) {
+                evals += n;
+                ring_open = false;
+            } else {
+                const int j = __ffs(hit) - 1;
+                best_c = __shfl_sync(0xffffffffu, cc, j);
+                const int2 mv = ws.cand[j];
+                evals += j + 1;
+                bx = mv.x;
+                by = mv.y;
+                ring_improved = true;
+                ring_i += j + 1;
+                ring_open = ring_i < ring_n;
+            }
+            if (!ring_open) {
+                if (phase == PH_DIA) {
+                    if (!ring_improved) loops = LOOP_GUARD;  // rung done
+                } else if (!ring_improved || !pr.me_subpel_iter || (spat & 2) ||
+                           (pr.sp_maxit != 0 && iter >= pr.sp_maxit)) {
+                    loops = LOOP_GUARD;  // step done
+                }
+            }
+        }
+        __syncwarp();
     }
     // ---- seed restore (mb16.rs:3297-3300) ----
     if (pr.me_snap && seed_c < best_c) {
         bx = seed_x; by = seed_y; best_c = seed_c;
     }
     out_x = bx; out_y = by; out_c = best_c;
-#undef L_FP
 }
 
 __device__ __forceinline__ bool job_shape_ok(int w, int h) {
