@@ -506,7 +506,7 @@ __device__ __forceinline__ bool job_shape_ok(int w, int h) {
 
 constexpr int ME_WARPS = 4;
 #ifndef ME_MIN_BLOCKS
-#define ME_MIN_BLOCKS 3
+#define ME_MIN_BLOCKS 4
 #endif
 
 __global__ void __launch_bounds__(32 * ME_WARPS) me_search_kernel(const h264a_picture* __restrict__ pics, int npics,
