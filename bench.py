@@ -147,6 +147,47 @@ def cpu_baseline(frames: np.ndarray, nthreads: int, lam: float, gate: int):
     return frames.shape[0] * W * H / dt / 1e6, dt
 
 
+def cpu_model() -> dict:
+    """Host CPU model name and online core count (stated with every CPU number)."""
+    model = "unknown"
+    try:
+        for ln in open("/proc/cpuinfo"):
+            if ln.startswith("model name"):
+                model = ln.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return {"model": model, "nproc": os.cpu_count()}
+
+
+def cpu_stages(frames: np.ndarray, lam: float, gate: int) -> dict:
+    """Per-stage time of the CPU restatement on one thread over `frames`
+    (planes of the n-1 references, plain-ME and MC+T/Q of the n-1 P frames,
+    HalfRes lookahead of all n), in ms per frame and Mpx/s."""
+    from oracle import oracle as O
+
+    n = frames.shape[0]
+    params = O.balanced_params()
+    t = {}
+    t0 = time.perf_counter()
+    planes = [O.build_planes4(frames[i], 32) for i in range(n - 1)]
+    t["planes"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    picks = [O.me_frame(frames[i], frames[i - 1], planes[i - 1], params, lam, gate)[0] for i in range(1, n)]
+    t["me"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    for i in range(1, n):
+        O.mc_tq_frame(frames[i], frames[i - 1], picks[i - 1], QP)
+    t["tq"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    O.lookahead_clip(frames, mode=2, nthreads=1)
+    t["la"] = time.perf_counter() - t0
+    out = {k: {"ms_per_frame": round(v * 1e3 / n, 3), "mpx_s": round(n * W * H / v / 1e6, 3)} for k, v in t.items()}
+    tot = sum(t.values())
+    out["total"] = {"ms_per_frame": round(tot * 1e3 / n, 3), "mpx_s": round(n * W * H / tot / 1e6, 3)}
+    return out
+
+
 def run_reference(args, ws, rank):
     if rank != 0:
         return
@@ -174,7 +215,8 @@ def run_reference(args, ws, rank):
         "config": {"workload": "1080p 60-frame clip, pixel path (planes, plain-ME, MC+T/Q, HalfRes lookahead)",
                    "sample_frames_per_step": sample, "qp": QP},
         "cpu_baseline": {"value": round(value, 3), "unit": "Mpx/s", "cores": nthreads, "kind": "port",
-                         "sample": f"{sample} frames of the 1080p clip per step"},
+                         "sample": f"{sample} frames of the 1080p clip per step, frames split over the threads",
+                         "cpu": cpu_model()},
         "e2e": {"value": round(value, 3), "unit": "Mpx/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -351,9 +393,11 @@ def run_ours(args, ws, rank, local):
         # the host path and the device-resident path must agree
         assert np.array_equal(outs_np["coeffs"], coeffs.cpu().numpy())
     if rank == 0 and ws == 1 and not args.no_cpu:
-        v, dt = cpu_baseline(np.ascontiguousarray(f[:3]), 1, lam, gate)
+        sample = np.ascontiguousarray(f[:3])
+        v, dt = cpu_baseline(sample, 1, lam, gate)
         line["cpu_baseline"] = {"value": round(v, 3), "unit": "Mpx/s", "cores": 1, "kind": "port",
-                                "sample": "3 frames of the 1080p clip (2 P frames + lookahead), one thread"}
+                                "sample": "3 frames of the 1080p clip (2 P frames + lookahead), one thread",
+                                "cpu": cpu_model(), "stages": cpu_stages(sample, lam, gate)}
     if rank == 0:
         print(json.dumps(line), flush=True)
     acc.close()
