@@ -340,10 +340,10 @@ def run_ours(args, ws, rank, local):
         "kernel": "me_frames_kernel (persistent plain-ME)", "bound": "int32", "achieved": round(achieved, 1),
         "peak": round(int32_peak, 1), "unit": "Gop/s", "frac": round(achieved / int32_peak, 4),
         "peak_source": "measured live by h264a_measure_int32_peak (INT32 is not in MEASURED_PEAKS.json)",
-        # dram__bytes_read.sum + dram__bytes_write.sum of one launch (ncu, 16-frame batch of
-        # 122,400 MBs: 180.08 MB), scaled by MBs to this launch
-        "traffic": int(180.08e6 / 122400 * (n - 1) * nmb),
-        "traffic_source": "ncu capture of a 16-frame 1080p launch, scaled by macroblocks",
+        # dram__bytes_read.sum + dram__bytes_write.sum of one launch (ncu --set full of the
+        # 60-frame step: 481,440 MBs, 1151.9 MB + 35.5 MB), scaled by MBs to this launch
+        "traffic": int(1187.4e6 / 481440 * (n - 1) * nmb),
+        "traffic_source": "ncu capture of the 60-frame 1080p launch, scaled by macroblocks",
         "work": {"satd_4x4_evals_per_step": work4x4, "ops_per_4x4": SATD_OPS_PER_4X4},
         "hpel_kernel": {"bound": "hbm", "achieved_gbs": round(hpel_bytes / (stage["hpel"] * 1e-3) / 1e9, 1),
                         "peak_gbs": hbm_peak, "frac": round(hpel_bytes / (stage["hpel"] * 1e-3) / 1e9 / hbm_peak, 4),
