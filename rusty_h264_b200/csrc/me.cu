@@ -50,16 +50,15 @@ struct WarpScratch {
 // the bulk-copy (TMA) engine: WIN_H rows of WIN_W bytes per plane, every
 // search of the MB (16x16 and its partitions) then reads its candidates from
 // shared memory.  Candidates whose reads leave the window take the plane path
-// (pred_rows), which gives the same bytes.  32 bytes of padding follow every
-// fourth row, so the rows that one candidate's 16 lanes read together (four
-// apart) land in four different 8-bank groups.
-constexpr int WIN_W = 64, WIN_H = 44;
-constexpr int WIN_PLANE = WIN_H * WIN_W + (WIN_H / 4) * 32;  // bytes per plane (a multiple of 16)
+// (pred_rows), which gives the same bytes.  Rows are WIN_STRIDE = 80 bytes
+// apart: a block's four rows are then load-immediate offsets of its first, and
+// the rows one candidate's 16 lanes read together (four apart) fall in at most
+// two lanes per bank.
+constexpr int WIN_W = 64, WIN_H = 42, WIN_STRIDE = 80;
+constexpr int WIN_PLANE = WIN_H * WIN_STRIDE;  // bytes per plane (a multiple of 16)
 constexpr int WIN_BYTES = 4 * WIN_PLANE;
 constexpr int WIN_R = 12;  // the window starts this far up/left of the predicted position
 constexpr int WIN_OFF = -(1 << 30);  // window offset of a search without one: below -2^29 for any MV, so every read misses
-
-__device__ __forceinline__ int win_row(int y) { return y * WIN_W + ((y >> 2) << 5); }
 
 __device__ __forceinline__ uint32_t lds_u32(uint32_t addr) {
     uint32_t v;
@@ -74,22 +73,17 @@ __device__ __forceinline__ void win_rows(uint32_t win, int wx, int wy, int fx, i
     const uint32_t pb = phase_bits(fx, fy);
     const int pa = int(pb & 3), pbb = int((pb >> 2) & 3);
     const int xa = wx + int((pb >> 4) & 1), ya = wy + int((pb >> 5) & 1);
-    const uint32_t a = win + uint32_t(pa * WIN_PLANE + (xa & ~3));
+    const uint32_t a = win + uint32_t(pa * WIN_PLANE + ya * WIN_STRIDE + (xa & ~3));
     const uint32_t sha = uint32_t(xa & 3) * 8u;
 #pragma unroll
-    for (int r = 0; r < 4; r++) {
-        const uint32_t ar = a + uint32_t(win_row(ya + r));
-        out[r] = __funnelshift_r(lds_u32(ar), lds_u32(ar + 4), sha);
-    }
+    for (int r = 0; r < 4; r++) out[r] = __funnelshift_r(lds_u32(a + r * WIN_STRIDE), lds_u32(a + r * WIN_STRIDE + 4), sha);
     if (pbb != 0) {
         const int xb = wx + int((pb >> 6) & 1), yb = wy + int((pb >> 7) & 1);
-        const uint32_t b = win + uint32_t(pbb * WIN_PLANE + (xb & ~3));
+        const uint32_t b = win + uint32_t(pbb * WIN_PLANE + yb * WIN_STRIDE + (xb & ~3));
         const uint32_t shb = uint32_t(xb & 3) * 8u;
 #pragma unroll
-        for (int r = 0; r < 4; r++) {
-            const uint32_t br = b + uint32_t(win_row(yb + r));
-            out[r] = avg_up4(out[r], __funnelshift_r(lds_u32(br), lds_u32(br + 4), shb));
-        }
+        for (int r = 0; r < 4; r++)
+            out[r] = avg_up4(out[r], __funnelshift_r(lds_u32(b + r * WIN_STRIDE), lds_u32(b + r * WIN_STRIDE + 4), shb));
     }
 }
 
@@ -156,8 +150,6 @@ __device__ __forceinline__ void geom_init(SearchGeom& g, WarpScratch& ws, const 
 __device__ __forceinline__ void eval_round(const SearchGeom& g, WarpScratch& ws, int n, int metric) {
     const int nb = 1 << g.lg_nb;
     const int npass = ((n << g.lg_nb) + 31) >> 5;
-    Planes P;
-    P.base = ws.base; P.pw = ws.pw; P.ph = ws.ph; P.pad = ws.pad; P.ps = (long long)ws.pw * ws.ph;
     for (int k0 = 0; k0 < npass; k0 += ME_MAX_PASS) {
     uint32_t pr4[ME_MAX_PASS][4];
 #pragma unroll
@@ -168,10 +160,13 @@ __device__ __forceinline__ void eval_round(const SearchGeom& g, WarpScratch& ws,
             const int2 mv = ws.cand[c];
             const int dx = mv.x >> 2, dy = mv.y >> 2;
             const int wx = g.wox + dx, wy = g.woy + dy;
-            if (win_covers(wx, wy))
+            if (win_covers(wx, wy)) {
                 win_rows(g.win, wx, wy, mv.x & 3, mv.y & 3, pr4[kk]);
-            else
+            } else {
+                Planes P;
+                P.base = ws.base; P.pw = ws.pw; P.ph = ws.ph; P.pad = ws.pad; P.ps = (long long)ws.pw * ws.ph;
                 pred_rows(P, g.lx + g.bxo + dx, g.ly + g.byo + dy, mv.x & 3, mv.y & 3, pr4[kk]);
+            }
         }
     }
 #pragma unroll
@@ -751,7 +746,7 @@ __global__ void __launch_bounds__(32 * ME_WARPS, ME_MIN_BLOCKS) me_frames_kernel
             const long long ps = (long long)pw * ph;
             for (int i = lane; i < 4 * WIN_H; i += 32) {
                 const int pl = i / WIN_H, r = i - pl * WIN_H;
-                bulk_g2s(win + uint32_t(pl * WIN_PLANE + win_row(r)),
+                bulk_g2s(win + uint32_t(pl * WIN_PLANE + r * WIN_STRIDE),
                          pc.d_planes + ps * pl + (long long)(wy0 + r) * pw + wx0, WIN_W, bar);
             }
         }
