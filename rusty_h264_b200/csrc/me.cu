@@ -233,6 +233,19 @@ constexpr int PH_SEEDS = 0, PH_SNAP = 1, PH_DIA = 2, PH_REPRICE = 3, PH_SUB = 4,
 constexpr int EV_START = 0, EV_SEEDS = 1, EV_SNAP = 2, EV_FIXED = 3, EV_RING = 4, EV_REPRICE = 5;
 constexpr int LOOP_GUARD = 1 << 20;  // iterations of one rung / sub-pel step
 
+// Points of a cascading ring priced per round: the first round prices
+// RING_FIRST of them, later rounds (after the centre moved) up to RING_REST.
+// A ring of eight sub-pel points usually improves once or twice, mostly
+// early, so pricing only the first four up front wastes fewer evaluations
+// on points the walk never reaches from the old centre; the order of the
+// walk and its result do not depend on these sizes.
+#ifndef RING_FIRST
+#define RING_FIRST 4
+#endif
+#ifndef RING_REST
+#define RING_REST 8
+#endif
+
 // motion_search (mb16.rs:2433-3302) of the partition in `g` (warp-cooperative,
 // uniform control flow).  preds: npred (x,y) pairs, preds[0] the mvd centre;
 // start: refine-only start MV or nullptr.  Returns the reference's evaluation
@@ -311,7 +324,7 @@ __device__ __forceinline__ void motion_search_warp(const SearchGeom& g, const Me
             } else if (phase == PH_DIA) {
                 // diamond ladder (mb16.rs:2616-2727)
                 if (ring_open) {
-                    kind = EV_RING; n = ring_n - ring_i; metric = m_fp; lam = l_fp;
+                    kind = EV_RING; n = min(ring_n - ring_i, RING_REST); metric = m_fp; lam = l_fp;
                     if (g.lane < n)
                         ws.cand[g.lane] = make_int2(bx + ring_dx(ring_i + g.lane) * step, by + ring_dy(ring_i + g.lane) * step);
                     break;
@@ -361,7 +374,7 @@ __device__ __forceinline__ void motion_search_warp(const SearchGeom& g, const Me
                 }
             } else {  // PH_SUB: sub-pel rings (mb16.rs:2956-3283)
                 if (ring_open) {
-                    kind = EV_RING; n = ring_n - ring_i; metric = m_main; lam = ws.lam_r;
+                    kind = EV_RING; n = min(ring_n - ring_i, RING_REST); metric = m_main; lam = ws.lam_r;
                     if (g.lane < n)
                         ws.cand[g.lane] = make_int2(bx + ring_dx(ring_i + g.lane) * step, by + ring_dy(ring_i + g.lane) * step);
                     break;
@@ -400,10 +413,11 @@ __device__ __forceinline__ void motion_search_warp(const SearchGeom& g, const Me
                     }
                 }
                 iter++;
-                if (g.lane < sp_nring)
+                n = min(sp_nring, RING_FIRST);
+                if (g.lane < n)
                     ws.cand[g.lane] = make_int2(bx + ring_dx(g.lane) * step, by + ring_dy(g.lane) * step);
                 ring_open = true; ring_improved = false; ring_i = 0; ring_n = sp_nring;
-                kind = EV_RING; n = sp_nring; metric = m_main; lam = ws.lam_r;
+                kind = EV_RING; metric = m_main; lam = ws.lam_r;
             }
         }
         if (kind < 0) break;
@@ -464,7 +478,8 @@ __device__ __forceinline__ void motion_search_warp(const SearchGeom& g, const Me
             const unsigned hit = __ballot_sync(0xffffffffu, g.lane < n && (long long)cc < best_c);
             if (hit == 0) {
                 evals += n;
-                ring_open = false;
+                ring_i += n;
+                ring_open = ring_i < ring_n;  // the rest of the ring, around the same centre
             } else {
                 const int j = __ffs(hit) - 1;
                 best_c = __shfl_sync(0xffffffffu, cc, j);
