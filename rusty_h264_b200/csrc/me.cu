@@ -229,8 +229,8 @@ __device__ __forceinline__ long long cand_cost64(const MeParamsDev& pr, const Wa
 }
 
 // Search phases and what an evaluation round's results are for.
-constexpr int PH_SEEDS = 0, PH_SNAP = 1, PH_DIA = 2, PH_REPRICE = 3, PH_SUB = 4, PH_DONE = 5;
-constexpr int EV_START = 0, EV_SEEDS = 1, EV_SNAP = 2, EV_FIXED = 3, EV_RING = 4, EV_REPRICE = 5;
+constexpr int PH_SEEDS = 0, PH_DIA = 2, PH_REPRICE = 3, PH_SUB = 4, PH_DONE = 5;
+constexpr int EV_START = 0, EV_SEEDS = 1, EV_FIXED = 3, EV_RING = 4, EV_REPRICE = 5;
 constexpr int LOOP_GUARD = 1 << 20;  // iterations of one rung / sub-pel step
 
 // Points of a cascading ring priced per round: the first round prices
@@ -253,8 +253,9 @@ constexpr int LOOP_GUARD = 1 << 20;  // iterations of one rung / sub-pel step
 //
 // The search is written as one loop around a single evaluation round, so the
 // round's code exists once per kernel: each iteration plans the next batch of
-// candidates from the phase state (seeds, integer snap, diamond ladder, B2
-// reprice, sub-pel rings), prices it, and folds the result back into the state.
+// candidates from the phase state (seeds together with the snaps of sub-pel
+// predictors, diamond ladder, B2 reprice, sub-pel rings), prices it, and folds
+// the result back into the state.
 //  * fixed-centre batches (the FC diamond, sp_fc rings) price all points and
 //    take the first strict minimum, like the reference's argmin loops;
 //  * cascading rings (the centre moves mid-ring) price the remaining points
@@ -274,8 +275,23 @@ __device__ __forceinline__ void motion_search_warp(const SearchGeom& g, const Me
         ws.lam_r = pr.kind != 0 ? lambda_me * 0.25 : lambda_me;
         ws.lam_fp = lambda_me * (sadfp ? pr.sadfp_lambda : 1.0);
     }
-    if (g.lane >= 1 && g.lane <= npred && !refine_only)
-        ws.cand[g.lane] = make_int2(preds[2 * (g.lane - 1)], preds[2 * (g.lane - 1) + 1]);
+    // Seeds in ws.cand[0..npred]; with the integer snap on, the snapped
+    // position of every sub-pel predictor follows them, so the snap
+    // (mb16.rs:2597-2607) is priced in the seed round: slot npred+1+k holds the
+    // snap of the k-th sub-pel predictor (bit i of `snaps` set for predictor i).
+    unsigned snaps = 0u;
+    if (!refine_only) {
+        int qx = 0, qy = 0;
+        const bool mine = g.lane >= 1 && g.lane <= npred;
+        if (mine) {
+            qx = preds[2 * (g.lane - 1)];
+            qy = preds[2 * (g.lane - 1) + 1];
+            ws.cand[g.lane] = make_int2(qx, qy);
+        }
+        snaps = __ballot_sync(0xffffffffu, pr.me_snap && mine && ((qx & 3) != 0 || (qy & 3) != 0));
+        if ((snaps >> g.lane) & 1u)
+            ws.cand[npred + 1 + __popc(snaps & ((1u << g.lane) - 1u))] = make_int2(((qx + 2) >> 2) * 4, ((qy + 2) >> 2) * 4);
+    }
     __syncwarp();
     const int m_fp = sadfp ? MET_SAD : m_main;
     const double l_fp = sadfp ? ws.lam_fp : ws.lam_r;  // cost_fp's λ (cost's λ when B2 is off)
@@ -311,15 +327,7 @@ __device__ __forceinline__ void motion_search_warp(const SearchGeom& g, const Me
                     kind = EV_START; n = 1; metric = m_main; lam = ws.lam_r;
                 } else {
                     if (g.lane == 0) ws.cand[0] = make_int2(0, 0);
-                    kind = EV_SEEDS; n = npred + 1; metric = m_fp; lam = l_fp;
-                }
-            } else if (phase == PH_SNAP) {
-                // integer snap (mb16.rs:2597-2607)
-                if (!refine_only && pr.me_snap && ((bx & 3) != 0 || (by & 3) != 0)) {
-                    if (g.lane == 0) ws.cand[0] = make_int2(((bx + 2) >> 2) * 4, ((by + 2) >> 2) * 4);
-                    kind = EV_SNAP; n = 1; metric = m_fp; lam = l_fp;
-                } else {
-                    phase = PH_DIA;
+                    kind = EV_SEEDS; n = npred + 1 + __popc(snaps); metric = m_fp; lam = l_fp;
                 }
             } else if (phase == PH_DIA) {
                 // diamond ladder (mb16.rs:2616-2727)
@@ -437,21 +445,25 @@ __device__ __forceinline__ void motion_search_warp(const SearchGeom& g, const Me
             // sequential strict-< scan: (0,0) first, then the predictors in order
             best_c = __shfl_sync(0xffffffffu, cc, 0);
             bx = 0; by = 0;
-            for (int i = 1; i < n; i++) {
+            int wi = 0;
+            for (int i = 1; i <= npred; i++) {
                 const long long ci = __shfl_sync(0xffffffffu, cc, i);
                 if (ci < best_c) {
                     best_c = ci;
                     bx = ws.cand[i].x;
                     by = ws.cand[i].y;
+                    wi = i;
                 }
             }
-            evals += n;
+            evals += npred + 1;
             seed_x = bx; seed_y = by; seed_c = best_c;
-            phase = PH_SNAP;
-        } else if (kind == EV_SNAP) {
-            bx = ws.cand[0].x; by = ws.cand[0].y;
-            best_c = cand_cost64(pr, ws, 0, lam);
-            evals += 1;
+            if ((snaps >> wi) & 1u) {
+                // the winner is a sub-pel predictor: take its snap, priced in this round
+                const int si_ = npred + 1 + __popc(snaps & ((1u << wi) - 1u));
+                bx = ws.cand[si_].x; by = ws.cand[si_].y;
+                best_c = cand_cost64(pr, ws, si_, lam);
+                evals += 1;
+            }
             phase = PH_DIA;
         } else if (kind == EV_REPRICE) {
             best_c = cand_cost64(pr, ws, 0, lam);
