@@ -60,12 +60,6 @@ constexpr int WIN_BYTES = 4 * WIN_PLANE;
 constexpr int WIN_R = 12;  // the window starts this far up/left of the predicted position
 constexpr int WIN_OFF = -(1 << 30);  // window offset of a search without one: below -2^29 for any MV, so every read misses
 
-__device__ __forceinline__ uint32_t lds_u32(uint32_t addr) {
-    uint32_t v;
-    asm volatile("ld.shared.u32 %0, [%1];" : "=r"(v) : "r"(addr));
-    return v;
-}
-
 // Rows of the 4x4 block at window position (wx, wy) (full-pel part of the MV
 // applied) at phase (fx, fy): the same operand table and averaging as
 // pred_rows, read from the staged window at shared address `win`.
