@@ -221,6 +221,16 @@ typedef struct {
     int16_t *d_coeffs;       /* 256 i16 per MB */
 } h264a_tq_frame;
 H264A_API int h264a_mc_tq_frames(h264a_ctx *ctx, const h264a_tq_frame *h_frames, int nframes, void *stream);
+/* h264a_mc_tq_frames plus the inter MB's luma reconstruction of
+ * mb16.rs:3575-3605 (dequantize, transform.rs:233; inverse 4x4 + add + clamp,
+ * idct_four_t4_rec, accel/src/transform_quant.rs:96): d_rec receives the
+ * cw x ch reconstructed luma (4-byte aligned), the next frame's reference
+ * picture, without leaving the device. */
+typedef struct {
+    h264a_tq_frame tq;
+    uint8_t *d_rec;
+} h264a_tq_rec_frame;
+H264A_API int h264a_mc_tq_rec_frames(h264a_ctx *ctx, const h264a_tq_rec_frame *h_frames, int nframes, void *stream);
 
 /* ---- a16-a19: mb-tree lookahead ------------------------------------------ */
 /* downsample2x (encoder/src/mbtree.rs:61-74) of n frames cw x ch -> cw/2 x ch/2. */

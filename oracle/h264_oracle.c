@@ -292,6 +292,87 @@ void or_mb_luma_tq(const uint8_t *src, int ss, const uint8_t *pred16, int qp, in
     for (int qi = 0; qi < 4; qi++) or_quant_four_4x4(out + qi * 64, ff, mf);
 }
 
+/* ---- reconstruction: dequant + inverse 4x4 + add ---------------------------- */
+
+/* NORM_ADJUST (transform.rs:15-22) by qp % 6 and position group; the group of
+ * raster position idx is POS_GROUP_FLAT (transform.rs:48-52): (row, col) both
+ * even -> 0, both odd -> 1, else 2. */
+static const int32_t OR_NORM_ADJUST[6][3] = {{10, 16, 13}, {11, 18, 14}, {13, 20, 16},
+                                             {14, 23, 18}, {16, 25, 20}, {18, 29, 23}};
+static int or_pos_group4(int idx) {
+    int r = (idx >> 2) & 1, c = idx & 1;
+    return (r == 0 && c == 0) ? 0 : ((r == 1 && c == 1) ? 1 : 2);
+}
+
+/* dequantize (transform.rs:233-284), flat scaling list: LevelScale =
+ * 16 * NORM_ADJUST; qp >= 24: (l * ls) << (qp/6 - 4), else
+ * (l * ls + 2^(3 - qp/6)) >> (4 - qp/6). */
+void or_dequant4x4(const int32_t lv[16], int qp, int32_t out[16]) {
+    int m = qp % 6, shift = qp / 6;
+    for (int i = 0; i < 16; i++) {
+        int32_t ls = 16 * OR_NORM_ADJUST[m][or_pos_group4(i)];
+        if (qp >= 24)
+            out[i] = (int32_t)((uint32_t)(lv[i] * ls) << (shift - 4));
+        else
+            out[i] = (lv[i] * ls + (1 << (3 - shift))) >> (4 - shift);
+    }
+}
+
+/* inv_1d + inverse_core (transform_quant.rs:30-35, 56-69): rows first, then
+ * columns, then (x + 32) >> 6. */
+static void or_inv_1d(int32_t d0, int32_t d1, int32_t d2, int32_t d3, int32_t o[4]) {
+    int32_t e0 = d0 + d2, e1 = d0 - d2, e2 = (d1 >> 1) - d3, e3 = d1 + (d3 >> 1);
+    o[0] = e0 + e3; o[1] = e1 + e2; o[2] = e1 - e2; o[3] = e0 - e3;
+}
+void or_inverse_core4(int32_t m[16]) {
+    int32_t o[4];
+    for (int r = 0; r < 4; r++) {
+        or_inv_1d(m[r * 4], m[r * 4 + 1], m[r * 4 + 2], m[r * 4 + 3], o);
+        for (int k = 0; k < 4; k++) m[r * 4 + k] = o[k];
+    }
+    for (int c = 0; c < 4; c++) {
+        or_inv_1d(m[c], m[4 + c], m[8 + c], m[12 + c], o);
+        for (int k = 0; k < 4; k++) m[k * 4 + c] = o[k];
+    }
+    for (int i = 0; i < 16; i++) m[i] = (m[i] + 32) >> 6;
+}
+
+/* idct_four_t4_rec_scalar (transform_quant.rs:96-119): four coefficient
+ * blocks in SUBBLOCKS order, each inverse-transformed and added to pred with
+ * clamping into rec. */
+void or_idct_four_t4_rec(uint8_t *rec, int srec, const uint8_t *pred, int spred, const int16_t dct[64]) {
+    static const int SB[4][2] = {{0, 0}, {4, 0}, {0, 4}, {4, 4}};
+    for (int k = 0; k < 4; k++) {
+        int32_t m[16];
+        for (int i = 0; i < 16; i++) m[i] = dct[k * 16 + i];
+        or_inverse_core4(m);
+        for (int dy = 0; dy < 4; dy++)
+            for (int dx = 0; dx < 4; dx++) {
+                int v = pred[(SB[k][1] + dy) * spred + SB[k][0] + dx] + m[dy * 4 + dx];
+                rec[(SB[k][1] + dy) * srec + SB[k][0] + dx] = (uint8_t)(v < 0 ? 0 : (v > 255 ? 255 : v));
+            }
+    }
+}
+
+/* The inter MB's luma reconstruction (mb16.rs:3575-3605): per 8x8 quad the
+ * levels of its four blocks are dequantized, cast to i16 (the reference's
+ * `deq[i] as i16`), inverse-transformed and added to the 16x16 prediction.
+ * (A quad with no coded block copies the prediction, which is the same bytes:
+ * the inverse of all-zero levels is zero.) */
+void or_mb_luma_rec(uint8_t *rec, int srec, const uint8_t *pred16, const int16_t levels[256], int qp) {
+    static const int Q[4][2] = {{0, 0}, {8, 0}, {0, 8}, {8, 8}};
+    for (int qi = 0; qi < 4; qi++) {
+        int16_t dct_in[64];
+        for (int k = 0; k < 4; k++) {
+            int32_t lv[16], dq[16];
+            for (int i = 0; i < 16; i++) lv[i] = levels[(qi * 4 + k) * 16 + i];
+            or_dequant4x4(lv, qp, dq);
+            for (int i = 0; i < 16; i++) dct_in[k * 16 + i] = (int16_t)dq[i];
+        }
+        or_idct_four_t4_rec(rec + Q[qi][1] * srec + Q[qi][0], srec, pred16 + Q[qi][1] * 16 + Q[qi][0], 16, dct_in);
+    }
+}
+
 /* ======================================================================== */
 /* Inter prediction (crates/rusty_h264-common/src/inter.rs)                 */
 /* ======================================================================== */

@@ -48,6 +48,10 @@ void or_dct_four_t4(int16_t dct[64], const uint8_t *src, int ss, const uint8_t *
 void or_quant_four_4x4(int16_t dct[64], const int16_t ff[8], const int16_t mf[8]);
 /* one macroblock's luma T/Q exactly as mb16.rs:3436-3450 runs it */
 void or_mb_luma_tq(const uint8_t *src, int ss, const uint8_t *pred16, int qp, int dz_div, int16_t out[256]);
+void or_dequant4x4(const int32_t lv[16], int qp, int32_t out[16]);
+void or_inverse_core4(int32_t m[16]);
+void or_idct_four_t4_rec(uint8_t *rec, int srec, const uint8_t *pred, int spred, const int16_t dct[64]);
+void or_mb_luma_rec(uint8_t *rec, int srec, const uint8_t *pred16, const int16_t levels[256], int qp);
 
 /* ---- inter prediction (crates/rusty_h264-common/src/inter.rs) ------------- */
 int32_t or_median3(int32_t a, int32_t b, int32_t c);

@@ -176,6 +176,21 @@ void or_mc_tq_frame(const uint8_t *src, const uint8_t *ref, int cw, int ch, cons
         }
 }
 
+/* MC + luma T/Q and the luma reconstruction of every MB of a frame
+ * (mb16.rs:3436-3450 and 3575-3605): coeffs as or_mc_tq_frame, rec cw x ch. */
+void or_mc_tq_rec_frame(const uint8_t *src, const uint8_t *ref, int cw, int ch, const int32_t *picks, int qp,
+                        int dz_div, int16_t *coeffs, uint8_t *rec) {
+    int mb_w = cw / 16, mb_h = ch / 16;
+    for (int mby = 0; mby < mb_h; mby++)
+        for (int mbx = 0; mbx < mb_w; mbx++) {
+            int m = mby * mb_w + mbx;
+            uint8_t pred[256];
+            mb_pred_for_pick(ref, cw, ch, mbx, mby, picks + 6 * m, pred);
+            or_mb_luma_tq(src + (int64_t)mby * 16 * cw + mbx * 16, cw, pred, qp, dz_div, coeffs + (int64_t)m * 256);
+            or_mb_luma_rec(rec + (int64_t)mby * 16 * cw + mbx * 16, cw, pred, coeffs + (int64_t)m * 256, qp);
+        }
+}
+
 typedef struct {
     const uint8_t *frames;
     uint8_t *half;

@@ -183,6 +183,38 @@ def mc_tq_frame(src, ref, picks, qp, dz_div=6):
     return out
 
 
+def mc_tq_rec_frame(src, ref, picks, qp, dz_div=6):
+    """(coeffs, rec): MC + luma T/Q and the luma reconstruction of a frame."""
+    ch, cw = src.shape
+    nmb = (cw // 16) * (ch // 16)
+    out = np.zeros((nmb, 256), np.int16)
+    rec = np.zeros((ch, cw), np.uint8)
+    lib().or_mc_tq_rec_frame(ptr(src), ptr(ref), cw, ch, ptr(np.ascontiguousarray(picks), i32p), qp, dz_div,
+                             ptr(out, i16p), ptr(rec))
+    return out, rec
+
+
+def dequant4x4(levels, qp) -> np.ndarray:
+    lv = np.ascontiguousarray(levels, np.int32)
+    out = np.zeros(16, np.int32)
+    lib().or_dequant4x4(ptr(lv, i32p), int(qp), ptr(out, i32p))
+    return out
+
+
+def inverse_core4(coeffs) -> np.ndarray:
+    m = np.array(coeffs, np.int32)
+    lib().or_inverse_core4(ptr(m, i32p))
+    return m
+
+
+def idct_four_t4_rec(pred8: np.ndarray, dct64: np.ndarray) -> np.ndarray:
+    """idct_four_t4_rec over an 8x8 region: pred 8x8 u8 (stride 8), 64 i16."""
+    rec = np.zeros((8, 8), np.uint8)
+    lib().or_idct_four_t4_rec(ptr(rec), 8, ptr(np.ascontiguousarray(pred8)), 8,
+                              ptr(np.ascontiguousarray(dct64, np.int16), i16p))
+    return rec
+
+
 def downsample2x(y):
     ch, cw = y.shape
     out = np.empty((ch // 2, cw // 2), np.uint8)

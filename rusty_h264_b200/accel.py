@@ -72,6 +72,10 @@ class TqFrame(C.Structure):
                 ("d_coeffs", C.c_void_p)]
 
 
+class TqRecFrame(C.Structure):
+    _fields_ = [("tq", TqFrame), ("d_rec", C.c_void_p)]
+
+
 # Every entry point the header declares (checked by tests/test_capi_symbols.py).
 EXPORTS = (
     "h264a_version", "h264a_last_error", "h264a_ctx_create", "h264a_ctx_destroy", "h264a_sync",
@@ -80,6 +84,7 @@ EXPORTS = (
     "h264a_me_search", "h264a_me_frames", "h264a_fullpel_grid", "h264a_dct_quant_4x4", "h264a_dct_quant_8x8",
     "h264a_mc_tq_frames", "h264a_downsample2x", "h264a_lookahead_costs", "h264a_pixel_path_host",
     "h264a_selftest_bounded_wait", "h264a_measure_int32_peak", "h264a_me_frames_noalloc",
+    "h264a_mc_tq_rec_frames",
 )
 
 _lib = None
@@ -112,6 +117,7 @@ def load_library() -> C.CDLL:
     L.h264a_dct_quant_4x4.argtypes = [vp, vp, i32, vp, i32, vp, vp, i32, i32, vp, vp]
     L.h264a_dct_quant_8x8.argtypes = [vp, vp, i32, vp, i32, vp, vp, vp, i32, i32, vp, vp]
     L.h264a_mc_tq_frames.argtypes = [vp, vp, i32, vp]
+    L.h264a_mc_tq_rec_frames.argtypes = [vp, vp, i32, vp]
     L.h264a_downsample2x.argtypes = [vp, vp, i32, i32, i32, sz, vp, vp]
     L.h264a_lookahead_costs.argtypes = [vp, vp, vp, i32, i32, i32, i32, vp, vp, vp, vp]
     L.h264a_pixel_path_host.argtypes = [vp, vp, i32, i32, i32, C.POINTER(MeParams), vp, f64, i64, i32, i32, vp, vp, vp,
@@ -303,6 +309,10 @@ class Accel:
     def mc_tq_frames(self, frames: Sequence[TqFrame]):
         arr = (TqFrame * len(frames))(*frames)
         self._check(self.L.h264a_mc_tq_frames(self.ctx, C.cast(arr, C.c_void_p), len(frames), self._stream()))
+
+    def mc_tq_rec_frames(self, frames: Sequence[TqRecFrame]):
+        arr = (TqRecFrame * len(frames))(*frames)
+        self._check(self.L.h264a_mc_tq_rec_frames(self.ctx, C.cast(arr, C.c_void_p), len(frames), self._stream()))
 
     # ---- a16-a19 ------------------------------------------------------------------
     def downsample2x(self, frames):

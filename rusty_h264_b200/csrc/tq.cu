@@ -63,7 +63,7 @@ __device__ __forceinline__ void forward_core4(int m[16]) {
 // Residual -> dct_four_t4's i16 cast -> quant_four_4x4 (pos = (row&1)*4+col),
 // written as 16 consecutive i16 (two 16-byte stores).
 __device__ __forceinline__ void tq4x4_store(const uint32_t s[4], const uint32_t p[4], const int16_t* ff,
-                                            const int16_t* mf, int16_t* out) {
+                                            const int16_t* mf, int16_t* out, int lv[16] = nullptr) {
     int m[16];
 #pragma unroll
     for (int r = 0; r < 4; r++)
@@ -81,6 +81,7 @@ __device__ __forceinline__ void tq4x4_store(const uint32_t s[4], const uint32_t 
             const int c = int(int16_t(m[idx]));
             const int lvl = ((abs(c) + int(ff[pos])) * int(mf[pos])) >> 16;
             v2[k] = int(int16_t(c < 0 ? -lvl : lvl));
+            if (lv) lv[idx] = v2[k];
         }
         w[i >> 1] = (uint32_t(uint16_t(v2[0]))) | (uint32_t(uint16_t(v2[1])) << 16);
     }
@@ -195,6 +196,52 @@ __global__ void __launch_bounds__(256) dct_quant_8x8_kernel(const uint8_t* __res
     }
 }
 
+// ---- reconstruction ------------------------------------------------------------
+
+// 16 * NORM_ADJUST (transform.rs:15-22) by qp % 6 and position group (both
+// even 0, both odd 1, else 2: POS_GROUP_FLAT, transform.rs:48-52).
+__constant__ int kLevelScale[6][3] = {{160, 256, 208}, {176, 288, 224}, {208, 320, 256},
+                                      {224, 368, 288}, {256, 400, 320}, {288, 464, 368}};
+
+// The inter MB's luma reconstruction of one 4x4 block (mb16.rs:3575-3605):
+// dequantize (transform.rs:233-284, flat scaling) each level, cast it to i16
+// as the reference does, inverse core transform rows then columns with
+// (x + 32) >> 6 (transform_quant.rs:30-35, 56-69), add the prediction and
+// clamp (idct_four_t4_rec, transform_quant.rs:96-119).  Four packed rows out.
+__device__ __forceinline__ void rec4x4(const int lv[16], const uint32_t p[4], int qp, uint32_t out[4]) {
+    const int m6 = qp % 6, shift = qp / 6;
+    int m[16];
+#pragma unroll
+    for (int i = 0; i < 16; i++) {
+        const int g = ((i >> 2) & 1) == (i & 1) ? ((i & 1) ? 1 : 0) : 2;
+        const int ls = kLevelScale[m6][g];
+        const int d = qp >= 24 ? int(uint32_t(lv[i] * ls) << (shift - 4)) : (lv[i] * ls + (1 << (3 - shift))) >> (4 - shift);
+        m[i] = int(int16_t(d));
+    }
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+        const int d0 = m[r * 4], d1 = m[r * 4 + 1], d2 = m[r * 4 + 2], d3 = m[r * 4 + 3];
+        const int e0 = d0 + d2, e1 = d0 - d2, e2 = (d1 >> 1) - d3, e3 = d1 + (d3 >> 1);
+        m[r * 4] = e0 + e3; m[r * 4 + 1] = e1 + e2; m[r * 4 + 2] = e1 - e2; m[r * 4 + 3] = e0 - e3;
+    }
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+        const int d0 = m[c], d1 = m[4 + c], d2 = m[8 + c], d3 = m[12 + c];
+        const int e0 = d0 + d2, e1 = d0 - d2, e2 = (d1 >> 1) - d3, e3 = d1 + (d3 >> 1);
+        m[c] = e0 + e3; m[4 + c] = e1 + e2; m[8 + c] = e1 - e2; m[12 + c] = e0 - e3;
+    }
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+        uint32_t w = 0;
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const int v = byte_of(p[r], c) + ((m[r * 4 + c] + 32) >> 6);
+            w |= uint32_t(v < 0 ? 0 : (v > 255 ? 255 : v)) << (8 * c);
+        }
+        out[r] = w;
+    }
+}
+
 // ---- fused MC + luma T/Q of whole frames ---------------------------------------
 
 struct TqFrameDesc {
@@ -204,6 +251,7 @@ struct TqFrameDesc {
     int16_t* coeffs;
     int mb_w;
     int nmb;
+    uint8_t* rec;  // cw x ch luma reconstruction, or nullptr
 };
 
 constexpr int TQ_MAXF = 96;
@@ -242,7 +290,17 @@ __global__ void mc_tq_frames_kernel(const __grid_constant__ TqBatch batch, long 
     const int qi = (by >= 8 ? 2 : 0) + (bx >= 8 ? 1 : 0);
     const int k = ((by & 4) ? 2 : 0) + ((bx & 4) ? 1 : 0);
     const int q = fd.qp > 51 ? 51 : (fd.qp < 0 ? 0 : fd.qp);
-    tq4x4_store(s, p, qt.ff[q], qt.mf[q], fd.coeffs + (long long)m * 256 + qi * 64 + k * 16);
+    if (fd.rec == nullptr) {
+        tq4x4_store(s, p, qt.ff[q], qt.mf[q], fd.coeffs + (long long)m * 256 + qi * 64 + k * 16);
+        return;
+    }
+    int lv[16];
+    tq4x4_store(s, p, qt.ff[q], qt.mf[q], fd.coeffs + (long long)m * 256 + qi * 64 + k * 16, lv);
+    uint32_t r4[4];
+    rec4x4(lv, p, q, r4);
+    // x is a multiple of 4 and cw of 16, so each row is one aligned word
+#pragma unroll
+    for (int i = 0; i < 4; i++) *reinterpret_cast<uint32_t*>(fd.rec + (long long)(y + i) * fd.pic.cw + x) = r4[i];
 }
 
 }  // namespace h264a
@@ -282,11 +340,16 @@ extern "C" int h264a_dct_quant_8x8(h264a_ctx* ctx, const uint8_t* d_src, int ss,
     return check_launch("dct_quant_8x8_kernel");
 }
 
-extern "C" int h264a_mc_tq_frames(h264a_ctx* ctx, const h264a_tq_frame* h_frames, int nframes, void* stream) {
+// Shared by h264a_mc_tq_frames and h264a_mc_tq_rec_frames: frame i's T/Q
+// input is frames[i], its reconstruction target recs[i] (recs may be null).
+static int mc_tq_launch(h264a_ctx* ctx, const h264a_tq_frame* h_frames, uint8_t* const* recs, int nframes,
+                        void* stream) {
     if (!ctx || !h_frames || nframes < 1) return fail(H264A_E_ARG, "mc_tq_frames: bad arguments");
     const int dz = h_frames[0].dz_div;
     for (int i = 0; i < nframes; i++) {
         const h264a_tq_frame& f = h_frames[i];
+        if (recs && (!recs[i] || (reinterpret_cast<uintptr_t>(recs[i]) & 3) != 0))
+            return fail(H264A_E_ARG, "mc_tq_rec_frames: reconstruction buffers must be non-null and 4-byte aligned");
         if (!f.pic.d_src || !f.pic.d_planes || !f.d_picks || !f.d_coeffs)
             return fail(H264A_E_ARG, "mc_tq_frames: null frame pointer");
         if (f.pic.cw < 16 || f.pic.ch < 16 || f.pic.cw % 16 || f.pic.ch % 16 || f.pic.pad < 3 || f.pic.pad > 128)
@@ -307,7 +370,8 @@ extern "C" int h264a_mc_tq_frames(h264a_ctx* ctx, const h264a_tq_frame* h_frames
         long long total = 0;
         for (int k = 0; k < gn; k++) {
             const h264a_tq_frame& f = h_frames[g0 + k];
-            b.f[k] = {f.pic, f.d_picks, f.qp, f.d_coeffs, f.pic.cw / 16, (f.pic.cw / 16) * (f.pic.ch / 16)};
+            b.f[k] = {f.pic, f.d_picks, f.qp, f.d_coeffs, f.pic.cw / 16, (f.pic.cw / 16) * (f.pic.ch / 16),
+                      recs ? recs[g0 + k] : nullptr};
             b.mb_base[k] = int(total);
             total += b.f[k].nmb;
         }
@@ -317,4 +381,20 @@ extern "C" int h264a_mc_tq_frames(h264a_ctx* ctx, const h264a_tq_frame* h_frames
         if (rc) return rc;
     }
     return H264A_OK;
+}
+
+extern "C" int h264a_mc_tq_frames(h264a_ctx* ctx, const h264a_tq_frame* h_frames, int nframes, void* stream) {
+    return mc_tq_launch(ctx, h_frames, nullptr, nframes, stream);
+}
+
+extern "C" int h264a_mc_tq_rec_frames(h264a_ctx* ctx, const h264a_tq_rec_frame* h_frames, int nframes,
+                                      void* stream) {
+    if (!h_frames || nframes < 1) return fail(H264A_E_ARG, "mc_tq_rec_frames: bad arguments");
+    std::vector<h264a_tq_frame> tq(nframes);
+    std::vector<uint8_t*> rec(nframes);
+    for (int i = 0; i < nframes; i++) {
+        tq[i] = h_frames[i].tq;
+        rec[i] = h_frames[i].d_rec;
+    }
+    return mc_tq_launch(ctx, tq.data(), rec.data(), nframes, stream);
 }

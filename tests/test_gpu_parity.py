@@ -446,6 +446,36 @@ def test_mc_tq_frames_matches_oracle(acc, cif):
         assert np.array_equal(co.cpu().numpy(), O.mc_tq_frame(src, ref, picks, q, 6))
 
 
+@pytest.mark.parametrize("qp", [0, 10, 24, 30, 51])
+def test_mc_tq_rec_frames_matches_oracle(acc, cif, qp):
+    """MC + T/Q with the luma reconstruction (mb16.rs:3575-3605): coefficients
+    and reconstructed frames bit-exact with the oracle, across the qp < 24 and
+    qp >= 24 dequant arms."""
+    params = O.balanced_params()
+    lam = float(np.sqrt(A.frame_lambda(max(qp, 12))))
+    frames, keep, outs = [], [], []
+    for f in (1, 2):
+        src, ref = cif[f], cif[f - 1]
+        picks, _ = O.me_frame(src, ref, O.build_planes4(ref, 32), params, lam, A.split_gate_for_qp(max(qp, 12)))
+        d_src, d_pl = dev(acc, src), acc.hpel_build(dev(acc, ref[None]), 32)[0]
+        d_pk = dev(acc, picks)
+        co = acc.zeros((picks.shape[0], 256), acc.torch.int16)
+        rec = acc.torch.full((288, 352), 7, dtype=acc.torch.uint8, device="cuda:0")
+        keep += [d_src, d_pl, d_pk]
+        outs.append((co, rec, src, ref, picks))
+        tq = A.TqFrame(A.Picture(d_src.data_ptr(), d_pl.data_ptr(), 352, 288, 32), d_pk.data_ptr(), qp, 6,
+                       co.data_ptr())
+        frames.append(A.TqRecFrame(tq, rec.data_ptr()))
+    acc.mc_tq_rec_frames(frames)
+    acc.sync()
+    for co, rec, src, ref, picks in outs:
+        wc, wr = O.mc_tq_rec_frame(src, ref, picks, qp, 6)
+        assert np.array_equal(co.cpu().numpy(), wc)
+        assert np.array_equal(rec.cpu().numpy(), wr)
+    # the reconstruction is the prediction plus a bounded error
+    assert np.abs(outs[0][1].cpu().numpy().astype(int) - cif[1].astype(int)).mean() < (40 if qp > 40 else 12)
+
+
 # ---------------------------------------------------------------------------
 # a16-a19 lookahead
 # ---------------------------------------------------------------------------

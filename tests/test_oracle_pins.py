@@ -377,3 +377,103 @@ def test_hpel_block_matches_mc_luma():
                             assert d == np_satd_sum(src[y0:y0 + bh, x0:x0 + bw], want)
                             checked += 1
     assert checked > 2000
+
+
+# ---------------------------------------------------------------------------
+# reconstruction: dequantize + inverse 4x4 + add (transform.rs:233, 381;
+# accel/src/transform_quant.rs:56-119)
+# ---------------------------------------------------------------------------
+
+NORM_ADJUST = [[10, 16, 13], [11, 18, 14], [13, 20, 16], [14, 23, 18], [16, 25, 20], [18, 29, 23]]
+POS_GROUP_FLAT = [0, 2, 0, 2, 2, 1, 2, 1, 0, 2, 0, 2, 2, 1, 2, 1]
+
+
+def np_dequant(levels, qp):
+    """dequantize spelled out as transform.rs:233-284 writes it."""
+    m, shift = qp % 6, qp // 6
+    out = []
+    for i, lv in enumerate(levels):
+        ls = 16 * NORM_ADJUST[m][POS_GROUP_FLAT[i]]
+        out.append((lv * ls) << (shift - 4) if qp >= 24 else (lv * ls + (1 << (3 - shift))) >> (4 - shift))
+    return out
+
+
+def np_inv_1d(d0, d1, d2, d3):
+    e0, e1, e2, e3 = d0 + d2, d0 - d2, (d1 >> 1) - d3, d1 + (d3 >> 1)
+    return [e0 + e3, e1 + e2, e1 - e2, e0 - e3]
+
+
+def np_inverse(coeffs, rows_first=True, norm=True):
+    m = [list(coeffs[r * 4:r * 4 + 4]) for r in range(4)]
+    def rows(m):
+        return [np_inv_1d(*m[r]) for r in range(4)]
+    def cols(m):
+        t = [np_inv_1d(m[0][c], m[1][c], m[2][c], m[3][c]) for c in range(4)]
+        return [[t[c][r] for c in range(4)] for r in range(4)]
+    m = cols(rows(m)) if rows_first else rows(cols(m))
+    flat = [v for row in m for v in row]
+    return [(v + 32) >> 6 for v in flat] if norm else flat
+
+
+def test_dequant_matches_the_reference_formula():
+    """transform.rs:1064-1125 (dequant_4x4_matches_scalar): the xorshift32
+    stream from 0x2f6e_1c37, 64 cases per qp with magnitudes 3, 11 and 15 bits
+    and zero, every qp 0..51."""
+    st = 0x2F6E1C37
+
+    def rnd():
+        nonlocal st
+        st ^= (st << 13) & 0xFFFFFFFF
+        st ^= st >> 17
+        st ^= (st << 5) & 0xFFFFFFFF
+        return st
+
+    for qp in range(52):
+        for case in range(64):
+            lv = []
+            for _ in range(16):
+                r = rnd()
+                mag = [r & 0x7, r & 0x7FF, r & 0x7FFF, 0][case % 4]
+                lv.append(-mag if r & 0x80000000 else mag)
+            assert list(O.dequant4x4(lv, qp)) == np_dequant(lv, qp), (qp, case)
+
+
+def test_inverse_core_is_row_first():
+    """transform.rs:1268-1331: this block tells the two orders apart, and the
+    inverse transform is rows first."""
+    coeffs = [9, 2, -1, 2, -2, 2, -2, 1, -1, -2, 3, 5, -1, -1, -5, 3]
+    assert np_inverse(coeffs, True, False) != np_inverse(coeffs, False, False)
+    assert list(O.inverse_core4(coeffs)) == np_inverse(coeffs, True)
+    # scaled up, the order shows in the normalized output too
+    rng = np.random.default_rng(5)
+    differ = 0
+    for _ in range(500):
+        c = [int(v) for v in rng.integers(-3000, 3000, 16)]
+        want = np_inverse(c, True)
+        assert list(O.inverse_core4(c)) == want
+        differ += want != np_inverse(c, False)
+    assert differ > 0
+
+
+def test_dc_only_inverse_is_flat():
+    """transform.rs:341-356 (dequantize_dc4): a DC-only block inverts to the
+    flat (f + 32) >> 6 at every position."""
+    for f in (-4096, -65, 0, 31, 32, 64, 1000, 20000):
+        assert list(O.inverse_core4([f] + [0] * 15)) == [(f + 32) >> 6] * 16
+
+
+def test_idct_rec_matches_reference():
+    """accel/src/transform_quant.rs:169-195 (idct_rec_matches_reference): the
+    pred/dct patterns of 128 seeds through idct_four_t4_rec."""
+    sub = [(0, 0), (4, 0), (0, 4), (4, 4)]
+    for seed in range(128):
+        pred = np.array([(i * 7 + seed * 3) & 0xFF for i in range(64)], np.uint8).reshape(8, 8)
+        dct = np.array([((i * 53 + seed * 29) % 4096) - 2048 for i in range(64)], np.int16)
+        got = O.idct_four_t4_rec(pred, dct)
+        for k, (ox, oy) in enumerate(sub):
+            m = np_inverse([int(v) for v in dct[k * 16:k * 16 + 16]], True)
+            for dy in range(4):
+                for dx in range(4):
+                    want = min(255, max(0, int(pred[oy + dy, ox + dx]) + m[dy * 4 + dx]))
+                    assert got[oy + dy, ox + dx] == want, (seed, k)
+
