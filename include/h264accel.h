@@ -231,6 +231,26 @@ typedef struct {
     uint8_t *d_rec;
 } h264a_tq_rec_frame;
 H264A_API int h264a_mc_tq_rec_frames(h264a_ctx *ctx, const h264a_tq_rec_frame *h_frames, int nframes, void *stream);
+/* The inter MB's chroma (mb16.rs:3408-3428, 3465-3500, 3606-3628): mc_chroma
+ * (inter.rs:1268) of each partition with its luma MV, dct_four_t4 +
+ * quant_four_4x4 at chroma_qp(qp) (predict.rs:64), the 2x2 DC through
+ * forward_quant_chroma_dc (transform.rs:1023, inter dead-zone), and, when
+ * d_rec_u/d_rec_v are given, the reconstruction (dequantize with the DC from
+ * inverse_quant_chroma_dc, idct_four_t4_rec).  Out: 128 i16 per MB, U then V,
+ * four 4x4 blocks each in the order (0,0),(4,0),(0,4),(4,4), 16 levels per
+ * block in raster order with slot 0 holding the block's DC level (the
+ * Hadamard output of that index). */
+typedef struct {
+    const uint8_t *d_src_u, *d_src_v; /* (cw/2) x (ch/2) source chroma, 4-byte aligned */
+    const uint8_t *d_ref_u, *d_ref_v; /* the reference picture's chroma, 4-byte aligned */
+    int32_t cw, ch;                   /* luma size, MB-aligned */
+    const int32_t *d_picks;           /* 6 i32 per MB, as h264a_me_frames writes */
+    int32_t qp;                       /* luma QP 0..51 */
+    int16_t *d_coeffs;                /* 128 i16 per MB, 16-byte aligned */
+    uint8_t *d_rec_u, *d_rec_v;       /* reconstruction planes, or both NULL */
+} h264a_tq_chroma_frame;
+H264A_API int h264a_mc_tq_chroma_frames(h264a_ctx *ctx, const h264a_tq_chroma_frame *h_frames, int nframes,
+                                        void *stream);
 
 /* ---- a16-a19: mb-tree lookahead ------------------------------------------ */
 /* downsample2x (encoder/src/mbtree.rs:61-74) of n frames cw x ch -> cw/2 x ch/2. */

@@ -373,6 +373,46 @@ void or_mb_luma_rec(uint8_t *rec, int srec, const uint8_t *pred16, const int16_t
     }
 }
 
+/* ---- chroma: QP map, 2x2 DC transform and quant ------------------------- */
+
+/* chroma_qp (predict.rs:64-73): identity below 30, then the QPC table. */
+int or_chroma_qp(int qp) {
+    static const int QPC[22] = {29, 30, 31, 32, 32, 33, 34, 34, 35, 35, 36, 36, 37, 37, 37, 38, 38, 38, 39, 39, 39, 39};
+    return qp < 30 ? qp : QPC[qp - 30];
+}
+
+/* hadamard_2x2 (transform.rs:1017-1021). */
+static void or_hadamard2x2(const int32_t d[4], int32_t o[4]) {
+    o[0] = d[0] + d[1] + d[2] + d[3];
+    o[1] = d[0] - d[1] + d[2] - d[3];
+    o[2] = d[0] + d[1] - d[2] - d[3];
+    o[3] = d[0] - d[1] - d[2] + d[3];
+}
+
+/* forward_quant_chroma_dc (transform.rs:1023-1035). */
+void or_forward_quant_chroma_dc(const int32_t dc[4], int qp, int intra, int32_t out[4]) {
+    int32_t f[4];
+    or_hadamard2x2(dc, f);
+    int m = qp % 6;
+    int qbits = 15 + qp / 6;
+    int64_t off = intra ? ((int64_t)1 << qbits) / 3 : ((int64_t)1 << qbits) / 6;
+    int64_t mf = QUANT_MF[m][0];
+    for (int i = 0; i < 4; i++) {
+        int64_t a = f[i] < 0 ? -(int64_t)f[i] : f[i];
+        int64_t level = (a * mf + 2 * off) >> (qbits + 1);
+        out[i] = (int32_t)(f[i] < 0 ? -level : level);
+    }
+}
+
+/* inverse_quant_chroma_dc (transform.rs:1038-1050). */
+void or_inverse_quant_chroma_dc(const int32_t levels[4], int qp, int32_t out[4]) {
+    int32_t g[4];
+    or_hadamard2x2(levels, g);
+    int m = qp % 6, shift = qp / 6;
+    int32_t ls = 16 * OR_NORM_ADJUST[m][0];
+    for (int i = 0; i < 4; i++) out[i] = (int32_t)((uint32_t)(g[i] * ls) << shift) >> 5;
+}
+
 /* ======================================================================== */
 /* Inter prediction (crates/rusty_h264-common/src/inter.rs)                 */
 /* ======================================================================== */
@@ -969,6 +1009,24 @@ void or_motion_search(const or_me_frame *fr, const or_me_params *pr, int lx, int
     }
     if (pr->me_snap && seed_c < best_c) { bx_ = seed_x; by_ = seed_y; best_c = seed_c; }
     out->mvx = bx_; out->mvy = by_; out->cost = best_c; out->evals = m.evals;
+}
+
+/* mc_chroma (inter.rs:1268-1361): eighth-pel bilinear of a bw x bh chroma
+ * block, every tap read with clamped coordinates; the copy and tile fast
+ * paths of the reference give the same values. */
+void or_mc_chroma(const uint8_t *ref, int cw, int ch, int x0, int y0, int bw, int bh, int32_t mvx, int32_t mvy,
+                  uint8_t *out) {
+    int ix0 = x0 + (mvx >> 3), iy0 = y0 + (mvy >> 3);
+    int fx = mvx & 7, fy = mvy & 7;
+    int wa = (8 - fx) * (8 - fy), wb = fx * (8 - fy), wc = (8 - fx) * fy, wd = fx * fy;
+    for (int dy = 0; dy < bh; dy++)
+        for (int dx = 0; dx < bw; dx++) {
+            int x = ix0 + dx, y = iy0 + dy;
+            int xa = x < 0 ? 0 : (x > cw - 1 ? cw - 1 : x), xb = x + 1 < 0 ? 0 : (x + 1 > cw - 1 ? cw - 1 : x + 1);
+            int ya = y < 0 ? 0 : (y > ch - 1 ? ch - 1 : y), yb = y + 1 < 0 ? 0 : (y + 1 > ch - 1 ? ch - 1 : y + 1);
+            int v = wa * ref[ya * cw + xa] + wb * ref[ya * cw + xb] + wc * ref[yb * cw + xa] + wd * ref[yb * cw + xb];
+            out[dy * bw + dx] = (uint8_t)((v + 32) >> 6);
+        }
 }
 
 /* ---- plain-ME frame model --------------------------------------------------- */

@@ -52,6 +52,11 @@ void or_dequant4x4(const int32_t lv[16], int qp, int32_t out[16]);
 void or_inverse_core4(int32_t m[16]);
 void or_idct_four_t4_rec(uint8_t *rec, int srec, const uint8_t *pred, int spred, const int16_t dct[64]);
 void or_mb_luma_rec(uint8_t *rec, int srec, const uint8_t *pred16, const int16_t levels[256], int qp);
+int or_chroma_qp(int qp);
+void or_forward_quant_chroma_dc(const int32_t dc[4], int qp, int intra, int32_t out[4]);
+void or_inverse_quant_chroma_dc(const int32_t levels[4], int qp, int32_t out[4]);
+void or_mc_chroma(const uint8_t *ref, int cw, int ch, int x0, int y0, int bw, int bh, int32_t mvx, int32_t mvy,
+                  uint8_t *out);
 
 /* ---- inter prediction (crates/rusty_h264-common/src/inter.rs) ------------- */
 int32_t or_median3(int32_t a, int32_t b, int32_t c);

@@ -191,6 +191,71 @@ void or_mc_tq_rec_frame(const uint8_t *src, const uint8_t *ref, int cw, int ch, 
         }
 }
 
+/* The inter MB's chroma of mb16.rs:3408-3428, 3465-3500 and 3606-3628, per
+ * MB: mc_chroma of each partition with the luma MV, per plane dct_four_t4 +
+ * quant_four_4x4 at chroma_qp(qp) with the AC levels kept and slot 0 taken by
+ * the block's DC (the 2x2 forward_quant_chroma_dc level, inter dead-zone);
+ * reconstruction: dequantize of the AC levels, the DC replaced by
+ * inverse_quant_chroma_dc (both cast to i16), idct_four_t4_rec onto the
+ * prediction.  coeffs: 128 i16 per MB (U then V, SUBBLOCKS order, 16 each);
+ * rec_u / rec_v may be NULL. */
+void or_mc_tq_chroma_frame(const uint8_t *src_u, const uint8_t *src_v, const uint8_t *ref_u, const uint8_t *ref_v,
+                           int cw, int ch, const int32_t *picks, int qp, int16_t *coeffs, uint8_t *rec_u,
+                           uint8_t *rec_v) {
+    int mb_w = cw / 16, mb_h = ch / 16, ccw = cw / 2, cch = ch / 2;
+    int qpc = or_chroma_qp(qp);
+    int16_t ff[8], mf[8];
+    or_quant_dz_ff(qpc, 6, ff);
+    or_quant_mf_oh(qpc, mf);
+    for (int mby = 0; mby < mb_h; mby++)
+        for (int mbx = 0; mbx < mb_w; mbx++) {
+            int m = mby * mb_w + mbx;
+            const int32_t *pk = picks + 6 * m;
+            for (int c = 0; c < 2; c++) {
+                const uint8_t *rf = c == 0 ? ref_u : ref_v, *sc = c == 0 ? src_u : src_v;
+                uint8_t pred[64];
+                int shape = pk[0];
+                if (shape == 0) {
+                    or_mc_chroma(rf, ccw, cch, mbx * 8, mby * 8, 8, 8, pk[1], pk[2], pred);
+                } else {
+                    for (int k = 0; k < 2; k++) {
+                        int ox = shape == 2 ? 4 * k : 0, oy = shape == 1 ? 4 * k : 0;
+                        int bw = shape == 2 ? 4 : 8, bh = shape == 1 ? 4 : 8;
+                        uint8_t t[64];
+                        or_mc_chroma(rf, ccw, cch, mbx * 8 + ox, mby * 8 + oy, bw, bh, pk[1 + 2 * k], pk[2 + 2 * k], t);
+                        for (int r = 0; r < bh; r++) memcpy(pred + (oy + r) * 8 + ox, t + r * bw, bw);
+                    }
+                }
+                int16_t cd[64];
+                const uint8_t *s8 = sc + (int64_t)mby * 8 * ccw + mbx * 8;
+                or_dct_four_t4(cd, s8, ccw, pred, 8);
+                int32_t dc[4] = {cd[0], cd[16], cd[32], cd[48]};
+                or_quant_four_4x4(cd, ff, mf);
+                int32_t dl[4], rdc[4];
+                or_forward_quant_chroma_dc(dc, qpc, 0, dl);
+                or_inverse_quant_chroma_dc(dl, qpc, rdc);
+                int16_t *out = coeffs + (int64_t)m * 128 + c * 64;
+                for (int i = 0; i < 4; i++) {
+                    out[i * 16] = (int16_t)dl[i];
+                    for (int j = 1; j < 16; j++) out[i * 16 + j] = cd[i * 16 + j];
+                }
+                uint8_t *rp = c == 0 ? rec_u : rec_v;
+                if (rp) {
+                    int16_t d[64];
+                    for (int i = 0; i < 4; i++) {
+                        int32_t lv[16], dq[16];
+                        lv[0] = 0;
+                        for (int j = 1; j < 16; j++) lv[j] = cd[i * 16 + j];
+                        or_dequant4x4(lv, qpc, dq);
+                        for (int j = 0; j < 16; j++) d[i * 16 + j] = (int16_t)dq[j];
+                        d[i * 16] = (int16_t)rdc[i];
+                    }
+                    or_idct_four_t4_rec(rp + (int64_t)mby * 8 * ccw + mbx * 8, ccw, pred, 8, d);
+                }
+            }
+        }
+}
+
 typedef struct {
     const uint8_t *frames;
     uint8_t *half;

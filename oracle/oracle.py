@@ -74,6 +74,7 @@ def lib():
         L.or_la_mc_satd.restype = C.c_int64
         L.or_candidate_dist.restype = C.c_int64
         L.or_num_threads.restype = C.c_int
+        L.or_chroma_qp.restype = C.c_int
         L.or_motion_search_flat.argtypes = [u8p, u8p, u8p, C.c_int, C.c_int, C.c_int, C.POINTER(MeParamsFlat), u16p,
                                             C.c_int, C.c_int, C.c_int, C.c_int, i32p, C.c_int, C.c_double, i32p,
                                             i32p, i64p, i32p]
@@ -192,6 +193,42 @@ def mc_tq_rec_frame(src, ref, picks, qp, dz_div=6):
     lib().or_mc_tq_rec_frame(ptr(src), ptr(ref), cw, ch, ptr(np.ascontiguousarray(picks), i32p), qp, dz_div,
                              ptr(out, i16p), ptr(rec))
     return out, rec
+
+
+def mc_tq_chroma_frame(src_u, src_v, ref_u, ref_v, picks, qp, rec=True):
+    """(coeffs (nmb, 128) i16, rec_u, rec_v): the inter MBs' chroma MC, T/Q and
+    reconstruction of a frame."""
+    cch, ccw = src_u.shape
+    nmb = (ccw // 8) * (cch // 8)
+    out = np.zeros((nmb, 128), np.int16)
+    ru = np.zeros((cch, ccw), np.uint8) if rec else None
+    rv = np.zeros((cch, ccw), np.uint8) if rec else None
+    c = [np.ascontiguousarray(a) for a in (src_u, src_v, ref_u, ref_v)]
+    lib().or_mc_tq_chroma_frame(ptr(c[0]), ptr(c[1]), ptr(c[2]), ptr(c[3]), 2 * ccw, 2 * cch,
+                                ptr(np.ascontiguousarray(picks), i32p), int(qp), ptr(out, i16p),
+                                ptr(ru) if rec else None, ptr(rv) if rec else None)
+    return out, ru, rv
+
+
+def mc_chroma(ref: np.ndarray, x0, y0, bw, bh, mvx, mvy) -> np.ndarray:
+    ch, cw = ref.shape
+    out = np.zeros((bh, bw), np.uint8)
+    lib().or_mc_chroma(ptr(np.ascontiguousarray(ref)), cw, ch, x0, y0, bw, bh, mvx, mvy, ptr(out))
+    return out
+
+
+def chroma_qp(qp) -> int:
+    return lib().or_chroma_qp(int(qp))
+
+
+def chroma_dc_quant(dc, qp, intra=False):
+    """(levels, reconstructed DCs) of a 2x2 chroma DC block."""
+    d = np.ascontiguousarray(dc, np.int32)
+    lv = np.zeros(4, np.int32)
+    rd = np.zeros(4, np.int32)
+    lib().or_forward_quant_chroma_dc(ptr(d, i32p), int(qp), int(intra), ptr(lv, i32p))
+    lib().or_inverse_quant_chroma_dc(ptr(lv, i32p), int(qp), ptr(rd, i32p))
+    return lv, rd
 
 
 def dequant4x4(levels, qp) -> np.ndarray:

@@ -476,6 +476,46 @@ def test_mc_tq_rec_frames_matches_oracle(acc, cif, qp):
     assert np.abs(outs[0][1].cpu().numpy().astype(int) - cif[1].astype(int)).mean() < (40 if qp > 40 else 12)
 
 
+@pytest.mark.parametrize("qp", [0, 20, 29, 30, 36, 51])
+def test_mc_tq_chroma_frames_matches_oracle(acc, qp):
+    """The inter MB's chroma MC + T/Q (with the 2x2 DC) and reconstruction,
+    bit-exact with the oracle for every pick shape, across the chroma-QP map
+    and both dequant arms; one frame without reconstruction."""
+    y, _, _ = synth.cif_clip(4, 1)
+    luma = synth.coded_luma(y)
+    # textured chroma: the half-res luma, and its negative shifted by a few pixels
+    u = np.stack([O.downsample2x(a) for a in luma])
+    v = np.ascontiguousarray(255 - np.roll(u, (3, -5), (1, 2)))
+    lam = float(np.sqrt(A.frame_lambda(max(qp, 12))))
+    frames, keep, outs = [], [], []
+    for f in (1, 2, 3):
+        src, ref = luma[f], luma[f - 1]
+        picks, _ = O.me_frame(src, ref, O.build_planes4(ref, 32), O.balanced_params(), lam, 0)
+        # force every shape: the search's picks, then 16x8 and 8x16 with distinct MVs
+        if f == 2:
+            picks[::3, 0] = 1
+            picks[1::3, 0] = 2
+            picks[:, 3] = picks[:, 1] + 5
+            picks[:, 4] = picks[:, 2] - 3
+        d = [dev(acc, a) for a in (u[f], v[f], u[f - 1], v[f - 1], picks)]
+        co = acc.zeros((picks.shape[0], 128), acc.torch.int16)
+        want_rec = f != 3
+        ru = acc.torch.full((144, 176), 3, dtype=acc.torch.uint8, device="cuda:0") if want_rec else None
+        rv = acc.torch.full((144, 176), 3, dtype=acc.torch.uint8, device="cuda:0") if want_rec else None
+        keep += d + [co, ru, rv]
+        outs.append((co, ru, rv, f, picks))
+        frames.append(A.TqChromaFrame(d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(), d[3].data_ptr(), 352, 288,
+                                      d[4].data_ptr(), qp, co.data_ptr(), ru.data_ptr() if want_rec else None,
+                                      rv.data_ptr() if want_rec else None))
+    acc.mc_tq_chroma_frames(frames)
+    acc.sync()
+    for co, ru, rv, f, picks in outs:
+        wc, wu, wv = O.mc_tq_chroma_frame(u[f], v[f], u[f - 1], v[f - 1], picks, qp)
+        assert np.array_equal(co.cpu().numpy(), wc), (qp, f)
+        if ru is not None:
+            assert np.array_equal(ru.cpu().numpy(), wu) and np.array_equal(rv.cpu().numpy(), wv), (qp, f)
+
+
 # ---------------------------------------------------------------------------
 # a16-a19 lookahead
 # ---------------------------------------------------------------------------

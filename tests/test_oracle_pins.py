@@ -477,3 +477,58 @@ def test_idct_rec_matches_reference():
                     want = min(255, max(0, int(pred[oy + dy, ox + dx]) + m[dy * 4 + dx]))
                     assert got[oy + dy, ox + dx] == want, (seed, k)
 
+
+# ---------------------------------------------------------------------------
+# chroma: mc_chroma (inter.rs:1268), chroma_qp (predict.rs:64), the 2x2 DC
+# (transform.rs:1017-1050)
+# ---------------------------------------------------------------------------
+
+def test_chroma_known_answers():
+    """predict.rs:868-872 (chroma_qp_mapping), inter.rs:2066-2080
+    (mc_chroma_zero_mv_copies, mc_chroma_bilinear_midpoint)."""
+    assert (O.chroma_qp(20), O.chroma_qp(30), O.chroma_qp(51)) == (20, 29, 39)
+    r = np.array([0, 1, 2, 3, 10, 11, 12, 13, 20, 21, 22, 23, 30, 31, 32, 33], np.uint8).reshape(4, 4)
+    assert list(O.mc_chroma(r, 1, 1, 2, 2, 0, 0).ravel()) == [11, 12, 21, 22]
+    assert int(O.mc_chroma(np.array([[0, 8], [0, 8]], np.uint8), 0, 0, 1, 1, 4, 0)[0, 0]) == 4
+
+
+def test_mc_chroma_matches_per_pixel():
+    """inter.rs:1952-1990 (mc_chroma_block_matches_per_pixel): the LCG
+    reference picture (state 0xabcd_1234, x·1664525 + 1013904223, top byte),
+    four block sizes at three positions, every MV in -12..12."""
+    cw, ch = 24, 20
+    st = 0xABCD1234
+    ref = []
+    for _ in range(cw * ch):
+        st = (st * 1664525 + 1013904223) & 0xFFFFFFFF
+        ref.append(st >> 24)
+    ref = np.array(ref, np.uint8).reshape(ch, cw)
+
+    def at(x, y):
+        return int(ref[min(max(y, 0), ch - 1), min(max(x, 0), cw - 1)])
+
+    for bw, bh in [(8, 8), (4, 4), (8, 4), (4, 8)]:
+        for x0, y0 in [(4, 4), (0, 0), (cw - bw, ch - bh)]:
+            for mvx in range(-12, 13):
+                for mvy in range(-12, 13, 5):
+                    got = O.mc_chroma(ref, x0, y0, bw, bh, mvx, mvy)
+                    ix0, iy0, fx, fy = x0 + (mvx >> 3), y0 + (mvy >> 3), mvx & 7, mvy & 7
+                    for dy in range(bh):
+                        for dx in range(bw):
+                            x, y = ix0 + dx, iy0 + dy
+                            v = ((8 - fx) * (8 - fy) * at(x, y) + fx * (8 - fy) * at(x + 1, y) +
+                                 (8 - fx) * fy * at(x, y + 1) + fx * fy * at(x + 1, y + 1) + 32) >> 6
+                            assert got[dy, dx] == v, (bw, bh, x0, y0, mvx, mvy)
+
+
+def test_chroma_dc_end_to_end_flat_block():
+    """transform.rs:1402-1420: a flat chroma DC block survives the 2x2 forward
+    quant, the inverse and the 4x4 inverse within 1 + 2^(qp/6)."""
+    for r in (4, -6, 11):
+        for qp in (0, 18, 30):
+            lv, rd = O.chroma_dc_quant([16 * r] * 4, qp, intra=True)
+            tol = 1 + (1 << (qp // 6))
+            for d in rd:
+                for v in O.inverse_core4([int(d)] + [0] * 15):
+                    assert abs(int(v) - r) <= tol, (r, qp)
+
