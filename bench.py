@@ -325,6 +325,31 @@ def run_ours(args, ws, rank, local):
             stage_ms[k].append(a.elapsed_time(b))
     acc.sync()
     stage = {k: float(np.mean(v)) for k, v in stage_ms.items()}
+
+    # The reconstruction side (not part of `value`): MC + T/Q with the luma
+    # reconstruction, and the chroma MC + T/Q + reconstruction, over the same
+    # 59 P frames.  The half-res luma planes of the lookahead stand in for the
+    # chroma planes (960x544, textured).
+    rec = torch.empty((n, ch, cw), dtype=torch.uint8, device=dev)
+    ccoef = torch.empty((n, nmb, 128), dtype=torch.int16, device=dev)
+    crec = torch.empty((2, n, ch // 2, cw // 2), dtype=torch.uint8, device=dev)
+    rec_frames = [A.TqRecFrame(tq_frames[i - 1], rec[i].data_ptr()) for i in range(1, n)]
+    chroma_frames = [A.TqChromaFrame(half[i].data_ptr(), half[i].data_ptr(), half[i - 1].data_ptr(),
+                                     half[i - 1].data_ptr(), cw, ch, picks[i].data_ptr(), qp, ccoef[i].data_ptr(),
+                                     crec[0, i].data_ptr(), crec[1, i].data_ptr()) for i in range(1, n)]
+    extra = {"mc_tq_rec": [], "chroma_mc_tq_rec": []}
+    for _ in range(max(3, args.steps // 2) + 1):
+        a, b, c2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        a.record(stream)
+        acc.mc_tq_rec_frames(rec_frames)
+        b.record(stream)
+        acc.mc_tq_chroma_frames(chroma_frames)
+        c2.record(stream)
+        torch.cuda.synchronize()
+        extra["mc_tq_rec"].append(a.elapsed_time(b))
+        extra["chroma_mc_tq_rec"].append(b.elapsed_time(c2))
+    acc.sync()
+    extra_ms = {k: round(float(np.mean(v[1:])), 4) for k, v in extra.items()}
     work4x4 = int(picks[1:, :, 5].sum().item())
     int32_peak = acc.measure_int32_peak()
     me_ops = work4x4 * SATD_OPS_PER_4X4
@@ -357,6 +382,7 @@ def run_ours(args, ws, rank, local):
                    "frames_per_step": n, "qp": qp, "preset": "balanced", "split_partitions": True,
                    "l2": "inputs and outputs (~1 GB) exceed L2; no flush", "parallelism": f"replicas x{ws}"},
         "stage_ms": {k: round(v, 4) for k, v in stage.items()},
+        "reconstruction_ms": dict(extra_ms, note="timed separately over the same 59 P frames, not part of value"),
         "roofline": roofline,
         "clocks": clk,
         "gpu_launches": kernels_per_step * args.steps,
