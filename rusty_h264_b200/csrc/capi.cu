@@ -105,7 +105,11 @@ extern "C" int h264a_ctx_create(int device, h264a_ctx** out) {
     h264a_ctx* c = new h264a_ctx();
     c->device = device;
     c->num_sms = prop.multiProcessorCount;
-    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+    bool ev_ok = true;
+    for (int i = 0; i < PP_CHUNKS + 2; i++)
+        ev_ok = ev_ok && cudaEventCreateWithFlags(&c->pp_ev[i], cudaEventDisableTiming) == cudaSuccess;
+    if (!ev_ok || cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaMalloc(&c->d_counter, 4 * sizeof(int32_t)) != cudaSuccess ||
         cudaMalloc(&c->d_status, sizeof(int32_t)) != cudaSuccess ||
         cudaMemset(c->d_status, 0, sizeof(int32_t)) != cudaSuccess) {
@@ -121,11 +125,15 @@ extern "C" int h264a_ctx_destroy(h264a_ctx* ctx) {
     if (!ctx) return H264A_OK;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
     if (ctx->d_counter) cudaFree(ctx->d_counter);
     if (ctx->d_status) cudaFree(ctx->d_status);
     if (ctx->d_flags) cudaFree(ctx->d_flags);
     if (ctx->pp_buf) cudaFree(ctx->pp_buf);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
+    for (int i = 0; i < PP_CHUNKS + 2; i++)
+        if (ctx->pp_ev[i]) cudaEventDestroy(ctx->pp_ev[i]);
     delete ctx;
     return H264A_OK;
 }
@@ -258,8 +266,17 @@ extern "C" int h264a_pixel_path_host(h264a_ctx* ctx, const uint8_t* h_frames, in
     int32_t* d_inter = reinterpret_cast<int32_t*>(base + o_inter);
     int32_t* d_mvs = reinterpret_cast<int32_t*>(base + o_mvs);
     uint16_t* d_tab = reinterpret_cast<uint16_t*>(base + o_tab);
-    cudaStream_t st = ctx->stream;
-    H264A_CUDA(cudaMemcpyAsync(d_frames, h_frames, fs * n, cudaMemcpyHostToDevice, st));
+    // Two streams: the frames go up in PP_CHUNKS chunks on the copy stream
+    // while the compute stream builds each chunk's planes and half-res
+    // frames; after ME and T/Q the coefficients come down on the copy stream
+    // while the compute stream runs the lookahead.
+    cudaStream_t st = ctx->stream, cs = ctx->copy_stream;
+    const int nk = n < PP_CHUNKS ? n : PP_CHUNKS;
+    for (int k = 0; k < nk; k++) {
+        const int a = int((long long)k * n / nk), b = int((long long)(k + 1) * n / nk);
+        H264A_CUDA(cudaMemcpyAsync(d_frames + fs * a, h_frames + fs * a, fs * (b - a), cudaMemcpyHostToDevice, cs));
+        H264A_CUDA(cudaEventRecord(ctx->pp_ev[k], cs));
+    }
     h264a_me_params prm = *params;
     if (prm.mv_cost_kind == 1 || prm.mv_cost_kind == 2) {
         H264A_CUDA(cudaMemcpyAsync(d_tab, h_mv_cost_tab, sizeof(uint16_t) * 4096, cudaMemcpyHostToDevice, st));
@@ -269,9 +286,18 @@ extern "C" int h264a_pixel_path_host(h264a_ctx* ctx, const uint8_t* h_frames, in
     H264A_CUDA(cudaMemsetAsync(d_costs, 0, sizeof(int64_t) * 2 * nmb, st));
     H264A_CUDA(cudaMemsetAsync(d_coeffs, 0, sizeof(int16_t) * 256 * nmb, st));
     int rc;
-    if (n > 1) {
-        rc = h264a_hpel_build(ctx, d_frames, cw, ch, pad, n - 1, fs, d_planes, st);
+    for (int k = 0; k < nk; k++) {
+        const int a = int((long long)k * n / nk), b = int((long long)(k + 1) * n / nk);
+        H264A_CUDA(cudaStreamWaitEvent(st, ctx->pp_ev[k], 0));
+        const int refs = (b < n - 1 ? b : n - 1) - a;  // reference pictures 0..n-2 in this chunk
+        if (refs > 0) {
+            rc = h264a_hpel_build(ctx, d_frames + fs * a, cw, ch, pad, refs, fs, d_planes + p4 * a, st);
+            if (rc) return rc;
+        }
+        rc = h264a_downsample2x(ctx, d_frames + fs * a, cw, ch, b - a, fs, d_half + hs * a, st);
         if (rc) return rc;
+    }
+    if (n > 1) {
         std::vector<h264a_me_frame> mf(n - 1);
         std::vector<h264a_tq_frame> tf(n - 1);
         for (int f = 1; f < n; f++) {
@@ -284,15 +310,18 @@ extern "C" int h264a_pixel_path_host(h264a_ctx* ctx, const uint8_t* h_frames, in
         rc = h264a_mc_tq_frames(ctx, tf.data(), n - 1, st);
         if (rc) return rc;
     }
-    rc = h264a_downsample2x(ctx, d_frames, cw, ch, n, fs, d_half, st);
-    if (rc) return rc;
+    H264A_CUDA(cudaEventRecord(ctx->pp_ev[PP_CHUNKS], st));
     rc = h264a_lookahead_costs(ctx, d_frames, d_half, cw, ch, n, 2, d_intra, d_inter, d_mvs, st);
     if (rc) return rc;
-    H264A_CUDA(cudaMemcpyAsync(h_picks, d_picks, sizeof(int32_t) * 6 * nmb * n, cudaMemcpyDeviceToHost, st));
-    H264A_CUDA(cudaMemcpyAsync(h_costs, d_costs, sizeof(int64_t) * 2 * nmb * n, cudaMemcpyDeviceToHost, st));
-    H264A_CUDA(cudaMemcpyAsync(h_coeffs, d_coeffs, sizeof(int16_t) * 256 * nmb * n, cudaMemcpyDeviceToHost, st));
-    H264A_CUDA(cudaMemcpyAsync(h_la_intra, d_intra, sizeof(int32_t) * nmb * n, cudaMemcpyDeviceToHost, st));
-    H264A_CUDA(cudaMemcpyAsync(h_la_inter, d_inter, sizeof(int32_t) * nmb * n, cudaMemcpyDeviceToHost, st));
-    H264A_CUDA(cudaMemcpyAsync(h_la_mvs, d_mvs, sizeof(int32_t) * 2 * nmb * n, cudaMemcpyDeviceToHost, st));
+    H264A_CUDA(cudaEventRecord(ctx->pp_ev[PP_CHUNKS + 1], st));
+    H264A_CUDA(cudaStreamWaitEvent(cs, ctx->pp_ev[PP_CHUNKS], 0));
+    H264A_CUDA(cudaMemcpyAsync(h_picks, d_picks, sizeof(int32_t) * 6 * nmb * n, cudaMemcpyDeviceToHost, cs));
+    H264A_CUDA(cudaMemcpyAsync(h_costs, d_costs, sizeof(int64_t) * 2 * nmb * n, cudaMemcpyDeviceToHost, cs));
+    H264A_CUDA(cudaMemcpyAsync(h_coeffs, d_coeffs, sizeof(int16_t) * 256 * nmb * n, cudaMemcpyDeviceToHost, cs));
+    H264A_CUDA(cudaStreamWaitEvent(cs, ctx->pp_ev[PP_CHUNKS + 1], 0));
+    H264A_CUDA(cudaMemcpyAsync(h_la_intra, d_intra, sizeof(int32_t) * nmb * n, cudaMemcpyDeviceToHost, cs));
+    H264A_CUDA(cudaMemcpyAsync(h_la_inter, d_inter, sizeof(int32_t) * nmb * n, cudaMemcpyDeviceToHost, cs));
+    H264A_CUDA(cudaMemcpyAsync(h_la_mvs, d_mvs, sizeof(int32_t) * 2 * nmb * n, cudaMemcpyDeviceToHost, cs));
+    H264A_CUDA(cudaStreamSynchronize(cs));
     return h264a_sync(ctx, st);
 }

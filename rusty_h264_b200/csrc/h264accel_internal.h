@@ -21,10 +21,14 @@ struct h264a_ctx {
     size_t flags_cap = 0;      // MBs the scratch holds
     int32_t *d_status = nullptr;
     int32_t epoch = 0;         // value a finished MB writes into its flag
-    // cached buffers of h264a_pixel_path_host
+    // cached buffers of h264a_pixel_path_host, its copy stream and events
+    // (PP_CHUNKS upload chunks, then T/Q done and lookahead done)
     void *pp_buf = nullptr;
     size_t pp_bytes = 0;
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t pp_ev[6] = {};
 };
+constexpr int PP_CHUNKS = 4;
 
 namespace h264a {
 
