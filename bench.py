@@ -327,8 +327,8 @@ def run_ours(args, ws, rank, local):
     stage = {k: float(np.mean(v)) for k, v in stage_ms.items()}
 
     # The reconstruction side (not part of `value`): MC + T/Q with the luma
-    # reconstruction, and the chroma MC + T/Q + reconstruction, over the same
-    # 59 P frames.  The half-res luma planes of the lookahead stand in for the
+    # reconstruction, the chroma MC + T/Q + reconstruction, and the in-loop
+    # deblocking of the reconstructed pictures, over the same 59 P frames.  The half-res luma planes of the lookahead stand in for the
     # chroma planes (960x544, textured).
     rec = torch.empty((n, ch, cw), dtype=torch.uint8, device=dev)
     ccoef = torch.empty((n, nmb, 128), dtype=torch.int16, device=dev)
@@ -337,17 +337,22 @@ def run_ours(args, ws, rank, local):
     chroma_frames = [A.TqChromaFrame(half[i].data_ptr(), half[i].data_ptr(), half[i - 1].data_ptr(),
                                      half[i - 1].data_ptr(), cw, ch, picks[i].data_ptr(), qp, ccoef[i].data_ptr(),
                                      crec[0, i].data_ptr(), crec[1, i].data_ptr()) for i in range(1, n)]
-    extra = {"mc_tq_rec": [], "chroma_mc_tq_rec": []}
+    db_frames = [A.DeblockFrame(rec[i].data_ptr(), crec[0, i].data_ptr(), crec[1, i].data_ptr(), cw, ch,
+                                picks[i].data_ptr(), coeffs[i].data_ptr(), qp, 0, 0, 0) for i in range(1, n)]
+    extra = {"mc_tq_rec": [], "chroma_mc_tq_rec": [], "deblock": []}
     for _ in range(max(3, args.steps // 2) + 1):
-        a, b, c2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        a, b, c2, d2 = (torch.cuda.Event(enable_timing=True) for _ in range(4))
         a.record(stream)
         acc.mc_tq_rec_frames(rec_frames)
         b.record(stream)
         acc.mc_tq_chroma_frames(chroma_frames)
         c2.record(stream)
+        acc.deblock_frames(db_frames)
+        d2.record(stream)
         torch.cuda.synchronize()
         extra["mc_tq_rec"].append(a.elapsed_time(b))
         extra["chroma_mc_tq_rec"].append(b.elapsed_time(c2))
+        extra["deblock"].append(c2.elapsed_time(d2))
     acc.sync()
     extra_ms = {k: round(float(np.mean(v[1:])), 4) for k, v in extra.items()}
     work4x4 = int(picks[1:, :, 5].sum().item())

@@ -252,6 +252,22 @@ typedef struct {
 H264A_API int h264a_mc_tq_chroma_frames(h264a_ctx *ctx, const h264a_tq_chroma_frame *h_frames, int nframes,
                                         void *stream);
 
+/* In-loop deblocking (crates/rusty_h264-common/src/deblock.rs, filter_frame)
+ * of reconstructed plain-ME P pictures: every MB inter with reference 0,
+ * 4x4 transforms, one QP; bS from the picks and the luma levels (2 with
+ * coefficients on either side, 1 for MVs 4 quarter-pels apart, else 0).  The
+ * planes are filtered in place, MBs in the reference's raster order (as a
+ * wavefront on the GPU); d_u / d_v may both be NULL (luma only). */
+typedef struct {
+    uint8_t *d_y, *d_u, *d_v;  /* cw x ch luma, (cw/2) x (ch/2) chroma, 4-byte aligned */
+    int32_t cw, ch;            /* MB-aligned */
+    const int32_t *d_picks;    /* 6 i32 per MB, as h264a_me_frames writes */
+    const int16_t *d_coeffs;   /* 256 i16 luma levels per MB (h264a_mc_tq_frames), 16-byte aligned */
+    int32_t qp;                /* the picture's QP, 0..51 */
+    int32_t offset_a, offset_b, chroma_qp_offset; /* slice filter offsets and the chroma QP offset */
+} h264a_deblock_frame;
+H264A_API int h264a_deblock_frames(h264a_ctx *ctx, const h264a_deblock_frame *h_frames, int nframes, void *stream);
+
 /* ---- a16-a19: mb-tree lookahead ------------------------------------------ */
 /* downsample2x (encoder/src/mbtree.rs:61-74) of n frames cw x ch -> cw/2 x ch/2. */
 H264A_API int h264a_downsample2x(h264a_ctx *ctx, const uint8_t *d_frames, int cw, int ch, int n, size_t frame_stride,

@@ -256,6 +256,184 @@ void or_mc_tq_chroma_frame(const uint8_t *src_u, const uint8_t *src_v, const uin
         }
 }
 
+/* ---- in-loop deblocking of a plain-ME P picture ---------------------------
+ * crates/rusty_h264-common/src/deblock.rs, restated for the pictures this path
+ * produces: every MB inter with reference 0, 4x4 transforms (no t8x8), one QP.
+ * Spec Tables 8-16/8-17 (deblock.rs:11-41): alpha, beta by indexA/indexB,
+ * tc0 by [indexA][bS-1]. */
+static const int DB_ALPHA[52] = {0,  0,  0,  0,  0,  0,  0,  0,  0,  0,   0,   0,   0,   0,   0,   0,   4,   4,
+                                 5,  6,  7,  8,  9,  10, 12, 13, 15, 17,  20,  22,  25,  28,  32,  36,  40,  45,
+                                 50, 56, 63, 71, 80, 90, 101, 113, 127, 144, 162, 182, 203, 226, 255, 255};
+static const int DB_BETA[52] = {0, 0, 0, 0, 0, 0, 0, 0,  0,  0,  0,  0,  0,  0,  0,  0,  2,  2,  2,  3,  3,  3,  3,  4,  4,  4,
+                                6, 6, 7, 7, 8, 8, 9, 9, 10, 10, 11, 11, 12, 12, 13, 13, 14, 14, 15, 15, 16, 16, 17, 17, 18, 18};
+static const int DB_TC0[52][3] = {
+    {0, 0, 0},  {0, 0, 0},  {0, 0, 0},   {0, 0, 0},   {0, 0, 0},   {0, 0, 0},   {0, 0, 0},   {0, 0, 0},
+    {0, 0, 0},  {0, 0, 0},  {0, 0, 0},   {0, 0, 0},   {0, 0, 0},   {0, 0, 0},   {0, 0, 0},   {0, 0, 0},
+    {0, 0, 0},  {0, 0, 1},  {0, 0, 1},   {0, 0, 1},   {0, 0, 1},   {0, 1, 1},   {0, 1, 1},   {1, 1, 1},
+    {1, 1, 1},  {1, 1, 1},  {1, 1, 1},   {1, 1, 2},   {1, 1, 2},   {1, 1, 2},   {1, 1, 2},   {1, 2, 3},
+    {1, 2, 3},  {2, 2, 3},  {2, 2, 4},   {2, 3, 4},   {2, 3, 4},   {3, 3, 5},   {3, 4, 6},   {3, 4, 6},
+    {4, 5, 7},  {4, 5, 8},  {4, 6, 9},   {5, 7, 10},  {6, 8, 11},  {6, 8, 13},  {7, 10, 14}, {8, 11, 16},
+    {9, 12, 18}, {10, 13, 20}, {11, 15, 23}, {13, 17, 25}};
+
+void or_deblock_tables(int32_t *alpha, int32_t *beta, int32_t *tc0) {
+    for (int i = 0; i < 52; i++) {
+        alpha[i] = DB_ALPHA[i];
+        beta[i] = DB_BETA[i];
+        for (int k = 0; k < 3; k++) tc0[3 * i + k] = DB_TC0[i][k];
+    }
+}
+
+static int db_clip1(int v) { return v < 0 ? 0 : (v > 255 ? 255 : v); }
+static int db_clip3(int lo, int hi, int v) { return v < lo ? lo : (v > hi ? hi : v); }
+static int db_abs(int v) { return v < 0 ? -v : v; }
+
+/* filter_luma_line (deblock.rs:67-115): one line across an edge, q0 at p[0],
+ * samples `step` apart. */
+static void db_luma_line(uint8_t *q, int64_t step, int bs, int alpha, int beta, int tc0) {
+    int p0 = q[-step], p1 = q[-2 * step], p2 = q[-3 * step], p3 = q[-4 * step];
+    int q0 = q[0], q1 = q[step], q2 = q[2 * step], q3 = q[3 * step];
+    if (db_abs(p0 - q0) >= alpha || db_abs(p1 - p0) >= beta || db_abs(q1 - q0) >= beta) return;
+    int ap = db_abs(p2 - p0), aq = db_abs(q2 - q0);
+    if (bs < 4) {
+        int tc = tc0 + (ap < beta) + (aq < beta);
+        int delta = db_clip3(-tc, tc, (((q0 - p0) << 2) + (p1 - q1) + 4) >> 3);
+        q[-step] = (uint8_t)db_clip1(p0 + delta);
+        q[0] = (uint8_t)db_clip1(q0 - delta);
+        if (ap < beta) q[-2 * step] = (uint8_t)db_clip1(p1 + db_clip3(-tc0, tc0, (p2 + ((p0 + q0 + 1) >> 1) - (p1 << 1)) >> 1));
+        if (aq < beta) q[step] = (uint8_t)db_clip1(q1 + db_clip3(-tc0, tc0, (q2 + ((p0 + q0 + 1) >> 1) - (q1 << 1)) >> 1));
+    } else {
+        int strong = db_abs(p0 - q0) < (alpha >> 2) + 2;
+        if (strong && ap < beta) {
+            q[-step] = (uint8_t)db_clip1((p2 + 2 * p1 + 2 * p0 + 2 * q0 + q1 + 4) >> 3);
+            q[-2 * step] = (uint8_t)db_clip1((p2 + p1 + p0 + q0 + 2) >> 2);
+            q[-3 * step] = (uint8_t)db_clip1((2 * p3 + 3 * p2 + p1 + p0 + q0 + 4) >> 3);
+        } else {
+            q[-step] = (uint8_t)db_clip1((2 * p1 + p0 + q1 + 2) >> 2);
+        }
+        if (strong && aq < beta) {
+            q[0] = (uint8_t)db_clip1((q2 + 2 * q1 + 2 * q0 + 2 * p0 + p1 + 4) >> 3);
+            q[step] = (uint8_t)db_clip1((q2 + q1 + q0 + p0 + 2) >> 2);
+            q[2 * step] = (uint8_t)db_clip1((2 * q3 + 3 * q2 + q1 + q0 + p0 + 4) >> 3);
+        } else {
+            q[0] = (uint8_t)db_clip1((2 * q1 + q0 + p1 + 2) >> 2);
+        }
+    }
+}
+
+/* filter_chroma_line (deblock.rs:117-137). */
+static void db_chroma_line(uint8_t *q, int64_t step, int bs, int alpha, int beta, int tc0) {
+    int p0 = q[-step], p1 = q[-2 * step], q0 = q[0], q1 = q[step];
+    if (db_abs(p0 - q0) >= alpha || db_abs(p1 - p0) >= beta || db_abs(q1 - q0) >= beta) return;
+    if (bs < 4) {
+        int tc = tc0 + 1;
+        int delta = db_clip3(-tc, tc, (((q0 - p0) << 2) + (p1 - q1) + 4) >> 3);
+        q[-step] = (uint8_t)db_clip1(p0 + delta);
+        q[0] = (uint8_t)db_clip1(q0 - delta);
+    } else {
+        q[-step] = (uint8_t)db_clip1((2 * p1 + p0 + q1 + 2) >> 2);
+        q[0] = (uint8_t)db_clip1((2 * q1 + q0 + p1 + 2) >> 2);
+    }
+}
+
+/* thresholds (deblock.rs:1921-1929). */
+static void db_thresholds(int qpav, int oa, int ob, int *alpha, int *beta, const int **tc0) {
+    int ia = db_clip3(0, 51, qpav + oa), ib = db_clip3(0, 51, qpav + ob);
+    *alpha = DB_ALPHA[ia];
+    *beta = DB_BETA[ib];
+    *tc0 = DB_TC0[ia];
+}
+
+/* bS of an edge between two inter blocks, both ref 0 (bs_inter + bs1_tile's
+ * single-list arm, deblock.rs:328-333, 396-404): 2 with coefficients on either
+ * side, else 1 when the MVs differ by 4 quarter-pels in x or y, else 0. */
+static int db_bs(int nzp, int nzq, int32_t pmx, int32_t pmy, int32_t qmx, int32_t qmy) {
+    if (nzp || nzq) return 2;
+    return (db_abs(pmx - qmx) >= 4 || db_abs(pmy - qmy) >= 4) ? 1 : 0;
+}
+
+/* The MV and coefficient flag of 4x4 block (bx, by) of MB m. */
+static void db_block(const int32_t *picks, const int16_t *coeffs, int m, int bx, int by, int32_t mv[2], int *nz) {
+    const int32_t *pk = picks + 6 * m;
+    int part = pk[0] == 1 ? (by >= 2) : (pk[0] == 2 ? (bx >= 2) : 0);
+    mv[0] = pk[1 + 2 * part];
+    mv[1] = pk[2 + 2 * part];
+    int qi = (by >= 2 ? 2 : 0) + (bx >= 2 ? 1 : 0), k = (by & 1) * 2 + (bx & 1);
+    const int16_t *c = coeffs + (int64_t)m * 256 + (qi * 4 + k) * 16;
+    *nz = 0;
+    for (int i = 0; i < 16; i++) *nz |= c[i] != 0;
+}
+
+/* filter_frame_rows (deblock.rs:2135-2700) over the plain-ME picture: MBs in
+ * raster order; per MB the luma vertical edges (block columns 0..3, the MB
+ * edge skipped at the picture's left), then the horizontal ones, then per
+ * chroma plane its vertical edges (chroma columns 0 and 4, bS of luma edges 0
+ * and 2, one segment per two chroma lines) and horizontal edges; MB edges
+ * average the two MBs' QPs (equal here), chroma uses chroma_qp(qp + offset).
+ * u and v may be NULL (luma only). */
+void or_deblock_frame_plain(uint8_t *y, uint8_t *u, uint8_t *v, int cw, int ch, const int32_t *picks,
+                            const int16_t *coeffs, int qp, int offset_a, int offset_b, int chroma_qp_offset) {
+    int mb_w = cw / 16, mb_h = ch / 16, ccw = cw / 2;
+    int qpc = or_chroma_qp(db_clip3(0, 51, qp + chroma_qp_offset));
+    int ay, by_, ac, bc;
+    const int *ty, *tc;
+    db_thresholds(qp, offset_a, offset_b, &ay, &by_, &ty);  /* (qp + qp + 1) >> 1 == qp on MB edges too */
+    db_thresholds(qpc, offset_a, offset_b, &ac, &bc, &tc);
+    for (int mby = 0; mby < mb_h; mby++)
+        for (int mbx = 0; mbx < mb_w; mbx++) {
+            int m = mby * mb_w + mbx;
+            int bs_v[4][4], bs_h[4][4];
+            for (int e = 0; e < 4; e++)
+                for (int sg = 0; sg < 4; sg++) {
+                    int32_t mp[2], mq[2];
+                    int nzp, nzq;
+                    /* vertical edge e, block row sg */
+                    bs_v[e][sg] = 0;
+                    if (e > 0 || mbx > 0) {
+                        db_block(picks, coeffs, e > 0 ? m : m - 1, e > 0 ? e - 1 : 3, sg, mp, &nzp);
+                        db_block(picks, coeffs, m, e, sg, mq, &nzq);
+                        bs_v[e][sg] = db_bs(nzp, nzq, mp[0], mp[1], mq[0], mq[1]);
+                    }
+                    /* horizontal edge e, block column sg */
+                    bs_h[e][sg] = 0;
+                    if (e > 0 || mby > 0) {
+                        db_block(picks, coeffs, e > 0 ? m : m - mb_w, sg, e > 0 ? e - 1 : 3, mp, &nzp);
+                        db_block(picks, coeffs, m, sg, e, mq, &nzq);
+                        bs_h[e][sg] = db_bs(nzp, nzq, mp[0], mp[1], mq[0], mq[1]);
+                    }
+                }
+            for (int e = 0; e < 4; e++)
+                for (int sg = 0; sg < 4; sg++) {
+                    int bs = bs_v[e][sg];
+                    if (!bs) continue;
+                    for (int r = 0; r < 4; r++)
+                        db_luma_line(y + (int64_t)(mby * 16 + sg * 4 + r) * cw + mbx * 16 + e * 4, 1, bs, ay, by_, ty[bs - 1]);
+                }
+            for (int e = 0; e < 4; e++)
+                for (int sg = 0; sg < 4; sg++) {
+                    int bs = bs_h[e][sg];
+                    if (!bs) continue;
+                    for (int c = 0; c < 4; c++)
+                        db_luma_line(y + (int64_t)(mby * 16 + e * 4) * cw + mbx * 16 + sg * 4 + c, cw, bs, ay, by_, ty[bs - 1]);
+                }
+            for (int pl = 0; pl < 2; pl++) {
+                uint8_t *cp = pl == 0 ? u : v;
+                if (!cp) continue;
+                for (int ce = 0; ce < 4; ce += 2)
+                    for (int r = 0; r < 8; r++) {
+                        int bs = bs_v[ce][(r * 2) / 4];
+                        if (!bs) continue;
+                        db_chroma_line(cp + (int64_t)(mby * 8 + r) * ccw + mbx * 8 + ce * 2, 1, bs, ac, bc, tc[bs - 1]);
+                    }
+                for (int ce = 0; ce < 4; ce += 2)
+                    for (int c = 0; c < 8; c++) {
+                        int bs = bs_h[ce][(c * 2) / 4];
+                        if (!bs) continue;
+                        db_chroma_line(cp + (int64_t)(mby * 8 + ce * 2) * ccw + mbx * 8 + c, ccw, bs, ac, bc, tc[bs - 1]);
+                    }
+            }
+        }
+}
+
 typedef struct {
     const uint8_t *frames;
     uint8_t *half;

@@ -210,6 +210,28 @@ def mc_tq_chroma_frame(src_u, src_v, ref_u, ref_v, picks, qp, rec=True):
     return out, ru, rv
 
 
+def deblock_frame(y, u, v, picks, coeffs, qp, offset_a=0, offset_b=0, chroma_qp_offset=0):
+    """In-loop deblocking of a plain-ME picture: returns filtered copies of
+    (y, u, v); u and v may be None."""
+    ch, cw = y.shape
+    yo = np.array(y, np.uint8, copy=True)
+    uo = None if u is None else np.array(u, np.uint8, copy=True)
+    vo = None if v is None else np.array(v, np.uint8, copy=True)
+    lib().or_deblock_frame_plain(ptr(yo), None if uo is None else ptr(uo), None if vo is None else ptr(vo), cw, ch,
+                                 ptr(np.ascontiguousarray(picks), i32p),
+                                 ptr(np.ascontiguousarray(coeffs, np.int16), i16p), int(qp), int(offset_a),
+                                 int(offset_b), int(chroma_qp_offset))
+    return yo, uo, vo
+
+
+def deblock_tables():
+    a = np.zeros(52, np.int32)
+    b = np.zeros(52, np.int32)
+    t = np.zeros((52, 3), np.int32)
+    lib().or_deblock_tables(ptr(a, i32p), ptr(b, i32p), ptr(t, i32p))
+    return a, b, t
+
+
 def mc_chroma(ref: np.ndarray, x0, y0, bw, bh, mvx, mvy) -> np.ndarray:
     ch, cw = ref.shape
     out = np.zeros((bh, bw), np.uint8)

@@ -76,6 +76,12 @@ class TqRecFrame(C.Structure):
     _fields_ = [("tq", TqFrame), ("d_rec", C.c_void_p)]
 
 
+class DeblockFrame(C.Structure):
+    _fields_ = [("d_y", C.c_void_p), ("d_u", C.c_void_p), ("d_v", C.c_void_p), ("cw", C.c_int32), ("ch", C.c_int32),
+                ("d_picks", C.c_void_p), ("d_coeffs", C.c_void_p), ("qp", C.c_int32), ("offset_a", C.c_int32),
+                ("offset_b", C.c_int32), ("chroma_qp_offset", C.c_int32)]
+
+
 class TqChromaFrame(C.Structure):
     _fields_ = [("d_src_u", C.c_void_p), ("d_src_v", C.c_void_p), ("d_ref_u", C.c_void_p), ("d_ref_v", C.c_void_p),
                 ("cw", C.c_int32), ("ch", C.c_int32), ("d_picks", C.c_void_p), ("qp", C.c_int32),
@@ -90,7 +96,7 @@ EXPORTS = (
     "h264a_me_search", "h264a_me_frames", "h264a_fullpel_grid", "h264a_dct_quant_4x4", "h264a_dct_quant_8x8",
     "h264a_mc_tq_frames", "h264a_downsample2x", "h264a_lookahead_costs", "h264a_pixel_path_host",
     "h264a_selftest_bounded_wait", "h264a_measure_int32_peak", "h264a_me_frames_noalloc",
-    "h264a_mc_tq_rec_frames", "h264a_mc_tq_chroma_frames",
+    "h264a_mc_tq_rec_frames", "h264a_mc_tq_chroma_frames", "h264a_deblock_frames",
 )
 
 _lib = None
@@ -125,6 +131,7 @@ def load_library() -> C.CDLL:
     L.h264a_mc_tq_frames.argtypes = [vp, vp, i32, vp]
     L.h264a_mc_tq_rec_frames.argtypes = [vp, vp, i32, vp]
     L.h264a_mc_tq_chroma_frames.argtypes = [vp, vp, i32, vp]
+    L.h264a_deblock_frames.argtypes = [vp, vp, i32, vp]
     L.h264a_downsample2x.argtypes = [vp, vp, i32, i32, i32, sz, vp, vp]
     L.h264a_lookahead_costs.argtypes = [vp, vp, vp, i32, i32, i32, i32, vp, vp, vp, vp]
     L.h264a_pixel_path_host.argtypes = [vp, vp, i32, i32, i32, C.POINTER(MeParams), vp, f64, i64, i32, i32, vp, vp, vp,
@@ -316,6 +323,10 @@ class Accel:
     def mc_tq_frames(self, frames: Sequence[TqFrame]):
         arr = (TqFrame * len(frames))(*frames)
         self._check(self.L.h264a_mc_tq_frames(self.ctx, C.cast(arr, C.c_void_p), len(frames), self._stream()))
+
+    def deblock_frames(self, frames: Sequence[DeblockFrame]):
+        arr = (DeblockFrame * len(frames))(*frames)
+        self._check(self.L.h264a_deblock_frames(self.ctx, C.cast(arr, C.c_void_p), len(frames), self._stream()))
 
     def mc_tq_chroma_frames(self, frames: Sequence[TqChromaFrame]):
         arr = (TqChromaFrame * len(frames))(*frames)

@@ -590,50 +590,6 @@ struct FrameBatch {
     int n;
 };
 
-constexpr int SPIN_LIMIT = 1000 * 1000;  // ~0.5 s of polling (a 200 ns sleep per poll)
-
-// Number of MBs (x, y) of a W x H frame with x + 2y < t: rows y < a are
-// full (t - 2y >= W), rows a <= y < b hold t - 2y MBs.
-__device__ __forceinline__ int wave_prefix(int W, int H, int t) {
-    const int a = t >= W ? min((t - W) / 2 + 1, H) : 0;
-    const int b = t >= 1 ? min((t - 1) / 2 + 1, H) : 0;
-    return a * W + (b - a) * t - (b - a) * (a + b - 1);
-}
-
-// The k-th MB of a W x H frame in wavefront order.
-__device__ __forceinline__ void wave_mb(int W, int H, int k, int& x, int& y) {
-    int lo = 0, hi = (W - 1) + 2 * (H - 1);  // find the diagonal t with prefix(t) <= k < prefix(t+1)
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (wave_prefix(W, H, mid) <= k) lo = mid; else hi = mid - 1;
-    }
-    const int t = lo;
-    const int ylo = t - (W - 1) > 0 ? (t - (W - 1) + 1) >> 1 : 0;
-    y = ylo + (k - wave_prefix(W, H, t));
-    x = t - 2 * y;
-}
-
-__device__ __forceinline__ int ld_acquire(const int* p) {
-    int v;
-    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-__device__ __forceinline__ void st_release(int* p, int v) {
-    asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-
-// Waits (bounded) until flag == epoch; on timeout records `code` in status.
-__device__ void wait_flag(const int* flag, int epoch, int* status, int code, int limit) {
-    for (int it = 0;; it++) {
-        if (ld_acquire(flag) == epoch) return;
-        if (it >= limit) {
-            atomicCAS(status, 0, code);
-            return;
-        }
-        __nanosleep(200);
-    }
-}
-
 // mbarrier and bulk-copy primitives (shared addresses are 32-bit).
 __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");

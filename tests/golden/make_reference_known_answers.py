@@ -32,10 +32,29 @@ def extract_quant_mf_oh(ref_root: str):
     return table, f"crates/rusty_h264-common/src/transform.rs:{line}"
 
 
+def extract_deblock_tables(ref_root: str):
+    """ALPHA[52], BETA[52] and TC0[52][3] (spec Tables 8-16/8-17) as the
+    reference's deblock.rs holds them."""
+    path = "crates/rusty_h264-common/src/deblock.rs"
+    src = open(os.path.join(ref_root, path)).read()
+    out = {}
+    for name in ("ALPHA", "BETA"):
+        m = re.search(r"const " + name + r": \[i32; 52\] = \[(.*?)\];", src, re.S)
+        vals = [int(v) for v in m.group(1).replace("\n", " ").split(",") if v.strip()]
+        assert len(vals) == 52
+        out[name.lower()] = {"source": f"{path}:{src[: m.start()].count(chr(10)) + 1}", "values": vals}
+    m = re.search(r"const TC0: \[\[i32; 3\]; 52\] = \[(.*?)\n\];", src, re.S)
+    rows = [[int(v) for v in r.split(",")] for r in re.findall(r"\[([0-9,\s]+)\]", m.group(1))]
+    assert len(rows) == 52 and all(len(r) == 3 for r in rows)
+    out["tc0"] = {"source": f"{path}:{src[: m.start()].count(chr(10)) + 1}", "rows": rows}
+    return out
+
+
 def main(ref_root: str):
     qmf, qmf_src = extract_quant_mf_oh(ref_root)
     out = {
         "quant_mf_oh": {"source": qmf_src, "rows": qmf},
+        "deblock": extract_deblock_tables(ref_root),
         "median3": {
             "source": "crates/rusty_h264-common/src/inter.rs:1994-1999 (median_of_three)",
             "cases": [[1, 2, 3, 2], [3, 1, 2, 2], [-5, 0, 5, 0], [7, 7, 2, 7]],

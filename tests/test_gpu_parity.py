@@ -516,6 +516,53 @@ def test_mc_tq_chroma_frames_matches_oracle(acc, qp):
             assert np.array_equal(ru.cpu().numpy(), wu) and np.array_equal(rv.cpu().numpy(), wv), (qp, f)
 
 
+@pytest.mark.parametrize("qp,offs", [(22, (0, 0, 0)), (30, (0, 0, 0)), (36, (2, -1, 3)), (45, (-2, 3, -4)), (51, (0, 0, 0))])
+def test_deblock_frames_matches_oracle(acc, qp, offs):
+    """In-loop deblocking of reconstructed plain-ME pictures, bit-exact with
+    the oracle: three CIF pictures with chroma and a 160x96 one luma-only, in
+    one wavefront launch; picks forced through every shape on one picture."""
+    y, _, _ = synth.cif_clip(4, 2)
+    luma = synth.coded_luma(y)
+    half = np.stack([O.downsample2x(a) for a in luma])
+    lam = float(np.sqrt(A.frame_lambda(qp)))
+    frames, keep, cases = [], [], []
+    for f in (1, 2, 3, 4):
+        small = f == 4
+        src, ref = (np.ascontiguousarray(luma[1, 64:160, 96:256]), np.ascontiguousarray(luma[0, 64:160, 96:256])) \
+            if small else (luma[f], luma[f - 1])
+        picks, _ = O.me_frame(src, ref, O.build_planes4(ref, 32), O.balanced_params(), lam, A.split_gate_for_qp(qp))
+        if f == 2:
+            picks[::3, 0] = 1
+            picks[1::3, 0] = 2
+            picks[:, 3] = picks[:, 1] + 5
+            picks[:, 4] = picks[:, 2] - 3
+        coeffs, rec = O.mc_tq_rec_frame(src, ref, picks, qp, 6)
+        ch, cw = src.shape
+        if small:
+            ru = rv = None
+        else:
+            _, ru, rv = O.mc_tq_chroma_frame(half[f], 255 - half[f], half[f - 1], 255 - half[f - 1], picks, qp)
+        dy = dev(acc, rec)
+        du, dv = (dev(acc, ru), dev(acc, rv)) if ru is not None else (None, None)
+        dp, dc = dev(acc, picks), dev(acc, coeffs)
+        keep += [dy, du, dv, dp, dc]
+        cases.append((dy, du, dv, rec, ru, rv, picks, coeffs))
+        frames.append(A.DeblockFrame(dy.data_ptr(), du.data_ptr() if du is not None else None,
+                                     dv.data_ptr() if dv is not None else None, cw, ch, dp.data_ptr(), dc.data_ptr(),
+                                     qp, *offs))
+    acc.deblock_frames(frames)
+    acc.sync()
+    changed = 0
+    for dy, du, dv, rec, ru, rv, picks, coeffs in cases:
+        wy, wu, wv = O.deblock_frame(rec, ru, rv, picks, coeffs, qp, *offs)
+        got = dy.cpu().numpy()
+        assert np.array_equal(got, wy), qp
+        changed += int((wy != rec).sum())
+        if du is not None:
+            assert np.array_equal(du.cpu().numpy(), wu) and np.array_equal(dv.cpu().numpy(), wv), qp
+    assert changed > 0  # the filter did something on these pictures
+
+
 # ---------------------------------------------------------------------------
 # a16-a19 lookahead
 # ---------------------------------------------------------------------------

@@ -532,3 +532,78 @@ def test_chroma_dc_end_to_end_flat_block():
                 for v in O.inverse_core4([int(d)] + [0] * 15):
                     assert abs(int(v) - r) <= tol, (r, qp)
 
+
+# ---------------------------------------------------------------------------
+# in-loop deblocking (deblock.rs) of plain-ME pictures
+# ---------------------------------------------------------------------------
+
+def test_deblock_tables_match_reference():
+    """ALPHA, BETA and TC0 as extracted from the reference's deblock.rs."""
+    g = GOLD["deblock"]
+    a, b, t = O.deblock_tables()
+    assert list(a) == g["alpha"]["values"] and list(b) == g["beta"]["values"] and t.tolist() == g["tc0"]["rows"]
+
+
+def _plain_picks(nmb, mv=(0, 0)):
+    p = np.zeros((nmb, 6), np.int32)
+    p[:, 1], p[:, 2], p[:, 3], p[:, 4] = mv[0], mv[1], mv[0], mv[1]
+    return p
+
+
+def test_deblock_leaves_flat_and_unfiltered_pictures():
+    """A flat picture has nothing to smooth; a picture with no coefficients
+    and one MV everywhere has bS 0 on every edge."""
+    rng = np.random.default_rng(2)
+    nmb = 6 * 4
+    flat = np.full((64, 96), 77, np.uint8)
+    co = np.zeros((nmb, 256), np.int16)
+    co[::3, 5] = 7
+    y, u, v = O.deblock_frame(flat, flat[:32, :48], flat[:32, :48], _plain_picks(nmb), co, 30)
+    assert (y == 77).all() and (u == 77).all() and (v == 77).all()
+    tex = rng.integers(0, 256, (64, 96)).astype(np.uint8)
+    y, _, _ = O.deblock_frame(tex, None, None, _plain_picks(nmb, (8, -4)), np.zeros((nmb, 256), np.int16), 40)
+    assert np.array_equal(y, tex)
+
+
+def np_luma_line(line, bs, alpha, beta, tc0):
+    """filter_luma_line (deblock.rs:67-115) on p3 p2 p1 p0 q0 q1 q2 q3."""
+    p3, p2, p1, p0, q0, q1, q2, q3 = (int(v) for v in line)
+    out = list(line)
+    clip1 = lambda v: min(255, max(0, v))
+    clip3 = lambda lo, hi, v: min(hi, max(lo, v))
+    if abs(p0 - q0) >= alpha or abs(p1 - p0) >= beta or abs(q1 - q0) >= beta:
+        return out
+    ap, aq = abs(p2 - p0), abs(q2 - q0)
+    tc = tc0 + (ap < beta) + (aq < beta)
+    delta = clip3(-tc, tc, (((q0 - p0) << 2) + (p1 - q1) + 4) >> 3)
+    out[3], out[4] = clip1(p0 + delta), clip1(q0 - delta)
+    if ap < beta:
+        out[2] = clip1(p1 + clip3(-tc0, tc0, (p2 + ((p0 + q0 + 1) >> 1) - (p1 << 1)) >> 1))
+    if aq < beta:
+        out[5] = clip1(q1 + clip3(-tc0, tc0, (q2 + ((p0 + q0 + 1) >> 1) - (q1 << 1)) >> 1))
+    return out
+
+
+def test_deblock_single_mb_edge_matches_line_filter():
+    """Two MBs side by side, coefficients only in the right MB's first block
+    column: bS 2 on the MB edge's rows of that block and on its internal edge,
+    0 elsewhere.  Each filtered line equals filter_luma_line restated here."""
+    rng = np.random.default_rng(8)
+    base = rng.integers(90, 110, (16, 32)).astype(np.int32)
+    base[:, 16:] += 12  # a step at the MB edge
+    y = base.astype(np.uint8)
+    co = np.zeros((2, 256), np.int16)
+    co[1, 0] = 3  # MB 1, region 0, sub-block 0: block (0, 0)
+    qp = 36
+    a, b, t = O.deblock_tables()
+    got, _, _ = O.deblock_frame(y, None, None, _plain_picks(2), co, qp)
+    want = y.astype(np.int32).copy()
+    # vertical MB edge x=16, rows 0..3 (block row 0) bS 2; internal edge x=20 rows 0..3 bS 2
+    for x in (16, 20):
+        for r in range(4):
+            want[r, x - 4:x + 4] = np_luma_line(want[r, x - 4:x + 4], 2, a[qp], b[qp], t[qp][1])
+    # horizontal internal edge y=4 at columns 16..19 (block (0,0) above block (0,1)) bS 2
+    for c in range(16, 20):
+        want[0:8, c] = np_luma_line(want[0:8, c], 2, a[qp], b[qp], t[qp][1])
+    assert np.array_equal(got.astype(np.int32), want)
+
