@@ -6,9 +6,11 @@
 //  * inter_cost + frame_costs: the seeded full-pel diamond.  The seed chain
 //    (left MV, else top MV; mbtree.rs:225-231) makes every row a sequential
 //    chain that starts from column 0, and column 0 a chain down the frame.
-//    Frames are independent (source domain, f against f-1), so one warp walks
-//    the column-0 chain of each frame, then one warp per (frame, row) walks
-//    the rest of the row.  Inside a search the warp prices the four ring
+//    Frames are independent (source domain, f against f-1).  One persistent
+//    kernel deals the column-0 chains first (one warp per frame, publishing
+//    each MB's flag as it finishes), then the rows in row order across frames:
+//    a row's warp waits (bounded) only for its own column-0 MB, so rows start
+//    while column 0 is still walking down the frame.  Inside a search the warp prices the four ring
 //    points of the cascading diamond together and takes the first improvement,
 //    re-pricing the rest of the ring around the moved centre (the reference's
 //    evaluation order).
@@ -221,38 +223,52 @@ __device__ void la_mb(const LaBufs& b, int f, int mbx, int mby, int sfx, int sfy
 
 constexpr int LA_WARPS = 4;
 
-// Column 0 of every frame f >= 1 (one warp per frame).
-__global__ void __launch_bounds__(32 * LA_WARPS) la_col0_kernel(LaBufs b) {
+// Column-0 chains and row chains in one persistent launch: tickets 0..n-2
+// walk column 0 of frames 1..n-1 and publish flag (f-1)*mb_h + y after MB
+// (0, y); later tickets take row y of frame f (rows in order, frames
+// interleaved), wait for that flag and walk columns 1.. seeded by the left
+// neighbour.
+__global__ void __launch_bounds__(32 * LA_WARPS) la_chains_kernel(LaBufs b, int* __restrict__ counter,
+                                                                 int* __restrict__ flags, int epoch,
+                                                                 int* __restrict__ status, int spin_limit) {
     __shared__ int2 cs[LA_WARPS][32];
     __shared__ int ds[LA_WARPS][32];
     const int w = threadIdx.x >> 5;
-    const int f = 1 + blockIdx.x * LA_WARPS + w;
-    if (f >= b.n) return;
-    int sx = 0, sy = 0;
-    for (int mby = 0; mby < b.mb_h; mby++) {
-        int mx, my;
-        la_mb(b, f, 0, mby, sx, sy, cs[w], ds[w], mx, my);
-        sx = mx;
-        sy = my;
-    }
-}
-
-// Columns 1.. of every row of every frame f >= 1 (one warp per row), seeded by
-// the left neighbour (column 0 comes from la_col0_kernel).
-__global__ void __launch_bounds__(32 * LA_WARPS) la_rows_kernel(LaBufs b) {
-    __shared__ int2 cs[LA_WARPS][32];
-    __shared__ int ds[LA_WARPS][32];
-    const int w = threadIdx.x >> 5;
-    const long long r = (long long)blockIdx.x * LA_WARPS + w;  // (frame-1) * mb_h + row
-    if (r >= (long long)(b.n - 1) * b.mb_h) return;
-    const int f = 1 + int(r / b.mb_h), mby = int(r % b.mb_h);
-    const long long gm0 = (long long)b.mb_w * b.mb_h * f + (long long)mby * b.mb_w;
-    int sx = b.mvs[2 * gm0], sy = b.mvs[2 * gm0 + 1];
-    for (int mbx = 1; mbx < b.mb_w; mbx++) {
-        int mx, my;
-        la_mb(b, f, mbx, mby, sx, sy, cs[w], ds[w], mx, my);
-        sx = mx;
-        sy = my;
+    const int lane = threadIdx.x & 31;
+    const int nf = b.n - 1;
+    for (;;) {
+        int t = 0;
+        if (lane == 0) t = atomicAdd(counter, 1);
+        t = __shfl_sync(0xffffffffu, t, 0);
+        if (t < nf) {
+            const int f = 1 + t;
+            int sx = 0, sy = 0;
+            for (int mby = 0; mby < b.mb_h; mby++) {
+                int mx, my;
+                la_mb(b, f, 0, mby, sx, sy, cs[w], ds[w], mx, my);
+                sx = mx;
+                sy = my;
+                if (lane == 0) {
+                    __threadfence();
+                    st_release(flags + (f - 1) * b.mb_h + mby, epoch);
+                }
+                __syncwarp();
+            }
+            continue;
+        }
+        const long long r = (long long)t - nf;
+        if (r >= (long long)nf * b.mb_h) return;
+        const int mby = int(r / nf), f = 1 + int(r % nf);
+        if (lane == 0) wait_flag(flags + (f - 1) * b.mb_h + mby, epoch, status, 1, spin_limit);
+        __syncwarp();
+        const long long gm0 = (long long)b.mb_w * b.mb_h * f + (long long)mby * b.mb_w;
+        int sx = __ldcg(b.mvs + 2 * gm0), sy = __ldcg(b.mvs + 2 * gm0 + 1);
+        for (int mbx = 1; mbx < b.mb_w; mbx++) {
+            int mx, my;
+            la_mb(b, f, mbx, mby, sx, sy, cs[w], ds[w], mx, my);
+            sx = mx;
+            sy = my;
+        }
     }
 }
 
@@ -290,10 +306,19 @@ extern "C" int h264a_lookahead_costs(h264a_ctx* ctx, const uint8_t* d_full, cons
                                                                     ch / 16, n, d_intra, d_inter, d_mvs);
     int rc = check_launch("la_intra_kernel");
     if (rc || n < 2) return rc;
-    la_col0_kernel<<<unsigned((n - 1 + LA_WARPS - 1) / LA_WARPS), 32 * LA_WARPS, 0, st>>>(b);
-    rc = check_launch("la_col0_kernel");
+    const long long chains = (long long)(n - 1) * (1 + ch / 16);
+    if ((long long)(n - 1) * (ch / 16) > (1 << 24)) return fail(H264A_E_ARG, "lookahead_costs: too many rows");
+    rc = ensure_me_scratch(ctx, size_t(n - 1) * (ch / 16));
     if (rc) return rc;
-    const long long rows = (long long)(n - 1) * (ch / 16);
-    la_rows_kernel<<<unsigned((rows + LA_WARPS - 1) / LA_WARPS), 32 * LA_WARPS, 0, st>>>(b);
-    return check_launch("la_rows_kernel");
+    H264A_CUDA(cudaMemsetAsync(ctx->d_counter, 0, sizeof(int32_t), st));
+    const int epoch = next_epoch(ctx, st);
+    if (epoch < 0) return H264A_E_CUDA;
+    int per_sm = 0;
+    H264A_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, la_chains_kernel, 32 * LA_WARPS, 0));
+    long long blocks = (long long)ctx->num_sms * (per_sm > 0 ? per_sm : 1);
+    const long long need = (chains + LA_WARPS - 1) / LA_WARPS;
+    if (blocks > need) blocks = need;
+    la_chains_kernel<<<unsigned(blocks), 32 * LA_WARPS, 0, st>>>(b, ctx->d_counter, ctx->d_flags, epoch, ctx->d_status,
+                                                                SPIN_LIMIT);
+    return check_launch("la_chains_kernel");
 }
