@@ -515,6 +515,379 @@ __device__ __forceinline__ void motion_search_warp(const SearchGeom& g, const Me
     out_x = bx; out_y = by; out_c = best_c;
 }
 
+// ---------------------------------------------------------------------------
+// Searches of one MB in lane groups
+// ---------------------------------------------------------------------------
+// The plain-ME frame pass runs best_part's searches of an MB with this one
+// search body: first the 16x16 search with the whole warp as one group (one
+// lane per 4x4 block, two candidates per pass); then, when the 16x16 J
+// exceeds the gate, the four partition searches (16x8 top, 16x8 bottom,
+// 8x16 left, 8x16 right) side by side, lane group g = lane / 8 searching
+// partition g with one candidate per pass.  The partitions share their seeds
+// [pmv, mv16], mvd centre and λ (mb16.rs:8869-8913), so the four searches are
+// independent; each group carries its own copy of the search state (the
+// state machine of motion_search_warp, every decision taken per group) and
+// the warp loops until every group is done.  Candidates and distortions of a
+// group live in its slots ws.cand / ws.dist [gb, gb + group size).
+
+struct GroupGeom {
+    SearchGeom s;     // the lane's partition origin, its 4x4 block, window offsets, source rows
+    int rw, rh;       // partition size
+    int gb;           // first slot of the lane's group
+    int gl;           // lane within the group
+    int lg;           // log2 lanes per group (5: one group, 3: four groups)
+    unsigned gmask;   // the group's bits in a ballot, shifted down to bit 0
+};
+
+// mode 0: the MB's 16x16 search (one group); mode 1: its four partitions.
+__device__ __forceinline__ void group_geom_init(GroupGeom& q, WarpScratch& ws, const h264a_picture& pc, int mx, int my,
+                                                int mode, uint32_t win) {
+    const int lane = threadIdx.x & 31;
+    SearchGeom& g = q.s;
+    int x = mx, y = my;
+    if (mode == 0) {
+        q.gb = 0;
+        q.gl = lane;
+        q.lg = 5;
+        q.gmask = 0xffffffffu;
+        q.rw = 16;
+        q.rh = 16;
+        g.lg_nb = 4;
+    } else {
+        const int grp = lane >> 3;
+        q.gb = grp * 8;
+        q.gl = lane & 7;
+        q.lg = 3;
+        q.gmask = 0xffu;
+        q.rw = grp < 2 ? 16 : 8;
+        q.rh = grp < 2 ? 8 : 16;
+        g.lg_nb = 3;
+        x += grp == 3 ? 8 : 0;
+        y += grp == 1 ? 8 : 0;
+    }
+    if (lane == 0) {
+        ws.base = pc.d_planes;
+        ws.pad = pc.pad;
+        ws.pw = pc.cw + 2 * pc.pad;
+        ws.ph = pc.ch + 2 * pc.pad;
+        ws.cw = pc.cw;
+        ws.ch = pc.ch;
+    }
+    g.lx = x; g.ly = y;
+    g.win = win;
+    g.lane = lane;
+    const int blk = q.gl & ((1 << g.lg_nb) - 1);
+    const int nbx = q.rw >> 2;
+    g.bxo = (blk % nbx) * 4;
+    g.byo = (blk / nbx) * 4;
+    if (ws.win_ok) {
+        g.wox = x + g.bxo + pc.pad - ws.wx0;
+        g.woy = y + g.byo + pc.pad - ws.wy0;
+    } else {
+        g.wox = WIN_OFF;
+        g.woy = WIN_OFF;
+    }
+    uint32_t srow[4];
+#pragma unroll
+    for (int r = 0; r < 4; r++) srow[r] = ld4u(pc.d_src + (long long)(y + g.byo + r) * pc.cw + x + g.bxo);
+    split_pairs(srow, g.spa, g.spb);
+    __syncwarp();
+}
+
+// Distortions of each group's candidates ws.cand[gb..gb+n) (n and metric per
+// group) into ws.dist.  A group prices 2^(lg - lg_nb) candidates per pass;
+// passes run to the largest need over the groups.
+__device__ __forceinline__ void eval_round_group(const GroupGeom& q, WarpScratch& ws, int n, int metric) {
+    const SearchGeom& g = q.s;
+    const int cps = q.lg - g.lg_nb;  // log2 candidates per pass of a group
+    const int nb = 1 << g.lg_nb;
+    const int npass = __reduce_max_sync(0xffffffffu, (n + (1 << cps) - 1) >> cps);
+    const int sub = q.gl >> g.lg_nb;  // which of the pass's candidates the lane serves
+    for (int k0 = 0; k0 < npass; k0 += ME_MAX_PASS) {
+        uint32_t pr4[ME_MAX_PASS][4];
+#pragma unroll
+        for (int kk = 0; kk < ME_MAX_PASS; kk++) {
+            const int c = ((k0 + kk) << cps) + sub;
+            if (k0 + kk < npass && c < n) {
+                const int2 mv = ws.cand[q.gb + c];
+                const int dx = mv.x >> 2, dy = mv.y >> 2;
+                const int wx = g.wox + dx, wy = g.woy + dy;
+                if (win_covers(wx, wy)) {
+                    win_rows(g.win, wx, wy, mv.x & 3, mv.y & 3, pr4[kk]);
+                } else {
+                    Planes P;
+                    P.base = ws.base; P.pw = ws.pw; P.ph = ws.ph; P.pad = ws.pad; P.ps = (long long)ws.pw * ws.ph;
+                    pred_rows(P, g.lx + g.bxo + dx, g.ly + g.byo + dy, mv.x & 3, mv.y & 3, pr4[kk]);
+                }
+            }
+        }
+#pragma unroll
+        for (int kk = 0; kk < ME_MAX_PASS; kk++) {
+            const int k = k0 + kk;
+            if (k < npass) {
+                const int c = (k << cps) + sub;
+                int d = 0;
+                if (c < n) {
+                    if (metric == MET_SAD) {
+                        uint32_t srow[4];
+#pragma unroll
+                        for (int r = 0; r < 4; r++) srow[r] = g.spa[r] | (g.spb[r] << 8);
+                        d = sad4x4_rows(srow, pr4[kk]);
+                    } else {
+                        d = satd4x4_packed(g.spa, g.spb, pr4[kk]);
+                    }
+                }
+                d = warp_seg_sum(d, nb);
+                if (c < n && (q.gl & (nb - 1)) == 0) ws.dist[q.gb + c] = d;
+            }
+        }
+    }
+    __syncwarp();
+}
+
+__device__ __forceinline__ bool group_in_plane_window(const GroupGeom& q, const WarpScratch& ws, int mvx, int mvy) {
+    const int px = q.s.lx + (mvx >> 2) + ws.pad, py = q.s.ly + (mvy >> 2) + ws.pad;
+    return px >= 0 && py >= 0 && px + q.rw + 1 <= ws.pw && py + q.rh + 1 <= ws.ph;
+}
+
+// motion_search (mb16.rs:2433-3302) of the lane's partition, every group at
+// once; same phases, order and pricing as motion_search_warp.
+__device__ __forceinline__ void motion_search_group(const GroupGeom& q, const MeParamsDev& pr, WarpScratch& ws,
+                                                    const int* preds, int npred, double lambda_me, int& out_x,
+                                                    int& out_y, long long& out_c, int& evals) {
+    const int gl = q.gl, gb = q.gb;
+    const bool sadfp = !pr.fast && pr.sadfp;
+    const int m_main = pr.use_sad ? MET_SAD : MET_SATD;
+    if (q.s.lane == 0) {
+        ws.cx = preds[0];
+        ws.cy = preds[1];
+        ws.lam_me = lambda_me;
+        ws.lam_r = pr.kind != 0 ? lambda_me * 0.25 : lambda_me;
+        ws.lam_fp = lambda_me * (sadfp ? pr.sadfp_lambda : 1.0);
+    }
+    // seeds and the snaps of sub-pel predictors (as motion_search_warp), per group
+    int qx = 0, qy = 0;
+    const bool mine = gl >= 1 && gl <= npred;
+    if (mine) {
+        qx = preds[2 * (gl - 1)];
+        qy = preds[2 * (gl - 1) + 1];
+        ws.cand[gb + gl] = make_int2(qx, qy);
+    }
+    const unsigned snaps =
+        (__ballot_sync(0xffffffffu, pr.me_snap && mine && ((qx & 3) != 0 || (qy & 3) != 0)) >> gb) & q.gmask;
+    if ((snaps >> gl) & 1u)
+        ws.cand[gb + npred + 1 + __popc(snaps & ((1u << gl) - 1u))] = make_int2(((qx + 2) >> 2) * 4, ((qy + 2) >> 2) * 4);
+    __syncwarp();
+    const int m_fp = sadfp ? MET_SAD : m_main;
+    const double l_fp = sadfp ? ws.lam_fp : ws.lam_r;
+    const int rw = q.rw, rh = q.rh;
+    const bool fc = !pr.fast && pr.fc;  // 16x16, 16x8 and 8x16 are x4 shapes
+    const uint32_t dmask = pr.fast ? 0u : pr.dia_mask;
+    const int spat = pr.subpel_pat >= 0 ? pr.subpel_pat : (pr.sp_single_pass ? 2 : 0);
+    const bool sp_fc = pr.sp_fc && !pr.fast;
+    const int sp_nring = (spat & 1) ? 4 : 8;
+
+    evals = 0;
+    int bx = 0, by = 0, seed_x = 0, seed_y = 0;
+    long long best_c = 0, seed_c = 0;
+    int phase = PH_SEEDS;
+    int si = -1, sk = -1, loops = 0, iter = 0, step = 0;
+    bool ring_open = false, ring_improved = false;
+    int ring_i = 0, ring_n = 0;
+    for (;;) {
+        // ---------- plan (per group) ----------
+        int kind = -1, n = 0, metric = m_main;
+        double lam = ws.lam_r;
+        while (kind < 0 && phase != PH_DONE) {
+            if (phase == PH_SEEDS) {
+                if (gl == 0) ws.cand[gb] = make_int2(0, 0);
+                kind = EV_SEEDS; n = npred + 1 + __popc(snaps); metric = m_fp; lam = l_fp;
+            } else if (phase == PH_DIA) {
+                if (ring_open) {
+                    kind = EV_RING; n = min(ring_n - ring_i, RING_REST); metric = m_fp; lam = l_fp;
+                    if (gl < n)
+                        ws.cand[gb + gl] = make_int2(bx + ring_dx(ring_i + gl) * step, by + ring_dy(ring_i + gl) * step);
+                    break;
+                }
+                if (si < 0 || loops >= LOOP_GUARD) {
+                    int nsi = si + 1;
+                    if (pr.fast) nsi = nsi >= 2 ? 5 : nsi;
+                    else
+                        while (nsi < 5 && !(dmask & (1u << nsi))) nsi++;
+                    if (nsi >= 5) {
+                        phase = PH_REPRICE;
+                        continue;
+                    }
+                    si = nsi;
+                    step = pr.fast ? (si == 0 ? 16 : 4) : (64 >> si);
+                    loops = 0;
+                }
+                loops++;
+                bool fixed = false;
+                if (fc && (bx & 3) == 0 && (by & 3) == 0) {
+                    const int st = step >> 2;
+                    const int px = q.s.lx + (bx >> 2), py = q.s.ly + (by >> 2);
+                    fixed = px - st >= 0 && py - st >= 0 && px + st + rw <= ws.cw && py + st + rh <= ws.ch;
+                }
+                if (gl < 4) ws.cand[gb + gl] = make_int2(bx + ring_dx(gl) * step, by + ring_dy(gl) * step);
+                if (fixed) {
+                    kind = EV_FIXED; n = 4;
+                    metric = rw == 16 ? (sadfp ? MET_SAD : MET_SATD) : m_fp;
+                    lam = rw == 16 ? ws.lam_fp : l_fp;
+                } else {
+                    ring_open = true; ring_improved = false; ring_i = 0; ring_n = 4;
+                    kind = EV_RING; n = 4; metric = m_fp; lam = l_fp;
+                }
+            } else if (phase == PH_REPRICE) {
+                if (sadfp) {
+                    if (gl == 0) {
+                        ws.cand[gb] = make_int2(bx, by);
+                        ws.cand[gb + 1] = make_int2(seed_x, seed_y);
+                    }
+                    kind = EV_REPRICE; n = 2; metric = m_main; lam = ws.lam_r;
+                } else {
+                    phase = PH_SUB;
+                }
+            } else {  // PH_SUB
+                if (ring_open) {
+                    kind = EV_RING; n = min(ring_n - ring_i, RING_REST); metric = m_main; lam = ws.lam_r;
+                    if (gl < n)
+                        ws.cand[gb + gl] = make_int2(bx + ring_dx(ring_i + gl) * step, by + ring_dy(ring_i + gl) * step);
+                    break;
+                }
+                if (!pr.subpel) {
+                    phase = PH_DONE;
+                    continue;
+                }
+                if (sk < 0 || loops >= LOOP_GUARD) {
+                    if (++sk >= 2) {
+                        phase = PH_DONE;
+                        continue;
+                    }
+                    step = sk == 0 ? 2 : 1;
+                    loops = 0;
+                    iter = 0;
+                }
+                loops++;
+                if (sp_fc && (spat & 1) == 0 && (step == 1 || ((bx & 3) == 0 && (by & 3) == 0))) {
+                    bool all = true;
+                    for (int i = 0; i < 8; i++) {
+                        const int qx2 = bx + ring_dx(i) * step, qy2 = by + ring_dy(i) * step;
+                        all = all && group_in_plane_window(q, ws, qx2, qy2) && (step == 2 || ((qx2 | qy2) & 1));
+                    }
+                    if (all) {
+                        iter++;
+                        if (gl < 8) ws.cand[gb + gl] = make_int2(bx + ring_dx(gl) * step, by + ring_dy(gl) * step);
+                        kind = EV_FIXED; n = 8;
+                        metric = rw == 16 ? MET_SATD : m_main;
+                        lam = rw == 16 ? ws.lam_me : ws.lam_r;
+                        break;
+                    }
+                }
+                iter++;
+                n = min(sp_nring, RING_FIRST);
+                if (gl < n) ws.cand[gb + gl] = make_int2(bx + ring_dx(gl) * step, by + ring_dy(gl) * step);
+                ring_open = true; ring_improved = false; ring_i = 0; ring_n = sp_nring;
+                kind = EV_RING; metric = m_main; lam = ws.lam_r;
+            }
+        }
+        if (kind < 0) n = 0;
+        if (__all_sync(0xffffffffu, kind < 0)) break;
+        __syncwarp();
+
+        // ---------- price ----------
+        eval_round_group(q, ws, n, metric);
+        int cc = INT_MAX;  // dist + λ·rate of slot gb + gl, as lane_cost prices it
+        if (gl < n) {
+            const int2 mv = ws.cand[gb + gl];
+            const long long c = (long long)ws.dist[gb + gl] + lam_cost(lam, rate_of(pr, ws, mv.x, mv.y));
+            cc = c > INT_MAX - 1 ? INT_MAX - 1 : int(c);
+        }
+        // group-wide collectives, taken by every lane
+        int gmin = cc;
+        for (int o = 1; o < (1 << q.lg); o <<= 1) gmin = min(gmin, __shfl_xor_sync(0xffffffffu, gmin, o));
+        const unsigned at = (__ballot_sync(0xffffffffu, cc == gmin) >> gb) & q.gmask;
+        const unsigned hit = (__ballot_sync(0xffffffffu, gl < n && (long long)cc < best_c) >> gb) & q.gmask;
+        const int jhit = hit ? __ffs(hit) - 1 : 0;
+        const int cj = __shfl_sync(0xffffffffu, cc, gb + jhit);
+        int c_seed[3];
+#pragma unroll
+        for (int i = 0; i < 3; i++) c_seed[i] = __shfl_sync(0xffffffffu, cc, gb + i);
+
+        // ---------- fold (per group) ----------
+        if (kind == EV_SEEDS) {
+            best_c = c_seed[0];
+            bx = 0; by = 0;
+            int wi = 0;
+            for (int i = 1; i <= npred; i++) {
+                const long long ci = c_seed[i];
+                if (ci < best_c) {
+                    best_c = ci;
+                    bx = ws.cand[gb + i].x;
+                    by = ws.cand[gb + i].y;
+                    wi = i;
+                }
+            }
+            evals += npred + 1;
+            seed_x = bx; seed_y = by; seed_c = best_c;
+            if ((snaps >> wi) & 1u) {
+                const int sl = gb + npred + 1 + __popc(snaps & ((1u << wi) - 1u));
+                bx = ws.cand[sl].x; by = ws.cand[sl].y;
+                best_c = cand_cost64(pr, ws, sl, lam);
+                evals += 1;
+            }
+            phase = PH_DIA;
+        } else if (kind == EV_REPRICE) {
+            best_c = cand_cost64(pr, ws, gb, lam);
+            seed_c = cand_cost64(pr, ws, gb + 1, lam);
+            evals += 2;
+            phase = PH_SUB;
+        } else if (kind == EV_FIXED) {
+            evals += n;
+            const int bi = (long long)gmin < best_c ? __ffs(at) - 1 : -1;
+            if (bi >= 0) {
+                best_c = gmin;
+                bx += ring_dx(bi) * step;
+                by += ring_dy(bi) * step;
+            }
+            if (phase == PH_DIA) {
+                if (bi < 0) loops = LOOP_GUARD;
+            } else {
+                const bool stop = bi < 0 || !pr.me_subpel_iter || (spat & 2) || (pr.sp_maxit != 0 && iter >= pr.sp_maxit);
+                if (stop) loops = LOOP_GUARD;
+            }
+        } else if (kind == EV_RING) {
+            if (hit == 0) {
+                evals += n;
+                ring_i += n;
+                ring_open = ring_i < ring_n;
+            } else {
+                best_c = cj;
+                const int2 mv = ws.cand[gb + jhit];
+                evals += jhit + 1;
+                bx = mv.x;
+                by = mv.y;
+                ring_improved = true;
+                ring_i += jhit + 1;
+                ring_open = ring_i < ring_n;
+            }
+            if (!ring_open) {
+                if (phase == PH_DIA) {
+                    if (!ring_improved) loops = LOOP_GUARD;
+                } else if (!ring_improved || !pr.me_subpel_iter || (spat & 2) ||
+                           (pr.sp_maxit != 0 && iter >= pr.sp_maxit)) {
+                    loops = LOOP_GUARD;
+                }
+            }
+        }
+        __syncwarp();
+    }
+    if (pr.me_snap && seed_c < best_c) {
+        bx = seed_x; by = seed_y; best_c = seed_c;
+    }
+    out_x = bx; out_y = by; out_c = best_c;
+}
+
 __device__ __forceinline__ bool job_shape_ok(int w, int h) {
     return (w == 16 && (h == 16 || h == 8)) || (w == 8 && (h == 16 || h == 8 || h == 4)) ||
            (w == 4 && (h == 8 || h == 4));
@@ -730,34 +1103,45 @@ __global__ void __launch_bounds__(32 * ME_WARPS, ME_MIN_BLOCKS) me_frames_kernel
         if (lane == 0) scratch[w].win_ok = win_ok;
         __syncwarp();
         int preds[4] = {pmv.x, pmv.y, 0, 0};
-        // best_part for 16x16, then (J above the gate) the four partitions
-        // seeded with [pmv, mv16]; one inlined search body.
+        // best_part for 16x16 (the warp as one group), then, J above the gate,
+        // the four partitions seeded with [pmv, mv16] side by side; one call
+        // site, so the search body exists once in the kernel.
         int evals = 0, shape = 0, mv0x = 0, mv0y = 0, mv1x = 0, mv1y = 0;
-        long long c16 = 0, best = 0, pc0 = 0;
-        int px0 = 0, py0 = 0;
-        for (int k5 = 0; k5 < 5; k5++) {
-            if (k5 == 1 && !(fd.split_gate >= 0 && c16 > fd.split_gate)) break;
-            const int ox = k5 == 4 ? 8 : 0, oy = k5 == 2 ? 8 : 0;
-            const int ww = k5 == 0 ? 16 : (k5 <= 2 ? 16 : 8), hh = k5 == 0 ? 16 : (k5 <= 2 ? 8 : 16);
-            SearchGeom geo;
-            geom_init(geo, scratch[w], pc, lx + ox, ly + oy, ww, hh, win);
-            if (k5 == 0 && win_ok) {
+        long long c16 = 0, best = 0;
+        for (int mode = 0; mode < 2; mode++) {
+            if (mode == 1 && !(fd.split_gate >= 0 && c16 > fd.split_gate)) break;
+            GroupGeom qg;
+            group_geom_init(qg, scratch[w], pc, lx, ly, mode, win);
+            if (mode == 0 && win_ok) {
                 wait_window(bar, parity, status, 3, spin_limit);
                 parity ^= 1u;
             }
             int rx, ry, ev;
             long long rc;
-            motion_search_warp(geo, prm, scratch[w], preds, k5 == 0 ? 1 : 2, nullptr, fd.lambda_me, rx, ry, rc, ev);
-            evals += ev << geo.lg_nb;  // 4x4-block evaluations
-            if (k5 == 0) {
+            motion_search_group(qg, prm, scratch[w], preds, mode == 0 ? 1 : 2, fd.lambda_me, rx, ry, rc, ev);
+            if (mode == 0) {
+                evals = ev << 4;  // 4x4-block evaluations
                 c16 = rc; best = rc;
                 mv0x = mv1x = rx; mv0y = mv1y = ry;
                 preds[2] = rx; preds[3] = ry;
-            } else if (k5 == 1 || k5 == 3) {
-                px0 = rx; py0 = ry; pc0 = rc;
-            } else if (pc0 + rc < best) {  // k5 == 2: the 16x8 pair, k5 == 4: the 8x16 pair
-                best = pc0 + rc; shape = k5 == 2 ? 1 : 2;
-                mv0x = px0; mv0y = py0; mv1x = rx; mv1y = ry;
+            } else {
+                int px[4], py[4];
+                long long pcost[4];
+#pragma unroll
+                for (int gi = 0; gi < 4; gi++) {
+                    px[gi] = __shfl_sync(0xffffffffu, rx, 8 * gi);
+                    py[gi] = __shfl_sync(0xffffffffu, ry, 8 * gi);
+                    pcost[gi] = __shfl_sync(0xffffffffu, rc, 8 * gi);
+                    evals += __shfl_sync(0xffffffffu, ev, 8 * gi) << 3;
+                }
+                if (pcost[0] + pcost[1] < best) {  // 16x8 top + bottom
+                    best = pcost[0] + pcost[1]; shape = 1;
+                    mv0x = px[0]; mv0y = py[0]; mv1x = px[1]; mv1y = py[1];
+                }
+                if (pcost[2] + pcost[3] < best) {  // 8x16 left + right
+                    best = pcost[2] + pcost[3]; shape = 2;
+                    mv0x = px[2]; mv0y = py[2]; mv1x = px[3]; mv1y = py[3];
+                }
             }
         }
         if (lane == 0) {
