@@ -88,9 +88,10 @@ __device__ __forceinline__ bool win_covers(int wx, int wy) {
     return wx >= 0 && ((wx + 1) & ~3) <= WIN_W - 8 && wy >= 0 && wy + 5 <= WIN_H;
 }
 
-// Passes whose plane loads are in flight together (a 16x16 ring of 8 takes
-// four 32-lane passes, done as two groups).
-constexpr int ME_MAX_PASS = 2;
+// Passes whose plane loads are issued together before their SATD: one, since
+// the window reads are shared-memory loads and batching passes only costs
+// registers.
+constexpr int ME_MAX_PASS = 1;
 
 // Register-resident part of one search (every function below is inlined, so
 // nothing of it is ever addressed in local memory); the rest is in the
@@ -228,16 +229,16 @@ constexpr int EV_START = 0, EV_SEEDS = 1, EV_FIXED = 3, EV_RING = 4, EV_REPRICE 
 constexpr int LOOP_GUARD = 1 << 20;  // iterations of one rung / sub-pel step
 
 // Points of a cascading ring priced per round: the first round prices
-// RING_FIRST of them, later rounds (after the centre moved) up to RING_REST.
-// A ring of eight sub-pel points usually improves once or twice, mostly
-// early, so pricing only the first four up front wastes fewer evaluations
-// on points the walk never reaches from the old centre; the order of the
-// walk and its result do not depend on these sizes.
+// RING_FIRST of them, later rounds (after the centre moved, or none improved)
+// up to RING_REST.  A ring of eight sub-pel points usually improves once or
+// twice, mostly early, so pricing a few points at a time wastes fewer
+// evaluations on points the walk reaches from a different centre; the order
+// of the walk and its result do not depend on these sizes.
 #ifndef RING_FIRST
-#define RING_FIRST 4
+#define RING_FIRST 2
 #endif
 #ifndef RING_REST
-#define RING_REST 8
+#define RING_REST 4
 #endif
 
 // motion_search (mb16.rs:2433-3302) of the partition in `g` (warp-cooperative,
