@@ -82,12 +82,14 @@ __global__ void la_intra_kernel(const uint8_t* __restrict__ pics, size_t fstride
     }
 }
 
-// One warp's view of the SATD search of a bs x bs block (full-pel steps around
-// a seed that may carry a sub-pel fraction).
+// One lane's view of the SATD search of a bs x bs block.  The warp holds two
+// searches, lane group g = lane / 16 (slots 16g.. of the candidate and
+// distortion arrays), each walking its own row chain; a group prices
+// 16 / (bs/4)^2 candidates per pass (four 8x8 or one 16x16).
 struct LaSearch {
     const uint8_t* cur;
     const uint8_t* ref;
-    int w, h, bs, lg_nb, lane, bxo, byo, x0, y0;
+    int w, h, bs, lg_nb, gl, gb, bxo, byo, x0, y0;
     uint32_t srow[4];
     int2* cand;
     int* dist;
@@ -95,24 +97,29 @@ struct LaSearch {
     __device__ void init(const uint8_t* c, const uint8_t* r, int pw, int ph, int b, int bx0, int by0, int2* cs,
                          int* ds) {
         cur = c; ref = r; w = pw; h = ph; bs = b; x0 = bx0; y0 = by0; cand = cs; dist = ds;
-        lane = threadIdx.x & 31;
+        const int lane = threadIdx.x & 31;
+        gl = lane & 15;
+        gb = lane & 16;
         lg_nb = b == 16 ? 4 : 2;
         const int nbx = b / 4;
-        const int sb = lane & ((1 << lg_nb) - 1);
+        const int sb = gl & ((1 << lg_nb) - 1);
         bxo = (sb % nbx) * 4;
         byo = (sb / nbx) * 4;
 #pragma unroll
         for (int r = 0; r < 4; r++) srow[r] = ld4u(cur + (long long)(y0 + byo + r) * w + x0 + bxo);
     }
 
-    // SATD of cand[0..n) (full-pel MVs, quarter-pel units) into dist.
+    // SATD of each group's cand[gb..gb+n) (full-pel MVs, quarter-pel units)
+    // into dist; passes run to the larger group's need.
     __device__ void eval(int n) {
         const int nb = 1 << lg_nb;
-        for (int base = 0; base < (n << lg_nb); base += 32) {
-            const int c = (base + lane) >> lg_nb;
+        const int cps = 4 - lg_nb;  // log2 candidates per pass of a group
+        const int npass = __reduce_max_sync(0xffffffffu, (n + (1 << cps) - 1) >> cps);
+        for (int k = 0; k < npass; k++) {
+            const int c = (k << cps) + (gl >> lg_nb);
             int d = 0;
             if (c < n) {
-                const int2 mv = cand[c];
+                const int2 mv = cand[gb + c];
                 uint32_t p[4];
                 if (((mv.x | mv.y) & 3) == 0)
                     fullpel_rows_clamped(ref, w, h, x0 + bxo + (mv.x >> 2), y0 + byo + (mv.y >> 2), p);
@@ -121,58 +128,89 @@ struct LaSearch {
                 d = satd4x4_rows(srow, p);
             }
             d = warp_seg_sum(d, nb);
-            if (c < n && (lane & (nb - 1)) == 0) dist[c] = d;
+            if (c < n && (gl & (nb - 1)) == 0) dist[gb + c] = d;
         }
         __syncwarp();
     }
 };
 
-// inter_cost (mbtree.rs:154-197): returns cost (capped to i32) and MV.
-__device__ void la_inter_cost(LaSearch& s, int seedx, int seedy, int max_step, int& cost, int& mvx, int& mvy) {
-    if (s.lane == 0) {
-        s.cand[0] = make_int2(0, 0);
-        s.cand[1] = make_int2(seedx, seedy);
-    }
-    __syncwarp();
-    s.eval(2);
-    long long best = s.dist[0];
+// The four-point diamond in the order mbtree.rs:181 walks it:
+// right, left, down, up.
+__device__ __forceinline__ int la_ring_dx(int k) { return k == 0 ? 1 : (k == 1 ? -1 : 0); }
+__device__ __forceinline__ int la_ring_dy(int k) { return k == 2 ? 1 : (k == 3 ? -1 : 0); }
+
+// inter_cost (mbtree.rs:154-197) of each group's block: (0,0) and the seed,
+// then the cascading four-point diamond at steps max_step .. 1 full pixels
+// (first improvement moves the centre, the rest of the ring is priced around
+// it; a ring that moved is walked again at the same step), stopping at once
+// when (0,0) costs nothing.  `active` false: the group takes no part.
+__device__ void la_inter_cost(LaSearch& s, bool active, int seedx, int seedy, int max_step, int& cost, int& mvx,
+                              int& mvy) {
+    const int gl = s.gl, gb = s.gb;
+    int phase = active ? 0 : 2;  // 0 seeds, 1 rings, 2 done
+    int step = max_step, ri = 0, guard = 0;
+    bool moved = false;
+    long long best = 0;
     int bx = 0, by = 0;
-    if (best != 0) {
-        if ((seedx != 0 || seedy != 0) && s.dist[1] < best) {
-            best = s.dist[1];
-            bx = seedx;
-            by = seedy;
+    for (;;) {
+        int n = 0;
+        if (phase == 0) {
+            if (gl == 0) {
+                s.cand[gb] = make_int2(0, 0);
+                s.cand[gb + 1] = make_int2(seedx, seedy);
+            }
+            n = 2;
+        } else if (phase == 1) {
+            n = 4 - ri;
+            if (gl < n)
+                s.cand[gb + gl] = make_int2(bx + la_ring_dx(ri + gl) * step * 4, by + la_ring_dy(ri + gl) * step * 4);
         }
+        if (__all_sync(0xffffffffu, phase == 2)) break;
         __syncwarp();
-        const int rx[4] = {1, -1, 0, 0}, ry[4] = {0, 0, 1, -1};
-        for (int step = max_step; step >= 1; step >>= 1) {
-            for (int guard = 0; guard < (1 << 20); guard++) {
-                bool moved = false;
-                int i = 0;
-                while (i < 4) {
-                    const int n = 4 - i;
-                    if (s.lane < n) s.cand[s.lane] = make_int2(bx + rx[i + s.lane] * step * 4, by + ry[i + s.lane] * step * 4);
-                    __syncwarp();
-                    s.eval(n);
-                    const int d = s.lane < n ? s.dist[s.lane] : 0;
-                    const unsigned hit = __ballot_sync(0xffffffffu, s.lane < n && (long long)d < best);
-                    if (hit == 0) {
-                        __syncwarp();
-                        break;
-                    }
-                    const int j = __ffs(hit) - 1;
-                    best = __shfl_sync(0xffffffffu, d, j);
-                    bx = s.cand[j].x;
-                    by = s.cand[j].y;
-                    moved = true;
-                    i += j + 1;
-                    __syncwarp();
+        s.eval(n);
+        const int d = gl < n ? s.dist[gb + gl] : 0;
+        const unsigned hit = (__ballot_sync(0xffffffffu, gl < n && (long long)d < best) >> gb) & 0xffffu;
+        const int j = hit ? __ffs(hit) - 1 : 0;
+        const int dj = __shfl_sync(0xffffffffu, d, gb + j);
+        const int d0 = __shfl_sync(0xffffffffu, d, gb), d1 = __shfl_sync(0xffffffffu, d, gb + 1);
+        if (phase == 0) {
+            best = d0;
+            if (best == 0) {
+                phase = 2;
+            } else {
+                if ((seedx != 0 || seedy != 0) && (long long)d1 < best) {
+                    best = d1;
+                    bx = seedx;
+                    by = seedy;
                 }
-                if (!moved) break;
+                phase = 1;
+            }
+        } else if (phase == 1) {
+            bool ring_end;
+            if (hit) {
+                best = dj;
+                bx = s.cand[gb + j].x;
+                by = s.cand[gb + j].y;
+                moved = true;
+                ri += j + 1;
+                ring_end = ri >= 4;
+            } else {
+                ring_end = true;
+            }
+            if (ring_end) {
+                if (moved && ++guard < (1 << 20)) {
+                    ri = 0;  // walk the ring again at this step
+                } else {
+                    step >>= 1;
+                    ri = 0;
+                    guard = 0;
+                    if (step == 0) phase = 2;
+                }
+                moved = false;
             }
         }
+        __syncwarp();
     }
-    __syncwarp();
     cost = best > 0x7fffffffLL ? 0x7fffffff : int(best);
     mvx = bx;
     mvy = by;
@@ -188,8 +226,8 @@ struct LaBufs {
 };
 
 // frame_costs for MB (mbx, mby) of frame f >= 1 given the full-res seed.
-__device__ void la_mb(const LaBufs& b, int f, int mbx, int mby, int sfx, int sfy, int2* cs, int* ds, int& outx,
-                      int& outy) {
+__device__ void la_mb(const LaBufs& b, bool active, int f, int mbx, int mby, int sfx, int sfy, int2* cs, int* ds,
+                      int& outx, int& outy) {
     const long long nmb = (long long)b.mb_w * b.mb_h;
     const long long gm = nmb * f + (long long)mby * b.mb_w + mbx;
     const int cwh = b.cw / 2, chh = b.ch / 2;
@@ -198,20 +236,20 @@ __device__ void la_mb(const LaBufs& b, int f, int mbx, int mby, int sfx, int sfy
     int cost, mx, my;
     if (b.mode == 0) {  // FullRes
         s.init(b.full + fs * f, b.full + fs * (f - 1), b.cw, b.ch, 16, mbx * 16, mby * 16, cs, ds);
-        la_inter_cost(s, sfx, sfy, 8, cost, mx, my);
+        la_inter_cost(s, active, sfx, sfy, 8, cost, mx, my);
     } else {
         s.init(b.half + hs * f, b.half + hs * (f - 1), cwh, chh, 8, mbx * 8, mby * 8, cs, ds);
         int hx, hy;
-        la_inter_cost(s, sfx / 2, sfy / 2, 8, cost, hx, hy);
+        la_inter_cost(s, active, sfx / 2, sfy / 2, 8, cost, hx, hy);
         if (b.mode == 2) {  // HalfRes
             mx = hx * 2;
             my = hy * 2;
         } else {  // Hybrid: refine at full-res from the coarse MV
             s.init(b.full + fs * f, b.full + fs * (f - 1), b.cw, b.ch, 16, mbx * 16, mby * 16, cs, ds);
-            la_inter_cost(s, hx * 2, hy * 2, 2, cost, mx, my);
+            la_inter_cost(s, active, hx * 2, hy * 2, 2, cost, mx, my);
         }
     }
-    if (s.lane == 0) {
+    if (active && s.gl == 0) {
         const int ic = b.intra[gm];
         b.inter[gm] = cost < ic ? cost : ic;
         b.mvs[2 * gm] = mx;
@@ -223,32 +261,37 @@ __device__ void la_mb(const LaBufs& b, int f, int mbx, int mby, int sfx, int sfy
 
 constexpr int LA_WARPS = 4;
 
-// Column-0 chains and row chains in one persistent launch: tickets 0..n-2
-// walk column 0 of frames 1..n-1 and publish flag (f-1)*mb_h + y after MB
-// (0, y); later tickets take row y of frame f (rows in order, frames
-// interleaved), wait for that flag and walk columns 1.. seeded by the left
-// neighbour.
-__global__ void __launch_bounds__(32 * LA_WARPS) la_chains_kernel(LaBufs b, int* __restrict__ counter,
+// Column-0 chains and row chains in one persistent launch, two chains per
+// warp (lane group g = lane / 16 walks the second).  Tickets 0 .. ceil(nf/2)-1
+// walk column 0 of frames 1+2t+g and publish flag (f-1)*mb_h + y after MB
+// (0, y); later tickets take rows 2p and 2p+1 of the row order (rows in
+// order, frames interleaved), each group waiting for its own column-0 flag
+// and walking columns 1.. seeded by the left neighbour.
+__global__ void __launch_bounds__(32 * LA_WARPS, 4) la_chains_kernel(LaBufs b, int* __restrict__ counter,
                                                                  int* __restrict__ flags, int epoch,
                                                                  int* __restrict__ status, int spin_limit) {
     __shared__ int2 cs[LA_WARPS][32];
     __shared__ int ds[LA_WARPS][32];
     const int w = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
+    const int grp = lane >> 4, gl = lane & 15;
     const int nf = b.n - 1;
+    const int ncol = (nf + 1) / 2;
+    const long long nrows = (long long)nf * b.mb_h;
     for (;;) {
         int t = 0;
         if (lane == 0) t = atomicAdd(counter, 1);
         t = __shfl_sync(0xffffffffu, t, 0);
-        if (t < nf) {
-            const int f = 1 + t;
+        if (t < ncol) {
+            const int f = 1 + 2 * t + grp;
+            const bool active = f <= nf;
             int sx = 0, sy = 0;
             for (int mby = 0; mby < b.mb_h; mby++) {
                 int mx, my;
-                la_mb(b, f, 0, mby, sx, sy, cs[w], ds[w], mx, my);
+                la_mb(b, active, active ? f : 1, 0, mby, sx, sy, cs[w], ds[w], mx, my);
                 sx = mx;
                 sy = my;
-                if (lane == 0) {
+                if (active && gl == 0) {
                     __threadfence();
                     st_release(flags + (f - 1) * b.mb_h + mby, epoch);
                 }
@@ -256,16 +299,17 @@ __global__ void __launch_bounds__(32 * LA_WARPS) la_chains_kernel(LaBufs b, int*
             }
             continue;
         }
-        const long long r = (long long)t - nf;
-        if (r >= (long long)nf * b.mb_h) return;
-        const int mby = int(r / nf), f = 1 + int(r % nf);
-        if (lane == 0) wait_flag(flags + (f - 1) * b.mb_h + mby, epoch, status, 1, spin_limit);
+        const long long r = 2 * ((long long)t - ncol) + grp;
+        if (2 * ((long long)t - ncol) >= nrows) return;
+        const bool active = r < nrows;
+        const int mby = active ? int(r / nf) : 0, f = active ? 1 + int(r % nf) : 1;
+        if (active && gl == 0) wait_flag(flags + (f - 1) * b.mb_h + mby, epoch, status, 1, spin_limit);
         __syncwarp();
         const long long gm0 = (long long)b.mb_w * b.mb_h * f + (long long)mby * b.mb_w;
-        int sx = __ldcg(b.mvs + 2 * gm0), sy = __ldcg(b.mvs + 2 * gm0 + 1);
+        int sx = active ? __ldcg(b.mvs + 2 * gm0) : 0, sy = active ? __ldcg(b.mvs + 2 * gm0 + 1) : 0;
         for (int mbx = 1; mbx < b.mb_w; mbx++) {
             int mx, my;
-            la_mb(b, f, mbx, mby, sx, sy, cs[w], ds[w], mx, my);
+            la_mb(b, active, f, mbx, mby, sx, sy, cs[w], ds[w], mx, my);
             sx = mx;
             sy = my;
         }
@@ -306,7 +350,7 @@ extern "C" int h264a_lookahead_costs(h264a_ctx* ctx, const uint8_t* d_full, cons
                                                                     ch / 16, n, d_intra, d_inter, d_mvs);
     int rc = check_launch("la_intra_kernel");
     if (rc || n < 2) return rc;
-    const long long chains = (long long)(n - 1) * (1 + ch / 16);
+    const long long chains = ((long long)(n - 1) * (ch / 16) + 1) / 2 + (n - 1 + 1) / 2;  // two chains per warp
     if ((long long)(n - 1) * (ch / 16) > (1 << 24)) return fail(H264A_E_ARG, "lookahead_costs: too many rows");
     rc = ensure_me_scratch(ctx, size_t(n - 1) * (ch / 16));
     if (rc) return rc;
