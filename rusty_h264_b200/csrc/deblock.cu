@@ -10,7 +10,11 @@
 // prediction.  One persistent kernel deals MB tickets in that order (frames
 // interleaved, bounded waits on the neighbours' flags); a warp filters its MB
 // on shared-memory tiles (20x20 luma and 10x12 per chroma plane, the MB plus
-// the samples its edges reach) and writes them back through L2.
+// the samples its edges reach) and writes them back through L2.  No MB
+// earlier in the order writes an MB's own samples, so they and bS are loaded
+// before the wait; after it only the neighbours' strips are fetched, and luma
+// (lanes 0..15) and chroma (lanes 16..31) are filtered side by side, one line
+// per lane through all edges of a direction.
 //
 // Pictures of this path: every MB inter with reference 0, 4x4 transforms,
 // one QP per picture.  bS (bs_inter and the single-list arm of bs1_tile,
@@ -151,13 +155,22 @@ __global__ void __launch_bounds__(32 * DB_WARPS) deblock_frames_kernel(const __g
         wave_mb(fd.mb_w, fd.mb_h, k, mbx, mby);
         const int m = mby * fd.mb_w + mbx;
         int* fl = flags + fd.flag_base;
-        if (lane == 0) {
-            if (mbx > 0) wait_flag(fl + m - 1, epoch, status, 1, spin_limit);
-            if (mby > 0) wait_flag(fl + m - fd.mb_w + (mbx < fd.mb_w - 1 ? 1 : 0), epoch, status, 1, spin_limit);
+        const int y0 = mby * 16, x0 = mbx * 16;
+        const int cy0 = mby * 8, cx0 = mbx * 8, ccw = fd.cw / 2;
+        const bool has_c = fd.uv[0] != nullptr;
+        // ---- before the wait: the MB's own samples (no MB earlier in the
+        // order writes them) and bS: lanes 0..15 the vertical edges (edge
+        // e = lane / 4, block row lane % 4), lanes 16..31 the horizontal ones ----
+        for (int i = lane; i < 64; i += 32) {
+            const int r = i >> 2, c4 = (i & 3) * 4;
+            *reinterpret_cast<uint32_t*>(lt + (4 + r) * LT + 4 + c4) =
+                __ldcg(reinterpret_cast<const unsigned int*>(fd.y + (long long)(y0 + r) * fd.cw + x0 + c4));
         }
-        __syncwarp();
-        // ---- bS: lanes 0..15 the vertical edges (edge e = lane / 4, block row
-        // lane % 4), lanes 16..31 the horizontal ones ----
+        if (has_c) {
+            const int pl = lane >> 4, r = (lane >> 1) & 7, c4 = (lane & 1) * 4;
+            *reinterpret_cast<uint32_t*>(&ctile[w][pl][(2 + r) * CT + 4 + c4]) =
+                __ldcg(reinterpret_cast<const unsigned int*>(fd.uv[pl] + (long long)(cy0 + r) * ccw + cx0 + c4));
+        }
         {
             const int hor = lane >> 4, e = (lane >> 2) & 3, sg = lane & 3;
             int bs = 0;
@@ -175,76 +188,72 @@ __global__ void __launch_bounds__(32 * DB_WARPS) deblock_frames_kernel(const __g
             }
             bsw[w][lane] = bs;
         }
-        // ---- luma tile: frame rows 16y-4.., columns 16x-4.., through L2 ----
-        const int y0 = mby * 16 - 4, x0 = mbx * 16 - 4;
-        for (int i = lane; i < LT * (LT / 4); i += 32) {
-            const int r = i / (LT / 4), c4 = (i - r * (LT / 4)) * 4;
-            uint32_t v = 0;
-            if (y0 + r >= 0 && x0 + c4 >= 0)
-                v = __ldcg(reinterpret_cast<const unsigned int*>(fd.y + (long long)(y0 + r) * fd.cw + x0 + c4));
-            *reinterpret_cast<uint32_t*>(lt + r * LT + c4) = v;
+        // ---- wait for the left (lane 0) and top-right (lane 1) neighbours ----
+        if (lane == 0 && mbx > 0) wait_flag(fl + m - 1, epoch, status, 1, spin_limit);
+        if (lane == 1 && mby > 0)
+            wait_flag(fl + m - fd.mb_w + (mbx < fd.mb_w - 1 ? 1 : 0), epoch, status, 1, spin_limit);
+        __syncwarp();
+        // ---- the neighbours' samples the edges reach, through L2: luma left
+        // strip (lanes 0..15, row `lane`) and top strip (lanes 16..31); chroma
+        // left strips (lanes 0..15) and top strips (lanes 16..23) ----
+        const bool lok = lane < 16 ? mbx > 0 : mby > 0;
+        const int lr = lane < 16 ? lane : ((lane - 16) >> 2) - 4, lc = lane < 16 ? -4 : (lane & 3) * 4;
+        unsigned int* lg = reinterpret_cast<unsigned int*>(fd.y + (long long)(y0 + lr) * fd.cw + x0 + lc);
+        uint32_t* ls = reinterpret_cast<uint32_t*>(lt + (4 + lr) * LT + 4 + lc);
+        const bool cok = has_c && lane < 24 && (lane < 16 ? mbx > 0 : mby > 0);
+        const int cpl = lane < 16 ? lane >> 3 : (lane >> 2) & 1;
+        const int cr = lane < 16 ? lane & 7 : ((lane >> 1) & 1) - 2, cc = lane < 16 ? -4 : (lane & 1) * 4;
+        unsigned int* cg = cok ? reinterpret_cast<unsigned int*>(fd.uv[cpl] + (long long)(cy0 + cr) * ccw + cx0 + cc)
+                               : nullptr;
+        uint32_t* cs = reinterpret_cast<uint32_t*>(&ctile[w][cpl][(2 + cr) * CT + 4 + cc]);
+        if (lok) *ls = __ldcg(lg);
+        if (cok) *cs = __ldcg(cg);
+        __syncwarp();
+        // ---- vertical edges: lanes 0..15 luma row `lane` (edges 0..3), lanes
+        // 16..31 chroma row lane & 7 of plane (lane >> 3) & 1 (columns 0, 4) ----
+        const int pl = (lane >> 3) & 1, li = lane & 7;
+        if (lane < 16) {
+            uint8_t* row = lt + (4 + lane) * LT + 4;
+            for (int e = mbx > 0 ? 0 : 1; e < 4; e++) {
+                const int bs = bsw[w][e * 4 + (lane >> 2)];
+                if (bs) luma_line(row + 4 * e, 1, bs, fd.alpha_y, fd.beta_y, fd.tc_y[bs - 1]);
+            }
+        } else if (has_c) {
+            uint8_t* row = &ctile[w][pl][(2 + li) * CT + 4];
+            for (int ce = mbx > 0 ? 0 : 2; ce < 4; ce += 2) {  // luma edges 0 and 2
+                const int bs = bsw[w][ce * 4 + (li >> 1)];
+                if (bs) chroma_line(row + 2 * ce, 1, bs, fd.alpha_c, fd.beta_c, fd.tc_c[bs - 1]);
+            }
         }
         __syncwarp();
-        for (int e = 0; e < 4; e++) {  // vertical edges, one line per lane
-            if (e == 0 && mbx == 0) continue;
-            if (lane < 16) {
-                const int bs = bsw[w][e * 4 + (lane >> 2)];
-                if (bs) luma_line(lt + (4 + lane) * LT + 4 + 4 * e, 1, bs, fd.alpha_y, fd.beta_y, fd.tc_y[bs - 1]);
-            }
-            __syncwarp();
-        }
-        for (int e = 0; e < 4; e++) {  // horizontal edges
-            if (e == 0 && mby == 0) continue;
-            if (lane < 16) {
+        // ---- horizontal edges: luma column `lane`, chroma column lane & 7 ----
+        if (lane < 16) {
+            uint8_t* col = lt + 4 * LT + 4 + lane;
+            for (int e = mby > 0 ? 0 : 1; e < 4; e++) {
                 const int bs = bsw[w][16 + e * 4 + (lane >> 2)];
-                if (bs) luma_line(lt + (4 + 4 * e) * LT + 4 + lane, LT, bs, fd.alpha_y, fd.beta_y, fd.tc_y[bs - 1]);
+                if (bs) luma_line(col + 4 * e * LT, LT, bs, fd.alpha_y, fd.beta_y, fd.tc_y[bs - 1]);
             }
-            __syncwarp();
+        } else if (has_c) {
+            uint8_t* col = &ctile[w][pl][2 * CT + 4 + li];
+            for (int ce = mby > 0 ? 0 : 2; ce < 4; ce += 2) {
+                const int bs = bsw[w][16 + ce * 4 + (li >> 1)];
+                if (bs) chroma_line(col + 2 * ce * CT, CT, bs, fd.alpha_c, fd.beta_c, fd.tc_c[bs - 1]);
+            }
         }
-        for (int i = lane; i < LT * (LT / 4); i += 32) {
-            const int r = i / (LT / 4), c4 = (i - r * (LT / 4)) * 4;
-            if ((r < 4 && c4 < 4) || y0 + r < 0 || x0 + c4 < 0) continue;  // the top-left corner is not this MB's
+        __syncwarp();
+        // ---- write back: the MB and the strips ----
+        for (int i = lane; i < 64; i += 32) {
+            const int r = i >> 2, c4 = (i & 3) * 4;
             __stcg(reinterpret_cast<unsigned int*>(fd.y + (long long)(y0 + r) * fd.cw + x0 + c4),
-                   *reinterpret_cast<const uint32_t*>(lt + r * LT + c4));
+                   *reinterpret_cast<const uint32_t*>(lt + (4 + r) * LT + 4 + c4));
         }
-        // ---- chroma: rows 8y-2.., columns 8x-4.. (two planes, lanes 0..7 and 8..15) ----
-        if (fd.uv[0] != nullptr) {
-            const int cy0 = mby * 8 - 2, cx0 = mbx * 8 - 4, ccw = fd.cw / 2;
-            for (int i = lane; i < 2 * CR * (CT / 4); i += 32) {
-                const int pl = i / (CR * (CT / 4)), ii = i - pl * CR * (CT / 4);
-                const int r = ii / (CT / 4), c4 = (ii - r * (CT / 4)) * 4;
-                uint32_t v = 0;
-                if (cy0 + r >= 0 && cx0 + c4 >= 0)
-                    v = __ldcg(reinterpret_cast<const unsigned int*>(fd.uv[pl] + (long long)(cy0 + r) * ccw + cx0 + c4));
-                *reinterpret_cast<uint32_t*>(&ctile[w][pl][r * CT + c4]) = v;
-            }
-            __syncwarp();
-            const int pl = (lane >> 3) & 1, li = lane & 7;
-            uint8_t* ct = ctile[w][pl];
-            for (int ce = 0; ce < 4; ce += 2) {  // vertical chroma edges: columns 0 and 4 (luma edges 0 and 2)
-                if (ce == 0 && mbx == 0) continue;
-                if (lane < 16) {
-                    const int bs = bsw[w][ce * 4 + (li * 2) / 4];
-                    if (bs) chroma_line(ct + (2 + li) * CT + 4 + 2 * ce, 1, bs, fd.alpha_c, fd.beta_c, fd.tc_c[bs - 1]);
-                }
-                __syncwarp();
-            }
-            for (int ce = 0; ce < 4; ce += 2) {  // horizontal chroma edges: rows 0 and 4
-                if (ce == 0 && mby == 0) continue;
-                if (lane < 16) {
-                    const int bs = bsw[w][16 + ce * 4 + (li * 2) / 4];
-                    if (bs) chroma_line(ct + (2 + 2 * ce) * CT + 4 + li, CT, bs, fd.alpha_c, fd.beta_c, fd.tc_c[bs - 1]);
-                }
-                __syncwarp();
-            }
-            for (int i = lane; i < 2 * CR * (CT / 4); i += 32) {
-                const int p = i / (CR * (CT / 4)), ii = i - p * CR * (CT / 4);
-                const int r = ii / (CT / 4), c4 = (ii - r * (CT / 4)) * 4;
-                if ((r < 2 && c4 < 4) || cy0 + r < 0 || cx0 + c4 < 0) continue;
-                __stcg(reinterpret_cast<unsigned int*>(fd.uv[p] + (long long)(cy0 + r) * ccw + cx0 + c4),
-                       *reinterpret_cast<const uint32_t*>(&ctile[w][p][r * CT + c4]));
-            }
+        if (lok) __stcg(lg, *ls);
+        if (has_c) {
+            const int p = lane >> 4, r = (lane >> 1) & 7, c4 = (lane & 1) * 4;
+            __stcg(reinterpret_cast<unsigned int*>(fd.uv[p] + (long long)(cy0 + r) * ccw + cx0 + c4),
+                   *reinterpret_cast<const uint32_t*>(&ctile[w][p][(2 + r) * CT + 4 + c4]));
         }
+        if (cok) __stcg(cg, *cs);
         __syncwarp();
         if (lane == 0) {
             __threadfence();

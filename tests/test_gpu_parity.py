@@ -563,6 +563,42 @@ def test_deblock_frames_matches_oracle(acc, qp, offs):
     assert changed > 0  # the filter did something on these pictures
 
 
+def test_deblock_frames_1080p_wavefront(acc):
+    """Six 1920x1088 pictures with chroma in one wavefront launch, so that
+    thousands of MB tickets are in flight at once, bit-exact with the oracle.
+    Picks are seeded synthetic ones (every shape, MVs around the clip's
+    background motion, some far off) and the pictures are the oracle's
+    reconstruction from them, so bS 0, 1 and 2 all occur."""
+    qp, w, h = 34, 1920, 1088
+    y, _, _ = synth.hd_clip(7, 3, w, h)
+    luma = synth.coded_luma(y)
+    half = np.stack([O.downsample2x(a) for a in luma])
+    rng = np.random.default_rng(11)
+    nmb = (w // 16) * (h // 16)
+    frames, keep, cases = [], [], []
+    for f in range(1, 7):
+        picks = np.zeros((nmb, 6), np.int32)
+        picks[:, 0] = rng.integers(0, 3, nmb)
+        jit = rng.integers(-8, 9, (nmb, 2)) * (rng.random((nmb, 1)) < 0.4)
+        picks[:, 1:3] = np.array([-5, 2]) + jit
+        jit1 = rng.integers(-6, 7, (nmb, 2)) * (rng.random((nmb, 1)) < 0.5)
+        picks[:, 3:5] = np.where(picks[:, :1] == 0, picks[:, 1:3], picks[:, 1:3] + jit1)
+        coeffs, rec = O.mc_tq_rec_frame(luma[f], luma[f - 1], picks, qp, 6)
+        _, ru, rv = O.mc_tq_chroma_frame(half[f], 255 - half[f], half[f - 1], 255 - half[f - 1], picks, qp)
+        dy, du, dv, dp, dc = (dev(acc, a) for a in (rec, ru, rv, picks, coeffs))
+        keep += [dy, du, dv, dp, dc]
+        cases.append((dy, du, dv, rec, ru, rv, picks, coeffs))
+        frames.append(A.DeblockFrame(dy.data_ptr(), du.data_ptr(), dv.data_ptr(), w, h, dp.data_ptr(), dc.data_ptr(),
+                                     qp, 0, 0, 0))
+    acc.deblock_frames(frames)
+    acc.sync()
+    for k, (dy, du, dv, rec, ru, rv, picks, coeffs) in enumerate(cases):
+        wy, wu, wv = O.deblock_frame(rec, ru, rv, picks, coeffs, qp)
+        assert (wy != rec).sum() > 1000
+        assert np.array_equal(dy.cpu().numpy(), wy), k
+        assert np.array_equal(du.cpu().numpy(), wu) and np.array_equal(dv.cpu().numpy(), wv), k
+
+
 # ---------------------------------------------------------------------------
 # a16-a19 lookahead
 # ---------------------------------------------------------------------------
