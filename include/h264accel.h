@@ -16,8 +16,11 @@
  *    context's device); h_* are host pointers.  Callers own every buffer.
  *  - `stream` is a cudaStream_t (NULL = the device's default stream, as in the
  *    CUDA runtime).  Calls only enqueue work; results are ready when the
- *    stream is synchronised (h264a_sync).  h264a_me_frames serialises on the
- *    context's work-queue scratch: one context per concurrent stream.
+ *    stream is synchronised (h264a_sync).  The persistent wavefront kernels
+ *    serialise on a context's work-queue scratch: h264a_me_frames and
+ *    h264a_deblock_frames share one queue, h264a_lookahead_costs has a second,
+ *    so within one context the lookahead may run on another stream beside
+ *    either of them; otherwise use one context per concurrent stream.
  *  - Planes: a reference picture's cached planes are one buffer F|H|V|C, each
  *    pw*ph bytes with pw = cw + 2*pad, ph = ch + 2*pad, stride pw: the
  *    HpelPlanes layout of crates/rusty_h264-common/src/inter.rs:707-730.

@@ -51,34 +51,36 @@ MeParamsDev to_dev(const h264a_me_params& p) {
     return d;
 }
 
-int ensure_me_scratch(h264a_ctx* ctx, size_t n) {
-    if (n <= ctx->flags_cap) return H264A_OK;
-    if (ctx->d_flags) cudaFree(ctx->d_flags);
-    ctx->d_flags = nullptr;
-    ctx->flags_cap = 0;
+int ensure_me_scratch(h264a_ctx* ctx, size_t n, int queue) {
+    WorkQueue& q = ctx->q[queue];
+    if (n <= q.flags_cap) return H264A_OK;
+    if (q.d_flags) cudaFree(q.d_flags);
+    q.d_flags = nullptr;
+    q.flags_cap = 0;
     size_t cap = n < 4096 ? 4096 : n + n / 4;
     cap = (cap + 63) & ~size_t(63);
     const size_t bytes = cap * sizeof(int32_t);  // one done flag per MB
-    if (cudaMalloc(&ctx->d_flags, bytes) != cudaSuccess) {
+    if (cudaMalloc(&q.d_flags, bytes) != cudaSuccess) {
         cudaGetLastError();
         return fail(H264A_E_NOMEM, "persistent-kernel scratch: cudaMalloc failed");
     }
-    H264A_CUDA(cudaMemset(ctx->d_flags, 0, bytes));
-    ctx->flags_cap = cap;
-    ctx->epoch = 0;
+    H264A_CUDA(cudaMemset(q.d_flags, 0, bytes));
+    q.flags_cap = cap;
+    q.epoch = 0;
     return H264A_OK;
 }
 
-int next_epoch(h264a_ctx* ctx, cudaStream_t st) {
-    if (ctx->epoch >= 0x7ffffff0) {  // wrap: clear the flags so stale values never match
-        if (cudaMemsetAsync(ctx->d_flags, 0, ctx->flags_cap * sizeof(int32_t), st) != cudaSuccess) {
+int next_epoch(h264a_ctx* ctx, cudaStream_t st, int queue) {
+    WorkQueue& q = ctx->q[queue];
+    if (q.epoch >= 0x7ffffff0) {  // wrap: clear the flags so stale values never match
+        if (cudaMemsetAsync(q.d_flags, 0, q.flags_cap * sizeof(int32_t), st) != cudaSuccess) {
             cudaGetLastError();
             set_error("persistent-kernel flags: reset failed");
             return -1;
         }
-        ctx->epoch = 0;
+        q.epoch = 0;
     }
-    return ++ctx->epoch;
+    return ++q.epoch;
 }
 
 }  // namespace h264a
@@ -106,17 +108,18 @@ extern "C" int h264a_ctx_create(int device, h264a_ctx** out) {
     c->device = device;
     c->num_sms = prop.multiProcessorCount;
     bool ev_ok = true;
-    for (int i = 0; i < PP_CHUNKS + 2; i++)
+    for (int i = 0; i < PP_EVENTS; i++)
         ev_ok = ev_ok && cudaEventCreateWithFlags(&c->pp_ev[i], cudaEventDisableTiming) == cudaSuccess;
     if (!ev_ok || cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaMalloc(&c->d_counter, 4 * sizeof(int32_t)) != cudaSuccess ||
+        cudaMalloc(&c->d_counters, NUM_QUEUES * Q_COUNTER_STRIDE * sizeof(int32_t)) != cudaSuccess ||
         cudaMalloc(&c->d_status, sizeof(int32_t)) != cudaSuccess ||
         cudaMemset(c->d_status, 0, sizeof(int32_t)) != cudaSuccess) {
         const cudaError_t e = cudaGetLastError();
         h264a_ctx_destroy(c);
         return cuda_fail(e, "ctx_create");
     }
+    for (int i = 0; i < NUM_QUEUES; i++) c->q[i].d_counter = c->d_counters + i * Q_COUNTER_STRIDE;
     *out = c;
     return H264A_OK;
 }
@@ -126,13 +129,14 @@ extern "C" int h264a_ctx_destroy(h264a_ctx* ctx) {
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
-    if (ctx->d_counter) cudaFree(ctx->d_counter);
+    if (ctx->d_counters) cudaFree(ctx->d_counters);
     if (ctx->d_status) cudaFree(ctx->d_status);
-    if (ctx->d_flags) cudaFree(ctx->d_flags);
+    for (int i = 0; i < NUM_QUEUES; i++)
+        if (ctx->q[i].d_flags) cudaFree(ctx->q[i].d_flags);
     if (ctx->pp_buf) cudaFree(ctx->pp_buf);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
-    for (int i = 0; i < PP_CHUNKS + 2; i++)
+    for (int i = 0; i < PP_EVENTS; i++)
         if (ctx->pp_ev[i]) cudaEventDestroy(ctx->pp_ev[i]);
     delete ctx;
     return H264A_OK;
@@ -310,15 +314,15 @@ extern "C" int h264a_pixel_path_host(h264a_ctx* ctx, const uint8_t* h_frames, in
         rc = h264a_mc_tq_frames(ctx, tf.data(), n - 1, st);
         if (rc) return rc;
     }
-    H264A_CUDA(cudaEventRecord(ctx->pp_ev[PP_CHUNKS], st));
+    H264A_CUDA(cudaEventRecord(ctx->pp_ev[PP_EV_TQ], st));
     rc = h264a_lookahead_costs(ctx, d_frames, d_half, cw, ch, n, 2, d_intra, d_inter, d_mvs, st);
     if (rc) return rc;
-    H264A_CUDA(cudaEventRecord(ctx->pp_ev[PP_CHUNKS + 1], st));
-    H264A_CUDA(cudaStreamWaitEvent(cs, ctx->pp_ev[PP_CHUNKS], 0));
+    H264A_CUDA(cudaEventRecord(ctx->pp_ev[PP_EV_LA], st));
+    H264A_CUDA(cudaStreamWaitEvent(cs, ctx->pp_ev[PP_EV_TQ], 0));
     H264A_CUDA(cudaMemcpyAsync(h_picks, d_picks, sizeof(int32_t) * 6 * nmb * n, cudaMemcpyDeviceToHost, cs));
     H264A_CUDA(cudaMemcpyAsync(h_costs, d_costs, sizeof(int64_t) * 2 * nmb * n, cudaMemcpyDeviceToHost, cs));
     H264A_CUDA(cudaMemcpyAsync(h_coeffs, d_coeffs, sizeof(int16_t) * 256 * nmb * n, cudaMemcpyDeviceToHost, cs));
-    H264A_CUDA(cudaStreamWaitEvent(cs, ctx->pp_ev[PP_CHUNKS + 1], 0));
+    H264A_CUDA(cudaStreamWaitEvent(cs, ctx->pp_ev[PP_EV_LA], 0));
     H264A_CUDA(cudaMemcpyAsync(h_la_intra, d_intra, sizeof(int32_t) * nmb * n, cudaMemcpyDeviceToHost, cs));
     H264A_CUDA(cudaMemcpyAsync(h_la_inter, d_inter, sizeof(int32_t) * nmb * n, cudaMemcpyDeviceToHost, cs));
     H264A_CUDA(cudaMemcpyAsync(h_la_mvs, d_mvs, sizeof(int32_t) * 2 * nmb * n, cudaMemcpyDeviceToHost, cs));

@@ -61,6 +61,9 @@ struct DbBatch {
 };
 
 constexpr int DB_WARPS = 4;
+// Resident CTAs per SM: 8 x 4 warps hold about two and a half wavefront steps
+// of a 59-picture 1080p batch; more only adds warps polling flags.
+constexpr int DB_BLOCKS_PER_SM = 8;
 constexpr int LT = 20;            // luma tile: 20 x 20 (stride 20), the MB at (4, 4)
 constexpr int CT = 12, CR = 10;   // chroma tile: 10 rows x 12 (stride 12), the MB at (2, 4)
 
@@ -254,11 +257,8 @@ __global__ void __launch_bounds__(32 * DB_WARPS) deblock_frames_kernel(const __g
                    *reinterpret_cast<const uint32_t*>(&ctile[w][p][(2 + r) * CT + 4 + c4]));
         }
         if (cok) __stcg(cg, *cs);
-        __syncwarp();
-        if (lane == 0) {
-            __threadfence();
-            st_release(fl + m, epoch);
-        }
+        __syncwarp();  // every lane's stores ordered before lane 0's release
+        if (lane == 0) st_release(fl + m, epoch);
         __syncwarp();
     }
 }
@@ -334,15 +334,16 @@ extern "C" int h264a_deblock_frames(h264a_ctx* ctx, const h264a_deblock_frame* h
         if (acc != total) return fail(H264A_E_ARG, "deblock_frames: internal queue layout error");
         int rc = ensure_me_scratch(ctx, size_t(total));
         if (rc) return rc;
-        H264A_CUDA(cudaMemsetAsync(ctx->d_counter, 0, sizeof(int32_t), st));
+        H264A_CUDA(cudaMemsetAsync(ctx->q[Q_MAIN].d_counter, 0, sizeof(int32_t), st));
         const int epoch = next_epoch(ctx, st);
         if (epoch < 0) return H264A_E_CUDA;
         int per_sm = 0;
         H264A_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, deblock_frames_kernel, 32 * DB_WARPS, 0));
+        if (per_sm > DB_BLOCKS_PER_SM) per_sm = DB_BLOCKS_PER_SM;
         long long blocks = (long long)ctx->num_sms * (per_sm > 0 ? per_sm : 1);
         const long long need = (total + DB_WARPS - 1) / DB_WARPS;
         if (blocks > need) blocks = need;
-        deblock_frames_kernel<<<unsigned(blocks), 32 * DB_WARPS, 0, st>>>(b, total, ctx->d_counter, ctx->d_flags,
+        deblock_frames_kernel<<<unsigned(blocks), 32 * DB_WARPS, 0, st>>>(b, total, ctx->q[Q_MAIN].d_counter, ctx->q[Q_MAIN].d_flags,
                                                                           epoch, ctx->d_status, SPIN_LIMIT);
         rc = check_launch("deblock_frames_kernel");
         if (rc) return rc;

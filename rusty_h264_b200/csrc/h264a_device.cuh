@@ -361,6 +361,10 @@ __device__ __forceinline__ int ld_acquire(const int* p) {
     asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
 }
+// Release store at GPU scope: the thread's earlier stores, and those of the
+// lanes that a __syncwarp ordered before it, are visible to any thread whose
+// ld_acquire reads the value (a release fence and a store in one; no separate
+// __threadfence is needed).
 __device__ __forceinline__ void st_release(int* p, int v) {
     asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }

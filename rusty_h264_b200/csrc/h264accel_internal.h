@@ -9,26 +9,39 @@
 
 #include "../../include/h264accel.h"
 
+// The work queue of a persistent wavefront kernel: its ticket counter, one
+// done flag per MB (flags_cap MBs) and the value a finished MB writes into
+// its flag.
+struct WorkQueue {
+    int32_t *d_counter = nullptr;  // a word of h264a_ctx::d_counters
+    int32_t *d_flags = nullptr;
+    size_t flags_cap = 0;
+    int32_t epoch = 0;
+};
+// Q_MAIN serves plain-ME, deblocking and the bounded-wait self-test;
+// Q_LOOKAHEAD the lookahead, which can therefore run on another stream beside
+// them.  The counters sit 128 bytes apart.
+constexpr int Q_MAIN = 0, Q_LOOKAHEAD = 1, NUM_QUEUES = 2, Q_COUNTER_STRIDE = 32;
+// h264a_pixel_path_host: PP_CHUNKS upload chunks; its events are the
+// uploads, T/Q done and lookahead done.
+constexpr int PP_CHUNKS = 4;
+constexpr int PP_EV_TQ = PP_CHUNKS, PP_EV_LA = PP_CHUNKS + 1, PP_EVENTS = PP_CHUNKS + 2;
+
 struct h264a_ctx {
     int device = 0;
     int num_sms = 0;
     cudaStream_t stream = nullptr;
-    // device scratch of the persistent ME kernel: the work-queue counter, one
-    // done flag per MB (flags_cap MBs), and a status word (the code of a
-    // bounded wait that ran out)
-    int32_t *d_counter = nullptr;
-    int32_t *d_flags = nullptr;
-    size_t flags_cap = 0;      // MBs the scratch holds
+    // device scratch of the persistent kernels: the work queues and a status
+    // word (the code of a bounded wait that ran out)
+    int32_t *d_counters = nullptr;
+    WorkQueue q[NUM_QUEUES];
     int32_t *d_status = nullptr;
-    int32_t epoch = 0;         // value a finished MB writes into its flag
     // cached buffers of h264a_pixel_path_host, its copy stream and events
-    // (PP_CHUNKS upload chunks, then T/Q done and lookahead done)
     void *pp_buf = nullptr;
     size_t pp_bytes = 0;
     cudaStream_t copy_stream = nullptr;
-    cudaEvent_t pp_ev[6] = {};
+    cudaEvent_t pp_ev[PP_EVENTS] = {};
 };
-constexpr int PP_CHUNKS = 4;
 
 namespace h264a {
 
@@ -38,10 +51,11 @@ int cuda_fail(cudaError_t e, const char *what);
 // `stream` follows the CUDA convention: NULL is the device's default stream.
 inline cudaStream_t pick_stream(h264a_ctx *, void *s) { return reinterpret_cast<cudaStream_t>(s); }
 int check_launch(const char *what);
-// grows the per-MB done flags to at least n entries (zeroed, epoch reset)
-int ensure_me_scratch(h264a_ctx *ctx, size_t n);
+// grows the per-MB done flags of work queue `queue` to at least n entries
+// (zeroed, epoch reset)
+int ensure_me_scratch(h264a_ctx *ctx, size_t n, int queue = Q_MAIN);
 // the flag value of the next persistent launch on `st`
-int next_epoch(h264a_ctx *ctx, cudaStream_t st);
+int next_epoch(h264a_ctx *ctx, cudaStream_t st, int queue = Q_MAIN);
 
 // Device-side mirror of h264a_me_params with only the fields the kernels read.
 struct MeParamsDev {

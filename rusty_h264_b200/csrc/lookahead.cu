@@ -291,10 +291,7 @@ __global__ void __launch_bounds__(32 * LA_WARPS, 4) la_chains_kernel(LaBufs b, i
                 la_mb(b, active, active ? f : 1, 0, mby, sx, sy, cs[w], ds[w], mx, my);
                 sx = mx;
                 sy = my;
-                if (active && gl == 0) {
-                    __threadfence();
-                    st_release(flags + (f - 1) * b.mb_h + mby, epoch);
-                }
+                if (active && gl == 0) st_release(flags + (f - 1) * b.mb_h + mby, epoch);  // after the lane's MV store
                 __syncwarp();
             }
             continue;
@@ -352,17 +349,17 @@ extern "C" int h264a_lookahead_costs(h264a_ctx* ctx, const uint8_t* d_full, cons
     if (rc || n < 2) return rc;
     const long long chains = ((long long)(n - 1) * (ch / 16) + 1) / 2 + (n - 1 + 1) / 2;  // two chains per warp
     if ((long long)(n - 1) * (ch / 16) > (1 << 24)) return fail(H264A_E_ARG, "lookahead_costs: too many rows");
-    rc = ensure_me_scratch(ctx, size_t(n - 1) * (ch / 16));
+    rc = ensure_me_scratch(ctx, size_t(n - 1) * (ch / 16), Q_LOOKAHEAD);
     if (rc) return rc;
-    H264A_CUDA(cudaMemsetAsync(ctx->d_counter, 0, sizeof(int32_t), st));
-    const int epoch = next_epoch(ctx, st);
+    H264A_CUDA(cudaMemsetAsync(ctx->q[Q_LOOKAHEAD].d_counter, 0, sizeof(int32_t), st));
+    const int epoch = next_epoch(ctx, st, Q_LOOKAHEAD);
     if (epoch < 0) return H264A_E_CUDA;
     int per_sm = 0;
     H264A_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, la_chains_kernel, 32 * LA_WARPS, 0));
     long long blocks = (long long)ctx->num_sms * (per_sm > 0 ? per_sm : 1);
     const long long need = (chains + LA_WARPS - 1) / LA_WARPS;
     if (blocks > need) blocks = need;
-    la_chains_kernel<<<unsigned(blocks), 32 * LA_WARPS, 0, st>>>(b, ctx->d_counter, ctx->d_flags, epoch, ctx->d_status,
+    la_chains_kernel<<<unsigned(blocks), 32 * LA_WARPS, 0, st>>>(b, ctx->q[Q_LOOKAHEAD].d_counter, ctx->q[Q_LOOKAHEAD].d_flags, epoch, ctx->d_status,
                                                                 SPIN_LIMIT);
     return check_launch("la_chains_kernel");
 }

@@ -669,9 +669,9 @@ __device__ __forceinline__ void motion_search_group(const GroupGeom& q, const Me
     // seeds and the snaps of sub-pel predictors (as motion_search_warp), per group
     int qx = 0, qy = 0;
     const bool mine = gl >= 1 && gl <= npred;
-    if (mine) {
-        qx = preds[2 * (gl - 1)];
-        qy = preds[2 * (gl - 1) + 1];
+    if (mine) {  // npred <= 2: lane 1 the first predictor, lane 2 the second
+        qx = gl == 1 ? preds[0] : preds[2];
+        qy = gl == 1 ? preds[1] : preds[3];
         ws.cand[gb + gl] = make_int2(qx, qy);
     }
     const unsigned snaps =
@@ -690,7 +690,7 @@ __device__ __forceinline__ void motion_search_group(const GroupGeom& q, const Me
 
     evals = 0;
     int bx = 0, by = 0, seed_x = 0, seed_y = 0;
-    long long best_c = 0, seed_c = 0;
+    int best_c = 0, seed_c = 0;  // costs below 2^30 (lane_cost), compared as i32
     int phase = PH_SEEDS;
     int si = -1, sk = -1, loops = 0, iter = 0, step = 0;
     bool ring_open = false, ring_improved = false;
@@ -808,7 +808,7 @@ __device__ __forceinline__ void motion_search_group(const GroupGeom& q, const Me
         int gmin = cc;
         for (int o = 1; o < (1 << q.lg); o <<= 1) gmin = min(gmin, __shfl_xor_sync(0xffffffffu, gmin, o));
         const unsigned at = (__ballot_sync(0xffffffffu, cc == gmin) >> gb) & q.gmask;
-        const unsigned hit = (__ballot_sync(0xffffffffu, gl < n && (long long)cc < best_c) >> gb) & q.gmask;
+        const unsigned hit = (__ballot_sync(0xffffffffu, gl < n && cc < best_c) >> gb) & q.gmask;
         const int jhit = hit ? __ffs(hit) - 1 : 0;
         const int cj = __shfl_sync(0xffffffffu, cc, gb + jhit);
         int c_seed[3];
@@ -820,9 +820,10 @@ __device__ __forceinline__ void motion_search_group(const GroupGeom& q, const Me
             best_c = c_seed[0];
             bx = 0; by = 0;
             int wi = 0;
-            for (int i = 1; i <= npred; i++) {
-                const long long ci = c_seed[i];
-                if (ci < best_c) {
+#pragma unroll
+            for (int i = 1; i < 3; i++) {
+                const int ci = c_seed[i];
+                if (i <= npred && ci < best_c) {
                     best_c = ci;
                     bx = ws.cand[gb + i].x;
                     by = ws.cand[gb + i].y;
@@ -834,18 +835,18 @@ __device__ __forceinline__ void motion_search_group(const GroupGeom& q, const Me
             if ((snaps >> wi) & 1u) {
                 const int sl = gb + npred + 1 + __popc(snaps & ((1u << wi) - 1u));
                 bx = ws.cand[sl].x; by = ws.cand[sl].y;
-                best_c = cand_cost64(pr, ws, sl, lam);
+                best_c = int(cand_cost64(pr, ws, sl, lam));
                 evals += 1;
             }
             phase = PH_DIA;
         } else if (kind == EV_REPRICE) {
-            best_c = cand_cost64(pr, ws, gb, lam);
-            seed_c = cand_cost64(pr, ws, gb + 1, lam);
+            best_c = int(cand_cost64(pr, ws, gb, lam));
+            seed_c = int(cand_cost64(pr, ws, gb + 1, lam));
             evals += 2;
             phase = PH_SUB;
         } else if (kind == EV_FIXED) {
             evals += n;
-            const int bi = (long long)gmin < best_c ? __ffs(at) - 1 : -1;
+            const int bi = gmin < best_c ? __ffs(at) - 1 : -1;
             if (bi >= 0) {
                 best_c = gmin;
                 bx += ring_dx(bi) * step;
@@ -1150,8 +1151,7 @@ __global__ void __launch_bounds__(32 * ME_WARPS, ME_MIN_BLOCKS) me_frames_kernel
             p[0] = shape; p[1] = mv0x; p[2] = mv0y; p[3] = mv1x; p[4] = mv1y; p[5] = evals;
             fd.costs[2 * m] = best;
             fd.costs[2 * m + 1] = c16;
-            __threadfence();
-            st_release(fl + m, epoch);
+            st_release(fl + m, epoch);  // orders the pick's stores before the flag
         }
         __syncwarp();
     }
@@ -1184,8 +1184,8 @@ extern "C" int h264a_selftest_bounded_wait(h264a_ctx* ctx, int spin_limit, void*
     if (rc) return rc;
     cudaStream_t st = pick_stream(ctx, stream);
     // the counter word is zero-initialised scratch that no kernel of this call writes
-    H264A_CUDA(cudaMemsetAsync(ctx->d_counter, 0, sizeof(int32_t), st));
-    bounded_wait_selftest_kernel<<<1, 32, 0, st>>>(ctx->d_counter, ctx->d_status, spin_limit);
+    H264A_CUDA(cudaMemsetAsync(ctx->q[Q_MAIN].d_counter, 0, sizeof(int32_t), st));
+    bounded_wait_selftest_kernel<<<1, 32, 0, st>>>(ctx->q[Q_MAIN].d_counter, ctx->d_status, spin_limit);
     return check_launch("bounded_wait_selftest_kernel");
 }
 
@@ -1258,13 +1258,13 @@ extern "C" int h264a_me_frames(h264a_ctx* ctx, const h264a_me_frame* h_frames, i
         if (acc != total) return fail(H264A_E_ARG, "me_frames: internal queue layout error");
         int rc = ensure_me_scratch(ctx, size_t(total));
         if (rc) return rc;
-        H264A_CUDA(cudaMemsetAsync(ctx->d_counter, 0, sizeof(int32_t), st));
+        H264A_CUDA(cudaMemsetAsync(ctx->q[Q_MAIN].d_counter, 0, sizeof(int32_t), st));
         const int epoch = next_epoch(ctx, st);
         if (epoch < 0) return H264A_E_CUDA;
         long long blocks = (long long)ctx->num_sms * per_sm;
         const long long need = (total + ME_WARPS - 1) / ME_WARPS;
         if (blocks > need) blocks = need;
-        me_frames_kernel<<<unsigned(blocks), 32 * ME_WARPS, ME_WARPS * WIN_BYTES, st>>>(fb, total, prm, ctx->d_counter, ctx->d_flags,
+        me_frames_kernel<<<unsigned(blocks), 32 * ME_WARPS, ME_WARPS * WIN_BYTES, st>>>(fb, total, prm, ctx->q[Q_MAIN].d_counter, ctx->q[Q_MAIN].d_flags,
                                                                      epoch, ctx->d_status, SPIN_LIMIT);
         rc = check_launch("me_frames_kernel");
         if (rc) return rc;

@@ -628,6 +628,46 @@ def test_lookahead_flat_and_static(acc):
     assert np.array_equal(inter.cpu().numpy(), wn) and np.array_equal(mvs.cpu().numpy(), wm)
 
 
+def test_lookahead_beside_me_in_one_context(acc):
+    """The lookahead has a work queue of its own in a context, so it may run
+    on a second stream while plain-ME runs on the first; both give the
+    results of the same calls made one after the other, on ten 1080p
+    frames."""
+    torch = acc.torch
+    y, _, _ = synth.hd_clip(10, 2)
+    f = synth.coded_luma(y)
+    n, ch, cw = f.shape
+    nmb = (cw // 16) * (ch // 16)
+    d = dev(acc, f)
+    planes = acc.hpel_build(d[: n - 1], 32)
+    half = acc.downsample2x(d)
+    acc.sync()
+    params = A.default_me_params()
+    lam = float(np.sqrt(A.frame_lambda(27)) * 1.25)
+    gate = A.split_gate_for_qp(27)
+    runs = []
+    for concurrent in (False, True):
+        picks = acc.zeros((n, nmb, 6), torch.int32)
+        costs = acc.zeros((n, nmb, 2), torch.int64)
+        frames = [A.MeFrame(A.Picture(d[i].data_ptr(), planes[i - 1].data_ptr(), cw, ch, 32), lam, gate,
+                            picks[i].data_ptr(), costs[i].data_ptr()) for i in range(1, n)]
+        main, side = torch.cuda.current_stream(), torch.cuda.Stream()
+        side.wait_stream(main)
+        if concurrent:
+            with torch.cuda.stream(side):
+                la = acc.lookahead_costs(d, half, 2)
+            acc.me_frames(frames, params)
+        else:
+            acc.me_frames(frames, params)
+            la = acc.lookahead_costs(d, half, 2)
+        main.wait_stream(side)
+        torch.cuda.synchronize()
+        acc.sync()
+        runs.append([picks, costs, *la])
+    for a, b in zip(*runs):
+        assert torch.equal(a, b)
+
+
 # ---------------------------------------------------------------------------
 # The whole path through the host-buffer entry point
 # ---------------------------------------------------------------------------
@@ -647,6 +687,20 @@ def test_pixel_path_host_cif_matches_oracle(acc, cif):
     gate = A.split_gate_for_qp(qp)
     got = acc.pixel_path_host(cif, params, lam, gate, qp)
     want = O.pixel_path_clip(cif, O.balanced_params(), lam, gate, qp, nthreads=4)
+    compare_pixel_path(got, want)
+
+
+def test_pixel_path_host_40_frames_matches_oracle(acc):
+    """40 CIF frames through the host-buffer entry point (39 P frames in one
+    wavefront launch)."""
+    y, _, _ = synth.cif_clip(40, 5)
+    frames = synth.coded_luma(y)
+    params = A.default_me_params()
+    qp = 30
+    lam = float(np.sqrt(A.frame_lambda(qp)))
+    gate = A.split_gate_for_qp(qp)
+    got = acc.pixel_path_host(frames, params, lam, gate, qp)
+    want = O.pixel_path_clip(frames, O.balanced_params(), lam, gate, qp, nthreads=8)
     compare_pixel_path(got, want)
 
 
