@@ -299,7 +299,8 @@ def run_ours(args, ws, rank, local):
         else:
             stream.wait_stream(side)
 
-    kernels_per_step = 1 + ((n - 1 + 95) // 96) + ((n - 1 + 95) // 96) + 1 + 3
+    # hpel_build, me_frames and mc_tq_frames per 96 frames, downsample2x, la_intra, la_chains
+    kernels_per_step = 1 + 2 * ((n - 1 + 95) // 96) + 1 + 2
 
     def barrier():
         if ws > 1:

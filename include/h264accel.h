@@ -173,6 +173,23 @@ typedef struct {
 H264A_API int h264a_me_frames(h264a_ctx *ctx, const h264a_me_frame *h_frames, int nframes, const h264a_me_params *params,
                     void *stream);
 
+/* h264a_me_frames with the MC + luma T/Q of each MB's pick (as
+ * h264a_mc_tq_frames, mb16.rs:3436-3450) in the same launch: the warp that
+ * publishes an MB's pick then transforms and quantises the MB's 16 blocks, so
+ * each MB's coefficients are written as soon as its pick is known and no
+ * second pass reads the frames again.  d_coeffs: 256 i16 per MB, 16-byte
+ * aligned, in any memory the device can write (device memory, or mapped
+ * pinned host memory).  Outputs equal h264a_me_frames followed by
+ * h264a_mc_tq_frames. */
+typedef struct {
+    h264a_me_frame me;
+    int32_t qp, dz_div;
+    int16_t *d_coeffs;
+} h264a_me_tq_frame;
+
+H264A_API int h264a_me_tq_frames(h264a_ctx *ctx, const h264a_me_tq_frame *h_frames, int nframes,
+                                 const h264a_me_params *params, void *stream);
+
 /* h264a_me_frames for callers that cannot allocate device memory when they
  * run motion estimation (an encoder thread that must not block on the CUDA
  * allocator, or a host that gives this library a fixed memory budget and owns
@@ -290,7 +307,10 @@ H264A_API int h264a_lookahead_costs(h264a_ctx *ctx, const uint8_t *d_full, const
  * frames, and copies the results back.  Output arrays are per frame (frame 0
  * rows are zero for picks/costs/coeffs): h_picks 6 i32/MB, h_costs 2 i64/MB,
  * h_coeffs 256 i16/MB, h_la_intra/h_la_inter 1 i32/MB, h_la_mvs 2 i32/MB.
- * Device buffers are cached in the context between calls of the same shape. */
+ * ME runs with the MC + T/Q fused in, the lookahead beside it, and the rows
+ * of MBs that are final come down while the launch still runs (pinned output
+ * buffers make those copies asynchronous).  Device buffers are cached in the
+ * context between calls of the same shape. */
 H264A_API int h264a_pixel_path_host(h264a_ctx *ctx, const uint8_t *h_frames, int n, int cw, int ch, const h264a_me_params *params,
                           const uint16_t *h_mv_cost_tab, double lambda_me, int64_t split_gate, int qp, int dz_div,
                           int32_t *h_picks, int64_t *h_costs, int16_t *h_coeffs, int32_t *h_la_intra,

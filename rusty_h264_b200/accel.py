@@ -67,6 +67,10 @@ class MeFrame(C.Structure):
                 ("d_costs", C.c_void_p)]
 
 
+class MeTqFrame(C.Structure):
+    _fields_ = [("me", MeFrame), ("qp", C.c_int32), ("dz_div", C.c_int32), ("d_coeffs", C.c_void_p)]
+
+
 class TqFrame(C.Structure):
     _fields_ = [("pic", Picture), ("d_picks", C.c_void_p), ("qp", C.c_int32), ("dz_div", C.c_int32),
                 ("d_coeffs", C.c_void_p)]
@@ -96,7 +100,7 @@ EXPORTS = (
     "h264a_me_search", "h264a_me_frames", "h264a_fullpel_grid", "h264a_dct_quant_4x4", "h264a_dct_quant_8x8",
     "h264a_mc_tq_frames", "h264a_downsample2x", "h264a_lookahead_costs", "h264a_pixel_path_host",
     "h264a_selftest_bounded_wait", "h264a_measure_int32_peak", "h264a_me_frames_noalloc",
-    "h264a_mc_tq_rec_frames", "h264a_mc_tq_chroma_frames", "h264a_deblock_frames",
+    "h264a_mc_tq_rec_frames", "h264a_mc_tq_chroma_frames", "h264a_deblock_frames", "h264a_me_tq_frames",
 )
 
 _lib = None
@@ -125,6 +129,7 @@ def load_library() -> C.CDLL:
     L.h264a_build_mv_cost_table.restype = None
     L.h264a_me_search.argtypes = [vp, vp, i32, C.POINTER(MeParams), vp, i32, vp, vp]
     L.h264a_me_frames.argtypes = [vp, vp, i32, C.POINTER(MeParams), vp]
+    L.h264a_me_tq_frames.argtypes = [vp, vp, i32, C.POINTER(MeParams), vp]
     L.h264a_fullpel_grid.argtypes = [vp, C.POINTER(Picture), i32, vp, vp, i32, i32, vp, f64, vp, vp, vp, vp]
     L.h264a_dct_quant_4x4.argtypes = [vp, vp, i32, vp, i32, vp, vp, i32, i32, vp, vp]
     L.h264a_dct_quant_8x8.argtypes = [vp, vp, i32, vp, i32, vp, vp, vp, i32, i32, vp, vp]
@@ -290,6 +295,12 @@ class Accel:
         arr = (MeFrame * len(frames))(*frames)
         self._check(self.L.h264a_me_frames(self.ctx, C.cast(arr, C.c_void_p), len(frames), C.byref(params),
                                            self._stream()))
+
+    def me_tq_frames(self, frames: Sequence[MeTqFrame], params: MeParams):
+        """me_frames with each MB's MC + luma T/Q fused into the same launch."""
+        arr = (MeTqFrame * len(frames))(*frames)
+        self._check(self.L.h264a_me_tq_frames(self.ctx, C.cast(arr, C.c_void_p), len(frames), C.byref(params),
+                                              self._stream()))
 
     def fullpel_grid(self, pic: Picture, R: int, centers=None, pmv=None, metric=0, kind=0, tab=None, lam=0.0,
                      want_grids=True):

@@ -4,6 +4,8 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <chrono>
+#include <thread>
 #include <vector>
 
 #include "h264accel_internal.h"
@@ -112,6 +114,7 @@ extern "C" int h264a_ctx_create(int device, h264a_ctx** out) {
         ev_ok = ev_ok && cudaEventCreateWithFlags(&c->pp_ev[i], cudaEventDisableTiming) == cudaSuccess;
     if (!ev_ok || cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->la_stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaMalloc(&c->d_counters, NUM_QUEUES * Q_COUNTER_STRIDE * sizeof(int32_t)) != cudaSuccess ||
         cudaMalloc(&c->d_status, sizeof(int32_t)) != cudaSuccess ||
         cudaMemset(c->d_status, 0, sizeof(int32_t)) != cudaSuccess) {
@@ -129,13 +132,17 @@ extern "C" int h264a_ctx_destroy(h264a_ctx* ctx) {
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
+    if (ctx->la_stream) cudaStreamSynchronize(ctx->la_stream);
     if (ctx->d_counters) cudaFree(ctx->d_counters);
     if (ctx->d_status) cudaFree(ctx->d_status);
     for (int i = 0; i < NUM_QUEUES; i++)
         if (ctx->q[i].d_flags) cudaFree(ctx->q[i].d_flags);
     if (ctx->pp_buf) cudaFree(ctx->pp_buf);
+    if (ctx->pp_row_count) cudaFree(ctx->pp_row_count);
+    if (ctx->pp_rows_host) cudaFreeHost(ctx->pp_rows_host);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
+    if (ctx->la_stream) cudaStreamDestroy(ctx->la_stream);
     for (int i = 0; i < PP_EVENTS; i++)
         if (ctx->pp_ev[i]) cudaEventDestroy(ctx->pp_ev[i]);
     delete ctx;
@@ -224,6 +231,26 @@ extern "C" void h264a_build_mv_cost_table(uint16_t* h_out) {
 
 static size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
 
+// Grows the row-completion buffers of h264a_pixel_path_host to `rows` rows.
+static int ensure_pp_rows(h264a_ctx* ctx, size_t rows) {
+    if (rows <= ctx->pp_rows_cap) return H264A_OK;
+    if (ctx->pp_row_count) cudaFree(ctx->pp_row_count);
+    if (ctx->pp_rows_host) cudaFreeHost(ctx->pp_rows_host);
+    ctx->pp_row_count = ctx->pp_rows_host = ctx->pp_rows_dev = nullptr;
+    ctx->pp_rows_cap = 0;
+    const size_t bytes = rows * sizeof(int32_t);
+    if (cudaMalloc(&ctx->pp_row_count, bytes) != cudaSuccess ||
+        cudaHostAlloc(reinterpret_cast<void**>(&ctx->pp_rows_host), bytes, cudaHostAllocMapped) != cudaSuccess ||
+        cudaHostGetDevicePointer(reinterpret_cast<void**>(&ctx->pp_rows_dev), ctx->pp_rows_host, 0) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(H264A_E_NOMEM, "pixel_path_host: row-completion buffers");
+    }
+    memset(ctx->pp_rows_host, 0, bytes);
+    ctx->pp_token = 0;
+    ctx->pp_rows_cap = rows;
+    return H264A_OK;
+}
+
 extern "C" int h264a_pixel_path_host(h264a_ctx* ctx, const uint8_t* h_frames, int n, int cw, int ch,
                                      const h264a_me_params* params, const uint16_t* h_mv_cost_tab, double lambda_me,
                                      int64_t split_gate, int qp, int dz_div, int32_t* h_picks, int64_t* h_costs,
@@ -270,11 +297,18 @@ extern "C" int h264a_pixel_path_host(h264a_ctx* ctx, const uint8_t* h_frames, in
     int32_t* d_inter = reinterpret_cast<int32_t*>(base + o_inter);
     int32_t* d_mvs = reinterpret_cast<int32_t*>(base + o_mvs);
     uint16_t* d_tab = reinterpret_cast<uint16_t*>(base + o_tab);
-    // Two streams: the frames go up in PP_CHUNKS chunks on the copy stream
-    // while the compute stream builds each chunk's planes and half-res
-    // frames; after ME and T/Q the coefficients come down on the copy stream
-    // while the compute stream runs the lookahead.
-    cudaStream_t st = ctx->stream, cs = ctx->copy_stream;
+    // Three streams.  The frames go up in PP_CHUNKS chunks on the copy
+    // stream while the compute stream builds each chunk's planes and half-res
+    // frames.  Then the lookahead (its own work queue) runs on the lookahead
+    // stream beside plain-ME with the fused MC + T/Q on the compute stream.
+    // An MB row of every frame is final once all its MBs have stored their
+    // coefficients (the kernel sets a host-visible word per row), and the
+    // rows happen to finish from about half-way through the launch; this
+    // thread polls those words and queues each band of finished rows, of all
+    // frames at once, for download, so that little is left to copy when the
+    // launch ends.
+    cudaStream_t st = ctx->stream, cs = ctx->copy_stream, ls = ctx->la_stream;
+    const int mb_w = cw / 16, mb_h = ch / 16;
     const int nk = n < PP_CHUNKS ? n : PP_CHUNKS;
     for (int k = 0; k < nk; k++) {
         const int a = int((long long)k * n / nk), b = int((long long)(k + 1) * n / nk);
@@ -286,10 +320,14 @@ extern "C" int h264a_pixel_path_host(h264a_ctx* ctx, const uint8_t* h_frames, in
         H264A_CUDA(cudaMemcpyAsync(d_tab, h_mv_cost_tab, sizeof(uint16_t) * 4096, cudaMemcpyHostToDevice, st));
         prm.d_mv_cost_tab = d_tab;
     }
-    H264A_CUDA(cudaMemsetAsync(d_picks, 0, sizeof(int32_t) * 6 * nmb, st));
-    H264A_CUDA(cudaMemsetAsync(d_costs, 0, sizeof(int64_t) * 2 * nmb, st));
-    H264A_CUDA(cudaMemsetAsync(d_coeffs, 0, sizeof(int16_t) * 256 * nmb, st));
-    int rc;
+    int rc = ensure_pp_rows(ctx, size_t(n > 1 ? n - 1 : 1) * mb_h);
+    if (rc) return rc;
+    if (ctx->pp_token >= 0x7ffffff0) {  // stale words must never equal a new token
+        memset(ctx->pp_rows_host, 0, ctx->pp_rows_cap * sizeof(int32_t));
+        ctx->pp_token = 0;
+    }
+    const int32_t token = ++ctx->pp_token;
+    H264A_CUDA(cudaMemsetAsync(ctx->pp_row_count, 0, ctx->pp_rows_cap * sizeof(int32_t), st));
     for (int k = 0; k < nk; k++) {
         const int a = int((long long)k * n / nk), b = int((long long)(k + 1) * n / nk);
         H264A_CUDA(cudaStreamWaitEvent(st, ctx->pp_ev[k], 0));
@@ -301,27 +339,68 @@ extern "C" int h264a_pixel_path_host(h264a_ctx* ctx, const uint8_t* h_frames, in
         rc = h264a_downsample2x(ctx, d_frames + fs * a, cw, ch, b - a, fs, d_half + hs * a, st);
         if (rc) return rc;
     }
+    H264A_CUDA(cudaEventRecord(ctx->pp_ev[PP_EV_INPUTS], st));
+    H264A_CUDA(cudaStreamWaitEvent(ls, ctx->pp_ev[PP_EV_INPUTS], 0));
+    rc = h264a_lookahead_costs(ctx, d_frames, d_half, cw, ch, n, 2, d_intra, d_inter, d_mvs, ls);
+    if (rc) return rc;
+    H264A_CUDA(cudaEventRecord(ctx->pp_ev[PP_EV_LA], ls));
     if (n > 1) {
         std::vector<h264a_me_frame> mf(n - 1);
-        std::vector<h264a_tq_frame> tf(n - 1);
+        std::vector<MeTqOut> tq(n - 1);
         for (int f = 1; f < n; f++) {
             h264a_picture pic{d_frames + fs * f, d_planes + p4 * (f - 1), cw, ch, pad};
             mf[f - 1] = {pic, lambda_me, split_gate, d_picks + 6 * nmb * f, d_costs + 2 * nmb * f};
-            tf[f - 1] = {pic, d_picks + 6 * nmb * f, qp, dz_div, d_coeffs + 256 * nmb * f};
+            tq[f - 1] = MeTqOut{d_coeffs + 256 * nmb * f, qp, dz_div, ctx->pp_row_count + size_t(f - 1) * mb_h,
+                                ctx->pp_rows_dev + size_t(f - 1) * mb_h, token};
         }
-        rc = h264a_me_frames(ctx, mf.data(), n - 1, &prm, st);
-        if (rc) return rc;
-        rc = h264a_mc_tq_frames(ctx, tf.data(), n - 1, st);
+        rc = me_frames_run(ctx, mf.data(), n - 1, &prm, tq.data(), st);
         if (rc) return rc;
     }
     H264A_CUDA(cudaEventRecord(ctx->pp_ev[PP_EV_TQ], st));
-    rc = h264a_lookahead_costs(ctx, d_frames, d_half, cw, ch, n, 2, d_intra, d_inter, d_mvs, st);
-    if (rc) return rc;
-    H264A_CUDA(cudaEventRecord(ctx->pp_ev[PP_EV_LA], st));
-    H264A_CUDA(cudaStreamWaitEvent(cs, ctx->pp_ev[PP_EV_TQ], 0));
-    H264A_CUDA(cudaMemcpyAsync(h_picks, d_picks, sizeof(int32_t) * 6 * nmb * n, cudaMemcpyDeviceToHost, cs));
-    H264A_CUDA(cudaMemcpyAsync(h_costs, d_costs, sizeof(int64_t) * 2 * nmb * n, cudaMemcpyDeviceToHost, cs));
-    H264A_CUDA(cudaMemcpyAsync(h_coeffs, d_coeffs, sizeof(int16_t) * 256 * nmb * n, cudaMemcpyDeviceToHost, cs));
+    // frame 0 (the IDR) has no pick or coefficients: the kernels never write its rows
+    memset(h_picks, 0, sizeof(int32_t) * 6 * nmb);
+    memset(h_costs, 0, sizeof(int64_t) * 2 * nmb);
+    memset(h_coeffs, 0, sizeof(int16_t) * 256 * nmb);
+    // rows [r0, r1) of every P frame: one strided copy per output
+    auto copy_rows = [&](int r0, int r1) -> int {
+        const size_t m0 = nmb + size_t(r0) * mb_w, mc = size_t(r1 - r0) * mb_w;
+        const size_t hgt = size_t(n - 1);
+        H264A_CUDA(cudaMemcpy2DAsync(h_coeffs + 256 * m0, 512 * nmb, d_coeffs + 256 * m0, 512 * nmb, 512 * mc, hgt,
+                                     cudaMemcpyDeviceToHost, cs));
+        H264A_CUDA(cudaMemcpy2DAsync(h_picks + 6 * m0, 24 * nmb, d_picks + 6 * m0, 24 * nmb, 24 * mc, hgt,
+                                     cudaMemcpyDeviceToHost, cs));
+        H264A_CUDA(cudaMemcpy2DAsync(h_costs + 2 * m0, 16 * nmb, d_costs + 2 * m0, 16 * nmb, 16 * mc, hgt,
+                                     cudaMemcpyDeviceToHost, cs));
+        return H264A_OK;
+    };
+    if (n > 1) {
+        const volatile int32_t* rows = ctx->pp_rows_host;
+        std::vector<int> prefix(n - 1, 0);  // finished rows of each P frame, counted from the top
+        int sent = 0;                       // rows of every P frame queued for download
+        for (;;) {
+            const cudaError_t q = cudaEventQuery(ctx->pp_ev[PP_EV_TQ]);  // before the words: done means all final
+            if (q != cudaSuccess && q != cudaErrorNotReady) {
+                cudaGetLastError();
+                return cuda_fail(q, "pixel_path_host: ME + T/Q");
+            }
+            int ready = mb_h;
+            if (q != cudaSuccess) {
+                for (int f = 0; f < n - 1; f++) {
+                    int r = prefix[f];
+                    while (r < mb_h && rows[size_t(f) * mb_h + r] == token) r++;
+                    prefix[f] = r;
+                    ready = r < ready ? r : ready;
+                }
+            }
+            if (ready > sent) {
+                rc = copy_rows(sent, ready);
+                if (rc) return rc;
+                sent = ready;
+            }
+            if (sent == mb_h) break;
+            std::this_thread::sleep_for(std::chrono::microseconds(100));
+        }
+    }
     H264A_CUDA(cudaStreamWaitEvent(cs, ctx->pp_ev[PP_EV_LA], 0));
     H264A_CUDA(cudaMemcpyAsync(h_la_intra, d_intra, sizeof(int32_t) * nmb * n, cudaMemcpyDeviceToHost, cs));
     H264A_CUDA(cudaMemcpyAsync(h_la_inter, d_inter, sizeof(int32_t) * nmb * n, cudaMemcpyDeviceToHost, cs));

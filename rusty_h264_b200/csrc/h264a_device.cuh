@@ -361,6 +361,16 @@ __device__ __forceinline__ int ld_acquire(const int* p) {
     asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
 }
+// Fetch-and-add at GPU scope with acquire and release semantics.
+__device__ __forceinline__ int atom_add_acq_rel(int* p, int v) {
+    int old;
+    asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+// Release store at system scope (a word the host polls in mapped memory).
+__device__ __forceinline__ void st_release_sys(int* p, int v) {
+    asm volatile("st.release.sys.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
 // Release store at GPU scope: the thread's earlier stores, and those of the
 // lanes that a __syncwarp ordered before it, are visible to any thread whose
 // ld_acquire reads the value (a release fence and a store in one; no separate

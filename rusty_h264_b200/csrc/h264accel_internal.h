@@ -23,9 +23,9 @@ struct WorkQueue {
 // them.  The counters sit 128 bytes apart.
 constexpr int Q_MAIN = 0, Q_LOOKAHEAD = 1, NUM_QUEUES = 2, Q_COUNTER_STRIDE = 32;
 // h264a_pixel_path_host: PP_CHUNKS upload chunks; its events are the
-// uploads, T/Q done and lookahead done.
+// uploads, planes and half-res frames ready, ME + T/Q done, lookahead done.
 constexpr int PP_CHUNKS = 4;
-constexpr int PP_EV_TQ = PP_CHUNKS, PP_EV_LA = PP_CHUNKS + 1, PP_EVENTS = PP_CHUNKS + 2;
+constexpr int PP_EV_INPUTS = PP_CHUNKS, PP_EV_TQ = PP_CHUNKS + 1, PP_EV_LA = PP_CHUNKS + 2, PP_EVENTS = PP_CHUNKS + 3;
 
 struct h264a_ctx {
     int device = 0;
@@ -36,11 +36,21 @@ struct h264a_ctx {
     int32_t *d_counters = nullptr;
     WorkQueue q[NUM_QUEUES];
     int32_t *d_status = nullptr;
-    // cached buffers of h264a_pixel_path_host, its copy stream and events
+    // cached buffers of h264a_pixel_path_host, its copy and lookahead streams
+    // and events
     void *pp_buf = nullptr;
     size_t pp_bytes = 0;
     cudaStream_t copy_stream = nullptr;
+    cudaStream_t la_stream = nullptr;
     cudaEvent_t pp_ev[PP_EVENTS] = {};
+    // row completion of the fused ME + T/Q launch: device counters, and
+    // mapped pinned words the host polls (pp_rows_cap rows), with the token
+    // of the current call
+    int32_t *pp_row_count = nullptr;
+    int32_t *pp_rows_host = nullptr;
+    int32_t *pp_rows_dev = nullptr;
+    size_t pp_rows_cap = 0;
+    int32_t pp_token = 0;
 };
 
 namespace h264a {
@@ -54,6 +64,19 @@ int check_launch(const char *what);
 // grows the per-MB done flags of work queue `queue` to at least n entries
 // (zeroed, epoch reset)
 int ensure_me_scratch(h264a_ctx *ctx, size_t n, int queue = Q_MAIN);
+// Per-frame outputs of the MC + luma T/Q fused into the plain-ME kernel:
+// coefficients (256 i16 per MB, 16-byte aligned), the QP and dead-zone
+// divisor, and optional row completion words (see FrameDesc in me.cu).
+struct MeTqOut {
+    int16_t *coeffs;
+    int qp, dz_div;
+    int32_t *row_count;  // optional: mb_h zeroed counters
+    int32_t *row_done;   // with row_count: mb_h words the host can read
+    int32_t row_token;
+};
+// plain-ME of frames, with the fused T/Q when tq is given (one entry per frame)
+int me_frames_run(h264a_ctx *ctx, const h264a_me_frame *h_frames, int nframes, const h264a_me_params *params,
+                  const MeTqOut *tq, void *stream);
 // the flag value of the next persistent launch on `st`
 int next_epoch(h264a_ctx *ctx, cudaStream_t st, int queue = Q_MAIN);
 

@@ -20,7 +20,7 @@
 #include <string>
 #include <vector>
 
-#include "h264a_device.cuh"
+#include "tq_device.cuh"
 
 namespace h264a {
 
@@ -948,6 +948,16 @@ struct FrameDesc {
     int64_t* costs;
     int flag_base;
     int mb_w, mb_h;
+    // the fused MC + luma T/Q (h264a_me_tq_frames): coefficients out, or
+    // nullptr for none, and the frame QP's quant row
+    int16_t* coeffs;
+    int16_t qff[8], qmf[8];
+    // optional row completion (h264a_pixel_path_host): one counter per MB row
+    // (zeroed), and a host-visible word per row set to row_token once every
+    // MB of the row has its pick and coefficients stored
+    int32_t* row_count;
+    int32_t* row_done;
+    int32_t row_token;
 };
 
 // One launch's frames, passed by value.  Frames are sorted by MB count
@@ -1153,6 +1163,32 @@ __global__ void __launch_bounds__(32 * ME_WARPS, ME_MIN_BLOCKS) me_frames_kernel
             fd.costs[2 * m + 1] = c16;
             st_release(fl + m, epoch);  // orders the pick's stores before the flag
         }
+        // MC + luma T/Q of the MB under its pick (mb16.rs:3436-3450, as
+        // mc_tq_frames_kernel): after the publish, so off the wavefront's
+        // path; lane = 4x4 block, the prediction from the staged window
+        // when it covers the block's MV.
+        if (fd.coeffs != nullptr && lane < 16) {
+            const int bx = (lane & 3) * 4, by = (lane >> 2) * 4;
+            const int part = shape == 1 ? (by >= 8) : (shape == 2 ? (bx >= 8) : 0);
+            const int mvx = part ? mv1x : mv0x, mvy = part ? mv1y : mv0y;
+            const int x = lx + bx, y = ly + by;
+            uint32_t sr[4], pr[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) sr[i] = ld4u(pc.d_src + (long long)(y + i) * pc.cw + x);
+            const int wx = x + pc.pad - scratch[w].wx0 + (mvx >> 2), wy = y + pc.pad - scratch[w].wy0 + (mvy >> 2);
+            if (win_ok && win_covers(wx, wy)) {
+                win_rows(win, wx, wy, mvx & 3, mvy & 3, pr);
+            } else {
+                Planes P;
+                P.base = pc.d_planes; P.pw = pw; P.ph = ph; P.pad = pc.pad; P.ps = (long long)pw * ph;
+                pred_rows(P, x + (mvx >> 2), y + (mvy >> 2), mvx & 3, mvy & 3, pr);
+            }
+            const int qi = (by >= 8 ? 2 : 0) + (bx >= 8 ? 1 : 0), k = ((by & 4) ? 2 : 0) + ((bx & 4) ? 1 : 0);
+            tq4x4_store(sr, pr, fd.qff, fd.qmf, fd.coeffs + (long long)m * 256 + qi * 64 + k * 16);
+        }
+        __syncwarp();  // the lanes' stores ordered before lane 0's count
+        if (fd.row_count != nullptr && lane == 0 && atom_add_acq_rel(fd.row_count + mby, 1) == fd.mb_w - 1)
+            st_release_sys(fd.row_done + mby, fd.row_token);  // the row's last MB: tell the host
         __syncwarp();
     }
 }
@@ -1202,8 +1238,10 @@ extern "C" int h264a_me_search(h264a_ctx* ctx, const h264a_picture* d_pics, int 
     return check_launch("me_search_kernel");
 }
 
-extern "C" int h264a_me_frames(h264a_ctx* ctx, const h264a_me_frame* h_frames, int nframes,
-                               const h264a_me_params* params, void* stream) {
+// Plain-ME of a batch of frames (h264a_me_frames); with `tq`, each frame's
+// MC + luma T/Q is fused in (h264a_me_tq_frames, h264a_pixel_path_host).
+int h264a::me_frames_run(h264a_ctx* ctx, const h264a_me_frame* h_frames, int nframes,
+                         const h264a_me_params* params, const MeTqOut* tq, void* stream) {
     if (!ctx || !h_frames || !params) return fail(H264A_E_ARG, "me_frames: null pointer");
     if (nframes < 1) return fail(H264A_E_ARG, "me_frames: need at least one frame");
     if ((params->mv_cost_kind == 1 || params->mv_cost_kind == 2) && !params->d_mv_cost_tab)
@@ -1245,6 +1283,14 @@ extern "C" int h264a_me_frames(h264a_ctx* ctx, const h264a_me_frame* h_frames, i
             d.mb_w = f.pic.cw / 16;
             d.mb_h = f.pic.ch / 16;
             d.flag_base = int(total);
+            if (tq) {
+                const MeTqOut& t = tq[order[g0 + k]];
+                d.coeffs = t.coeffs;
+                make_quant_row4(t.qp, t.dz_div, d.qff, d.qmf);
+                d.row_count = t.row_count;
+                d.row_done = t.row_done;
+                d.row_token = t.row_token;
+            }
             total += (long long)d.mb_w * d.mb_h;
         }
         long long acc = 0;
@@ -1270,6 +1316,28 @@ extern "C" int h264a_me_frames(h264a_ctx* ctx, const h264a_me_frame* h_frames, i
         if (rc) return rc;
     }
     return H264A_OK;
+}
+
+extern "C" int h264a_me_frames(h264a_ctx* ctx, const h264a_me_frame* h_frames, int nframes,
+                               const h264a_me_params* params, void* stream) {
+    return me_frames_run(ctx, h_frames, nframes, params, nullptr, stream);
+}
+
+extern "C" int h264a_me_tq_frames(h264a_ctx* ctx, const h264a_me_tq_frame* h_frames, int nframes,
+                                  const h264a_me_params* params, void* stream) {
+    if (!ctx || !h_frames || !params) return fail(H264A_E_ARG, "me_tq_frames: null pointer");
+    if (nframes < 1) return fail(H264A_E_ARG, "me_tq_frames: need at least one frame");
+    std::vector<h264a_me_frame> me(nframes);
+    std::vector<MeTqOut> tq(nframes);
+    for (int i = 0; i < nframes; i++) {
+        const h264a_me_tq_frame& f = h_frames[i];
+        if (!f.d_coeffs || (reinterpret_cast<uintptr_t>(f.d_coeffs) & 15) != 0)
+            return fail(H264A_E_ARG, "me_tq_frames: coefficients must be non-null and 16-byte aligned");
+        if (f.qp < 0 || f.qp > 51 || f.dz_div < 1) return fail(H264A_E_ARG, "me_tq_frames: qp out of 0..51 or dz_div < 1");
+        me[i] = f.me;
+        tq[i] = MeTqOut{f.d_coeffs, f.qp, f.dz_div, nullptr, nullptr, 0};
+    }
+    return me_frames_run(ctx, me.data(), nframes, params, tq.data(), stream);
 }
 
 // ---------------------------------------------------------------------------

@@ -63,6 +63,7 @@ def test_struct_layouts_match_header(tmp_path):
 
     mirrors = {"h264a_picture": accel.Picture, "h264a_candidate": accel.Candidate, "h264a_me_params": accel.MeParams,
                "h264a_me_job": accel.MeJob, "h264a_me_result": accel.MeResult, "h264a_me_frame": accel.MeFrame,
+               "h264a_me_tq_frame": accel.MeTqFrame,
                "h264a_tq_frame": accel.TqFrame, "h264a_tq_rec_frame": accel.TqRecFrame,
                "h264a_tq_chroma_frame": accel.TqChromaFrame, "h264a_deblock_frame": accel.DeblockFrame}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "h264accel.h"', "int main(void) {"]

@@ -446,6 +446,42 @@ def test_mc_tq_frames_matches_oracle(acc, cif):
         assert np.array_equal(co.cpu().numpy(), O.mc_tq_frame(src, ref, picks, q, 6))
 
 
+@pytest.mark.parametrize("split", [False, True])
+def test_me_tq_frames_matches_oracle(acc, cif, split):
+    """Plain-ME with each MB's MC + luma T/Q in the same launch: picks, costs
+    and coefficients bit-exact with the oracle's me_frame + mc_tq_frame.  The
+    batch mixes CIF pairs at three QPs, a 160x96 pair, and a pair whose
+    reference is the source moved by (21, 9) pixels, so that early MBs' final
+    MVs lie outside the staged window and their prediction comes from the
+    planes."""
+    params = A.default_me_params()
+    lam = float(np.sqrt(A.frame_lambda(26)))
+    gate = A.split_gate_for_qp(26) if split else -1
+    moved = np.ascontiguousarray(np.roll(cif[2], (9, 21), (0, 1)))
+    small = np.ascontiguousarray(cif[:, 32:128, 48:208])
+    pairs = [(cif[1], cif[0], 22), (cif[2], cif[1], 30), (cif[3], cif[2], 40), (small[1], small[0], 27),
+             (cif[2], moved, 26)]
+    frames, keep, outs = [], [], []
+    for src, ref, q in pairs:
+        ch, cw = src.shape
+        nmb = (cw // 16) * (ch // 16)
+        d_src, d_pl = dev(acc, src), acc.hpel_build(dev(acc, ref[None]), 32)[0]
+        picks = acc.zeros((nmb, 6), acc.torch.int32)
+        costs = acc.zeros((nmb, 2), acc.torch.int64)
+        co = acc.zeros((nmb, 256), acc.torch.int16)
+        keep += [d_src, d_pl]
+        outs.append((picks, costs, co, src, ref, q))
+        me = A.MeFrame(A.Picture(d_src.data_ptr(), d_pl.data_ptr(), cw, ch, 32), lam, gate, picks.data_ptr(),
+                       costs.data_ptr())
+        frames.append(A.MeTqFrame(me, q, 6, co.data_ptr()))
+    acc.me_tq_frames(frames, params)
+    acc.sync()
+    for picks, costs, co, src, ref, q in outs:
+        wp, wc = O.me_frame(src, ref, O.build_planes4(ref, 32), O.balanced_params(), lam, gate)
+        assert np.array_equal(picks.cpu().numpy()[:, :5], wp[:, :5]) and np.array_equal(costs.cpu().numpy(), wc), q
+        assert np.array_equal(co.cpu().numpy(), O.mc_tq_frame(src, ref, wp, q, 6)), q
+
+
 @pytest.mark.parametrize("qp", [0, 10, 24, 30, 51])
 def test_mc_tq_rec_frames_matches_oracle(acc, cif, qp):
     """MC + T/Q with the luma reconstruction (mb16.rs:3575-3605): coefficients
@@ -702,6 +738,31 @@ def test_pixel_path_host_40_frames_matches_oracle(acc):
     got = acc.pixel_path_host(frames, params, lam, gate, qp)
     want = O.pixel_path_clip(frames, O.balanced_params(), lam, gate, qp, nthreads=8)
     compare_pixel_path(got, want)
+
+
+def test_pixel_path_host_pinned_outputs_matches_oracle(acc):
+    """Outputs in pinned host memory, where the bands of finished MB rows
+    come down while the launch still runs: the results equal the oracle's,
+    frame 0's rows are zero, and a second call into the same buffers (filled
+    with -1 at first) gives the same."""
+    torch = acc.torch
+    y, _, _ = synth.cif_clip(12, 9)
+    frames = synth.coded_luma(y)
+    n, ch, cw = frames.shape
+    nmb = (cw // 16) * (ch // 16)
+    params = A.default_me_params()
+    qp = 28
+    lam = float(np.sqrt(A.frame_lambda(qp)))
+    gate = A.split_gate_for_qp(qp)
+    out = {k: torch.full(shape, -1, dtype=dt).pin_memory().numpy() for k, shape, dt in (
+        ("picks", (n, nmb, 6), torch.int32), ("costs", (n, nmb, 2), torch.int64),
+        ("coeffs", (n, nmb, 256), torch.int16), ("la_intra", (n, nmb), torch.int32),
+        ("la_inter", (n, nmb), torch.int32), ("la_mvs", (n, nmb, 2), torch.int32))}
+    for _ in range(2):  # a second call into the same buffers
+        got = acc.pixel_path_host(frames, params, lam, gate, qp, out=out)
+        want = O.pixel_path_clip(frames, O.balanced_params(), lam, gate, qp, nthreads=8)
+        compare_pixel_path(got, want)
+        assert (got["picks"][0] == 0).all() and (got["coeffs"][0] == 0).all() and (got["costs"][0] == 0).all()
 
 
 def test_pixel_path_host_1080p_matches_oracle(acc):
