@@ -381,6 +381,8 @@ extern "C" int h264a_pixel_path_host(h264a_ctx* ctx, const uint8_t* h_frames, in
             const cudaError_t q = cudaEventQuery(ctx->pp_ev[PP_EV_TQ]);  // before the words: done means all final
             if (q != cudaSuccess && q != cudaErrorNotReady) {
                 cudaGetLastError();
+                cudaStreamSynchronize(cs);  // no copy into the caller's buffers outlives the call
+                cudaGetLastError();
                 return cuda_fail(q, "pixel_path_host: ME + T/Q");
             }
             int ready = mb_h;
@@ -394,7 +396,11 @@ extern "C" int h264a_pixel_path_host(h264a_ctx* ctx, const uint8_t* h_frames, in
             }
             if (ready > sent) {
                 rc = copy_rows(sent, ready);
-                if (rc) return rc;
+                if (rc) {
+                    cudaStreamSynchronize(cs);
+                    cudaGetLastError();
+                    return rc;
+                }
                 sent = ready;
             }
             if (sent == mb_h) break;
