@@ -147,6 +147,18 @@ def cpu_baseline(frames: np.ndarray, nthreads: int, lam: float, gate: int):
     return frames.shape[0] * W * H / dt / 1e6, dt
 
 
+def _grid_roofline(nmb: int, R: int, grid_ms: dict, int32_peak: float) -> dict:
+    """INT32 roofline of the exhaustive grid on one frame: SAD is 2 lane-ops
+    per 4 pixels (__vsadu4 + accumulate), SATD 112 per 4x4 block."""
+    cands = nmb * (2 * R + 1) ** 2
+    ops = {"sad": cands * 256 // 2, "satd": cands * 16 * SATD_OPS_PER_4X4}
+    out = {"bound": "int32", "R": R, "unit": "Gop/s", "peak": round(int32_peak, 1), "frame": "one 1920x1088 frame"}
+    for k, ms in grid_ms.items():
+        g = ops[k] / (ms * 1e-3) / 1e9
+        out[k] = {"ms": round(ms, 4), "ops": ops[k], "achieved": round(g, 1), "frac": round(g / int32_peak, 4)}
+    return out
+
+
 def cpu_model() -> dict:
     """Host CPU model name and online core count (stated with every CPU number)."""
     model = "unknown"
@@ -371,6 +383,24 @@ def run_ours(args, ws, rank, local):
         extra["deblock"].append(c2.elapsed_time(d2))
     acc.sync()
     extra_ms = {k: round(float(np.mean(v[1:])), 4) for k, v in extra.items()}
+
+    # The exhaustive full-pel probe as cost grids (h264a_fullpel_grid, not part
+    # of value): one frame at R = 32, the SAD and the SATD argmin timed apart.
+    grid_r = 32
+    pic1 = A.Picture(d_frames[1].data_ptr(), planes[0].data_ptr(), cw, ch, pad)
+    grid_ms = {}
+    for metric, key in ((0, "sad"), (1, "satd")):
+        ts = []
+        for rep in range(4):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            acc.fullpel_grid(pic1, grid_r, metric=metric, want_grids=False)
+            b.record(stream)
+            torch.cuda.synchronize()
+            if rep:
+                ts.append(a.elapsed_time(b))
+        grid_ms[key] = float(np.mean(ts))
+    acc.sync()
     work4x4 = int(picks[1:, :, 5].sum().item())
     int32_peak = acc.measure_int32_peak()
     # The same ME over the first third of the P frames: a launch's time is set
@@ -409,6 +439,7 @@ def run_ours(args, ws, rank, local):
                           "me_ms_third_of_frames": round(float(np.mean(sub_ms)), 3), "frames_in_third": sub_n,
                           "note": "a third of the frames takes most of the launch time: the wavefront's critical "
                                   "path, not INT32 throughput, bounds the kernel"},
+        "fullpel_grid_kernel": _grid_roofline(nmb, grid_r, grid_ms, int32_peak),
         "hpel_kernel": {"bound": "hbm", "achieved_gbs": round(hpel_bytes / (stage["hpel"] * 1e-3) / 1e9, 1),
                         "peak_gbs": hbm_peak, "frac": round(hpel_bytes / (stage["hpel"] * 1e-3) / 1e9 / hbm_peak, 4),
                         "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback 6650"},

@@ -5,9 +5,9 @@
 // dist + (λ·bits(mv − pmv)) in raster order with first-wins ties, the order of
 // the exhaustive probe in motion_search (mb16.rs:2889-2900).
 //
-// One CTA per MB.  The (16+2R)² search window (edge reads clamped, i.e. read
-// from the padded F plane with clamping) is staged once in shared memory and
-// the source MB is held in registers.
+// One CTA per MB and metric.  The (16+2R)² search window (edge reads clamped,
+// i.e. read from the padded F plane with clamping) is staged once in shared
+// memory and the source MB is held in registers.
 //  * SAD: a thread owns one column offset and a run of K row offsets; every
 //    window row is loaded and byte-aligned once and feeds the K candidates it
 //    overlaps with one packed __vsadu4 per 4 pixels.
@@ -40,7 +40,11 @@ __device__ __forceinline__ uint32_t win_word(const uint8_t* row, int x) {
     return sh ? __funnelshift_r(w[0], w[1], sh) : w[0];
 }
 
-__global__ void __launch_bounds__(GRID_THREADS) fullpel_grid_kernel(GridArgs a) {
+// One metric per instance (METRIC 0 SAD, 1 SATD), so that each keeps the
+// source MB in registers without spilling at two CTAs per SM; the instance
+// whose metric is a.metric also forms the argmin.
+template <int METRIC>
+__global__ void __launch_bounds__(GRID_THREADS, 2) fullpel_grid_kernel(GridArgs a) {
     extern __shared__ __align__(16) uint8_t win[];
     __shared__ long long red_key[GRID_THREADS / 32];
     const int mb = blockIdx.x;
@@ -58,27 +62,32 @@ __global__ void __launch_bounds__(GRID_THREADS) fullpel_grid_kernel(GridArgs a) 
     const int wrows = ws + GRID_K;                 // spare rows for the last partial SAD chunk
     // stage the clamped window: picture coords (lx+cxf-R+x, ly+cyf-R+y)
     const int ox = lx + cxf - R + a.P.pad, oy = ly + cyf - R + a.P.pad;
-    for (int i = threadIdx.x; i < wrows * pitch; i += blockDim.x) {
-        const int y = i / pitch, x = i - y * pitch;
-        uint8_t v = 0;
-        if (y < ws && x < ws) {
-            const int py = clampi(oy + y, 0, a.P.ph - 1), px = clampi(ox + x, 0, a.P.pw - 1);
-            v = __ldg(a.P.base + (long long)py * a.P.pw + px);
-        }
-        win[i] = v;
+    for (int y = threadIdx.x >> 5; y < wrows; y += GRID_THREADS / 32) {  // a row per warp, lanes along it
+        const uint8_t* prow = a.P.base + (long long)clampi(oy + y, 0, a.P.ph - 1) * a.P.pw;
+        for (int x = threadIdx.x & 31; x < pitch; x += 32)
+            win[y * pitch + x] = (y < ws && x < ws) ? __ldg(prow + clampi(ox + x, 0, a.P.pw - 1)) : uint8_t(0);
     }
+    // the source MB: in registers for SAD, in shared memory for SATD (whose
+    // four candidates' rows need the registers)
+    __shared__ uint32_t src_s[16][4];
     uint32_t s[16][4];
+    if (METRIC == 0) {
 #pragma unroll
-    for (int r = 0; r < 16; r++)
+        for (int r = 0; r < 16; r++)
 #pragma unroll
-        for (int c = 0; c < 4; c++) s[r][c] = ld4u(a.src + (long long)(ly + r) * a.cw + lx + 4 * c);
+            for (int c = 0; c < 4; c++) s[r][c] = ld4u(a.src + (long long)(ly + r) * a.cw + lx + 4 * c);
+    } else if (threadIdx.x < 64) {
+        src_s[threadIdx.x >> 2][threadIdx.x & 3] =
+            ld4u(a.src + (long long)(ly + (threadIdx.x >> 2)) * a.cw + lx + 4 * (threadIdx.x & 3));
+    }
     __syncthreads();
 
     long long best_key = LLONG_MAX;  // (cost << 32) | scan index; min = first-wins argmin
     const long long grid_base = (long long)mb * n * n;
+    const bool argmin = a.metric == METRIC;
 
     // ---- SAD ----
-    if (a.sad_grid || a.metric == 0) {
+    if (METRIC == 0) {
         const int chunks = (n + GRID_K - 1) / GRID_K;
         for (int item = threadIdx.x; item < n * chunks; item += blockDim.x) {
             const int dxi = item % n, ch = item / n;
@@ -106,7 +115,7 @@ __global__ void __launch_bounds__(GRID_THREADS) fullpel_grid_kernel(GridArgs a) 
                 if (dyi < n) {
                     const int idx = dyi * n + dxi;
                     if (a.sad_grid) a.sad_grid[grid_base + idx] = acc[k];
-                    if (a.metric == 0) {
+                    if (argmin) {
                         const int mvx = (cxf + dxi - R) * 4, mvy = (cyf + dyi - R) * 4;
                         const long long cost =
                             acc[k] + lam_cost(a.lambda, mvbits(a.kind, a.tab, mvx - pmx) + mvbits(a.kind, a.tab, mvy - pmy));
@@ -118,7 +127,7 @@ __global__ void __launch_bounds__(GRID_THREADS) fullpel_grid_kernel(GridArgs a) 
         }
     }
     // ---- SATD ----
-    if (a.satd_grid || a.metric == 1) {
+    if (METRIC == 1) {
         const int gx = (n + 3) / 4;  // groups of four adjacent column offsets
         for (int item = threadIdx.x; item < gx * n; item += blockDim.x) {
             const int g = item % gx, dyi = item / gx;
@@ -138,7 +147,8 @@ __global__ void __launch_bounds__(GRID_THREADS) fullpel_grid_kernel(GridArgs a) 
                         p[2][r] = __funnelshift_r(lo, hi, 16);
                         p[3][r] = __funnelshift_r(lo, hi, 24);
                     }
-                    const uint32_t sr[4] = {s[by * 4][bx], s[by * 4 + 1][bx], s[by * 4 + 2][bx], s[by * 4 + 3][bx]};
+                    const uint32_t sr[4] = {src_s[by * 4][bx], src_s[by * 4 + 1][bx], src_s[by * 4 + 2][bx],
+                                            src_s[by * 4 + 3][bx]};
 #pragma unroll
                     for (int q = 0; q < 4; q++) acc[q] += satd4x4_rows(sr, p[q]);
                 }
@@ -149,7 +159,7 @@ __global__ void __launch_bounds__(GRID_THREADS) fullpel_grid_kernel(GridArgs a) 
                 if (dxi < n) {
                     const int idx = dyi * n + dxi;
                     if (a.satd_grid) a.satd_grid[grid_base + idx] = acc[q];
-                    if (a.metric == 1) {
+                    if (argmin) {
                         const int mvx = (cxf + dxi - R) * 4, mvy = (cyf + dyi - R) * 4;
                         const long long cost =
                             acc[q] + lam_cost(a.lambda, mvbits(a.kind, a.tab, mvx - pmx) + mvbits(a.kind, a.tab, mvy - pmy));
@@ -168,7 +178,7 @@ __global__ void __launch_bounds__(GRID_THREADS) fullpel_grid_kernel(GridArgs a) 
     }
     if ((threadIdx.x & 31) == 0) red_key[threadIdx.x >> 5] = best_key;
     __syncthreads();
-    if (threadIdx.x == 0 && a.best) {
+    if (threadIdx.x == 0 && a.best && argmin) {
         long long k = red_key[0];
         for (int i = 1; i < GRID_THREADS / 32; i++) k = red_key[i] < k ? red_key[i] : k;
         const int idx = int(k & 0xffffffffLL);
@@ -222,8 +232,22 @@ extern "C" int h264a_fullpel_grid(h264a_ctx* ctx, const h264a_picture* h_pic, in
     const int ws = 16 + 2 * R;
     const int pitch = (ws + 4 + 3) & ~3;
     const size_t smem = (size_t)(ws + GRID_K) * pitch;
-    if (smem > 48 * 1024) H264A_CUDA(cudaFuncSetAttribute(fullpel_grid_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     const int nmb = (pc.cw / 16) * (pc.ch / 16);
-    fullpel_grid_kernel<<<nmb, GRID_THREADS, smem, pick_stream(ctx, stream)>>>(a);
-    return check_launch("fullpel_grid_kernel");
+    cudaStream_t st = pick_stream(ctx, stream);
+    // one launch per metric wanted (its grid, or the argmin's metric)
+    if (d_sad_grid || metric == 0) {
+        if (smem > 48 * 1024)
+            H264A_CUDA(cudaFuncSetAttribute(fullpel_grid_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+        fullpel_grid_kernel<0><<<nmb, GRID_THREADS, smem, st>>>(a);
+        const int rc = check_launch("fullpel_grid_kernel<SAD>");
+        if (rc) return rc;
+    }
+    if (d_satd_grid || metric == 1) {
+        if (smem > 48 * 1024)
+            H264A_CUDA(cudaFuncSetAttribute(fullpel_grid_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+        fullpel_grid_kernel<1><<<nmb, GRID_THREADS, smem, st>>>(a);
+        const int rc = check_launch("fullpel_grid_kernel<SATD>");
+        if (rc) return rc;
+    }
+    return H264A_OK;
 }
