@@ -20,6 +20,9 @@
 #include <string>
 #include <vector>
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include "tq_device.cuh"
 
 namespace h264a {
@@ -941,6 +944,10 @@ __global__ void __launch_bounds__(32 * ME_WARPS) me_search_kernel(const h264a_pi
 // ---------------------------------------------------------------------------
 
 struct FrameDesc {
+    // the reference picture's F|H|V|C planes as a 3D tensor (x, y, plane)
+    // with an 80 x 42 x 4 box, the shape of an MB's window; tmap_ok 0 means
+    // the window is staged row by row instead
+    CUtensorMap tmap;
     h264a_picture pic;
     double lambda_me;
     long long split_gate;
@@ -958,6 +965,7 @@ struct FrameDesc {
     int32_t* row_count;
     int32_t* row_done;
     int32_t row_token;
+    int32_t tmap_ok;
 };
 
 // One launch's frames, passed by value.  Frames are sorted by MB count
@@ -974,6 +982,7 @@ struct FrameBatch {
     long long seg_start[ME_MAXF + 1];
     int n;
 };
+static_assert(sizeof(FrameBatch) + 512 <= 32764, "me_frames_kernel's parameters must fit the 32 KB parameter space");
 
 // mbarrier and bulk-copy primitives (shared addresses are 32-bit).
 __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
@@ -995,6 +1004,16 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
                  "l"(src), "r"(bytes), "r"(bar)
                  : "memory");
+}
+
+// One tiled TMA copy of the box at (x, y, 0) of `map` into shared memory,
+// completing on `bar` (no multicast).
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(
+            dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(0), "r"(bar)
+        : "memory");
 }
 
 // Waits (bounded) for the phase `parity` of the warp's window barrier; on
@@ -1102,14 +1121,21 @@ __global__ void __launch_bounds__(32 * ME_WARPS, ME_MIN_BLOCKS) me_frames_kernel
                 scratch[w].wy0 = wy0;
                 // the previous MB's window reads are complete (the warp is converged here)
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                mbar_expect_tx(bar, uint32_t(4 * WIN_H * WIN_W));
+                if (fd.tmap_ok) {  // the whole window in one tensor copy
+                    mbar_expect_tx(bar, uint32_t(WIN_BYTES));
+                    tma_load_3d(win, &fd.tmap, wx0, wy0, bar);
+                } else {
+                    mbar_expect_tx(bar, uint32_t(4 * WIN_H * WIN_W));
+                }
             }
             __syncwarp();
-            const long long ps = (long long)pw * ph;
-            for (int i = lane; i < 4 * WIN_H; i += 32) {
-                const int pl = i / WIN_H, r = i - pl * WIN_H;
-                bulk_g2s(win + uint32_t(pl * WIN_PLANE + r * WIN_STRIDE),
-                         pc.d_planes + ps * pl + (long long)(wy0 + r) * pw + wx0, WIN_W, bar);
+            if (!fd.tmap_ok) {  // a bulk copy per plane row
+                const long long ps = (long long)pw * ph;
+                for (int i = lane; i < 4 * WIN_H; i += 32) {
+                    const int pl = i / WIN_H, r = i - pl * WIN_H;
+                    bulk_g2s(win + uint32_t(pl * WIN_PLANE + r * WIN_STRIDE),
+                             pc.d_planes + ps * pl + (long long)(wy0 + r) * pw + wx0, WIN_W, bar);
+                }
             }
         }
         if (lane == 0) scratch[w].win_ok = win_ok;
@@ -1203,6 +1229,38 @@ __global__ void bounded_wait_selftest_kernel(const int* flag, int* status, int l
 
 using namespace h264a;
 
+// The F|H|V|C planes of a reference picture as a 3D u8 tensor (pw, ph, 4)
+// whose 80 x 42 x 4 box is an MB's window in the WIN_STRIDE / WIN_PLANE
+// layout.  Returns 0 when the planes cannot be described (alignment, or no
+// driver entry point), and the kernel then stages the window row by row.
+static int encode_window_map(CUtensorMap* map, const uint8_t* planes, int pw, int ph) {
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    static bool looked_up = false;
+    if (!looked_up) {
+        looked_up = true;
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+        else
+            cudaGetLastError();
+    }
+    if (!encode || (reinterpret_cast<uintptr_t>(planes) & 15) != 0 || pw % 16 != 0 || pw < WIN_W || ph < WIN_H)
+        return 0;
+    static_assert(WIN_STRIDE % 16 == 0 && WIN_PLANE == WIN_H * WIN_STRIDE && WIN_BYTES == 4 * WIN_PLANE,
+                  "the window is one dense 3D box");
+    const cuuint64_t dim[3] = {cuuint64_t(pw), cuuint64_t(ph), 4};
+    const cuuint64_t stride[2] = {cuuint64_t(pw), cuuint64_t(pw) * cuuint64_t(ph)};  // bytes, dims 1 and 2
+    const cuuint32_t box[3] = {WIN_STRIDE, WIN_H, 4};
+    const cuuint32_t estride[3] = {1, 1, 1};
+    return encode(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<uint8_t*>(planes), dim, stride, box, estride,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS
+               ? 1
+               : 0;
+}
+
 // Dynamic shared memory of me_frames_kernel, its opt-in above 48 KB, and the
 // CTAs per SM it reaches.
 static int me_frames_setup(int& per_sm) {
@@ -1276,6 +1334,7 @@ int h264a::me_frames_run(h264a_ctx* ctx, const h264a_me_frame* h_frames, int nfr
             const h264a_me_frame& f = h_frames[order[g0 + k]];
             FrameDesc& d = fb.f[k];
             d.pic = f.pic;
+            d.tmap_ok = encode_window_map(&d.tmap, f.pic.d_planes, f.pic.cw + 2 * f.pic.pad, f.pic.ch + 2 * f.pic.pad);
             d.lambda_me = f.lambda_me;
             d.split_gate = f.split_gate;
             d.picks = f.d_picks;
@@ -1436,6 +1495,7 @@ extern "C" int h264a_me_frames_noalloc(const h264a_me_frame* h_frames, int nfram
         const h264a_me_frame& f = h_frames[order[k]];
         FrameDesc& d = fb.f[k];
         d.pic = f.pic;
+        d.tmap_ok = encode_window_map(&d.tmap, f.pic.d_planes, f.pic.cw + 2 * f.pic.pad, f.pic.ch + 2 * f.pic.pad);
         d.lambda_me = f.lambda_me;
         d.split_gate = f.split_gate;
         d.picks = f.d_picks;
