@@ -544,8 +544,9 @@ struct GroupGeom {
 };
 
 // mode 0: the MB's 16x16 search (one group); mode 1: its four partitions.
+// pre: for mode 0, the lane's source rows already loaded (block lane & 15).
 __device__ __forceinline__ void group_geom_init(GroupGeom& q, WarpScratch& ws, const h264a_picture& pc, int mx, int my,
-                                                int mode, uint32_t win) {
+                                                int mode, uint32_t win, const uint32_t* pre) {
     const int lane = threadIdx.x & 31;
     SearchGeom& g = q.s;
     int x = mx, y = my;
@@ -593,7 +594,7 @@ __device__ __forceinline__ void group_geom_init(GroupGeom& q, WarpScratch& ws, c
     }
     uint32_t srow[4];
 #pragma unroll
-    for (int r = 0; r < 4; r++) srow[r] = ld4u(pc.d_src + (long long)(y + g.byo + r) * pc.cw + x + g.bxo);
+    for (int r = 0; r < 4; r++) srow[r] = pre ? pre[r] : ld4u(pc.d_src + (long long)(y + g.byo + r) * pc.cw + x + g.bxo);
     split_pairs(srow, g.spa, g.spb);
     __syncwarp();
 }
@@ -1089,6 +1090,13 @@ __global__ void __launch_bounds__(32 * ME_WARPS, ME_MIN_BLOCKS) me_frames_kernel
         wave_mb(fd.mb_w, fd.mb_h, k, mbx, mby);
         const int m = mby * fd.mb_w + mbx;
         int* fl = flags + fd.flag_base;
+        const int lx = mbx * 16, ly = mby * 16;
+        // the source rows of the lane's 4x4 block in the 16x16 search (block
+        // lane & 15), loaded before the neighbour wait: the source is an input
+        uint32_t src4[4];
+#pragma unroll
+        for (int r = 0; r < 4; r++)
+            src4[r] = ld4u(fd.pic.d_src + (long long)(ly + ((lane >> 2) & 3) * 4 + r) * fd.pic.cw + lx + (lane & 3) * 4);
         // dependencies: left, and top-right (or top at the right edge)
         if (lane == 0) {
             if (mbx > 0) wait_flag(fl + m - 1, epoch, status, 1, spin_limit);
@@ -1106,7 +1114,6 @@ __global__ void __launch_bounds__(32 * ME_WARPS, ME_MIN_BLOCKS) me_frames_kernel
             c = da ? pick_mv_at(fd.picks, m - fd.mb_w - 1, 3, 3) : make_int2(0, 0);
         }
         const int2 pmv = predict_mv_ref0(aa, a, ba, bb, cav, c);
-        const int lx = mbx * 16, ly = mby * 16;
         // stage the window: WIN_R rows/columns up-left of the predicted
         // position, the x origin on a 16-byte boundary (bulk-copy alignment)
         const h264a_picture& pc = fd.pic;
@@ -1149,7 +1156,7 @@ __global__ void __launch_bounds__(32 * ME_WARPS, ME_MIN_BLOCKS) me_frames_kernel
         for (int mode = 0; mode < 2; mode++) {
             if (mode == 1 && !(fd.split_gate >= 0 && c16 > fd.split_gate)) break;
             GroupGeom qg;
-            group_geom_init(qg, scratch[w], pc, lx, ly, mode, win);
+            group_geom_init(qg, scratch[w], pc, lx, ly, mode, win, mode == 0 ? src4 : nullptr);
             if (mode == 0 && win_ok) {
                 wait_window(bar, parity, status, 3, spin_limit);
                 parity ^= 1u;
@@ -1198,9 +1205,8 @@ __global__ void __launch_bounds__(32 * ME_WARPS, ME_MIN_BLOCKS) me_frames_kernel
             const int part = shape == 1 ? (by >= 8) : (shape == 2 ? (bx >= 8) : 0);
             const int mvx = part ? mv1x : mv0x, mvy = part ? mv1y : mv0y;
             const int x = lx + bx, y = ly + by;
-            uint32_t sr[4], pr[4];
-#pragma unroll
-            for (int i = 0; i < 4; i++) sr[i] = ld4u(pc.d_src + (long long)(y + i) * pc.cw + x);
+            uint32_t pr[4];
+            const uint32_t* sr = src4;  // lane < 16: the same block as the 16x16 search
             const int wx = x + pc.pad - scratch[w].wx0 + (mvx >> 2), wy = y + pc.pad - scratch[w].wy0 + (mvy >> 2);
             if (win_ok && win_covers(wx, wy)) {
                 win_rows(win, wx, wy, mvx & 3, mvy & 3, pr);
