@@ -657,18 +657,46 @@ __device__ __forceinline__ bool group_in_plane_window(const GroupGeom& q, const 
 
 // motion_search (mb16.rs:2433-3302) of the lane's partition, every group at
 // once; same phases, order and pricing as motion_search_warp.
-__device__ __forceinline__ void motion_search_group(const GroupGeom& q, const MeParamsDev& pr, WarpScratch& ws,
+// The search's knobs: read from the parameters, or, for the Balanced preset
+// (BAL, h264a_me_params_default), compile-time constants, so that the control
+// logic of every round folds to the preset's path.
+template <bool BAL>
+struct Knobs {
+    const MeParamsDev& p;
+    __device__ __forceinline__ bool fast() const { return BAL ? false : p.fast != 0; }
+    __device__ __forceinline__ bool use_sad() const { return BAL ? false : p.use_sad != 0; }
+    __device__ __forceinline__ bool sadfp() const { return BAL ? false : p.sadfp != 0; }
+    __device__ __forceinline__ int kind() const { return BAL ? 0 : p.kind; }
+    __device__ __forceinline__ bool me_snap() const { return BAL ? true : p.me_snap != 0; }
+    __device__ __forceinline__ bool fc() const { return BAL ? true : p.fc != 0; }
+    __device__ __forceinline__ uint32_t dia_mask() const { return BAL ? 0x1cu : p.dia_mask; }
+    __device__ __forceinline__ bool subpel() const { return BAL ? true : p.subpel != 0; }
+    __device__ __forceinline__ int subpel_pat() const { return BAL ? -1 : p.subpel_pat; }
+    __device__ __forceinline__ bool sp_single_pass() const { return BAL ? true : p.sp_single_pass != 0; }
+    __device__ __forceinline__ bool me_subpel_iter() const { return BAL ? true : p.me_subpel_iter != 0; }
+    __device__ __forceinline__ int sp_maxit() const { return BAL ? 0 : p.sp_maxit; }
+    __device__ __forceinline__ bool sp_fc() const { return BAL ? false : p.sp_fc != 0; }
+    __device__ __forceinline__ double sadfp_lambda() const { return p.sadfp_lambda; }
+    // rate of an MV against the search's mvd centre (mb16.rs:2454-2482)
+    __device__ __forceinline__ uint32_t rate(const WarpScratch& ws, int mvx, int mvy) const {
+        return mvbits(kind(), p.tab, mvx - ws.cx) + mvbits(kind(), p.tab, mvy - ws.cy);
+    }
+};
+
+template <bool BAL>
+__device__ __forceinline__ void motion_search_group(const GroupGeom& q, const MeParamsDev& prm, WarpScratch& ws,
                                                     const int* preds, int npred, double lambda_me, int& out_x,
                                                     int& out_y, long long& out_c, int& evals) {
+    const Knobs<BAL> pr{prm};
     const int gl = q.gl, gb = q.gb;
-    const bool sadfp = !pr.fast && pr.sadfp;
-    const int m_main = pr.use_sad ? MET_SAD : MET_SATD;
+    const bool sadfp = !pr.fast() && pr.sadfp();
+    const int m_main = pr.use_sad() ? MET_SAD : MET_SATD;
     if (q.s.lane == 0) {
         ws.cx = preds[0];
         ws.cy = preds[1];
         ws.lam_me = lambda_me;
-        ws.lam_r = pr.kind != 0 ? lambda_me * 0.25 : lambda_me;
-        ws.lam_fp = lambda_me * (sadfp ? pr.sadfp_lambda : 1.0);
+        ws.lam_r = pr.kind() != 0 ? lambda_me * 0.25 : lambda_me;
+        ws.lam_fp = lambda_me * (sadfp ? pr.sadfp_lambda() : 1.0);
     }
     // seeds and the snaps of sub-pel predictors (as motion_search_warp), per group
     int qx = 0, qy = 0;
@@ -679,17 +707,17 @@ __device__ __forceinline__ void motion_search_group(const GroupGeom& q, const Me
         ws.cand[gb + gl] = make_int2(qx, qy);
     }
     const unsigned snaps =
-        (__ballot_sync(0xffffffffu, pr.me_snap && mine && ((qx & 3) != 0 || (qy & 3) != 0)) >> gb) & q.gmask;
+        (__ballot_sync(0xffffffffu, pr.me_snap() && mine && ((qx & 3) != 0 || (qy & 3) != 0)) >> gb) & q.gmask;
     if ((snaps >> gl) & 1u)
         ws.cand[gb + npred + 1 + __popc(snaps & ((1u << gl) - 1u))] = make_int2(((qx + 2) >> 2) * 4, ((qy + 2) >> 2) * 4);
     __syncwarp();
     const int m_fp = sadfp ? MET_SAD : m_main;
     const double l_fp = sadfp ? ws.lam_fp : ws.lam_r;
     const int rw = q.rw, rh = q.rh;
-    const bool fc = !pr.fast && pr.fc;  // 16x16, 16x8 and 8x16 are x4 shapes
-    const uint32_t dmask = pr.fast ? 0u : pr.dia_mask;
-    const int spat = pr.subpel_pat >= 0 ? pr.subpel_pat : (pr.sp_single_pass ? 2 : 0);
-    const bool sp_fc = pr.sp_fc && !pr.fast;
+    const bool fc = !pr.fast() && pr.fc();  // 16x16, 16x8 and 8x16 are x4 shapes
+    const uint32_t dmask = pr.fast() ? 0u : pr.dia_mask();
+    const int spat = pr.subpel_pat() >= 0 ? pr.subpel_pat() : (pr.sp_single_pass() ? 2 : 0);
+    const bool sp_fc = pr.sp_fc() && !pr.fast();
     const int sp_nring = (spat & 1) ? 4 : 8;
 
     evals = 0;
@@ -716,7 +744,7 @@ __device__ __forceinline__ void motion_search_group(const GroupGeom& q, const Me
                 }
                 if (si < 0 || loops >= LOOP_GUARD) {
                     int nsi = si + 1;
-                    if (pr.fast) nsi = nsi >= 2 ? 5 : nsi;
+                    if (pr.fast()) nsi = nsi >= 2 ? 5 : nsi;
                     else
                         while (nsi < 5 && !(dmask & (1u << nsi))) nsi++;
                     if (nsi >= 5) {
@@ -724,7 +752,7 @@ __device__ __forceinline__ void motion_search_group(const GroupGeom& q, const Me
                         continue;
                     }
                     si = nsi;
-                    step = pr.fast ? (si == 0 ? 16 : 4) : (64 >> si);
+                    step = pr.fast() ? (si == 0 ? 16 : 4) : (64 >> si);
                     loops = 0;
                 }
                 loops++;
@@ -760,7 +788,7 @@ __device__ __forceinline__ void motion_search_group(const GroupGeom& q, const Me
                         ws.cand[gb + gl] = make_int2(bx + ring_dx(ring_i + gl) * step, by + ring_dy(ring_i + gl) * step);
                     break;
                 }
-                if (!pr.subpel) {
+                if (!pr.subpel()) {
                     phase = PH_DONE;
                     continue;
                 }
@@ -798,6 +826,13 @@ __device__ __forceinline__ void motion_search_group(const GroupGeom& q, const Me
         }
         if (kind < 0) n = 0;
         if (__all_sync(0xffffffffu, kind < 0)) break;
+        // which collectives this round's folds need, decided before the pricing
+        // (votes off the critical path): the group minimum for fixed-centre
+        // rings, the first improvement for cascading rings, the seed costs for
+        // the seed and reprice rounds
+        const bool need_min = __any_sync(0xffffffffu, kind == EV_FIXED);
+        const bool need_hit = __any_sync(0xffffffffu, kind == EV_RING);
+        const bool need_seed = __any_sync(0xffffffffu, kind == EV_SEEDS || kind == EV_REPRICE);
         __syncwarp();
 
         // ---------- price ----------
@@ -805,19 +840,29 @@ __device__ __forceinline__ void motion_search_group(const GroupGeom& q, const Me
         int cc = INT_MAX;  // dist + λ·rate of slot gb + gl, as lane_cost prices it
         if (gl < n) {
             const int2 mv = ws.cand[gb + gl];
-            const long long c = (long long)ws.dist[gb + gl] + lam_cost(lam, rate_of(pr, ws, mv.x, mv.y));
+            const long long c = (long long)ws.dist[gb + gl] + lam_cost(lam, pr.rate(ws, mv.x, mv.y));
             cc = c > INT_MAX - 1 ? INT_MAX - 1 : int(c);
         }
-        // group-wide collectives, taken by every lane
+        // group-wide collectives, taken by every lane (each only in rounds
+        // where some group's fold reads it; the conditions are warp-uniform)
         int gmin = cc;
-        for (int o = 1; o < (1 << q.lg); o <<= 1) gmin = min(gmin, __shfl_xor_sync(0xffffffffu, gmin, o));
-        const unsigned at = (__ballot_sync(0xffffffffu, cc == gmin) >> gb) & q.gmask;
-        const unsigned hit = (__ballot_sync(0xffffffffu, gl < n && cc < best_c) >> gb) & q.gmask;
-        const int jhit = hit ? __ffs(hit) - 1 : 0;
-        const int cj = __shfl_sync(0xffffffffu, cc, gb + jhit);
-        int c_seed[3];
+        unsigned at = 0;
+        if (need_min) {
+            for (int o = 1; o < (1 << q.lg); o <<= 1) gmin = min(gmin, __shfl_xor_sync(0xffffffffu, gmin, o));
+            at = (__ballot_sync(0xffffffffu, cc == gmin) >> gb) & q.gmask;
+        }
+        unsigned hit = 0;
+        int jhit = 0, cj = 0;
+        if (need_hit) {
+            hit = (__ballot_sync(0xffffffffu, gl < n && cc < best_c) >> gb) & q.gmask;
+            jhit = hit ? __ffs(hit) - 1 : 0;
+            cj = __shfl_sync(0xffffffffu, cc, gb + jhit);
+        }
+        int c_seed[3] = {0, 0, 0};
+        if (need_seed) {
 #pragma unroll
-        for (int i = 0; i < 3; i++) c_seed[i] = __shfl_sync(0xffffffffu, cc, gb + i);
+            for (int i = 0; i < 3; i++) c_seed[i] = __shfl_sync(0xffffffffu, cc, gb + i);
+        }
 
         // ---------- fold (per group) ----------
         if (kind == EV_SEEDS) {
@@ -839,13 +884,13 @@ __device__ __forceinline__ void motion_search_group(const GroupGeom& q, const Me
             if ((snaps >> wi) & 1u) {
                 const int sl = gb + npred + 1 + __popc(snaps & ((1u << wi) - 1u));
                 bx = ws.cand[sl].x; by = ws.cand[sl].y;
-                best_c = int(cand_cost64(pr, ws, sl, lam));
+                best_c = int(((long long)ws.dist[sl] + lam_cost(lam, pr.rate(ws, ws.cand[sl].x, ws.cand[sl].y))));
                 evals += 1;
             }
             phase = PH_DIA;
         } else if (kind == EV_REPRICE) {
-            best_c = int(cand_cost64(pr, ws, gb, lam));
-            seed_c = int(cand_cost64(pr, ws, gb + 1, lam));
+            best_c = int(((long long)ws.dist[gb] + lam_cost(lam, pr.rate(ws, ws.cand[gb].x, ws.cand[gb].y))));
+            seed_c = int(((long long)ws.dist[gb + 1] + lam_cost(lam, pr.rate(ws, ws.cand[gb + 1].x, ws.cand[gb + 1].y))));
             evals += 2;
             phase = PH_SUB;
         } else if (kind == EV_FIXED) {
@@ -859,7 +904,7 @@ __device__ __forceinline__ void motion_search_group(const GroupGeom& q, const Me
             if (phase == PH_DIA) {
                 if (bi < 0) loops = LOOP_GUARD;
             } else {
-                const bool stop = bi < 0 || !pr.me_subpel_iter || (spat & 2) || (pr.sp_maxit != 0 && iter >= pr.sp_maxit);
+                const bool stop = bi < 0 || !pr.me_subpel_iter() || (spat & 2) || (pr.sp_maxit() != 0 && iter >= pr.sp_maxit());
                 if (stop) loops = LOOP_GUARD;
             }
         } else if (kind == EV_RING) {
@@ -880,15 +925,15 @@ __device__ __forceinline__ void motion_search_group(const GroupGeom& q, const Me
             if (!ring_open) {
                 if (phase == PH_DIA) {
                     if (!ring_improved) loops = LOOP_GUARD;
-                } else if (!ring_improved || !pr.me_subpel_iter || (spat & 2) ||
-                           (pr.sp_maxit != 0 && iter >= pr.sp_maxit)) {
+                } else if (!ring_improved || !pr.me_subpel_iter() || (spat & 2) ||
+                           (pr.sp_maxit() != 0 && iter >= pr.sp_maxit())) {
                     loops = LOOP_GUARD;
                 }
             }
         }
         __syncwarp();
     }
-    if (pr.me_snap && seed_c < best_c) {
+    if (pr.me_snap() && seed_c < best_c) {
         bx = seed_x; by = seed_y; best_c = seed_c;
     }
     out_x = bx; out_y = by; out_c = best_c;
@@ -1056,6 +1101,7 @@ __device__ __forceinline__ int2 predict_mv_ref0(bool aa, int2 a, bool ba, int2 b
 // for 16x16 and, when its J exceeds the gate, for the four 16x8/8x16
 // partitions (mb16.rs:8869-8913), and publishes the pick.
 // Dynamic shared memory: ME_WARPS windows of WIN_BYTES.
+template <bool BAL>
 __global__ void __launch_bounds__(32 * ME_WARPS, ME_MIN_BLOCKS) me_frames_kernel(const __grid_constant__ FrameBatch batch,
                                                                     long long total,
                                                                     const __grid_constant__ MeParamsDev prm,
@@ -1163,7 +1209,7 @@ __global__ void __launch_bounds__(32 * ME_WARPS, ME_MIN_BLOCKS) me_frames_kernel
             }
             int rx, ry, ev;
             long long rc;
-            motion_search_group(qg, prm, scratch[w], preds, mode == 0 ? 1 : 2, fd.lambda_me, rx, ry, rc, ev);
+            motion_search_group<BAL>(qg, prm, scratch[w], preds, mode == 0 ? 1 : 2, fd.lambda_me, rx, ry, rc, ev);
             if (mode == 0) {
                 evals = ev << 4;  // 4x4-block evaluations
                 c16 = rc; best = rc;
@@ -1271,11 +1317,30 @@ static int encode_window_map(CUtensorMap* map, const uint8_t* planes, int pw, in
 // CTAs per SM it reaches.
 static int me_frames_setup(int& per_sm) {
     const int smem = ME_WARPS * WIN_BYTES;
-    H264A_CUDA(cudaFuncSetAttribute(me_frames_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    H264A_CUDA(cudaFuncSetAttribute(me_frames_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    H264A_CUDA(cudaFuncSetAttribute(me_frames_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     per_sm = 0;
-    H264A_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, me_frames_kernel, 32 * ME_WARPS, smem));
+    H264A_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, me_frames_kernel<false>, 32 * ME_WARPS, smem));
     if (per_sm < 1) per_sm = 1;
     return H264A_OK;
+}
+
+// True when the parameters are the Balanced preset's (h264a_me_params_default):
+// the frame kernel then runs its instance with those knobs as constants.
+static bool balanced_preset(const MeParamsDev& p) {
+    return p.fast == 0 && p.use_sad == 0 && p.sadfp == 0 && p.kind == 0 && p.me_snap == 1 && p.fc == 1 &&
+           p.dia_mask == 0x1cu && p.subpel == 1 && p.subpel_pat == -1 && p.sp_single_pass == 1 &&
+           p.me_subpel_iter == 1 && p.sp_maxit == 0 && p.sp_fc == 0;
+}
+
+static void launch_me_frames(const MeParamsDev& prm, unsigned blocks, cudaStream_t st, const FrameBatch& fb,
+                             long long total, int* counter, int* flags, int epoch, int* status) {
+    if (balanced_preset(prm))
+        me_frames_kernel<true><<<blocks, 32 * ME_WARPS, ME_WARPS * WIN_BYTES, st>>>(fb, total, prm, counter, flags, epoch,
+                                                                                status, SPIN_LIMIT);
+    else
+        me_frames_kernel<false><<<blocks, 32 * ME_WARPS, ME_WARPS * WIN_BYTES, st>>>(fb, total, prm, counter, flags,
+                                                                                 epoch, status, SPIN_LIMIT);
 }
 
 extern "C" int h264a_selftest_bounded_wait(h264a_ctx* ctx, int spin_limit, void* stream) {
@@ -1375,8 +1440,8 @@ int h264a::me_frames_run(h264a_ctx* ctx, const h264a_me_frame* h_frames, int nfr
         long long blocks = (long long)ctx->num_sms * per_sm;
         const long long need = (total + ME_WARPS - 1) / ME_WARPS;
         if (blocks > need) blocks = need;
-        me_frames_kernel<<<unsigned(blocks), 32 * ME_WARPS, ME_WARPS * WIN_BYTES, st>>>(fb, total, prm, ctx->q[Q_MAIN].d_counter, ctx->q[Q_MAIN].d_flags,
-                                                                     epoch, ctx->d_status, SPIN_LIMIT);
+        launch_me_frames(prm, unsigned(blocks), st, fb, total, ctx->q[Q_MAIN].d_counter, ctx->q[Q_MAIN].d_flags, epoch,
+                         ctx->d_status);
         rc = check_launch("me_frames_kernel");
         if (rc) return rc;
     }
@@ -1530,7 +1595,6 @@ extern "C" int h264a_me_frames_noalloc(const h264a_me_frame* h_frames, int nfram
     const long long need = (total + ME_WARPS - 1) / ME_WARPS;
     if (blocks > need) blocks = need;
     const MeParamsDev prm = to_dev(*params);
-    me_frames_kernel<<<unsigned(blocks), 32 * ME_WARPS, ME_WARPS * WIN_BYTES, st>>>(fb, total, prm, scratch, scratch + 1, epoch,
-                                                                 d_status, SPIN_LIMIT);
+    launch_me_frames(prm, unsigned(blocks), st, fb, total, scratch, scratch + 1, epoch, d_status);
     return check_launch("me_frames_kernel (no-alloc)");
 }
