@@ -602,6 +602,8 @@ __device__ __forceinline__ void group_geom_init(GroupGeom& q, WarpScratch& ws, c
 // Distortions of each group's candidates ws.cand[gb..gb+n) (n and metric per
 // group) into ws.dist.  A group prices 2^(lg - lg_nb) candidates per pass;
 // passes run to the largest need over the groups.
+// SATD_ONLY: the caller's preset never prices with SAD (Balanced).
+template <bool SATD_ONLY>
 __device__ __forceinline__ void eval_round_group(const GroupGeom& q, WarpScratch& ws, int n, int metric) {
     const SearchGeom& g = q.s;
     const int cps = q.lg - g.lg_nb;  // log2 candidates per pass of a group
@@ -633,7 +635,7 @@ __device__ __forceinline__ void eval_round_group(const GroupGeom& q, WarpScratch
                 const int c = (k << cps) + sub;
                 int d = 0;
                 if (c < n) {
-                    if (metric == MET_SAD) {
+                    if (!SATD_ONLY && metric == MET_SAD) {
                         uint32_t srow[4];
 #pragma unroll
                         for (int r = 0; r < 4; r++) srow[r] = g.spa[r] | (g.spb[r] << 8);
@@ -836,7 +838,7 @@ __device__ __forceinline__ void motion_search_group(const GroupGeom& q, const Me
         __syncwarp();
 
         // ---------- price ----------
-        eval_round_group(q, ws, n, metric);
+        eval_round_group<BAL>(q, ws, n, metric);
         int cc = INT_MAX;  // dist + λ·rate of slot gb + gl, as lane_cost prices it
         if (gl < n) {
             const int2 mv = ws.cand[gb + gl];
