@@ -1288,18 +1288,15 @@ using namespace h264a;
 // layout.  Returns 0 when the planes cannot be described (alignment, or no
 // driver entry point), and the kernel then stages the window row by row.
 static int encode_window_map(CUtensorMap* map, const uint8_t* planes, int pw, int ph) {
-    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
-    static bool looked_up = false;
-    if (!looked_up) {
-        looked_up = true;
+    static const PFN_cuTensorMapEncodeTiled_v12000 encode = [] {  // looked up once, thread-safely
         void* fn = nullptr;
         cudaDriverEntryPointQueryResult q;
         if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
             q == cudaDriverEntryPointSuccess)
-            encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
-        else
-            cudaGetLastError();
-    }
+            return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+        cudaGetLastError();
+        return PFN_cuTensorMapEncodeTiled_v12000(nullptr);
+    }();
     if (!encode || (reinterpret_cast<uintptr_t>(planes) & 15) != 0 || pw % 16 != 0 || pw < WIN_W || ph < WIN_H)
         return 0;
     static_assert(WIN_STRIDE % 16 == 0 && WIN_PLANE == WIN_H * WIN_STRIDE && WIN_BYTES == 4 * WIN_PLANE,
