@@ -600,14 +600,16 @@ __device__ __forceinline__ void group_geom_init(GroupGeom& q, WarpScratch& ws, c
 }
 
 // Distortions of each group's candidates ws.cand[gb..gb+n) (n and metric per
-// group) into ws.dist.  A group prices 2^(lg - lg_nb) candidates per pass;
-// passes run to the largest need over the groups.
-// SATD_ONLY: the caller's preset never prices with SAD (Balanced).
+// group) added into ws.dist, which the caller has zeroed: each lane adds its
+// 4x4 block's distortion to its candidate's slot with a shared-memory atomic
+// (exact, so the order does not matter), which has a shorter dependency chain
+// than a shuffle tree over the candidate's lanes.  A group prices
+// 2^(lg - lg_nb) candidates per pass; passes run to the largest need over the
+// groups.  SATD_ONLY: the caller's preset never prices with SAD (Balanced).
 template <bool SATD_ONLY>
 __device__ __forceinline__ void eval_round_group(const GroupGeom& q, WarpScratch& ws, int n, int metric) {
     const SearchGeom& g = q.s;
     const int cps = q.lg - g.lg_nb;  // log2 candidates per pass of a group
-    const int nb = 1 << g.lg_nb;
     const int npass = __reduce_max_sync(0xffffffffu, (n + (1 << cps) - 1) >> cps);
     const int sub = q.gl >> g.lg_nb;  // which of the pass's candidates the lane serves
     for (int k0 = 0; k0 < npass; k0 += ME_MAX_PASS) {
@@ -644,8 +646,7 @@ __device__ __forceinline__ void eval_round_group(const GroupGeom& q, WarpScratch
                         d = satd4x4_packed(g.spa, g.spb, pr4[kk]);
                     }
                 }
-                d = warp_seg_sum(d, nb);
-                if (c < n && (q.gl & (nb - 1)) == 0) ws.dist[q.gb + c] = d;
+                if (c < n) atomicAdd(&ws.dist[q.gb + c], d);  // the candidate's blocks, summed in shared memory
             }
         }
     }
@@ -835,6 +836,8 @@ __device__ __forceinline__ void motion_search_group(const GroupGeom& q, const Me
         const bool need_min = __any_sync(0xffffffffu, kind == EV_FIXED);
         const bool need_hit = __any_sync(0xffffffffu, kind == EV_RING);
         const bool need_seed = __any_sync(0xffffffffu, kind == EV_SEEDS || kind == EV_REPRICE);
+        if (gl < n) ws.dist[gb + gl] = 0;  // the pricing adds each lane's block into its candidate's slot
+        __syncwarp();
         __syncwarp();
 
         // ---------- price ----------
