@@ -110,9 +110,9 @@ struct LaSearch {
     }
 
     // SATD of each group's cand[gb..gb+n) (full-pel MVs, quarter-pel units)
-    // into dist; passes run to the larger group's need.
+    // added into dist (zeroed by the caller) by shared-memory atomics of the
+    // lanes' 4x4 blocks; passes run to the larger group's need.
     __device__ void eval(int n) {
-        const int nb = 1 << lg_nb;
         const int cps = 4 - lg_nb;  // log2 candidates per pass of a group
         const int npass = __reduce_max_sync(0xffffffffu, (n + (1 << cps) - 1) >> cps);
         for (int k = 0; k < npass; k++) {
@@ -127,8 +127,7 @@ struct LaSearch {
                     subpel_rows_clamped(ref, w, h, x0 + bxo + (mv.x >> 2), y0 + byo + (mv.y >> 2), mv.x & 3, mv.y & 3, p);
                 d = satd4x4_rows(srow, p);
             }
-            d = warp_seg_sum(d, nb);
-            if (c < n && (gl & (nb - 1)) == 0) dist[gb + c] = d;
+            if (c < n) atomicAdd(&dist[gb + c], d);  // the candidate's blocks, summed in shared memory
         }
         __syncwarp();
     }
@@ -166,6 +165,7 @@ __device__ void la_inter_cost(LaSearch& s, bool active, int seedx, int seedy, in
                 s.cand[gb + gl] = make_int2(bx + la_ring_dx(ri + gl) * step * 4, by + la_ring_dy(ri + gl) * step * 4);
         }
         if (__all_sync(0xffffffffu, phase == 2)) break;
+        if (gl < n) s.dist[gb + gl] = 0;  // eval adds each lane's block into its candidate's slot
         __syncwarp();
         s.eval(n);
         const int d = gl < n ? s.dist[gb + gl] : 0;
