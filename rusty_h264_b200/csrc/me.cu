@@ -145,8 +145,9 @@ __device__ __forceinline__ void geom_init(SearchGeom& g, WarpScratch& ws, const 
 // Distortions of ws.cand[0..n) under `metric` into ws.dist.  All the round's
 // plane loads are issued before any is consumed, so a round pays one memory
 // latency however many passes it takes.
+// Distortions of ws.cand[0..n) added into ws.dist (zeroed by the caller) by
+// shared-memory atomics of the lanes' 4x4 blocks.
 __device__ __forceinline__ void eval_round(const SearchGeom& g, WarpScratch& ws, int n, int metric) {
-    const int nb = 1 << g.lg_nb;
     const int npass = ((n << g.lg_nb) + 31) >> 5;
     for (int k0 = 0; k0 < npass; k0 += ME_MAX_PASS) {
     uint32_t pr4[ME_MAX_PASS][4];
@@ -183,8 +184,7 @@ __device__ __forceinline__ void eval_round(const SearchGeom& g, WarpScratch& ws,
                     d = satd4x4_packed(g.spa, g.spb, pr4[kk]);
                 }
             }
-            d = warp_seg_sum(d, nb);
-            if (c < n && (g.lane & (nb - 1)) == 0) ws.dist[c] = d;
+            if (c < n) atomicAdd(&ws.dist[c], d);  // the candidate's blocks, summed in shared memory
         }
     }
     }
@@ -427,6 +427,7 @@ __device__ __forceinline__ void motion_search_warp(const SearchGeom& g, const Me
             }
         }
         if (kind < 0) break;
+        if (g.lane < n) ws.dist[g.lane] = 0;  // eval_round adds each lane's block into its candidate's slot
         __syncwarp();
 
         // ---------- price the round ----------
