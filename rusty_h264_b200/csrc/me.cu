@@ -4,7 +4,9 @@
 // One warp runs one search.  Each lane owns one 4x4 sub-block of the
 // partition (its source rows stay in registers for the whole search), so a
 // pass over 32 lanes prices 32/nb candidates at once (nb = sub-blocks per
-// partition).  Control flow is warp-uniform and replays the reference exactly:
+// partition); a candidate's distortion is the sum of its lanes' blocks, added
+// with shared-memory atomics.  Control flow is warp-uniform and replays the
+// reference exactly:
 //  * fixed-centre diamond passes and batched rings price their 4/8 candidates
 //    together, then take the first strict-minimum like the reference's argmin;
 //  * cascading rings (the centre moves mid-ring) are priced speculatively
@@ -1103,10 +1105,12 @@ __device__ __forceinline__ int2 predict_mv_ref0(bool aa, int2 a, bool ba, int2 b
 // wavefront order (frames interleaved), waits (bounded, status 1) until the
 // MB's left and top-right neighbours are published, derives the median
 // predictor from their picks, stages the reference window around it in
-// shared memory (bulk copies; status 3 if they do not land), runs best_part
+// shared memory (one TMA tensor copy, or bulk copies row by row when the
+// planes have no tensor map; status 3 if they do not land), runs best_part
 // for 16x16 and, when its J exceeds the gate, for the four 16x8/8x16
-// partitions (mb16.rs:8869-8913), and publishes the pick.
-// Dynamic shared memory: ME_WARPS windows of WIN_BYTES.
+// partitions (mb16.rs:8869-8913), and publishes the pick (then, for
+// h264a_me_tq_frames, the MB's MC + T/Q).  BAL: the Balanced preset's knobs
+// as constants.  Dynamic shared memory: ME_WARPS windows of WIN_BYTES.
 template <bool BAL>
 __global__ void __launch_bounds__(32 * ME_WARPS, ME_MIN_BLOCKS) me_frames_kernel(const __grid_constant__ FrameBatch batch,
                                                                     long long total,
