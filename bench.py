@@ -63,9 +63,11 @@ def dist_init():
     if ws > 1:
         import datetime
 
+        import torch
         import torch.distributed as dist
 
-        backend = "nccl"
+        # NCCL for the GPU ranks; the reference arm's ranks need no GPU (gloo)
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
         dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
     return ws, rank, local
 

@@ -148,9 +148,11 @@ __global__ void __launch_bounds__(32 * DB_WARPS) deblock_frames_kernel(const __g
         if (lane == 0) t = atomicAdd(counter, 1);
         t = __shfl_sync(0xffffffffu, t, 0);
         if (t >= total) return;
-        int j = 0;
-        while (j + 1 < batch.n && batch.seg_start[j + 1] <= t) j++;
-        const long long u = t - batch.seg_start[j];
+        // segments are dealt from s = 0 (every frame, j = n - 1) on
+        int s = 0;
+        while (s + 1 < batch.n && batch.seg_start[s + 1] <= t) s++;
+        const int j = batch.n - 1 - s;
+        const long long u = t - batch.seg_start[s];
         const int nxt = j + 1 < batch.n ? batch.f[j + 1].mb_w * batch.f[j + 1].mb_h : 0;
         const DbFrameDesc& fd = batch.f[int(u % (j + 1))];
         const int k = nxt + int(u / (j + 1));
@@ -324,8 +326,9 @@ extern "C" int h264a_deblock_frames(h264a_ctx* ctx, const h264a_deblock_frame* h
             total += (long long)d.mb_w * d.mb_h;
         }
         long long acc = 0;
-        for (int jj = 0; jj < gn; jj++) {
-            b.seg_start[jj] = acc;
+        for (int s = 0; s < gn; s++) {
+            const int jj = gn - 1 - s;
+            b.seg_start[s] = acc;
             const long long nj = (long long)b.f[jj].mb_w * b.f[jj].mb_h;
             const long long nn = jj + 1 < gn ? (long long)b.f[jj + 1].mb_w * b.f[jj + 1].mb_h : 0;
             acc += (nj - nn) * (jj + 1);

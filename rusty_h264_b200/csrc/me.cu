@@ -1025,7 +1025,9 @@ struct FrameDesc {
 // One launch's frames, passed by value.  Frames are sorted by MB count
 // (descending) and the work queue deals the k-th MB of every frame that has
 // one before the (k+1)-th of any frame: segment j covers positions
-// [nmb[j+1], nmb[j]) of frames 0..j, so its tickets are (nmb[j]-nmb[j+1])*(j+1).
+// [nmb[j+1], nmb[j]) of frames 0..j, so its tickets are (nmb[j]-nmb[j+1])*(j+1),
+// and segments are dealt from j = n-1 (every frame) down to j = 0 (the
+// largest frame's tail): seg_start[s] is the first ticket of j = n-1-s.
 // Within a frame the k-th MB is taken in wavefront order (anti-diagonals
 // t = x + 2y, then y): every MB's neighbours (left, top, top-left, top-right)
 // lie on earlier diagonals, so a window of resident warps always holds MBs
@@ -1136,9 +1138,11 @@ __global__ void __launch_bounds__(32 * ME_WARPS, ME_MIN_BLOCKS) me_frames_kernel
         if (lane == 0) t = atomicAdd(counter, 1);
         t = __shfl_sync(0xffffffffu, t, 0);
         if (t >= total) return;
-        int j = 0;
-        while (j + 1 < batch.n && batch.seg_start[j + 1] <= t) j++;
-        const long long u = t - batch.seg_start[j];
+        // segments are dealt from s = 0 (every frame, j = n - 1) on
+        int s = 0;
+        while (s + 1 < batch.n && batch.seg_start[s + 1] <= t) s++;
+        const int j = batch.n - 1 - s;
+        const long long u = t - batch.seg_start[s];
         const int nxt = j + 1 < batch.n ? batch.f[j + 1].mb_w * batch.f[j + 1].mb_h : 0;
         const FrameDesc& fd = batch.f[int(u % (j + 1))];
         const int k = nxt + int(u / (j + 1));  // position in the frame's wavefront order
@@ -1340,6 +1344,22 @@ static bool balanced_preset(const MeParamsDev& p) {
            p.me_subpel_iter == 1 && p.sp_maxit == 0 && p.sp_fc == 0;
 }
 
+// Fills seg_start of a batch whose fb.n frames are sorted by MB count,
+// descending, in dealing order (segment j = n-1-s at index s); returns the
+// ticket count, which equals the batch's MB count.
+static long long fill_segments(FrameBatch& fb) {
+    long long acc = 0;
+    for (int s = 0; s < fb.n; s++) {
+        const int j = fb.n - 1 - s;
+        fb.seg_start[s] = acc;
+        const long long nj = (long long)fb.f[j].mb_w * fb.f[j].mb_h;
+        const long long nn = j + 1 < fb.n ? (long long)fb.f[j + 1].mb_w * fb.f[j + 1].mb_h : 0;
+        acc += (nj - nn) * (j + 1);
+    }
+    fb.seg_start[fb.n] = acc;
+    return acc;
+}
+
 static void launch_me_frames(const MeParamsDev& prm, unsigned blocks, cudaStream_t st, const FrameBatch& fb,
                              long long total, int* counter, int* flags, int epoch, int* status) {
     if (balanced_preset(prm))
@@ -1430,15 +1450,7 @@ int h264a::me_frames_run(h264a_ctx* ctx, const h264a_me_frame* h_frames, int nfr
             }
             total += (long long)d.mb_w * d.mb_h;
         }
-        long long acc = 0;
-        for (int j = 0; j < gn; j++) {
-            fb.seg_start[j] = acc;
-            const long long nj = (long long)fb.f[j].mb_w * fb.f[j].mb_h;
-            const long long nn = j + 1 < gn ? (long long)fb.f[j + 1].mb_w * fb.f[j + 1].mb_h : 0;
-            acc += (nj - nn) * (j + 1);
-        }
-        fb.seg_start[gn] = acc;
-        if (acc != total) return fail(H264A_E_ARG, "me_frames: internal queue layout error");
+        if (fill_segments(fb) != total) return fail(H264A_E_ARG, "me_frames: internal queue layout error");
         int rc = ensure_me_scratch(ctx, size_t(total));
         if (rc) return rc;
         H264A_CUDA(cudaMemsetAsync(ctx->q[Q_MAIN].d_counter, 0, sizeof(int32_t), st));
@@ -1567,7 +1579,6 @@ extern "C" int h264a_me_frames_noalloc(const h264a_me_frame* h_frames, int nfram
     FrameBatch fb;
     memset(&fb, 0, sizeof fb);
     fb.n = nframes;
-    long long acc = 0;
     total = 0;
     for (int k = 0; k < nframes; k++) {
         const h264a_me_frame& f = h_frames[order[k]];
@@ -1583,13 +1594,7 @@ extern "C" int h264a_me_frames_noalloc(const h264a_me_frame* h_frames, int nfram
         d.flag_base = int(total);
         total += (long long)d.mb_w * d.mb_h;
     }
-    for (int j = 0; j < nframes; j++) {
-        fb.seg_start[j] = acc;
-        const long long nj = (long long)fb.f[j].mb_w * fb.f[j].mb_h;
-        const long long nn = j + 1 < nframes ? (long long)fb.f[j + 1].mb_w * fb.f[j + 1].mb_h : 0;
-        acc += (nj - nn) * (j + 1);
-    }
-    fb.seg_start[nframes] = acc;
+    fill_segments(fb);
     // the counter and the caller's status word must start at zero; the flags
     // need no clearing because every launch waits for its own epoch value
     H264A_CUDA(cudaMemsetAsync(scratch, 0, sizeof(int), st));

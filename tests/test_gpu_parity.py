@@ -299,6 +299,25 @@ def test_me_frames_single_mb_and_flat(acc):
         assert np.array_equal(picks[:, :5], wp[:, :5]) and np.array_equal(costs, wc)
 
 
+def test_me_frames_2160p_720p_cif_in_one_launch(acc):
+    """The resolutions of the multi-stream workload (CIF, 720p, 2160p) in one
+    wavefront launch, frames of different sizes interleaving in the queue,
+    bit-exact with the oracle (the 2160p pair alone is 32,400 MBs)."""
+    params = A.default_me_params()
+    lam = float(np.sqrt(A.frame_lambda(27)) * 1.25)
+    gate = A.split_gate_for_qp(27)
+    pairs = []
+    for seed, (w, h) in ((1, (3840, 2160)), (2, (1280, 720)), (3, (352, 288))):
+        y, _, _ = synth.cif_clip(2, seed, w, h)
+        f = synth.coded_luma(y)
+        pairs.append((f[1], f[0]))
+    got = run_me_frames(acc, pairs, params, lam, gate)
+    op = O.balanced_params()
+    for (src, ref), (picks, costs) in zip(pairs, got):
+        wp, wc = O.me_frame(src, ref, O.build_planes4(ref, 32), op, lam, gate)
+        assert np.array_equal(picks[:, :5], wp[:, :5]) and np.array_equal(costs, wc), src.shape
+
+
 @pytest.mark.parametrize("pad", [32, 35, 16])
 def test_me_frames_window_edges(acc, cif, pad):
     """The per-MB shared-memory window and the plane path it falls back to:
@@ -631,6 +650,39 @@ def test_deblock_frames_1080p_wavefront(acc):
     for k, (dy, du, dv, rec, ru, rv, picks, coeffs) in enumerate(cases):
         wy, wu, wv = O.deblock_frame(rec, ru, rv, picks, coeffs, qp)
         assert (wy != rec).sum() > 1000
+        assert np.array_equal(dy.cpu().numpy(), wy), k
+        assert np.array_equal(du.cpu().numpy(), wu) and np.array_equal(dv.cpu().numpy(), wv), k
+
+
+def test_deblock_frames_mixed_sizes_wavefront(acc):
+    """A 1920x1088 picture, a CIF one and a 160x96 one in one wavefront
+    launch: the 1080p picture alone has more MBs (8,160) than the kernel keeps
+    resident, so its tail tickets must be dealt after the segments that hold
+    every picture's first MBs. Bit-exact with the oracle."""
+    qp = 31
+    rng = np.random.default_rng(5)
+    frames, keep, cases = [], [], []
+    for seed, (w, h) in ((4, (160, 96)), (5, (1920, 1088)), (6, (352, 288))):
+        y, _, _ = synth.cif_clip(2, seed, w, h)
+        luma = synth.coded_luma(y)
+        half = np.stack([O.downsample2x(a) for a in luma])
+        nmb = (w // 16) * (h // 16)
+        picks = np.zeros((nmb, 6), np.int32)
+        picks[:, 0] = rng.integers(0, 3, nmb)
+        picks[:, 1:3] = rng.integers(-9, 10, (nmb, 2))
+        picks[:, 3:5] = np.where(picks[:, :1] == 0, picks[:, 1:3], picks[:, 1:3] + rng.integers(-4, 5, (nmb, 2)))
+        coeffs, rec = O.mc_tq_rec_frame(luma[1], luma[0], picks, qp, 6)
+        _, ru, rv = O.mc_tq_chroma_frame(half[1], 255 - half[1], half[0], 255 - half[0], picks, qp)
+        dy, du, dv, dp, dc = (dev(acc, a) for a in (rec, ru, rv, picks, coeffs))
+        keep += [dy, du, dv, dp, dc]
+        cases.append((dy, du, dv, rec, ru, rv, picks, coeffs))
+        frames.append(A.DeblockFrame(dy.data_ptr(), du.data_ptr(), dv.data_ptr(), w, h, dp.data_ptr(), dc.data_ptr(),
+                                     qp, 0, 0, 0))
+    acc.deblock_frames(frames)
+    acc.sync()
+    for k, (dy, du, dv, rec, ru, rv, picks, coeffs) in enumerate(cases):
+        wy, wu, wv = O.deblock_frame(rec, ru, rv, picks, coeffs, qp)
+        assert (wy != rec).sum() > 0
         assert np.array_equal(dy.cpu().numpy(), wy), k
         assert np.array_equal(du.cpu().numpy(), wu) and np.array_equal(dv.cpu().numpy(), wv), k
 
