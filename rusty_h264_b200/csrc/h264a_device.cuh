@@ -6,6 +6,7 @@
 #pragma once
 
 #include <cstdint>
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "h264accel_internal.h"
@@ -399,6 +400,52 @@ __device__ __forceinline__ int warp_seg_sum(int v, int seg) {
     // sum over aligned groups of `seg` lanes (seg a power of two <= 32)
     for (int o = seg >> 1; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
+}
+
+// ---------------------------------------------------------------------------
+// Bulk copies into shared memory (ME reference windows, lookahead windows)
+// ---------------------------------------------------------------------------
+
+// mbarrier and bulk-copy primitives (shared addresses are 32-bit).
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+
+// One tiled TMA copy of the box at (x, y, z) of `map` into shared memory,
+// completing on `bar` (no multicast).  x * 1 byte must be a multiple of 16.
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map, int x, int y, int z, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(
+            dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(bar)
+        : "memory");
+}
+
+// Waits (bounded) for the phase `parity` of the warp's window barrier; on
+// timeout records `code` in status and keeps waiting (again bounded) so that
+// no copy is left in flight into the window.
+__device__ __forceinline__ void wait_window(uint32_t bar, uint32_t parity, int* status, int code, int limit) {
+    for (int it = 0; !mbar_try_wait(bar, parity); it++) {
+        if (it == limit) atomicCAS(status, 0, code);
+        if (it >= 2 * limit) break;
+    }
 }
 
 }  // namespace h264a

@@ -2,6 +2,7 @@
 // libh264accel_cuda.so (context, error reporting, launch helpers).
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -77,6 +78,10 @@ struct MeTqOut {
 // plain-ME of frames, with the fused T/Q when tq is given (one entry per frame)
 int me_frames_run(h264a_ctx *ctx, const h264a_me_frame *h_frames, int nframes, const h264a_me_params *params,
                   const MeTqOut *tq, void *stream);
+// A tiled TMA map of a dense 3D u8 tensor (w x h x d, rows of w bytes, planes
+// of w*h), box bw x bh x bd, no multicast; 0 when the driver entry point is
+// missing or the layout breaks the TMA rules (the caller then copies without).
+int encode_u8_map_3d(CUtensorMap* map, const uint8_t* base, int w, int h, int d, int bw, int bh, int bd);
 // the flag value of the next persistent launch on `st`
 int next_epoch(h264a_ctx *ctx, cudaStream_t st, int queue = Q_MAIN);
 

@@ -14,6 +14,12 @@
 //    points of the cascading diamond together and takes the first improvement,
 //    re-pricing the rest of the ring around the moved centre (the reference's
 //    evaluation order).
+//    In HalfRes mode (the default) each chain reads its block's candidates
+//    from a shared-memory window (the block +-16 rows, 48 columns), copied by
+//    TMA one block ahead; candidates outside it, or outside the picture, read
+//    the clamped picture.  The kernel is instantiated per mode.
+#include <cstring>
+
 #include "h264a_device.cuh"
 
 namespace h264a {
@@ -86,6 +92,24 @@ __global__ void la_intra_kernel(const uint8_t* __restrict__ pics, size_t fstride
 // searches, lane group g = lane / 16 (slots 16g.. of the candidate and
 // distortion arrays), each walking its own row chain; a group prices
 // 16 / (bs/4)^2 candidates per pass (four 8x8 or one 16x16).
+// HalfRes reference windows: per chain two buffers of LA_WIN_H rows of
+// LA_WIN_W bytes (the block +-16 rows, and 48 columns from the 16-byte boundary
+// at or left of the block's x - 16), filled by a TMA copy one block ahead.
+constexpr int LA_WIN_W = 48, LA_WIN_H = 40, LA_WIN_BYTES = LA_WIN_W * LA_WIN_H;
+constexpr int LA_WIN_BUF = 2048;  // buffer stride: 128-byte aligned, with room for a row read's second word
+extern __shared__ __align__(128) uint8_t la_win[];
+
+// The four rows of a 4x4 block at window column cx, row cy of the buffer at
+// byte offset `off` of la_win (two aligned words and a funnel shift per row).
+__device__ __forceinline__ void la_win_rows(int off, int cx, int cy, uint32_t p[4]) {
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+        const int a = off + (cy + r) * LA_WIN_W + cx;
+        const uint32_t* wp = reinterpret_cast<const uint32_t*>(la_win + (a & ~3));
+        p[r] = __funnelshift_r(wp[0], wp[1], uint32_t(a & 3) * 8u);
+    }
+}
+
 struct LaSearch {
     const uint8_t* cur;
     const uint8_t* ref;
@@ -93,10 +117,26 @@ struct LaSearch {
     uint32_t srow[4];
     int2* cand;
     int* dist;
+    // the block's window (wbuf < 0: none): buffer offset, the lane's 4x4 block
+    // at MV (0,0) in window coordinates, and the window columns/rows a 4x4
+    // read may start at (inside the window and the picture) as bytes
+    // xlo | xhi << 8 | ylo << 16 | yhi << 24
+    int wbuf, wox, woy;
+    uint32_t wlim;
+
+    __device__ void set_window(int buf, int wx0, int wy0) {
+        wbuf = buf;
+        wox = x0 + bxo - wx0;
+        woy = y0 + byo - wy0;
+        const int xlo = max(0, -wx0), xhi = min(LA_WIN_W, w - wx0) - 4;
+        const int ylo = max(0, -wy0), yhi = min(LA_WIN_H, h - wy0) - 4;
+        wlim = uint32_t(xlo) | uint32_t(xhi) << 8 | uint32_t(ylo) << 16 | uint32_t(yhi) << 24;
+    }
 
     __device__ void init(const uint8_t* c, const uint8_t* r, int pw, int ph, int b, int bx0, int by0, int2* cs,
                          int* ds) {
         cur = c; ref = r; w = pw; h = ph; bs = b; x0 = bx0; y0 = by0; cand = cs; dist = ds;
+        wbuf = -1;
         const int lane = threadIdx.x & 31;
         gl = lane & 15;
         gb = lane & 16;
@@ -112,6 +152,7 @@ struct LaSearch {
     // SATD of each group's cand[gb..gb+n) (full-pel MVs, quarter-pel units)
     // added into dist (zeroed by the caller) by shared-memory atomics of the
     // lanes' 4x4 blocks; passes run to the larger group's need.
+    template <bool FULLPEL>  // FULLPEL: every candidate is a full-pel MV (HalfRes, FullRes)
     __device__ void eval(int n) {
         const int cps = 4 - lg_nb;  // log2 candidates per pass of a group
         const int npass = __reduce_max_sync(0xffffffffu, (n + (1 << cps) - 1) >> cps);
@@ -121,9 +162,14 @@ struct LaSearch {
             if (c < n) {
                 const int2 mv = cand[gb + c];
                 uint32_t p[4];
-                if (((mv.x | mv.y) & 3) == 0)
-                    fullpel_rows_clamped(ref, w, h, x0 + bxo + (mv.x >> 2), y0 + byo + (mv.y >> 2), p);
-                else  // a sub-pel seed (Hybrid mode halves a full-res MV): mc_luma on the plain picture
+                if (FULLPEL || ((mv.x | mv.y) & 3) == 0) {
+                    const int cx = wox + (mv.x >> 2), cy = woy + (mv.y >> 2);
+                    if (wbuf >= 0 && cx >= int(wlim & 255u) && cx <= int((wlim >> 8) & 255u) &&
+                        cy >= int((wlim >> 16) & 255u) && cy <= int(wlim >> 24))
+                        la_win_rows(wbuf, cx, cy, p);
+                    else
+                        fullpel_rows_clamped(ref, w, h, x0 + bxo + (mv.x >> 2), y0 + byo + (mv.y >> 2), p);
+                } else  // a sub-pel seed (Hybrid mode halves a full-res MV): mc_luma on the plain picture
                     subpel_rows_clamped(ref, w, h, x0 + bxo + (mv.x >> 2), y0 + byo + (mv.y >> 2), mv.x & 3, mv.y & 3, p);
                 d = satd4x4_rows(srow, p);
             }
@@ -143,6 +189,7 @@ __device__ __forceinline__ int la_ring_dy(int k) { return k == 2 ? 1 : (k == 3 ?
 // (first improvement moves the centre, the rest of the ring is priced around
 // it; a ring that moved is walked again at the same step), stopping at once
 // when (0,0) costs nothing.  `active` false: the group takes no part.
+template <bool FULLPEL>
 __device__ void la_inter_cost(LaSearch& s, bool active, int seedx, int seedy, int max_step, int& cost, int& mvx,
                               int& mvy) {
     const int gl = s.gl, gb = s.gb;
@@ -167,7 +214,7 @@ __device__ void la_inter_cost(LaSearch& s, bool active, int seedx, int seedy, in
         if (__all_sync(0xffffffffu, phase == 2)) break;
         if (gl < n) s.dist[gb + gl] = 0;  // eval adds each lane's block into its candidate's slot
         __syncwarp();
-        s.eval(n);
+        s.eval<FULLPEL>(n);
         const int d = gl < n ? s.dist[gb + gl] : 0;
         const unsigned hit = (__ballot_sync(0xffffffffu, gl < n && (long long)d < best) >> gb) & 0xffffu;
         const int j = hit ? __ffs(hit) - 1 : 0;
@@ -217,6 +264,8 @@ __device__ void la_inter_cost(LaSearch& s, bool active, int seedx, int seedy, in
 }
 
 struct LaBufs {
+    CUtensorMap hmap;     // the half-res frames as (cw/2, ch/2, n), box LA_WIN_W x LA_WIN_H x 1
+    int hmap_ok;          // HalfRes mode with a valid map: searches read windows
     const uint8_t* full;  // n frames cw x ch
     const uint8_t* half;  // n frames cw/2 x ch/2 (modes 1, 2)
     int cw, ch, mb_w, mb_h, n, mode;
@@ -225,32 +274,39 @@ struct LaBufs {
     int32_t* mvs;
 };
 
+// Window origin of half-res block column mbx: 16 columns left of the block,
+// rounded down to a 16-byte boundary (the TMA x alignment).
+__device__ __forceinline__ int la_win_x0(int mbx) { return (mbx * 8 - 16) & ~15; }
+
 // frame_costs for MB (mbx, mby) of frame f >= 1 given the full-res seed.
+template <int MODE>
 __device__ void la_mb(const LaBufs& b, bool active, int f, int mbx, int mby, int sfx, int sfy, int2* cs, int* ds,
-                      int& outx, int& outy) {
+                      int wbuf, int& outx, int& outy) {
     const long long nmb = (long long)b.mb_w * b.mb_h;
     const long long gm = nmb * f + (long long)mby * b.mb_w + mbx;
     const int cwh = b.cw / 2, chh = b.ch / 2;
     const size_t fs = (size_t)b.cw * b.ch, hs = (size_t)cwh * chh;
     LaSearch s;
     int cost, mx, my;
-    if (b.mode == 0) {  // FullRes
+    // an input (la_intra_kernel's output): read before the search, used after it
+    const int ic = active && (threadIdx.x & 15) == 0 ? __ldg(b.intra + gm) : 0;
+    if (MODE == 0) {  // FullRes
         s.init(b.full + fs * f, b.full + fs * (f - 1), b.cw, b.ch, 16, mbx * 16, mby * 16, cs, ds);
-        la_inter_cost(s, active, sfx, sfy, 8, cost, mx, my);
+        la_inter_cost<true>(s, active, sfx, sfy, 8, cost, mx, my);
     } else {
         s.init(b.half + hs * f, b.half + hs * (f - 1), cwh, chh, 8, mbx * 8, mby * 8, cs, ds);
+        if (wbuf >= 0) s.set_window(wbuf, la_win_x0(mbx), mby * 8 - 16);
         int hx, hy;
-        la_inter_cost(s, active, sfx / 2, sfy / 2, 8, cost, hx, hy);
-        if (b.mode == 2) {  // HalfRes
+        la_inter_cost<MODE == 2>(s, active, sfx / 2, sfy / 2, 8, cost, hx, hy);
+        if (MODE == 2) {  // HalfRes
             mx = hx * 2;
             my = hy * 2;
         } else {  // Hybrid: refine at full-res from the coarse MV
             s.init(b.full + fs * f, b.full + fs * (f - 1), b.cw, b.ch, 16, mbx * 16, mby * 16, cs, ds);
-            la_inter_cost(s, active, hx * 2, hy * 2, 2, cost, mx, my);
+            la_inter_cost<true>(s, active, hx * 2, hy * 2, 2, cost, mx, my);
         }
     }
     if (active && s.gl == 0) {
-        const int ic = b.intra[gm];
         b.inter[gm] = cost < ic ? cost : ic;
         b.mvs[2 * gm] = mx;
         b.mvs[2 * gm + 1] = my;
@@ -266,18 +322,46 @@ constexpr int LA_WARPS = 4;
 // walk column 0 of frames 1+2t+g and publish flag (f-1)*mb_h + y after MB
 // (0, y); later tickets take rows 2p and 2p+1 of the row order (rows in
 // order, frames interleaved), each group waiting for its own column-0 flag
-// and walking columns 1.. seeded by the left neighbour.
-__global__ void __launch_bounds__(32 * LA_WARPS, 4) la_chains_kernel(LaBufs b, int* __restrict__ counter,
-                                                                 int* __restrict__ flags, int epoch,
-                                                                 int* __restrict__ status, int spin_limit) {
+// and walking columns 1.. seeded by the left neighbour.  In HalfRes mode each
+// chain's next block window is copied (TMA, lane 0 of the group) while the
+// current block is searched; every copy issued is waited for (bounded,
+// status 3) before the block that reads it.
+template <int MODE>  // b.mode, as a constant
+__global__ void __launch_bounds__(32 * LA_WARPS, 4) la_chains_kernel(const __grid_constant__ LaBufs b,
+                                                                 int* __restrict__ counter, int* __restrict__ flags,
+                                                                 int epoch, int* __restrict__ status, int spin_limit) {
     __shared__ int2 cs[LA_WARPS][32];
     __shared__ int ds[LA_WARPS][32];
+    __shared__ __align__(8) unsigned long long la_bar[LA_WARPS][2][2];
     const int w = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     const int grp = lane >> 4, gl = lane & 15;
     const int nf = b.n - 1;
     const int ncol = (nf + 1) / 2;
     const long long nrows = (long long)nf * b.mb_h;
+    const int buf0 = ((w * 2 + grp) * 2) * LA_WIN_BUF;  // this chain's two buffers in la_win
+    const uint32_t win0 = uint32_t(__cvta_generic_to_shared(la_win)) + uint32_t(buf0);
+    const uint32_t bar0 = uint32_t(__cvta_generic_to_shared(&la_bar[w][grp][0]));
+    if (b.hmap_ok && gl == 0) {
+        mbar_init(bar0, 1);
+        mbar_init(bar0 + 8, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncwarp();
+    uint32_t parity = 0;  // bit k: the phase buffer k completes next
+    // window of block (mbx, mby) of frame f into buffer k (lane 0 of the group);
+    // the group's earlier reads of the buffer are complete (converged warp)
+    auto issue = [&](int k, int f, int mbx, int mby) {
+        if (gl == 0) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            mbar_expect_tx(bar0 + 8 * k, uint32_t(LA_WIN_BYTES));
+            tma_load_3d(win0 + uint32_t(k * LA_WIN_BUF), &b.hmap, la_win_x0(mbx), mby * 8 - 16, f - 1, bar0 + 8 * k);
+        }
+    };
+    auto wait = [&](int k) {
+        wait_window(bar0 + 8 * k, (parity >> k) & 1u, status, 3, spin_limit);
+        parity ^= 1u << k;
+    };
     for (;;) {
         int t = 0;
         if (lane == 0) t = atomicAdd(counter, 1);
@@ -285,10 +369,15 @@ __global__ void __launch_bounds__(32 * LA_WARPS, 4) la_chains_kernel(LaBufs b, i
         if (t < ncol) {
             const int f = 1 + 2 * t + grp;
             const bool active = f <= nf;
+            const bool uw = active && b.hmap_ok;
+            if (uw) issue(0, f, 0, 0);
             int sx = 0, sy = 0;
             for (int mby = 0; mby < b.mb_h; mby++) {
+                const int k = mby & 1;
+                if (uw && mby + 1 < b.mb_h) issue(k ^ 1, f, 0, mby + 1);
+                if (uw) wait(k);
                 int mx, my;
-                la_mb(b, active, active ? f : 1, 0, mby, sx, sy, cs[w], ds[w], mx, my);
+                la_mb<MODE>(b, active, active ? f : 1, 0, mby, sx, sy, cs[w], ds[w], uw ? buf0 + k * LA_WIN_BUF : -1, mx, my);
                 sx = mx;
                 sy = my;
                 if (active && gl == 0) st_release(flags + (f - 1) * b.mb_h + mby, epoch);  // after the lane's MV store
@@ -299,16 +388,22 @@ __global__ void __launch_bounds__(32 * LA_WARPS, 4) la_chains_kernel(LaBufs b, i
         const long long r = 2 * ((long long)t - ncol) + grp;
         if (2 * ((long long)t - ncol) >= nrows) return;
         const bool active = r < nrows;
+        const bool uw = active && b.hmap_ok && b.mb_w > 1;
         const int mby = active ? int(r / nf) : 0, f = active ? 1 + int(r % nf) : 1;
+        if (uw) issue(0, f, 1, mby);  // the window is an input: no need to wait for column 0
         if (active && gl == 0) wait_flag(flags + (f - 1) * b.mb_h + mby, epoch, status, 1, spin_limit);
         __syncwarp();
         const long long gm0 = (long long)b.mb_w * b.mb_h * f + (long long)mby * b.mb_w;
         int sx = active ? __ldcg(b.mvs + 2 * gm0) : 0, sy = active ? __ldcg(b.mvs + 2 * gm0 + 1) : 0;
         for (int mbx = 1; mbx < b.mb_w; mbx++) {
+            const int k = (mbx - 1) & 1;
+            if (uw && mbx + 1 < b.mb_w) issue(k ^ 1, f, mbx + 1, mby);
+            if (uw) wait(k);
             int mx, my;
-            la_mb(b, active, f, mbx, mby, sx, sy, cs[w], ds[w], mx, my);
+            la_mb<MODE>(b, active, f, mbx, mby, sx, sy, cs[w], ds[w], uw ? buf0 + k * LA_WIN_BUF : -1, mx, my);
             sx = mx;
             sy = my;
+            __syncwarp();
         }
     }
 }
@@ -338,7 +433,11 @@ extern "C" int h264a_lookahead_costs(h264a_ctx* ctx, const uint8_t* d_full, cons
     if (mode != 0 && !d_half) return fail(H264A_E_ARG, "lookahead_costs: modes 1 and 2 need the half-res frames");
     if (cw < 16 || ch < 16 || cw % 16 || ch % 16 || n < 1) return fail(H264A_E_ARG, "lookahead_costs: bad geometry");
     cudaStream_t st = pick_stream(ctx, stream);
-    LaBufs b{d_full, d_half, cw, ch, cw / 16, ch / 16, n, mode, d_intra, d_inter, d_mvs};
+    LaBufs b;
+    memset(&b, 0, sizeof b);
+    b.full = d_full; b.half = d_half; b.cw = cw; b.ch = ch; b.mb_w = cw / 16; b.mb_h = ch / 16; b.n = n; b.mode = mode;
+    b.intra = d_intra; b.inter = d_inter; b.mvs = d_mvs;
+    b.hmap_ok = mode == 2 ? encode_u8_map_3d(&b.hmap, d_half, cw / 2, ch / 2, n, LA_WIN_W, LA_WIN_H, 1) : 0;
     const LaGeom g = mode == 2 ? LaGeom{8, cw / 2, ch / 2} : LaGeom{16, cw, ch};
     const size_t fstride = mode == 2 ? (size_t)(cw / 2) * (ch / 2) : (size_t)cw * ch;
     const long long nmb = (long long)(cw / 16) * (ch / 16);
@@ -354,12 +453,14 @@ extern "C" int h264a_lookahead_costs(h264a_ctx* ctx, const uint8_t* d_full, cons
     H264A_CUDA(cudaMemsetAsync(ctx->q[Q_LOOKAHEAD].d_counter, 0, sizeof(int32_t), st));
     const int epoch = next_epoch(ctx, st, Q_LOOKAHEAD);
     if (epoch < 0) return H264A_E_CUDA;
+    const int smem = LA_WARPS * 2 * 2 * LA_WIN_BUF;  // two window buffers per chain
+    auto kern = mode == 0 ? la_chains_kernel<0> : (mode == 1 ? la_chains_kernel<1> : la_chains_kernel<2>);
     int per_sm = 0;
-    H264A_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, la_chains_kernel, 32 * LA_WARPS, 0));
+    H264A_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * LA_WARPS, smem));
     long long blocks = (long long)ctx->num_sms * (per_sm > 0 ? per_sm : 1);
     const long long need = (chains + LA_WARPS - 1) / LA_WARPS;
     if (blocks > need) blocks = need;
-    la_chains_kernel<<<unsigned(blocks), 32 * LA_WARPS, 0, st>>>(b, ctx->q[Q_LOOKAHEAD].d_counter, ctx->q[Q_LOOKAHEAD].d_flags, epoch, ctx->d_status,
-                                                                SPIN_LIMIT);
+    kern<<<unsigned(blocks), 32 * LA_WARPS, smem, st>>>(b, ctx->q[Q_LOOKAHEAD].d_counter, ctx->q[Q_LOOKAHEAD].d_flags,
+                                                        epoch, ctx->d_status, SPIN_LIMIT);
     return check_launch("la_chains_kernel");
 }

@@ -1040,48 +1040,6 @@ struct FrameBatch {
 };
 static_assert(sizeof(FrameBatch) + 512 <= 32764, "me_frames_kernel's parameters must fit the 32 KB parameter space");
 
-// mbarrier and bulk-copy primitives (shared addresses are 32-bit).
-__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
-        : "=r"(ok)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
-                 "l"(src), "r"(bytes), "r"(bar)
-                 : "memory");
-}
-
-// One tiled TMA copy of the box at (x, y, 0) of `map` into shared memory,
-// completing on `bar` (no multicast).
-__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar) {
-    asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(
-            dst),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(0), "r"(bar)
-        : "memory");
-}
-
-// Waits (bounded) for the phase `parity` of the warp's window barrier; on
-// timeout records `code` in status and keeps waiting (again bounded) so that
-// no copy is left in flight into the window.
-__device__ __forceinline__ void wait_window(uint32_t bar, uint32_t parity, int* status, int code, int limit) {
-    for (int it = 0; !mbar_try_wait(bar, parity); it++) {
-        if (it == limit) atomicCAS(status, 0, code);
-        if (it >= 2 * limit) break;
-    }
-}
-
 // The MV of neighbour MB `m`'s 4x4 block at (bx4, by4) under its pick.
 __device__ __forceinline__ int2 pick_mv_at(const int32_t* picks, int m, int bx4, int by4) {
     const int32_t* p = picks + 6 * m;
@@ -1190,7 +1148,7 @@ __global__ void __launch_bounds__(32 * ME_WARPS, ME_MIN_BLOCKS) me_frames_kernel
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 if (fd.tmap_ok) {  // the whole window in one tensor copy
                     mbar_expect_tx(bar, uint32_t(WIN_BYTES));
-                    tma_load_3d(win, &fd.tmap, wx0, wy0, bar);
+                    tma_load_3d(win, &fd.tmap, wx0, wy0, 0, bar);
                 } else {
                     mbar_expect_tx(bar, uint32_t(4 * WIN_H * WIN_W));
                 }
@@ -1295,11 +1253,8 @@ __global__ void bounded_wait_selftest_kernel(const int* flag, int* status, int l
 
 using namespace h264a;
 
-// The F|H|V|C planes of a reference picture as a 3D u8 tensor (pw, ph, 4)
-// whose 80 x 42 x 4 box is an MB's window in the WIN_STRIDE / WIN_PLANE
-// layout.  Returns 0 when the planes cannot be described (alignment, or no
-// driver entry point), and the kernel then stages the window row by row.
-static int encode_window_map(CUtensorMap* map, const uint8_t* planes, int pw, int ph) {
+namespace h264a {
+int encode_u8_map_3d(CUtensorMap* map, const uint8_t* base, int w, int h, int d, int bw, int bh, int bd) {
     static const PFN_cuTensorMapEncodeTiled_v12000 encode = [] {  // looked up once, thread-safely
         void* fn = nullptr;
         cudaDriverEntryPointQueryResult q;
@@ -1309,19 +1264,29 @@ static int encode_window_map(CUtensorMap* map, const uint8_t* planes, int pw, in
         cudaGetLastError();
         return PFN_cuTensorMapEncodeTiled_v12000(nullptr);
     }();
-    if (!encode || (reinterpret_cast<uintptr_t>(planes) & 15) != 0 || pw % 16 != 0 || pw < WIN_W || ph < WIN_H)
+    if (!encode || (reinterpret_cast<uintptr_t>(base) & 15) != 0 || w % 16 != 0 || bw % 16 != 0 || w < bw || h < bh ||
+        d < bd || bw > 256 || bh > 256 || bd > 256 || bd < 1)
         return 0;
-    static_assert(WIN_STRIDE % 16 == 0 && WIN_PLANE == WIN_H * WIN_STRIDE && WIN_BYTES == 4 * WIN_PLANE,
-                  "the window is one dense 3D box");
-    const cuuint64_t dim[3] = {cuuint64_t(pw), cuuint64_t(ph), 4};
-    const cuuint64_t stride[2] = {cuuint64_t(pw), cuuint64_t(pw) * cuuint64_t(ph)};  // bytes, dims 1 and 2
-    const cuuint32_t box[3] = {WIN_STRIDE, WIN_H, 4};
+    const cuuint64_t dim[3] = {cuuint64_t(w), cuuint64_t(h), cuuint64_t(d)};
+    const cuuint64_t stride[2] = {cuuint64_t(w), cuuint64_t(w) * cuuint64_t(h)};  // bytes, dims 1 and 2
+    const cuuint32_t box[3] = {cuuint32_t(bw), cuuint32_t(bh), cuuint32_t(bd)};
     const cuuint32_t estride[3] = {1, 1, 1};
-    return encode(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<uint8_t*>(planes), dim, stride, box, estride,
+    return encode(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<uint8_t*>(base), dim, stride, box, estride,
                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS
                ? 1
                : 0;
+}
+}  // namespace h264a
+
+// The F|H|V|C planes of a reference picture as a 3D u8 tensor (pw, ph, 4)
+// whose 80 x 42 x 4 box is an MB's window in the WIN_STRIDE / WIN_PLANE
+// layout.  Returns 0 when the planes cannot be described (alignment, or no
+// driver entry point), and the kernel then stages the window row by row.
+static int encode_window_map(CUtensorMap* map, const uint8_t* planes, int pw, int ph) {
+    static_assert(WIN_STRIDE % 16 == 0 && WIN_PLANE == WIN_H * WIN_STRIDE && WIN_BYTES == 4 * WIN_PLANE,
+                  "the window is one dense 3D box");
+    return encode_u8_map_3d(map, planes, pw, ph, 4, WIN_STRIDE, WIN_H, 4);
 }
 
 // Dynamic shared memory of me_frames_kernel, its opt-in above 48 KB, and the
