@@ -114,7 +114,7 @@ struct LaSearch {
     const uint8_t* cur;
     const uint8_t* ref;
     int w, h, bs, lg_nb, gl, gb, bxo, byo, x0, y0;
-    uint32_t srow[4];
+    uint32_t spa[4], spb[4];  // the source rows split into column pairs (split_pairs)
     int2* cand;
     int* dist;
     // the block's window (wbuf < 0: none): buffer offset, the lane's 4x4 block
@@ -145,8 +145,12 @@ struct LaSearch {
         const int sb = gl & ((1 << lg_nb) - 1);
         bxo = (sb % nbx) * 4;
         byo = (sb / nbx) * 4;
+        {
+            uint32_t srow[4];
 #pragma unroll
-        for (int r = 0; r < 4; r++) srow[r] = ld4u(cur + (long long)(y0 + byo + r) * w + x0 + bxo);
+            for (int r = 0; r < 4; r++) srow[r] = ld4u(cur + (long long)(y0 + byo + r) * w + x0 + bxo);
+            split_pairs(srow, spa, spb);
+        }
     }
 
     // SATD of each group's cand[gb..gb+n) (full-pel MVs, quarter-pel units)
@@ -171,7 +175,7 @@ struct LaSearch {
                         fullpel_rows_clamped(ref, w, h, x0 + bxo + (mv.x >> 2), y0 + byo + (mv.y >> 2), p);
                 } else  // a sub-pel seed (Hybrid mode halves a full-res MV): mc_luma on the plain picture
                     subpel_rows_clamped(ref, w, h, x0 + bxo + (mv.x >> 2), y0 + byo + (mv.y >> 2), mv.x & 3, mv.y & 3, p);
-                d = satd4x4_rows(srow, p);
+                d = satd4x4_packed(spa, spb, p);
             }
             if (c < n) atomicAdd(&dist[gb + c], d);  // the candidate's blocks, summed in shared memory
         }

@@ -705,6 +705,34 @@ def test_lookahead_matches_oracle(acc, cif, mode):
     assert np.array_equal(mvs.cpu().numpy(), wm)
 
 
+@pytest.mark.parametrize("cw,ch,pan", [(352, 288, (44, 26)), (208, 144, (6, -4))])
+def test_lookahead_window_misses_and_no_window(acc, cw, ch, pan):
+    """HalfRes searches on a panning texture: a 44x26-pixel pan per frame
+    walks candidates out of the block's shared-memory window (they read the
+    clamped picture instead), and a 208-pixel clip has 104-byte half-res rows,
+    which no tensor map can describe, so it searches without windows. All
+    three outputs bit-exact with the oracle."""
+    rng = np.random.default_rng(cw)
+    H, W = ch + 4 * abs(pan[1]) + 16, cw + 4 * abs(pan[0]) + 16
+    tex = rng.random((H, W))
+    for _ in range(3):  # smooth it, so that the diamond can follow the pan
+        tex = (tex + np.roll(tex, 1, 0) + np.roll(tex, 1, 1) + np.roll(tex, (1, 1), (0, 1))) / 4
+    tex = (255 * (tex - tex.min()) / (tex.max() - tex.min())).astype(np.uint8)
+    oy, ox = 2 * abs(pan[1]) + 8, 2 * abs(pan[0]) + 8
+    clip = np.stack([tex[oy + k * pan[1]:oy + k * pan[1] + ch, ox + k * pan[0]:ox + k * pan[0] + cw] for k in range(3)])
+    clip = np.ascontiguousarray(clip)
+    full = dev(acc, clip)
+    half = acc.downsample2x(full)
+    intra, inter, mvs = acc.lookahead_costs(full, half, 2)
+    acc.sync()
+    wi, wn, wm = O.lookahead_clip(clip, 2)
+    assert np.array_equal(intra.cpu().numpy(), wi)
+    assert np.array_equal(inter.cpu().numpy(), wn)
+    assert np.array_equal(mvs.cpu().numpy(), wm)
+    if pan[0] > 16:
+        assert (np.abs(wm[1:, :, 0]) >= 32).mean() > 0.25  # the search follows the pan past the window
+
+
 def test_lookahead_flat_and_static(acc):
     flat = np.full((3, 32, 32), 77, np.uint8)
     full = dev(acc, flat)
