@@ -12,7 +12,11 @@ lookahead (downsample + frame costs) of all 60 frames.
   and coefficients (~1 GB) exceed the 126 MB L2, so no flush is needed.
 * e2e: the same work through h264a_pixel_path_host from pinned host memory,
   host->device copy of the frames and device->host copy of every result
-  inside the timed region (the call synchronises; wall-clock timed).
+  inside the timed region, over K steps streamed the way an encoder feeds
+  consecutive batches: each step's upload is queued (h264a_pixel_path_prefetch)
+  before the previous step's call, so it overlaps that call's compute
+  (wall-clock timed from the first upload to the last result).  The line also
+  gives one synchronous call on its own (upload inside the call).
 * roofline: the dominant kernel (the persistent ME kernel) against the INT32
   issue rate measured on this device by h264a_measure_int32_peak; the
   algorithmic work is 112 integer ops per 4x4 Hadamard-SATD evaluation the
@@ -469,25 +473,36 @@ def run_ours(args, ws, rank, local):
                     la_mvs=torch.zeros((n, nmb, 2), dtype=torch.int32).pin_memory())
         outs_np = {k: v.numpy() for k, v in outs.items()}
         fr_np = host_frames.numpy()
-        for _ in range(args.warmup):
-            acc.pixel_path_host(fr_np, params, lam, gate, qp, out=outs_np)
+        def stream(steps):
+            # every step's frames go up inside the loop; step k+1's upload is
+            # queued before step k's call and overlaps its compute
+            acc.pixel_path_prefetch(fr_np)
+            for k in range(steps):
+                if k + 1 < steps:
+                    acc.pixel_path_prefetch(fr_np)
+                acc.pixel_path_host(fr_np, params, lam, gate, qp, out=outs_np)
+
+        stream(args.warmup)
         barrier()
-        ts = []
-        for _ in range(args.steps):
-            s0 = time.perf_counter()
-            acc.pixel_path_host(fr_np, params, lam, gate, qp, out=outs_np)
-            ts.append(time.perf_counter() - s0)
-        e2e_ms = float(np.mean(ts)) * 1e3
+        s0 = time.perf_counter()
+        stream(args.steps)
+        e2e_ms = (time.perf_counter() - s0) * 1e3 / args.steps
+        s0 = time.perf_counter()  # one synchronous call on its own, for comparison
+        acc.pixel_path_host(fr_np, params, lam, gate, qp, out=outs_np)
+        single_ms = (time.perf_counter() - s0) * 1e3
         if ws > 1:
             import torch.distributed as dist
 
-            tt = torch.tensor([e2e_ms], device=dev)
+            tt = torch.tensor([e2e_ms, single_ms], device=dev)
             dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            e2e_ms = float(tt.item())
+            e2e_ms, single_ms = (float(v) for v in tt.tolist())
         d2h = sum(v.numel() * v.element_size() for v in outs.values())
         line["e2e"] = {"value": round(ws * n * W * H / (e2e_ms * 1e-3) / 1e6, 2), "unit": "Mpx/s",
                        "h2d_bytes_per_step": int(f.nbytes), "d2h_bytes_per_step": int(d2h),
-                       "ms_per_step": round(e2e_ms, 3), "timing": "wall clock around the synchronous C-ABI call"}
+                       "ms_per_step": round(e2e_ms, 3),
+                       "timing": "wall clock over the streamed steps (each upload queued before the previous "
+                                 "step's call, h264a_pixel_path_prefetch)",
+                       "single_call_ms": round(single_ms, 3)}
         # the host path and the device-resident path must agree
         for k, t in (("picks", picks), ("coeffs", coeffs), ("la_intra", la_intra), ("la_inter", la_inter),
                      ("la_mvs", la_mvs)):

@@ -315,6 +315,16 @@ H264A_API int h264a_pixel_path_host(h264a_ctx *ctx, const uint8_t *h_frames, int
                           const uint16_t *h_mv_cost_tab, double lambda_me, int64_t split_gate, int qp, int dz_div,
                           int32_t *h_picks, int64_t *h_costs, int16_t *h_coeffs, int32_t *h_la_intra,
                           int32_t *h_la_inter, int32_t *h_la_mvs);
+/* Queues the upload of n frames (cw x ch, contiguous; pinned memory makes it
+ * asynchronous) into one of the context's two input slots, on a stream of its
+ * own, and returns.  The next h264a_pixel_path_host call with the same
+ * h_frames, n, cw and ch takes the frames from that slot instead of uploading
+ * them, so a caller that prefetches batch k+1 before the call for batch k
+ * overlaps each upload with the previous batch's compute.  The caller must not
+ * change the frames until that call.  At most two prefetches may be pending
+ * (H264A_E_ARG otherwise); a call whose frames match no pending prefetch
+ * uploads them itself. */
+H264A_API int h264a_pixel_path_prefetch(h264a_ctx *ctx, const uint8_t *h_frames, int n, int cw, int ch);
 
 /* ---- diagnostics ----------------------------------------------------------- */
 /* Failure-detection self-test: one warp runs the persistent kernel's bounded

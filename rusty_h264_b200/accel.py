@@ -99,6 +99,7 @@ EXPORTS = (
     "h264a_block_metric", "h264a_candidate_dist", "h264a_me_params_default", "h264a_build_mv_cost_table",
     "h264a_me_search", "h264a_me_frames", "h264a_fullpel_grid", "h264a_dct_quant_4x4", "h264a_dct_quant_8x8",
     "h264a_mc_tq_frames", "h264a_downsample2x", "h264a_lookahead_costs", "h264a_pixel_path_host",
+    "h264a_pixel_path_prefetch",
     "h264a_selftest_bounded_wait", "h264a_measure_int32_peak", "h264a_me_frames_noalloc",
     "h264a_mc_tq_rec_frames", "h264a_mc_tq_chroma_frames", "h264a_deblock_frames", "h264a_me_tq_frames",
 )
@@ -139,6 +140,7 @@ def load_library() -> C.CDLL:
     L.h264a_deblock_frames.argtypes = [vp, vp, i32, vp]
     L.h264a_downsample2x.argtypes = [vp, vp, i32, i32, i32, sz, vp, vp]
     L.h264a_lookahead_costs.argtypes = [vp, vp, vp, i32, i32, i32, i32, vp, vp, vp, vp]
+    L.h264a_pixel_path_prefetch.argtypes = [vp, vp, i32, i32, i32]
     L.h264a_pixel_path_host.argtypes = [vp, vp, i32, i32, i32, C.POINTER(MeParams), vp, f64, i64, i32, i32, vp, vp, vp,
                                         vp, vp, vp]
     L.h264a_selftest_bounded_wait.argtypes = [vp, i32, vp]
@@ -195,6 +197,7 @@ class Accel:
             raise RuntimeError("rusty_h264_b200 needs a CUDA device (sm_100a); none is visible")
         self.L = load_library()
         self.device = device
+        self._prefetched = []  # (address, array) of frames whose upload may still be pending
         torch.cuda.set_device(device)
         ctx = C.c_void_p()
         self._check(self.L.h264a_ctx_create(device, C.byref(ctx)))
@@ -377,6 +380,16 @@ class Accel:
         return v.value
 
     # ---- end to end from host memory --------------------------------------------
+    def pixel_path_prefetch(self, frames: np.ndarray):
+        """Queues the upload of frames (n, ch, cw) u8, C-contiguous (pinned for
+        an asynchronous copy), for the next pixel_path_host call on them.  The
+        array is kept alive here until then; do not change it meanwhile."""
+        if not frames.flags.c_contiguous or frames.dtype != np.uint8 or frames.ndim != 3:
+            raise ValueError("pixel_path_prefetch needs a C-contiguous (n, ch, cw) uint8 array")
+        n, ch, cw = frames.shape
+        self._check(self.L.h264a_pixel_path_prefetch(self.ctx, frames.ctypes.data_as(C.c_void_p), n, cw, ch))
+        self._prefetched.append((frames.ctypes.data, frames))  # released by the call that takes it
+
     def pixel_path_host(self, frames: np.ndarray, params: MeParams, lambda_me: float, split_gate: int, qp: int,
                         dz_div: int = 6, tab: Optional[np.ndarray] = None, out=None):
         n, ch, cw = frames.shape
@@ -391,4 +404,8 @@ class Accel:
             self.ctx, ptr(fr), n, cw, ch, C.byref(params), None if tab is None else ptr(tab), float(lambda_me),
             int(split_gate), qp, dz_div, ptr(out["picks"]), ptr(out["costs"]), ptr(out["coeffs"]),
             ptr(out["la_intra"]), ptr(out["la_inter"]), ptr(out["la_mvs"])))
+        for i, (addr, _) in enumerate(self._prefetched):  # the oldest prefetch of these frames is used up
+            if addr == fr.ctypes.data:
+                del self._prefetched[i]
+                break
         return out

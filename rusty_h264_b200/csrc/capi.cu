@@ -112,7 +112,10 @@ extern "C" int h264a_ctx_create(int device, h264a_ctx** out) {
     bool ev_ok = true;
     for (int i = 0; i < PP_EVENTS; i++)
         ev_ok = ev_ok && cudaEventCreateWithFlags(&c->pp_ev[i], cudaEventDisableTiming) == cudaSuccess;
+    for (int i = 0; i < PP_SLOTS; i++)
+        ev_ok = ev_ok && cudaEventCreateWithFlags(&c->pp_in[i].ev, cudaEventDisableTiming) == cudaSuccess;
     if (!ev_ok || cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->pf_stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&c->la_stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaMalloc(&c->d_counters, NUM_QUEUES * Q_COUNTER_STRIDE * sizeof(int32_t)) != cudaSuccess ||
@@ -133,6 +136,7 @@ extern "C" int h264a_ctx_destroy(h264a_ctx* ctx) {
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
     if (ctx->la_stream) cudaStreamSynchronize(ctx->la_stream);
+    if (ctx->pf_stream) cudaStreamSynchronize(ctx->pf_stream);
     if (ctx->d_counters) cudaFree(ctx->d_counters);
     if (ctx->d_status) cudaFree(ctx->d_status);
     for (int i = 0; i < NUM_QUEUES; i++)
@@ -143,8 +147,13 @@ extern "C" int h264a_ctx_destroy(h264a_ctx* ctx) {
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
     if (ctx->la_stream) cudaStreamDestroy(ctx->la_stream);
+    if (ctx->pf_stream) cudaStreamDestroy(ctx->pf_stream);
     for (int i = 0; i < PP_EVENTS; i++)
         if (ctx->pp_ev[i]) cudaEventDestroy(ctx->pp_ev[i]);
+    for (int i = 0; i < PP_SLOTS; i++) {
+        if (ctx->pp_in[i].d) cudaFree(ctx->pp_in[i].d);
+        if (ctx->pp_in[i].ev) cudaEventDestroy(ctx->pp_in[i].ev);
+    }
     delete ctx;
     return H264A_OK;
 }
@@ -251,6 +260,43 @@ static int ensure_pp_rows(h264a_ctx* ctx, size_t rows) {
     return H264A_OK;
 }
 
+// Grows input slot `s` to `bytes`.  Only called for a slot that holds no
+// pending upload and that no call is using, so nothing on the device reads it.
+static int ensure_slot(PpInput& s, size_t bytes) {
+    if (bytes <= s.cap) return H264A_OK;
+    if (s.d) cudaFree(s.d);
+    s.d = nullptr;
+    s.cap = 0;
+    if (cudaMalloc(&s.d, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(H264A_E_NOMEM, "pixel_path: input slot allocation failed");
+    }
+    s.cap = bytes;
+    return H264A_OK;
+}
+
+extern "C" int h264a_pixel_path_prefetch(h264a_ctx* ctx, const uint8_t* h_frames, int n, int cw, int ch) {
+    if (!ctx || !h_frames) return fail(H264A_E_ARG, "pixel_path_prefetch: null pointer");
+    if (n < 1 || cw < 16 || ch < 16 || cw % 16 || ch % 16) return fail(H264A_E_ARG, "pixel_path_prefetch: bad geometry");
+    int k = -1;
+    for (int i = 0; i < PP_SLOTS && k < 0; i++)
+        if (!ctx->pp_in[i].pending) k = i;
+    if (k < 0) return fail(H264A_E_ARG, "pixel_path_prefetch: two uploads are already pending");
+    PpInput& in = ctx->pp_in[k];
+    const size_t bytes = size_t(cw) * ch * n;
+    const int rc = ensure_slot(in, bytes);
+    if (rc) return rc;
+    H264A_CUDA(cudaMemcpyAsync(in.d, h_frames, bytes, cudaMemcpyHostToDevice, ctx->pf_stream));
+    H264A_CUDA(cudaEventRecord(in.ev, ctx->pf_stream));
+    in.h = h_frames;
+    in.n = n;
+    in.cw = cw;
+    in.ch = ch;
+    in.pending = 1;
+    in.seq = ++ctx->pp_seq;
+    return H264A_OK;
+}
+
 extern "C" int h264a_pixel_path_host(h264a_ctx* ctx, const uint8_t* h_frames, int n, int cw, int ch,
                                      const h264a_me_params* params, const uint16_t* h_mv_cost_tab, double lambda_me,
                                      int64_t split_gate, int qp, int dz_div, int32_t* h_picks, int64_t* h_costs,
@@ -266,7 +312,6 @@ extern "C" int h264a_pixel_path_host(h264a_ctx* ctx, const uint8_t* h_frames, in
     const size_t fs = size_t(cw) * ch, hs = fs / 4, p4 = size_t(4) * pw * ph;
     // one cached device arena
     size_t off = 0;
-    const size_t o_frames = off; off = align256(off + fs * n);
     const size_t o_planes = off; off = align256(off + p4 * (n > 1 ? n - 1 : 1));
     const size_t o_half = off; off = align256(off + hs * n);
     const size_t o_picks = off; off = align256(off + sizeof(int32_t) * 6 * nmb * n);
@@ -287,7 +332,35 @@ extern "C" int h264a_pixel_path_host(h264a_ctx* ctx, const uint8_t* h_frames, in
         ctx->pp_bytes = off;
     }
     char* base = reinterpret_cast<char*>(ctx->pp_buf);
-    uint8_t* d_frames = reinterpret_cast<uint8_t*>(base + o_frames);
+    // the input slot: the oldest pending prefetch of these frames, else a
+    // free slot the call uploads into (if both hold other prefetches, the
+    // newest is given up: a later call of its frames uploads them again)
+    int use = -1;
+    for (int i = 0; i < PP_SLOTS; i++) {
+        const PpInput& c = ctx->pp_in[i];
+        if (c.pending && c.h == h_frames && c.n == n && c.cw == cw && c.ch == ch &&
+            (use < 0 || c.seq < ctx->pp_in[use].seq))
+            use = i;
+    }
+    const bool prefetched = use >= 0;
+    if (!prefetched) {
+        for (int i = 0; i < PP_SLOTS && use < 0; i++)
+            if (!ctx->pp_in[i].pending) use = i;
+        if (use < 0) {
+            use = ctx->pp_in[0].seq > ctx->pp_in[1].seq ? 0 : 1;
+            H264A_CUDA(cudaEventSynchronize(ctx->pp_in[use].ev));
+        }
+        ctx->pp_in[use].pending = 0;
+        const int rs = ensure_slot(ctx->pp_in[use], fs * n);
+        if (rs) return rs;
+        ctx->pp_in[use].h = h_frames;
+        ctx->pp_in[use].n = n;
+        ctx->pp_in[use].cw = cw;
+        ctx->pp_in[use].ch = ch;
+    }
+    PpInput& in = ctx->pp_in[use];
+    in.pending = 0;
+    uint8_t* d_frames = in.d;
     uint8_t* d_planes = reinterpret_cast<uint8_t*>(base + o_planes);
     uint8_t* d_half = reinterpret_cast<uint8_t*>(base + o_half);
     int32_t* d_picks = reinterpret_cast<int32_t*>(base + o_picks);
@@ -299,7 +372,8 @@ extern "C" int h264a_pixel_path_host(h264a_ctx* ctx, const uint8_t* h_frames, in
     uint16_t* d_tab = reinterpret_cast<uint16_t*>(base + o_tab);
     // Three streams.  The frames go up in PP_CHUNKS chunks on the copy
     // stream while the compute stream builds each chunk's planes and half-res
-    // frames.  Then the lookahead (its own work queue) runs on the lookahead
+    // frames (frames prefetched by h264a_pixel_path_prefetch are one chunk,
+    // ready when its upload event fires).  Then the lookahead (its own work queue) runs on the lookahead
     // stream beside plain-ME with the fused MC + T/Q on the compute stream.
     // An MB row of every frame is final once all its MBs have stored their
     // coefficients (the kernel sets a host-visible word per row), and the
@@ -309,8 +383,8 @@ extern "C" int h264a_pixel_path_host(h264a_ctx* ctx, const uint8_t* h_frames, in
     // launch ends.
     cudaStream_t st = ctx->stream, cs = ctx->copy_stream, ls = ctx->la_stream;
     const int mb_w = cw / 16, mb_h = ch / 16;
-    const int nk = n < PP_CHUNKS ? n : PP_CHUNKS;
-    for (int k = 0; k < nk; k++) {
+    const int nk = prefetched ? 1 : (n < PP_CHUNKS ? n : PP_CHUNKS);
+    for (int k = 0; k < nk && !prefetched; k++) {
         const int a = int((long long)k * n / nk), b = int((long long)(k + 1) * n / nk);
         H264A_CUDA(cudaMemcpyAsync(d_frames + fs * a, h_frames + fs * a, fs * (b - a), cudaMemcpyHostToDevice, cs));
         H264A_CUDA(cudaEventRecord(ctx->pp_ev[k], cs));
@@ -330,7 +404,7 @@ extern "C" int h264a_pixel_path_host(h264a_ctx* ctx, const uint8_t* h_frames, in
     H264A_CUDA(cudaMemsetAsync(ctx->pp_row_count, 0, ctx->pp_rows_cap * sizeof(int32_t), st));
     for (int k = 0; k < nk; k++) {
         const int a = int((long long)k * n / nk), b = int((long long)(k + 1) * n / nk);
-        H264A_CUDA(cudaStreamWaitEvent(st, ctx->pp_ev[k], 0));
+        H264A_CUDA(cudaStreamWaitEvent(st, prefetched ? in.ev : ctx->pp_ev[k], 0));
         const int refs = (b < n - 1 ? b : n - 1) - a;  // reference pictures 0..n-2 in this chunk
         if (refs > 0) {
             rc = h264a_hpel_build(ctx, d_frames + fs * a, cw, ch, pad, refs, fs, d_planes + p4 * a, st);

@@ -28,6 +28,20 @@ constexpr int Q_MAIN = 0, Q_LOOKAHEAD = 1, NUM_QUEUES = 2, Q_COUNTER_STRIDE = 32
 constexpr int PP_CHUNKS = 4;
 constexpr int PP_EV_INPUTS = PP_CHUNKS, PP_EV_TQ = PP_CHUNKS + 1, PP_EV_LA = PP_CHUNKS + 2, PP_EVENTS = PP_CHUNKS + 3;
 
+// An input slot of h264a_pixel_path_host: a device copy of a batch of frames,
+// uploaded by h264a_pixel_path_prefetch ahead of the call that uses it
+// (pending until that call takes it) or by the call itself.
+struct PpInput {
+    uint8_t *d = nullptr;
+    size_t cap = 0;
+    const uint8_t *h = nullptr;  // the host frames it holds
+    int n = 0, cw = 0, ch = 0;
+    int pending = 0;             // prefetched, not yet used by a call
+    long long seq = 0;           // prefetch order
+    cudaEvent_t ev = nullptr;    // the upload is complete
+};
+constexpr int PP_SLOTS = 2;
+
 struct h264a_ctx {
     int device = 0;
     int num_sms = 0;
@@ -52,6 +66,10 @@ struct h264a_ctx {
     int32_t *pp_rows_dev = nullptr;
     size_t pp_rows_cap = 0;
     int32_t pp_token = 0;
+    // input slots and the stream their prefetch uploads run on
+    PpInput pp_in[PP_SLOTS];
+    long long pp_seq = 0;
+    cudaStream_t pf_stream = nullptr;
 };
 
 namespace h264a {

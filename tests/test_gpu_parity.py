@@ -845,6 +845,38 @@ def test_pixel_path_host_pinned_outputs_matches_oracle(acc):
         assert (got["picks"][0] == 0).all() and (got["coeffs"][0] == 0).all() and (got["costs"][0] == 0).all()
 
 
+def test_pixel_path_prefetch_matches_oracle(acc):
+    """Batches uploaded ahead of their calls by pixel_path_prefetch (pinned
+    host frames): every call equals the oracle. Covered: two pending
+    prefetches, a third refused, a call whose frames match none of them (it
+    uploads them itself and gives up the newer prefetch), a prefetch of another
+    geometry, and the streaming loop on one buffer (prefetch k+1, then call k)."""
+    torch = acc.torch
+    params, qp = A.default_me_params(), 28
+    lam = float(np.sqrt(A.frame_lambda(qp)))
+    gate = A.split_gate_for_qp(qp)
+    clips = [synth.coded_luma(synth.cif_clip(5, seed)[0]) for seed in (3, 4, 5)]
+    clips.append(synth.coded_luma(synth.cif_clip(4, 6, 176, 144)[0]))
+    a, b, c, s = (torch.from_numpy(np.ascontiguousarray(x)).pin_memory().numpy() for x in clips)
+    want = [O.pixel_path_clip(x, O.balanced_params(), lam, gate, qp, nthreads=8) for x in (a, b, c, s)]
+    run = lambda x: acc.pixel_path_host(x, params, lam, gate, qp)
+    acc.pixel_path_prefetch(a)
+    acc.pixel_path_prefetch(b)
+    with pytest.raises(A.AccelError):
+        acc.pixel_path_prefetch(c)  # two uploads are already pending
+    compare_pixel_path(run(c), want[2])
+    compare_pixel_path(run(a), want[0])
+    acc.pixel_path_prefetch(s)
+    compare_pixel_path(run(b), want[1])
+    compare_pixel_path(run(s), want[3])
+    acc.pixel_path_prefetch(a)
+    for k in range(3):
+        if k < 2:
+            acc.pixel_path_prefetch(a)
+        compare_pixel_path(run(a), want[0])
+    assert acc._prefetched == []
+
+
 def test_pixel_path_host_1080p_matches_oracle(acc):
     y, _, _ = synth.hd_clip(3, 1)
     frames = synth.coded_luma(y)
