@@ -417,7 +417,24 @@ extern "C" int h264a_pixel_path_host(h264a_ctx* ctx, const uint8_t* h_frames, in
     H264A_CUDA(cudaStreamWaitEvent(ls, ctx->pp_ev[PP_EV_INPUTS], 0));
     rc = h264a_lookahead_costs(ctx, d_frames, d_half, cw, ch, n, 2, d_intra, d_inter, d_mvs, ls);
     if (rc) return rc;
-    H264A_CUDA(cudaEventRecord(ctx->pp_ev[PP_EV_LA], ls));
+    // From here on copies into the caller's buffers may be in flight on the
+    // copy and lookahead streams: every return drains both first.
+    auto drain = [&](int code) {
+        cudaStreamSynchronize(cs);
+        cudaStreamSynchronize(ls);
+        cudaGetLastError();
+        return code;
+    };
+    auto check = [&](cudaError_t e, const char* what) { return e == cudaSuccess ? H264A_OK : drain(cuda_fail(e, what)); };
+    // the lookahead ends long before ME: its results come down under ME
+    if ((rc = check(cudaMemcpyAsync(h_la_intra, d_intra, sizeof(int32_t) * nmb * n, cudaMemcpyDeviceToHost, ls),
+                    "pixel_path_host: lookahead download")) ||
+        (rc = check(cudaMemcpyAsync(h_la_inter, d_inter, sizeof(int32_t) * nmb * n, cudaMemcpyDeviceToHost, ls),
+                    "pixel_path_host: lookahead download")) ||
+        (rc = check(cudaMemcpyAsync(h_la_mvs, d_mvs, sizeof(int32_t) * 2 * nmb * n, cudaMemcpyDeviceToHost, ls),
+                    "pixel_path_host: lookahead download")) ||
+        (rc = check(cudaEventRecord(ctx->pp_ev[PP_EV_LA], ls), "pixel_path_host: lookahead event")))
+        return rc;
     if (n > 1) {
         std::vector<h264a_me_frame> mf(n - 1);
         std::vector<MeTqOut> tq(n - 1);
@@ -428,9 +445,9 @@ extern "C" int h264a_pixel_path_host(h264a_ctx* ctx, const uint8_t* h_frames, in
                                 ctx->pp_rows_dev + size_t(f - 1) * mb_h, token};
         }
         rc = me_frames_run(ctx, mf.data(), n - 1, &prm, tq.data(), st);
-        if (rc) return rc;
+        if (rc) return drain(rc);
     }
-    H264A_CUDA(cudaEventRecord(ctx->pp_ev[PP_EV_TQ], st));
+    if ((rc = check(cudaEventRecord(ctx->pp_ev[PP_EV_TQ], st), "pixel_path_host: ME + T/Q event"))) return rc;
     // frame 0 (the IDR) has no pick or coefficients: the kernels never write its rows
     memset(h_picks, 0, sizeof(int32_t) * 6 * nmb);
     memset(h_costs, 0, sizeof(int64_t) * 2 * nmb);
@@ -455,9 +472,7 @@ extern "C" int h264a_pixel_path_host(h264a_ctx* ctx, const uint8_t* h_frames, in
             const cudaError_t q = cudaEventQuery(ctx->pp_ev[PP_EV_TQ]);  // before the words: done means all final
             if (q != cudaSuccess && q != cudaErrorNotReady) {
                 cudaGetLastError();
-                cudaStreamSynchronize(cs);  // no copy into the caller's buffers outlives the call
-                cudaGetLastError();
-                return cuda_fail(q, "pixel_path_host: ME + T/Q");
+                return drain(cuda_fail(q, "pixel_path_host: ME + T/Q"));  // no copy outlives the call
             }
             int ready = mb_h;
             if (q != cudaSuccess) {
@@ -470,21 +485,15 @@ extern "C" int h264a_pixel_path_host(h264a_ctx* ctx, const uint8_t* h_frames, in
             }
             if (ready > sent) {
                 rc = copy_rows(sent, ready);
-                if (rc) {
-                    cudaStreamSynchronize(cs);
-                    cudaGetLastError();
-                    return rc;
-                }
+                if (rc) return drain(rc);
                 sent = ready;
             }
             if (sent == mb_h) break;
             std::this_thread::sleep_for(std::chrono::microseconds(100));
         }
     }
-    H264A_CUDA(cudaStreamWaitEvent(cs, ctx->pp_ev[PP_EV_LA], 0));
-    H264A_CUDA(cudaMemcpyAsync(h_la_intra, d_intra, sizeof(int32_t) * nmb * n, cudaMemcpyDeviceToHost, cs));
-    H264A_CUDA(cudaMemcpyAsync(h_la_inter, d_inter, sizeof(int32_t) * nmb * n, cudaMemcpyDeviceToHost, cs));
-    H264A_CUDA(cudaMemcpyAsync(h_la_mvs, d_mvs, sizeof(int32_t) * 2 * nmb * n, cudaMemcpyDeviceToHost, cs));
-    H264A_CUDA(cudaStreamSynchronize(cs));
+    const cudaError_t e_cs = cudaStreamSynchronize(cs), e_ls = cudaStreamSynchronize(ls);
+    if (e_cs != cudaSuccess || e_ls != cudaSuccess)
+        return drain(cuda_fail(e_cs != cudaSuccess ? e_cs : e_ls, "pixel_path_host: result downloads"));
     return h264a_sync(ctx, st);
 }
