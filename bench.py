@@ -57,6 +57,8 @@ def parse():
     ap.add_argument("--frames", type=int, default=FRAMES)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--mixed", action="store_true",
+                    help="also time plain-ME over the 16-stream mixed-resolution batch (not part of value)")
     return ap.parse_args()
 
 
@@ -89,6 +91,95 @@ def clip(seed: int, frames: int):
     except OSError:
         pass
     return f
+
+
+# The mixed-resolution batch: (width, height, streams), 16 streams of 30 frames.
+MIXED = ((352, 288, 4), (1280, 720, 6), (1920, 1080, 4), (3840, 2160, 2))
+MIXED_FRAMES = 30
+
+
+def mixed_stream(args):
+    """Coded luma of one stream of the mixed batch (the 1080p generator at w x h)."""
+    seed, w, h = args
+    from rusty_h264_b200 import synth
+
+    cache = os.path.join("/tmp", f"h264a_mixed_s{seed}_{w}x{h}_f{MIXED_FRAMES}.npy")
+    if os.path.exists(cache):
+        return np.load(cache)
+    y, _, _ = synth.hd_clip(MIXED_FRAMES, seed, w, h)
+    f = synth.coded_luma(y)
+    try:
+        np.save(cache, f)
+    except OSError:
+        pass
+    return f
+
+
+def mixed_inputs():
+    """The 16 streams, generated in a spawn-started process pool."""
+    import concurrent.futures as cf
+    import multiprocessing as mp
+
+    jobs = []
+    for w, h, k in MIXED:
+        jobs += [(1000 + len(jobs), w, h) for _ in range(k)]
+    with cf.ProcessPoolExecutor(max_workers=min(len(jobs), os.cpu_count() or 1),
+                                mp_context=mp.get_context("spawn")) as ex:
+        return list(ex.map(mixed_stream, jobs))
+
+
+def mixed_batch(acc, torch, streams, params, lam: float, gate: int):
+    """Plain-ME (one reference) of every P frame of the mixed batch in one
+    h264a_me_frames call: one persistent wavefront launch over all 464 frames,
+    largest first (the frame table in device memory).  Every stream's
+    picks and costs must equal the same stream run on its own; then the
+    batched call is timed with CUDA events (3 warm-up, 5 timed)."""
+    from rusty_h264_b200 import accel as A
+
+    bufs, frames_all, per_stream = [], [], []
+    for f in streams:
+        n, ch, cw = f.shape
+        nmb = (cw // 16) * (ch // 16)
+        d = torch.from_numpy(f).cuda()
+        planes = acc.hpel_build(d[: n - 1], 32)
+        picks = torch.zeros((n, nmb, 6), dtype=torch.int32, device="cuda")
+        costs = torch.zeros((n, nmb, 2), dtype=torch.int64, device="cuda")
+        fr = [A.MeFrame(A.Picture(d[i].data_ptr(), planes[i - 1].data_ptr(), cw, ch, 32), lam, gate,
+                        picks[i].data_ptr(), costs[i].data_ptr()) for i in range(1, n)]
+        bufs.append((d, planes, picks, costs))
+        frames_all += fr
+        per_stream.append(fr)
+    acc.sync()
+    alone = []
+    for s, fr in enumerate(per_stream):
+        acc.me_frames(fr, params)
+        acc.sync()
+        alone.append((bufs[s][2].clone(), bufs[s][3].clone()))
+    for b in bufs:
+        b[2].zero_()
+        b[3].zero_()
+    acc.me_frames(frames_all, params)
+    acc.sync()
+    for s, b in enumerate(bufs):
+        assert torch.equal(b[2], alone[s][0]) and torch.equal(b[3], alone[s][1]), f"stream {s}: batched != alone"
+    ts = []
+    for it in range(8):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        acc.me_frames(frames_all, params)
+        e1.record()
+        torch.cuda.synchronize()
+        if it >= 3:
+            ts.append(e0.elapsed_time(e1))
+    acc.sync()
+    ms = float(np.median(ts))
+    px = sum((f.shape[0] - 1) * f.shape[1] * f.shape[2] for f in streams)
+    mbs = sum((f.shape[0] - 1) * (f.shape[1] // 16) * (f.shape[2] // 16) for f in streams)
+    return {"streams": "4 x 352x288, 6 x 1280x720, 4 x 1920x1080, 2 x 3840x2160; 30 frames each, 1080p generator",
+            "p_frames": len(frames_all), "macroblocks": int(mbs), "me_ms": round(ms, 3),
+            "me_mpx_s": round(px / (ms * 1e-3) / 1e6, 1), "launches": 1,
+            "batched_equals_alone": True,
+            "note": "plain-ME of all P frames, one reference; not part of value"}
 
 
 class ClockSampler:
@@ -245,6 +336,7 @@ def run_ours(args, ws, rank, local):
 
     from rusty_h264_b200 import accel as A
 
+    mixed_streams = mixed_inputs() if args.mixed and rank == 0 else None  # host work, before any GPU call
     torch.cuda.set_device(local)
     acc = A.Accel(local)
     n = args.frames
@@ -513,6 +605,8 @@ def run_ours(args, ws, rank, local):
         line["cpu_baseline"] = {"value": round(v, 3), "unit": "Mpx/s", "cores": 1, "kind": "port",
                                 "sample": "3 frames of the 1080p clip (2 P frames + lookahead), one thread",
                                 "cpu": cpu_model(), "stages": cpu_stages(sample, lam, gate)}
+    if args.mixed and rank == 0:
+        line["mixed_batch"] = mixed_batch(acc, torch, mixed_streams, params, lam, gate)
     if rank == 0:
         print(json.dumps(line), flush=True)
     acc.close()

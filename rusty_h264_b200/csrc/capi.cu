@@ -142,6 +142,9 @@ extern "C" int h264a_ctx_destroy(h264a_ctx* ctx) {
     for (int i = 0; i < NUM_QUEUES; i++)
         if (ctx->q[i].d_flags) cudaFree(ctx->q[i].d_flags);
     if (ctx->pp_buf) cudaFree(ctx->pp_buf);
+    if (ctx->me_tab) cudaFree(ctx->me_tab);
+    if (ctx->me_tab_host) cudaFreeHost(ctx->me_tab_host);
+    if (ctx->me_tab_ev) cudaEventDestroy(ctx->me_tab_ev);
     if (ctx->pp_row_count) cudaFree(ctx->pp_row_count);
     if (ctx->pp_rows_host) cudaFreeHost(ctx->pp_rows_host);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -168,7 +171,12 @@ extern "C" int h264a_sync(h264a_ctx* ctx, void* stream) {
     H264A_CUDA(cudaMemcpy(&status, ctx->d_status, sizeof status, cudaMemcpyDeviceToHost));
     if (status != 0) {
         H264A_CUDA(cudaMemset(ctx->d_status, 0, sizeof(int32_t)));
-        return fail(H264A_E_TIMEOUT, "a bounded wait for a neighbouring macroblock ran out (status " +
+        // the code a persistent kernel recorded when its wait gave up
+        const char* what = status == 1   ? "for a neighbouring macroblock's flag"
+                           : status == 2 ? "of the self-test, on a flag nothing sets"
+                           : status == 3 ? "for a window copy into shared memory"
+                                         : "";
+        return fail(H264A_E_TIMEOUT, std::string("a bounded wait ") + what + " ran out (status " +
                                          std::to_string(status) + ")");
     }
     return H264A_OK;

@@ -66,6 +66,13 @@ struct h264a_ctx {
     int32_t *pp_rows_dev = nullptr;
     size_t pp_rows_cap = 0;
     int32_t pp_token = 0;
+    // frame table of plain-ME launches over more than 96 frames: the device
+    // copy, its pinned staging buffer (me_tab_cap bytes each) and the event
+    // of the last upload from it
+    void *me_tab = nullptr;
+    void *me_tab_host = nullptr;
+    size_t me_tab_cap = 0;
+    cudaEvent_t me_tab_ev = nullptr;
     // input slots and the stream their prefetch uploads run on
     PpInput pp_in[PP_SLOTS];
     long long pp_seq = 0;

@@ -1027,7 +1027,9 @@ struct FrameDesc {
 // one before the (k+1)-th of any frame: segment j covers positions
 // [nmb[j+1], nmb[j]) of frames 0..j, so its tickets are (nmb[j]-nmb[j+1])*(j+1),
 // and segments are dealt from j = n-1 (every frame) down to j = 0 (the
-// largest frame's tail): seg_start[s] is the first ticket of j = n-1-s.
+// largest frame's tail).  Only the non-empty segments are stored (one per
+// distinct frame size): seg_start[s] is the first ticket of segment seg_j[s],
+// seg_start[nseg] the ticket count.
 // Within a frame the k-th MB is taken in wavefront order (anti-diagonals
 // t = x + 2y, then y): every MB's neighbours (left, top, top-left, top-right)
 // lie on earlier diagonals, so a window of resident warps always holds MBs
@@ -1036,7 +1038,29 @@ constexpr int ME_MAXF = 96;
 struct FrameBatch {
     FrameDesc f[ME_MAXF];
     long long seg_start[ME_MAXF + 1];
-    int n;
+    int seg_j[ME_MAXF];
+    int n, nseg;
+};
+// The frame table as the kernel body reads it: the launch's parameters
+// (FrameBatch, up to ME_MAXF frames) or arrays in device memory (any count).
+struct ParamTable {
+    const FrameBatch& b;
+    __device__ __forceinline__ int n() const { return b.n; }
+    __device__ __forceinline__ int nseg() const { return b.nseg; }
+    __device__ __forceinline__ long long seg(int s) const { return b.seg_start[s]; }
+    __device__ __forceinline__ int segj(int s) const { return b.seg_j[s]; }
+    __device__ __forceinline__ const FrameDesc& fr(int i) const { return b.f[i]; }
+};
+struct DeviceTable {
+    const FrameDesc* f;
+    const long long* seg_start;
+    const int* seg_j;
+    int nf, ns;
+    __device__ __forceinline__ int n() const { return nf; }
+    __device__ __forceinline__ int nseg() const { return ns; }
+    __device__ __forceinline__ long long seg(int s) const { return __ldg(seg_start + s); }
+    __device__ __forceinline__ int segj(int s) const { return __ldg(seg_j + s); }
+    __device__ __forceinline__ const FrameDesc& fr(int i) const { return f[i]; }
 };
 static_assert(sizeof(FrameBatch) + 512 <= 32764, "me_frames_kernel's parameters must fit the 32 KB parameter space");
 
@@ -1071,13 +1095,10 @@ __device__ __forceinline__ int2 predict_mv_ref0(bool aa, int2 a, bool ba, int2 b
 // partitions (mb16.rs:8869-8913), and publishes the pick (then, for
 // h264a_me_tq_frames, the MB's MC + T/Q).  BAL: the Balanced preset's knobs
 // as constants.  Dynamic shared memory: ME_WARPS windows of WIN_BYTES.
-template <bool BAL>
-__global__ void __launch_bounds__(32 * ME_WARPS, ME_MIN_BLOCKS) me_frames_kernel(const __grid_constant__ FrameBatch batch,
-                                                                    long long total,
-                                                                    const __grid_constant__ MeParamsDev prm,
-                                                                    int* __restrict__ counter, int* __restrict__ flags,
-                                                                    int epoch, int* __restrict__ status,
-                                                                    int spin_limit) {
+template <bool BAL, class TAB>
+__device__ __forceinline__ void me_frames_body(const TAB& tab, long long total, const MeParamsDev& prm,
+                                               int* __restrict__ counter, int* __restrict__ flags, int epoch,
+                                               int* __restrict__ status, int spin_limit) {
     __shared__ WarpScratch scratch[ME_WARPS];
     __shared__ __align__(8) unsigned long long win_bar[ME_WARPS];
     extern __shared__ __align__(128) uint8_t me_win[];
@@ -1096,13 +1117,13 @@ __global__ void __launch_bounds__(32 * ME_WARPS, ME_MIN_BLOCKS) me_frames_kernel
         if (lane == 0) t = atomicAdd(counter, 1);
         t = __shfl_sync(0xffffffffu, t, 0);
         if (t >= total) return;
-        // segments are dealt from s = 0 (every frame, j = n - 1) on
+        // the ticket's segment (dealt in order), frame and wavefront position
         int s = 0;
-        while (s + 1 < batch.n && batch.seg_start[s + 1] <= t) s++;
-        const int j = batch.n - 1 - s;
-        const long long u = t - batch.seg_start[s];
-        const int nxt = j + 1 < batch.n ? batch.f[j + 1].mb_w * batch.f[j + 1].mb_h : 0;
-        const FrameDesc& fd = batch.f[int(u % (j + 1))];
+        while (s + 1 < tab.nseg() && tab.seg(s + 1) <= t) s++;
+        const int j = tab.segj(s);
+        const long long u = t - tab.seg(s);
+        const int nxt = j + 1 < tab.n() ? tab.fr(j + 1).mb_w * tab.fr(j + 1).mb_h : 0;
+        const FrameDesc& fd = tab.fr(int(u % (j + 1)));
         const int k = nxt + int(u / (j + 1));  // position in the frame's wavefront order
         int mbx, mby;
         wave_mb(fd.mb_w, fd.mb_h, k, mbx, mby);
@@ -1243,6 +1264,26 @@ __global__ void __launch_bounds__(32 * ME_WARPS, ME_MIN_BLOCKS) me_frames_kernel
     }
 }
 
+template <bool BAL>
+__global__ void __launch_bounds__(32 * ME_WARPS, ME_MIN_BLOCKS)
+    me_frames_kernel(const __grid_constant__ FrameBatch batch, long long total, const __grid_constant__ MeParamsDev prm,
+                     int* __restrict__ counter, int* __restrict__ flags, int epoch, int* __restrict__ status,
+                     int spin_limit) {
+    me_frames_body<BAL>(ParamTable{batch}, total, prm, counter, flags, epoch, status, spin_limit);
+}
+
+// The same kernel over a frame table in device memory (more than ME_MAXF
+// frames in one wavefront launch); the frames' tensor maps are read there.
+template <bool BAL>
+__global__ void __launch_bounds__(32 * ME_WARPS, ME_MIN_BLOCKS)
+    me_frames_dkernel(const FrameDesc* __restrict__ frames, const long long* __restrict__ seg_start,
+                      const int* __restrict__ seg_j, int nframes, int nseg, long long total,
+                      const __grid_constant__ MeParamsDev prm, int* __restrict__ counter, int* __restrict__ flags,
+                      int epoch, int* __restrict__ status, int spin_limit) {
+    me_frames_body<BAL>(DeviceTable{frames, seg_start, seg_j, nframes, nseg}, total, prm, counter, flags, epoch,
+                        status, spin_limit);
+}
+
 // One warp waits on a flag that nothing sets; the bounded wait must give up
 // after `limit` polls and record status code 2.
 __global__ void bounded_wait_selftest_kernel(const int* flag, int* status, int limit) {
@@ -1295,6 +1336,8 @@ static int me_frames_setup(int& per_sm) {
     const int smem = ME_WARPS * WIN_BYTES;
     H264A_CUDA(cudaFuncSetAttribute(me_frames_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     H264A_CUDA(cudaFuncSetAttribute(me_frames_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    H264A_CUDA(cudaFuncSetAttribute(me_frames_dkernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    H264A_CUDA(cudaFuncSetAttribute(me_frames_dkernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     per_sm = 0;
     H264A_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, me_frames_kernel<false>, 32 * ME_WARPS, smem));
     if (per_sm < 1) per_sm = 1;
@@ -1309,20 +1352,43 @@ static bool balanced_preset(const MeParamsDev& p) {
            p.me_subpel_iter == 1 && p.sp_maxit == 0 && p.sp_fc == 0;
 }
 
-// Fills seg_start of a batch whose fb.n frames are sorted by MB count,
-// descending, in dealing order (segment j = n-1-s at index s); returns the
-// ticket count, which equals the batch's MB count.
-static long long fill_segments(FrameBatch& fb) {
+// The non-empty segments of the ticket order of nf frames sorted by MB count,
+// descending: segment j (positions [nmb(j+1), nmb(j)) of frames 0..j) has
+// (nmb(j) - nmb(j+1)) * (j+1) tickets, and segments are dealt from
+// j = nf-1 down.  Writes their first tickets (start[nseg] = the ticket count,
+// which equals the frames' MB count) and j values; returns nseg.
+static int make_segments(const FrameDesc* f, int nf, long long* start, int* segj) {
     long long acc = 0;
-    for (int s = 0; s < fb.n; s++) {
-        const int j = fb.n - 1 - s;
-        fb.seg_start[s] = acc;
-        const long long nj = (long long)fb.f[j].mb_w * fb.f[j].mb_h;
-        const long long nn = j + 1 < fb.n ? (long long)fb.f[j + 1].mb_w * fb.f[j + 1].mb_h : 0;
+    int ns = 0;
+    for (int j = nf - 1; j >= 0; j--) {
+        const long long nj = (long long)f[j].mb_w * f[j].mb_h;
+        const long long nn = j + 1 < nf ? (long long)f[j + 1].mb_w * f[j + 1].mb_h : 0;
+        if (nj == nn) continue;
+        start[ns] = acc;
+        segj[ns] = j;
+        ns++;
         acc += (nj - nn) * (j + 1);
     }
-    fb.seg_start[fb.n] = acc;
-    return acc;
+    start[ns] = acc;
+    return ns;
+}
+
+// fb.nseg and the segment arrays of a batch of fb.n sorted frames; returns the
+// ticket count.
+static long long fill_segments(FrameBatch& fb) {
+    fb.nseg = make_segments(fb.f, fb.n, fb.seg_start, fb.seg_j);
+    return fb.seg_start[fb.nseg];
+}
+
+static void launch_me_frames_dtab(const MeParamsDev& prm, unsigned blocks, cudaStream_t st, const FrameDesc* frames,
+                                  const long long* seg_start, const int* seg_j, int nframes, int nseg, long long total,
+                                  int* counter, int* flags, int epoch, int* status) {
+    if (balanced_preset(prm))
+        me_frames_dkernel<true><<<blocks, 32 * ME_WARPS, ME_WARPS * WIN_BYTES, st>>>(
+            frames, seg_start, seg_j, nframes, nseg, total, prm, counter, flags, epoch, status, SPIN_LIMIT);
+    else
+        me_frames_dkernel<false><<<blocks, 32 * ME_WARPS, ME_WARPS * WIN_BYTES, st>>>(
+            frames, seg_start, seg_j, nframes, nseg, total, prm, counter, flags, epoch, status, SPIN_LIMIT);
 }
 
 static void launch_me_frames(const MeParamsDev& prm, unsigned blocks, cudaStream_t st, const FrameBatch& fb,
@@ -1381,55 +1447,89 @@ int h264a::me_frames_run(h264a_ctx* ctx, const h264a_me_frame* h_frames, int nfr
     int per_sm = 0;
     int rc0 = me_frames_setup(per_sm);
     if (rc0) return rc0;
-    // frames are launched in groups of up to ME_MAXF, largest first
+    // One wavefront launch over all frames, largest first: the frame table in
+    // the kernel's parameters up to ME_MAXF frames, in device memory beyond.
     std::vector<int> order(nframes);
     for (int i = 0; i < nframes; i++) order[i] = i;
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
         return (long long)h_frames[a].pic.cw * h_frames[a].pic.ch > (long long)h_frames[b].pic.cw * h_frames[b].pic.ch;
     });
-    for (int g0 = 0; g0 < nframes; g0 += ME_MAXF) {
-        const int gn = nframes - g0 < ME_MAXF ? nframes - g0 : ME_MAXF;
+    std::vector<FrameDesc> desc(nframes);
+    memset(desc.data(), 0, sizeof(FrameDesc) * nframes);
+    long long total = 0;
+    for (int k = 0; k < nframes; k++) {
+        const h264a_me_frame& f = h_frames[order[k]];
+        FrameDesc& d = desc[k];
+        d.pic = f.pic;
+        d.tmap_ok = encode_window_map(&d.tmap, f.pic.d_planes, f.pic.cw + 2 * f.pic.pad, f.pic.ch + 2 * f.pic.pad);
+        d.lambda_me = f.lambda_me;
+        d.split_gate = f.split_gate;
+        d.picks = f.d_picks;
+        d.costs = f.d_costs;
+        d.mb_w = f.pic.cw / 16;
+        d.mb_h = f.pic.ch / 16;
+        d.flag_base = int(total);
+        if (tq) {
+            const MeTqOut& t = tq[order[k]];
+            d.coeffs = t.coeffs;
+            make_quant_row4(t.qp, t.dz_div, d.qff, d.qmf);
+            d.row_count = t.row_count;
+            d.row_done = t.row_done;
+            d.row_token = t.row_token;
+        }
+        total += (long long)d.mb_w * d.mb_h;
+        if (total >= (1LL << 31)) return fail(H264A_E_ARG, "me_frames: too many macroblocks in one call");
+    }
+    std::vector<long long> seg(nframes + 1);
+    std::vector<int> segj(nframes);
+    const int nseg = make_segments(desc.data(), nframes, seg.data(), segj.data());
+    if (seg[nseg] != total) return fail(H264A_E_ARG, "me_frames: internal queue layout error");
+    int rc = ensure_me_scratch(ctx, size_t(total));
+    if (rc) return rc;
+    H264A_CUDA(cudaMemsetAsync(ctx->q[Q_MAIN].d_counter, 0, sizeof(int32_t), st));
+    const int epoch = next_epoch(ctx, st);
+    if (epoch < 0) return H264A_E_CUDA;
+    long long blocks = (long long)ctx->num_sms * per_sm;
+    const long long need = (total + ME_WARPS - 1) / ME_WARPS;
+    if (blocks > need) blocks = need;
+    if (nframes <= ME_MAXF) {
         FrameBatch fb;
         memset(&fb, 0, sizeof fb);
-        fb.n = gn;
-        long long total = 0;
-        for (int k = 0; k < gn; k++) {
-            const h264a_me_frame& f = h_frames[order[g0 + k]];
-            FrameDesc& d = fb.f[k];
-            d.pic = f.pic;
-            d.tmap_ok = encode_window_map(&d.tmap, f.pic.d_planes, f.pic.cw + 2 * f.pic.pad, f.pic.ch + 2 * f.pic.pad);
-            d.lambda_me = f.lambda_me;
-            d.split_gate = f.split_gate;
-            d.picks = f.d_picks;
-            d.costs = f.d_costs;
-            d.mb_w = f.pic.cw / 16;
-            d.mb_h = f.pic.ch / 16;
-            d.flag_base = int(total);
-            if (tq) {
-                const MeTqOut& t = tq[order[g0 + k]];
-                d.coeffs = t.coeffs;
-                make_quant_row4(t.qp, t.dz_div, d.qff, d.qmf);
-                d.row_count = t.row_count;
-                d.row_done = t.row_done;
-                d.row_token = t.row_token;
-            }
-            total += (long long)d.mb_w * d.mb_h;
-        }
+        fb.n = nframes;
+        memcpy(fb.f, desc.data(), sizeof(FrameDesc) * nframes);
         if (fill_segments(fb) != total) return fail(H264A_E_ARG, "me_frames: internal queue layout error");
-        int rc = ensure_me_scratch(ctx, size_t(total));
-        if (rc) return rc;
-        H264A_CUDA(cudaMemsetAsync(ctx->q[Q_MAIN].d_counter, 0, sizeof(int32_t), st));
-        const int epoch = next_epoch(ctx, st);
-        if (epoch < 0) return H264A_E_CUDA;
-        long long blocks = (long long)ctx->num_sms * per_sm;
-        const long long need = (total + ME_WARPS - 1) / ME_WARPS;
-        if (blocks > need) blocks = need;
         launch_me_frames(prm, unsigned(blocks), st, fb, total, ctx->q[Q_MAIN].d_counter, ctx->q[Q_MAIN].d_flags, epoch,
                          ctx->d_status);
-        rc = check_launch("me_frames_kernel");
-        if (rc) return rc;
+        return check_launch("me_frames_kernel");
     }
-    return H264A_OK;
+    // the table, its segment starts and j values in one device buffer, uploaded
+    // from a pinned staging buffer (reused once its previous upload is done)
+    const size_t b_desc = sizeof(FrameDesc) * nframes, b_seg = sizeof(long long) * (nseg + 1),
+                 b_j = sizeof(int) * nseg, bytes = b_desc + b_seg + b_j;
+    if (!ctx->me_tab_ev) H264A_CUDA(cudaEventCreateWithFlags(&ctx->me_tab_ev, cudaEventDisableTiming));
+    H264A_CUDA(cudaEventSynchronize(ctx->me_tab_ev));
+    if (bytes > ctx->me_tab_cap) {
+        if (ctx->me_tab) cudaFree(ctx->me_tab);
+        if (ctx->me_tab_host) cudaFreeHost(ctx->me_tab_host);
+        ctx->me_tab = ctx->me_tab_host = nullptr;
+        ctx->me_tab_cap = 0;
+        if (cudaMalloc(&ctx->me_tab, bytes) != cudaSuccess || cudaMallocHost(&ctx->me_tab_host, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(H264A_E_NOMEM, "me_frames: frame table allocation failed");
+        }
+        ctx->me_tab_cap = bytes;
+    }
+    char* hst = static_cast<char*>(ctx->me_tab_host);
+    memcpy(hst, desc.data(), b_desc);
+    memcpy(hst + b_desc, seg.data(), b_seg);
+    memcpy(hst + b_desc + b_seg, segj.data(), b_j);
+    H264A_CUDA(cudaMemcpyAsync(ctx->me_tab, hst, bytes, cudaMemcpyHostToDevice, st));
+    H264A_CUDA(cudaEventRecord(ctx->me_tab_ev, st));
+    char* dv = static_cast<char*>(ctx->me_tab);
+    launch_me_frames_dtab(prm, unsigned(blocks), st, reinterpret_cast<const FrameDesc*>(dv),
+                          reinterpret_cast<const long long*>(dv + b_desc), reinterpret_cast<const int*>(dv + b_desc + b_seg),
+                          nframes, nseg, total, ctx->q[Q_MAIN].d_counter, ctx->q[Q_MAIN].d_flags, epoch, ctx->d_status);
+    return check_launch("me_frames_dkernel");
 }
 
 extern "C" int h264a_me_frames(h264a_ctx* ctx, const h264a_me_frame* h_frames, int nframes,

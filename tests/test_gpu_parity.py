@@ -299,6 +299,27 @@ def test_me_frames_single_mb_and_flat(acc):
         assert np.array_equal(picks[:, :5], wp[:, :5]) and np.array_equal(costs, wc)
 
 
+@pytest.mark.parametrize("variant", ["balanced", "sadfp"])
+def test_me_frames_more_than_96_frames_in_one_launch(acc, variant):
+    """137 frames of three sizes in one call: more than a launch's parameters
+    hold, so the frame table goes to device memory and one wavefront launch
+    deals them all. Bit-exact with the oracle frame by frame, for the
+    Balanced instance and the generic one."""
+    params = A.default_me_params() if variant == "balanced" else A.default_me_params(sadfp=1)
+    op = O.balanced_params() if variant == "balanced" else oracle_params({"sadfp": 1})
+    lam = float(np.sqrt(A.frame_lambda(30)))
+    gate = A.split_gate_for_qp(30)
+    pairs = []
+    for i, (w, h) in enumerate([(160, 96)] * 100 + [(352, 288)] * 7 + [(64, 48)] * 30):
+        y, _, _ = synth.cif_clip(2, 50 + i, w, h)
+        f = synth.coded_luma(y)
+        pairs.append((f[1], f[0]))
+    got = run_me_frames(acc, pairs, params, lam, gate)
+    for k, ((src, ref), (picks, costs)) in enumerate(zip(pairs, got)):
+        wp, wc = O.me_frame(src, ref, O.build_planes4(ref, 32), op, lam, gate)
+        assert np.array_equal(picks[:, :5], wp[:, :5]) and np.array_equal(costs, wc), (k, src.shape)
+
+
 def test_me_frames_2160p_720p_cif_in_one_launch(acc):
     """The resolutions of the multi-stream workload (CIF, 720p, 2160p) in one
     wavefront launch, frames of different sizes interleaving in the queue,
@@ -898,7 +919,8 @@ def test_pixel_path_host_1080p_matches_oracle(acc):
 
 def test_bounded_wait_times_out_and_context_survives(acc, cif):
     assert acc.selftest_bounded_wait(2000) == A.H264A_E_TIMEOUT
-    assert b"bounded wait" in acc.L.h264a_last_error()
+    msg = acc.L.h264a_last_error()
+    assert b"bounded wait" in msg and b"self-test" in msg and b"status 2" in msg
     # the context and device still work afterwards
     got = acc.hpel_build(dev(acc, cif[:1]), 32)
     acc.sync()
