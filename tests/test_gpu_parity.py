@@ -358,12 +358,15 @@ def test_me_frames_window_edges(acc, cif, pad):
         assert np.array_equal(picks[:, :5], wp[:, :5]) and np.array_equal(costs, wc), pad
 
 
-def test_fullpel_grid_matches_oracle(acc, cif):
+@pytest.mark.parametrize("R,stride", [(8, 7), (16, 29), (32, 53)])
+def test_fullpel_grid_matches_oracle(acc, cif, R, stride):
+    """SAD and SATD grids and both argmins against the oracle on a strided
+    subset of MBs (and the last one): R = 8, 16 and 32, whose SAD launches
+    take different numbers of MBs per CTA."""
     src, ref = cif[3], cif[2]
     planes = O.build_planes4(ref, 32)
     d_src, d_pl = dev(acc, src), dev(acc, planes)
     pic = A.Picture(d_src.data_ptr(), d_pl.data_ptr(), 352, 288, 32)
-    R = 8
     nmb = 22 * 18
     rng = np.random.default_rng(9)
     centers = rng.integers(-64, 65, (nmb, 2)).astype(np.int32)
@@ -371,7 +374,7 @@ def test_fullpel_grid_matches_oracle(acc, cif):
     tab = O.mv_cost_table()
     lam = 6.5
     n = 2 * R + 1
-    checked = range(0, nmb, 7)
+    checked = list(range(0, nmb, stride)) + [nmb - 1]
     oracle_grids = {}
     for m in checked:
         mbx, mby = m % 22, m // 22
