@@ -161,7 +161,11 @@ H264A_API int h264a_me_search(h264a_ctx *ctx, const h264a_picture *d_pics, int n
  * different frames interleave); each MB waits (bounded) for its left and
  * top-right neighbours.  Picks: 6 i32 per MB {shape 0/1/2, mv0x, mv0y, mv1x,
  * mv1y, work} where work counts the 4x4-block distortion evaluations the
- * reference performs for the MB; costs: 2 i64 per MB {pick J, 16x16 J}. */
+ * reference performs for the MB; costs: 2 i64 per MB {pick J, 16x16 J}.
+ * Up to 96 frames the launch carries the frame table in its parameters; a
+ * call of more frames uploads it through a staging buffer of the context and
+ * waits for that buffer's previous upload, so such calls do not belong in a
+ * stream capture (h264a_me_frames_noalloc is the capturable form). */
 typedef struct {
     h264a_picture pic;
     double lambda_me;
