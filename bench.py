@@ -531,7 +531,7 @@ def run_ours(args, ws, rank, local):
         "peak_source": "measured live by h264a_measure_int32_peak (INT32 is not in MEASURED_PEAKS.json)",
         # dram__bytes_read.sum + dram__bytes_write.sum of one launch (ncu --set full of the
         # 60-frame step: 481,440 MBs, 1374.5 MB + 42.6 MB), scaled by MBs to this launch
-        "traffic": int(1417.1e6 / 481440 * (n - 1) * nmb),
+        "traffic": int(1415.2e6 / 481440 * (n - 1) * nmb),
         "traffic_source": "ncu capture of the 60-frame 1080p launch, scaled by macroblocks",
         "work": {"satd_4x4_evals_per_step": work4x4, "ops_per_4x4": SATD_OPS_PER_4X4},
         "critical_path": {"me_ms_all_frames": round(stage["me"], 3), "frames": n - 1,
