@@ -607,3 +607,49 @@ def test_deblock_single_mb_edge_matches_line_filter():
         want[0:8, c] = np_luma_line(want[0:8, c], 2, a[qp], b[qp], t[qp][1])
     assert np.array_equal(got.astype(np.int32), want)
 
+
+def _lcg32_bytes(seed: int, n: int) -> np.ndarray:
+    """n draws (s >> 24) of the LCG s <- s*1664525 + 1013904223 mod 2^32,
+    computed 4096 at a time from the jump-ahead multipliers (same stream as
+    stepping Lcg32 n times)."""
+    a, c, blk = 1664525, 1013904223, 4096
+    mul = np.empty(blk, np.uint64)
+    add = np.empty(blk, np.uint64)
+    m, k = 1, 0
+    for i in range(blk):  # state_{i+1} = mul[i] * state_0 + add[i]
+        m, k = (m * a) & 0xFFFFFFFF, (k * a + c) & 0xFFFFFFFF
+        mul[i], add[i] = m, k
+    out = np.empty(n, np.uint8)
+    st = seed & 0xFFFFFFFF
+    for o in range(0, n, blk):
+        v = (mul * np.uint64(st) + add) & np.uint64(0xFFFFFFFF)
+        take = min(blk, n - o)
+        out[o:o + take] = (v[:take] >> np.uint64(24)).astype(np.uint8)
+        st = int(v[-1])
+    return out
+
+
+def test_lcg32_jump_ahead_matches_stepping():
+    st = Lcg32(0xDEAD_BEEF)
+    want = np.array([st.next() >> 24 for _ in range(5000)], np.uint8)
+    assert np.array_equal(_lcg32_bytes(0xDEAD_BEEF, 5000), want)
+
+
+def test_coded_plane_extension_matches_per_pixel():
+    """mb16.rs:1552-1584 (clamp_plane_matches_per_pixel_oracle, its LCG
+    0xDEAD_BEEF stream and seven geometries): the coded-size edge extension the
+    tests and the benchmark apply to every frame (rusty_h264_b200.synth.
+    coded_luma, restating clamp_plane mb16.rs:1523) equals the per-pixel
+    definition out[y][x] = plane[min(y, h-1)][min(x, w-1)]."""
+    from rusty_h264_b200 import synth
+
+    cases = [(1920, 1080, 1920, 1088), (960, 540, 960, 544), (352, 288, 352, 288), (100, 100, 112, 112),
+             (37, 5, 48, 16), (16, 1, 16, 16), (1, 1, 16, 16)]
+    stream = _lcg32_bytes(0xDEAD_BEEF, sum(w * h for w, h, _, _ in cases))
+    o = 0
+    for w, h, ow, oh in cases:
+        plane = stream[o:o + w * h].reshape(h, w)
+        o += w * h
+        got = synth.coded_luma(plane)
+        want = plane[np.minimum(np.arange(oh), h - 1)[:, None], np.minimum(np.arange(ow), w - 1)[None, :]]
+        assert got.shape == (oh, ow) and np.array_equal(got, want), (w, h, ow, oh)
