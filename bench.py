@@ -410,8 +410,8 @@ def run_ours(args, ws, rank, local):
         else:
             stream.wait_stream(side)
 
-    # hpel_build, me_frames and mc_tq_frames per 96 frames, downsample2x, la_intra, la_chains
-    kernels_per_step = 1 + 2 * ((n - 1 + 95) // 96) + 1 + 2
+    # hpel_build, one me_frames launch, mc_tq_frames per 96 frames, downsample2x, la_intra, la_chains
+    kernels_per_step = 1 + 1 + (n - 1 + 95) // 96 + 1 + 2
 
     def barrier():
         if ws > 1:
