@@ -183,22 +183,66 @@ def mixed_batch(acc, torch, streams, params, lam: float, gate: int):
 
 
 class ClockSampler:
-    """nvidia-smi clock/throttle sampling during the timed region."""
+    """SM clock and clock-event (throttle) reasons sampled during the timed
+    region: NVML polled every 5 ms from a thread (reads only), or nvidia-smi
+    at 100 ms where NVML cannot be loaded.  The device is found by its PCI bus
+    id, so a remapped CUDA_VISIBLE_DEVICES still samples the right GPU."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clock-event reason bits
+    REASONS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40}
 
     def __init__(self, device: int):
         self.device = device
         self.proc = None
         self.lines = []
+        self.nv = None
+        self.samples = []
+        self.busid = None
+        try:
+            import torch
+
+            pr = torch.cuda.get_device_properties(device)
+            self.busid = f"{pr.pci_domain_id:08X}:{pr.pci_bus_id:02X}:{pr.pci_device_id:02X}.0"
+        except Exception:
+            pass
+
+    def _nvml_sample(self):
+        nv, h = self.nv
+        get_reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            nv.nvmlDeviceGetCurrentClocksThrottleReasons
+        return (nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM), nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM),
+                int(get_reasons(h)))
+
+    def _poll(self):
+        while not self.done.is_set():
+            try:
+                self.samples.append(self._nvml_sample())
+            except Exception:
+                pass
+            self.done.wait(0.005)
 
     def start(self):
         try:
+            import pynvml as nv
+
+            nv.nvmlInit()
+            h = nv.nvmlDeviceGetHandleByPciBusId(self.busid) if self.busid else nv.nvmlDeviceGetHandleByIndex(self.device)
+            self.nv = (nv, h)
+            self._nvml_sample()
+            self.done = threading.Event()
+            self.t = threading.Thread(target=self._poll, daemon=True)
+            self.t.start()
+            return
+        except Exception:
+            self.nv = None
+        try:
             self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                ["nvidia-smi", "-i", self.busid or str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
         except OSError:
@@ -209,6 +253,19 @@ class ClockSampler:
             self.lines.append(ln.strip())
 
     def stop(self):
+        if self.nv is not None:
+            self.done.set()
+            self.t.join(timeout=5)
+            if not self.samples:
+                try:
+                    self.samples.append(self._nvml_sample())
+                except Exception:
+                    pass
+            sm = [x[0] for x in self.samples]
+            reasons = {nm for nm, bit in self.REASONS.items() if any(x[2] & bit for x in self.samples)}
+            return {"sm_mhz": float(np.median(sm)) if sm else None,
+                    "sm_max_mhz": max(x[1] for x in self.samples) if self.samples else None,
+                    "reasons": sorted(reasons), "samples": len(sm), "source": "nvml, 5 ms"}
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -231,7 +288,7 @@ class ClockSampler:
                 if v.lower().startswith("active"):
                     reasons.add(nm)
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "source": "nvidia-smi, 100 ms"}
 
 
 def cpu_baseline(frames: np.ndarray, nthreads: int, lam: float, gate: int):
