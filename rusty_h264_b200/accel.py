@@ -205,8 +205,9 @@ class Accel:
 
     def close(self):
         if getattr(self, "ctx", None):
-            self.L.h264a_ctx_destroy(self.ctx)
+            self.L.h264a_ctx_destroy(self.ctx)  # waits for pending prefetch uploads
             self.ctx = None
+            self._prefetched = []
 
     def __del__(self):
         try:
