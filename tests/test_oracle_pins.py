@@ -653,3 +653,126 @@ def test_coded_plane_extension_matches_per_pixel():
         got = synth.coded_luma(plane)
         want = plane[np.minimum(np.arange(oh), h - 1)[:, None], np.minimum(np.arange(ow), w - 1)[None, :]]
         assert got.shape == (oh, ow) and np.array_equal(got, want), (w, h, ow, oh)
+
+
+# ---------------------------------------------------------------------------
+# mb-tree lookahead (mbtree.rs:61-263), restated independently of the C oracle
+# ---------------------------------------------------------------------------
+
+def np_downsample2x(y):
+    """downsample2x (mbtree.rs:61-74): (sum of each 2x2 + 2) / 4."""
+    s = y[0::2, 0::2].astype(np.int64) + y[0::2, 1::2] + y[1::2, 0::2] + y[1::2, 1::2]
+    return ((s + 2) // 4).astype(np.uint8)
+
+
+def np_intra_cost(pic, bx0, by0, bs):
+    """intra_cost (mbtree.rs:78-93): the 4x4 Hadamard magnitudes of the block
+    without each DC term (the block sum), at least 1."""
+    tot = 0
+    for by in range(by0, by0 + bs, 4):
+        for bx in range(bx0, bx0 + bs, 4):
+            h = H4 @ pic[by:by + 4, bx:bx + 4].astype(np.int64) @ H4.T
+            tot += int(np.abs(h).sum() - abs(h[0, 0]))
+    return max(min(tot, 2**31 - 1), 1)
+
+
+def np_mc_satd(cur, ref, bx0, by0, bs, mv):
+    """mc_satd (mbtree.rs:102-147): SATD of the block against the reference at
+    a quarter-pel MV, every read clamped (the in-place and mc_luma arms agree)."""
+    pred = np_luma_sample_block(ref, bx0, by0, bs, bs, mv[0], mv[1])
+    return np_satd_sum(cur[by0:by0 + bs, bx0:bx0 + bs], pred)
+
+
+def np_inter_cost(cur, ref, bx0, by0, bs, seed, max_step):
+    """inter_cost (mbtree.rs:154-197): (0,0), the seed when nonzero, then the
+    four-point diamond (+x, -x, +y, -y, each around the centre as it moves) at
+    steps max_step .. 1, a step repeated while it moves; 0 at (0,0) ends it."""
+    best_mv = (0, 0)
+    best = np_mc_satd(cur, ref, bx0, by0, bs, best_mv)
+    if best == 0:
+        return 0, best_mv
+    if seed != (0, 0):
+        c = np_mc_satd(cur, ref, bx0, by0, bs, seed)
+        if c < best:
+            best, best_mv = c, seed
+    step = max_step
+    while step >= 1:
+        while True:
+            moved = False
+            for dx, dy in ((step, 0), (-step, 0), (0, step), (0, -step)):
+                mv = (best_mv[0] + dx * 4, best_mv[1] + dy * 4)
+                c = np_mc_satd(cur, ref, bx0, by0, bs, mv)
+                if c < best:
+                    best, best_mv, moved = c, mv, True
+            if not moved:
+                break
+        step >>= 1
+    return min(best, 2**31 - 1), best_mv
+
+
+def np_lookahead_clip(frames, mode):
+    """frame_costs (mbtree.rs:208-263) of every frame against the previous one
+    (frame 0 intra only): raster order, seed = left MV, else top MV; HalfRes
+    searches and scores at half resolution, Hybrid refines at full resolution
+    from the half-res MV.  Halving the seed truncates toward zero, as Rust's /."""
+    n, ch, cw = frames.shape
+    mb_w, mb_h = cw // 16, ch // 16
+    half = np.stack([np_downsample2x(f) for f in frames])
+    halve = lambda v: int(v / 2)
+    intra = np.zeros((n, mb_w * mb_h), np.int32)
+    inter = np.zeros_like(intra)
+    mvs = np.zeros((n, mb_w * mb_h, 2), np.int32)
+    for f in range(n):
+        for m in range(mb_w * mb_h):
+            mbx, mby = m % mb_w, m // mb_w
+            seed = tuple(mvs[f, m - 1]) if mbx > 0 else (tuple(mvs[f, m - mb_w]) if mby > 0 else (0, 0))
+            seed = (int(seed[0]), int(seed[1]))
+            ic = np_intra_cost(half[f], mbx * 8, mby * 8, 8) if mode == 2 else np_intra_cost(frames[f], mbx * 16, mby * 16, 16)
+            if f == 0:
+                cost, mv = ic, (0, 0)
+            elif mode == 0:
+                c, mv = np_inter_cost(frames[f], frames[f - 1], mbx * 16, mby * 16, 16, seed, 8)
+                cost = min(c, ic)
+            elif mode == 2:
+                c, mvp = np_inter_cost(half[f], half[f - 1], mbx * 8, mby * 8, 8, (halve(seed[0]), halve(seed[1])), 8)
+                cost, mv = min(c, ic), (mvp[0] * 2, mvp[1] * 2)
+            else:
+                _, mvp = np_inter_cost(half[f], half[f - 1], mbx * 8, mby * 8, 8, (halve(seed[0]), halve(seed[1])), 8)
+                c, mv = np_inter_cost(frames[f], frames[f - 1], mbx * 16, mby * 16, 16, (mvp[0] * 2, mvp[1] * 2), 2)
+                cost = min(c, ic)
+            intra[f, m], inter[f, m], mvs[f, m] = ic, cost, mv
+    return intra, inter, mvs
+
+
+def _panning_clip(n, cw, ch, pan, seed):
+    rng = np.random.default_rng(seed)
+    H, W = ch + abs(pan[1]) * n + 16, cw + abs(pan[0]) * n + 16
+    tex = rng.random((H, W))
+    for _ in range(3):
+        tex = (tex + np.roll(tex, 1, 0) + np.roll(tex, 1, 1) + np.roll(tex, (1, 1), (0, 1))) / 4
+    tex = (255 * (tex - tex.min()) / (tex.max() - tex.min())).astype(np.uint8)
+    oy, ox = abs(pan[1]) * n // 2 + 8, abs(pan[0]) * n // 2 + 8
+    return np.ascontiguousarray(np.stack([tex[oy + k * pan[1]:oy + k * pan[1] + ch, ox + k * pan[0]:ox + k * pan[0] + cw]
+                                          for k in range(n)]))
+
+
+def test_downsample2x_matches_numpy():
+    rng = np.random.default_rng(1)
+    for cw, ch in ((32, 16), (96, 48), (352, 288)):
+        y = rng.integers(0, 256, (ch, cw)).astype(np.uint8)
+        assert np.array_equal(O.downsample2x(y), np_downsample2x(y))
+
+
+@pytest.mark.parametrize("mode", [2, 1, 0])
+def test_lookahead_oracle_matches_numpy_restatement(mode):
+    """The C oracle's frame_costs against the independent numpy/Python
+    restatement above, on a synthetic clip (moving boxes over noise) and a
+    panning texture that moves the diamond several steps, in all three modes."""
+    from rusty_h264_b200 import synth
+
+    y, _, _ = synth.cif_clip(3, 11, 96, 64)
+    for clip in (synth.coded_luma(y), _panning_clip(3, 96, 64, (7, -3), 5)):
+        got = O.lookahead_clip(clip, mode)
+        want = np_lookahead_clip(clip, mode)
+        for g, w, name in zip(got, want, ("intra", "inter", "mvs")):
+            assert np.array_equal(g, w), (mode, name)
