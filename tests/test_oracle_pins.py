@@ -776,3 +776,151 @@ def test_lookahead_oracle_matches_numpy_restatement(mode):
         want = np_lookahead_clip(clip, mode)
         for g, w, name in zip(got, want, ("intra", "inter", "mvs")):
             assert np.array_equal(g, w), (mode, name)
+
+
+# ---------------------------------------------------------------------------
+# plain-ME of a frame (motion_search + best_part + the split decision), Balanced
+# preset, restated independently of the C oracle from mb16.rs / inter.rs
+# ---------------------------------------------------------------------------
+
+def np_mvbits(d):
+    """mvbits kind 0 (mb16.rs:2454-2482): the se(v) Exp-Golomb length of d."""
+    code = 2 * d - 1 if d > 0 else -2 * d
+    return 1 + 2 * ((code + 1).bit_length() - 1)
+
+
+def np_motion_search(src, ref, lx, ly, rw, rh, preds, lam):
+    """motion_search (mb16.rs:2433-3302) under the Balanced preset: seeds (0,0)
+    then the predictors, the centre snapped to full-pel, the ladder of 4-point
+    diamonds at 16, 8, 4 quarter-pel (fixed-centre argmin where the +-step box
+    is inside the picture, first-improvement cascade otherwise, a rung walked
+    while it moves), one pass of the 8-point half-pel then quarter-pel rings
+    (each point around the centre as it moves), and the pre-snap seed kept if
+    cheaper.  Distortion: the exact 4x4 Hadamard SATD against the clamped
+    luma_sample prediction; rate: (lambda * bits) truncated."""
+    ch, cw = src.shape
+    center = preds[0]
+    memo = {}
+
+    def cost(mv):
+        if mv not in memo:
+            pred = np_luma_sample_block(ref, lx, ly, rw, rh, mv[0], mv[1])
+            rate = np_mvbits(mv[0] - center[0]) + np_mvbits(mv[1] - center[1])
+            memo[mv] = np_satd_sum(src[ly:ly + rh, lx:lx + rw], pred) + int(lam * rate)
+        return memo[mv]
+
+    best, best_c = (0, 0), cost((0, 0))
+    for p in preds:
+        if cost(p) < best_c:
+            best, best_c = p, cost(p)
+    seed_mv, seed_c = best, best_c
+    if best[0] & 3 or best[1] & 3:
+        best = (((best[0] + 2) // 4) * 4, ((best[1] + 2) // 4) * 4)
+        best_c = cost(best)
+    for step in (16, 8, 4):
+        ring = ((step, 0), (-step, 0), (0, step), (0, -step))
+        while True:
+            s = step >> 2
+            bx, by = lx + (best[0] >> 2), ly + (best[1] >> 2)
+            if (best[0] & 3) == 0 and (best[1] & 3) == 0 and bx - s >= 0 and by - s >= 0 and \
+                    bx + s + rw <= cw and by + s + rh <= ch:
+                bi, bc = None, best_c
+                for d in ring:
+                    c = cost((best[0] + d[0], best[1] + d[1]))
+                    if c < bc:
+                        bi, bc = d, c
+                if bi is None:
+                    break
+                best, best_c = (best[0] + bi[0], best[1] + bi[1]), bc
+                continue
+            moved = False
+            for d in ring:
+                mv = (best[0] + d[0], best[1] + d[1])
+                if cost(mv) < best_c:
+                    best, best_c, moved = mv, cost(mv), True
+            if not moved:
+                break
+    for step in (2, 1):
+        for d in ((step, 0), (-step, 0), (0, step), (0, -step), (step, step), (-step, -step), (step, -step),
+                  (-step, step)):
+            mv = (best[0] + d[0], best[1] + d[1])
+            if cost(mv) < best_c:
+                best, best_c = mv, cost(mv)
+    if seed_c < best_c:
+        best, best_c = seed_mv, seed_c
+    return best, best_c
+
+
+def np_predict_mv(a, b, c):
+    """predict_mv (inter.rs:36-69) for ref 0 with neighbours None (unavailable)
+    or their MVs (every coded neighbour refers to ref 0)."""
+    (mva, ra), (mvb, rb), (mvc, rc) = ((n, 0) if n is not None else ((0, 0), -1) for n in (a, b, c))
+    if b is None and c is None and a is not None:
+        mvb, rb, mvc, rc = mva, ra, mva, ra
+    if (ra == 0) + (rb == 0) + (rc == 0) == 1:
+        return mva if ra == 0 else (mvb if rb == 0 else mvc)
+    med = lambda x, y, z: sorted((x, y, z))[1]
+    return (med(mva[0], mvb[0], mvc[0]), med(mva[1], mvb[1], mvc[1]))
+
+
+def np_me_frame(src, ref, lam, gate):
+    """The plain-ME frame model: every MB in raster order coded inter with ref
+    0; the neighbours of its top-left 4x4 block (mv_neighbors_block,
+    mb16.rs:1871: left, top, top-right else top-left) give predict_mv;
+    best_part 16x16 seeded [pmv], and when its J exceeds the gate the 16x8 and
+    8x16 halves seeded [pmv, mv16], the shape taken on strictly lower summed J
+    (mb16.rs:8869-8913)."""
+    ch, cw = src.shape
+    mb_w, mb_h = cw // 16, ch // 16
+    picks = np.zeros((mb_w * mb_h, 6), np.int32)
+    costs = np.zeros((mb_w * mb_h, 2), np.int64)
+    blk = {}  # (bx4, by4) -> MV of coded 4x4 blocks
+
+    def get(bx, by):
+        return blk.get((bx, by)) if 0 <= bx < mb_w * 4 and 0 <= by < mb_h * 4 else None
+
+    for m in range(mb_w * mb_h):
+        mbx, mby = m % mb_w, m // mb_w
+        lx, ly, bx, by = mbx * 16, mby * 16, mbx * 4, mby * 4
+        c = get(bx + 4, by - 1)
+        pmv = np_predict_mv(get(bx - 1, by), get(bx, by - 1), c if c is not None else get(bx - 1, by - 1))
+        mv16, c16 = np_motion_search(src, ref, lx, ly, 16, 16, [pmv], lam)
+        shape, mv0, mv1, best = 0, mv16, mv16, c16
+        if gate >= 0 and c16 > gate:
+            seeds = [pmv, mv16]
+            (mt, ct), (mb_, cb) = (np_motion_search(src, ref, lx, ly + o, 16, 8, seeds, lam) for o in (0, 8))
+            (ml, cl), (mr, cr) = (np_motion_search(src, ref, lx + o, ly, 8, 16, seeds, lam) for o in (0, 8))
+            if ct + cb < best:
+                shape, mv0, mv1, best = 1, mt, mb_, ct + cb
+            if cl + cr < best:
+                shape, mv0, mv1, best = 2, ml, mr, cl + cr
+        picks[m, :5] = (shape, mv0[0], mv0[1], mv1[0], mv1[1])
+        costs[m] = (best, c16)
+        for j in range(4):
+            for i in range(4):
+                part = (j >= 2) if shape == 1 else ((i >= 2) if shape == 2 else 0)
+                blk[(bx + i, by + j)] = mv1 if part else mv0
+    return picks, costs
+
+
+@pytest.mark.parametrize("gate_on", [False, True])
+def test_me_frame_oracle_matches_numpy_restatement(gate_on):
+    """The C oracle's plain-ME frame (or_me_frame_plain) against the
+    independent restatement above, Balanced preset, on a 96x64 crop of the
+    CIF clip and on a panning texture, with and without the partition split."""
+    from rusty_h264_b200 import synth
+    from rusty_h264_b200 import accel as A
+
+    qp = 27
+    lam = float(np.sqrt(A.frame_lambda(qp)) * 1.25)
+    qstep16 = (10, 11, 13, 14, 16, 18)[qp % 6] << (qp // 6)
+    gate = ((30 * (qstep16 + 160)) >> 3) * 2 if gate_on else -1
+    assert not gate_on or gate == A.split_gate_for_qp(qp)
+    y, _, _ = synth.cif_clip(3, 7)
+    crop = np.ascontiguousarray(synth.coded_luma(y)[:, 96:160, 128:224])
+    for frames in (crop, _panning_clip(2, 96, 64, (5, -3), 9)):
+        src, ref = frames[1], frames[0]
+        wp, wc = O.me_frame(src, ref, O.build_planes4(ref, 32), O.balanced_params(), lam, gate)
+        gp, gc = np_me_frame(src, ref, lam, gate)
+        assert np.array_equal(wp[:, :5], gp[:, :5]), np.argwhere(wp[:, :5] != gp[:, :5])[:4]
+        assert np.array_equal(wc, gc)
