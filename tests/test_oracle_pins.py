@@ -924,3 +924,68 @@ def test_me_frame_oracle_matches_numpy_restatement(gate_on):
         gp, gc = np_me_frame(src, ref, lam, gate)
         assert np.array_equal(wp[:, :5], gp[:, :5]), np.argwhere(wp[:, :5] != gp[:, :5])[:4]
         assert np.array_equal(wc, gc)
+
+
+# ---------------------------------------------------------------------------
+# MC + luma T/Q of picked MBs (mb16.rs:3436-3450), restated independently
+# ---------------------------------------------------------------------------
+
+# H.264 forward quantization multipliers per qp % 6 for the (even,even),
+# (odd,odd) and mixed positions (transform.rs QUANT_MF).
+QUANT_MF_STD = [[13107, 5243, 8066], [11916, 4660, 7490], [10082, 4194, 6554], [9362, 3647, 5825],
+                [8192, 3355, 5243], [7282, 2893, 4559]]
+
+
+def np_quant_dz_ff(qp, dz):
+    """quant_dz_ff (transform.rs:144-156): round(F / MF) per openh264 slot, with
+    F = 2^(15 + qp/6) / dz and slots in groups (0,2,0,2,2,1,2,1)."""
+    f = (1 << (15 + qp // 6)) // dz
+    return [(f + QUANT_MF_STD[qp % 6][g] // 2) // QUANT_MF_STD[qp % 6][g] for g in (0, 2, 0, 2, 2, 1, 2, 1)]
+
+
+def np_mc_tq_frame(src, ref, picks, qp, dz=6):
+    """Per MB: the prediction of each 4x4 block under its partition's MV
+    (luma_sample), the 4x4 forward core Cf.d.Cf^T of each sub-block in the
+    dct[256] order (quadrants (0,0),(8,0),(0,8),(8,8), sub-blocks
+    (0,0),(4,0),(0,4),(4,4)), then ((|c| + FF[pos]) * MF[pos]) >> 16 with the
+    sign, pos = (row & 1) * 4 + col, MF = QUANT_MF_OH[qp]."""
+    ch, cw = src.shape
+    mb_w = cw // 16
+    ff = np.array(np_quant_dz_ff(qp, dz), np.int64)
+    mf = np.array(GOLD["quant_mf_oh"]["rows"][qp], np.int64)
+    pos = np.array([((i // 4) & 1) * 4 + i % 4 for i in range(16)])
+    out = np.zeros((len(picks), 256), np.int16)
+    for m, (shape, m0x, m0y, m1x, m1y) in enumerate(picks[:, :5]):
+        lx, ly = (m % mb_w) * 16, (m // mb_w) * 16
+        pred = np.zeros((16, 16), np.int64)
+        for by in range(0, 16, 4):
+            for bx in range(0, 16, 4):
+                part = (by >= 8) if shape == 1 else ((bx >= 8) if shape == 2 else False)
+                mvx, mvy = (m1x, m1y) if part else (m0x, m0y)
+                pred[by:by + 4, bx:bx + 4] = np_luma_sample_block(ref, lx + bx, ly + by, 4, 4, int(mvx), int(mvy))
+        d = src[ly:ly + 16, lx:lx + 16].astype(np.int64) - pred
+        for qi, (qx, qy) in enumerate(((0, 0), (8, 0), (0, 8), (8, 8))):
+            for k, (ox, oy) in enumerate(((0, 0), (4, 0), (0, 4), (4, 4))):
+                c = (CF @ d[qy + oy:qy + oy + 4, qx + ox:qx + ox + 4] @ CF.T).reshape(16)
+                lvl = ((np.abs(c) + ff[pos]) * mf[pos]) >> 16
+                out[m, qi * 64 + k * 16:qi * 64 + k * 16 + 16] = np.where(c < 0, -lvl, lvl)
+    return out
+
+
+@pytest.mark.parametrize("qp", [0, 20, 27, 51])
+def test_mc_tq_oracle_matches_numpy_restatement(qp):
+    """The C oracle's MC + luma T/Q of picked MBs against the restatement above,
+    on the panning texture's plain-ME picks (16x16, 16x8 and 8x16, sub-pel MVs)
+    and on picks forced through every shape with far and fractional MVs."""
+    from rusty_h264_b200 import accel as A
+
+    frames = _panning_clip(2, 96, 64, (5, -3), 9)
+    src, ref = frames[1], frames[0]
+    lam = float(np.sqrt(A.frame_lambda(27)) * 1.25)
+    picks, _ = O.me_frame(src, ref, O.build_planes4(ref, 32), O.balanced_params(), lam, A.split_gate_for_qp(27))
+    rng = np.random.default_rng(qp)
+    forced = picks.copy()
+    forced[:, 0] = np.arange(len(forced)) % 3
+    forced[:, 1:5] = rng.integers(-160, 161, (len(forced), 4))
+    for p in (picks, forced):
+        assert np.array_equal(O.mc_tq_frame(src, ref, p, qp, 6), np_mc_tq_frame(src, ref, p, qp)), qp
