@@ -22,9 +22,10 @@ lookahead (downsample + frame costs) of all 60 frames.
   algorithmic work is 112 integer ops per 4x4 Hadamard-SATD evaluation the
   reference performs (the kernel reports the count per MB).
 * cpu_baseline: the C restatement of the reference path (oracle/) on one host
-  core over a 3-frame sample of the same clip.
+  core over an 8-frame sample of the same clip.
 
---impl reference times that CPU restatement with all host threads instead.
+--impl reference times that CPU restatement with all host threads over the
+whole 60-frame clip instead.
 With --gpus N (torchrun) every rank runs an independent replica on its own
 clip (distinct seed): replicas only, no collective on the data path.
 """
@@ -291,6 +292,13 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm), "source": "nvidia-smi, 100 ms"}
 
 
+def workload_config(frames: int, ws: int) -> dict:
+    """The `config` both arms print: the same workload, so their lines compare."""
+    return {"workload": "1080p 60-frame clip, pixel path (planes, plain-ME, MC+T/Q, HalfRes lookahead)",
+            "frames_per_step": frames, "qp": QP, "preset": "balanced", "split_partitions": True,
+            "l2": "inputs and outputs (~1 GB) exceed L2; no flush", "parallelism": f"replicas x{ws}"}
+
+
 def cpu_baseline(frames: np.ndarray, nthreads: int, lam: float, gate: int):
     """The CPU restatement of the reference path on a bounded sample."""
     from oracle import oracle as O
@@ -365,10 +373,10 @@ def run_reference(args, ws, rank):
     lam = float(np.sqrt(frame_lambda(QP)) * 1.25)
     gate = split_gate_for_qp(QP)
     f = clip(1, args.frames)
-    sample = min(args.frames, max(3, nthreads + 1))
+    sample = args.frames  # the whole clip: the same workload as the GPU arm
     frames = np.ascontiguousarray(f[:sample])
     for _ in range(args.warmup):
-        cpu_baseline(frames[:3], nthreads, lam, gate)
+        cpu_baseline(frames, nthreads, lam, gate)
     times = []
     for _ in range(args.steps):
         _, dt = cpu_baseline(frames, nthreads, lam, gate)
@@ -379,10 +387,9 @@ def run_reference(args, ws, rank):
         "metric": METRIC, "value": round(value, 3), "unit": "Mpx/s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u8/i32", "data": "synthetic (seeded 1080p generator)", "impl": "reference",
-        "config": {"workload": "1080p 60-frame clip, pixel path (planes, plain-ME, MC+T/Q, HalfRes lookahead)",
-                   "sample_frames_per_step": sample, "qp": QP},
+        "config": workload_config(sample, ws),
         "cpu_baseline": {"value": round(value, 3), "unit": "Mpx/s", "cores": nthreads, "kind": "port",
-                         "sample": f"{sample} frames of the 1080p clip per step, frames split over the threads",
+                         "sample": f"all {sample} frames of the 1080p clip per step, frames split over the threads",
                          "cpu": cpu_model()},
         "e2e": {"value": round(value, 3), "unit": "Mpx/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -604,9 +611,7 @@ def run_ours(args, ws, rank, local):
         "metric": METRIC, "value": round(value, 2), "unit": "Mpx/s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u8/i32", "data": "synthetic (seeded 1080p generator, per-rank seed)",
-        "config": {"workload": "1080p 60-frame clip, pixel path (planes, plain-ME, MC+T/Q, HalfRes lookahead)",
-                   "frames_per_step": n, "qp": qp, "preset": "balanced", "split_partitions": True,
-                   "l2": "inputs and outputs (~1 GB) exceed L2; no flush", "parallelism": f"replicas x{ws}"},
+        "config": workload_config(n, ws),
         "stage_ms": {k: round(v, 4) for k, v in stage.items()},
         "reconstruction_ms": dict(extra_ms, note="timed separately over the same 59 P frames, not part of value"),
         "roofline": roofline,
@@ -658,10 +663,10 @@ def run_ours(args, ws, rank, local):
                      ("la_mvs", la_mvs)):
             assert np.array_equal(outs_np[k], t.cpu().numpy()), k
     if rank == 0 and ws == 1 and not args.no_cpu:
-        sample = np.ascontiguousarray(f[:3])
+        sample = np.ascontiguousarray(f[:8])
         v, dt = cpu_baseline(sample, 1, lam, gate)
         line["cpu_baseline"] = {"value": round(v, 3), "unit": "Mpx/s", "cores": 1, "kind": "port",
-                                "sample": "3 frames of the 1080p clip (2 P frames + lookahead), one thread",
+                                "sample": "8 frames of the 1080p clip (7 P frames + lookahead), one thread",
                                 "cpu": cpu_model(), "stages": cpu_stages(sample, lam, gate)}
     if args.mixed and rank == 0:
         line["mixed_batch"] = mixed_batch(acc, torch, mixed_streams, params, lam, gate)

@@ -165,7 +165,7 @@ H264A_API int h264a_me_search(h264a_ctx *ctx, const h264a_picture *d_pics, int n
  * Up to 96 frames the launch carries the frame table in its parameters; a
  * call of more frames uploads it through a staging buffer of the context and
  * waits for that buffer's previous upload, so such calls do not belong in a
- * stream capture (h264a_me_frames_noalloc is the capturable form). */
+ * stream capture. */
 typedef struct {
     h264a_picture pic;
     double lambda_me;
@@ -203,11 +203,15 @@ H264A_API int h264a_me_tq_frames(h264a_ctx *ctx, const h264a_me_tq_frame *h_fram
  * covers at most H264A_NOALLOC_MAX_MBS macroblocks (sum over its frames) and at
  * most 96 frames; larger requests return H264A_E_ARG.  The array is set up
  * (its device address looked up) on the first call on each device, so make
- * that first call before any stream capture.  Every call on a device shares
- * the array: calls that overlap on the GPU race and must not be issued on
- * concurrent streams.  The caller passes a device int32 d_status, which the
- * call zeroes and the kernel sets to non-zero if a bounded wait ran out; read
- * it after synchronising `stream`.  Outputs as h264a_me_frames. */
+ * that first call before any stream capture; the address is kept for the
+ * process, so do not call this entry point again on a device whose primary
+ * context was reset (cudaDeviceReset).  Every call on a device shares the
+ * array and clears the part it uses (queue counter and its macroblocks'
+ * flags) on `stream` before its launch: calls that overlap on the GPU race
+ * and must not be issued on concurrent streams.  The caller passes a device
+ * int32 d_status, which the call zeroes and the kernel sets to non-zero if a
+ * bounded wait ran out; read it after synchronising `stream`.  Outputs as
+ * h264a_me_frames. */
 #define H264A_NOALLOC_MAX_MBS 65536
 H264A_API int h264a_me_frames_noalloc(const h264a_me_frame *h_frames, int nframes, const h264a_me_params *params,
                                       int32_t *d_status, void *stream);

@@ -1575,11 +1575,15 @@ namespace h264a {
 // [0] work-queue counter, [1..] per-MB done flags.
 static __device__ __align__(256) int g_noalloc_scratch[1 + H264A_NOALLOC_MAX_MBS];
 
+// The device address of g_noalloc_scratch on each device (nullptr: not yet
+// looked up).  It is looked up once per device and kept; a caller that resets
+// a device's primary context (cudaDeviceReset) must not call this entry point
+// on that device again in the same process.
 struct NoallocDevice {
-    int* scratch;  // device address of g_noalloc_scratch on this device (nullptr: not set up)
-    int epoch;     // flag value of the latest launch on this device
+    int* scratch;
 };
 constexpr int kNoallocMaxDevices = 64;
+constexpr int kNoallocFlag = 1;  // the value a published MB's flag takes
 static NoallocDevice g_noalloc_dev[kNoallocMaxDevices];
 static std::mutex g_noalloc_mu;
 
@@ -1609,7 +1613,6 @@ extern "C" int h264a_me_frames_noalloc(const h264a_me_frame* h_frames, int nfram
     if (dev < 0 || dev >= kNoallocMaxDevices) return fail(H264A_E_ARG, "me_frames_noalloc: device index too large");
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     int* scratch;
-    int epoch;
     {
         std::lock_guard<std::mutex> lock(g_noalloc_mu);
         NoallocDevice& nd = g_noalloc_dev[dev];
@@ -1619,13 +1622,7 @@ extern "C" int h264a_me_frames_noalloc(const h264a_me_frame* h_frames, int nfram
             void* p = nullptr;
             H264A_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
             nd.scratch = static_cast<int*>(p);
-            nd.epoch = 0;
         }
-        if (nd.epoch >= 0x7ffffff0) {  // flags from older launches must never equal the new value
-            H264A_CUDA(cudaMemsetAsync(nd.scratch + 1, 0, sizeof(int) * H264A_NOALLOC_MAX_MBS, st));
-            nd.epoch = 0;
-        }
-        epoch = ++nd.epoch;
         scratch = nd.scratch;
     }
     // frames largest first, dealt round-robin in wavefront order (as h264a_me_frames)
@@ -1660,9 +1657,11 @@ extern "C" int h264a_me_frames_noalloc(const h264a_me_frame* h_frames, int nfram
         total += (long long)d.mb_w * d.mb_h;
     }
     fill_segments(fb);
-    // the counter and the caller's status word must start at zero; the flags
-    // need no clearing because every launch waits for its own epoch value
-    H264A_CUDA(cudaMemsetAsync(scratch, 0, sizeof(int), st));
+    // The counter, this call's flags and the caller's status word start at
+    // zero: they are cleared on the stream ahead of the launch (at most
+    // 256 KiB), and each MB's flag is set to 1 when its pick is published.
+    // Nothing of an earlier call's array contents is read.
+    H264A_CUDA(cudaMemsetAsync(scratch, 0, sizeof(int) * size_t(1 + total), st));
     H264A_CUDA(cudaMemsetAsync(d_status, 0, sizeof(int32_t), st));
     int per_sm = 0, sms = 0;
     const int rc0 = me_frames_setup(per_sm);
@@ -1672,6 +1671,6 @@ extern "C" int h264a_me_frames_noalloc(const h264a_me_frame* h_frames, int nfram
     const long long need = (total + ME_WARPS - 1) / ME_WARPS;
     if (blocks > need) blocks = need;
     const MeParamsDev prm = to_dev(*params);
-    launch_me_frames(prm, unsigned(blocks), st, fb, total, scratch, scratch + 1, epoch, d_status);
+    launch_me_frames(prm, unsigned(blocks), st, fb, total, scratch, scratch + 1, kNoallocFlag, d_status);
     return check_launch("me_frames_kernel (no-alloc)");
 }

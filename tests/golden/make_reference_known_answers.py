@@ -102,4 +102,6 @@ def main(ref_root: str):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_reference_known_answers.py <path to the rusty_h264 checkout>")
+    main(sys.argv[1])

@@ -916,6 +916,49 @@ def test_pixel_path_host_1080p_matches_oracle(acc):
     assert (got["la_inter"] <= got["la_intra"]).all() and (got["la_intra"] >= 1).all()
 
 
+def test_bench_workload_matches_oracle(acc):
+    """The benchmarked workload itself: the seed-1 1080p clip of 60 frames, QP
+    27, lme = sqrt(lambda)*1.25, partitions on, Balanced preset, through
+    h264a_pixel_path_host as bench.py's e2e leg runs it.  In this frame model
+    P frame f depends only on source frames f and f-1, so the oracle run on
+    the pair (f-1, f) is an exact check of frame f: P frames 1, 2, 30, 58 and
+    59 are checked that way, and the lookahead of all 60 frames in full."""
+    y, _, _ = synth.hd_clip(60, 1)
+    frames = synth.coded_luma(y)
+    params = A.default_me_params()
+    qp = 27
+    lam = float(np.sqrt(A.frame_lambda(qp)) * 1.25)
+    gate = A.split_gate_for_qp(qp)
+    got = acc.pixel_path_host(frames, params, lam, gate, qp)
+    for f in (1, 2, 30, 58, 59):
+        want = O.pixel_path_clip(np.ascontiguousarray(frames[f - 1:f + 1]), O.balanced_params(), lam, gate, qp,
+                                 nthreads=8)
+        assert np.array_equal(got["picks"][f][:, :5], want["picks"][1][:, :5]), f
+        assert np.array_equal(got["costs"][f], want["costs"][1]), f
+        assert np.array_equal(got["coeffs"][f], want["coeffs"][1]), f
+    intra, inter, mvs = O.lookahead_clip(frames, mode=2, nthreads=8)
+    assert np.array_equal(got["la_intra"], intra)
+    assert np.array_equal(got["la_inter"], inter)
+    assert np.array_equal(got["la_mvs"], mvs)
+    # the partition searches ran on this clip (the gate opens for many MBs)
+    assert (got["picks"][1:, :, 0] > 0).mean() > 0.05
+
+
+def test_cif_workload_whole_path_matches_oracle(acc):
+    """The CPU-runnable workload verbatim: the CIF clip (gradient + moving
+    noise box) of 30 frames at QP 26 through the whole path, every frame
+    against the oracle."""
+    y, _, _ = synth.cif_clip(30, 0)
+    frames = synth.coded_luma(y)
+    params = A.default_me_params()
+    qp = 26
+    lam = float(np.sqrt(A.frame_lambda(qp)))
+    gate = A.split_gate_for_qp(qp)
+    got = acc.pixel_path_host(frames, params, lam, gate, qp)
+    want = O.pixel_path_clip(frames, O.balanced_params(), lam, gate, qp, nthreads=8)
+    compare_pixel_path(got, want)
+
+
 # ---------------------------------------------------------------------------
 # Failure handling
 # ---------------------------------------------------------------------------

@@ -5,10 +5,16 @@ budget).  Through the C ABI it must give exactly what h264a_me_frames gives
 (integer work: zero tolerance), on two calls in a row sharing its fixed
 scratch array, and refuse a request larger than that array.
 
-This file is collected last on purpose: it runs alone in a fresh process as
-well as after the rest of the suite.
+This file is collected last, so a run that stops at the first failure has run
+every other test before it.  The comparison runs here, after the rest of the
+suite in the same process, and once more in a fresh Python process of its own
+(test_noalloc_in_a_fresh_process), where the entry point's first call on the
+device is the one that looks up its scratch array.
 """
 import ctypes as C
+import os
+import subprocess
+import sys
 
 import numpy as np
 import pytest
@@ -90,3 +96,15 @@ def test_noalloc_rejects_requests_beyond_its_scratch(acc):
     rc = call_noalloc(acc, frames, A.default_me_params(), status)
     assert rc == -1
     assert b"exceed" in acc.L.h264a_last_error()
+
+
+def test_noalloc_in_a_fresh_process():
+    """The two-call comparison again, alone in a new interpreter: there the
+    no-alloc entry's set-up (the per-device address lookup) runs on a device
+    that nothing else in the process has touched through it before."""
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    node = os.path.abspath(__file__) + "::test_noalloc_matches_me_frames_on_two_consecutive_calls"
+    r = subprocess.run([sys.executable, "-m", "pytest", "-q", "-x", "-m", "gpu", "-p", "no:cacheprovider", node],
+                       cwd=root, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-3000:]
+    assert "2 passed" in r.stdout, r.stdout[-3000:]
