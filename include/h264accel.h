@@ -334,6 +334,89 @@ H264A_API int h264a_pixel_path_host(h264a_ctx *ctx, const uint8_t *h_frames, int
  * uploads them itself. */
 H264A_API int h264a_pixel_path_prefetch(h264a_ctx *ctx, const uint8_t *h_frames, int n, int cw, int ch);
 
+/* ---- learned motion-vector proposals ----------------------------------------- */
+/* A small conv net that proposes the 8 most likely full-pel MVs of every
+ * 16x16 MB of a frame; h264a_me_frames_learned then prices them with the
+ * search's exact integer cost and refines the best with motion_search's
+ * sub-pel refinement.  No counterpart in the reference, which runs
+ * motion_search (mb16.rs:2433) on every MB.
+ *   Input per frame pair (current frame, reference frame): a 2-channel image
+ * (reference, current) as (u8 - 128) / 64.  Trunk over the whole image: three
+ * 3x3 stride-2 convs (2->16->32->32 channels, zero padding at the frame
+ * edges), a map of 32 features per 8x8 pixels.  Per MB: the 6x6 cells of its
+ * co-located 48x48 region (zero outside the map) and the MVs of three
+ * neighbour MBs (left, top, top-right) -> FC 1168->256 -> head 256->296
+ * logits, of which the first 289 are the full-pel offsets (dx, dy) in
+ * [-8, 8]^2, class (dy+8)*17 + dx+8.  bf16 weights and activations, fp32
+ * accumulation on the tensor cores; trained with Adam on softmax
+ * cross-entropy against the plain search's 16x16 MVs.
+ *   A batch is npairs frame pairs of one geometry (cw x ch, at most
+ * H264A_MVNET_MAX_PIXELS pixels in all) and its samples are every MB of
+ * them, pair-major, raster order within a pair: d_nmv holds 6 i16 per MB
+ * (the neighbour MVs, quarter-pel), d_labels 1 i16 per MB (class 0..288).
+ * A net owns its parameters, optimiser state and the workspace of one batch;
+ * calls on one net must not overlap. */
+#define H264A_MVNET_NPARAMS 389528
+#define H264A_MVNET_MAX_PIXELS 8388608
+typedef struct h264a_mvnet h264a_mvnet;
+typedef struct {
+    const uint8_t *d_cur;    /* current frame luma, cw x ch, stride cw */
+    const uint8_t *d_ref;    /* reference frame luma, same geometry */
+} h264a_mvnet_pair;
+/* seeded He-normal initialisation (zero biases) */
+H264A_API int h264a_mvnet_create(int device, uint64_t seed, h264a_mvnet **out);
+H264A_API int h264a_mvnet_destroy(h264a_mvnet *net);
+/* flat fp32 parameter vector (w1 16x3x3x2, b1 16, w2 32x3x3x16, b2 32,
+ * w3 32x3x3x32, b3 32, w4 256x1168, b4 256, w5 296x256, b5 296; conv weights
+ * [out][ky][kx][in]); set_params also resets the optimiser state */
+H264A_API int h264a_mvnet_set_params(h264a_mvnet *net, const float *h_params);
+H264A_API int h264a_mvnet_get_params(h264a_mvnet *net, float *h_params);
+/* logits of every MB of a batch (npairs * nmb x 296 fp32, device) */
+H264A_API int h264a_mvnet_forward(h264a_mvnet *net, const h264a_mvnet_pair *d_pairs, int npairs, int cw, int ch,
+                                  const int16_t *d_nmv, float *d_logits, void *stream);
+/* mean cross-entropy loss (d_loss, 1 fp32) of a batch and its gradient
+ * (d_grads, NPARAMS fp32), without updating the parameters */
+H264A_API int h264a_mvnet_grads(h264a_mvnet *net, const h264a_mvnet_pair *d_pairs, int npairs, int cw, int ch,
+                                const int16_t *d_nmv, const int16_t *d_labels, float *d_grads, float *d_loss,
+                                void *stream);
+/* one Adam step (beta 0.9 / 0.999, eps 1e-8) at learning rate lr on a batch;
+ * d_loss (optional) receives the batch's loss before the step */
+H264A_API int h264a_mvnet_train_step(h264a_mvnet *net, const h264a_mvnet_pair *d_pairs, int npairs, int cw, int ch,
+                                     const int16_t *d_nmv, const int16_t *d_labels, float lr, float *d_loss,
+                                     void *stream);
+/* Proposals for every MB of whole frames: d_props receives 16 i32 per MB
+ * (8 quarter-pel MVs, most likely first).  d_guide_mvs (optional, 2 i32 per
+ * MB) are the MVs the neighbour features are read from -- the HalfRes
+ * lookahead's MVs (h264a_lookahead_costs) are known before motion estimation
+ * starts, so proposals for a whole batch of frames come from one pass. */
+typedef struct {
+    const uint8_t *d_cur, *d_ref;
+    int32_t cw, ch;
+    const int32_t *d_guide_mvs;
+    int32_t *d_props;
+} h264a_mvnet_frame;
+H264A_API int h264a_mvnet_propose(h264a_mvnet *net, const h264a_mvnet_frame *h_frames, int nframes, void *stream);
+
+/* h264a_me_frames with the learned proposals in each MB's 16x16 search: the
+ * search prices the median predictor and the MB's 8 proposals (d_props, 16
+ * i32 per MB, as h264a_mvnet_propose writes them) with its exact integer cost
+ * J = SATD + (lambda*bits) as i64.  If the cheapest proposal's SATD exceeds
+ * the predictor's by more than fallback_t, the MB runs the plain search
+ * (motion_search from its predictors, mb16.rs:2433) and d_fallback[mb] = 1;
+ * otherwise the search continues as motion_search with the cheapest of the
+ * nine as its start vector (mb16.rs:2445: no full-pel phase, the sub-pel
+ * refinement only) and d_fallback[mb] = 0 (d_fallback optional).  Partitions,
+ * neighbours, outputs and the queue as h264a_me_frames.  No counterpart in
+ * the reference. */
+typedef struct {
+    h264a_me_frame me;
+    const int32_t *d_props;
+    int32_t fallback_t;
+    int32_t *d_fallback;
+} h264a_me_learned_frame;
+H264A_API int h264a_me_frames_learned(h264a_ctx *ctx, const h264a_me_learned_frame *h_frames, int nframes,
+                                      const h264a_me_params *params, void *stream);
+
 /* ---- diagnostics ----------------------------------------------------------- */
 /* Failure-detection self-test: one warp runs the persistent kernel's bounded
  * wait on a flag that nothing sets, giving up after spin_limit polls.  The next

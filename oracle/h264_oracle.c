@@ -1058,8 +1058,47 @@ static void best_part1(const or_me_frame *fr, const or_me_params *pr, const or_m
     or_motion_search(fr, pr, rx, ry, rw, rh, seeds, 1 + nextra, lme, NULL, res);
 }
 
+/* The learned-proposal 16x16 search (no counterpart in the reference): price
+ * the median predictor and the MB's 8 proposals with motion_search's `cost`
+ * closure (mb16.rs:2540-2566, mvd centre = the predictor); if the cheapest
+ * proposal's distortion exceeds the predictor's by more than prop_t, run the
+ * plain search (*fell = 1), else motion_search with the cheapest of the nine
+ * (first wins, the predictor first) as its start vector (mb16.rs:2445). */
+static void learned_16x16(const or_me_frame *fr, const or_me_params *pr, const or_mv_neighbor nb[3], int lx, int ly,
+                          double lme, const int32_t *props, int32_t prop_t, or_me_result *res, int32_t *fell) {
+    int32_t pmv[2];
+    or_predict_mv(&nb[0], &nb[1], &nb[2], 0, pmv);
+    const double lam_r = pr->mv_cost_kind != 0 ? lme * 0.25 : lme;
+    int32_t cand[9][2];
+    cand[0][0] = pmv[0]; cand[0][1] = pmv[1];
+    for (int i = 0; i < 8; i++) { cand[i + 1][0] = props[2 * i]; cand[i + 1][1] = props[2 * i + 1]; }
+    int bi = 0, bp = 1;
+    int64_t cbest = 0, cprop = 0, dist[9];
+    for (int i = 0; i < 9; i++) {
+        uint32_t rate = or_mvbits(pr->mv_cost_kind, pr->mv_cost_tab, cand[i][0] - pmv[0]) +
+                        or_mvbits(pr->mv_cost_kind, pr->mv_cost_tab, cand[i][1] - pmv[1]);
+        dist[i] = or_mc_satd_hp(fr, 1, lx, ly, 16, 16, cand[i][0], cand[i][1]);
+        int64_t c = dist[i] + (int64_t)(lam_r * (double)rate);
+        if (i == 0 || c < cbest) { cbest = c; bi = i; }
+        if (i == 1 || (i > 1 && c < cprop)) { cprop = c; bp = i; }
+    }
+    *fell = dist[bp] > dist[0] + prop_t;
+    if (*fell) or_motion_search(fr, pr, lx, ly, 16, 16, pmv, 1, lme, NULL, res);
+    else or_motion_search(fr, pr, lx, ly, 16, 16, pmv, 1, lme, cand[bi], res);
+}
+
+void or_me_frame_learned(const or_me_frame *fr, const or_me_params *pr, double lambda_me, int64_t split_gate,
+                         const int32_t *props, int32_t prop_t, or_mb_pick *out, int32_t *fell);
+
 void or_me_frame_plain(const or_me_frame *fr, const or_me_params *pr, double lambda_me, int64_t split_gate,
                        or_mb_pick *out) {
+    or_me_frame_learned(fr, pr, lambda_me, split_gate, NULL, 0, out, NULL);
+}
+
+/* or_me_frame_plain, with the learned 16x16 search when props (16 i32 per MB)
+ * is given; fell (optional) receives each MB's fallback flag. */
+void or_me_frame_learned(const or_me_frame *fr, const or_me_params *pr, double lambda_me, int64_t split_gate,
+                         const int32_t *props, int32_t prop_t, or_mb_pick *out, int32_t *fell) {
     int mb_w = fr->cw / 16, mb_h = fr->ch / 16;
     int w4 = mb_w * 4, h4 = mb_h * 4;
     blk4 *g = (blk4 *)calloc((size_t)w4 * h4, sizeof(blk4));
@@ -1069,7 +1108,13 @@ void or_me_frame_plain(const or_me_frame *fr, const or_me_params *pr, double lam
             or_mv_neighbor nb[3];
             mv_neighbors_block(g, w4, h4, mbx * 4, mby * 4, 4, nb);
             or_me_result r16;
-            best_part1(fr, pr, nb, lx, ly, 16, 16, NULL, 0, lambda_me, &r16);
+            if (props) {
+                int32_t f = 0;
+                learned_16x16(fr, pr, nb, lx, ly, lambda_me, props + 16 * (mby * mb_w + mbx), prop_t, &r16, &f);
+                if (fell) fell[mby * mb_w + mbx] = f;
+            } else {
+                best_part1(fr, pr, nb, lx, ly, 16, 16, NULL, 0, lambda_me, &r16);
+            }
             or_mb_pick *pk = &out[mby * mb_w + mbx];
             pk->shape = 0;
             pk->mv[0][0] = pk->mv[1][0] = r16.mvx;

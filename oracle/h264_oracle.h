@@ -129,6 +129,8 @@ void or_motion_search(const or_me_frame *fr, const or_me_params *pr, int lx, int
 typedef struct { int32_t shape; int32_t mv[2][2]; int64_t cost; int64_t cost16; int32_t mv16[2]; } or_mb_pick;
 void or_me_frame_plain(const or_me_frame *fr, const or_me_params *pr, double lambda_me,
                        int64_t split_gate, or_mb_pick *out /* mb_w*mb_h */);
+void or_me_frame_learned(const or_me_frame *fr, const or_me_params *pr, double lambda_me, int64_t split_gate,
+                         const int32_t *props, int32_t prop_t, or_mb_pick *out, int32_t *fell);
 
 /* Exhaustive full-pel grid over ±R around each MB (16x16 SAD and SATD), the
  * ME-oracle-probe order (mb16.rs:2889-2900: dy outer, dx inner, strict <). */

@@ -119,9 +119,22 @@ void or_build_planes4(const uint8_t *ref, int cw, int ch, int pad, uint8_t *plan
 
 /* Plain-ME frame model over one (src, ref) pair; picks written flat:
  * per MB {shape, mv0x, mv0y, mv1x, mv1y, cost_lo, cost_hi, evals-unused}. */
+void or_me_frame_learned_flat(const uint8_t *src, const uint8_t *ref, const uint8_t *planes4, int cw, int ch, int pad,
+                              const or_me_params_flat *pf, const uint16_t *tab, double lambda_me, int64_t split_gate,
+                              const int32_t *props, int32_t prop_t, int32_t *picks, int64_t *costs, int32_t *fell);
+
 void or_me_frame_flat(const uint8_t *src, const uint8_t *ref, const uint8_t *planes4, int cw, int ch, int pad,
                       const or_me_params_flat *pf, const uint16_t *tab, double lambda_me, int64_t split_gate,
                       int32_t *picks /* 6 per MB */, int64_t *costs /* 2 per MB: pick, 16x16 */) {
+    or_me_frame_learned_flat(src, ref, planes4, cw, ch, pad, pf, tab, lambda_me, split_gate, NULL, 0, picks, costs,
+                             NULL);
+}
+
+/* or_me_frame_flat with the learned 16x16 search (props: 16 i32 per MB, NULL
+ * for the plain search); fell (optional): the fallback flag per MB. */
+void or_me_frame_learned_flat(const uint8_t *src, const uint8_t *ref, const uint8_t *planes4, int cw, int ch, int pad,
+                              const or_me_params_flat *pf, const uint16_t *tab, double lambda_me, int64_t split_gate,
+                              const int32_t *props, int32_t prop_t, int32_t *picks, int64_t *costs, int32_t *fell) {
     int pw = cw + 2 * pad, ph = ch + 2 * pad;
     size_t ps = (size_t)pw * ph;
     or_me_frame fr;
@@ -132,7 +145,7 @@ void or_me_frame_flat(const uint8_t *src, const uint8_t *ref, const uint8_t *pla
     unflatten(pf, tab, &p);
     int nmb = (cw / 16) * (ch / 16);
     or_mb_pick *pk = (or_mb_pick *)malloc(sizeof(or_mb_pick) * nmb);
-    or_me_frame_plain(&fr, &p, lambda_me, split_gate, pk);
+    or_me_frame_learned(&fr, &p, lambda_me, split_gate, props, prop_t, pk, fell);
     for (int i = 0; i < nmb; i++) {
         picks[6 * i + 0] = pk[i].shape;
         picks[6 * i + 1] = pk[i].mv[0][0];

@@ -80,6 +80,8 @@ def lib():
                                             i32p, i64p, i32p]
         L.or_me_frame_flat.argtypes = [u8p, u8p, u8p, C.c_int, C.c_int, C.c_int, C.POINTER(MeParamsFlat), u16p,
                                        C.c_double, C.c_int64, i32p, i64p]
+        L.or_me_frame_learned_flat.argtypes = [u8p, u8p, u8p, C.c_int, C.c_int, C.c_int, C.POINTER(MeParamsFlat),
+                                               u16p, C.c_double, C.c_int64, i32p, C.c_int32, i32p, i64p, i32p]
         L.or_pixel_path_clip.argtypes = [u8p, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(MeParamsFlat), u16p,
                                          C.c_double, C.c_int64, C.c_int, C.c_int, i32p, i64p, i16p, i32p, i32p, i32p,
                                          C.c_int]
@@ -173,6 +175,23 @@ def me_frame(src, ref, planes4, params, lambda_me, split_gate=-1, tab=None, pad=
     lib().or_me_frame_flat(ptr(src), ptr(ref), ptr(planes4), cw, ch, pad, C.byref(params), ptr(tab, u16p),
                            float(lambda_me), int(split_gate), ptr(picks, i32p), ptr(costs, i64p))
     return picks, costs
+
+
+def me_frame_learned(src, ref, planes4, params, lambda_me, props, prop_t, split_gate=-1, tab=None, pad=32):
+    """me_frame with the learned 16x16 search over props (nmb, 16) i32;
+    returns (picks, costs, fallback flags)."""
+    ch, cw = src.shape
+    nmb = (cw // 16) * (ch // 16)
+    picks = np.zeros((nmb, 6), np.int32)
+    costs = np.zeros((nmb, 2), np.int64)
+    fell = np.zeros(nmb, np.int32)
+    props = np.ascontiguousarray(props, np.int32)
+    assert props.shape == (nmb, 16)
+    tab = mv_cost_table() if tab is None else tab
+    lib().or_me_frame_learned_flat(ptr(src), ptr(ref), ptr(planes4), cw, ch, pad, C.byref(params), ptr(tab, u16p),
+                                   float(lambda_me), int(split_gate), ptr(props, i32p), int(prop_t), ptr(picks, i32p),
+                                   ptr(costs, i64p), ptr(fell, i32p))
+    return picks, costs, fell
 
 
 def mc_tq_frame(src, ref, picks, qp, dz_div=6):

@@ -67,6 +67,10 @@ class MeFrame(C.Structure):
                 ("d_costs", C.c_void_p)]
 
 
+class MeLearnedFrame(C.Structure):
+    _fields_ = [("me", MeFrame), ("d_props", C.c_void_p), ("fallback_t", C.c_int32), ("d_fallback", C.c_void_p)]
+
+
 class MeTqFrame(C.Structure):
     _fields_ = [("me", MeFrame), ("qp", C.c_int32), ("dz_div", C.c_int32), ("d_coeffs", C.c_void_p)]
 
@@ -102,6 +106,9 @@ EXPORTS = (
     "h264a_pixel_path_prefetch",
     "h264a_selftest_bounded_wait", "h264a_measure_int32_peak", "h264a_me_frames_noalloc",
     "h264a_mc_tq_rec_frames", "h264a_mc_tq_chroma_frames", "h264a_deblock_frames", "h264a_me_tq_frames",
+    "h264a_mvnet_create", "h264a_mvnet_destroy", "h264a_mvnet_set_params", "h264a_mvnet_get_params",
+    "h264a_mvnet_forward", "h264a_mvnet_grads", "h264a_mvnet_train_step", "h264a_mvnet_propose",
+    "h264a_me_frames_learned",
 )
 
 _lib = None
@@ -146,6 +153,15 @@ def load_library() -> C.CDLL:
     L.h264a_selftest_bounded_wait.argtypes = [vp, i32, vp]
     L.h264a_measure_int32_peak.argtypes = [vp, C.POINTER(C.c_double)]
     L.h264a_me_frames_noalloc.argtypes = [vp, i32, C.POINTER(MeParams), vp, vp]
+    L.h264a_me_frames_learned.argtypes = [vp, vp, i32, C.POINTER(MeParams), vp]
+    L.h264a_mvnet_create.argtypes = [i32, C.c_uint64, C.POINTER(vp)]
+    L.h264a_mvnet_destroy.argtypes = [vp]
+    L.h264a_mvnet_set_params.argtypes = [vp, vp]
+    L.h264a_mvnet_get_params.argtypes = [vp, vp]
+    L.h264a_mvnet_forward.argtypes = [vp, vp, i32, i32, i32, vp, vp, vp]
+    L.h264a_mvnet_grads.argtypes = [vp, vp, i32, i32, i32, vp, vp, vp, vp, vp]
+    L.h264a_mvnet_train_step.argtypes = [vp, vp, i32, i32, i32, vp, vp, C.c_float, vp, vp]
+    L.h264a_mvnet_propose.argtypes = [vp, vp, i32, vp]
     _lib = L
     return L
 
@@ -299,6 +315,12 @@ class Accel:
         arr = (MeFrame * len(frames))(*frames)
         self._check(self.L.h264a_me_frames(self.ctx, C.cast(arr, C.c_void_p), len(frames), C.byref(params),
                                            self._stream()))
+
+    def me_frames_learned(self, frames: Sequence[MeLearnedFrame], params: MeParams):
+        """me_frames with the learned proposals in each MB's 16x16 search."""
+        arr = (MeLearnedFrame * len(frames))(*frames)
+        self._check(self.L.h264a_me_frames_learned(self.ctx, C.cast(arr, C.c_void_p), len(frames), C.byref(params),
+                                                   self._stream()))
 
     def me_tq_frames(self, frames: Sequence[MeTqFrame], params: MeParams):
         """me_frames with each MB's MC + luma T/Q fused into the same launch."""

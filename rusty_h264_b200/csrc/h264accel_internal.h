@@ -100,9 +100,17 @@ struct MeTqOut {
     int32_t *row_done;   // with row_count: mb_h words the host can read
     int32_t row_token;
 };
-// plain-ME of frames, with the fused T/Q when tq is given (one entry per frame)
+// Per-frame inputs of the learned-proposal search: 16 i32 of proposals per
+// MB, an optional fallback flag per MB, and the fallback threshold.
+struct MeLearnIn {
+    const int32_t *props;
+    int32_t *fallback;
+    int32_t prop_t;
+};
+// plain-ME of frames, with the fused T/Q when tq is given (one entry per
+// frame), and the learned-proposal 16x16 search when learn is given
 int me_frames_run(h264a_ctx *ctx, const h264a_me_frame *h_frames, int nframes, const h264a_me_params *params,
-                  const MeTqOut *tq, void *stream);
+                  const MeTqOut *tq, void *stream, const MeLearnIn *learn = nullptr);
 // A tiled TMA map of a dense 3D u8 tensor (w x h x d, rows of w bytes, planes
 // of w*h), box bw x bh x bd, no multicast; 0 when the driver entry point is
 // missing or the layout breaks the TMA rules (the caller then copies without).

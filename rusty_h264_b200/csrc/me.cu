@@ -229,8 +229,11 @@ __device__ __forceinline__ long long cand_cost64(const MeParamsDev& pr, const Wa
 }
 
 // Search phases and what an evaluation round's results are for.
-constexpr int PH_SEEDS = 0, PH_DIA = 2, PH_REPRICE = 3, PH_SUB = 4, PH_DONE = 5;
-constexpr int EV_START = 0, EV_SEEDS = 1, EV_FIXED = 3, EV_RING = 4, EV_REPRICE = 5;
+constexpr int PH_SEEDS = 0, PH_PROP = 1, PH_DIA = 2, PH_REPRICE = 3, PH_SUB = 4, PH_DONE = 5;
+constexpr int EV_START = 0, EV_SEEDS = 1, EV_PROP = 2, EV_FIXED = 3, EV_RING = 4, EV_REPRICE = 5;
+// Candidates of the learned search's proposal round: the median predictor
+// and the network's 8 proposals.
+constexpr int N_PROP = 8;
 constexpr int LOOP_GUARD = 1 << 20;  // iterations of one rung / sub-pel step
 
 // Points of a cascading ring priced per round: the first round prices
@@ -689,10 +692,18 @@ struct Knobs {
     }
 };
 
-template <bool BAL>
+// LEARN (the learned-proposal kernels) with use_prop (their 16x16 search): the
+// search first prices the median predictor preds[0..1] and the 8 proposals
+// (lane gl of the group holds proposal gl - 1 in `prop`) with the search's
+// own cost; when the best proposal's distortion exceeds the predictor's by
+// more than prop_t it falls back to the plain search (fell = 1), otherwise it
+// continues as motion_search with the cheapest of the nine as its start
+// vector (mb16.rs:2445, 2579-2596: refine-only, no full-pel phase).
+template <bool BAL, bool LEARN = false>
 __device__ __forceinline__ void motion_search_group(const GroupGeom& q, const MeParamsDev& prm, WarpScratch& ws,
                                                     const int* preds, int npred, double lambda_me, int& out_x,
-                                                    int& out_y, long long& out_c, int& evals) {
+                                                    int& out_y, long long& out_c, int& evals, bool use_prop = false,
+                                                    int2 prop = make_int2(0, 0), int prop_t = 0, int* fell = nullptr) {
     const Knobs<BAL> pr{prm};
     const int gl = q.gl, gb = q.gb;
     const bool sadfp = !pr.fast() && pr.sadfp();
@@ -729,7 +740,7 @@ __device__ __forceinline__ void motion_search_group(const GroupGeom& q, const Me
     evals = 0;
     int bx = 0, by = 0, seed_x = 0, seed_y = 0;
     int best_c = 0, seed_c = 0;  // costs below 2^30 (lane_cost), compared as i32
-    int phase = PH_SEEDS;
+    int phase = (LEARN && use_prop) ? PH_PROP : PH_SEEDS;
     int si = -1, sk = -1, loops = 0, iter = 0, step = 0;
     bool ring_open = false, ring_improved = false;
     int ring_i = 0, ring_n = 0;
@@ -741,6 +752,9 @@ __device__ __forceinline__ void motion_search_group(const GroupGeom& q, const Me
             if (phase == PH_SEEDS) {
                 if (gl == 0) ws.cand[gb] = make_int2(0, 0);
                 kind = EV_SEEDS; n = npred + 1 + __popc(snaps); metric = m_fp; lam = l_fp;
+            } else if (LEARN && phase == PH_PROP) {
+                if (gl <= N_PROP) ws.cand[gb + gl] = gl == 0 ? make_int2(preds[0], preds[1]) : prop;
+                kind = EV_PROP; n = N_PROP + 1; metric = m_main; lam = ws.lam_r;
             } else if (phase == PH_DIA) {
                 if (ring_open) {
                     kind = EV_RING; n = min(ring_n - ring_i, RING_REST); metric = m_fp; lam = l_fp;
@@ -896,6 +910,36 @@ __device__ __forceinline__ void motion_search_group(const GroupGeom& q, const Me
                 evals += 1;
             }
             phase = PH_DIA;
+        } else if (LEARN && kind == EV_PROP) {
+            // the cheapest of the nine (first wins, the predictor first), and
+            // the cheapest proposal's distortion against the predictor's
+            int bi = 0, bp = 1;
+            long long cbest = 0, cprop = 0;
+            for (int i = 0; i <= N_PROP; i++) {
+                const int2 mv = ws.cand[gb + i];
+                const long long c = (long long)ws.dist[gb + i] + lam_cost(lam, pr.rate(ws, mv.x, mv.y));
+                if (i == 0 || c < cbest) { cbest = c; bi = i; }
+                if (i == 1 || (i > 1 && c < cprop)) { cprop = c; bp = i; }
+            }
+            evals += N_PROP + 1;
+            const bool fb = (long long)ws.dist[gb + bp] > (long long)ws.dist[gb] + prop_t;
+            if (fell) *fell = fb ? 1 : 0;
+            if (fb) {
+                // the plain search's seed slots again (the round above used
+                // them; fb is the same in every lane of the 16x16 group)
+                __syncwarp();
+                if (mine) ws.cand[gb + gl] = make_int2(qx, qy);
+                if ((snaps >> gl) & 1u)
+                    ws.cand[gb + npred + 1 + __popc(snaps & ((1u << gl) - 1u))] =
+                        make_int2(((qx + 2) >> 2) * 4, ((qy + 2) >> 2) * 4);
+                phase = PH_SEEDS;
+            } else {
+                bx = ws.cand[gb + bi].x;
+                by = ws.cand[gb + bi].y;
+                best_c = cbest > INT_MAX - 1 ? INT_MAX - 1 : int(cbest);
+                seed_x = bx; seed_y = by; seed_c = best_c;
+                phase = PH_SUB;  // a start vector: no full-pel phase, no B2 reprice
+            }
         } else if (kind == EV_REPRICE) {
             best_c = int(((long long)ws.dist[gb] + lam_cost(lam, pr.rate(ws, ws.cand[gb].x, ws.cand[gb].y))));
             seed_c = int(((long long)ws.dist[gb + 1] + lam_cost(lam, pr.rate(ws, ws.cand[gb + 1].x, ws.cand[gb + 1].y))));
@@ -1020,6 +1064,11 @@ struct FrameDesc {
     int32_t* row_done;
     int32_t row_token;
     int32_t tmap_ok;
+    // the learned-proposal kernels (h264a_me_frames_learned): 16 i32 per MB
+    // of proposals, the fallback threshold, and an optional fallback flag per MB
+    const int32_t* props;
+    int32_t* fallback;
+    int32_t prop_t;
 };
 
 // One launch's frames, passed by value.  Frames are sorted by MB count
@@ -1095,7 +1144,7 @@ __device__ __forceinline__ int2 predict_mv_ref0(bool aa, int2 a, bool ba, int2 b
 // partitions (mb16.rs:8869-8913), and publishes the pick (then, for
 // h264a_me_tq_frames, the MB's MC + T/Q).  BAL: the Balanced preset's knobs
 // as constants.  Dynamic shared memory: ME_WARPS windows of WIN_BYTES.
-template <bool BAL, class TAB>
+template <bool BAL, bool LEARN, class TAB>
 __device__ __forceinline__ void me_frames_body(const TAB& tab, long long total, const MeParamsDev& prm,
                                                int* __restrict__ counter, int* __restrict__ flags, int epoch,
                                                int* __restrict__ status, int spin_limit) {
@@ -1136,6 +1185,12 @@ __device__ __forceinline__ void me_frames_body(const TAB& tab, long long total, 
 #pragma unroll
         for (int r = 0; r < 4; r++)
             src4[r] = ld4u(fd.pic.d_src + (long long)(ly + ((lane >> 2) & 3) * 4 + r) * fd.pic.cw + lx + (lane & 3) * 4);
+        // the learned search's proposal (lanes 1..8), also an input
+        int2 prop = make_int2(0, 0);
+        if (LEARN && lane >= 1 && lane <= N_PROP) {
+            const int32_t* pp = fd.props + 16LL * m + 2 * (lane - 1);
+            prop = make_int2(__ldg(pp), __ldg(pp + 1));
+        }
         // dependencies: left, and top-right (or top at the right edge)
         if (lane == 0) {
             if (mbx > 0) wait_flag(fl + m - 1, epoch, status, 1, spin_limit);
@@ -1190,7 +1245,7 @@ __device__ __forceinline__ void me_frames_body(const TAB& tab, long long total, 
         // best_part for 16x16 (the warp as one group), then, J above the gate,
         // the four partitions seeded with [pmv, mv16] side by side; one call
         // site, so the search body exists once in the kernel.
-        int evals = 0, shape = 0, mv0x = 0, mv0y = 0, mv1x = 0, mv1y = 0;
+        int evals = 0, shape = 0, mv0x = 0, mv0y = 0, mv1x = 0, mv1y = 0, fell = 0;
         long long c16 = 0, best = 0;
         for (int mode = 0; mode < 2; mode++) {
             if (mode == 1 && !(fd.split_gate >= 0 && c16 > fd.split_gate)) break;
@@ -1202,7 +1257,8 @@ __device__ __forceinline__ void me_frames_body(const TAB& tab, long long total, 
             }
             int rx, ry, ev;
             long long rc;
-            motion_search_group<BAL>(qg, prm, scratch[w], preds, mode == 0 ? 1 : 2, fd.lambda_me, rx, ry, rc, ev);
+            motion_search_group<BAL, LEARN>(qg, prm, scratch[w], preds, mode == 0 ? 1 : 2, fd.lambda_me, rx, ry, rc, ev,
+                                            LEARN && mode == 0, prop, fd.prop_t, &fell);
             if (mode == 0) {
                 evals = ev << 4;  // 4x4-block evaluations
                 c16 = rc; best = rc;
@@ -1233,6 +1289,7 @@ __device__ __forceinline__ void me_frames_body(const TAB& tab, long long total, 
             p[0] = shape; p[1] = mv0x; p[2] = mv0y; p[3] = mv1x; p[4] = mv1y; p[5] = evals;
             fd.costs[2 * m] = best;
             fd.costs[2 * m + 1] = c16;
+            if (LEARN && fd.fallback) fd.fallback[m] = fell;
             st_release(fl + m, epoch);  // orders the pick's stores before the flag
         }
         // MC + luma T/Q of the MB under its pick (mb16.rs:3436-3450, as
@@ -1264,24 +1321,24 @@ __device__ __forceinline__ void me_frames_body(const TAB& tab, long long total, 
     }
 }
 
-template <bool BAL>
+template <bool BAL, bool LEARN = false>
 __global__ void __launch_bounds__(32 * ME_WARPS, ME_MIN_BLOCKS)
     me_frames_kernel(const __grid_constant__ FrameBatch batch, long long total, const __grid_constant__ MeParamsDev prm,
                      int* __restrict__ counter, int* __restrict__ flags, int epoch, int* __restrict__ status,
                      int spin_limit) {
-    me_frames_body<BAL>(ParamTable{batch}, total, prm, counter, flags, epoch, status, spin_limit);
+    me_frames_body<BAL, LEARN>(ParamTable{batch}, total, prm, counter, flags, epoch, status, spin_limit);
 }
 
 // The same kernel over a frame table in device memory (more than ME_MAXF
 // frames in one wavefront launch); the frames' tensor maps are read there.
-template <bool BAL>
+template <bool BAL, bool LEARN = false>
 __global__ void __launch_bounds__(32 * ME_WARPS, ME_MIN_BLOCKS)
     me_frames_dkernel(const FrameDesc* __restrict__ frames, const long long* __restrict__ seg_start,
                       const int* __restrict__ seg_j, int nframes, int nseg, long long total,
                       const __grid_constant__ MeParamsDev prm, int* __restrict__ counter, int* __restrict__ flags,
                       int epoch, int* __restrict__ status, int spin_limit) {
-    me_frames_body<BAL>(DeviceTable{frames, seg_start, seg_j, nframes, nseg}, total, prm, counter, flags, epoch,
-                        status, spin_limit);
+    me_frames_body<BAL, LEARN>(DeviceTable{frames, seg_start, seg_j, nframes, nseg}, total, prm, counter, flags, epoch,
+                               status, spin_limit);
 }
 
 // One warp waits on a flag that nothing sets; the bounded wait must give up
@@ -1332,14 +1389,22 @@ static int encode_window_map(CUtensorMap* map, const uint8_t* planes, int pw, in
 
 // Dynamic shared memory of me_frames_kernel, its opt-in above 48 KB, and the
 // CTAs per SM it reaches.
-static int me_frames_setup(int& per_sm) {
+static int me_frames_setup(int& per_sm, bool learn = false) {
     const int smem = ME_WARPS * WIN_BYTES;
     H264A_CUDA(cudaFuncSetAttribute(me_frames_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     H264A_CUDA(cudaFuncSetAttribute(me_frames_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     H264A_CUDA(cudaFuncSetAttribute(me_frames_dkernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     H264A_CUDA(cudaFuncSetAttribute(me_frames_dkernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    H264A_CUDA(cudaFuncSetAttribute(me_frames_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    H264A_CUDA(cudaFuncSetAttribute(me_frames_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    H264A_CUDA(cudaFuncSetAttribute(me_frames_dkernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    H264A_CUDA(cudaFuncSetAttribute(me_frames_dkernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     per_sm = 0;
-    H264A_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, me_frames_kernel<false>, 32 * ME_WARPS, smem));
+    if (learn)
+        H264A_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, me_frames_kernel<false, true>, 32 * ME_WARPS,
+                                                                 smem));
+    else
+        H264A_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, me_frames_kernel<false>, 32 * ME_WARPS, smem));
     if (per_sm < 1) per_sm = 1;
     return H264A_OK;
 }
@@ -1382,23 +1447,39 @@ static long long fill_segments(FrameBatch& fb) {
 
 static void launch_me_frames_dtab(const MeParamsDev& prm, unsigned blocks, cudaStream_t st, const FrameDesc* frames,
                                   const long long* seg_start, const int* seg_j, int nframes, int nseg, long long total,
-                                  int* counter, int* flags, int epoch, int* status) {
-    if (balanced_preset(prm))
-        me_frames_dkernel<true><<<blocks, 32 * ME_WARPS, ME_WARPS * WIN_BYTES, st>>>(
-            frames, seg_start, seg_j, nframes, nseg, total, prm, counter, flags, epoch, status, SPIN_LIMIT);
+                                  int* counter, int* flags, int epoch, int* status, bool learn = false) {
+    const size_t sm = ME_WARPS * WIN_BYTES;
+    const bool bal = balanced_preset(prm);
+    if (learn && bal)
+        me_frames_dkernel<true, true><<<blocks, 32 * ME_WARPS, sm, st>>>(frames, seg_start, seg_j, nframes, nseg, total,
+                                                                        prm, counter, flags, epoch, status, SPIN_LIMIT);
+    else if (learn)
+        me_frames_dkernel<false, true><<<blocks, 32 * ME_WARPS, sm, st>>>(frames, seg_start, seg_j, nframes, nseg, total,
+                                                                         prm, counter, flags, epoch, status, SPIN_LIMIT);
+    else if (bal)
+        me_frames_dkernel<true><<<blocks, 32 * ME_WARPS, sm, st>>>(frames, seg_start, seg_j, nframes, nseg, total, prm,
+                                                                  counter, flags, epoch, status, SPIN_LIMIT);
     else
-        me_frames_dkernel<false><<<blocks, 32 * ME_WARPS, ME_WARPS * WIN_BYTES, st>>>(
-            frames, seg_start, seg_j, nframes, nseg, total, prm, counter, flags, epoch, status, SPIN_LIMIT);
+        me_frames_dkernel<false><<<blocks, 32 * ME_WARPS, sm, st>>>(frames, seg_start, seg_j, nframes, nseg, total, prm,
+                                                                   counter, flags, epoch, status, SPIN_LIMIT);
 }
 
 static void launch_me_frames(const MeParamsDev& prm, unsigned blocks, cudaStream_t st, const FrameBatch& fb,
-                             long long total, int* counter, int* flags, int epoch, int* status) {
-    if (balanced_preset(prm))
-        me_frames_kernel<true><<<blocks, 32 * ME_WARPS, ME_WARPS * WIN_BYTES, st>>>(fb, total, prm, counter, flags, epoch,
-                                                                                status, SPIN_LIMIT);
+                             long long total, int* counter, int* flags, int epoch, int* status, bool learn = false) {
+    const size_t sm = ME_WARPS * WIN_BYTES;
+    const bool bal = balanced_preset(prm);
+    if (learn && bal)
+        me_frames_kernel<true, true><<<blocks, 32 * ME_WARPS, sm, st>>>(fb, total, prm, counter, flags, epoch, status,
+                                                                       SPIN_LIMIT);
+    else if (learn)
+        me_frames_kernel<false, true><<<blocks, 32 * ME_WARPS, sm, st>>>(fb, total, prm, counter, flags, epoch, status,
+                                                                        SPIN_LIMIT);
+    else if (bal)
+        me_frames_kernel<true><<<blocks, 32 * ME_WARPS, sm, st>>>(fb, total, prm, counter, flags, epoch, status,
+                                                                 SPIN_LIMIT);
     else
-        me_frames_kernel<false><<<blocks, 32 * ME_WARPS, ME_WARPS * WIN_BYTES, st>>>(fb, total, prm, counter, flags,
-                                                                                 epoch, status, SPIN_LIMIT);
+        me_frames_kernel<false><<<blocks, 32 * ME_WARPS, sm, st>>>(fb, total, prm, counter, flags, epoch, status,
+                                                                  SPIN_LIMIT);
 }
 
 extern "C" int h264a_selftest_bounded_wait(h264a_ctx* ctx, int spin_limit, void* stream) {
@@ -1428,7 +1509,7 @@ extern "C" int h264a_me_search(h264a_ctx* ctx, const h264a_picture* d_pics, int 
 // Plain-ME of a batch of frames (h264a_me_frames); with `tq`, each frame's
 // MC + luma T/Q is fused in (h264a_me_tq_frames, h264a_pixel_path_host).
 int h264a::me_frames_run(h264a_ctx* ctx, const h264a_me_frame* h_frames, int nframes,
-                         const h264a_me_params* params, const MeTqOut* tq, void* stream) {
+                         const h264a_me_params* params, const MeTqOut* tq, void* stream, const MeLearnIn* learn) {
     if (!ctx || !h_frames || !params) return fail(H264A_E_ARG, "me_frames: null pointer");
     if (nframes < 1) return fail(H264A_E_ARG, "me_frames: need at least one frame");
     if ((params->mv_cost_kind == 1 || params->mv_cost_kind == 2) && !params->d_mv_cost_tab)
@@ -1445,7 +1526,7 @@ int h264a::me_frames_run(h264a_ctx* ctx, const h264a_me_frame* h_frames, int nfr
     cudaStream_t st = pick_stream(ctx, stream);
     const MeParamsDev prm = to_dev(*params);
     int per_sm = 0;
-    int rc0 = me_frames_setup(per_sm);
+    int rc0 = me_frames_setup(per_sm, learn != nullptr);
     if (rc0) return rc0;
     // One wavefront launch over all frames, largest first: the frame table in
     // the kernel's parameters up to ME_MAXF frames, in device memory beyond.
@@ -1477,6 +1558,12 @@ int h264a::me_frames_run(h264a_ctx* ctx, const h264a_me_frame* h_frames, int nfr
             d.row_done = t.row_done;
             d.row_token = t.row_token;
         }
+        if (learn) {
+            const MeLearnIn& l = learn[order[k]];
+            d.props = l.props;
+            d.fallback = l.fallback;
+            d.prop_t = l.prop_t;
+        }
         total += (long long)d.mb_w * d.mb_h;
         if (total >= (1LL << 31)) return fail(H264A_E_ARG, "me_frames: too many macroblocks in one call");
     }
@@ -1499,7 +1586,7 @@ int h264a::me_frames_run(h264a_ctx* ctx, const h264a_me_frame* h_frames, int nfr
         memcpy(fb.f, desc.data(), sizeof(FrameDesc) * nframes);
         if (fill_segments(fb) != total) return fail(H264A_E_ARG, "me_frames: internal queue layout error");
         launch_me_frames(prm, unsigned(blocks), st, fb, total, ctx->q[Q_MAIN].d_counter, ctx->q[Q_MAIN].d_flags, epoch,
-                         ctx->d_status);
+                         ctx->d_status, learn != nullptr);
         return check_launch("me_frames_kernel");
     }
     // the table, its segment starts and j values in one device buffer, uploaded
@@ -1528,13 +1615,30 @@ int h264a::me_frames_run(h264a_ctx* ctx, const h264a_me_frame* h_frames, int nfr
     char* dv = static_cast<char*>(ctx->me_tab);
     launch_me_frames_dtab(prm, unsigned(blocks), st, reinterpret_cast<const FrameDesc*>(dv),
                           reinterpret_cast<const long long*>(dv + b_desc), reinterpret_cast<const int*>(dv + b_desc + b_seg),
-                          nframes, nseg, total, ctx->q[Q_MAIN].d_counter, ctx->q[Q_MAIN].d_flags, epoch, ctx->d_status);
+                          nframes, nseg, total, ctx->q[Q_MAIN].d_counter, ctx->q[Q_MAIN].d_flags, epoch, ctx->d_status,
+                          learn != nullptr);
     return check_launch("me_frames_dkernel");
 }
 
 extern "C" int h264a_me_frames(h264a_ctx* ctx, const h264a_me_frame* h_frames, int nframes,
                                const h264a_me_params* params, void* stream) {
     return me_frames_run(ctx, h_frames, nframes, params, nullptr, stream);
+}
+
+extern "C" int h264a_me_frames_learned(h264a_ctx* ctx, const h264a_me_learned_frame* h_frames, int nframes,
+                                       const h264a_me_params* params, void* stream) {
+    if (!ctx || !h_frames || !params) return fail(H264A_E_ARG, "me_frames_learned: null pointer");
+    if (nframes < 1) return fail(H264A_E_ARG, "me_frames_learned: need at least one frame");
+    std::vector<h264a_me_frame> me(nframes);
+    std::vector<MeLearnIn> ln(nframes);
+    for (int i = 0; i < nframes; i++) {
+        const h264a_me_learned_frame& f = h_frames[i];
+        if (!f.d_props) return fail(H264A_E_ARG, "me_frames_learned: null proposals");
+        if (f.fallback_t < 0) return fail(H264A_E_ARG, "me_frames_learned: negative fallback threshold");
+        me[i] = f.me;
+        ln[i] = MeLearnIn{f.d_props, f.d_fallback, f.fallback_t};
+    }
+    return me_frames_run(ctx, me.data(), nframes, params, nullptr, stream, ln.data());
 }
 
 extern "C" int h264a_me_tq_frames(h264a_ctx* ctx, const h264a_me_tq_frame* h_frames, int nframes,

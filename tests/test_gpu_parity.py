@@ -286,6 +286,58 @@ def test_me_frames_matches_oracle(acc, cif, split, variant):
         assert np.array_equal(costs, wc), variant
 
 
+@pytest.mark.parametrize("prop_t", [0, 300, 1 << 30])
+def test_me_frames_learned_matches_oracle(acc, prop_t):
+    """The learned-proposal search (h264a_me_frames_learned) against the
+    oracle's or_me_frame_learned on 4 CIF P frames in one launch: proposals
+    scattered around each MB's plain pick (exact, a few pixels off, far off),
+    the split gate on, at thresholds where every MB, some and none fall back."""
+    torch = acc.torch
+    y, _, _ = synth.cif_clip(5, 2)
+    clip = synth.coded_luma(y)
+    n, ch, cw = clip.shape
+    nmb = (cw // 16) * (ch // 16)
+    qp = 27
+    lam = float(np.sqrt(A.frame_lambda(qp)) * 1.25)
+    gate = A.split_gate_for_qp(qp)
+    params = A.default_me_params()
+    d = dev(acc, clip)
+    planes = acc.hpel_build(d[: n - 1], 32)
+    rng = np.random.default_rng(17)
+    pl_np = planes.cpu().numpy()
+    frames, outs, want = [], [], []
+    for f in range(1, n):
+        plain, _ = O.me_frame(clip[f], clip[f - 1], pl_np[f - 1], O.balanced_params(), lam, gate)
+        props = np.zeros((nmb, 16), np.int32)
+        for i in range(8):
+            k = rng.integers(0, 3, nmb)
+            off = np.where(k[:, None] == 0, 0, np.where(k[:, None] == 1, rng.integers(-3, 4, (nmb, 2)),
+                                                         rng.integers(-8, 9, (nmb, 2))))
+            props[:, 2 * i:2 * i + 2] = ((plain[:, 1:3] + 2) // 4 + off) * 4
+        want.append(O.me_frame_learned(clip[f], clip[f - 1], pl_np[f - 1], O.balanced_params(), lam, props, prop_t,
+                                       gate))
+        d_props = dev(acc, props)
+        pk = acc.zeros((nmb, 6), torch.int32)
+        co = acc.zeros((nmb, 2), torch.int64)
+        fb = torch.full((nmb,), -1, dtype=torch.int32, device="cuda:0")
+        outs.append((d_props, pk, co, fb))
+        frames.append(A.MeLearnedFrame(A.MeFrame(A.Picture(d[f].data_ptr(), planes[f - 1].data_ptr(), cw, ch, 32), lam,
+                                                 gate, pk.data_ptr(), co.data_ptr()), d_props.data_ptr(), prop_t,
+                                       fb.data_ptr()))
+    acc.me_frames_learned(frames, params)
+    acc.sync()
+    fell_total = 0
+    for (_, pk, co, fb), (wp, wc, wf) in zip(outs, want):
+        assert np.array_equal(fb.cpu().numpy(), wf)
+        assert np.array_equal(pk.cpu().numpy()[:, :5], wp[:, :5])
+        assert np.array_equal(co.cpu().numpy(), wc)
+        fell_total += int(wf.sum())
+    if prop_t >= 1 << 30:
+        assert fell_total == 0
+    elif prop_t == 0:
+        assert fell_total > 0
+
+
 def test_me_frames_single_mb_and_flat(acc):
     flat = np.full((2, 16, 16), 90, np.uint8)
     rng = np.random.default_rng(3)

@@ -789,7 +789,7 @@ def np_mvbits(d):
     return 1 + 2 * ((code + 1).bit_length() - 1)
 
 
-def np_motion_search(src, ref, lx, ly, rw, rh, preds, lam):
+def np_motion_search(src, ref, lx, ly, rw, rh, preds, lam, start=None):
     """motion_search (mb16.rs:2433-3302) under the Balanced preset: seeds (0,0)
     then the predictors, the centre snapped to full-pel, the ladder of 4-point
     diamonds at 16, 8, 4 quarter-pel (fixed-centre argmin where the +-step box
@@ -797,7 +797,9 @@ def np_motion_search(src, ref, lx, ly, rw, rh, preds, lam):
     while it moves), one pass of the 8-point half-pel then quarter-pel rings
     (each point around the centre as it moves), and the pre-snap seed kept if
     cheaper.  Distortion: the exact 4x4 Hadamard SATD against the clamped
-    luma_sample prediction; rate: (lambda * bits) truncated."""
+    luma_sample prediction; rate: (lambda * bits) truncated.  With a start
+    vector (mb16.rs:2445) the search prices only it, skips the snap and the
+    diamond ladder, and refines it with the sub-pel rings."""
     ch, cw = src.shape
     center = preds[0]
     memo = {}
@@ -809,15 +811,18 @@ def np_motion_search(src, ref, lx, ly, rw, rh, preds, lam):
             memo[mv] = np_satd_sum(src[ly:ly + rh, lx:lx + rw], pred) + int(lam * rate)
         return memo[mv]
 
-    best, best_c = (0, 0), cost((0, 0))
-    for p in preds:
-        if cost(p) < best_c:
-            best, best_c = p, cost(p)
+    if start is not None:
+        best, best_c = start, cost(start)
+    else:
+        best, best_c = (0, 0), cost((0, 0))
+        for p in preds:
+            if cost(p) < best_c:
+                best, best_c = p, cost(p)
     seed_mv, seed_c = best, best_c
-    if best[0] & 3 or best[1] & 3:
+    if start is None and (best[0] & 3 or best[1] & 3):
         best = (((best[0] + 2) // 4) * 4, ((best[1] + 2) // 4) * 4)
         best_c = cost(best)
-    for step in (16, 8, 4):
+    for step in ((16, 8, 4) if start is None else ()):
         ring = ((step, 0), (-step, 0), (0, step), (0, -step))
         while True:
             s = step >> 2
@@ -863,18 +868,41 @@ def np_predict_mv(a, b, c):
     return (med(mva[0], mvb[0], mvc[0]), med(mva[1], mvb[1], mvc[1]))
 
 
-def np_me_frame(src, ref, lam, gate):
+def np_learned_16x16(src, ref, lx, ly, pmv, props, prop_t, lam):
+    """The learned-proposal 16x16 search (no counterpart in the reference):
+    the predictor and the 8 proposals priced with the search's cost; if the
+    cheapest proposal's SATD exceeds the predictor's by more than prop_t, the
+    plain search, else motion_search from the cheapest of the nine (the
+    predictor first on ties).  Returns (mv, J, fell back)."""
+    cands = [tuple(pmv)] + [(int(props[2 * i]), int(props[2 * i + 1])) for i in range(8)]
+    dist, cost = [], []
+    for mv in cands:
+        pred = np_luma_sample_block(ref, lx, ly, 16, 16, mv[0], mv[1])
+        d = np_satd_sum(src[ly:ly + 16, lx:lx + 16], pred)
+        dist.append(d)
+        cost.append(d + int(lam * (np_mvbits(mv[0] - pmv[0]) + np_mvbits(mv[1] - pmv[1]))))
+    bp = 1 + int(np.argmin(cost[1:]))
+    if dist[bp] > dist[0] + prop_t:
+        mv, c = np_motion_search(src, ref, lx, ly, 16, 16, [tuple(pmv)], lam)
+        return mv, c, True
+    mv, c = np_motion_search(src, ref, lx, ly, 16, 16, [tuple(pmv)], lam, start=cands[int(np.argmin(cost))])
+    return mv, c, False
+
+
+def np_me_frame(src, ref, lam, gate, props=None, prop_t=0):
     """The plain-ME frame model: every MB in raster order coded inter with ref
     0; the neighbours of its top-left 4x4 block (mv_neighbors_block,
     mb16.rs:1871: left, top, top-right else top-left) give predict_mv;
     best_part 16x16 seeded [pmv], and when its J exceeds the gate the 16x8 and
     8x16 halves seeded [pmv, mv16], the shape taken on strictly lower summed J
-    (mb16.rs:8869-8913)."""
+    (mb16.rs:8869-8913).  With props (16 i32 per MB) the 16x16 search is
+    np_learned_16x16; the fallback flags are returned as a third array."""
     ch, cw = src.shape
     mb_w, mb_h = cw // 16, ch // 16
     picks = np.zeros((mb_w * mb_h, 6), np.int32)
     costs = np.zeros((mb_w * mb_h, 2), np.int64)
     blk = {}  # (bx4, by4) -> MV of coded 4x4 blocks
+    fell = np.zeros(mb_w * mb_h, np.int32)
 
     def get(bx, by):
         return blk.get((bx, by)) if 0 <= bx < mb_w * 4 and 0 <= by < mb_h * 4 else None
@@ -884,7 +912,11 @@ def np_me_frame(src, ref, lam, gate):
         lx, ly, bx, by = mbx * 16, mby * 16, mbx * 4, mby * 4
         c = get(bx + 4, by - 1)
         pmv = np_predict_mv(get(bx - 1, by), get(bx, by - 1), c if c is not None else get(bx - 1, by - 1))
-        mv16, c16 = np_motion_search(src, ref, lx, ly, 16, 16, [pmv], lam)
+        if props is None:
+            mv16, c16 = np_motion_search(src, ref, lx, ly, 16, 16, [pmv], lam)
+        else:
+            mv16, c16, fb = np_learned_16x16(src, ref, lx, ly, pmv, props[m], prop_t, lam)
+            fell[m] = fb
         shape, mv0, mv1, best = 0, mv16, mv16, c16
         if gate >= 0 and c16 > gate:
             seeds = [pmv, mv16]
@@ -900,7 +932,7 @@ def np_me_frame(src, ref, lam, gate):
             for i in range(4):
                 part = (j >= 2) if shape == 1 else ((i >= 2) if shape == 2 else 0)
                 blk[(bx + i, by + j)] = mv1 if part else mv0
-    return picks, costs
+    return (picks, costs) if props is None else (picks, costs, fell)
 
 
 @pytest.mark.parametrize("gate_on", [False, True])
@@ -924,6 +956,38 @@ def test_me_frame_oracle_matches_numpy_restatement(gate_on):
         gp, gc = np_me_frame(src, ref, lam, gate)
         assert np.array_equal(wp[:, :5], gp[:, :5]), np.argwhere(wp[:, :5] != gp[:, :5])[:4]
         assert np.array_equal(wc, gc)
+
+
+@pytest.mark.parametrize("prop_t", [0, 40, 1 << 30])
+def test_learned_me_frame_oracle_matches_numpy_restatement(prop_t):
+    """The C oracle's learned-proposal frame (or_me_frame_learned) against the
+    restatement above: proposals scattered around the true motion of a
+    panning texture (some exact, some off by a few pixels, some far), with
+    the split gate on, at thresholds that make every MB, some MBs and no MB
+    fall back."""
+    from rusty_h264_b200 import accel as A
+
+    qp = 27
+    lam = float(np.sqrt(A.frame_lambda(qp)) * 1.25)
+    gate = A.split_gate_for_qp(qp)
+    frames = _panning_clip(2, 96, 64, (5, -3), 11)
+    src, ref = frames[1], frames[0]
+    nmb = 6 * 4
+    rng = np.random.default_rng(prop_t % 997)
+    props = np.zeros((nmb, 16), np.int32)
+    for m in range(nmb):
+        for i in range(8):
+            k = rng.integers(0, 3)
+            off = (0, 0) if k == 0 else (tuple(rng.integers(-3, 4, 2)) if k == 1 else tuple(rng.integers(-8, 9, 2)))
+            props[m, 2 * i] = 4 * (-5 + off[0])
+            props[m, 2 * i + 1] = 4 * (3 + off[1])
+    wp, wc, wf = O.me_frame_learned(src, ref, O.build_planes4(ref, 32), O.balanced_params(), lam, props, prop_t, gate)
+    gp, gc, gf = np_me_frame(src, ref, lam, gate, props, prop_t)
+    assert np.array_equal(wf, gf)
+    assert np.array_equal(wp[:, :5], gp[:, :5]), np.argwhere(wp[:, :5] != gp[:, :5])[:4]
+    assert np.array_equal(wc, gc)
+    if prop_t >= 1 << 30:
+        assert not wf.any()
 
 
 # ---------------------------------------------------------------------------
