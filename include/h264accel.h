@@ -417,6 +417,72 @@ typedef struct {
 H264A_API int h264a_me_frames_learned(h264a_ctx *ctx, const h264a_me_learned_frame *h_frames, int nframes,
                                       const h264a_me_params *params, void *stream);
 
+/* ---- the closed reconstruction loop ------------------------------------------ */
+/* The pixel path as the encoder runs it: every P frame searches, predicts
+ * from and reconstructs against the deblocked reconstruction of the frame
+ * before it, as the reference searches RefFrames built from its
+ * reconstructed planes (encoder/src/lib.rs:228-262; luma reconstruction
+ * mb16.rs:3575-3605, chroma mb16.rs:3606-3628, deblock.rs filter_frame with
+ * zero offsets).  Frame 0 reconstructs to itself (coded losslessly in this
+ * frame model); frames 1..n-1 run plain-ME (or, with a net, the learned
+ * search, its proposals computed from the source frame and the previous
+ * reconstruction, guide MVs from the HalfRes lookahead of the source),
+ * MC + T/Q and reconstruction of luma and chroma, and deblocking.  The frames
+ * run one after another on the device (frame f may read any row of
+ * rec(f-1)); each frame's MBs run as a wavefront.  Inputs: n frames of luma
+ * (cw x ch) and chroma (cw/2 x ch/2), contiguous, host memory.  Outputs per
+ * frame (frame 0 rows zero): picks 6 i32/MB, costs 2 i64/MB, luma levels 256
+ * i16/MB, chroma levels 128 i16/MB (as h264a_mc_tq_chroma_frames), the
+ * reconstruction, and with a net its proposals (16 i32/MB) and fallback flags
+ * (1 i32/MB); all but picks and costs optional.  Synchronous. */
+typedef struct {
+    const uint8_t *h_y, *h_u, *h_v;
+    int32_t n, cw, ch;
+    double lambda_me;
+    int64_t split_gate;
+    int32_t qp, dz_div;
+    h264a_mvnet *net;            /* NULL: plain search */
+    int32_t fallback_t;
+    int32_t *h_picks;
+    int64_t *h_costs;
+    int16_t *h_coeffs, *h_ccoeffs;
+    uint8_t *h_rec_y, *h_rec_u, *h_rec_v;
+    int32_t *h_props, *h_fallback;
+} h264a_closed_job;
+H264A_API int h264a_pixel_path_closed(h264a_ctx *ctx, const h264a_closed_job *job, const h264a_me_params *params,
+                                      const uint16_t *h_mv_cost_tab);
+
+/* ---- Annex-B output of the frame model (host) ---------------------------------- */
+/* A decodable H.264 Baseline stream (CAVLC) of n frames of the frame model:
+ * SPS, PPS, frame 0 as an IDR picture of I_PCM macroblocks (its lossless
+ * reconstruction is the source frame), frames 1..n-1 as P pictures, one slice
+ * each, every MB coded (mb_skip_run 0) as P_L0_16x16 / P_L0_L0_16x8 /
+ * P_L0_L0_8x16 per its pick with reference 0, its MVs against the standard's
+ * MV predictor, its levels (h264a_mc_tq_rec_frames' 256 luma levels and
+ * h264a_mc_tq_chroma_frames' 128 chroma levels per MB) as CAVLC residual
+ * blocks at the picture's QP.  Syntax after the reference's writer: CAVLC P
+ * slices (encoder/src/mb16.rs:5266-5845), residual blocks
+ * (common/src/cavlc.rs:485), parameter sets and NAL framing
+ * (common/src/nal.rs).  width/height: display size (even, cropped from the
+ * MB-aligned coded size).  With h_out NULL only *out_len is computed;
+ * h_frame_bytes (optional, n entries) receives each frame's bytes (frame 0
+ * with the parameter sets).  Host only, no GPU needed. */
+typedef struct {
+    int32_t width, height, cw, ch, n, qp;
+    const uint8_t *h_y0, *h_u0, *h_v0;  /* frame 0 (cw x ch, cw/2 x ch/2) */
+    const int32_t *h_picks;             /* n x nmb x 6 (frame 0 unused) */
+    const int16_t *h_coeffs;            /* n x nmb x 256 */
+    const int16_t *h_ccoeffs;           /* n x nmb x 128 */
+} h264a_stream_frames;
+H264A_API int h264a_write_stream_cavlc(const h264a_stream_frames *in, uint8_t *h_out, size_t cap, size_t *out_len,
+                                       int64_t *h_frame_bytes);
+/* The writer's VLC tables, for checking against the standard's: table 0
+ * coeff_token (nC class i 0..2, TotalCoeff j, TrailingOnes k), 1 chroma-DC
+ * coeff_token (j, k), 2 total_zeros (TotalCoeff j 1..15, total_zeros k),
+ * 3 chroma-DC total_zeros, 4 run_before (min(zerosLeft,7) j, run k), 5 the
+ * inter coded_block_pattern j -> codeNum (in *bits). */
+H264A_API int h264a_cavlc_table_code(int table, int i, int j, int k, int *len, int *bits);
+
 /* ---- diagnostics ----------------------------------------------------------- */
 /* Failure-detection self-test: one warp runs the persistent kernel's bounded
  * wait on a flag that nothing sets, giving up after spin_limit polls.  The next

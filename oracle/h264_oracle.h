@@ -131,6 +131,9 @@ void or_me_frame_plain(const or_me_frame *fr, const or_me_params *pr, double lam
                        int64_t split_gate, or_mb_pick *out /* mb_w*mb_h */);
 void or_me_frame_learned(const or_me_frame *fr, const or_me_params *pr, double lambda_me, int64_t split_gate,
                          const int32_t *props, int32_t prop_t, or_mb_pick *out, int32_t *fell);
+/* in-loop deblocking of a plain-ME P picture (h264_oracle_par.c) */
+void or_deblock_frame_plain(uint8_t *y, uint8_t *u, uint8_t *v, int cw, int ch, const int32_t *picks,
+                            const int16_t *coeffs, int qp, int offset_a, int offset_b, int chroma_qp_offset);
 
 /* Exhaustive full-pel grid over ±R around each MB (16x16 SAD and SATD), the
  * ME-oracle-probe order (mb16.rs:2889-2900: dy outer, dx inner, strict <). */

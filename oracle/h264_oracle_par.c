@@ -529,3 +529,48 @@ void or_pixel_path_clip(const uint8_t *frames, int nframes, int cw, int ch, int 
     par_for(nframes - 1, nthreads, pp_frame, &a);
     or_lookahead_clip(frames, nframes, cw, ch, 2, la_intra, la_inter, la_mvs, nthreads);
 }
+
+/* The closed reconstruction loop over a clip of n frames (luma cw x ch,
+ * chroma cw/2 x ch/2, each contiguous).  Frame 0 reconstructs to itself (the
+ * frame model codes it losslessly).  P frame f runs the frame's motion search
+ * against the planes of the deblocked reconstruction of frame f-1, as the
+ * reference encoder searches RefFrames built from reconstructed planes
+ * (encoder/src/lib.rs:228-262), predicts from that reconstruction, and its
+ * luma (mb16.rs:3575-3605) and chroma (mb16.rs:3606-3628) reconstruction,
+ * deblocked (deblock.rs filter_frame; offsets 0), is frame f+1's reference.
+ * props (optional, 16 i32 per MB per frame) switch the 16x16 search to the
+ * learned-proposal search with threshold prop_t.  Outputs per frame (frame 0
+ * rows zero): picks 6 i32/MB, costs 2 i64/MB, luma levels 256 i16/MB, chroma
+ * levels 128 i16/MB, the reconstruction, fallback flags (optional). */
+void or_closed_loop_clip(const uint8_t *y, const uint8_t *u, const uint8_t *v, int n, int cw, int ch, int pad,
+                         const or_me_params_flat *pf, const uint16_t *tab, double lambda_me, int64_t split_gate,
+                         int qp, int dz_div, const int32_t *props, int32_t prop_t, int32_t *picks, int64_t *costs,
+                         int16_t *coeffs, int16_t *ccoeffs, uint8_t *rec_y, uint8_t *rec_u, uint8_t *rec_v,
+                         int32_t *fell) {
+    int nmb = (cw / 16) * (ch / 16);
+    size_t fs = (size_t)cw * ch, cs = fs / 4;
+    int pw = cw + 2 * pad, ph = ch + 2 * pad;
+    uint8_t *planes = (uint8_t *)malloc((size_t)4 * pw * ph);
+    memset(picks, 0, sizeof(int32_t) * 6 * nmb);
+    memset(costs, 0, sizeof(int64_t) * 2 * nmb);
+    memset(coeffs, 0, sizeof(int16_t) * 256 * nmb);
+    memset(ccoeffs, 0, sizeof(int16_t) * 128 * nmb);
+    if (fell) memset(fell, 0, sizeof(int32_t) * nmb);
+    memcpy(rec_y, y, fs);
+    memcpy(rec_u, u, cs);
+    memcpy(rec_v, v, cs);
+    for (int f = 1; f < n; f++) {
+        const uint8_t *ry = rec_y + fs * (f - 1), *ru = rec_u + cs * (f - 1), *rv = rec_v + cs * (f - 1);
+        uint8_t *oy = rec_y + fs * f, *ou = rec_u + cs * f, *ov = rec_v + cs * f;
+        int32_t *pk = picks + (size_t)6 * nmb * f;
+        int16_t *co = coeffs + (size_t)256 * nmb * f;
+        or_build_planes4(ry, cw, ch, pad, planes);
+        or_me_frame_learned_flat(y + fs * f, ry, planes, cw, ch, pad, pf, tab, lambda_me, split_gate,
+                                 props ? props + (size_t)16 * nmb * f : NULL, prop_t, pk,
+                                 costs + (size_t)2 * nmb * f, fell ? fell + (size_t)nmb * f : NULL);
+        or_mc_tq_rec_frame(y + fs * f, ry, cw, ch, pk, qp, dz_div, co, oy);
+        or_mc_tq_chroma_frame(u + cs * f, v + cs * f, ru, rv, cw, ch, pk, qp, ccoeffs + (size_t)128 * nmb * f, ou, ov);
+        or_deblock_frame_plain(oy, ou, ov, cw, ch, pk, co, qp, 0, 0, 0);
+    }
+    free(planes);
+}

@@ -82,6 +82,9 @@ def lib():
                                        C.c_double, C.c_int64, i32p, i64p]
         L.or_me_frame_learned_flat.argtypes = [u8p, u8p, u8p, C.c_int, C.c_int, C.c_int, C.POINTER(MeParamsFlat),
                                                u16p, C.c_double, C.c_int64, i32p, C.c_int32, i32p, i64p, i32p]
+        L.or_closed_loop_clip.argtypes = [u8p, u8p, u8p, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(MeParamsFlat),
+                                          u16p, C.c_double, C.c_int64, C.c_int, C.c_int, i32p, C.c_int32, i32p, i64p,
+                                          i16p, i16p, u8p, u8p, u8p, i32p]
         L.or_pixel_path_clip.argtypes = [u8p, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(MeParamsFlat), u16p,
                                          C.c_double, C.c_int64, C.c_int, C.c_int, i32p, i64p, i16p, i32p, i32p, i32p,
                                          C.c_int]
@@ -325,3 +328,77 @@ def pixel_path_clip(frames: np.ndarray, params, lambda_me, split_gate, qp, dz_di
                              float(lambda_me), int(split_gate), qp, dz_div, ptr(picks, i32p), ptr(costs, i64p),
                              ptr(coeffs, i16p), ptr(intra, i32p), ptr(inter, i32p), ptr(mvs, i32p), nthreads)
     return dict(picks=picks, costs=costs, coeffs=coeffs, la_intra=intra, la_inter=inter, la_mvs=mvs)
+
+
+def closed_loop_clip(y, u, v, params, lambda_me, split_gate, qp, dz_div=6, pad=32, props=None, prop_t=0, tab=None):
+    """The closed reconstruction loop (or_closed_loop_clip) over luma y (n, ch,
+    cw) and chroma u, v (n, ch/2, cw/2): per frame picks, costs, luma and
+    chroma levels, the deblocked reconstruction and fallback flags."""
+    n, ch, cw = y.shape
+    nmb = (cw // 16) * (ch // 16)
+    out = dict(picks=np.zeros((n, nmb, 6), np.int32), costs=np.zeros((n, nmb, 2), np.int64),
+               coeffs=np.zeros((n, nmb, 256), np.int16), ccoeffs=np.zeros((n, nmb, 128), np.int16),
+               rec_y=np.zeros_like(y), rec_u=np.zeros_like(u), rec_v=np.zeros_like(v),
+               fallback=np.zeros((n, nmb), np.int32))
+    tab = mv_cost_table() if tab is None else tab
+    pr = None if props is None else np.ascontiguousarray(props, np.int32)
+    yc, uc, vc = (np.ascontiguousarray(a) for a in (y, u, v))
+    lib().or_closed_loop_clip(ptr(yc), ptr(uc), ptr(vc), n, cw, ch, pad, C.byref(params), ptr(tab, u16p),
+                              float(lambda_me), int(split_gate), qp, dz_div, None if pr is None else ptr(pr, i32p),
+                              int(prop_t), ptr(out["picks"], i32p), ptr(out["costs"], i64p), ptr(out["coeffs"], i16p),
+                              ptr(out["ccoeffs"], i16p), ptr(out["rec_y"]), ptr(out["rec_u"]), ptr(out["rec_v"]),
+                              ptr(out["fallback"], i32p))
+    return out
+
+
+class CavlcTables(C.Structure):
+    """or_cavlc_tables of h264_decoder.c."""
+    _fields_ = [("ct_len", (C.c_uint8 * 68) * 4), ("ct_bits", (C.c_uint8 * 68) * 4), ("cdc_len", C.c_uint8 * 20),
+                ("cdc_bits", C.c_uint8 * 20), ("tz_len", (C.c_uint8 * 16) * 15), ("tz_bits", (C.c_uint8 * 16) * 15),
+                ("ctz_len", (C.c_uint8 * 4) * 3), ("ctz_bits", (C.c_uint8 * 4) * 3), ("run_len", (C.c_uint8 * 15) * 7),
+                ("run_bits", (C.c_uint8 * 15) * 7), ("cbp_inter", C.c_uint8 * 48)]
+
+
+def reference_cavlc_tables():
+    """The decoder's VLC tables, as parsed from the reference's cavlc.rs
+    (tests/golden/reference_cavlc_tables.json)."""
+    import json
+    import os
+
+    here = os.path.dirname(os.path.abspath(__file__))
+    j = json.load(open(os.path.join(here, "..", "tests", "golden", "reference_cavlc_tables.json")))
+    t = CavlcTables()
+    flat = lambda a: [int(x) for row in (a if isinstance(a[0], list) else [a]) for x in row]
+    for field, key in (("ct_len", "COEFF_TOKEN_LEN"), ("ct_bits", "COEFF_TOKEN_BITS"),
+                       ("cdc_len", "CHROMA_DC_COEFF_TOKEN_LEN"), ("cdc_bits", "CHROMA_DC_COEFF_TOKEN_BITS"),
+                       ("tz_len", "TOTAL_ZEROS_LEN"), ("tz_bits", "TOTAL_ZEROS_BITS"),
+                       ("ctz_len", "CHROMA_DC_TOTAL_ZEROS_LEN"), ("ctz_bits", "CHROMA_DC_TOTAL_ZEROS_BITS"),
+                       ("run_len", "RUN_LEN"), ("run_bits", "RUN_BITS"), ("cbp_inter", "CBP_INTER")):
+        vals = flat(j[key])
+        dst = getattr(t, field)
+        C.memmove(C.addressof(dst), (C.c_uint8 * len(vals))(*vals), len(vals))
+    return t
+
+
+def decode_stream(data: bytes, cw: int, ch: int, max_frames: int):
+    """Frames (y, u, v) and the parsed picks / levels of a stream of the
+    library's subset (or_decode_stream); raises on a malformed stream."""
+    L = lib()
+    if not getattr(L, "_dec_ready", False):
+        L.or_decode_stream.argtypes = [u8p, C.c_size_t, C.POINTER(CavlcTables), C.c_int, C.c_int, C.c_int, u8p, u8p,
+                                       u8p, i32p, i16p, i16p]
+        L._dec_ready = True
+    nmb = (cw // 16) * (ch // 16)
+    y = np.zeros((max_frames, ch, cw), np.uint8)
+    u = np.zeros((max_frames, ch // 2, cw // 2), np.uint8)
+    v = np.zeros_like(u)
+    picks = np.zeros((max_frames, nmb, 6), np.int32)
+    coeffs = np.zeros((max_frames, nmb, 256), np.int16)
+    ccoeffs = np.zeros((max_frames, nmb, 128), np.int16)
+    buf = np.frombuffer(data, np.uint8).copy()
+    t = reference_cavlc_tables()
+    n = L.or_decode_stream(ptr(buf), len(buf), C.byref(t), cw, ch, max_frames, ptr(y), ptr(u), ptr(v),
+                           ptr(picks, i32p), ptr(coeffs, i16p), ptr(ccoeffs, i16p))
+    if n < 0:
+        raise ValueError(f"or_decode_stream: {n}")
+    return dict(y=y[:n], u=u[:n], v=v[:n], picks=picks[:n], coeffs=coeffs[:n], ccoeffs=ccoeffs[:n])

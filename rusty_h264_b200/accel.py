@@ -96,6 +96,21 @@ class TqChromaFrame(C.Structure):
                 ("d_coeffs", C.c_void_p), ("d_rec_u", C.c_void_p), ("d_rec_v", C.c_void_p)]
 
 
+class ClosedJob(C.Structure):
+    _fields_ = [("h_y", C.c_void_p), ("h_u", C.c_void_p), ("h_v", C.c_void_p), ("n", C.c_int32), ("cw", C.c_int32),
+                ("ch", C.c_int32), ("lambda_me", C.c_double), ("split_gate", C.c_int64), ("qp", C.c_int32),
+                ("dz_div", C.c_int32), ("net", C.c_void_p), ("fallback_t", C.c_int32), ("h_picks", C.c_void_p),
+                ("h_costs", C.c_void_p), ("h_coeffs", C.c_void_p), ("h_ccoeffs", C.c_void_p), ("h_rec_y", C.c_void_p),
+                ("h_rec_u", C.c_void_p), ("h_rec_v", C.c_void_p), ("h_props", C.c_void_p),
+                ("h_fallback", C.c_void_p)]
+
+
+class StreamFrames(C.Structure):
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("cw", C.c_int32), ("ch", C.c_int32), ("n", C.c_int32),
+                ("qp", C.c_int32), ("h_y0", C.c_void_p), ("h_u0", C.c_void_p), ("h_v0", C.c_void_p),
+                ("h_picks", C.c_void_p), ("h_coeffs", C.c_void_p), ("h_ccoeffs", C.c_void_p)]
+
+
 # Every entry point the header declares (checked by tests/test_capi_symbols.py).
 EXPORTS = (
     "h264a_version", "h264a_last_error", "h264a_ctx_create", "h264a_ctx_destroy", "h264a_sync",
@@ -108,7 +123,7 @@ EXPORTS = (
     "h264a_mc_tq_rec_frames", "h264a_mc_tq_chroma_frames", "h264a_deblock_frames", "h264a_me_tq_frames",
     "h264a_mvnet_create", "h264a_mvnet_destroy", "h264a_mvnet_set_params", "h264a_mvnet_get_params",
     "h264a_mvnet_forward", "h264a_mvnet_grads", "h264a_mvnet_train_step", "h264a_mvnet_propose",
-    "h264a_me_frames_learned",
+    "h264a_me_frames_learned", "h264a_pixel_path_closed", "h264a_write_stream_cavlc", "h264a_cavlc_table_code",
 )
 
 _lib = None
@@ -154,6 +169,9 @@ def load_library() -> C.CDLL:
     L.h264a_measure_int32_peak.argtypes = [vp, C.POINTER(C.c_double)]
     L.h264a_me_frames_noalloc.argtypes = [vp, i32, C.POINTER(MeParams), vp, vp]
     L.h264a_me_frames_learned.argtypes = [vp, vp, i32, C.POINTER(MeParams), vp]
+    L.h264a_pixel_path_closed.argtypes = [vp, C.POINTER(ClosedJob), C.POINTER(MeParams), vp]
+    L.h264a_write_stream_cavlc.argtypes = [C.POINTER(StreamFrames), vp, sz, C.POINTER(sz), vp]
+    L.h264a_cavlc_table_code.argtypes = [i32, i32, i32, i32, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L.h264a_mvnet_create.argtypes = [i32, C.c_uint64, C.POINTER(vp)]
     L.h264a_mvnet_destroy.argtypes = [vp]
     L.h264a_mvnet_set_params.argtypes = [vp, vp]
@@ -179,6 +197,30 @@ def mv_cost_table() -> np.ndarray:
     t = np.zeros(4096, np.uint16)
     load_library().h264a_build_mv_cost_table(t.ctypes.data_as(C.c_void_p))
     return t
+
+
+def write_stream_cavlc(y0, u0, v0, picks, coeffs, ccoeffs, qp: int, width: int = None, height: int = None):
+    """Annex-B bytes of the frame model's stream (h264a_write_stream_cavlc, host
+    only) and the bytes of each frame.  y0/u0/v0: frame 0; picks (n, nmb, 6),
+    coeffs (n, nmb, 256), ccoeffs (n, nmb, 128)."""
+    L = load_library()
+    ch, cw = y0.shape
+    n = picks.shape[0]
+    arrs = [np.ascontiguousarray(a) for a in (y0, u0, v0)] + [np.ascontiguousarray(picks, np.int32),
+                                                               np.ascontiguousarray(coeffs, np.int16),
+                                                               np.ascontiguousarray(ccoeffs, np.int16)]
+    sf = StreamFrames(width or cw, height or ch, cw, ch, n, qp, *[a.ctypes.data for a in arrs])
+    ln = C.c_size_t()
+    fb = np.zeros(n, np.int64)
+    rc = L.h264a_write_stream_cavlc(C.byref(sf), None, 0, C.byref(ln), None)
+    if rc != H264A_OK:
+        raise AccelError(rc, L.h264a_last_error().decode())
+    out = np.zeros(ln.value, np.uint8)
+    rc = L.h264a_write_stream_cavlc(C.byref(sf), out.ctypes.data_as(C.c_void_p), out.size, C.byref(ln),
+                                    fb.ctypes.data_as(C.c_void_p))
+    if rc != H264A_OK:
+        raise AccelError(rc, L.h264a_last_error().decode())
+    return out.tobytes(), fb
 
 
 def split_gate_for_qp(qp: int) -> int:
@@ -401,6 +443,31 @@ class Accel:
         v = C.c_double()
         self._check(self.L.h264a_measure_int32_peak(self.ctx, C.byref(v)))
         return v.value
+
+    # ---- the closed reconstruction loop -------------------------------------------
+    def pixel_path_closed(self, y: np.ndarray, u: np.ndarray, v: np.ndarray, params: MeParams, lambda_me: float,
+                          split_gate: int, qp: int, dz_div: int = 6, net=None, fallback_t: int = 0,
+                          tab: Optional[np.ndarray] = None):
+        """Luma y (n, ch, cw) and chroma u, v (n, ch/2, cw/2) u8 through the
+        closed loop; returns picks, costs, coeffs, ccoeffs, rec_y/u/v (and
+        props, fallback with a net)."""
+        n, ch, cw = y.shape
+        nmb = (cw // 16) * (ch // 16)
+        ins = [np.ascontiguousarray(a, np.uint8) for a in (y, u, v)]
+        out = dict(picks=np.zeros((n, nmb, 6), np.int32), costs=np.zeros((n, nmb, 2), np.int64),
+                   coeffs=np.zeros((n, nmb, 256), np.int16), ccoeffs=np.zeros((n, nmb, 128), np.int16),
+                   rec_y=np.zeros_like(ins[0]), rec_u=np.zeros_like(ins[1]), rec_v=np.zeros_like(ins[2]))
+        if net is not None:
+            out["props"] = np.zeros((n, nmb, 16), np.int32)
+            out["fallback"] = np.zeros((n, nmb), np.int32)
+        p = lambda k: out[k].ctypes.data if k in out else None
+        job = ClosedJob(ins[0].ctypes.data, ins[1].ctypes.data, ins[2].ctypes.data, n, cw, ch, float(lambda_me),
+                        int(split_gate), qp, dz_div, None if net is None else net.h.value, int(fallback_t),
+                        p("picks"), p("costs"), p("coeffs"), p("ccoeffs"), p("rec_y"), p("rec_u"), p("rec_v"),
+                        p("props"), p("fallback"))
+        self._check(self.L.h264a_pixel_path_closed(self.ctx, C.byref(job), C.byref(params),
+                                                   None if tab is None else tab.ctypes.data_as(C.c_void_p)))
+        return out
 
     # ---- end to end from host memory --------------------------------------------
     def pixel_path_prefetch(self, frames: np.ndarray):

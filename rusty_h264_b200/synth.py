@@ -28,6 +28,17 @@ def coded_luma(y: np.ndarray) -> np.ndarray:
     return np.ascontiguousarray(y[..., rows[:, None], cols[None, :]])
 
 
+def coded_chroma(c: np.ndarray) -> np.ndarray:
+    """4:2:0 chroma edge-clamped to half the coded luma size (the luma
+    rounded up to whole MBs), as the encoder prepares it
+    (crates/rusty_h264-encoder/src/mb16.rs:1504-1506)."""
+    h, w = c.shape[-2:]
+    ch, cw = (2 * h + 15) // 16 * 8, (2 * w + 15) // 16 * 8
+    rows = np.minimum(np.arange(ch), h - 1)
+    cols = np.minimum(np.arange(cw), w - 1)
+    return np.ascontiguousarray(c[..., rows[:, None], cols[None, :]])
+
+
 def _to_u8(x: np.ndarray) -> np.ndarray:
     return np.clip(np.rint(x), 0, 255).astype(np.uint8)
 
@@ -95,8 +106,11 @@ def _decimate_phases(tex4: np.ndarray) -> dict:
 
 
 def hd_clip(frames: int = 60, seed: int = 1, w: int = 1920, h: int = 1080, with_chroma: bool = False):
-    """Luma (and optionally chroma) of the 1080p synthetic workload, uint8."""
+    """Luma (and optionally chroma) of the 1080p synthetic workload, uint8.
+    Chroma (flat 128 plus sigma 1) comes from its own seeded stream, so the
+    luma is the same with or without it."""
     rng = np.random.default_rng(seed)
+    crng = np.random.default_rng([seed, 0xC4])
     # background texture at 4x, with margin for the whole clip's motion
     vx4, vy4 = 5, -2  # (1.25, -0.5) px/frame in quarter-pel units
     mx = abs(vx4) * frames // 4 + 8
@@ -134,6 +148,6 @@ def hd_clip(frames: int = 60, seed: int = 1, w: int = 1920, h: int = 1080, with_
         img += rng.normal(0.0, 1.5, (h, w)).astype(np.float32)
         ys[t] = _to_u8(img)
         if with_chroma:
-            us[t] = _to_u8(128 + rng.normal(0.0, 1.0, (h // 2, w // 2)))
-            vs[t] = _to_u8(128 + rng.normal(0.0, 1.0, (h // 2, w // 2)))
+            us[t] = _to_u8(128 + crng.normal(0.0, 1.0, (h // 2, w // 2)))
+            vs[t] = _to_u8(128 + crng.normal(0.0, 1.0, (h // 2, w // 2)))
     return ys, us, vs

@@ -1036,3 +1036,66 @@ def test_invalid_arguments_rejected_before_launch(acc, cif):
     rc = acc.L.h264a_block_metric(acc.ctx, 0, 12, 16, d.data_ptr(), d.data_ptr(), 16, d.data_ptr(), d.data_ptr(),
                                   None, None, 16, 1, d.data_ptr(), None)
     assert rc == -1
+
+
+# ---------------------------------------------------------------------------
+# The closed reconstruction loop (h264a_pixel_path_closed)
+# ---------------------------------------------------------------------------
+
+def _coded_yuv(y, u, v):
+    return synth.coded_luma(y), synth.coded_chroma(u), synth.coded_chroma(v)
+
+
+def _compare_closed(got, want, keys=("picks", "costs", "coeffs", "ccoeffs", "rec_y", "rec_u", "rec_v")):
+    for k in keys:
+        g, w = got[k], want[k]
+        if k == "picks":
+            g, w = g[..., :5], w[..., :5]
+        assert np.array_equal(g, w), (k, np.argwhere(g != w)[:3])
+
+
+def test_closed_loop_cif_30_frames_matches_oracle(acc):
+    """The CPU-runnable workload (CIF, 30 frames, QP 26) through the closed
+    loop: every frame's search runs on the deblocked reconstruction of the
+    frame before it; picks, costs, luma and chroma levels and every
+    reconstruction equal the oracle's."""
+    Y, U, V = _coded_yuv(*synth.cif_clip(30, 0))
+    qp = 26
+    lam = float(np.sqrt(A.frame_lambda(qp)))
+    gate = A.split_gate_for_qp(qp)
+    got = acc.pixel_path_closed(Y, U, V, A.default_me_params(), lam, gate, qp)
+    want = O.closed_loop_clip(Y, U, V, O.balanced_params(), lam, gate, qp)
+    _compare_closed(got, want)
+    assert (got["picks"][1:, :, 0] > 0).any()
+    # the reconstruction is not the source: the loop really closes
+    assert not np.array_equal(got["rec_y"][1:], Y[1:])
+
+
+def test_closed_loop_1080p_8_frames_matches_oracle(acc):
+    Y, U, V = _coded_yuv(*synth.hd_clip(8, 1, with_chroma=True))
+    qp = 27
+    lam = float(np.sqrt(A.frame_lambda(qp)) * 1.25)
+    gate = A.split_gate_for_qp(qp)
+    got = acc.pixel_path_closed(Y, U, V, A.default_me_params(), lam, gate, qp)
+    want = O.closed_loop_clip(Y, U, V, O.balanced_params(), lam, gate, qp)
+    _compare_closed(got, want)
+
+
+def test_closed_loop_learned_matches_oracle(acc):
+    """The learned search inside the closed loop: the proposals the network
+    made for each frame (from the source and the previous reconstruction)
+    fed to the oracle's closed loop give the same picks, levels and
+    reconstructions, with the same fallback flags."""
+    from rusty_h264_b200 import mvnet
+
+    Y, U, V = _coded_yuv(*synth.cif_clip(6, 4))
+    qp = 30
+    lam = float(np.sqrt(A.frame_lambda(qp)) * 1.25)
+    gate = A.split_gate_for_qp(qp)
+    net = mvnet.MvNet(acc, seed=21)
+    got = acc.pixel_path_closed(Y, U, V, A.default_me_params(), lam, gate, qp, net=net, fallback_t=100)
+    want = O.closed_loop_clip(Y, U, V, O.balanced_params(), lam, gate, qp, props=got["props"], prop_t=100)
+    _compare_closed(got, want)
+    assert np.array_equal(got["fallback"], want["fallback"])
+    assert (got["props"][1:] != 0).any()
+    net.close()
