@@ -60,6 +60,10 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--mixed", action="store_true",
                     help="also time plain-ME over the 16-stream mixed-resolution batch (not part of value)")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-proposal arm")
+    ap.add_argument("--learned-epochs", type=float, default=6.0)
+    ap.add_argument("--no-closed", action="store_true", help="skip the closed-loop and BD-rate records")
+    ap.add_argument("--bd-frames", type=int, default=16)
     return ap.parse_args()
 
 
@@ -181,6 +185,174 @@ def mixed_batch(acc, torch, streams, params, lam: float, gate: int):
             "me_mpx_s": round(px / (ms * 1e-3) / 1e6, 1), "launches": 1,
             "batched_equals_alone": True,
             "note": "plain-ME of all P frames, one reference; not part of value"}
+
+
+# Training clips of the learned proposals: the 1080p generator with seeds the
+# benchmarked clip (seed 1) does not use, at the four QPs of the BD-rate points.
+TRAIN_SEEDS = (100, 101, 102, 103)
+TRAIN_FRAMES = 16
+BD_QPS = (22, 27, 32, 37)
+
+
+def train_clip(seed):
+    from rusty_h264_b200 import synth
+
+    cache = os.path.join("/tmp", f"h264a_train_s{seed}_f{TRAIN_FRAMES}.npy")
+    if os.path.exists(cache):
+        return np.load(cache)
+    f = synth.coded_luma(synth.hd_clip(TRAIN_FRAMES, seed)[0])
+    try:
+        np.save(cache, f)
+    except OSError:
+        pass
+    return f
+
+
+def events_ms(torch, fn, reps=5, warm=2):
+    """Median CUDA-event time of fn() on the current stream."""
+    ts = []
+    for r in range(reps + warm):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        fn()
+        b.record()
+        torch.cuda.synchronize()
+        if r >= warm:
+            ts.append(a.elapsed_time(b))
+    return float(np.median(ts))
+
+
+def learned_arm(acc, torch, f, d_frames, planes, params, lam, gate, qp, plain_ms, plain_costs, epochs, train_clips):
+    """The learned-proposal arm at the benchmarked workload: the network
+    trained here by the library's kernels on clips of other seeds, then the
+    same pixel path with proposals (lookahead first for the guide MVs, the
+    proposals, learned ME, MC + T/Q), CUDA-event timed against the plain step's
+    ME; quality as the pick and 16x16 J against plain-ME's, and the fallback
+    rate."""
+    from rusty_h264_b200 import accel as A
+    from rusty_h264_b200 import mvnet
+
+    n, ch, cw = f.shape
+    nmb = (cw // 16) * (ch // 16)
+    t0 = time.perf_counter()
+    ts = mvnet.harvest(acc, train_clips, BD_QPS).finish()
+    harvest_s = time.perf_counter() - t0
+    net = mvnet.MvNet(acc, seed=1)
+    losses, train_s, steps = mvnet.train(net, ts, epochs=epochs, lr=2e-3, pairs_per_step=4, log_every=max(1, 10))
+    held = mvnet.harvest(acc, [f[:9]], (qp,)).finish()
+    topk = mvnet.evaluate_topk(net, held, (1, 8))
+    del held
+    half = torch.empty((n, ch // 2, cw // 2), dtype=torch.uint8, device=d_frames.device)
+    la = torch.empty((3, n, nmb, 2), dtype=torch.int32, device=d_frames.device)
+    props = torch.zeros((n, nmb, 16), dtype=torch.int32, device=d_frames.device)
+    picks = torch.zeros((n, nmb, 6), dtype=torch.int32, device=d_frames.device)
+    costs = torch.zeros((n, nmb, 2), dtype=torch.int64, device=d_frames.device)
+    coeffs = torch.zeros((n, nmb, 256), dtype=torch.int16, device=d_frames.device)
+    fb = torch.zeros((n, nmb), dtype=torch.int32, device=d_frames.device)
+    la_mvs = la[2]
+    pfr = [mvnet.MvnetFrame(d_frames[i].data_ptr(), d_frames[i - 1].data_ptr(), cw, ch, la_mvs[i].data_ptr(),
+                            props[i].data_ptr()) for i in range(1, n)]
+    T = 256
+    lfr = [A.MeLearnedFrame(A.MeFrame(A.Picture(d_frames[i].data_ptr(), planes[i - 1].data_ptr(), cw, ch, 32), lam,
+                                      gate, picks[i].data_ptr(), costs[i].data_ptr()), props[i].data_ptr(), T,
+                            fb[i].data_ptr()) for i in range(1, n)]
+    tqf = [A.TqFrame(A.Picture(d_frames[i].data_ptr(), planes[i - 1].data_ptr(), cw, ch, 32), picks[i].data_ptr(),
+                     qp, 6, coeffs[i].data_ptr()) for i in range(1, n)]
+    stage = {}
+
+    def lookahead():
+        acc._check(acc.L.h264a_downsample2x(acc.ctx, d_frames.data_ptr(), cw, ch, n, cw * ch, half.data_ptr(),
+                                            acc._stream()))
+        acc._check(acc.L.h264a_lookahead_costs(acc.ctx, d_frames.data_ptr(), half.data_ptr(), cw, ch, n, 2,
+                                               la[0].data_ptr(), la[1].data_ptr(), la_mvs.data_ptr(), acc._stream()))
+
+    def step():
+        acc.hpel_build(d_frames[: n - 1], 32, out=planes)
+        lookahead()
+        net.propose(pfr)
+        acc.me_frames_learned(lfr, params)
+        acc.mc_tq_frames(tqf)
+
+    step_ms = events_ms(torch, step)
+    stage["lookahead"] = events_ms(torch, lookahead)
+    stage["propose"] = events_ms(torch, lambda: net.propose(pfr))
+    stage["learned_me"] = events_ms(torch, lambda: acc.me_frames_learned(lfr, params))
+    acc.sync()
+    c = costs.cpu().numpy()[1:]
+    pc = plain_costs[1:]
+    out = {
+        "workload": "the same 60-frame 1080p clip and QP; proposals + learned 16x16 search, partitions as plain-ME",
+        "value": round(n * W * H / (step_ms * 1e-3) / 1e6, 2), "unit": "Mpx/s", "ms_per_step": round(step_ms, 3),
+        "stage_ms": {k: round(v, 3) for k, v in stage.items()},
+        "plain_me_ms": round(plain_ms, 3), "fallback_t": T,
+        "fallback_rate": round(float(fb.cpu().numpy()[1:].mean()), 4),
+        "J_pick_vs_plain": round(float(c[:, :, 0].sum() / pc[:, :, 0].sum() - 1), 5),
+        "J16_vs_plain": round(float(c[:, :, 1].sum() / pc[:, :, 1].sum() - 1), 5),
+        "training": {"items": len(ts), "mbs": int(len(ts) * nmb), "qps": list(BD_QPS),
+                     "clips": f"{len(train_clips)} x {TRAIN_FRAMES} frames, 1080p generator seeds {list(TRAIN_SEEDS)}",
+                     "steps": steps, "batch_mbs": int(4 * nmb), "seconds": round(train_s, 2),
+                     "harvest_seconds": round(harvest_s, 2), "loss_first": round(losses[0][1], 4),
+                     "loss_last": round(losses[-1][1], 4)},
+        "heldout_topk": {"top1": round(topk[1], 4), "top8": round(topk[8], 4),
+                         "note": "the benchmarked clip (not trained on), frames 1-8, plain 16x16 MVs as labels"},
+    }
+    del ts
+    return out, net
+
+
+def closed_loop_records(acc, f, params, lam_scale, net, bd_frames):
+    """The closed reconstruction loop over the benchmarked clip (with its
+    chroma), plain and learned, wall-clock timed through the synchronous host
+    entry (uploads, per-frame wavefronts, downloads); then the BD-rate of the
+    learned search against plain-ME over QP 22/27/32/37 on the clip's first
+    bd_frames frames: rate = the Annex-B bytes of the P frames
+    (h264a_write_stream_cavlc), PSNR = luma of the P frames' reconstruction
+    (the tests check that the decoder reproduces it exactly)."""
+    from rusty_h264_b200 import accel as A
+    from rusty_h264_b200 import bdrate, synth
+
+    n, ch, cw = f.shape
+    _, u, v = synth.hd_clip(n, 1, with_chroma=True)
+    U, V = synth.coded_chroma(u), synth.coded_chroma(v)
+    qp = QP
+    lam = float(np.sqrt(A.frame_lambda(qp)) * lam_scale)
+    gate = A.split_gate_for_qp(qp)
+    rec = {}
+    for name, nt in (("plain", None), ("learned", net)):
+        if name == "learned" and nt is None:
+            continue
+        acc.pixel_path_closed(f[:4], U[:4], V[:4], params, lam, gate, qp, net=nt, fallback_t=256)  # warm-up
+        t0 = time.perf_counter()
+        r = acc.pixel_path_closed(f, U, V, params, lam, gate, qp, net=nt, fallback_t=256)
+        dt = time.perf_counter() - t0
+        rec[name] = {"ms_per_clip": round(dt * 1e3, 2), "mpx_s": round(n * W * H / dt / 1e6, 2),
+                     "psnr_p_frames": round(bdrate.psnr(f[1:, :H], r["rec_y"][1:, :H]), 3)}
+        if name == "learned":
+            rec[name]["fallback_rate"] = round(float(r["fallback"][1:].mean()), 4)
+    curves = {"plain": [], "learned": []}
+    m = bd_frames
+    for q in BD_QPS:
+        lq = float(np.sqrt(A.frame_lambda(q)) * lam_scale)
+        gq = A.split_gate_for_qp(q)
+        for name, nt in (("plain", None), ("learned", net)):
+            if name == "learned" and nt is None:
+                continue
+            r = acc.pixel_path_closed(f[:m], U[:m], V[:m], params, lq, gq, q, net=nt, fallback_t=256)
+            data, fbytes = A.write_stream_cavlc(f[0], U[0], V[0], r["picks"], r["coeffs"], r["ccoeffs"], q, W, H)
+            curves[name].append((float(fbytes[1:].sum()), bdrate.psnr(f[1:m, :H], r["rec_y"][1:m, :H]),
+                                 float(len(data))))
+    out = {"workload": f"the 60-frame 1080p clip with chroma, QP {qp}; ME on the deblocked reconstruction of the "
+                       "previous frame, frame 0 coded losslessly (I_PCM)", **rec}
+    if curves["learned"]:
+        out["bd_rate"] = {
+            "qps": list(BD_QPS), "frames": m,
+            "plain": [(round(r, 0), round(d, 3)) for r, d, _ in curves["plain"]],
+            "learned": [(round(r, 0), round(d, 3)) for r, d, _ in curves["learned"]],
+            "bd_rate_pct_learned_vs_plain": round(bdrate.bd_rate([c[:2] for c in curves["plain"]],
+                                                                 [c[:2] for c in curves["learned"]]), 3),
+            "rate": "bytes of the P frames' NAL units (CAVLC, Baseline); PSNR of the P frames' luma",
+        }
+    return out
 
 
 class ClockSampler:
@@ -402,6 +574,7 @@ def run_ours(args, ws, rank, local):
     from rusty_h264_b200 import accel as A
 
     mixed_streams = mixed_inputs() if args.mixed and rank == 0 else None  # host work, before any GPU call
+    train_clips = [train_clip(s) for s in TRAIN_SEEDS] if not args.no_learned and rank == 0 else None
     torch.cuda.set_device(local)
     acc = A.Accel(local)
     n = args.frames
@@ -670,6 +843,15 @@ def run_ours(args, ws, rank, local):
                                 "cpu": cpu_model(), "stages": cpu_stages(sample, lam, gate)}
     if args.mixed and rank == 0:
         line["mixed_batch"] = mixed_batch(acc, torch, mixed_streams, params, lam, gate)
+    net = None
+    if not args.no_learned and rank == 0:
+        plain_costs = costs.cpu().numpy()
+        line["learned"], net = learned_arm(acc, torch, f, d_frames, planes, params, lam, gate, qp, stage["me"],
+                                           plain_costs, args.learned_epochs, train_clips)
+    if not args.no_closed and rank == 0:
+        line["closed_loop"] = closed_loop_records(acc, f, params, 1.25, net, args.bd_frames)
+    if net is not None:
+        net.close()
     if rank == 0:
         print(json.dumps(line), flush=True)
     acc.close()
