@@ -451,6 +451,31 @@ typedef struct {
 } h264a_closed_job;
 H264A_API int h264a_pixel_path_closed(h264a_ctx *ctx, const h264a_closed_job *job, const h264a_me_params *params,
                                       const uint16_t *h_mv_cost_tab);
+/* The same loop on device buffers, enqueued on `stream` (no allocation, no
+ * host copy): the caller passes the n source frames, room for their
+ * reconstruction (frame 0 is copied from the source), one picture's planes
+ * as scratch (4*(cw+64)*(ch+64) bytes), the outputs (levels 16-byte aligned,
+ * chroma 4-byte aligned), and with a net the proposals buffer (16 i32/MB per
+ * frame), optional fallback flags and the guide MVs (2 i32/MB per frame, the
+ * lookahead's, or NULL). */
+typedef struct {
+    const uint8_t *d_y, *d_u, *d_v;
+    uint8_t *d_rec_y, *d_rec_u, *d_rec_v;
+    uint8_t *d_planes;
+    int32_t n, cw, ch;
+    double lambda_me;
+    int64_t split_gate;
+    int32_t qp, dz_div;
+    h264a_mvnet *net;
+    int32_t fallback_t;
+    const int32_t *d_guide_mvs;
+    int32_t *d_picks;
+    int64_t *d_costs;
+    int16_t *d_coeffs, *d_ccoeffs;
+    int32_t *d_props, *d_fallback;
+} h264a_closed_dev;
+H264A_API int h264a_closed_frames(h264a_ctx *ctx, const h264a_closed_dev *job, const h264a_me_params *params,
+                                  void *stream);
 
 /* ---- Annex-B output of the frame model (host) ---------------------------------- */
 /* A decodable H.264 Baseline stream (CAVLC) of n frames of the frame model:

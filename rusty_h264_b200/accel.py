@@ -111,6 +111,16 @@ class StreamFrames(C.Structure):
                 ("h_picks", C.c_void_p), ("h_coeffs", C.c_void_p), ("h_ccoeffs", C.c_void_p)]
 
 
+class ClosedDev(C.Structure):
+    _fields_ = [("d_y", C.c_void_p), ("d_u", C.c_void_p), ("d_v", C.c_void_p), ("d_rec_y", C.c_void_p),
+                ("d_rec_u", C.c_void_p), ("d_rec_v", C.c_void_p), ("d_planes", C.c_void_p), ("n", C.c_int32),
+                ("cw", C.c_int32), ("ch", C.c_int32), ("lambda_me", C.c_double), ("split_gate", C.c_int64),
+                ("qp", C.c_int32), ("dz_div", C.c_int32), ("net", C.c_void_p), ("fallback_t", C.c_int32),
+                ("d_guide_mvs", C.c_void_p), ("d_picks", C.c_void_p), ("d_costs", C.c_void_p),
+                ("d_coeffs", C.c_void_p), ("d_ccoeffs", C.c_void_p), ("d_props", C.c_void_p),
+                ("d_fallback", C.c_void_p)]
+
+
 # Every entry point the header declares (checked by tests/test_capi_symbols.py).
 EXPORTS = (
     "h264a_version", "h264a_last_error", "h264a_ctx_create", "h264a_ctx_destroy", "h264a_sync",
@@ -124,6 +134,7 @@ EXPORTS = (
     "h264a_mvnet_create", "h264a_mvnet_destroy", "h264a_mvnet_set_params", "h264a_mvnet_get_params",
     "h264a_mvnet_forward", "h264a_mvnet_grads", "h264a_mvnet_train_step", "h264a_mvnet_propose",
     "h264a_me_frames_learned", "h264a_pixel_path_closed", "h264a_write_stream_cavlc", "h264a_cavlc_table_code",
+    "h264a_closed_frames",
 )
 
 _lib = None
@@ -170,6 +181,7 @@ def load_library() -> C.CDLL:
     L.h264a_me_frames_noalloc.argtypes = [vp, i32, C.POINTER(MeParams), vp, vp]
     L.h264a_me_frames_learned.argtypes = [vp, vp, i32, C.POINTER(MeParams), vp]
     L.h264a_pixel_path_closed.argtypes = [vp, C.POINTER(ClosedJob), C.POINTER(MeParams), vp]
+    L.h264a_closed_frames.argtypes = [vp, C.POINTER(ClosedDev), C.POINTER(MeParams), vp]
     L.h264a_write_stream_cavlc.argtypes = [C.POINTER(StreamFrames), vp, sz, C.POINTER(sz), vp]
     L.h264a_cavlc_table_code.argtypes = [i32, i32, i32, i32, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L.h264a_mvnet_create.argtypes = [i32, C.c_uint64, C.POINTER(vp)]
@@ -468,6 +480,11 @@ class Accel:
         self._check(self.L.h264a_pixel_path_closed(self.ctx, C.byref(job), C.byref(params),
                                                    None if tab is None else tab.ctypes.data_as(C.c_void_p)))
         return out
+
+    def closed_frames(self, job: ClosedDev, params: MeParams):
+        """The closed loop on device buffers (h264a_closed_frames), enqueued on
+        the current stream."""
+        self._check(self.L.h264a_closed_frames(self.ctx, C.byref(job), C.byref(params), self._stream()))
 
     # ---- end to end from host memory --------------------------------------------
     def pixel_path_prefetch(self, frames: np.ndarray):

@@ -142,6 +142,7 @@ extern "C" int h264a_ctx_destroy(h264a_ctx* ctx) {
     for (int i = 0; i < NUM_QUEUES; i++)
         if (ctx->q[i].d_flags) cudaFree(ctx->q[i].d_flags);
     if (ctx->pp_buf) cudaFree(ctx->pp_buf);
+    if (ctx->cl_buf) cudaFree(ctx->cl_buf);
     if (ctx->me_tab) cudaFree(ctx->me_tab);
     if (ctx->me_tab_host) cudaFreeHost(ctx->me_tab_host);
     if (ctx->me_tab_ev) cudaEventDestroy(ctx->me_tab_ev);

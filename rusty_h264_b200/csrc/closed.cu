@@ -20,26 +20,94 @@
 
 #include "h264accel_internal.h"
 
+using namespace h264a;
+
 namespace {
 
-struct DevBuf {
-    void* p = nullptr;
-    ~DevBuf() {
-        if (p) cudaFree(p);
-    }
-};
+int check_geometry(int n, int cw, int ch, int qp, int dz_div) {
+    if (n < 1 || cw < 16 || ch < 16 || cw % 16 || ch % 16 || (long long)cw * ch > (1LL << 26))
+        return fail(H264A_E_ARG, "closed loop: frames must be MB-aligned and at least one");
+    if (qp < 0 || qp > 51 || dz_div < 1) return fail(H264A_E_ARG, "closed loop: qp out of 0..51 or dz_div < 1");
+    return H264A_OK;
+}
 
-int dev_alloc(DevBuf& b, size_t bytes) {
-    if (cudaMalloc(&b.p, bytes) != cudaSuccess) {
-        cudaGetLastError();
-        return h264a::fail(H264A_E_NOMEM, "pixel_path_closed: cudaMalloc failed");
+// The per-frame launches of the loop on device buffers (checked by the caller).
+int closed_run(h264a_ctx* ctx, const h264a_closed_dev& j, const h264a_me_params& prm, cudaStream_t st) {
+    const int n = j.n, cw = j.cw, ch = j.ch, pad = 32;
+    const int nmb = (cw / 16) * (ch / 16);
+    const size_t fs = size_t(cw) * ch, cs = fs / 4;
+    H264A_CUDA(cudaMemsetAsync(j.d_picks, 0, sizeof(int32_t) * 6 * nmb, st));
+    H264A_CUDA(cudaMemsetAsync(j.d_costs, 0, sizeof(int64_t) * 2 * nmb, st));
+    H264A_CUDA(cudaMemsetAsync(j.d_coeffs, 0, sizeof(int16_t) * 256 * nmb, st));
+    H264A_CUDA(cudaMemsetAsync(j.d_ccoeffs, 0, sizeof(int16_t) * 128 * nmb, st));
+    if (j.net) {
+        H264A_CUDA(cudaMemsetAsync(j.d_props, 0, sizeof(int32_t) * 16 * nmb, st));
+        if (j.d_fallback) H264A_CUDA(cudaMemsetAsync(j.d_fallback, 0, sizeof(int32_t) * nmb, st));
+    }
+    // frame 0: coded losslessly, its reconstruction is the source
+    H264A_CUDA(cudaMemcpyAsync(j.d_rec_y, j.d_y, fs, cudaMemcpyDeviceToDevice, st));
+    H264A_CUDA(cudaMemcpyAsync(j.d_rec_u, j.d_u, cs, cudaMemcpyDeviceToDevice, st));
+    H264A_CUDA(cudaMemcpyAsync(j.d_rec_v, j.d_v, cs, cudaMemcpyDeviceToDevice, st));
+    for (int f = 1; f < n; f++) {
+        const uint8_t* ry = j.d_rec_y + (f - 1) * fs;
+        int rc = h264a_hpel_build(ctx, ry, cw, ch, pad, 1, fs, j.d_planes, st);
+        if (rc) return rc;
+        h264a_me_frame mf;
+        mf.pic = h264a_picture{j.d_y + f * fs, j.d_planes, cw, ch, pad};
+        mf.lambda_me = j.lambda_me;
+        mf.split_gate = j.split_gate;
+        mf.d_picks = j.d_picks + 6LL * nmb * f;
+        mf.d_costs = j.d_costs + 2LL * nmb * f;
+        if (j.net) {
+            h264a_mvnet_frame nf{j.d_y + f * fs, ry, cw, ch, j.d_guide_mvs ? j.d_guide_mvs + 2LL * nmb * f : nullptr,
+                                 j.d_props + 16LL * nmb * f};
+            rc = h264a_mvnet_propose(j.net, &nf, 1, st);
+            if (rc) return rc;
+            h264a_me_learned_frame lf{mf, j.d_props + 16LL * nmb * f, j.fallback_t,
+                                      j.d_fallback ? j.d_fallback + (long long)nmb * f : nullptr};
+            rc = h264a_me_frames_learned(ctx, &lf, 1, &prm, st);
+        } else {
+            rc = h264a_me_frames(ctx, &mf, 1, &prm, st);
+        }
+        if (rc) return rc;
+        h264a_tq_rec_frame tr;
+        tr.tq = h264a_tq_frame{mf.pic, mf.d_picks, j.qp, j.dz_div, j.d_coeffs + 256LL * nmb * f};
+        tr.d_rec = j.d_rec_y + f * fs;
+        rc = h264a_mc_tq_rec_frames(ctx, &tr, 1, st);
+        if (rc) return rc;
+        h264a_tq_chroma_frame cf{j.d_u + f * cs, j.d_v + f * cs, j.d_rec_u + (f - 1) * cs, j.d_rec_v + (f - 1) * cs,
+                                 cw, ch, mf.d_picks, j.qp, j.d_ccoeffs + 128LL * nmb * f, j.d_rec_u + f * cs,
+                                 j.d_rec_v + f * cs};
+        rc = h264a_mc_tq_chroma_frames(ctx, &cf, 1, st);
+        if (rc) return rc;
+        h264a_deblock_frame df{j.d_rec_y + f * fs, j.d_rec_u + f * cs, j.d_rec_v + f * cs, cw, ch, mf.d_picks,
+                               j.d_coeffs + 256LL * nmb * f, j.qp, 0, 0, 0};
+        rc = h264a_deblock_frames(ctx, &df, 1, st);
+        if (rc) return rc;
     }
     return H264A_OK;
 }
 
 }  // namespace
 
-using namespace h264a;
+extern "C" int h264a_closed_frames(h264a_ctx* ctx, const h264a_closed_dev* job, const h264a_me_params* params,
+                                   void* stream) {
+    if (!ctx || !job || !params) return fail(H264A_E_ARG, "closed_frames: null pointer");
+    const h264a_closed_dev& j = *job;
+    int rc = check_geometry(j.n, j.cw, j.ch, j.qp, j.dz_div);
+    if (rc) return rc;
+    if (!j.d_y || !j.d_u || !j.d_v || !j.d_rec_y || !j.d_rec_u || !j.d_rec_v || !j.d_planes || !j.d_picks ||
+        !j.d_costs || !j.d_coeffs || !j.d_ccoeffs || (j.net && !j.d_props))
+        return fail(H264A_E_ARG, "closed_frames: null device buffer");
+    if (((reinterpret_cast<uintptr_t>(j.d_coeffs) | reinterpret_cast<uintptr_t>(j.d_ccoeffs)) & 15) ||
+        ((reinterpret_cast<uintptr_t>(j.d_u) | reinterpret_cast<uintptr_t>(j.d_v) |
+          reinterpret_cast<uintptr_t>(j.d_rec_u) | reinterpret_cast<uintptr_t>(j.d_rec_v)) & 3))
+        return fail(H264A_E_ARG, "closed_frames: levels must be 16-byte and chroma 4-byte aligned");
+    if (j.net && j.fallback_t < 0) return fail(H264A_E_ARG, "closed_frames: negative fallback threshold");
+    if ((params->mv_cost_kind == 1 || params->mv_cost_kind == 2) && !params->d_mv_cost_tab)
+        return fail(H264A_E_ARG, "closed_frames: mv cost kinds 1 and 2 need d_mv_cost_tab");
+    return closed_run(ctx, j, *params, reinterpret_cast<cudaStream_t>(stream));
+}
 
 extern "C" int h264a_pixel_path_closed(h264a_ctx* ctx, const h264a_closed_job* job, const h264a_me_params* params,
                                        const uint16_t* h_mv_cost_tab) {
@@ -47,123 +115,102 @@ extern "C" int h264a_pixel_path_closed(h264a_ctx* ctx, const h264a_closed_job* j
     const int n = job->n, cw = job->cw, ch = job->ch;
     if (!job->h_y || !job->h_u || !job->h_v || !job->h_picks || !job->h_costs)
         return fail(H264A_E_ARG, "pixel_path_closed: null frame or output pointer");
-    if (n < 1 || cw < 16 || ch < 16 || cw % 16 || ch % 16 || (long long)cw * ch > (1LL << 26))
-        return fail(H264A_E_ARG, "pixel_path_closed: frames must be MB-aligned and at least one");
-    if (job->qp < 0 || job->qp > 51 || job->dz_div < 1) return fail(H264A_E_ARG, "pixel_path_closed: bad qp/dz_div");
+    int rc = check_geometry(n, cw, ch, job->qp, job->dz_div);
+    if (rc) return rc;
     if (job->net && job->fallback_t < 0) return fail(H264A_E_ARG, "pixel_path_closed: negative fallback threshold");
     if ((params->mv_cost_kind == 1 || params->mv_cost_kind == 2) && !h_mv_cost_tab)
         return fail(H264A_E_ARG, "pixel_path_closed: mv cost kinds 1 and 2 need the table");
     H264A_CUDA(cudaSetDevice(ctx->device));
     cudaStream_t st = ctx->stream;
-    const int pad = 32, pw = cw + 2 * pad, ph = ch + 2 * pad;
-    const int mb_w = cw / 16, mb_h = ch / 16, nmb = mb_w * mb_h;
-    const size_t fs = size_t(cw) * ch, cs = fs / 4, ps4 = size_t(4) * pw * ph;
-    // device layout: src Y|U|V, rec Y|U|V (n frames each), planes (one
-    // picture), picks, costs, luma and chroma levels, proposals, lookahead
-    DevBuf b_src, b_rec, b_planes, b_picks, b_costs, b_coef, b_ccoef, b_tab, b_props, b_fb, b_half, b_la;
-    int rc = dev_alloc(b_src, n * (fs + 2 * cs));
-    if (!rc) rc = dev_alloc(b_rec, n * (fs + 2 * cs));
-    if (!rc) rc = dev_alloc(b_planes, ps4);
-    if (!rc) rc = dev_alloc(b_picks, sizeof(int32_t) * 6 * nmb * n);
-    if (!rc) rc = dev_alloc(b_costs, sizeof(int64_t) * 2 * nmb * n);
-    if (!rc) rc = dev_alloc(b_coef, sizeof(int16_t) * 256 * nmb * n);
-    if (!rc) rc = dev_alloc(b_ccoef, sizeof(int16_t) * 128 * nmb * n);
-    if (!rc) rc = dev_alloc(b_tab, sizeof(uint16_t) * 4096);
-    if (!rc && job->net) rc = dev_alloc(b_props, sizeof(int32_t) * 16 * nmb * n);
-    if (!rc && job->net) rc = dev_alloc(b_fb, sizeof(int32_t) * nmb * n);
-    if (!rc && job->net) rc = dev_alloc(b_half, n * fs / 4);
-    if (!rc && job->net) rc = dev_alloc(b_la, sizeof(int32_t) * 4 * nmb * n);
-    if (rc) return rc;
-    uint8_t* sy = static_cast<uint8_t*>(b_src.p);
-    uint8_t* su = sy + n * fs;
-    uint8_t* sv = su + n * cs;
-    uint8_t* ry = static_cast<uint8_t*>(b_rec.p);
-    uint8_t* ru = ry + n * fs;
-    uint8_t* rv = ru + n * cs;
-    uint8_t* planes = static_cast<uint8_t*>(b_planes.p);
-    int32_t* picks = static_cast<int32_t*>(b_picks.p);
-    int64_t* costs = static_cast<int64_t*>(b_costs.p);
-    int16_t* coef = static_cast<int16_t*>(b_coef.p);
-    int16_t* ccoef = static_cast<int16_t*>(b_ccoef.p);
-    int32_t* props = static_cast<int32_t*>(b_props.p);
-    int32_t* fb = static_cast<int32_t*>(b_fb.p);
-    H264A_CUDA(cudaMemcpyAsync(sy, job->h_y, n * fs, cudaMemcpyHostToDevice, st));
-    H264A_CUDA(cudaMemcpyAsync(su, job->h_u, n * cs, cudaMemcpyHostToDevice, st));
-    H264A_CUDA(cudaMemcpyAsync(sv, job->h_v, n * cs, cudaMemcpyHostToDevice, st));
+    const int pw = cw + 64, ph = ch + 64, nmb = (cw / 16) * (ch / 16);
+    const size_t fs = size_t(cw) * ch, cs = fs / 4;
+    // one cached device buffer, 256-byte aligned parts: src Y|U|V, rec Y|U|V,
+    // planes, picks, costs, luma and chroma levels, mv-cost table, and with a
+    // net the proposals, fallback flags, half-res frames and lookahead outputs
+    size_t off = 0;
+    auto part = [&](size_t bytes) {
+        const size_t o = off;
+        off += (bytes + 255) & ~size_t(255);
+        return o;
+    };
+    const size_t o_sy = part(n * fs), o_su = part(n * cs), o_sv = part(n * cs);
+    const size_t o_ry = part(n * fs), o_ru = part(n * cs), o_rv = part(n * cs);
+    const size_t o_pl = part(size_t(4) * pw * ph), o_pk = part(sizeof(int32_t) * 6 * nmb * n);
+    const size_t o_co = part(sizeof(int64_t) * 2 * nmb * n), o_lv = part(sizeof(int16_t) * 256 * nmb * n);
+    const size_t o_cl = part(sizeof(int16_t) * 128 * nmb * n), o_tab = part(sizeof(uint16_t) * 4096);
+    size_t o_pr = 0, o_fb = 0, o_half = 0, o_la = 0;
+    if (job->net) {
+        o_pr = part(sizeof(int32_t) * 16 * nmb * n);
+        o_fb = part(sizeof(int32_t) * nmb * n);
+        o_half = part(n * fs / 4);
+        o_la = part(sizeof(int32_t) * 4 * nmb * n);
+    }
+    if (off > ctx->cl_bytes) {
+        if (ctx->cl_buf) cudaFree(ctx->cl_buf);
+        ctx->cl_buf = nullptr;
+        ctx->cl_bytes = 0;
+        if (cudaMalloc(&ctx->cl_buf, off) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(H264A_E_NOMEM, "pixel_path_closed: cudaMalloc failed");
+        }
+        ctx->cl_bytes = off;
+    }
+    char* b = static_cast<char*>(ctx->cl_buf);
+    h264a_closed_dev j;
+    memset(&j, 0, sizeof j);
+    j.d_y = reinterpret_cast<uint8_t*>(b + o_sy);
+    j.d_u = reinterpret_cast<uint8_t*>(b + o_su);
+    j.d_v = reinterpret_cast<uint8_t*>(b + o_sv);
+    j.d_rec_y = reinterpret_cast<uint8_t*>(b + o_ry);
+    j.d_rec_u = reinterpret_cast<uint8_t*>(b + o_ru);
+    j.d_rec_v = reinterpret_cast<uint8_t*>(b + o_rv);
+    j.d_planes = reinterpret_cast<uint8_t*>(b + o_pl);
+    j.n = n; j.cw = cw; j.ch = ch;
+    j.lambda_me = job->lambda_me; j.split_gate = job->split_gate; j.qp = job->qp; j.dz_div = job->dz_div;
+    j.net = job->net; j.fallback_t = job->fallback_t;
+    j.d_picks = reinterpret_cast<int32_t*>(b + o_pk);
+    j.d_costs = reinterpret_cast<int64_t*>(b + o_co);
+    j.d_coeffs = reinterpret_cast<int16_t*>(b + o_lv);
+    j.d_ccoeffs = reinterpret_cast<int16_t*>(b + o_cl);
+    H264A_CUDA(cudaMemcpyAsync(const_cast<uint8_t*>(j.d_y), job->h_y, n * fs, cudaMemcpyHostToDevice, st));
+    H264A_CUDA(cudaMemcpyAsync(const_cast<uint8_t*>(j.d_u), job->h_u, n * cs, cudaMemcpyHostToDevice, st));
+    H264A_CUDA(cudaMemcpyAsync(const_cast<uint8_t*>(j.d_v), job->h_v, n * cs, cudaMemcpyHostToDevice, st));
     h264a_me_params prm = *params;
     if (h_mv_cost_tab) {
-        H264A_CUDA(cudaMemcpyAsync(b_tab.p, h_mv_cost_tab, sizeof(uint16_t) * 4096, cudaMemcpyHostToDevice, st));
-        prm.d_mv_cost_tab = static_cast<const uint16_t*>(b_tab.p);
+        H264A_CUDA(cudaMemcpyAsync(b + o_tab, h_mv_cost_tab, sizeof(uint16_t) * 4096, cudaMemcpyHostToDevice, st));
+        prm.d_mv_cost_tab = reinterpret_cast<const uint16_t*>(b + o_tab);
     }
-    H264A_CUDA(cudaMemsetAsync(picks, 0, sizeof(int32_t) * 6 * nmb, st));
-    H264A_CUDA(cudaMemsetAsync(costs, 0, sizeof(int64_t) * 2 * nmb, st));
-    H264A_CUDA(cudaMemsetAsync(coef, 0, sizeof(int16_t) * 256 * nmb, st));
-    H264A_CUDA(cudaMemsetAsync(ccoef, 0, sizeof(int16_t) * 128 * nmb, st));
-    // frame 0: coded losslessly, its reconstruction is the source
-    H264A_CUDA(cudaMemcpyAsync(ry, sy, fs, cudaMemcpyDeviceToDevice, st));
-    H264A_CUDA(cudaMemcpyAsync(ru, su, cs, cudaMemcpyDeviceToDevice, st));
-    H264A_CUDA(cudaMemcpyAsync(rv, sv, cs, cudaMemcpyDeviceToDevice, st));
-    int32_t* la_mvs = nullptr;
     if (job->net) {
         // guide MVs of the proposals: the HalfRes lookahead over the source
         // frames, known before any search runs
-        H264A_CUDA(cudaMemsetAsync(props, 0, sizeof(int32_t) * 16 * nmb, st));
-        H264A_CUDA(cudaMemsetAsync(fb, 0, sizeof(int32_t) * nmb, st));
-        uint8_t* half = static_cast<uint8_t*>(b_half.p);
-        int32_t* la = static_cast<int32_t*>(b_la.p);
-        la_mvs = la + 2 * nmb * n;
-        rc = h264a_downsample2x(ctx, sy, cw, ch, n, fs, half, st);
-        if (!rc) rc = h264a_lookahead_costs(ctx, sy, half, cw, ch, n, 2, la, la + nmb * n, la_mvs, st);
+        j.d_props = reinterpret_cast<int32_t*>(b + o_pr);
+        j.d_fallback = reinterpret_cast<int32_t*>(b + o_fb);
+        uint8_t* half = reinterpret_cast<uint8_t*>(b + o_half);
+        int32_t* la = reinterpret_cast<int32_t*>(b + o_la);
+        j.d_guide_mvs = la + 2 * nmb * n;
+        rc = h264a_downsample2x(ctx, j.d_y, cw, ch, n, fs, half, st);
+        if (!rc) rc = h264a_lookahead_costs(ctx, j.d_y, half, cw, ch, n, 2, la, la + nmb * n, la + 2 * nmb * n, st);
         if (rc) return rc;
     }
-    for (int f = 1; f < n && !rc; f++) {
-        rc = h264a_hpel_build(ctx, ry + (f - 1) * fs, cw, ch, pad, 1, fs, planes, st);
-        if (rc) break;
-        h264a_me_frame mf;
-        mf.pic = h264a_picture{sy + f * fs, planes, cw, ch, pad};
-        mf.lambda_me = job->lambda_me;
-        mf.split_gate = job->split_gate;
-        mf.d_picks = picks + 6LL * nmb * f;
-        mf.d_costs = costs + 2LL * nmb * f;
-        if (job->net) {
-            h264a_mvnet_frame nf{sy + f * fs, ry + (f - 1) * fs, cw, ch, la_mvs + 2LL * nmb * f, props + 16LL * nmb * f};
-            rc = h264a_mvnet_propose(job->net, &nf, 1, st);
-            if (rc) break;
-            h264a_me_learned_frame lf{mf, props + 16LL * nmb * f, job->fallback_t, fb + (long long)nmb * f};
-            rc = h264a_me_frames_learned(ctx, &lf, 1, &prm, st);
-        } else {
-            rc = h264a_me_frames(ctx, &mf, 1, &prm, st);
-        }
-        if (rc) break;
-        h264a_tq_rec_frame tr;
-        tr.tq = h264a_tq_frame{mf.pic, mf.d_picks, job->qp, job->dz_div, coef + 256LL * nmb * f};
-        tr.d_rec = ry + f * fs;
-        rc = h264a_mc_tq_rec_frames(ctx, &tr, 1, st);
-        if (rc) break;
-        h264a_tq_chroma_frame cf{su + f * cs, sv + f * cs, ru + (f - 1) * cs, rv + (f - 1) * cs, cw, ch, mf.d_picks,
-                                 job->qp, ccoef + 128LL * nmb * f, ru + f * cs, rv + f * cs};
-        rc = h264a_mc_tq_chroma_frames(ctx, &cf, 1, st);
-        if (rc) break;
-        h264a_deblock_frame df{ry + f * fs, ru + f * cs, rv + f * cs, cw, ch, mf.d_picks, coef + 256LL * nmb * f,
-                               job->qp, 0, 0, 0};
-        rc = h264a_deblock_frames(ctx, &df, 1, st);
-    }
+    rc = closed_run(ctx, j, prm, st);
     if (rc) {
         cudaStreamSynchronize(st);
         return rc;
     }
-    H264A_CUDA(cudaMemcpyAsync(job->h_picks, picks, sizeof(int32_t) * 6 * nmb * n, cudaMemcpyDeviceToHost, st));
-    H264A_CUDA(cudaMemcpyAsync(job->h_costs, costs, sizeof(int64_t) * 2 * nmb * n, cudaMemcpyDeviceToHost, st));
+    H264A_CUDA(cudaMemcpyAsync(job->h_picks, j.d_picks, sizeof(int32_t) * 6 * nmb * n, cudaMemcpyDeviceToHost, st));
+    H264A_CUDA(cudaMemcpyAsync(job->h_costs, j.d_costs, sizeof(int64_t) * 2 * nmb * n, cudaMemcpyDeviceToHost, st));
     if (job->h_coeffs)
-        H264A_CUDA(cudaMemcpyAsync(job->h_coeffs, coef, sizeof(int16_t) * 256 * nmb * n, cudaMemcpyDeviceToHost, st));
+        H264A_CUDA(cudaMemcpyAsync(job->h_coeffs, j.d_coeffs, sizeof(int16_t) * 256 * nmb * n, cudaMemcpyDeviceToHost, st));
     if (job->h_ccoeffs)
-        H264A_CUDA(cudaMemcpyAsync(job->h_ccoeffs, ccoef, sizeof(int16_t) * 128 * nmb * n, cudaMemcpyDeviceToHost, st));
-    if (job->h_rec_y) H264A_CUDA(cudaMemcpyAsync(job->h_rec_y, ry, n * fs, cudaMemcpyDeviceToHost, st));
-    if (job->h_rec_u) H264A_CUDA(cudaMemcpyAsync(job->h_rec_u, ru, n * cs, cudaMemcpyDeviceToHost, st));
-    if (job->h_rec_v) H264A_CUDA(cudaMemcpyAsync(job->h_rec_v, rv, n * cs, cudaMemcpyDeviceToHost, st));
+        H264A_CUDA(cudaMemcpyAsync(job->h_ccoeffs, j.d_ccoeffs, sizeof(int16_t) * 128 * nmb * n, cudaMemcpyDeviceToHost,
+                                   st));
+    if (job->h_rec_y) H264A_CUDA(cudaMemcpyAsync(job->h_rec_y, j.d_rec_y, n * fs, cudaMemcpyDeviceToHost, st));
+    if (job->h_rec_u) H264A_CUDA(cudaMemcpyAsync(job->h_rec_u, j.d_rec_u, n * cs, cudaMemcpyDeviceToHost, st));
+    if (job->h_rec_v) H264A_CUDA(cudaMemcpyAsync(job->h_rec_v, j.d_rec_v, n * cs, cudaMemcpyDeviceToHost, st));
     if (job->net && job->h_props)
-        H264A_CUDA(cudaMemcpyAsync(job->h_props, props, sizeof(int32_t) * 16 * nmb * n, cudaMemcpyDeviceToHost, st));
+        H264A_CUDA(cudaMemcpyAsync(job->h_props, j.d_props, sizeof(int32_t) * 16 * nmb * n, cudaMemcpyDeviceToHost, st));
     if (job->net && job->h_fallback)
-        H264A_CUDA(cudaMemcpyAsync(job->h_fallback, fb, sizeof(int32_t) * nmb * n, cudaMemcpyDeviceToHost, st));
+        H264A_CUDA(cudaMemcpyAsync(job->h_fallback, j.d_fallback, sizeof(int32_t) * nmb * n, cudaMemcpyDeviceToHost,
+                                   st));
     return h264a_sync(ctx, st);
 }

@@ -73,6 +73,9 @@ struct h264a_ctx {
     void *me_tab_host = nullptr;
     size_t me_tab_cap = 0;
     cudaEvent_t me_tab_ev = nullptr;
+    // cached device buffers of h264a_pixel_path_closed
+    void *cl_buf = nullptr;
+    size_t cl_bytes = 0;
     // input slots and the stream their prefetch uploads run on
     PpInput pp_in[PP_SLOTS];
     long long pp_seq = 0;

@@ -1099,3 +1099,33 @@ def test_closed_loop_learned_matches_oracle(acc):
     assert np.array_equal(got["fallback"], want["fallback"])
     assert (got["props"][1:] != 0).any()
     net.close()
+
+
+def test_closed_frames_device_path_equals_host_path(acc):
+    """h264a_closed_frames on device buffers gives what the host-buffer entry
+    gives (which the tests above pin to the oracle)."""
+    torch = acc.torch
+    Y, U, V = _coded_yuv(*synth.cif_clip(5, 6))
+    n, ch, cw = Y.shape
+    nmb = (cw // 16) * (ch // 16)
+    qp = 28
+    lam = float(np.sqrt(A.frame_lambda(qp)) * 1.25)
+    gate = A.split_gate_for_qp(qp)
+    params = A.default_me_params()
+    want = acc.pixel_path_closed(Y, U, V, params, lam, gate, qp)
+    dy, du, dv = dev(acc, Y), dev(acc, U), dev(acc, V)
+    ry, ru, rv = torch.empty_like(dy), torch.empty_like(du), torch.empty_like(dv)
+    planes = acc.empty((4 * (cw + 64) * (ch + 64),), torch.uint8)
+    pk = acc.empty((n, nmb, 6), torch.int32)
+    co = acc.empty((n, nmb, 2), torch.int64)
+    lv = acc.empty((n, nmb, 256), torch.int16)
+    cl = acc.empty((n, nmb, 128), torch.int16)
+    job = A.ClosedDev(dy.data_ptr(), du.data_ptr(), dv.data_ptr(), ry.data_ptr(), ru.data_ptr(), rv.data_ptr(),
+                      planes.data_ptr(), n, cw, ch, lam, gate, qp, 6, None, 0, None, pk.data_ptr(), co.data_ptr(),
+                      lv.data_ptr(), cl.data_ptr(), None, None)
+    for _ in range(2):  # twice into the same buffers
+        acc.closed_frames(job, params)
+        acc.sync()
+        got = dict(picks=pk.cpu().numpy(), costs=co.cpu().numpy(), coeffs=lv.cpu().numpy(), ccoeffs=cl.cpu().numpy(),
+                   rec_y=ry.cpu().numpy(), rec_u=ru.cpu().numpy(), rec_v=rv.cpu().numpy())
+        _compare_closed(got, want)
