@@ -549,14 +549,27 @@ struct GroupGeom {
     unsigned gmask;   // the group's bits in a ballot, shifted down to bit 0
 };
 
-// mode 0: the MB's 16x16 search (one group); mode 1: its four partitions.
+// mode 0: the MB's 16x16 search (one group); mode 1: its four partitions,
+// one lane group of 8 each; mode 2: partition `part` (0 16x8 top, 1 16x8
+// bottom, 2 8x16 left, 3 8x16 right) with the whole warp as one group, four
+// candidates per pass.
 // pre: for mode 0, the lane's source rows already loaded (block lane & 15).
 __device__ __forceinline__ void group_geom_init(GroupGeom& q, WarpScratch& ws, const h264a_picture& pc, int mx, int my,
-                                                int mode, uint32_t win, const uint32_t* pre) {
+                                                int mode, uint32_t win, const uint32_t* pre, int part = 0) {
     const int lane = threadIdx.x & 31;
     SearchGeom& g = q.s;
     int x = mx, y = my;
-    if (mode == 0) {
+    if (mode == 2) {
+        q.gb = 0;
+        q.gl = lane;
+        q.lg = 5;
+        q.gmask = 0xffffffffu;
+        q.rw = part < 2 ? 16 : 8;
+        q.rh = part < 2 ? 8 : 16;
+        g.lg_nb = 3;
+        x += part == 3 ? 8 : 0;
+        y += part == 1 ? 8 : 0;
+    } else if (mode == 0) {
         q.gb = 0;
         q.gl = lane;
         q.lg = 5;
@@ -1084,6 +1097,10 @@ struct FrameDesc {
 // lie on earlier diagonals, so a window of resident warps always holds MBs
 // that are ready, and no MB ever waits on a ticket dealt after its own.
 constexpr int ME_MAXF = 96;
+// Launches of at most this many frames run the wide kernel (a CTA per MB):
+// one frame's wavefront has at most a few dozen ready MBs, far fewer than the
+// resident warps, so each MB's own latency is what counts.
+constexpr int ME_WIDE_MAXF = 2;
 struct FrameBatch {
     FrameDesc f[ME_MAXF];
     long long seg_start[ME_MAXF + 1];
@@ -1321,6 +1338,227 @@ __device__ __forceinline__ void me_frames_body(const TAB& tab, long long total, 
     }
 }
 
+// The wide variant for launches of few frames (the closed loop's one frame
+// at a time), where the wavefront has far fewer ready MBs than resident warps
+// and an MB's own latency is the whole cost: a CTA of ME_WARPS (4) warps takes
+// one MB.  Warp 0 waits for the neighbours, stages the window and runs the
+// 16x16 search exactly as the narrow kernel does; when the gate opens, warp w
+// searches partition w with all 32 lanes (four candidates per pass instead of
+// one per 8-lane group), each warp with its own copy of the search state and
+// the same seeds, centre and lambda, so every partition's result equals the
+// narrow kernel's.  Warp 0 then picks the shape and publishes, as before.
+// Dynamic shared memory: one window of WIN_BYTES.
+struct WideMb {
+    int t;                  // the CTA's ticket
+    long long c16;          // 16x16 J
+    int mv16x, mv16y, ev16;
+    int px[4], py[4], pev[4];
+    long long pc[4];
+};
+
+template <bool BAL, bool LEARN, class TAB>
+__device__ __forceinline__ void me_frames_body_wide(const TAB& tab, long long total, const MeParamsDev& prm,
+                                                    int* __restrict__ counter, int* __restrict__ flags, int epoch,
+                                                    int* __restrict__ status, int spin_limit) {
+    __shared__ WarpScratch scratch[ME_WARPS];
+    __shared__ __align__(8) unsigned long long win_bar;
+    __shared__ WideMb mb;
+    extern __shared__ __align__(128) uint8_t me_win[];
+    const int w = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const uint32_t win = uint32_t(__cvta_generic_to_shared(me_win));
+    const uint32_t bar = uint32_t(__cvta_generic_to_shared(&win_bar));
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    uint32_t parity = 0;
+    for (;;) {
+        if (threadIdx.x == 0) mb.t = atomicAdd(counter, 1);
+        __syncthreads();
+        const int t = mb.t;
+        if (t >= total) return;
+        int s = 0;
+        while (s + 1 < tab.nseg() && tab.seg(s + 1) <= t) s++;
+        const int j = tab.segj(s);
+        const long long u = t - tab.seg(s);
+        const int nxt = j + 1 < tab.n() ? tab.fr(j + 1).mb_w * tab.fr(j + 1).mb_h : 0;
+        const FrameDesc& fd = tab.fr(int(u % (j + 1)));
+        const int k = nxt + int(u / (j + 1));
+        int mbx, mby;
+        wave_mb(fd.mb_w, fd.mb_h, k, mbx, mby);
+        const int m = mby * fd.mb_w + mbx;
+        int* fl = flags + fd.flag_base;
+        const int lx = mbx * 16, ly = mby * 16;
+        const h264a_picture& pc = fd.pic;
+        const int pw = pc.cw + 2 * pc.pad, ph = pc.ch + 2 * pc.pad;
+        const bool win_ok = ((reinterpret_cast<uintptr_t>(pc.d_planes) | uintptr_t(pw)) & 15) == 0 && pw >= WIN_W &&
+                            ph >= WIN_H;
+        int preds[4] = {0, 0, 0, 0};
+        int fell = 0;
+        if (w == 0) {
+            uint32_t src4[4];
+#pragma unroll
+            for (int r = 0; r < 4; r++)
+                src4[r] = ld4u(pc.d_src + (long long)(ly + ((lane >> 2) & 3) * 4 + r) * pc.cw + lx + (lane & 3) * 4);
+            int2 prop = make_int2(0, 0);
+            if (LEARN && lane >= 1 && lane <= N_PROP) {
+                const int32_t* pp = fd.props + 16LL * m + 2 * (lane - 1);
+                prop = make_int2(__ldg(pp), __ldg(pp + 1));
+            }
+            if (lane == 0) {
+                if (mbx > 0) wait_flag(fl + m - 1, epoch, status, 1, spin_limit);
+                if (mby > 0) wait_flag(fl + m - fd.mb_w + (mbx < fd.mb_w - 1 ? 1 : 0), epoch, status, 1, spin_limit);
+            }
+            __syncwarp();
+            const bool aa = mbx > 0, ba = mby > 0, ca = mby > 0 && mbx < fd.mb_w - 1, da = mbx > 0 && mby > 0;
+            const int2 a = aa ? pick_mv_at(fd.picks, m - 1, 3, 0) : make_int2(0, 0);
+            const int2 bb = ba ? pick_mv_at(fd.picks, m - fd.mb_w, 0, 3) : make_int2(0, 0);
+            int2 c = ca ? pick_mv_at(fd.picks, m - fd.mb_w + 1, 0, 3) : make_int2(0, 0);
+            bool cav = ca;
+            if (!ca) {
+                cav = da;
+                c = da ? pick_mv_at(fd.picks, m - fd.mb_w - 1, 3, 3) : make_int2(0, 0);
+            }
+            const int2 pmv = predict_mv_ref0(aa, a, ba, bb, cav, c);
+            if (win_ok) {
+                const int wx0 = min(max((lx + pc.pad + (pmv.x >> 2) - WIN_R) & ~15, 0), pw - WIN_W);
+                const int wy0 = min(max(ly + pc.pad + (pmv.y >> 2) - WIN_R, 0), ph - WIN_H);
+                if (lane == 0) {
+                    scratch[0].wx0 = wx0;
+                    scratch[0].wy0 = wy0;
+                    // every warp's reads of the previous MB's window are
+                    // complete (the CTA barrier at the end of the last MB)
+                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                    if (fd.tmap_ok) {
+                        mbar_expect_tx(bar, uint32_t(WIN_BYTES));
+                        tma_load_3d(win, &fd.tmap, wx0, wy0, 0, bar);
+                    } else {
+                        mbar_expect_tx(bar, uint32_t(4 * WIN_H * WIN_W));
+                    }
+                }
+                __syncwarp();
+                if (!fd.tmap_ok) {
+                    const long long ps = (long long)pw * ph;
+                    for (int i = lane; i < 4 * WIN_H; i += 32) {
+                        const int pl = i / WIN_H, r = i - pl * WIN_H;
+                        bulk_g2s(win + uint32_t(pl * WIN_PLANE + r * WIN_STRIDE),
+                                 pc.d_planes + ps * pl + (long long)(wy0 + r) * pw + wx0, WIN_W, bar);
+                    }
+                }
+            }
+            if (lane == 0) scratch[0].win_ok = win_ok;
+            __syncwarp();
+            preds[0] = pmv.x;
+            preds[1] = pmv.y;
+            GroupGeom qg;
+            group_geom_init(qg, scratch[0], pc, lx, ly, 0, win, src4);
+            if (win_ok) wait_window(bar, parity, status, 3, spin_limit);
+            int rx, ry, ev;
+            long long rc;
+            motion_search_group<BAL, LEARN>(qg, prm, scratch[0], preds, 1, fd.lambda_me, rx, ry, rc, ev, LEARN, prop,
+                                            fd.prop_t, &fell);
+            if (lane == 0) {
+                mb.c16 = rc;
+                mb.mv16x = rx;
+                mb.mv16y = ry;
+                mb.ev16 = ev << 4;
+            }
+        }
+        __syncthreads();
+        // warp 0 saw the window's copy complete before the barrier, so this
+        // wait of the other warps returns at once; every warp then tracks the
+        // barrier's next phase
+        if (w > 0 && win_ok) wait_window(bar, parity, status, 3, spin_limit);
+        if (win_ok) parity ^= 1u;
+        const bool gated = fd.split_gate >= 0 && mb.c16 > fd.split_gate;
+        if (gated) {
+            if (lane == 0 && w > 0) {
+                scratch[w].win_ok = scratch[0].win_ok;
+                scratch[w].wx0 = scratch[0].wx0;
+                scratch[w].wy0 = scratch[0].wy0;
+            }
+            __syncwarp();
+            if (w > 0) {
+                // the predictor, from warp 0's search state
+                preds[0] = scratch[0].cx;
+                preds[1] = scratch[0].cy;
+            }
+            preds[2] = mb.mv16x;
+            preds[3] = mb.mv16y;
+            GroupGeom qg;
+            group_geom_init(qg, scratch[w], pc, lx, ly, 2, win, nullptr, w);
+            int rx, ry, ev;
+            long long rc;
+            motion_search_group<BAL, false>(qg, prm, scratch[w], preds, 2, fd.lambda_me, rx, ry, rc, ev);
+            if (lane == 0) {
+                mb.px[w] = rx;
+                mb.py[w] = ry;
+                mb.pc[w] = rc;
+                mb.pev[w] = ev << 3;
+            }
+        }
+        __syncthreads();
+        if (w == 0) {
+            int evals = mb.ev16, shape = 0;
+            int mv0x = mb.mv16x, mv0y = mb.mv16y, mv1x = mb.mv16x, mv1y = mb.mv16y;
+            const long long c16 = mb.c16;
+            long long best = c16;
+            if (gated) {
+                evals += mb.pev[0] + mb.pev[1] + mb.pev[2] + mb.pev[3];
+                if (mb.pc[0] + mb.pc[1] < best) {  // 16x8 top + bottom
+                    best = mb.pc[0] + mb.pc[1]; shape = 1;
+                    mv0x = mb.px[0]; mv0y = mb.py[0]; mv1x = mb.px[1]; mv1y = mb.py[1];
+                }
+                if (mb.pc[2] + mb.pc[3] < best) {  // 8x16 left + right
+                    best = mb.pc[2] + mb.pc[3]; shape = 2;
+                    mv0x = mb.px[2]; mv0y = mb.py[2]; mv1x = mb.px[3]; mv1y = mb.py[3];
+                }
+            }
+            if (lane == 0) {
+                int32_t* p = fd.picks + 6 * m;
+                p[0] = shape; p[1] = mv0x; p[2] = mv0y; p[3] = mv1x; p[4] = mv1y; p[5] = evals;
+                fd.costs[2 * m] = best;
+                fd.costs[2 * m + 1] = c16;
+                if (LEARN && fd.fallback) fd.fallback[m] = fell;
+                st_release(fl + m, epoch);  // orders the pick's stores before the flag
+            }
+            if (fd.coeffs != nullptr && lane < 16) {
+                const int bx = (lane & 3) * 4, by = (lane >> 2) * 4;
+                const int part = shape == 1 ? (by >= 8) : (shape == 2 ? (bx >= 8) : 0);
+                const int mvx = part ? mv1x : mv0x, mvy = part ? mv1y : mv0y;
+                const int x = lx + bx, y = ly + by;
+                uint32_t sr[4], pr[4];
+#pragma unroll
+                for (int r = 0; r < 4; r++) sr[r] = ld4u(pc.d_src + (long long)(y + r) * pc.cw + x);
+                const int wx = x + pc.pad - scratch[0].wx0 + (mvx >> 2), wy = y + pc.pad - scratch[0].wy0 + (mvy >> 2);
+                if (win_ok && win_covers(wx, wy)) {
+                    win_rows(win, wx, wy, mvx & 3, mvy & 3, pr);
+                } else {
+                    Planes P;
+                    P.base = pc.d_planes; P.pw = pw; P.ph = ph; P.pad = pc.pad; P.ps = (long long)pw * ph;
+                    pred_rows(P, x + (mvx >> 2), y + (mvy >> 2), mvx & 3, mvy & 3, pr);
+                }
+                const int qi = (by >= 8 ? 2 : 0) + (bx >= 8 ? 1 : 0), kk = ((by & 4) ? 2 : 0) + ((bx & 4) ? 1 : 0);
+                tq4x4_store(sr, pr, fd.qff, fd.qmf, fd.coeffs + (long long)m * 256 + qi * 64 + kk * 16);
+            }
+            __syncwarp();
+            if (fd.row_count != nullptr && lane == 0 && atom_add_acq_rel(fd.row_count + mby, 1) == fd.mb_w - 1)
+                st_release_sys(fd.row_done + mby, fd.row_token);
+        }
+        __syncthreads();  // the MB's window and shared state are free for the next ticket
+    }
+}
+
+template <bool BAL, bool LEARN>
+__global__ void __launch_bounds__(32 * ME_WARPS, ME_MIN_BLOCKS)
+    me_frames_wide_kernel(const __grid_constant__ FrameBatch batch, long long total,
+                          const __grid_constant__ MeParamsDev prm, int* __restrict__ counter, int* __restrict__ flags,
+                          int epoch, int* __restrict__ status, int spin_limit) {
+    me_frames_body_wide<BAL, LEARN>(ParamTable{batch}, total, prm, counter, flags, epoch, status, spin_limit);
+}
+
 template <bool BAL, bool LEARN = false>
 __global__ void __launch_bounds__(32 * ME_WARPS, ME_MIN_BLOCKS)
     me_frames_kernel(const __grid_constant__ FrameBatch batch, long long total, const __grid_constant__ MeParamsDev prm,
@@ -1389,7 +1627,28 @@ static int encode_window_map(CUtensorMap* map, const uint8_t* planes, int pw, in
 
 // Dynamic shared memory of me_frames_kernel, its opt-in above 48 KB, and the
 // CTAs per SM it reaches.
+static int me_frames_setup_once(int& per_sm, bool learn);
+// Cached per device: the attributes and the occupancy of the frame kernels
+// (queried once, not on every launch).
 static int me_frames_setup(int& per_sm, bool learn = false) {
+    constexpr int kMaxDev = 64;
+    static int cached[kMaxDev][2];  // CTAs per SM + 1, 0 while unknown
+    static std::mutex mu;
+    int dev = 0;
+    H264A_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDev) return me_frames_setup_once(per_sm, learn);
+    std::lock_guard<std::mutex> lock(mu);
+    int& c = cached[dev][learn ? 1 : 0];
+    if (!c) {
+        const int rc = me_frames_setup_once(per_sm, learn);
+        if (rc) return rc;
+        c = per_sm + 1;
+    }
+    per_sm = c - 1;
+    return H264A_OK;
+}
+
+static int me_frames_setup_once(int& per_sm, bool learn) {
     const int smem = ME_WARPS * WIN_BYTES;
     H264A_CUDA(cudaFuncSetAttribute(me_frames_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     H264A_CUDA(cudaFuncSetAttribute(me_frames_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
@@ -1462,6 +1721,60 @@ static void launch_me_frames_dtab(const MeParamsDev& prm, unsigned blocks, cudaS
     else
         me_frames_dkernel<false><<<blocks, 32 * ME_WARPS, sm, st>>>(frames, seg_start, seg_j, nframes, nseg, total, prm,
                                                                    counter, flags, epoch, status, SPIN_LIMIT);
+}
+
+// CTAs per SM of the wide kernel (one window per CTA), cached per device
+static int me_wide_setup_once(int& per_sm);
+static int me_wide_setup(int& per_sm) {
+    constexpr int kMaxDev = 64;
+    static int cached[kMaxDev];
+    static std::mutex mu;
+    int dev = 0;
+    H264A_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDev) return me_wide_setup_once(per_sm);
+    std::lock_guard<std::mutex> lock(mu);
+    if (!cached[dev]) {
+        const int rc = me_wide_setup_once(per_sm);
+        if (rc) return rc;
+        cached[dev] = per_sm + 1;
+    }
+    per_sm = cached[dev] - 1;
+    return H264A_OK;
+}
+
+static int me_wide_setup_once(int& per_sm) {
+    const int smem = WIN_BYTES;
+    H264A_CUDA(cudaFuncSetAttribute(me_frames_wide_kernel<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    smem));
+    H264A_CUDA(cudaFuncSetAttribute(me_frames_wide_kernel<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    smem));
+    H264A_CUDA(cudaFuncSetAttribute(me_frames_wide_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    smem));
+    H264A_CUDA(cudaFuncSetAttribute(me_frames_wide_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    smem));
+    per_sm = 0;
+    H264A_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, me_frames_wide_kernel<false, true>,
+                                                             32 * ME_WARPS, smem));
+    if (per_sm < 1) per_sm = 1;
+    return H264A_OK;
+}
+
+static void launch_me_frames_wide(const MeParamsDev& prm, unsigned blocks, cudaStream_t st, const FrameBatch& fb,
+                                  long long total, int* counter, int* flags, int epoch, int* status, bool learn) {
+    const size_t sm = WIN_BYTES;
+    const bool bal = balanced_preset(prm);
+    if (learn && bal)
+        me_frames_wide_kernel<true, true><<<blocks, 32 * ME_WARPS, sm, st>>>(fb, total, prm, counter, flags, epoch,
+                                                                            status, SPIN_LIMIT);
+    else if (learn)
+        me_frames_wide_kernel<false, true><<<blocks, 32 * ME_WARPS, sm, st>>>(fb, total, prm, counter, flags, epoch,
+                                                                             status, SPIN_LIMIT);
+    else if (bal)
+        me_frames_wide_kernel<true, false><<<blocks, 32 * ME_WARPS, sm, st>>>(fb, total, prm, counter, flags, epoch,
+                                                                             status, SPIN_LIMIT);
+    else
+        me_frames_wide_kernel<false, false><<<blocks, 32 * ME_WARPS, sm, st>>>(fb, total, prm, counter, flags, epoch,
+                                                                              status, SPIN_LIMIT);
 }
 
 static void launch_me_frames(const MeParamsDev& prm, unsigned blocks, cudaStream_t st, const FrameBatch& fb,
@@ -1585,6 +1898,17 @@ int h264a::me_frames_run(h264a_ctx* ctx, const h264a_me_frame* h_frames, int nfr
         fb.n = nframes;
         memcpy(fb.f, desc.data(), sizeof(FrameDesc) * nframes);
         if (fill_segments(fb) != total) return fail(H264A_E_ARG, "me_frames: internal queue layout error");
+        if (nframes <= ME_WIDE_MAXF) {
+            // few frames: a CTA per MB, the partitions one warp each
+            int wide_sm = 0;
+            rc0 = me_wide_setup(wide_sm);
+            if (rc0) return rc0;
+            long long wblocks = (long long)ctx->num_sms * wide_sm;
+            if (wblocks > total) wblocks = total;
+            launch_me_frames_wide(prm, unsigned(wblocks), st, fb, total, ctx->q[Q_MAIN].d_counter,
+                                  ctx->q[Q_MAIN].d_flags, epoch, ctx->d_status, learn != nullptr);
+            return check_launch("me_frames_wide_kernel");
+        }
         launch_me_frames(prm, unsigned(blocks), st, fb, total, ctx->q[Q_MAIN].d_counter, ctx->q[Q_MAIN].d_flags, epoch,
                          ctx->d_status, learn != nullptr);
         return check_launch("me_frames_kernel");

@@ -1129,3 +1129,49 @@ def test_closed_frames_device_path_equals_host_path(acc):
         got = dict(picks=pk.cpu().numpy(), costs=co.cpu().numpy(), coeffs=lv.cpu().numpy(), ccoeffs=cl.cpu().numpy(),
                    rec_y=ry.cpu().numpy(), rec_u=ru.cpu().numpy(), rec_v=rv.cpu().numpy())
         _compare_closed(got, want)
+
+
+@pytest.mark.parametrize("learned", [False, True])
+def test_me_frames_wide_kernel_equals_batched(acc, learned):
+    """Frames run one at a time take the wide kernel (a CTA per MB, the four
+    partitions one warp each); the same frames in one call take the narrow
+    kernel (a warp per MB).  Picks, costs and fallback flags are identical,
+    and both equal the oracle (first frame)."""
+    torch = acc.torch
+    y, _, _ = synth.hd_clip(5, 12, 352, 288)
+    clip = synth.coded_luma(y)
+    n, ch, cw = clip.shape
+    nmb = (cw // 16) * (ch // 16)
+    qp = 27
+    lam = float(np.sqrt(A.frame_lambda(qp)) * 1.25)
+    gate = A.split_gate_for_qp(qp)
+    params = A.default_me_params()
+    d = dev(acc, clip)
+    planes = acc.hpel_build(d[: n - 1], 32)
+    rng = np.random.default_rng(3)
+    props = dev(acc, rng.integers(-8, 9, (n, nmb, 16)).astype(np.int32) * 4)
+    outs = []
+    for batched in (True, False):
+        pk = acc.zeros((n, nmb, 6), torch.int32)
+        co = acc.zeros((n, nmb, 2), torch.int64)
+        fb = acc.zeros((n, nmb), torch.int32)
+        fr = [A.MeFrame(A.Picture(d[i].data_ptr(), planes[i - 1].data_ptr(), cw, ch, 32), lam, gate,
+                        pk[i].data_ptr(), co[i].data_ptr()) for i in range(1, n)]
+        lf = [A.MeLearnedFrame(fr[i - 1], props[i].data_ptr(), 200, fb[i].data_ptr()) for i in range(1, n)]
+        calls = [lf] if batched else [[x] for x in lf]
+        for c in calls:
+            if learned:
+                acc.me_frames_learned(c, params)
+            else:
+                acc.me_frames([x.me for x in c], params)
+        acc.sync()
+        outs.append((pk.cpu().numpy(), co.cpu().numpy(), fb.cpu().numpy()))
+    (pa, ca, fa), (pb, cb_, fb_) = outs
+    assert np.array_equal(pa[..., :5], pb[..., :5]) and np.array_equal(ca, cb_)
+    assert np.array_equal(pa[..., 5], pb[..., 5])
+    if learned:
+        assert np.array_equal(fa, fb_)
+    else:
+        wp, wc = O.me_frame(clip[1], clip[0], O.build_planes4(clip[0], 32), O.balanced_params(), lam, gate)
+        assert np.array_equal(pb[1, :, :5], wp[:, :5]) and np.array_equal(cb_[1], wc)
+    assert (pb[1:, :, 0] > 0).any()  # the partition searches ran
