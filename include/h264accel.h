@@ -425,8 +425,9 @@ H264A_API int h264a_me_frames_learned(h264a_ctx *ctx, const h264a_me_learned_fra
  * mb16.rs:3575-3605, chroma mb16.rs:3606-3628, deblock.rs filter_frame with
  * zero offsets).  Frame 0 reconstructs to itself (coded losslessly in this
  * frame model); frames 1..n-1 run plain-ME (or, with a net, the learned
- * search, its proposals computed from the source frame and the previous
- * reconstruction, guide MVs from the HalfRes lookahead of the source),
+ * search: the proposals of every frame come first, in one batched pass over
+ * the source pairs (f, f-1) with guide MVs from the HalfRes lookahead, and
+ * the search prices them on the reconstruction),
  * MC + T/Q and reconstruction of luma and chroma, and deblocking.  The frames
  * run one after another on the device (frame f may read any row of
  * rec(f-1)); each frame's MBs run as a wavefront.  Inputs: n frames of luma

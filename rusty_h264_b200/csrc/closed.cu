@@ -5,8 +5,9 @@
 //
 // Per P frame f, on one stream, every step a kernel of this library:
 //   planes of rec(f-1)                          h264a_hpel_build
-//   [learned: proposals from (src f, rec f-1)]  h264a_mvnet_propose
 //   motion search of src f on those planes      h264a_me_frames / _learned
+//     (learned: the proposals of all frames come first, in one batched
+//     h264a_mvnet_propose pass over the source pairs (f, f-1))
 //   MC + luma T/Q + luma reconstruction         h264a_mc_tq_rec_frames
 //   chroma MC + T/Q + reconstruction            h264a_mc_tq_chroma_frames
 //   in-loop deblocking of rec(f)                h264a_deblock_frames
@@ -48,6 +49,18 @@ int closed_run(h264a_ctx* ctx, const h264a_closed_dev& j, const h264a_me_params&
     H264A_CUDA(cudaMemcpyAsync(j.d_rec_y, j.d_y, fs, cudaMemcpyDeviceToDevice, st));
     H264A_CUDA(cudaMemcpyAsync(j.d_rec_u, j.d_u, cs, cudaMemcpyDeviceToDevice, st));
     H264A_CUDA(cudaMemcpyAsync(j.d_rec_v, j.d_v, cs, cudaMemcpyDeviceToDevice, st));
+    if (j.net && n > 1) {
+        // the proposals of every P frame in one batched pass before the loop:
+        // from the source pair (f, f-1), so none of them waits for a
+        // reconstruction; the search prices them on rec(f-1)
+        std::vector<h264a_mvnet_frame> nf(n - 1);
+        for (int f = 1; f < n; f++)
+            nf[f - 1] = h264a_mvnet_frame{j.d_y + f * fs, j.d_y + (f - 1) * fs, cw, ch,
+                                          j.d_guide_mvs ? j.d_guide_mvs + 2LL * nmb * f : nullptr,
+                                          j.d_props + 16LL * nmb * f};
+        const int rc = h264a_mvnet_propose(j.net, nf.data(), n - 1, st);
+        if (rc) return rc;
+    }
     for (int f = 1; f < n; f++) {
         const uint8_t* ry = j.d_rec_y + (f - 1) * fs;
         int rc = h264a_hpel_build(ctx, ry, cw, ch, pad, 1, fs, j.d_planes, st);
@@ -59,10 +72,6 @@ int closed_run(h264a_ctx* ctx, const h264a_closed_dev& j, const h264a_me_params&
         mf.d_picks = j.d_picks + 6LL * nmb * f;
         mf.d_costs = j.d_costs + 2LL * nmb * f;
         if (j.net) {
-            h264a_mvnet_frame nf{j.d_y + f * fs, ry, cw, ch, j.d_guide_mvs ? j.d_guide_mvs + 2LL * nmb * f : nullptr,
-                                 j.d_props + 16LL * nmb * f};
-            rc = h264a_mvnet_propose(j.net, &nf, 1, st);
-            if (rc) return rc;
             h264a_me_learned_frame lf{mf, j.d_props + 16LL * nmb * f, j.fallback_t,
                                       j.d_fallback ? j.d_fallback + (long long)nmb * f : nullptr};
             rc = h264a_me_frames_learned(ctx, &lf, 1, &prm, st);

@@ -1083,9 +1083,9 @@ def test_closed_loop_1080p_8_frames_matches_oracle(acc):
 
 def test_closed_loop_learned_matches_oracle(acc):
     """The learned search inside the closed loop: the proposals the network
-    made for each frame (from the source and the previous reconstruction)
-    fed to the oracle's closed loop give the same picks, levels and
-    reconstructions, with the same fallback flags."""
+    made for each frame (from the source pairs, before the loop) fed to the
+    oracle's closed loop give the same picks, levels and reconstructions,
+    with the same fallback flags."""
     from rusty_h264_b200 import mvnet
 
     Y, U, V = _coded_yuv(*synth.cif_clip(6, 4))
