@@ -24,8 +24,10 @@ def acc():
 
 def small_batch(acc, P=3, cw=96, ch=64, seed=1):
     """P frame pairs of a textured clip, random neighbour MVs and labels."""
-    y, _, _ = synth.hd_clip(P + 1, 7 + seed, cw, ch)
-    clip = synth.coded_luma(y)
+    # a crop of the textured generator's CIF-size frames (its rectangles need
+    # frames wider and taller than 256 pixels)
+    y, _, _ = synth.hd_clip(P + 1, 7 + seed, 352, 288)
+    clip = np.ascontiguousarray(synth.coded_luma(y)[:, 16:16 + ch, 32:32 + cw])
     d = acc.to_dev(clip)
     pairs = acc.torch.tensor([[d[f].data_ptr(), d[f - 1].data_ptr()] for f in range(1, P + 1)], dtype=acc.torch.int64,
                              device="cuda:0")
