@@ -392,34 +392,29 @@ class ClosedBufs:
 
 
 def closed_stage_ms(acc, torch, A, cb, params, lam, gate, qp, reps=2):
-    """The closed loop's stages replayed one launch at a time with events
-    between them (the same launches h264a_closed_frames makes), for the
-    per-stage times and the ME kernel's share."""
-    n, cw, ch, nmb = cb.n, cb.cw, cb.ch, cb.nmb
-    fs, cs = cw * ch, cw * ch // 4
+    """The closed loop's launches replayed one frame at a time with events
+    between them (the same two launches per frame h264a_closed_frames makes:
+    the planes of rec(f-1), then h264a_closed_step_frame, the search with each
+    MB's reconstruction and deblocking fused in), for the per-stage times and
+    the fused kernel's average launch duration."""
+    n, cw, ch = cb.n, cb.cw, cb.ch
+    fs = cw * ch
     acc._check(acc.L.h264a_closed_frames(acc.ctx, C_byref(cb.job(A, lam, gate, qp)), C_byref(params), acc._stream()))
-    tot = {"hpel": 0.0, "me": 0.0, "mc_tq_rec": 0.0, "chroma": 0.0, "deblock": 0.0}
+    tot = {"hpel": 0.0, "me_rec_deblock": 0.0}
     for _ in range(reps):
         for f in range(1, n):
-            ev = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
             ev[0].record()
             acc._check(acc.L.h264a_hpel_build(acc.ctx, cb.ry[f - 1].data_ptr(), cw, ch, 32, 1, fs, cb.planes.data_ptr(),
                                               acc._stream()))
             ev[1].record()
             pic = A.Picture(cb.y[f].data_ptr(), cb.planes.data_ptr(), cw, ch, 32)
-            acc.me_frames([A.MeFrame(pic, lam, gate, cb.picks[f].data_ptr(), cb.costs[f].data_ptr())], params)
+            me = A.MeFrame(pic, lam, gate, cb.picks[f].data_ptr(), cb.costs[f].data_ptr())
+            acc.closed_step(A.ClosedStep(me, cb.u[f].data_ptr(), cb.v[f].data_ptr(), cb.ru[f - 1].data_ptr(),
+                                         cb.rv[f - 1].data_ptr(), cb.ry[f].data_ptr(), cb.ru[f].data_ptr(),
+                                         cb.rv[f].data_ptr(), cb.coeffs[f].data_ptr(), cb.ccoeffs[f].data_ptr(), qp,
+                                         6, None, None, 0), params)
             ev[2].record()
-            acc.mc_tq_rec_frames([A.TqRecFrame(A.TqFrame(pic, cb.picks[f].data_ptr(), qp, 6, cb.coeffs[f].data_ptr()),
-                                               cb.ry[f].data_ptr())])
-            ev[3].record()
-            acc.mc_tq_chroma_frames([A.TqChromaFrame(cb.u[f].data_ptr(), cb.v[f].data_ptr(), cb.ru[f - 1].data_ptr(),
-                                                     cb.rv[f - 1].data_ptr(), cw, ch, cb.picks[f].data_ptr(), qp,
-                                                     cb.ccoeffs[f].data_ptr(), cb.ru[f].data_ptr(),
-                                                     cb.rv[f].data_ptr())])
-            ev[4].record()
-            acc.deblock_frames([A.DeblockFrame(cb.ry[f].data_ptr(), cb.ru[f].data_ptr(), cb.rv[f].data_ptr(), cw, ch,
-                                               cb.picks[f].data_ptr(), cb.coeffs[f].data_ptr(), qp, 0, 0, 0)])
-            ev[5].record()
             torch.cuda.synchronize()
             for k, (a, b) in zip(tot, zip(ev[:-1], ev[1:])):
                 tot[k] += a.elapsed_time(b) / reps
@@ -932,9 +927,10 @@ def run_ours(args, ws, rank, local):
     cvalue = ws * n * W * H / (cms * 1e-3) / 1e6
     cstage = closed_stage_ms(acc, torch, A, cb, params, lam, gate, qp)
     cwork = int(cb.picks[1:, :, 5].sum().item())
-    c_achieved = cwork * SATD_OPS_PER_4X4 / (cstage["me"] * 1e-3) / 1e9
+    c_achieved = cwork * SATD_OPS_PER_4X4 / (cstage["me_rec_deblock"] * 1e-3) / 1e9
     croof = {
-        "kernel": "me_frames_kernel (persistent plain-ME, one launch per frame)", "bound": "int32",
+        "kernel": "me_frames_wide_kernel (one launch per frame: plain-ME, a CTA per MB, with each MB's MC + T/Q + "
+                  "reconstruction of luma and chroma and its deblocking fused in)", "bound": "int32",
         "achieved": round(c_achieved, 1), "peak": round(int32_peak, 1), "unit": "Gop/s",
         "frac": round(c_achieved / int32_peak, 4),
         "peak_source": "measured live by h264a_measure_int32_peak (INT32 is not in MEASURED_PEAKS.json)",
@@ -942,10 +938,10 @@ def run_ours(args, ws, rank, local):
         "traffic_source": "ncu capture of the 60-frame source-model launch (1415.2 MB over 481,440 MBs), scaled "
                           "by macroblocks to one frame's launch",
         "work": {"satd_4x4_evals_per_step": cwork, "ops_per_4x4": SATD_OPS_PER_4X4,
-                 "me_ms_per_step": round(cstage["me"], 3), "me_launches": n - 1},
-        "note": "each frame's ME launch is one wavefront of 254 anti-diagonals: bound by its critical path",
+                 "kernel_ms_per_step": round(cstage["me_rec_deblock"], 3), "launches": n - 1},
+        "note": "each frame's launch is one wavefront of 254 anti-diagonals: bound by its critical path",
     }
-    closed_launches = (n - 1) * 5 + 3  # per frame planes, ME, MC+T/Q+rec, chroma, deblock; lookahead 3
+    closed_launches = (n - 1) * 2 + 3  # per frame the planes and the fused search; lookahead 3
     line = {
         "metric": METRIC, "value": round(cvalue, 2), "unit": "Mpx/s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(cms, 4), "higher_is_better": True, "scaling": "weak",

@@ -477,6 +477,30 @@ typedef struct {
 } h264a_closed_dev;
 H264A_API int h264a_closed_frames(h264a_ctx *ctx, const h264a_closed_dev *job, const h264a_me_params *params,
                                   void *stream);
+/* One P frame of that loop, the encoder's per-frame call (encode_frame's
+ * motion search, mb16.rs inter MB coding and reconstruction, then
+ * deblock.rs filter_frame on the picture): frame f's search on the planes
+ * of rec(f-1) (me.pic: the source luma and those planes, built by
+ * h264a_hpel_build), and in the same launch each MB's MC + T/Q and
+ * reconstruction of luma and chroma and the in-loop deblocking of the
+ * picture, written to d_rec_y/u/v.  d_ref_u/v: the chroma reconstruction of
+ * frame f-1.  Levels as h264a_closed_frames' (16-byte aligned), planes 4-byte
+ * aligned.  d_props non-NULL: the learned 16x16 search with those proposals
+ * (16 i32/MB), fallback_t and optional d_fallback as h264a_me_frames_learned.
+ * Enqueued on `stream`; one kernel launch. */
+typedef struct {
+    h264a_me_frame me;
+    const uint8_t *d_u, *d_v;
+    const uint8_t *d_ref_u, *d_ref_v;
+    uint8_t *d_rec_y, *d_rec_u, *d_rec_v;
+    int16_t *d_coeffs, *d_ccoeffs;
+    int32_t qp, dz_div;
+    const int32_t *d_props;
+    int32_t *d_fallback;
+    int32_t fallback_t;
+} h264a_closed_step;
+H264A_API int h264a_closed_step_frame(h264a_ctx *ctx, const h264a_closed_step *step, const h264a_me_params *params,
+                                      void *stream);
 
 /* ---- Annex-B output of the frame model (host) ---------------------------------- */
 /* A decodable H.264 Baseline stream (CAVLC) of n frames of the frame model:

@@ -121,6 +121,13 @@ class ClosedDev(C.Structure):
                 ("d_fallback", C.c_void_p)]
 
 
+class ClosedStep(C.Structure):
+    _fields_ = [("me", MeFrame), ("d_u", C.c_void_p), ("d_v", C.c_void_p), ("d_ref_u", C.c_void_p),
+                ("d_ref_v", C.c_void_p), ("d_rec_y", C.c_void_p), ("d_rec_u", C.c_void_p), ("d_rec_v", C.c_void_p),
+                ("d_coeffs", C.c_void_p), ("d_ccoeffs", C.c_void_p), ("qp", C.c_int32), ("dz_div", C.c_int32),
+                ("d_props", C.c_void_p), ("d_fallback", C.c_void_p), ("fallback_t", C.c_int32)]
+
+
 # Every entry point the header declares (checked by tests/test_capi_symbols.py).
 EXPORTS = (
     "h264a_version", "h264a_last_error", "h264a_ctx_create", "h264a_ctx_destroy", "h264a_sync",
@@ -134,7 +141,7 @@ EXPORTS = (
     "h264a_mvnet_create", "h264a_mvnet_destroy", "h264a_mvnet_set_params", "h264a_mvnet_get_params",
     "h264a_mvnet_forward", "h264a_mvnet_grads", "h264a_mvnet_train_step", "h264a_mvnet_propose",
     "h264a_me_frames_learned", "h264a_pixel_path_closed", "h264a_write_stream_cavlc", "h264a_cavlc_table_code",
-    "h264a_closed_frames",
+    "h264a_closed_frames", "h264a_closed_step_frame",
 )
 
 _lib = None
@@ -182,6 +189,7 @@ def load_library() -> C.CDLL:
     L.h264a_me_frames_learned.argtypes = [vp, vp, i32, C.POINTER(MeParams), vp]
     L.h264a_pixel_path_closed.argtypes = [vp, C.POINTER(ClosedJob), C.POINTER(MeParams), vp]
     L.h264a_closed_frames.argtypes = [vp, C.POINTER(ClosedDev), C.POINTER(MeParams), vp]
+    L.h264a_closed_step_frame.argtypes = [vp, C.POINTER(ClosedStep), C.POINTER(MeParams), vp]
     L.h264a_write_stream_cavlc.argtypes = [C.POINTER(StreamFrames), vp, sz, C.POINTER(sz), vp]
     L.h264a_cavlc_table_code.argtypes = [i32, i32, i32, i32, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L.h264a_mvnet_create.argtypes = [i32, C.c_uint64, C.POINTER(vp)]
@@ -485,6 +493,12 @@ class Accel:
         """The closed loop on device buffers (h264a_closed_frames), enqueued on
         the current stream."""
         self._check(self.L.h264a_closed_frames(self.ctx, C.byref(job), C.byref(params), self._stream()))
+
+    def closed_step(self, step: ClosedStep, params: MeParams):
+        """One P frame of the closed loop (h264a_closed_step_frame): the search
+        with each MB's reconstruction and deblocking fused in, enqueued on the
+        current stream."""
+        self._check(self.L.h264a_closed_step_frame(self.ctx, C.byref(step), C.byref(params), self._stream()))
 
     # ---- end to end from host memory --------------------------------------------
     def pixel_path_prefetch(self, frames: np.ndarray):

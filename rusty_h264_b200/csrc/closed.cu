@@ -3,14 +3,16 @@
 // searches RefFrames built from its reconstructed planes
 // (crates/rusty_h264-encoder/src/lib.rs:228-262).
 //
-// Per P frame f, on one stream, every step a kernel of this library:
+// Per P frame f, on one stream, two kernels of this library:
 //   planes of rec(f-1)                          h264a_hpel_build
-//   motion search of src f on those planes      h264a_me_frames / _learned
-//     (learned: the proposals of all frames come first, in one batched
-//     h264a_mvnet_propose pass over the source pairs (f, f-1))
-//   MC + luma T/Q + luma reconstruction         h264a_mc_tq_rec_frames
-//   chroma MC + T/Q + reconstruction            h264a_mc_tq_chroma_frames
-//   in-loop deblocking of rec(f)                h264a_deblock_frames
+//   one wide motion-search launch (me_frames_wide_kernel) of src f on those
+//   planes, each MB's pick followed in the same CTA by its MC + T/Q +
+//   reconstruction of luma and chroma and its in-loop deblocking, in the
+//   search's wavefront order (the kernels h264a_mc_tq_rec_frames,
+//   h264a_mc_tq_chroma_frames and h264a_deblock_frames run as separate
+//   launches compute the same bytes)
+// With a proposal net the proposals of all frames come first, in one batched
+// h264a_mvnet_propose pass over the source pairs (f, f-1).
 // Frame f depends on all of rec(f-1) (a search may reach any row of the
 // reference), so the frames run one after another and the parallelism is the
 // MBs of one frame (the wavefront kernels).  Frame 0 reconstructs to itself
@@ -30,6 +32,18 @@ int check_geometry(int n, int cw, int ch, int qp, int dz_div) {
         return fail(H264A_E_ARG, "closed loop: frames must be MB-aligned and at least one");
     if (qp < 0 || qp > 51 || dz_div < 1) return fail(H264A_E_ARG, "closed loop: qp out of 0..51 or dz_div < 1");
     return H264A_OK;
+}
+
+// One frame of the loop: the search with each MB's reconstruction and
+// deblocking fused in (checked by the caller).
+int step_run(h264a_ctx* ctx, const h264a_closed_step& s, const h264a_me_params& prm, cudaStream_t st) {
+    const MeTqOut tq{s.d_coeffs, s.qp, s.dz_div, nullptr, nullptr, 0};
+    const MeRecIn rec{s.d_u, s.d_v, s.d_ref_u, s.d_ref_v, s.d_rec_y, s.d_rec_u, s.d_rec_v, s.d_ccoeffs};
+    if (s.d_props) {
+        const MeLearnIn ln{s.d_props, s.d_fallback, s.fallback_t};
+        return me_frames_run(ctx, &s.me, 1, &prm, &tq, st, &ln, &rec);
+    }
+    return me_frames_run(ctx, &s.me, 1, &prm, &tq, st, nullptr, &rec);
 }
 
 // The per-frame launches of the loop on device buffers (checked by the caller).
@@ -65,33 +79,27 @@ int closed_run(h264a_ctx* ctx, const h264a_closed_dev& j, const h264a_me_params&
         const uint8_t* ry = j.d_rec_y + (f - 1) * fs;
         int rc = h264a_hpel_build(ctx, ry, cw, ch, pad, 1, fs, j.d_planes, st);
         if (rc) return rc;
-        h264a_me_frame mf;
-        mf.pic = h264a_picture{j.d_y + f * fs, j.d_planes, cw, ch, pad};
-        mf.lambda_me = j.lambda_me;
-        mf.split_gate = j.split_gate;
-        mf.d_picks = j.d_picks + 6LL * nmb * f;
-        mf.d_costs = j.d_costs + 2LL * nmb * f;
-        if (j.net) {
-            h264a_me_learned_frame lf{mf, j.d_props + 16LL * nmb * f, j.fallback_t,
-                                      j.d_fallback ? j.d_fallback + (long long)nmb * f : nullptr};
-            rc = h264a_me_frames_learned(ctx, &lf, 1, &prm, st);
-        } else {
-            rc = h264a_me_frames(ctx, &mf, 1, &prm, st);
-        }
-        if (rc) return rc;
-        h264a_tq_rec_frame tr;
-        tr.tq = h264a_tq_frame{mf.pic, mf.d_picks, j.qp, j.dz_div, j.d_coeffs + 256LL * nmb * f};
-        tr.d_rec = j.d_rec_y + f * fs;
-        rc = h264a_mc_tq_rec_frames(ctx, &tr, 1, st);
-        if (rc) return rc;
-        h264a_tq_chroma_frame cf{j.d_u + f * cs, j.d_v + f * cs, j.d_rec_u + (f - 1) * cs, j.d_rec_v + (f - 1) * cs,
-                                 cw, ch, mf.d_picks, j.qp, j.d_ccoeffs + 128LL * nmb * f, j.d_rec_u + f * cs,
-                                 j.d_rec_v + f * cs};
-        rc = h264a_mc_tq_chroma_frames(ctx, &cf, 1, st);
-        if (rc) return rc;
-        h264a_deblock_frame df{j.d_rec_y + f * fs, j.d_rec_u + f * cs, j.d_rec_v + f * cs, cw, ch, mf.d_picks,
-                               j.d_coeffs + 256LL * nmb * f, j.qp, 0, 0, 0};
-        rc = h264a_deblock_frames(ctx, &df, 1, st);
+        h264a_closed_step sf;
+        sf.me.pic = h264a_picture{j.d_y + f * fs, j.d_planes, cw, ch, pad};
+        sf.me.lambda_me = j.lambda_me;
+        sf.me.split_gate = j.split_gate;
+        sf.me.d_picks = j.d_picks + 6LL * nmb * f;
+        sf.me.d_costs = j.d_costs + 2LL * nmb * f;
+        sf.d_u = j.d_u + f * cs;
+        sf.d_v = j.d_v + f * cs;
+        sf.d_ref_u = j.d_rec_u + (f - 1) * cs;
+        sf.d_ref_v = j.d_rec_v + (f - 1) * cs;
+        sf.d_rec_y = j.d_rec_y + f * fs;
+        sf.d_rec_u = j.d_rec_u + f * cs;
+        sf.d_rec_v = j.d_rec_v + f * cs;
+        sf.d_coeffs = j.d_coeffs + 256LL * nmb * f;
+        sf.d_ccoeffs = j.d_ccoeffs + 128LL * nmb * f;
+        sf.qp = j.qp;
+        sf.dz_div = j.dz_div;
+        sf.d_props = j.net ? j.d_props + 16LL * nmb * f : nullptr;
+        sf.d_fallback = j.net && j.d_fallback ? j.d_fallback + (long long)nmb * f : nullptr;
+        sf.fallback_t = j.fallback_t;
+        rc = step_run(ctx, sf, prm, st);
         if (rc) return rc;
     }
     return H264A_OK;
@@ -116,6 +124,15 @@ extern "C" int h264a_closed_frames(h264a_ctx* ctx, const h264a_closed_dev* job, 
     if ((params->mv_cost_kind == 1 || params->mv_cost_kind == 2) && !params->d_mv_cost_tab)
         return fail(H264A_E_ARG, "closed_frames: mv cost kinds 1 and 2 need d_mv_cost_tab");
     return closed_run(ctx, j, *params, reinterpret_cast<cudaStream_t>(stream));
+}
+
+extern "C" int h264a_closed_step_frame(h264a_ctx* ctx, const h264a_closed_step* step, const h264a_me_params* params,
+                                       void* stream) {
+    if (!ctx || !step || !params) return fail(H264A_E_ARG, "closed_step_frame: null pointer");
+    const h264a_closed_step& s = *step;
+    if (s.qp < 0 || s.qp > 51 || s.dz_div < 1) return fail(H264A_E_ARG, "closed_step_frame: qp out of 0..51 or dz_div < 1");
+    if (s.d_props && s.fallback_t < 0) return fail(H264A_E_ARG, "closed_step_frame: negative fallback threshold");
+    return step_run(ctx, s, *params, reinterpret_cast<cudaStream_t>(stream));
 }
 
 extern "C" int h264a_pixel_path_closed(h264a_ctx* ctx, const h264a_closed_job* job, const h264a_me_params* params,

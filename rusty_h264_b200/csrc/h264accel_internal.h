@@ -110,10 +110,23 @@ struct MeLearnIn {
     int32_t *fallback;
     int32_t prop_t;
 };
+// Per-frame reconstruction fused into the wide plain-ME kernel (the closed
+// loop): the frame's chroma source, the previous frame's chroma
+// reconstruction, the frame's reconstruction planes (written, then deblocked
+// in place) and chroma levels (128 i16 per MB, 16-byte aligned).  Luma levels
+// and the QP come from the frame's MeTqOut.
+struct MeRecIn {
+    const uint8_t *src_u, *src_v;
+    const uint8_t *ref_u, *ref_v;
+    uint8_t *rec_y, *rec_u, *rec_v;
+    int16_t *ccoeffs;
+};
 // plain-ME of frames, with the fused T/Q when tq is given (one entry per
-// frame), and the learned-proposal 16x16 search when learn is given
+// frame), the learned-proposal 16x16 search when learn is given, and the
+// fused reconstruction + deblocking when rec is given (tq required, at most
+// two frames)
 int me_frames_run(h264a_ctx *ctx, const h264a_me_frame *h_frames, int nframes, const h264a_me_params *params,
-                  const MeTqOut *tq, void *stream, const MeLearnIn *learn = nullptr);
+                  const MeTqOut *tq, void *stream, const MeLearnIn *learn = nullptr, const MeRecIn *rec = nullptr);
 // A tiled TMA map of a dense 3D u8 tensor (w x h x d, rows of w bytes, planes
 // of w*h), box bw x bh x bd, no multicast; 0 when the driver entry point is
 // missing or the layout breaks the TMA rules (the caller then copies without).

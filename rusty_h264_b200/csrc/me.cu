@@ -25,6 +25,7 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
+#include "deblock_device.cuh"
 #include "tq_device.cuh"
 
 namespace h264a {
@@ -1348,6 +1349,42 @@ __device__ __forceinline__ void me_frames_body(const TAB& tab, long long total, 
 // the same seeds, centre and lambda, so every partition's result equals the
 // narrow kernel's.  Warp 0 then picks the shape and publishes, as before.
 // Dynamic shared memory: one window of WIN_BYTES.
+// The closed loop's reconstruction of a frame, fused into the wide kernel:
+// after an MB's pick is published, its luma MC + T/Q + reconstruction (warp
+// 0), chroma MC + T/Q + reconstruction (warp 1), then the in-loop deblocking
+// of the MB (warp 2) in shared tiles, once the deblocking of its left and
+// top-right neighbours is done (bounded waits on a second run of flags, the
+// same wavefront order as the search).
+struct RecDesc {
+    const uint8_t* src_c[2];  // the frame's chroma source (U, V)
+    const uint8_t* ref_c[2];  // the chroma reconstruction of the previous frame
+    uint8_t* rec_y;           // the frame's reconstruction
+    uint8_t* rec_c[2];
+    int16_t* ccoeffs;         // chroma levels, 128 per MB
+    int qp, qpc;              // luma and chroma QP
+    int16_t cff[8], cmf[8];   // the chroma QP's quant row (inter dead-zone)
+    int dflag_base;           // the deblocking flags' offset in the flag array
+    DbThresh th;
+};
+
+// The wide kernel's frame table (at most ME_WIDE_MAXF frames), passed by value.
+struct WideBatch {
+    FrameDesc f[ME_WIDE_MAXF];
+    RecDesc rec[ME_WIDE_MAXF];
+    long long seg_start[ME_WIDE_MAXF + 1];
+    int seg_j[ME_WIDE_MAXF];
+    int n, nseg;
+};
+struct WideTable {
+    const WideBatch& b;
+    __device__ __forceinline__ int n() const { return b.n; }
+    __device__ __forceinline__ int nseg() const { return b.nseg; }
+    __device__ __forceinline__ long long seg(int s) const { return b.seg_start[s]; }
+    __device__ __forceinline__ int segj(int s) const { return b.seg_j[s]; }
+    __device__ __forceinline__ const FrameDesc& fr(int i) const { return b.f[i]; }
+    __device__ __forceinline__ const RecDesc& rd(int i) const { return b.rec[i]; }
+};
+
 struct WideMb {
     int t;                  // the CTA's ticket
     long long c16;          // 16x16 J
@@ -1356,13 +1393,19 @@ struct WideMb {
     long long pc[4];
 };
 
-template <bool BAL, bool LEARN, class TAB>
-__device__ __forceinline__ void me_frames_body_wide(const TAB& tab, long long total, const MeParamsDev& prm,
+template <bool BAL, bool LEARN, bool REC>
+__device__ __forceinline__ void me_frames_body_wide(const WideTable& tab, long long total, const MeParamsDev& prm,
                                                     int* __restrict__ counter, int* __restrict__ flags, int epoch,
                                                     int* __restrict__ status, int spin_limit) {
     __shared__ WarpScratch scratch[ME_WARPS];
     __shared__ __align__(8) unsigned long long win_bar;
     __shared__ WideMb mb;
+    // REC: the MB's reconstruction tiles (deblock_device.cuh's layout), its
+    // luma blocks' coefficient flags (raster order) and the edges' bS
+    __shared__ __align__(16) uint8_t rec_lt[REC ? LT * LT : 4];
+    __shared__ __align__(16) uint8_t rec_ct[2][REC ? CR * CT : 4];
+    __shared__ int rec_nz[16];
+    __shared__ int rec_bs[32];
     extern __shared__ __align__(128) uint8_t me_win[];
     const int w = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
@@ -1384,7 +1427,8 @@ __device__ __forceinline__ void me_frames_body_wide(const TAB& tab, long long to
         const int j = tab.segj(s);
         const long long u = t - tab.seg(s);
         const int nxt = j + 1 < tab.n() ? tab.fr(j + 1).mb_w * tab.fr(j + 1).mb_h : 0;
-        const FrameDesc& fd = tab.fr(int(u % (j + 1)));
+        const int fi = int(u % (j + 1));
+        const FrameDesc& fd = tab.fr(fi);
         const int k = nxt + int(u / (j + 1));
         int mbx, mby;
         wave_mb(fd.mb_w, fd.mb_h, k, mbx, mby);
@@ -1500,22 +1544,24 @@ __device__ __forceinline__ void me_frames_body_wide(const TAB& tab, long long to
             }
         }
         __syncthreads();
-        if (w == 0) {
-            int evals = mb.ev16, shape = 0;
-            int mv0x = mb.mv16x, mv0y = mb.mv16y, mv1x = mb.mv16x, mv1y = mb.mv16y;
-            const long long c16 = mb.c16;
-            long long best = c16;
-            if (gated) {
-                evals += mb.pev[0] + mb.pev[1] + mb.pev[2] + mb.pev[3];
-                if (mb.pc[0] + mb.pc[1] < best) {  // 16x8 top + bottom
-                    best = mb.pc[0] + mb.pc[1]; shape = 1;
-                    mv0x = mb.px[0]; mv0y = mb.py[0]; mv1x = mb.px[1]; mv1y = mb.py[1];
-                }
-                if (mb.pc[2] + mb.pc[3] < best) {  // 8x16 left + right
-                    best = mb.pc[2] + mb.pc[3]; shape = 2;
-                    mv0x = mb.px[2]; mv0y = mb.py[2]; mv1x = mb.px[3]; mv1y = mb.py[3];
-                }
+        // the shape decision (mb16.rs:8869-8913), taken by every warp from
+        // the shared results
+        int evals = mb.ev16, shape = 0;
+        int mv0x = mb.mv16x, mv0y = mb.mv16y, mv1x = mb.mv16x, mv1y = mb.mv16y;
+        const long long c16 = mb.c16;
+        long long best = c16;
+        if (gated) {
+            evals += mb.pev[0] + mb.pev[1] + mb.pev[2] + mb.pev[3];
+            if (mb.pc[0] + mb.pc[1] < best) {  // 16x8 top + bottom
+                best = mb.pc[0] + mb.pc[1]; shape = 1;
+                mv0x = mb.px[0]; mv0y = mb.py[0]; mv1x = mb.px[1]; mv1y = mb.py[1];
             }
+            if (mb.pc[2] + mb.pc[3] < best) {  // 8x16 left + right
+                best = mb.pc[2] + mb.pc[3]; shape = 2;
+                mv0x = mb.px[2]; mv0y = mb.py[2]; mv1x = mb.px[3]; mv1y = mb.py[3];
+            }
+        }
+        if (w == 0) {
             if (lane == 0) {
                 int32_t* p = fd.picks + 6 * m;
                 p[0] = shape; p[1] = mv0x; p[2] = mv0y; p[3] = mv1x; p[4] = mv1y; p[5] = evals;
@@ -1541,22 +1587,109 @@ __device__ __forceinline__ void me_frames_body_wide(const TAB& tab, long long to
                     pred_rows(P, x + (mvx >> 2), y + (mvy >> 2), mvx & 3, mvy & 3, pr);
                 }
                 const int qi = (by >= 8 ? 2 : 0) + (bx >= 8 ? 1 : 0), kk = ((by & 4) ? 2 : 0) + ((bx & 4) ? 1 : 0);
-                tq4x4_store(sr, pr, fd.qff, fd.qmf, fd.coeffs + (long long)m * 256 + qi * 64 + kk * 16);
+                int16_t* co = fd.coeffs + (long long)m * 256 + qi * 64 + kk * 16;
+                if (REC) {
+                    // mb16.rs:3575-3605: the luma reconstruction into the tile
+                    int lv[16];
+                    tq4x4_store(sr, pr, fd.qff, fd.qmf, co, lv);
+                    int any = 0;
+#pragma unroll
+                    for (int i = 0; i < 16; i++) any |= lv[i];
+                    rec_nz[lane] = any != 0;
+                    uint32_t r4[4];
+                    rec4x4(lv, pr, tab.rd(fi).qp, r4);
+#pragma unroll
+                    for (int r = 0; r < 4; r++)
+                        *reinterpret_cast<uint32_t*>(rec_lt + (4 + by + r) * LT + 4 + bx) = r4[r];
+                } else {
+                    tq4x4_store(sr, pr, fd.qff, fd.qmf, co);
+                }
             }
             __syncwarp();
             if (fd.row_count != nullptr && lane == 0 && atom_add_acq_rel(fd.row_count + mby, 1) == fd.mb_w - 1)
                 st_release_sys(fd.row_done + mby, fd.row_token);
         }
+        if (REC) {
+            const RecDesc& rd = tab.rd(fi);
+            const int cx0 = mbx * 8, cy0 = mby * 8;
+            if (w == 1) {
+                // chroma: lanes 0..7 are (plane, block k); lanes 8..31 shadow
+                // them so that the quads' shuffles run over the full warp
+                const int c = (lane >> 2) & 1, kb = lane & 3;
+                const int bx = (kb & 1) * 4, by = (kb >> 1) * 4;
+                const int part = shape == 1 ? (by >= 4) : (shape == 2 ? (bx >= 4) : 0);
+                const int mvx = part ? mv1x : mv0x, mvy = part ? mv1y : mv0y;
+                uint32_t r4[4];
+                chroma_tq_rec(rd.src_c[c], rd.ref_c[c], pc.cw / 2, pc.ch / 2, cx0 + bx, cy0 + by, mvx, mvy, kb, rd.qpc,
+                              rd.cff, rd.cmf, lane < 8 ? rd.ccoeffs + (long long)m * 128 + c * 64 + kb * 16 : nullptr,
+                              r4);
+                if (lane < 8) {
+#pragma unroll
+                    for (int r = 0; r < 4; r++)
+                        *reinterpret_cast<uint32_t*>(&rec_ct[c][(2 + by + r) * CT + 4 + bx]) = r4[r];
+                }
+            }
+            const bool left = mbx > 0, top = mby > 0;
+            int* dfl = flags + rd.dflag_base;
+            const DbStrips strips(lane, rd.rec_y, pc.cw, lx, ly, rd.rec_c, cx0, cy0, rec_lt, rec_ct[0], rec_ct[1], left,
+                                  top, true);
+            int nmx = 0, nmy = 0;
+            bool nnz = false;
+            if (w == 2) {
+                // the left and top-right neighbours' deblocking (so the top
+                // neighbour's too), then the strips their edges reach and the
+                // neighbours' blocks on this MB's edges
+                if (lane == 0 && left) wait_flag(dfl + m - 1, epoch, status, 1, spin_limit);
+                if (lane == 1 && top)
+                    wait_flag(dfl + m - fd.mb_w + (mbx < fd.mb_w - 1 ? 1 : 0), epoch, status, 1, spin_limit);
+                __syncwarp();
+                strips.load();
+                if (lane < 4 && left) block_state_at(fd.picks, fd.coeffs, m - 1, 3, lane, nmx, nmy, nnz);
+                if (lane >= 16 && lane < 20 && top)
+                    block_state_at(fd.picks, fd.coeffs, m - fd.mb_w, lane - 16, 3, nmx, nmy, nnz);
+            }
+            __syncthreads();  // the MB's tiles and coefficient flags are complete
+            if (w == 2) {
+                // bS: lanes 0..15 the vertical edges (edge e, block row sg),
+                // lanes 16..31 the horizontal ones (edge e, block column sg)
+                const int hor = lane >> 4, e = (lane >> 2) & 3, sg = lane & 3;
+                const int qbx = hor ? sg : e, qby = hor ? e : sg;
+                auto own = [&](int bx4, int by4, int& mx, int& my) {
+                    const int part = shape == 1 ? (by4 >= 2) : (shape == 2 ? (bx4 >= 2) : 0);
+                    mx = part ? mv1x : mv0x;
+                    my = part ? mv1y : mv0y;
+                };
+                int bs = 0;
+                if (e > 0 || (hor ? top : left)) {
+                    int pmx = nmx, pmy = nmy, qmx, qmy;
+                    bool pnz = nnz;
+                    if (e > 0) {
+                        const int pbx = hor ? sg : e - 1, pby = hor ? e - 1 : sg;
+                        own(pbx, pby, pmx, pmy);
+                        pnz = rec_nz[pby * 4 + pbx] != 0;
+                    }
+                    own(qbx, qby, qmx, qmy);
+                    bs = bs_of(pnz, rec_nz[qby * 4 + qbx] != 0, pmx, pmy, qmx, qmy);
+                }
+                rec_bs[lane] = bs;
+                __syncwarp();
+                deblock_mb_tiles(lane, rec_lt, rec_ct[0], rec_ct[1], rec_bs, left, top, true, rd.th);
+                db_store_mb(lane, rec_lt, rec_ct[0], rec_ct[1], rd.rec_y, pc.cw, lx, ly, rd.rec_c, cx0, cy0, true);
+                strips.store();
+                __syncwarp();  // every lane's stores ordered before lane 0's release
+                if (lane == 0) st_release(dfl + m, epoch);
+            }
+        }
         __syncthreads();  // the MB's window and shared state are free for the next ticket
     }
 }
 
-template <bool BAL, bool LEARN>
+template <bool BAL, bool LEARN, bool REC>
 __global__ void __launch_bounds__(32 * ME_WARPS, ME_MIN_BLOCKS)
-    me_frames_wide_kernel(const __grid_constant__ FrameBatch batch, long long total,
+    me_frames_wide_kernel(const __grid_constant__ WideBatch batch, long long total,
                           const __grid_constant__ MeParamsDev prm, int* __restrict__ counter, int* __restrict__ flags,
                           int epoch, int* __restrict__ status, int spin_limit) {
-    me_frames_body_wide<BAL, LEARN>(ParamTable{batch}, total, prm, counter, flags, epoch, status, spin_limit);
+    me_frames_body_wide<BAL, LEARN, REC>(WideTable{batch}, total, prm, counter, flags, epoch, status, spin_limit);
 }
 
 template <bool BAL, bool LEARN = false>
@@ -1742,39 +1875,58 @@ static int me_wide_setup(int& per_sm) {
     return H264A_OK;
 }
 
+template <bool BAL, bool LEARN, bool REC>
+static int wide_attr(int smem) {
+    H264A_CUDA(cudaFuncSetAttribute(me_frames_wide_kernel<BAL, LEARN, REC>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    return H264A_OK;
+}
+
 static int me_wide_setup_once(int& per_sm) {
     const int smem = WIN_BYTES;
-    H264A_CUDA(cudaFuncSetAttribute(me_frames_wide_kernel<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    smem));
-    H264A_CUDA(cudaFuncSetAttribute(me_frames_wide_kernel<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    smem));
-    H264A_CUDA(cudaFuncSetAttribute(me_frames_wide_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    smem));
-    H264A_CUDA(cudaFuncSetAttribute(me_frames_wide_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    smem));
+    int rc = wide_attr<false, false, false>(smem) | wide_attr<true, false, false>(smem) |
+             wide_attr<false, true, false>(smem) | wide_attr<true, true, false>(smem) |
+             wide_attr<false, false, true>(smem) | wide_attr<true, false, true>(smem) |
+             wide_attr<false, true, true>(smem) | wide_attr<true, true, true>(smem);
+    if (rc) return rc;
+    // the residency of the largest variant bounds the grid of every one
     per_sm = 0;
-    H264A_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, me_frames_wide_kernel<false, true>,
+    H264A_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, me_frames_wide_kernel<false, true, true>,
                                                              32 * ME_WARPS, smem));
+    int p2 = 0;
+    H264A_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&p2, me_frames_wide_kernel<false, true, false>,
+                                                             32 * ME_WARPS, smem));
+    if (p2 < per_sm) per_sm = p2;
     if (per_sm < 1) per_sm = 1;
     return H264A_OK;
 }
 
-static void launch_me_frames_wide(const MeParamsDev& prm, unsigned blocks, cudaStream_t st, const FrameBatch& fb,
-                                  long long total, int* counter, int* flags, int epoch, int* status, bool learn) {
+template <bool REC>
+static void launch_wide_t(const MeParamsDev& prm, unsigned blocks, cudaStream_t st, const WideBatch& wb,
+                          long long total, int* counter, int* flags, int epoch, int* status, bool learn) {
     const size_t sm = WIN_BYTES;
     const bool bal = balanced_preset(prm);
     if (learn && bal)
-        me_frames_wide_kernel<true, true><<<blocks, 32 * ME_WARPS, sm, st>>>(fb, total, prm, counter, flags, epoch,
-                                                                            status, SPIN_LIMIT);
+        me_frames_wide_kernel<true, true, REC><<<blocks, 32 * ME_WARPS, sm, st>>>(wb, total, prm, counter, flags,
+                                                                                 epoch, status, SPIN_LIMIT);
     else if (learn)
-        me_frames_wide_kernel<false, true><<<blocks, 32 * ME_WARPS, sm, st>>>(fb, total, prm, counter, flags, epoch,
-                                                                             status, SPIN_LIMIT);
+        me_frames_wide_kernel<false, true, REC><<<blocks, 32 * ME_WARPS, sm, st>>>(wb, total, prm, counter, flags,
+                                                                                  epoch, status, SPIN_LIMIT);
     else if (bal)
-        me_frames_wide_kernel<true, false><<<blocks, 32 * ME_WARPS, sm, st>>>(fb, total, prm, counter, flags, epoch,
-                                                                             status, SPIN_LIMIT);
+        me_frames_wide_kernel<true, false, REC><<<blocks, 32 * ME_WARPS, sm, st>>>(wb, total, prm, counter, flags,
+                                                                                  epoch, status, SPIN_LIMIT);
     else
-        me_frames_wide_kernel<false, false><<<blocks, 32 * ME_WARPS, sm, st>>>(fb, total, prm, counter, flags, epoch,
-                                                                              status, SPIN_LIMIT);
+        me_frames_wide_kernel<false, false, REC><<<blocks, 32 * ME_WARPS, sm, st>>>(wb, total, prm, counter, flags,
+                                                                                   epoch, status, SPIN_LIMIT);
+}
+
+static void launch_me_frames_wide(const MeParamsDev& prm, unsigned blocks, cudaStream_t st, const WideBatch& wb,
+                                  long long total, int* counter, int* flags, int epoch, int* status, bool learn,
+                                  bool rec) {
+    if (rec)
+        launch_wide_t<true>(prm, blocks, st, wb, total, counter, flags, epoch, status, learn);
+    else
+        launch_wide_t<false>(prm, blocks, st, wb, total, counter, flags, epoch, status, learn);
 }
 
 static void launch_me_frames(const MeParamsDev& prm, unsigned blocks, cudaStream_t st, const FrameBatch& fb,
@@ -1822,9 +1974,12 @@ extern "C" int h264a_me_search(h264a_ctx* ctx, const h264a_picture* d_pics, int 
 // Plain-ME of a batch of frames (h264a_me_frames); with `tq`, each frame's
 // MC + luma T/Q is fused in (h264a_me_tq_frames, h264a_pixel_path_host).
 int h264a::me_frames_run(h264a_ctx* ctx, const h264a_me_frame* h_frames, int nframes,
-                         const h264a_me_params* params, const MeTqOut* tq, void* stream, const MeLearnIn* learn) {
+                         const h264a_me_params* params, const MeTqOut* tq, void* stream, const MeLearnIn* learn,
+                         const MeRecIn* rec) {
     if (!ctx || !h_frames || !params) return fail(H264A_E_ARG, "me_frames: null pointer");
     if (nframes < 1) return fail(H264A_E_ARG, "me_frames: need at least one frame");
+    if (rec && (!tq || nframes > ME_WIDE_MAXF))
+        return fail(H264A_E_ARG, "me_frames: the fused reconstruction needs T/Q outputs and at most two frames");
     if ((params->mv_cost_kind == 1 || params->mv_cost_kind == 2) && !params->d_mv_cost_tab)
         return fail(H264A_E_ARG, "me_frames: mv cost kinds 1 and 2 need d_mv_cost_tab");
     for (int i = 0; i < nframes; i++) {
@@ -1850,6 +2005,8 @@ int h264a::me_frames_run(h264a_ctx* ctx, const h264a_me_frame* h_frames, int nfr
     });
     std::vector<FrameDesc> desc(nframes);
     memset(desc.data(), 0, sizeof(FrameDesc) * nframes);
+    RecDesc rdesc[ME_WIDE_MAXF];
+    memset(rdesc, 0, sizeof rdesc);
     long long total = 0;
     for (int k = 0; k < nframes; k++) {
         const h264a_me_frame& f = h_frames[order[k]];
@@ -1877,6 +2034,29 @@ int h264a::me_frames_run(h264a_ctx* ctx, const h264a_me_frame* h_frames, int nfr
             d.fallback = l.fallback;
             d.prop_t = l.prop_t;
         }
+        if (rec) {
+            const MeRecIn& r = rec[order[k]];
+            if (!r.src_u || !r.src_v || !r.ref_u || !r.ref_v || !r.rec_y || !r.rec_u || !r.rec_v || !r.ccoeffs)
+                return fail(H264A_E_ARG, "me_frames: null reconstruction pointer");
+            if (((reinterpret_cast<uintptr_t>(r.src_u) | reinterpret_cast<uintptr_t>(r.src_v) |
+                  reinterpret_cast<uintptr_t>(r.ref_u) | reinterpret_cast<uintptr_t>(r.ref_v) |
+                  reinterpret_cast<uintptr_t>(r.rec_y) | reinterpret_cast<uintptr_t>(r.rec_u) |
+                  reinterpret_cast<uintptr_t>(r.rec_v)) & 3) ||
+                ((reinterpret_cast<uintptr_t>(r.ccoeffs) | reinterpret_cast<uintptr_t>(tq[order[k]].coeffs)) & 15))
+                return fail(H264A_E_ARG, "me_frames: planes must be 4-byte and levels 16-byte aligned");
+            const int qp = tq[order[k]].qp;
+            if (qp < 0 || qp > 51) return fail(H264A_E_ARG, "me_frames: qp out of 0..51");
+            RecDesc& rd = rdesc[k];
+            rd.src_c[0] = r.src_u; rd.src_c[1] = r.src_v;
+            rd.ref_c[0] = r.ref_u; rd.ref_c[1] = r.ref_v;
+            rd.rec_y = r.rec_y;
+            rd.rec_c[0] = r.rec_u; rd.rec_c[1] = r.rec_v;
+            rd.ccoeffs = r.ccoeffs;
+            rd.qp = qp;
+            rd.qpc = chroma_qp_of(qp);
+            make_quant_row4(rd.qpc, 6, rd.cff, rd.cmf);  // chroma: the inter dead-zone
+            rd.th = db_thresholds(qp, 0, 0, 0);
+        }
         total += (long long)d.mb_w * d.mb_h;
         if (total >= (1LL << 31)) return fail(H264A_E_ARG, "me_frames: too many macroblocks in one call");
     }
@@ -1884,7 +2064,8 @@ int h264a::me_frames_run(h264a_ctx* ctx, const h264a_me_frame* h_frames, int nfr
     std::vector<int> segj(nframes);
     const int nseg = make_segments(desc.data(), nframes, seg.data(), segj.data());
     if (seg[nseg] != total) return fail(H264A_E_ARG, "me_frames: internal queue layout error");
-    int rc = ensure_me_scratch(ctx, size_t(total));
+    // the fused reconstruction's deblocking flags follow the search's
+    int rc = ensure_me_scratch(ctx, size_t(rec ? 2 * total : total));
     if (rc) return rc;
     H264A_CUDA(cudaMemsetAsync(ctx->q[Q_MAIN].d_counter, 0, sizeof(int32_t), st));
     const int epoch = next_epoch(ctx, st);
@@ -1892,23 +2073,33 @@ int h264a::me_frames_run(h264a_ctx* ctx, const h264a_me_frame* h_frames, int nfr
     long long blocks = (long long)ctx->num_sms * per_sm;
     const long long need = (total + ME_WARPS - 1) / ME_WARPS;
     if (blocks > need) blocks = need;
+    if (nframes <= ME_WIDE_MAXF) {
+        // few frames: a CTA per MB, the partitions one warp each
+        int wide_sm = 0;
+        rc0 = me_wide_setup(wide_sm);
+        if (rc0) return rc0;
+        long long wblocks = (long long)ctx->num_sms * wide_sm;
+        if (wblocks > total) wblocks = total;
+        WideBatch wb;
+        memset(&wb, 0, sizeof wb);
+        wb.n = nframes;
+        memcpy(wb.f, desc.data(), sizeof(FrameDesc) * nframes);
+        for (int k = 0; k < nframes; k++) {
+            wb.rec[k] = rdesc[k];
+            wb.rec[k].dflag_base = int(total) + desc[k].flag_base;
+        }
+        wb.nseg = make_segments(wb.f, wb.n, wb.seg_start, wb.seg_j);
+        if (wb.seg_start[wb.nseg] != total) return fail(H264A_E_ARG, "me_frames: internal queue layout error");
+        launch_me_frames_wide(prm, unsigned(wblocks), st, wb, total, ctx->q[Q_MAIN].d_counter, ctx->q[Q_MAIN].d_flags,
+                              epoch, ctx->d_status, learn != nullptr, rec != nullptr);
+        return check_launch("me_frames_wide_kernel");
+    }
     if (nframes <= ME_MAXF) {
         FrameBatch fb;
         memset(&fb, 0, sizeof fb);
         fb.n = nframes;
         memcpy(fb.f, desc.data(), sizeof(FrameDesc) * nframes);
         if (fill_segments(fb) != total) return fail(H264A_E_ARG, "me_frames: internal queue layout error");
-        if (nframes <= ME_WIDE_MAXF) {
-            // few frames: a CTA per MB, the partitions one warp each
-            int wide_sm = 0;
-            rc0 = me_wide_setup(wide_sm);
-            if (rc0) return rc0;
-            long long wblocks = (long long)ctx->num_sms * wide_sm;
-            if (wblocks > total) wblocks = total;
-            launch_me_frames_wide(prm, unsigned(wblocks), st, fb, total, ctx->q[Q_MAIN].d_counter,
-                                  ctx->q[Q_MAIN].d_flags, epoch, ctx->d_status, learn != nullptr);
-            return check_launch("me_frames_wide_kernel");
-        }
         launch_me_frames(prm, unsigned(blocks), st, fb, total, ctx->q[Q_MAIN].d_counter, ctx->q[Q_MAIN].d_flags, epoch,
                          ctx->d_status, learn != nullptr);
         return check_launch("me_frames_kernel");

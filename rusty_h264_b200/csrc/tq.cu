@@ -123,56 +123,6 @@ __global__ void __launch_bounds__(256) dct_quant_8x8_kernel(const uint8_t* __res
     }
 }
 
-// ---- reconstruction ------------------------------------------------------------
-
-// 16 * NORM_ADJUST (transform.rs:15-22) by qp % 6 and position group (both
-// even 0, both odd 1, else 2: POS_GROUP_FLAT, transform.rs:48-52).
-__constant__ int kLevelScale[6][3] = {{160, 256, 208}, {176, 288, 224}, {208, 320, 256},
-                                      {224, 368, 288}, {256, 400, 320}, {288, 464, 368}};
-
-// The inter MB's luma reconstruction of one 4x4 block (mb16.rs:3575-3605):
-// dequantize (transform.rs:233-284, flat scaling) each level, cast it to i16
-// as the reference does, inverse core transform rows then columns with
-// (x + 32) >> 6 (transform_quant.rs:30-35, 56-69), add the prediction and
-// clamp (idct_four_t4_rec, transform_quant.rs:96-119).  Four packed rows out.
-// dc_override (the chroma DC from inverse_quant_chroma_dc) replaces the
-// dequantized coefficient 0 when given.
-__device__ __forceinline__ void rec4x4(const int lv[16], const uint32_t p[4], int qp, uint32_t out[4],
-                                       int dc_override = INT_MIN) {
-    const int m6 = qp % 6, shift = qp / 6;
-    int m[16];
-#pragma unroll
-    for (int i = 0; i < 16; i++) {
-        const int g = ((i >> 2) & 1) == (i & 1) ? ((i & 1) ? 1 : 0) : 2;
-        const int ls = kLevelScale[m6][g];
-        const int d = qp >= 24 ? int(uint32_t(lv[i] * ls) << (shift - 4)) : (lv[i] * ls + (1 << (3 - shift))) >> (4 - shift);
-        m[i] = int(int16_t(d));
-    }
-    if (dc_override != INT_MIN) m[0] = int(int16_t(dc_override));
-#pragma unroll
-    for (int r = 0; r < 4; r++) {
-        const int d0 = m[r * 4], d1 = m[r * 4 + 1], d2 = m[r * 4 + 2], d3 = m[r * 4 + 3];
-        const int e0 = d0 + d2, e1 = d0 - d2, e2 = (d1 >> 1) - d3, e3 = d1 + (d3 >> 1);
-        m[r * 4] = e0 + e3; m[r * 4 + 1] = e1 + e2; m[r * 4 + 2] = e1 - e2; m[r * 4 + 3] = e0 - e3;
-    }
-#pragma unroll
-    for (int c = 0; c < 4; c++) {
-        const int d0 = m[c], d1 = m[4 + c], d2 = m[8 + c], d3 = m[12 + c];
-        const int e0 = d0 + d2, e1 = d0 - d2, e2 = (d1 >> 1) - d3, e3 = d1 + (d3 >> 1);
-        m[c] = e0 + e3; m[4 + c] = e1 + e2; m[8 + c] = e1 - e2; m[12 + c] = e0 - e3;
-    }
-#pragma unroll
-    for (int r = 0; r < 4; r++) {
-        uint32_t w = 0;
-#pragma unroll
-        for (int c = 0; c < 4; c++) {
-            const int v = byte_of(p[r], c) + ((m[r * 4 + c] + 32) >> 6);
-            w |= uint32_t(v < 0 ? 0 : (v > 255 ? 255 : v)) << (8 * c);
-        }
-        out[r] = w;
-    }
-}
-
 // ---- fused MC + luma T/Q of whole frames ---------------------------------------
 
 struct TqFrameDesc {
@@ -273,9 +223,6 @@ extern "C" int h264a_dct_quant_8x8(h264a_ctx* ctx, const uint8_t* d_src, int ss,
 
 // ---- the inter MB's chroma: MC, T/Q with the 2x2 DC, reconstruction -------------
 
-// QUANT_MF[m][0] (transform.rs:25-32), the chroma DC multiplier.
-__constant__ int kQuantMfDc[6] = {13107, 11916, 10082, 9362, 8192, 7282};
-
 struct TqcFrameDesc {
     const uint8_t* src[2];
     const uint8_t* ref[2];
@@ -291,41 +238,8 @@ struct TqcBatch {
     int n;
 };
 
-// Packed 4 pixels of one output row of mc_chroma (inter.rs:1268-1361):
-// (wa·a + wb·b + wc·c + wd·d + 32) >> 6 over rows y, y+1 of the clamped
-// reference, columns x..x+4.
-__device__ __forceinline__ uint32_t chroma_row(const uint8_t* ref, int w, int h, int x, int y, int wa, int wb, int wc,
-                                               int wd) {
-    const int ya = clampi(y, 0, h - 1), yb = clampi(y + 1, 0, h - 1);
-    const uint8_t* ra = ref + (long long)ya * w;
-    const uint8_t* rb = ref + (long long)yb * w;
-    int a[5], b[5];
-    if (x >= 0 && x + 5 <= w) {
-        const uint32_t a0 = ld4u(ra + x), b0 = ld4u(rb + x);
-#pragma unroll
-        for (int k = 0; k < 4; k++) { a[k] = byte_of(a0, k); b[k] = byte_of(b0, k); }
-        a[4] = __ldg(ra + x + 4);
-        b[4] = __ldg(rb + x + 4);
-    } else {
-#pragma unroll
-        for (int k = 0; k < 5; k++) {
-            const int xx = clampi(x + k, 0, w - 1);
-            a[k] = __ldg(ra + xx);
-            b[k] = __ldg(rb + xx);
-        }
-    }
-    uint32_t o = 0;
-#pragma unroll
-    for (int k = 0; k < 4; k++) o |= uint32_t((wa * a[k] + wb * a[k + 1] + wc * b[k] + wd * b[k + 1] + 32) >> 6) << (8 * k);
-    return o;
-}
-
-// One thread per (MB, plane, 4x4 block k in SUBBLOCKS order); the four
-// blocks of a plane are four consecutive lanes, which trade their DC
-// coefficients for the 2x2 transform.  mb16.rs:3408-3428 (chroma MC with the
-// partition's luma MV), 3465-3500 (dct_four_t4, quant_four_4x4 at the chroma
-// QP, forward_quant_chroma_dc, transform.rs:1023), 3606-3628 (dequantize with
-// the DC from inverse_quant_chroma_dc, transform.rs:1038, idct_four_t4_rec).
+// One thread per (MB, plane, 4x4 block k in SUBBLOCKS order), eight
+// consecutive lanes per MB: chroma_tq_rec with the MB's partition MV.
 __global__ void mc_tq_chroma_kernel(const __grid_constant__ TqcBatch batch, long long total_mb, QuantTables4 qt) {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const long long g = t >> 3;
@@ -346,61 +260,10 @@ __global__ void mc_tq_chroma_kernel(const __grid_constant__ TqcBatch batch, long
     const int part = shape == 1 ? (by >= 4) : (shape == 2 ? (bx >= 4) : 0);
     const int mvx = pk[1 + 2 * part], mvy = pk[2 + 2 * part];
     const int x = mbx * 8 + bx, y = mby * 8 + by;
-    const int fx = mvx & 7, fy = mvy & 7;
-    const int wa = (8 - fx) * (8 - fy), wb = fx * (8 - fy), wc = (8 - fx) * fy, wd = fx * fy;
-    uint32_t s[4], p[4];
-#pragma unroll
-    for (int r = 0; r < 4; r++) {
-        s[r] = *reinterpret_cast<const uint32_t*>(fd.src[c] + (long long)(y + r) * fd.ccw + x);
-        p[r] = chroma_row(fd.ref[c], fd.ccw, fd.cch, x + (mvx >> 3), y + r + (mvy >> 3), wa, wb, wc, wd);
-    }
-    int mm[16];
-#pragma unroll
-    for (int r = 0; r < 4; r++)
-#pragma unroll
-        for (int q = 0; q < 4; q++) mm[r * 4 + q] = byte_of(s[r], q) - byte_of(p[r], q);
-    forward_core4(mm);
-    const int dc = int(int16_t(mm[0]));
-    // AC levels (quant_four_4x4); slot 0 carries the DC level below
-    const int q = fd.qpc;
-    int lv[16];
-#pragma unroll
-    for (int i = 0; i < 16; i++) {
-        const int pos = ((i >> 2) & 1) * 4 + (i & 3);
-        const int cc = int(int16_t(mm[i]));
-        const int l = ((abs(cc) + int(qt.ff[q][pos])) * int(qt.mf[q][pos])) >> 16;
-        lv[i] = int(int16_t(cc < 0 ? -l : l));
-    }
-    // 2x2 DC: hadamard_2x2 of the four blocks' DCs, then quant (inter dead-zone)
-    const int base = threadIdx.x & ~3;
-    const int d0 = __shfl_sync(0xffffffffu, dc, base + 0), d1 = __shfl_sync(0xffffffffu, dc, base + 1);
-    const int d2 = __shfl_sync(0xffffffffu, dc, base + 2), d3 = __shfl_sync(0xffffffffu, dc, base + 3);
-    const int sb = k & 1 ? -1 : 1, sc = k & 2 ? -1 : 1;
-    const int f = d0 + sb * d1 + sc * d2 + sb * sc * d3;  // row k of the 2x2 Hadamard
-    const int m6 = q % 6, qbits = 15 + q / 6;
-    const long long off = (1LL << qbits) / 6;
-    const long long la = (long long)(f < 0 ? -f : f) * kQuantMfDc[m6] + 2 * off;
-    const int dl = int(f < 0 ? -(la >> (qbits + 1)) : (la >> (qbits + 1)));
-    int16_t* co = fd.coeffs + (long long)m * 128 + c * 64 + k * 16;
-    if (live) {
-        uint32_t w[8];
-#pragma unroll
-        for (int i = 0; i < 16; i += 2)
-            w[i >> 1] = uint32_t(uint16_t(i == 0 ? dl : lv[i])) | (uint32_t(uint16_t(lv[i + 1])) << 16);
-        uint4* o = reinterpret_cast<uint4*>(co);
-        o[0] = make_uint4(w[0], w[1], w[2], w[3]);
-        o[1] = make_uint4(w[4], w[5], w[6], w[7]);
-    }
-    // reconstruction: inverse_quant_chroma_dc of the DC levels, dequantize of
-    // the AC levels, both cast to i16, then the inverse 4x4 and the add
-    const int l0 = __shfl_sync(0xffffffffu, dl, base + 0), l1 = __shfl_sync(0xffffffffu, dl, base + 1);
-    const int l2 = __shfl_sync(0xffffffffu, dl, base + 2), l3 = __shfl_sync(0xffffffffu, dl, base + 3);
-    if (!live || fd.rec[c] == nullptr) return;
-    const int gk = l0 + sb * l1 + sc * l2 + sb * sc * l3;
-    const int rdc = int(uint32_t(gk * kLevelScale[m6][0]) << (q / 6)) >> 5;
-    lv[0] = 0;
     uint32_t r4[4];
-    rec4x4(lv, p, q, r4, rdc);
+    chroma_tq_rec(fd.src[c], fd.ref[c], fd.ccw, fd.cch, x, y, mvx, mvy, k, fd.qpc, qt.ff[fd.qpc], qt.mf[fd.qpc],
+                  live ? fd.coeffs + (long long)m * 128 + c * 64 + k * 16 : nullptr, r4);
+    if (!live || fd.rec[c] == nullptr) return;
 #pragma unroll
     for (int r = 0; r < 4; r++) *reinterpret_cast<uint32_t*>(fd.rec[c] + (long long)(y + r) * fd.ccw + x) = r4[r];
 }

@@ -61,11 +61,16 @@ def test_struct_layouts_match_header(tmp_path):
     """Every ctypes mirror has the size and field offsets the C compiler gives the header's struct."""
     import subprocess
 
+    from rusty_h264_b200.mvnet import MvnetFrame
+
     mirrors = {"h264a_picture": accel.Picture, "h264a_candidate": accel.Candidate, "h264a_me_params": accel.MeParams,
                "h264a_me_job": accel.MeJob, "h264a_me_result": accel.MeResult, "h264a_me_frame": accel.MeFrame,
                "h264a_me_tq_frame": accel.MeTqFrame,
                "h264a_tq_frame": accel.TqFrame, "h264a_tq_rec_frame": accel.TqRecFrame,
-               "h264a_tq_chroma_frame": accel.TqChromaFrame, "h264a_deblock_frame": accel.DeblockFrame}
+               "h264a_tq_chroma_frame": accel.TqChromaFrame, "h264a_deblock_frame": accel.DeblockFrame,
+               "h264a_me_learned_frame": accel.MeLearnedFrame, "h264a_closed_job": accel.ClosedJob,
+               "h264a_closed_dev": accel.ClosedDev, "h264a_closed_step": accel.ClosedStep,
+               "h264a_stream_frames": accel.StreamFrames, "h264a_mvnet_frame": MvnetFrame}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "h264accel.h"', "int main(void) {"]
     for cname, py in mirrors.items():
         lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')

@@ -1131,6 +1131,83 @@ def test_closed_frames_device_path_equals_host_path(acc):
         _compare_closed(got, want)
 
 
+def _closed_buffers(acc, Y, U, V):
+    torch = acc.torch
+    n, ch, cw = Y.shape
+    nmb = (cw // 16) * (ch // 16)
+    b = dict(y=dev(acc, Y), u=dev(acc, U), v=dev(acc, V))
+    b["ry"], b["ru"], b["rv"] = b["y"].clone(), b["u"].clone(), b["v"].clone()  # frame 0: lossless
+    b["planes"] = acc.empty((4 * (cw + 64) * (ch + 64),), torch.uint8)
+    b["picks"] = acc.zeros((n, nmb, 6), torch.int32)
+    b["costs"] = acc.zeros((n, nmb, 2), torch.int64)
+    b["coeffs"] = acc.zeros((n, nmb, 256), torch.int16)
+    b["ccoeffs"] = acc.zeros((n, nmb, 128), torch.int16)
+    return b
+
+
+def _closed_result(b):
+    return dict(picks=b["picks"].cpu().numpy(), costs=b["costs"].cpu().numpy(), coeffs=b["coeffs"].cpu().numpy(),
+                ccoeffs=b["ccoeffs"].cpu().numpy(), rec_y=b["ry"].cpu().numpy(), rec_u=b["ru"].cpu().numpy(),
+                rec_v=b["rv"].cpu().numpy())
+
+
+def test_closed_step_frame_and_unfused_launches_equal_the_loop(acc):
+    """The loop frame by frame through h264a_closed_step_frame (planes, then
+    the search with each MB's reconstruction and deblocking fused in), and the
+    same frames through the separate launches (plain-ME, MC + luma T/Q +
+    reconstruction, chroma, deblocking), both give what h264a_pixel_path_closed
+    gives."""
+    Y, U, V = _coded_yuv(*synth.cif_clip(5, 9))
+    n, ch, cw = Y.shape
+    fs = cw * ch
+    qp = 29
+    lam = float(np.sqrt(A.frame_lambda(qp)) * 1.25)
+    gate = A.split_gate_for_qp(qp)
+    params = A.default_me_params()
+    want = acc.pixel_path_closed(Y, U, V, params, lam, gate, qp)
+    for fused in (True, False):
+        b = _closed_buffers(acc, Y, U, V)
+        for f in range(1, n):
+            acc._check(acc.L.h264a_hpel_build(acc.ctx, b["ry"][f - 1].data_ptr(), cw, ch, 32, 1, fs,
+                                              b["planes"].data_ptr(), acc._stream()))
+            pic = A.Picture(b["y"][f].data_ptr(), b["planes"].data_ptr(), cw, ch, 32)
+            me = A.MeFrame(pic, lam, gate, b["picks"][f].data_ptr(), b["costs"][f].data_ptr())
+            if fused:
+                acc.closed_step(A.ClosedStep(me, b["u"][f].data_ptr(), b["v"][f].data_ptr(), b["ru"][f - 1].data_ptr(),
+                                             b["rv"][f - 1].data_ptr(), b["ry"][f].data_ptr(), b["ru"][f].data_ptr(),
+                                             b["rv"][f].data_ptr(), b["coeffs"][f].data_ptr(),
+                                             b["ccoeffs"][f].data_ptr(), qp, 6, None, None, 0), params)
+                continue
+            acc.me_frames([me], params)
+            acc.mc_tq_rec_frames([A.TqRecFrame(A.TqFrame(pic, b["picks"][f].data_ptr(), qp, 6,
+                                                         b["coeffs"][f].data_ptr()), b["ry"][f].data_ptr())])
+            acc.mc_tq_chroma_frames([A.TqChromaFrame(b["u"][f].data_ptr(), b["v"][f].data_ptr(),
+                                                     b["ru"][f - 1].data_ptr(), b["rv"][f - 1].data_ptr(), cw, ch,
+                                                     b["picks"][f].data_ptr(), qp, b["ccoeffs"][f].data_ptr(),
+                                                     b["ru"][f].data_ptr(), b["rv"][f].data_ptr())])
+            acc.deblock_frames([A.DeblockFrame(b["ry"][f].data_ptr(), b["ru"][f].data_ptr(), b["rv"][f].data_ptr(), cw,
+                                               ch, b["picks"][f].data_ptr(), b["coeffs"][f].data_ptr(), qp, 0, 0, 0)])
+        acc.sync()
+        _compare_closed(_closed_result(b), want)
+
+
+@pytest.mark.parametrize("h,w,qp", [(16, 16, 20), (32, 48, 36), (288, 32, 24), (48, 352, 44), (144, 176, 14)])
+def test_closed_loop_small_and_narrow_frames_match_oracle(acc, h, w, qp):
+    """Frames of one MB, one MB column or two MB rows (no top-right
+    neighbour, or none above) and QPs from 14 to 44 (every deblocking
+    threshold row, bS 0/1/2) through the fused loop equal the oracle."""
+    y, u, v = synth.cif_clip(4, 17 + h)
+    oy, ox = min(40, 288 - h), min(64, 352 - w)  # even: chroma at half the offsets
+    Y = np.ascontiguousarray(y[:, oy:oy + h, ox:ox + w])
+    U = np.ascontiguousarray(u[:, oy // 2:(oy + h) // 2, ox // 2:(ox + w) // 2])
+    V = np.ascontiguousarray(v[:, oy // 2:(oy + h) // 2, ox // 2:(ox + w) // 2])
+    lam = float(np.sqrt(A.frame_lambda(qp)) * 1.25)
+    gate = A.split_gate_for_qp(qp)
+    got = acc.pixel_path_closed(Y, U, V, A.default_me_params(), lam, gate, qp)
+    want = O.closed_loop_clip(Y, U, V, O.balanced_params(), lam, gate, qp)
+    _compare_closed(got, want)
+
+
 @pytest.mark.parametrize("learned", [False, True])
 def test_me_frames_wide_kernel_equals_batched(acc, learned):
     """Frames run one at a time take the wide kernel (a CTA per MB, the four
