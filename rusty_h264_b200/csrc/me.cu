@@ -32,6 +32,9 @@ namespace h264a {
 
 constexpr int MET_SATD = 0;
 constexpr int MET_SAD = 1;
+// Warps per CTA of the frame kernels (the narrow kernel's MBs per CTA, the
+// wide kernel's warps per MB).
+constexpr int ME_WARPS = 4;
 
 // Per-warp shared state: the round's candidates and distortions, and the
 // search's cold parameters (read a few times per round, so they live here
@@ -626,17 +629,23 @@ __device__ __forceinline__ void group_geom_init(GroupGeom& q, WarpScratch& ws, c
 // than a shuffle tree over the candidate's lanes.  A group prices
 // 2^(lg - lg_nb) candidates per pass; passes run to the largest need over the
 // groups.  SATD_ONLY: the caller's preset never prices with SAD (Balanced).
-template <bool SATD_ONLY>
-__device__ __forceinline__ void eval_round_group(const GroupGeom& q, WarpScratch& ws, int n, int metric) {
+// COOP (the wide kernel's 16x16 search, run by the CTA's ME_WARPS warps with
+// the same state): warp w prices candidates c with (c >> 1) % ME_WARPS == w,
+// two per pass, into the CTA-shared slots `dist` (its own slots only).
+template <bool SATD_ONLY, bool COOP = false>
+__device__ __forceinline__ void eval_round_group(const GroupGeom& q, WarpScratch& ws, int n, int metric,
+                                                 int* dist = nullptr) {
     const SearchGeom& g = q.s;
     const int cps = q.lg - g.lg_nb;  // log2 candidates per pass of a group
-    const int npass = __reduce_max_sync(0xffffffffu, (n + (1 << cps) - 1) >> cps);
+    const int npass = COOP ? (n + 2 * ME_WARPS - 1) / (2 * ME_WARPS)
+                           : __reduce_max_sync(0xffffffffu, (n + (1 << cps) - 1) >> cps);
     const int sub = q.gl >> g.lg_nb;  // which of the pass's candidates the lane serves
+    const int wofs = COOP ? 2 * int(threadIdx.x >> 5) : 0;
     for (int k0 = 0; k0 < npass; k0 += ME_MAX_PASS) {
         uint32_t pr4[ME_MAX_PASS][4];
 #pragma unroll
         for (int kk = 0; kk < ME_MAX_PASS; kk++) {
-            const int c = ((k0 + kk) << cps) + sub;
+            const int c = COOP ? (k0 + kk) * 2 * ME_WARPS + wofs + sub : ((k0 + kk) << cps) + sub;
             if (k0 + kk < npass && c < n) {
                 const int2 mv = ws.cand[q.gb + c];
                 const int dx = mv.x >> 2, dy = mv.y >> 2;
@@ -654,7 +663,7 @@ __device__ __forceinline__ void eval_round_group(const GroupGeom& q, WarpScratch
         for (int kk = 0; kk < ME_MAX_PASS; kk++) {
             const int k = k0 + kk;
             if (k < npass) {
-                const int c = (k << cps) + sub;
+                const int c = COOP ? k * 2 * ME_WARPS + wofs + sub : (k << cps) + sub;
                 int d = 0;
                 if (c < n) {
                     if (!SATD_ONLY && metric == MET_SAD) {
@@ -666,7 +675,7 @@ __device__ __forceinline__ void eval_round_group(const GroupGeom& q, WarpScratch
                         d = satd4x4_packed(g.spa, g.spb, pr4[kk]);
                     }
                 }
-                if (c < n) atomicAdd(&ws.dist[q.gb + c], d);  // the candidate's blocks, summed in shared memory
+                if (c < n) atomicAdd(COOP ? &dist[c] : &ws.dist[q.gb + c], d);  // the candidate's blocks, summed in shared memory
             }
         }
     }
@@ -713,11 +722,19 @@ struct Knobs {
 // more than prop_t it falls back to the plain search (fell = 1), otherwise it
 // continues as motion_search with the cheapest of the nine as its start
 // vector (mb16.rs:2445, 2579-2596: refine-only, no full-pel phase).
-template <bool BAL, bool LEARN = false>
+//
+// RF / RR: the ring batches (RING_FIRST / RING_REST) of this search; wider
+// batches where a pass prices more candidates at once.  COOP: the search is
+// run by all ME_WARPS warps of the CTA with identical state (each warp its
+// own `ws`, the same plan and fold), the pricing split between them
+// (eval_round_group) into the CTA-shared distortions cdist[2][32], one named
+// barrier per round (the two halves alternate by round).
+template <bool BAL, bool LEARN = false, int RF = RING_FIRST, int RR = RING_REST, bool COOP = false>
 __device__ __forceinline__ void motion_search_group(const GroupGeom& q, const MeParamsDev& prm, WarpScratch& ws,
                                                     const int* preds, int npred, double lambda_me, int& out_x,
                                                     int& out_y, long long& out_c, int& evals, bool use_prop = false,
-                                                    int2 prop = make_int2(0, 0), int prop_t = 0, int* fell = nullptr) {
+                                                    int2 prop = make_int2(0, 0), int prop_t = 0, int* fell = nullptr,
+                                                    int* cdist = nullptr) {
     const Knobs<BAL> pr{prm};
     const int gl = q.gl, gb = q.gb;
     const bool sadfp = !pr.fast() && pr.sadfp();
@@ -758,7 +775,12 @@ __device__ __forceinline__ void motion_search_group(const GroupGeom& q, const Me
     int si = -1, sk = -1, loops = 0, iter = 0, step = 0;
     bool ring_open = false, ring_improved = false;
     int ring_i = 0, ring_n = 0;
+    int round = 0;
     for (;;) {
+        // the round's distortion slots: the warp's own, or the CTA's half for
+        // this round
+        int* const dist = COOP ? cdist + 32 * (round & 1) : ws.dist + gb;
+        round++;
         // ---------- plan (per group) ----------
         int kind = -1, n = 0, metric = m_main;
         double lam = ws.lam_r;
@@ -771,7 +793,7 @@ __device__ __forceinline__ void motion_search_group(const GroupGeom& q, const Me
                 kind = EV_PROP; n = N_PROP + 1; metric = m_main; lam = ws.lam_r;
             } else if (phase == PH_DIA) {
                 if (ring_open) {
-                    kind = EV_RING; n = min(ring_n - ring_i, RING_REST); metric = m_fp; lam = l_fp;
+                    kind = EV_RING; n = min(ring_n - ring_i, RR); metric = m_fp; lam = l_fp;
                     if (gl < n)
                         ws.cand[gb + gl] = make_int2(bx + ring_dx(ring_i + gl) * step, by + ring_dy(ring_i + gl) * step);
                     break;
@@ -817,7 +839,7 @@ __device__ __forceinline__ void motion_search_group(const GroupGeom& q, const Me
                 }
             } else {  // PH_SUB
                 if (ring_open) {
-                    kind = EV_RING; n = min(ring_n - ring_i, RING_REST); metric = m_main; lam = ws.lam_r;
+                    kind = EV_RING; n = min(ring_n - ring_i, RR); metric = m_main; lam = ws.lam_r;
                     if (gl < n)
                         ws.cand[gb + gl] = make_int2(bx + ring_dx(ring_i + gl) * step, by + ring_dy(ring_i + gl) * step);
                     break;
@@ -852,7 +874,7 @@ __device__ __forceinline__ void motion_search_group(const GroupGeom& q, const Me
                     }
                 }
                 iter++;
-                n = min(sp_nring, RING_FIRST);
+                n = min(sp_nring, RF);
                 if (gl < n) ws.cand[gb + gl] = make_int2(bx + ring_dx(gl) * step, by + ring_dy(gl) * step);
                 ring_open = true; ring_improved = false; ring_i = 0; ring_n = sp_nring;
                 kind = EV_RING; metric = m_main; lam = ws.lam_r;
@@ -867,16 +889,23 @@ __device__ __forceinline__ void motion_search_group(const GroupGeom& q, const Me
         const bool need_min = __any_sync(0xffffffffu, kind == EV_FIXED);
         const bool need_hit = __any_sync(0xffffffffu, kind == EV_RING);
         const bool need_seed = __any_sync(0xffffffffu, kind == EV_SEEDS || kind == EV_REPRICE);
-        if (gl < n) ws.dist[gb + gl] = 0;  // the pricing adds each lane's block into its candidate's slot
+        if (COOP) {
+            // the warp zeroes the slots of the candidates it prices
+            const int zc = (gl >> 1) * 2 * ME_WARPS + 2 * int(threadIdx.x >> 5) + (gl & 1);
+            if (gl < 8 && zc < n) dist[zc] = 0;
+        } else if (gl < n) {
+            dist[gl] = 0;  // the pricing adds each lane's block into its candidate's slot
+        }
         __syncwarp();
         __syncwarp();
 
         // ---------- price ----------
-        eval_round_group<BAL>(q, ws, n, metric);
+        eval_round_group<BAL, COOP>(q, ws, n, metric, dist);
+        if (COOP) asm volatile("bar.sync 1, %0;" ::"n"(32 * ME_WARPS) : "memory");
         int cc = INT_MAX;  // dist + λ·rate of slot gb + gl, as lane_cost prices it
         if (gl < n) {
             const int2 mv = ws.cand[gb + gl];
-            const long long c = (long long)ws.dist[gb + gl] + lam_cost(lam, pr.rate(ws, mv.x, mv.y));
+            const long long c = (long long)dist[gl] + lam_cost(lam, pr.rate(ws, mv.x, mv.y));
             cc = c > INT_MAX - 1 ? INT_MAX - 1 : int(c);
         }
         // group-wide collectives, taken by every lane (each only in rounds
@@ -920,7 +949,7 @@ __device__ __forceinline__ void motion_search_group(const GroupGeom& q, const Me
             if ((snaps >> wi) & 1u) {
                 const int sl = gb + npred + 1 + __popc(snaps & ((1u << wi) - 1u));
                 bx = ws.cand[sl].x; by = ws.cand[sl].y;
-                best_c = int(((long long)ws.dist[sl] + lam_cost(lam, pr.rate(ws, ws.cand[sl].x, ws.cand[sl].y))));
+                best_c = int(((long long)dist[sl - gb] + lam_cost(lam, pr.rate(ws, ws.cand[sl].x, ws.cand[sl].y))));
                 evals += 1;
             }
             phase = PH_DIA;
@@ -931,12 +960,12 @@ __device__ __forceinline__ void motion_search_group(const GroupGeom& q, const Me
             long long cbest = 0, cprop = 0;
             for (int i = 0; i <= N_PROP; i++) {
                 const int2 mv = ws.cand[gb + i];
-                const long long c = (long long)ws.dist[gb + i] + lam_cost(lam, pr.rate(ws, mv.x, mv.y));
+                const long long c = (long long)dist[i] + lam_cost(lam, pr.rate(ws, mv.x, mv.y));
                 if (i == 0 || c < cbest) { cbest = c; bi = i; }
                 if (i == 1 || (i > 1 && c < cprop)) { cprop = c; bp = i; }
             }
             evals += N_PROP + 1;
-            const bool fb = (long long)ws.dist[gb + bp] > (long long)ws.dist[gb] + prop_t;
+            const bool fb = (long long)dist[bp] > (long long)dist[0] + prop_t;
             if (fell) *fell = fb ? 1 : 0;
             if (fb) {
                 // the plain search's seed slots again (the round above used
@@ -955,8 +984,8 @@ __device__ __forceinline__ void motion_search_group(const GroupGeom& q, const Me
                 phase = PH_SUB;  // a start vector: no full-pel phase, no B2 reprice
             }
         } else if (kind == EV_REPRICE) {
-            best_c = int(((long long)ws.dist[gb] + lam_cost(lam, pr.rate(ws, ws.cand[gb].x, ws.cand[gb].y))));
-            seed_c = int(((long long)ws.dist[gb + 1] + lam_cost(lam, pr.rate(ws, ws.cand[gb + 1].x, ws.cand[gb + 1].y))));
+            best_c = int(((long long)dist[0] + lam_cost(lam, pr.rate(ws, ws.cand[gb].x, ws.cand[gb].y))));
+            seed_c = int(((long long)dist[1] + lam_cost(lam, pr.rate(ws, ws.cand[gb + 1].x, ws.cand[gb + 1].y))));
             evals += 2;
             phase = PH_SUB;
         } else if (kind == EV_FIXED) {
@@ -1010,7 +1039,6 @@ __device__ __forceinline__ bool job_shape_ok(int w, int h) {
            (w == 4 && (h == 8 || h == 4));
 }
 
-constexpr int ME_WARPS = 4;
 #ifndef ME_MIN_BLOCKS
 #define ME_MIN_BLOCKS 4
 #endif
@@ -1387,6 +1415,7 @@ struct WideTable {
 
 struct WideMb {
     int t;                  // the CTA's ticket
+    int pmvx, pmvy;         // the median predictor
     long long c16;          // 16x16 J
     int mv16x, mv16y, ev16;
     int px[4], py[4], pev[4];
@@ -1400,6 +1429,7 @@ __device__ __forceinline__ void me_frames_body_wide(const WideTable& tab, long l
     __shared__ WarpScratch scratch[ME_WARPS];
     __shared__ __align__(8) unsigned long long win_bar;
     __shared__ WideMb mb;
+    __shared__ int coop_dist[2][32];  // the cooperative 16x16 search's distortions
     // REC: the MB's reconstruction tiles (deblock_device.cuh's layout), its
     // luma blocks' coefficient flags (raster order) and the edges' bS
     __shared__ __align__(16) uint8_t rec_lt[REC ? LT * LT : 4];
@@ -1441,16 +1471,19 @@ __device__ __forceinline__ void me_frames_body_wide(const WideTable& tab, long l
                             ph >= WIN_H;
         int preds[4] = {0, 0, 0, 0};
         int fell = 0;
-        if (w == 0) {
-            uint32_t src4[4];
+        // every warp's source rows of its lane's 4x4 block in the 16x16 search
+        // (block lane & 15) and, for the learned search, its proposal (lane
+        // gl holds proposal gl - 1), loaded before the neighbour wait
+        uint32_t src4[4];
 #pragma unroll
-            for (int r = 0; r < 4; r++)
-                src4[r] = ld4u(pc.d_src + (long long)(ly + ((lane >> 2) & 3) * 4 + r) * pc.cw + lx + (lane & 3) * 4);
-            int2 prop = make_int2(0, 0);
-            if (LEARN && lane >= 1 && lane <= N_PROP) {
-                const int32_t* pp = fd.props + 16LL * m + 2 * (lane - 1);
-                prop = make_int2(__ldg(pp), __ldg(pp + 1));
-            }
+        for (int r = 0; r < 4; r++)
+            src4[r] = ld4u(pc.d_src + (long long)(ly + ((lane >> 2) & 3) * 4 + r) * pc.cw + lx + (lane & 3) * 4);
+        int2 prop = make_int2(0, 0);
+        if (LEARN && lane >= 1 && lane <= N_PROP) {
+            const int32_t* pp = fd.props + 16LL * m + 2 * (lane - 1);
+            prop = make_int2(__ldg(pp), __ldg(pp + 1));
+        }
+        if (w == 0) {
             if (lane == 0) {
                 if (mbx > 0) wait_flag(fl + m - 1, epoch, status, 1, spin_limit);
                 if (mby > 0) wait_flag(fl + m - fd.mb_w + (mbx < fd.mb_w - 1 ? 1 : 0), epoch, status, 1, spin_limit);
@@ -1466,6 +1499,11 @@ __device__ __forceinline__ void me_frames_body_wide(const WideTable& tab, long l
                 c = da ? pick_mv_at(fd.picks, m - fd.mb_w - 1, 3, 3) : make_int2(0, 0);
             }
             const int2 pmv = predict_mv_ref0(aa, a, ba, bb, cav, c);
+            if (lane == 0) {
+                mb.pmvx = pmv.x;
+                mb.pmvy = pmv.y;
+                scratch[0].win_ok = win_ok;
+            }
             if (win_ok) {
                 const int wx0 = min(max((lx + pc.pad + (pmv.x >> 2) - WIN_R) & ~15, 0), pw - WIN_W);
                 const int wy0 = min(max(ly + pc.pad + (pmv.y >> 2) - WIN_R, 0), ph - WIN_H);
@@ -1492,50 +1530,45 @@ __device__ __forceinline__ void me_frames_body_wide(const WideTable& tab, long l
                     }
                 }
             }
-            if (lane == 0) scratch[0].win_ok = win_ok;
-            __syncwarp();
-            preds[0] = pmv.x;
-            preds[1] = pmv.y;
-            GroupGeom qg;
-            group_geom_init(qg, scratch[0], pc, lx, ly, 0, win, src4);
-            if (win_ok) wait_window(bar, parity, status, 3, spin_limit);
-            int rx, ry, ev;
-            long long rc;
-            motion_search_group<BAL, LEARN>(qg, prm, scratch[0], preds, 1, fd.lambda_me, rx, ry, rc, ev, LEARN, prop,
-                                            fd.prop_t, &fell);
-            if (lane == 0) {
-                mb.c16 = rc;
-                mb.mv16x = rx;
-                mb.mv16y = ry;
-                mb.ev16 = ev << 4;
-            }
         }
-        __syncthreads();
-        // warp 0 saw the window's copy complete before the barrier, so this
-        // wait of the other warps returns at once; every warp then tracks the
-        // barrier's next phase
-        if (w > 0 && win_ok) wait_window(bar, parity, status, 3, spin_limit);
-        if (win_ok) parity ^= 1u;
-        const bool gated = fd.split_gate >= 0 && mb.c16 > fd.split_gate;
+        __syncthreads();  // the predictor and the window's origin are in shared memory
+        if (lane == 0 && w > 0) {
+            scratch[w].win_ok = scratch[0].win_ok;
+            scratch[w].wx0 = scratch[0].wx0;
+            scratch[w].wy0 = scratch[0].wy0;
+        }
+        __syncwarp();
+        preds[0] = mb.pmvx;
+        preds[1] = mb.pmvy;
+        // the 16x16 search by all warps together (eight candidates per pass)
+        int rx16, ry16, ev16;
+        long long c16;
+        {
+            GroupGeom qg;
+            group_geom_init(qg, scratch[w], pc, lx, ly, 0, win, src4);
+            if (win_ok) wait_window(bar, parity, status, 3, spin_limit);
+            if (win_ok) parity ^= 1u;
+            motion_search_group<BAL, LEARN, 2 * ME_WARPS, 2 * ME_WARPS, true>(
+                qg, prm, scratch[w], preds, 1, fd.lambda_me, rx16, ry16, c16, ev16, LEARN, prop, fd.prop_t, &fell,
+                &coop_dist[0][0]);
+        }
+        if (w == 0 && lane == 0) {
+            mb.c16 = c16;
+            mb.mv16x = rx16;
+            mb.mv16y = ry16;
+            mb.ev16 = ev16 << 4;
+        }
+        // every warp holds the same 16x16 result: the gate and the partition
+        // searches' seeds need no barrier
+        const bool gated = fd.split_gate >= 0 && c16 > fd.split_gate;
         if (gated) {
-            if (lane == 0 && w > 0) {
-                scratch[w].win_ok = scratch[0].win_ok;
-                scratch[w].wx0 = scratch[0].wx0;
-                scratch[w].wy0 = scratch[0].wy0;
-            }
-            __syncwarp();
-            if (w > 0) {
-                // the predictor, from warp 0's search state
-                preds[0] = scratch[0].cx;
-                preds[1] = scratch[0].cy;
-            }
-            preds[2] = mb.mv16x;
-            preds[3] = mb.mv16y;
+            preds[2] = rx16;
+            preds[3] = ry16;
             GroupGeom qg;
             group_geom_init(qg, scratch[w], pc, lx, ly, 2, win, nullptr, w);
             int rx, ry, ev;
             long long rc;
-            motion_search_group<BAL, false>(qg, prm, scratch[w], preds, 2, fd.lambda_me, rx, ry, rc, ev);
+            motion_search_group<BAL, false, 4, 4>(qg, prm, scratch[w], preds, 2, fd.lambda_me, rx, ry, rc, ev);
             if (lane == 0) {
                 mb.px[w] = rx;
                 mb.py[w] = ry;
@@ -1546,9 +1579,8 @@ __device__ __forceinline__ void me_frames_body_wide(const WideTable& tab, long l
         __syncthreads();
         // the shape decision (mb16.rs:8869-8913), taken by every warp from
         // the shared results
-        int evals = mb.ev16, shape = 0;
-        int mv0x = mb.mv16x, mv0y = mb.mv16y, mv1x = mb.mv16x, mv1y = mb.mv16y;
-        const long long c16 = mb.c16;
+        int evals = ev16 << 4, shape = 0;
+        int mv0x = rx16, mv0y = ry16, mv1x = rx16, mv1y = ry16;
         long long best = c16;
         if (gated) {
             evals += mb.pev[0] + mb.pev[1] + mb.pev[2] + mb.pev[3];

@@ -233,6 +233,43 @@ def test_me_search_matches_oracle(acc, cif, name, ov, tab):
         assert (got[i, 0], got[i, 1], got[i, 2]) == (mx, my, cost), (name, i, j.x, j.y, j.w, j.h, preds, start)
 
 
+def test_me_search_known_answers(acc):
+    """The hand-traced cases of test_search_known_answers (the fixed arm's
+    lam_fp, the snap, the seed restore, the mid-ring centre move) through
+    h264a_me_search: the same vectors, costs and evaluation counts."""
+    import test_search_known_answers as K
+
+    n = 64
+    xx, yy = np.arange(n)[None, :], np.arange(n)[:, None]
+    ref2 = (10 + 2 * xx + yy).astype(np.uint8)
+    src2 = (ref2 + 3).astype(np.uint8)
+    cases = [  # (src, ref, x, y, preds, lambda, knobs, expected)
+        (K.ramp_src(6), K.REF, 32, [0, 0], 40.0, {"mv_cost_kind": 1}, ((0, 0), 1596, 6)),
+        (K.ramp_src(6), K.REF, 32, [0, 0], 40.0, {}, ((12, 0), 400, 18)),
+        (K.ramp_src(6), K.REF, 32, [0, 0], 10.0, {"mv_cost_kind": 1}, ((12, 0), 390, 18)),
+        (K.ramp_src(4), K.REF, 32, [6, 0], 40.0, {}, ((8, 0), 240, 7)),
+        (K.ramp_src(4), K.REF, 32, [6, 0], 40.0, {"me_snap": 0}, ((6, 0), 336, 6)),
+        (K.ramp_src(1), K.REF, 32, [2, 0], 40.0, {}, ((2, 0), 80, 7)),
+        (src2, ref2, 16, [0, 0], 4.0, {"me_fc": 0}, ((4, 4), 56, 10)),
+        (src2, ref2, 16, [0, 0], 4.0, {}, ((4, 4), 56, 14)),
+    ]
+    d_tab = dev(acc, O.mv_cost_table())
+    for src, ref, xy, preds, lam, kn, want in cases:
+        d_src, d_pl = dev(acc, src), dev(acc, O.build_planes4(ref, 32))
+        d_pics, _ = acc.pictures([d_src], [d_pl])
+        params = A.default_me_params(dia_mask=0b10000, subpel=0, **kn)
+        params.d_mv_cost_tab = d_tab.data_ptr()
+        j = A.MeJob()
+        j.pic, j.x, j.y, j.w, j.h, j.npred = 0, xy, xy, 16, 16, 1
+        j.preds[0], j.preds[1] = preds
+        j.lambda_me = lam
+        raw = acc.me_search(d_pics, 1, params, [j])
+        acc.sync()
+        got = acc.me_results(raw)[0]
+        assert got[4] == 0
+        assert ((int(got[0]), int(got[1])), int(got[2]), int(got[3])) == want, (kn, want)
+
+
 def test_me_search_rejects_bad_jobs(acc, cif):
     d_src, d_pl = dev(acc, cif[1]), dev(acc, O.build_planes4(cif[0], 32))
     d_pics, _ = acc.pictures([d_src], [d_pl])
