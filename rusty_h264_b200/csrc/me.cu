@@ -32,9 +32,14 @@ namespace h264a {
 
 constexpr int MET_SATD = 0;
 constexpr int MET_SAD = 1;
-// Warps per CTA of the frame kernels (the narrow kernel's MBs per CTA, the
-// wide kernel's warps per MB).
+// Warps per CTA of the narrow frame kernel (one MB per warp) and of the wide
+// one (one MB per CTA: the 16x16 search by all its warps, each partition by
+// one warp).  Four: one warp per SM sub-partition, since the warps of a team
+// repeat the same control code and two of them on one sub-partition would
+// share its issue slots.
 constexpr int ME_WARPS = 4;
+constexpr int ME_WIDE_WARPS = 4;
+constexpr int ME_PART_TEAM = ME_WIDE_WARPS / 4;  // warps per partition search
 
 // Per-warp shared state: the round's candidates and distortions, and the
 // search's cold parameters (read a few times per round, so they live here
@@ -629,23 +634,30 @@ __device__ __forceinline__ void group_geom_init(GroupGeom& q, WarpScratch& ws, c
 // than a shuffle tree over the candidate's lanes.  A group prices
 // 2^(lg - lg_nb) candidates per pass; passes run to the largest need over the
 // groups.  SATD_ONLY: the caller's preset never prices with SAD (Balanced).
-// COOP (the wide kernel's 16x16 search, run by the CTA's ME_WARPS warps with
-// the same state): warp w prices candidates c with (c >> 1) % ME_WARPS == w,
-// two per pass, into the CTA-shared slots `dist` (its own slots only).
-template <bool SATD_ONLY, bool COOP = false>
+// TW > 1 (a search run by a team of TW warps with the same state, the wide
+// kernel's): warp tw of the team prices, in each pass, the candidates
+// [tw * cpw, (tw + 1) * cpw) of that pass's TW * cpw (cpw = the warp's
+// candidates per pass), into the team's shared slots `dist` (its own slots
+// only).
+template <int TW>
+__device__ __forceinline__ int team_cand(int k, int cpw, int sub) {
+    return (k * TW + int(threadIdx.x >> 5) % TW) * cpw + sub;
+}
+
+template <bool SATD_ONLY, int TW = 1>
 __device__ __forceinline__ void eval_round_group(const GroupGeom& q, WarpScratch& ws, int n, int metric,
                                                  int* dist = nullptr) {
+    constexpr bool COOP = TW > 1;
     const SearchGeom& g = q.s;
     const int cps = q.lg - g.lg_nb;  // log2 candidates per pass of a group
-    const int npass = COOP ? (n + 2 * ME_WARPS - 1) / (2 * ME_WARPS)
+    const int npass = COOP ? (n + (TW << cps) - 1) / (TW << cps)
                            : __reduce_max_sync(0xffffffffu, (n + (1 << cps) - 1) >> cps);
     const int sub = q.gl >> g.lg_nb;  // which of the pass's candidates the lane serves
-    const int wofs = COOP ? 2 * int(threadIdx.x >> 5) : 0;
     for (int k0 = 0; k0 < npass; k0 += ME_MAX_PASS) {
         uint32_t pr4[ME_MAX_PASS][4];
 #pragma unroll
         for (int kk = 0; kk < ME_MAX_PASS; kk++) {
-            const int c = COOP ? (k0 + kk) * 2 * ME_WARPS + wofs + sub : ((k0 + kk) << cps) + sub;
+            const int c = COOP ? team_cand<TW>(k0 + kk, 1 << cps, sub) : ((k0 + kk) << cps) + sub;
             if (k0 + kk < npass && c < n) {
                 const int2 mv = ws.cand[q.gb + c];
                 const int dx = mv.x >> 2, dy = mv.y >> 2;
@@ -663,7 +675,7 @@ __device__ __forceinline__ void eval_round_group(const GroupGeom& q, WarpScratch
         for (int kk = 0; kk < ME_MAX_PASS; kk++) {
             const int k = k0 + kk;
             if (k < npass) {
-                const int c = COOP ? k * 2 * ME_WARPS + wofs + sub : (k << cps) + sub;
+                const int c = COOP ? team_cand<TW>(k, 1 << cps, sub) : (k << cps) + sub;
                 int d = 0;
                 if (c < n) {
                     if (!SATD_ONLY && metric == MET_SAD) {
@@ -724,12 +736,13 @@ struct Knobs {
 // vector (mb16.rs:2445, 2579-2596: refine-only, no full-pel phase).
 //
 // RF / RR: the ring batches (RING_FIRST / RING_REST) of this search; wider
-// batches where a pass prices more candidates at once.  COOP: the search is
-// run by all ME_WARPS warps of the CTA with identical state (each warp its
+// batches where a pass prices more candidates at once.  TW > 1: the search is
+// run by a team of TW consecutive warps with identical state (each warp its
 // own `ws`, the same plan and fold), the pricing split between them
-// (eval_round_group) into the CTA-shared distortions cdist[2][32], one named
-// barrier per round (the two halves alternate by round).
-template <bool BAL, bool LEARN = false, int RF = RING_FIRST, int RR = RING_REST, bool COOP = false>
+// (eval_round_group) into the team's shared distortions cdist[2][32], one
+// named barrier (1 + the team's index) per round, the two halves alternating
+// by round.
+template <bool BAL, bool LEARN = false, int RF = RING_FIRST, int RR = RING_REST, int TW = 1>
 __device__ __forceinline__ void motion_search_group(const GroupGeom& q, const MeParamsDev& prm, WarpScratch& ws,
                                                     const int* preds, int npred, double lambda_me, int& out_x,
                                                     int& out_y, long long& out_c, int& evals, bool use_prop = false,
@@ -775,10 +788,12 @@ __device__ __forceinline__ void motion_search_group(const GroupGeom& q, const Me
     int si = -1, sk = -1, loops = 0, iter = 0, step = 0;
     bool ring_open = false, ring_improved = false;
     int ring_i = 0, ring_n = 0;
+    constexpr bool COOP = TW > 1;
+    const int team_bar = 1 + int(threadIdx.x >> 5) / TW;
     int round = 0;
     for (;;) {
-        // the round's distortion slots: the warp's own, or the CTA's half for
-        // this round
+        // the round's distortion slots: the warp's own, or the team's half
+        // for this round
         int* const dist = COOP ? cdist + 32 * (round & 1) : ws.dist + gb;
         round++;
         // ---------- plan (per group) ----------
@@ -890,8 +905,10 @@ __device__ __forceinline__ void motion_search_group(const GroupGeom& q, const Me
         const bool need_hit = __any_sync(0xffffffffu, kind == EV_RING);
         const bool need_seed = __any_sync(0xffffffffu, kind == EV_SEEDS || kind == EV_REPRICE);
         if (COOP) {
-            // the warp zeroes the slots of the candidates it prices
-            const int zc = (gl >> 1) * 2 * ME_WARPS + 2 * int(threadIdx.x >> 5) + (gl & 1);
+            // the warp zeroes the slots of the candidates it prices (lane gl
+            // < 8: pass gl / cpw, candidate gl % cpw of the warp's share)
+            const int cpw = 1 << (q.lg - q.s.lg_nb);
+            const int zc = team_cand<TW>(gl / cpw, cpw, gl % cpw);
             if (gl < 8 && zc < n) dist[zc] = 0;
         } else if (gl < n) {
             dist[gl] = 0;  // the pricing adds each lane's block into its candidate's slot
@@ -900,8 +917,8 @@ __device__ __forceinline__ void motion_search_group(const GroupGeom& q, const Me
         __syncwarp();
 
         // ---------- price ----------
-        eval_round_group<BAL, COOP>(q, ws, n, metric, dist);
-        if (COOP) asm volatile("bar.sync 1, %0;" ::"n"(32 * ME_WARPS) : "memory");
+        eval_round_group<BAL, TW>(q, ws, n, metric, dist);
+        if (COOP) asm volatile("bar.sync %0, %1;" ::"r"(team_bar), "r"(32 * TW) : "memory");
         int cc = INT_MAX;  // dist + λ·rate of slot gb + gl, as lane_cost prices it
         if (gl < n) {
             const int2 mv = ws.cand[gb + gl];
@@ -1413,6 +1430,37 @@ struct WideTable {
     __device__ __forceinline__ const RecDesc& rd(int i) const { return b.rec[i]; }
 };
 
+// The wide kernel publishes each MB's pick to the wavefront as three 64-bit
+// words, each the launch's epoch (high half) and one MV (x, y as i16, low
+// half): the MVs of its blocks (3,0), (0,3) and (3,3), which are what its
+// right, lower (and lower-left) and lower-right neighbours' median predictors
+// read (mv_neighbors_block, mb16.rs:1871).  A waiting MB polls the words it
+// needs until their epoch is the launch's, so the flag and the data arrive in
+// one load and no release fence orders anything else.  MVs fit i16 because
+// the search keeps every block inside the padded picture (at most 8191
+// samples wide or high here).
+constexpr int EW_PER_MB = 3;
+__device__ __forceinline__ unsigned long long mv_word(int epoch, int x, int y) {
+    return ((unsigned long long)(unsigned)epoch << 32) | (uint32_t(uint16_t(x)) | (uint32_t(uint16_t(y)) << 16));
+}
+__device__ __forceinline__ void st_relaxed_u64(unsigned long long* p, unsigned long long v) {
+    asm volatile("st.relaxed.gpu.global.b64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+// Waits (bounded; status 1 on timeout) for the word to carry `epoch`; returns its MV.
+__device__ __forceinline__ int2 wait_mv_word(const unsigned long long* p, int epoch, int* status, int limit) {
+    unsigned long long v = 0;
+    for (int it = 0;; it++) {
+        asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+        if (int(v >> 32) == epoch) break;
+        if (it >= limit) {
+            atomicCAS(status, 0, 1);
+            break;
+        }
+        if (it >= 32) __nanosleep(64);
+    }
+    return make_int2(int(int16_t(v & 0xffffu)), int(int16_t((v >> 16) & 0xffffu)));
+}
+
 struct WideMb {
     int t;                  // the CTA's ticket
     int pmvx, pmvy;         // the median predictor
@@ -1426,10 +1474,11 @@ template <bool BAL, bool LEARN, bool REC>
 __device__ __forceinline__ void me_frames_body_wide(const WideTable& tab, long long total, const MeParamsDev& prm,
                                                     int* __restrict__ counter, int* __restrict__ flags, int epoch,
                                                     int* __restrict__ status, int spin_limit) {
-    __shared__ WarpScratch scratch[ME_WARPS];
+    __shared__ WarpScratch scratch[ME_WIDE_WARPS];
     __shared__ __align__(8) unsigned long long win_bar;
     __shared__ WideMb mb;
-    __shared__ int coop_dist[2][32];  // the cooperative 16x16 search's distortions
+    __shared__ int coop_dist[2][32];     // the team-wide 16x16 search's distortions
+    __shared__ int part_dist[4][2][32];  // each partition team's
     // REC: the MB's reconstruction tiles (deblock_device.cuh's layout), its
     // luma blocks' coefficient flags (raster order) and the edges' bS
     __shared__ __align__(16) uint8_t rec_lt[REC ? LT * LT : 4];
@@ -1463,7 +1512,7 @@ __device__ __forceinline__ void me_frames_body_wide(const WideTable& tab, long l
         int mbx, mby;
         wave_mb(fd.mb_w, fd.mb_h, k, mbx, mby);
         const int m = mby * fd.mb_w + mbx;
-        int* fl = flags + fd.flag_base;
+        unsigned long long* const ew = reinterpret_cast<unsigned long long*>(flags) + EW_PER_MB * (fd.flag_base + m);
         const int lx = mbx * 16, ly = mby * 16;
         const h264a_picture& pc = fd.pic;
         const int pw = pc.cw + 2 * pc.pad, ph = pc.ch + 2 * pc.pad;
@@ -1484,21 +1533,21 @@ __device__ __forceinline__ void me_frames_body_wide(const WideTable& tab, long l
             prop = make_int2(__ldg(pp), __ldg(pp + 1));
         }
         if (w == 0) {
-            if (lane == 0) {
-                if (mbx > 0) wait_flag(fl + m - 1, epoch, status, 1, spin_limit);
-                if (mby > 0) wait_flag(fl + m - fd.mb_w + (mbx < fd.mb_w - 1 ? 1 : 0), epoch, status, 1, spin_limit);
+            // the neighbours' published MVs: lane 0 the left MB's (3,0), lane
+            // 1 the top MB's (0,3), lane 2 the top-right MB's (0,3), lane 3
+            // the top-left MB's (3,3) when there is no top-right
+            const bool aa = mbx > 0, ba = mby > 0, ca = mby > 0 && mbx < fd.mb_w - 1, da = mbx > 0 && mby > 0;
+            int2 nv = make_int2(0, 0);
+            if (lane < 4 && (lane == 0 ? aa : (lane == 1 ? ba : (lane == 2 ? ca : (!ca && da))))) {
+                const int dm = lane == 0 ? -EW_PER_MB
+                                         : EW_PER_MB * (lane == 1 ? -fd.mb_w : (lane == 2 ? 1 - fd.mb_w : -1 - fd.mb_w));
+                nv = wait_mv_word(ew + dm + (lane == 0 ? 0 : (lane == 3 ? 2 : 1)), epoch, status, spin_limit);
             }
             __syncwarp();
-            const bool aa = mbx > 0, ba = mby > 0, ca = mby > 0 && mbx < fd.mb_w - 1, da = mbx > 0 && mby > 0;
-            const int2 a = aa ? pick_mv_at(fd.picks, m - 1, 3, 0) : make_int2(0, 0);
-            const int2 bb = ba ? pick_mv_at(fd.picks, m - fd.mb_w, 0, 3) : make_int2(0, 0);
-            int2 c = ca ? pick_mv_at(fd.picks, m - fd.mb_w + 1, 0, 3) : make_int2(0, 0);
-            bool cav = ca;
-            if (!ca) {
-                cav = da;
-                c = da ? pick_mv_at(fd.picks, m - fd.mb_w - 1, 3, 3) : make_int2(0, 0);
-            }
-            const int2 pmv = predict_mv_ref0(aa, a, ba, bb, cav, c);
+            const int2 a = make_int2(__shfl_sync(0xffffffffu, nv.x, 0), __shfl_sync(0xffffffffu, nv.y, 0));
+            const int2 bb = make_int2(__shfl_sync(0xffffffffu, nv.x, 1), __shfl_sync(0xffffffffu, nv.y, 1));
+            const int2 c = make_int2(__shfl_sync(0xffffffffu, nv.x, ca ? 2 : 3), __shfl_sync(0xffffffffu, nv.y, ca ? 2 : 3));
+            const int2 pmv = predict_mv_ref0(aa, a, ba, bb, ca || da, c);
             if (lane == 0) {
                 mb.pmvx = pmv.x;
                 mb.pmvy = pmv.y;
@@ -1540,7 +1589,8 @@ __device__ __forceinline__ void me_frames_body_wide(const WideTable& tab, long l
         __syncwarp();
         preds[0] = mb.pmvx;
         preds[1] = mb.pmvy;
-        // the 16x16 search by all warps together (eight candidates per pass)
+        // the 16x16 search by all warps together (2 * ME_WIDE_WARPS candidates
+        // per pass)
         int rx16, ry16, ev16;
         long long c16;
         {
@@ -1548,7 +1598,7 @@ __device__ __forceinline__ void me_frames_body_wide(const WideTable& tab, long l
             group_geom_init(qg, scratch[w], pc, lx, ly, 0, win, src4);
             if (win_ok) wait_window(bar, parity, status, 3, spin_limit);
             if (win_ok) parity ^= 1u;
-            motion_search_group<BAL, LEARN, 2 * ME_WARPS, 2 * ME_WARPS, true>(
+            motion_search_group<BAL, LEARN, 2 * ME_WIDE_WARPS, 2 * ME_WIDE_WARPS, ME_WIDE_WARPS>(
                 qg, prm, scratch[w], preds, 1, fd.lambda_me, rx16, ry16, c16, ev16, LEARN, prop, fd.prop_t, &fell,
                 &coop_dist[0][0]);
         }
@@ -1562,18 +1612,22 @@ __device__ __forceinline__ void me_frames_body_wide(const WideTable& tab, long l
         // searches' seeds need no barrier
         const bool gated = fd.split_gate >= 0 && c16 > fd.split_gate;
         if (gated) {
+            // partition w / ME_PART_TEAM by its team of warps
+            const int part = w / ME_PART_TEAM;
             preds[2] = rx16;
             preds[3] = ry16;
             GroupGeom qg;
-            group_geom_init(qg, scratch[w], pc, lx, ly, 2, win, nullptr, w);
+            group_geom_init(qg, scratch[w], pc, lx, ly, 2, win, nullptr, part);
             int rx, ry, ev;
             long long rc;
-            motion_search_group<BAL, false, 4, 4>(qg, prm, scratch[w], preds, 2, fd.lambda_me, rx, ry, rc, ev);
-            if (lane == 0) {
-                mb.px[w] = rx;
-                mb.py[w] = ry;
-                mb.pc[w] = rc;
-                mb.pev[w] = ev << 3;
+            motion_search_group<BAL, false, 4 * ME_PART_TEAM, 4 * ME_PART_TEAM, ME_PART_TEAM>(
+                qg, prm, scratch[w], preds, 2, fd.lambda_me, rx, ry, rc, ev, false, make_int2(0, 0), 0, nullptr,
+                &part_dist[part][0][0]);
+            if (lane == 0 && w % ME_PART_TEAM == 0) {
+                mb.px[part] = rx;
+                mb.py[part] = ry;
+                mb.pc[part] = rc;
+                mb.pev[part] = ev << 3;
             }
         }
         __syncthreads();
@@ -1600,7 +1654,11 @@ __device__ __forceinline__ void me_frames_body_wide(const WideTable& tab, long l
                 fd.costs[2 * m] = best;
                 fd.costs[2 * m + 1] = c16;
                 if (LEARN && fd.fallback) fd.fallback[m] = fell;
-                st_release(fl + m, epoch);  // orders the pick's stores before the flag
+            }
+            // the pick to the wavefront: blocks (3,0), (0,3), (3,3)
+            if (lane < EW_PER_MB) {
+                const bool second = lane == 0 ? shape == 2 : (lane == 1 ? shape == 1 : shape != 0);
+                st_relaxed_u64(ew + lane, mv_word(epoch, second ? mv1x : mv0x, second ? mv1y : mv0y));
             }
             if (fd.coeffs != nullptr && lane < 16) {
                 const int bx = (lane & 3) * 4, by = (lane >> 2) * 4;
@@ -1717,7 +1775,7 @@ __device__ __forceinline__ void me_frames_body_wide(const WideTable& tab, long l
 }
 
 template <bool BAL, bool LEARN, bool REC>
-__global__ void __launch_bounds__(32 * ME_WARPS, ME_MIN_BLOCKS)
+__global__ void __launch_bounds__(32 * ME_WIDE_WARPS, ME_MIN_BLOCKS)
     me_frames_wide_kernel(const __grid_constant__ WideBatch batch, long long total,
                           const __grid_constant__ MeParamsDev prm, int* __restrict__ counter, int* __restrict__ flags,
                           int epoch, int* __restrict__ status, int spin_limit) {
@@ -1924,10 +1982,10 @@ static int me_wide_setup_once(int& per_sm) {
     // the residency of the largest variant bounds the grid of every one
     per_sm = 0;
     H264A_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, me_frames_wide_kernel<false, true, true>,
-                                                             32 * ME_WARPS, smem));
+                                                             32 * ME_WIDE_WARPS, smem));
     int p2 = 0;
     H264A_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&p2, me_frames_wide_kernel<false, true, false>,
-                                                             32 * ME_WARPS, smem));
+                                                             32 * ME_WIDE_WARPS, smem));
     if (p2 < per_sm) per_sm = p2;
     if (per_sm < 1) per_sm = 1;
     return H264A_OK;
@@ -1939,16 +1997,16 @@ static void launch_wide_t(const MeParamsDev& prm, unsigned blocks, cudaStream_t 
     const size_t sm = WIN_BYTES;
     const bool bal = balanced_preset(prm);
     if (learn && bal)
-        me_frames_wide_kernel<true, true, REC><<<blocks, 32 * ME_WARPS, sm, st>>>(wb, total, prm, counter, flags,
+        me_frames_wide_kernel<true, true, REC><<<blocks, 32 * ME_WIDE_WARPS, sm, st>>>(wb, total, prm, counter, flags,
                                                                                  epoch, status, SPIN_LIMIT);
     else if (learn)
-        me_frames_wide_kernel<false, true, REC><<<blocks, 32 * ME_WARPS, sm, st>>>(wb, total, prm, counter, flags,
+        me_frames_wide_kernel<false, true, REC><<<blocks, 32 * ME_WIDE_WARPS, sm, st>>>(wb, total, prm, counter, flags,
                                                                                   epoch, status, SPIN_LIMIT);
     else if (bal)
-        me_frames_wide_kernel<true, false, REC><<<blocks, 32 * ME_WARPS, sm, st>>>(wb, total, prm, counter, flags,
+        me_frames_wide_kernel<true, false, REC><<<blocks, 32 * ME_WIDE_WARPS, sm, st>>>(wb, total, prm, counter, flags,
                                                                                   epoch, status, SPIN_LIMIT);
     else
-        me_frames_wide_kernel<false, false, REC><<<blocks, 32 * ME_WARPS, sm, st>>>(wb, total, prm, counter, flags,
+        me_frames_wide_kernel<false, false, REC><<<blocks, 32 * ME_WIDE_WARPS, sm, st>>>(wb, total, prm, counter, flags,
                                                                                    epoch, status, SPIN_LIMIT);
 }
 
@@ -2096,8 +2154,15 @@ int h264a::me_frames_run(h264a_ctx* ctx, const h264a_me_frame* h_frames, int nfr
     std::vector<int> segj(nframes);
     const int nseg = make_segments(desc.data(), nframes, seg.data(), segj.data());
     if (seg[nseg] != total) return fail(H264A_E_ARG, "me_frames: internal queue layout error");
-    // the fused reconstruction's deblocking flags follow the search's
-    int rc = ensure_me_scratch(ctx, size_t(rec ? 2 * total : total));
+    // The wide kernel (launches of at most ME_WIDE_MAXF frames) publishes MV
+    // words (2 * EW_PER_MB ints per MB), then the fused reconstruction's
+    // deblocking flags; its MVs are packed as i16, so the padded pictures must
+    // be at most 8191 samples wide and high.
+    bool wide = nframes <= ME_WIDE_MAXF;
+    for (int k = 0; k < nframes; k++)
+        if (desc[k].pic.cw + 2 * desc[k].pic.pad > 8191 || desc[k].pic.ch + 2 * desc[k].pic.pad > 8191) wide = false;
+    if (rec && !wide) return fail(H264A_E_ARG, "me_frames: the fused reconstruction needs pictures of at most 8191 - 2 pad samples");
+    int rc = ensure_me_scratch(ctx, size_t(wide ? (2 * EW_PER_MB + (rec ? 1 : 0)) * total : total));
     if (rc) return rc;
     H264A_CUDA(cudaMemsetAsync(ctx->q[Q_MAIN].d_counter, 0, sizeof(int32_t), st));
     const int epoch = next_epoch(ctx, st);
@@ -2105,8 +2170,8 @@ int h264a::me_frames_run(h264a_ctx* ctx, const h264a_me_frame* h_frames, int nfr
     long long blocks = (long long)ctx->num_sms * per_sm;
     const long long need = (total + ME_WARPS - 1) / ME_WARPS;
     if (blocks > need) blocks = need;
-    if (nframes <= ME_WIDE_MAXF) {
-        // few frames: a CTA per MB, the partitions one warp each
+    if (wide) {
+        // few frames: a CTA per MB, the partitions a team of two warps each
         int wide_sm = 0;
         rc0 = me_wide_setup(wide_sm);
         if (rc0) return rc0;
@@ -2118,7 +2183,7 @@ int h264a::me_frames_run(h264a_ctx* ctx, const h264a_me_frame* h_frames, int nfr
         memcpy(wb.f, desc.data(), sizeof(FrameDesc) * nframes);
         for (int k = 0; k < nframes; k++) {
             wb.rec[k] = rdesc[k];
-            wb.rec[k].dflag_base = int(total) + desc[k].flag_base;
+            wb.rec[k].dflag_base = int(2 * EW_PER_MB * total) + desc[k].flag_base;
         }
         wb.nseg = make_segments(wb.f, wb.n, wb.seg_start, wb.seg_j);
         if (wb.seg_start[wb.nseg] != total) return fail(H264A_E_ARG, "me_frames: internal queue layout error");
