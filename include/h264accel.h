@@ -428,9 +428,11 @@ H264A_API int h264a_me_frames_learned(h264a_ctx *ctx, const h264a_me_learned_fra
  * search: the proposals of every frame come first, in one batched pass over
  * the source pairs (f, f-1) with guide MVs from the HalfRes lookahead, and
  * the search prices them on the reconstruction),
- * MC + T/Q and reconstruction of luma and chroma, and deblocking.  The frames
- * run one after another on the device (frame f may read any row of
- * rec(f-1)); each frame's MBs run as a wavefront.  Inputs: n frames of luma
+ * MC + T/Q and reconstruction of luma and chroma, and deblocking.  Each
+ * frame's MBs run as a wavefront, and consecutive frames overlap in one
+ * launch: an MB of frame f waits only for the bands (MB rows) of rec(f-1)
+ * its search reads, whose planes are built as those rows are deblocked.
+ * Inputs: n frames of luma
  * (cw x ch) and chroma (cw/2 x ch/2), contiguous, host memory.  Outputs per
  * frame (frame 0 rows zero): picks 6 i32/MB, costs 2 i64/MB, luma levels 256
  * i16/MB, chroma levels 128 i16/MB (as h264a_mc_tq_chroma_frames), the
@@ -454,8 +456,10 @@ H264A_API int h264a_pixel_path_closed(h264a_ctx *ctx, const h264a_closed_job *jo
                                       const uint16_t *h_mv_cost_tab);
 /* The same loop on device buffers, enqueued on `stream` (no allocation, no
  * host copy): the caller passes the n source frames, room for their
- * reconstruction (frame 0 is copied from the source), one picture's planes
- * as scratch (4*(cw+64)*(ch+64) bytes), the outputs (levels 16-byte aligned,
+ * reconstruction (frame 0 is copied from the source), four pictures' planes
+ * as scratch (16*(cw+64)*(ch+64) bytes: the loop overlaps consecutive frames,
+ * each building its reconstruction's planes band by band while the next
+ * frame searches the finished bands), the outputs (levels 16-byte aligned,
  * chroma 4-byte aligned), and with a net the proposals buffer (16 i32/MB per
  * frame), optional fallback flags and the guide MVs (2 i32/MB per frame, the
  * lookahead's, or NULL). */

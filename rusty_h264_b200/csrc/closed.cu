@@ -3,20 +3,17 @@
 // searches RefFrames built from its reconstructed planes
 // (crates/rusty_h264-encoder/src/lib.rs:228-262).
 //
-// Per P frame f, on one stream, two kernels of this library:
-//   planes of rec(f-1)                          h264a_hpel_build
-//   one wide motion-search launch (me_frames_wide_kernel) of src f on those
-//   planes, each MB's pick followed in the same CTA by its MC + T/Q +
-//   reconstruction of luma and chroma and its in-loop deblocking, in the
-//   search's wavefront order (the kernels h264a_mc_tq_rec_frames,
-//   h264a_mc_tq_chroma_frames and h264a_deblock_frames run as separate
-//   launches compute the same bytes)
-// With a proposal net the proposals of all frames come first, in one batched
-// h264a_mvnet_propose pass over the source pairs (f, f-1).
-// Frame f depends on all of rec(f-1) (a search may reach any row of the
-// reference), so the frames run one after another and the parallelism is the
-// MBs of one frame (the wavefront kernels).  Frame 0 reconstructs to itself
-// (the frame model codes it losslessly).
+// The loop on the device: the planes of rec(0) (h264a_hpel_build), then
+// every P frame in one launch of the pipelined kernel (closed_pipe_kernel,
+// me.cu): each MB's search (the wide kernel's), its MC + T/Q and
+// reconstruction of luma and chroma and its in-loop deblocking in the same
+// CTA, and the planes of each reconstruction built band by band as its MB
+// rows are deblocked, so that frame f's wavefront runs while frame f-1's is
+// still finishing the rows below the ones f reads.  With a proposal net the
+// proposals of all frames come first, in one batched h264a_mvnet_propose pass
+// over the source pairs (f, f-1).  One P frame alone is
+// h264a_closed_step_frame (the planes of rec(f-1) are the caller's).
+// Frame 0 reconstructs to itself (the frame model codes it losslessly).
 #include <cstring>
 #include <string>
 #include <vector>
@@ -75,33 +72,24 @@ int closed_run(h264a_ctx* ctx, const h264a_closed_dev& j, const h264a_me_params&
         const int rc = h264a_mvnet_propose(j.net, nf.data(), n - 1, st);
         if (rc) return rc;
     }
-    for (int f = 1; f < n; f++) {
-        const uint8_t* ry = j.d_rec_y + (f - 1) * fs;
-        int rc = h264a_hpel_build(ctx, ry, cw, ch, pad, 1, fs, j.d_planes, st);
-        if (rc) return rc;
-        h264a_closed_step sf;
-        sf.me.pic = h264a_picture{j.d_y + f * fs, j.d_planes, cw, ch, pad};
-        sf.me.lambda_me = j.lambda_me;
-        sf.me.split_gate = j.split_gate;
-        sf.me.d_picks = j.d_picks + 6LL * nmb * f;
-        sf.me.d_costs = j.d_costs + 2LL * nmb * f;
-        sf.d_u = j.d_u + f * cs;
-        sf.d_v = j.d_v + f * cs;
-        sf.d_ref_u = j.d_rec_u + (f - 1) * cs;
-        sf.d_ref_v = j.d_rec_v + (f - 1) * cs;
-        sf.d_rec_y = j.d_rec_y + f * fs;
-        sf.d_rec_u = j.d_rec_u + f * cs;
-        sf.d_rec_v = j.d_rec_v + f * cs;
-        sf.d_coeffs = j.d_coeffs + 256LL * nmb * f;
-        sf.d_ccoeffs = j.d_ccoeffs + 128LL * nmb * f;
-        sf.qp = j.qp;
-        sf.dz_div = j.dz_div;
-        sf.d_props = j.net ? j.d_props + 16LL * nmb * f : nullptr;
-        sf.d_fallback = j.net && j.d_fallback ? j.d_fallback + (long long)nmb * f : nullptr;
-        sf.fallback_t = j.fallback_t;
-        rc = step_run(ctx, sf, prm, st);
-        if (rc) return rc;
-    }
+    // the planes of rec(0) in the first of the four plane buffers, then every
+    // P frame in one pipelined launch
+    int rc = h264a_hpel_build(ctx, j.d_rec_y, cw, ch, pad, 1, fs, j.d_planes, st);
+    if (rc) return rc;
+    ClosedPipeIn in;
+    in.n = n; in.cw = cw; in.ch = ch; in.pad = pad;
+    in.y = j.d_y; in.u = j.d_u; in.v = j.d_v;
+    in.rec_y = j.d_rec_y; in.rec_u = j.d_rec_u; in.rec_v = j.d_rec_v;
+    in.planes = j.d_planes;
+    in.lambda_me = j.lambda_me;
+    in.split_gate = j.split_gate;
+    in.qp = j.qp; in.dz_div = j.dz_div;
+    in.picks = j.d_picks; in.costs = j.d_costs; in.coeffs = j.d_coeffs; in.ccoeffs = j.d_ccoeffs;
+    in.props = j.net ? j.d_props : nullptr;
+    in.fallback = j.net ? j.d_fallback : nullptr;
+    in.prop_t = j.fallback_t;
+    rc = closed_pipe_run(ctx, in, &prm, st);
+    if (rc) return rc;
     return H264A_OK;
 }
 
@@ -161,7 +149,7 @@ extern "C" int h264a_pixel_path_closed(h264a_ctx* ctx, const h264a_closed_job* j
     };
     const size_t o_sy = part(n * fs), o_su = part(n * cs), o_sv = part(n * cs);
     const size_t o_ry = part(n * fs), o_ru = part(n * cs), o_rv = part(n * cs);
-    const size_t o_pl = part(size_t(4) * pw * ph), o_pk = part(sizeof(int32_t) * 6 * nmb * n);
+    const size_t o_pl = part(size_t(16) * pw * ph), o_pk = part(sizeof(int32_t) * 6 * nmb * n);
     const size_t o_co = part(sizeof(int64_t) * 2 * nmb * n), o_lv = part(sizeof(int16_t) * 256 * nmb * n);
     const size_t o_cl = part(sizeof(int16_t) * 128 * nmb * n), o_tab = part(sizeof(uint16_t) * 4096);
     size_t o_pr = 0, o_fb = 0, o_half = 0, o_la = 0;

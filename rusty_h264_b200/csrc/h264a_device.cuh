@@ -30,6 +30,17 @@ __device__ __forceinline__ uint32_t ld4u(const uint8_t* p) {
     return __funnelshift_r(lo, hi, sh);
 }
 
+// ld4u through L2 (buffers written during the launch).
+__device__ __forceinline__ uint32_t ld4u_cg(const uint8_t* p) {
+    const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+    const uint32_t* w = reinterpret_cast<const uint32_t*>(a & ~uintptr_t(3));
+    const uint32_t sh = uint32_t(a & 3) * 8u;
+    const uint32_t lo = __ldcg(w);
+    if (sh == 0) return lo;
+    const uint32_t hi = __ldcg(w + 1);
+    return __funnelshift_r(lo, hi, sh);
+}
+
 // Branch-free form of ld4u for reads whose following aligned word is known to
 // lie inside the buffer (plane reads inside the padded window).
 __device__ __forceinline__ uint32_t ld4u_nb(const uint8_t* p) {
@@ -141,8 +152,16 @@ struct Planes {
     const uint8_t* base;  // F at base, H at +ps, V at +2ps, C at +3ps
     int pw, ph, pad;
     long long ps;
+    // read through L2 rather than the read-only path: the planes are written
+    // during the launch that reads them (the pipelined closed loop)
+    bool cg = false;
     __device__ __forceinline__ const uint8_t* plane(int i) const { return base + ps * i; }
 };
+
+// A word or byte of a buffer through the read-only path, or through L2 for
+// buffers written during the launch.
+__device__ __forceinline__ uint32_t ldw(const uint32_t* p, bool cg) { return cg ? __ldcg(p) : __ldg(p); }
+__device__ __forceinline__ int ldb(const uint8_t* p, bool cg) { return cg ? __ldcg(p) : __ldg(p); }
 
 // Operand table of the quarter phases (inter.rs:1086-1099, mectx.rs:143-156):
 // plane a at (+dxa,+dya), plane b at (+dxb,+dyb); planes 0=F 1=H 2=V 3=C.
@@ -210,15 +229,19 @@ __device__ __forceinline__ void pred_rows(const Planes& P, int ix, int iy, int f
         const uint32_t pb = phase_bits(fx, fy);
         const int pa = int(pb & 3), pbb = int((pb >> 2) & 3);
         const uint8_t* a = P.base + P.ps * pa + (long long)(py + int((pb >> 5) & 1)) * P.pw + px + int((pb >> 4) & 1);
+        auto rd4 = [&](const uint8_t* q) {
+            const uintptr_t ad = reinterpret_cast<uintptr_t>(q);
+            const uint32_t* w = reinterpret_cast<const uint32_t*>(ad & ~uintptr_t(3));
+            return __funnelshift_r(ldw(w, P.cg), ldw(w + 1, P.cg), uint32_t(ad & 3) * 8u);
+        };
         if (pbb == 0) {
 #pragma unroll
-            for (int r = 0; r < 4; r++) out[r] = ld4u_nb(a + (long long)r * P.pw);
+            for (int r = 0; r < 4; r++) out[r] = rd4(a + (long long)r * P.pw);
         } else {
             const uint8_t* b =
                 P.base + P.ps * pbb + (long long)(py + int((pb >> 7) & 1)) * P.pw + px + int((pb >> 6) & 1);
 #pragma unroll
-            for (int r = 0; r < 4; r++)
-                out[r] = avg_up4(ld4u_nb(a + (long long)r * P.pw), ld4u_nb(b + (long long)r * P.pw));
+            for (int r = 0; r < 4; r++) out[r] = avg_up4(rd4(a + (long long)r * P.pw), rd4(b + (long long)r * P.pw));
         }
         return;
     }
@@ -232,9 +255,9 @@ __device__ __forceinline__ void pred_rows(const Planes& P, int ix, int iy, int f
         const int yb = clampi(py + r + op.dyb, 0, P.ph - 1);
 #pragma unroll
         for (int c = 0; c < 4; c++) {
-            int v = __ldg(A + (long long)ya * P.pw + clampi(px + c + op.dxa, 0, P.pw - 1));
+            int v = ldb(A + (long long)ya * P.pw + clampi(px + c + op.dxa, 0, P.pw - 1), P.cg);
             if (op.pb >= 0) {
-                const int u = __ldg(B + (long long)yb * P.pw + clampi(px + c + op.dxb, 0, P.pw - 1));
+                const int u = ldb(B + (long long)yb * P.pw + clampi(px + c + op.dxb, 0, P.pw - 1), P.cg);
                 v = (v + u + 1) >> 1;
             }
             w |= uint32_t(v) << (8 * c);
@@ -381,10 +404,12 @@ __device__ __forceinline__ void st_release(int* p, int v) {
 }
 
 // Waits (bounded) until flag == epoch; on timeout records `code` in status.
+// Once any wait of the launch has timed out (status non-zero, checked every
+// 256 polls) the others give up too, so a failed launch ends promptly.
 static __device__ void wait_flag(const int* flag, int epoch, int* status, int code, int limit) {
     for (int it = 0;; it++) {
         if (ld_acquire(flag) == epoch) return;
-        if (it >= limit) {
+        if (it >= limit || ((it & 255) == 255 && *reinterpret_cast<volatile int*>(status) != 0)) {
             atomicCAS(status, 0, code);
             return;
         }

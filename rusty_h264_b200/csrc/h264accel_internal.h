@@ -121,6 +121,28 @@ struct MeRecIn {
     uint8_t *rec_y, *rec_u, *rec_v;
     int16_t *ccoeffs;
 };
+// The pipelined closed loop (closed_pipe_kernel in me.cu): frames 1..n-1 of
+// a clip in one launch, each searched on the planes of the deblocked
+// reconstruction of the frame before it.  planes: four picture-plane buffers
+// (4 * (cw + 2 pad) * (ch + 2 pad) bytes each), buffer 0 holding the planes of
+// rec[0] (built by the caller, as is rec[0] itself); outputs per frame as
+// h264a_closed_dev's.  props non-null: the learned 16x16 search.
+struct ClosedPipeIn {
+    int n, cw, ch, pad;
+    const uint8_t *y, *u, *v;
+    uint8_t *rec_y, *rec_u, *rec_v;
+    uint8_t *planes;
+    double lambda_me;
+    int64_t split_gate;
+    int qp, dz_div;
+    int32_t *picks;
+    int64_t *costs;
+    int16_t *coeffs, *ccoeffs;
+    const int32_t *props;
+    int32_t *fallback;
+    int32_t prop_t;
+};
+int closed_pipe_run(h264a_ctx *ctx, const ClosedPipeIn &in, const h264a_me_params *params, cudaStream_t st);
 // plain-ME of frames, with the fused T/Q when tq is given (one entry per
 // frame), the learned-proposal 16x16 search when learn is given, and the
 // fused reconstruction + deblocking when rec is given (tq required, at most

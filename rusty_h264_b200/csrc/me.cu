@@ -26,6 +26,7 @@
 #include <cudaTypedefs.h>
 
 #include "deblock_device.cuh"
+#include "hpel_device.cuh"
 #include "tq_device.cuh"
 
 namespace h264a {
@@ -41,6 +42,28 @@ constexpr int ME_WARPS = 4;
 constexpr int ME_WIDE_WARPS = 4;
 constexpr int ME_PART_TEAM = ME_WIDE_WARPS / 4;  // warps per partition search
 
+// The reference picture's readiness in the pipelined closed loop: its planes
+// are built band by band (MB rows of 16 picture rows; band b's flag == epoch
+// means bands 0..b are complete), and a search waits (bounded) for the band
+// of every row it reads.
+struct BandWait {
+    const int* flags;
+    int nbands, epoch, limit;
+    int* status;
+};
+
+// Waits until the band holding picture row `row` of the reference is built
+// (nothing when the search has no BandWait); `ready` caches the highest band
+// seen complete.
+__device__ __forceinline__ void band_wait_row(const BandWait* bw, int* ready, int row) {
+    if (bw == nullptr) return;
+    int b = row < 16 ? 0 : row >> 4;
+    if (b >= bw->nbands) b = bw->nbands - 1;
+    if (b <= *reinterpret_cast<volatile int*>(ready)) return;
+    wait_flag(bw->flags + b, bw->epoch, bw->status, 1, bw->limit);
+    atomicMax(ready, b);
+}
+
 // Per-warp shared state: the round's candidates and distortions, and the
 // search's cold parameters (read a few times per round, so they live here
 // rather than in registers).
@@ -55,6 +78,8 @@ struct WarpScratch {
     double lam_me;        // λ itself (the batched sub-pel arms)
     int win_ok;           // the MB's reference window is staged in shared memory
     int wx0, wy0;         // its origin in padded-plane coordinates
+    const BandWait* bw;   // the reference's band readiness, or nullptr (complete)
+    int bready;           // the highest band seen complete
 };
 
 // ---------------------------------------------------------------------------
@@ -564,7 +589,8 @@ struct GroupGeom {
 // candidates per pass.
 // pre: for mode 0, the lane's source rows already loaded (block lane & 15).
 __device__ __forceinline__ void group_geom_init(GroupGeom& q, WarpScratch& ws, const h264a_picture& pc, int mx, int my,
-                                                int mode, uint32_t win, const uint32_t* pre, int part = 0) {
+                                                int mode, uint32_t win, const uint32_t* pre, int part = 0,
+                                                const BandWait* bw = nullptr, int bready = 0) {
     const int lane = threadIdx.x & 31;
     SearchGeom& g = q.s;
     int x = mx, y = my;
@@ -599,6 +625,8 @@ __device__ __forceinline__ void group_geom_init(GroupGeom& q, WarpScratch& ws, c
         y += grp == 1 ? 8 : 0;
     }
     if (lane == 0) {
+        ws.bw = bw;
+        ws.bready = bready;
         ws.base = pc.d_planes;
         ws.pad = pc.pad;
         ws.pw = pc.cw + 2 * pc.pad;
@@ -665,8 +693,10 @@ __device__ __forceinline__ void eval_round_group(const GroupGeom& q, WarpScratch
                 if (win_covers(wx, wy)) {
                     win_rows(g.win, wx, wy, mv.x & 3, mv.y & 3, pr4[kk]);
                 } else {
+                    band_wait_row(ws.bw, &ws.bready, g.ly + g.byo + dy + 5);
                     Planes P;
                     P.base = ws.base; P.pw = ws.pw; P.ph = ws.ph; P.pad = ws.pad; P.ps = (long long)ws.pw * ws.ph;
+                    P.cg = ws.bw != nullptr;
                     pred_rows(P, g.lx + g.bxo + dx, g.ly + g.byo + dy, mv.x & 3, mv.y & 3, pr4[kk]);
                 }
             }
@@ -1452,7 +1482,7 @@ __device__ __forceinline__ int2 wait_mv_word(const unsigned long long* p, int ep
     for (int it = 0;; it++) {
         asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
         if (int(v >> 32) == epoch) break;
-        if (it >= limit) {
+        if (it >= limit || ((it & 255) == 255 && *reinterpret_cast<volatile int*>(status) != 0)) {
             atomicCAS(status, 0, 1);
             break;
         }
@@ -1462,20 +1492,27 @@ __device__ __forceinline__ int2 wait_mv_word(const unsigned long long* p, int ep
 }
 
 struct WideMb {
-    int t;                  // the CTA's ticket
     int pmvx, pmvy;         // the median predictor
+    int bready;             // the reference's highest band seen complete (pipelined loop)
     long long c16;          // 16x16 J
     int mv16x, mv16y, ev16;
     int px[4], py[4], pev[4];
     long long pc[4];
 };
 
+// One MB of the wide kernels (a CTA per MB): the search (16x16 by all warps,
+// the partitions one warp each), the pick published to the wavefront as MV
+// words, and for h264a_me_tq_frames-style launches the MB's MC + T/Q; REC:
+// its reconstruction and deblocking (RecDesc).  ew_frame: the frame's MV
+// words; dfl: its deblocking flags; bw: the reference's band readiness
+// (pipelined closed loop) or nullptr.  The caller's CTA barrier after the
+// call frees the window and the shared state for the next MB.
 template <bool BAL, bool LEARN, bool REC>
-__device__ __forceinline__ void me_frames_body_wide(const WideTable& tab, long long total, const MeParamsDev& prm,
-                                                    int* __restrict__ counter, int* __restrict__ flags, int epoch,
-                                                    int* __restrict__ status, int spin_limit) {
+__device__ __forceinline__ void wide_mb(const FrameDesc& fd, const RecDesc& rd, int mbx, int mby,
+                                        const MeParamsDev& prm, unsigned long long* __restrict__ ew_frame,
+                                        int* __restrict__ dfl, const BandWait* bw, int epoch, int* __restrict__ status,
+                                        int spin_limit, uint32_t win, uint32_t bar, uint32_t& parity) {
     __shared__ WarpScratch scratch[ME_WIDE_WARPS];
-    __shared__ __align__(8) unsigned long long win_bar;
     __shared__ WideMb mb;
     __shared__ int coop_dist[2][32];     // the team-wide 16x16 search's distortions
     __shared__ int part_dist[4][2][32];  // each partition team's
@@ -1485,9 +1522,284 @@ __device__ __forceinline__ void me_frames_body_wide(const WideTable& tab, long l
     __shared__ __align__(16) uint8_t rec_ct[2][REC ? CR * CT : 4];
     __shared__ int rec_nz[16];
     __shared__ int rec_bs[32];
-    extern __shared__ __align__(128) uint8_t me_win[];
     const int w = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
+    const int m = mby * fd.mb_w + mbx;
+    unsigned long long* const ew = ew_frame + EW_PER_MB * m;
+    const int lx = mbx * 16, ly = mby * 16;
+    const h264a_picture& pc = fd.pic;
+    const int pw = pc.cw + 2 * pc.pad, ph = pc.ch + 2 * pc.pad;
+    const bool win_ok = ((reinterpret_cast<uintptr_t>(pc.d_planes) | uintptr_t(pw)) & 15) == 0 && pw >= WIN_W &&
+                        ph >= WIN_H;
+    int preds[4] = {0, 0, 0, 0};
+    int fell = 0;
+    // every warp's source rows of its lane's 4x4 block in the 16x16 search
+    // (block lane & 15) and, for the learned search, its proposal (lane
+    // gl holds proposal gl - 1), loaded before the neighbour wait
+    uint32_t src4[4];
+#pragma unroll
+    for (int r = 0; r < 4; r++)
+        src4[r] = ld4u(pc.d_src + (long long)(ly + ((lane >> 2) & 3) * 4 + r) * pc.cw + lx + (lane & 3) * 4);
+    int2 prop = make_int2(0, 0);
+    if (LEARN && lane >= 1 && lane <= N_PROP) {
+        const int32_t* pp = fd.props + 16LL * m + 2 * (lane - 1);
+        prop = make_int2(__ldg(pp), __ldg(pp + 1));
+    }
+    if (w == 0) {
+        // the neighbours' published MVs: lane 0 the left MB's (3,0), lane
+        // 1 the top MB's (0,3), lane 2 the top-right MB's (0,3), lane 3
+        // the top-left MB's (3,3) when there is no top-right
+        const bool aa = mbx > 0, ba = mby > 0, ca = mby > 0 && mbx < fd.mb_w - 1, da = mbx > 0 && mby > 0;
+        int2 nv = make_int2(0, 0);
+        if (lane < 4 && (lane == 0 ? aa : (lane == 1 ? ba : (lane == 2 ? ca : (!ca && da))))) {
+            const int dm = lane == 0 ? -EW_PER_MB
+                                     : EW_PER_MB * (lane == 1 ? -fd.mb_w : (lane == 2 ? 1 - fd.mb_w : -1 - fd.mb_w));
+            nv = wait_mv_word(ew + dm + (lane == 0 ? 0 : (lane == 3 ? 2 : 1)), epoch, status, spin_limit);
+        }
+        __syncwarp();
+        const int2 a = make_int2(__shfl_sync(0xffffffffu, nv.x, 0), __shfl_sync(0xffffffffu, nv.y, 0));
+        const int2 bb = make_int2(__shfl_sync(0xffffffffu, nv.x, 1), __shfl_sync(0xffffffffu, nv.y, 1));
+        const int2 c = make_int2(__shfl_sync(0xffffffffu, nv.x, ca ? 2 : 3), __shfl_sync(0xffffffffu, nv.y, ca ? 2 : 3));
+        const int2 pmv = predict_mv_ref0(aa, a, ba, bb, ca || da, c);
+        if (lane == 0) {
+            mb.pmvx = pmv.x;
+            mb.pmvy = pmv.y;
+            mb.bready = -1;
+            scratch[0].win_ok = win_ok;
+        }
+        if (win_ok) {
+            const int wx0 = min(max((lx + pc.pad + (pmv.x >> 2) - WIN_R) & ~15, 0), pw - WIN_W);
+            const int wy0 = min(max(ly + pc.pad + (pmv.y >> 2) - WIN_R, 0), ph - WIN_H);
+            if (lane == 0) {
+                scratch[0].wx0 = wx0;
+                scratch[0].wy0 = wy0;
+                // the window's reference rows are built (pipelined loop), and
+                // the generic-proxy writes of them are visible to the copy
+                band_wait_row(bw, &mb.bready, wy0 - pc.pad + WIN_H - 1);
+                if (bw != nullptr) asm volatile("fence.proxy.async.global;" ::: "memory");
+                // every warp's reads of the previous MB's window are
+                // complete (the CTA barrier at the end of the last MB)
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                if (fd.tmap_ok) {
+                    mbar_expect_tx(bar, uint32_t(WIN_BYTES));
+                    tma_load_3d(win, &fd.tmap, wx0, wy0, 0, bar);
+                } else {
+                    mbar_expect_tx(bar, uint32_t(4 * WIN_H * WIN_W));
+                }
+            }
+            __syncwarp();
+            if (!fd.tmap_ok) {
+                const long long ps = (long long)pw * ph;
+                for (int i = lane; i < 4 * WIN_H; i += 32) {
+                    const int pl = i / WIN_H, r = i - pl * WIN_H;
+                    bulk_g2s(win + uint32_t(pl * WIN_PLANE + r * WIN_STRIDE),
+                             pc.d_planes + ps * pl + (long long)(wy0 + r) * pw + wx0, WIN_W, bar);
+                }
+            }
+        }
+    }
+    __syncthreads();  // the predictor and the window's origin are in shared memory
+    if (lane == 0 && w > 0) {
+        scratch[w].win_ok = scratch[0].win_ok;
+        scratch[w].wx0 = scratch[0].wx0;
+        scratch[w].wy0 = scratch[0].wy0;
+    }
+    __syncwarp();
+    preds[0] = mb.pmvx;
+    preds[1] = mb.pmvy;
+    // the 16x16 search by all warps together (2 * ME_WIDE_WARPS candidates
+    // per pass)
+    int rx16, ry16, ev16;
+    long long c16;
+    {
+        GroupGeom qg;
+        group_geom_init(qg, scratch[w], pc, lx, ly, 0, win, src4, 0, bw, mb.bready);
+        if (win_ok) wait_window(bar, parity, status, 3, spin_limit);
+        if (win_ok) parity ^= 1u;
+        motion_search_group<BAL, LEARN, 2 * ME_WIDE_WARPS, 2 * ME_WIDE_WARPS, ME_WIDE_WARPS>(
+            qg, prm, scratch[w], preds, 1, fd.lambda_me, rx16, ry16, c16, ev16, LEARN, prop, fd.prop_t, &fell,
+            &coop_dist[0][0]);
+    }
+    if (w == 0 && lane == 0) {
+        mb.c16 = c16;
+        mb.mv16x = rx16;
+        mb.mv16y = ry16;
+        mb.ev16 = ev16 << 4;
+    }
+    // every warp holds the same 16x16 result: the gate and the partition
+    // searches' seeds need no barrier
+    const bool gated = fd.split_gate >= 0 && c16 > fd.split_gate;
+    if (gated) {
+        // partition w / ME_PART_TEAM by its team of warps
+        const int part = w / ME_PART_TEAM;
+        preds[2] = rx16;
+        preds[3] = ry16;
+        GroupGeom qg;
+        group_geom_init(qg, scratch[w], pc, lx, ly, 2, win, nullptr, part, bw, mb.bready);
+        int rx, ry, ev;
+        long long rc;
+        motion_search_group<BAL, false, 4 * ME_PART_TEAM, 4 * ME_PART_TEAM, ME_PART_TEAM>(
+            qg, prm, scratch[w], preds, 2, fd.lambda_me, rx, ry, rc, ev, false, make_int2(0, 0), 0, nullptr,
+            &part_dist[part][0][0]);
+        if (lane == 0 && w % ME_PART_TEAM == 0) {
+            mb.px[part] = rx;
+            mb.py[part] = ry;
+            mb.pc[part] = rc;
+            mb.pev[part] = ev << 3;
+        }
+    }
+    __syncthreads();
+    // the shape decision (mb16.rs:8869-8913), taken by every warp from
+    // the shared results
+    int evals = ev16 << 4, shape = 0;
+    int mv0x = rx16, mv0y = ry16, mv1x = rx16, mv1y = ry16;
+    long long best = c16;
+    if (gated) {
+        evals += mb.pev[0] + mb.pev[1] + mb.pev[2] + mb.pev[3];
+        if (mb.pc[0] + mb.pc[1] < best) {  // 16x8 top + bottom
+            best = mb.pc[0] + mb.pc[1]; shape = 1;
+            mv0x = mb.px[0]; mv0y = mb.py[0]; mv1x = mb.px[1]; mv1y = mb.py[1];
+        }
+        if (mb.pc[2] + mb.pc[3] < best) {  // 8x16 left + right
+            best = mb.pc[2] + mb.pc[3]; shape = 2;
+            mv0x = mb.px[2]; mv0y = mb.py[2]; mv1x = mb.px[3]; mv1y = mb.py[3];
+        }
+    }
+    if (w == 0) {
+        if (lane == 0) {
+            int32_t* p = fd.picks + 6 * m;
+            p[0] = shape; p[1] = mv0x; p[2] = mv0y; p[3] = mv1x; p[4] = mv1y; p[5] = evals;
+            fd.costs[2 * m] = best;
+            fd.costs[2 * m + 1] = c16;
+            if (LEARN && fd.fallback) fd.fallback[m] = fell;
+        }
+        // the pick to the wavefront: blocks (3,0), (0,3), (3,3)
+        if (lane < EW_PER_MB) {
+            const bool second = lane == 0 ? shape == 2 : (lane == 1 ? shape == 1 : shape != 0);
+            st_relaxed_u64(ew + lane, mv_word(epoch, second ? mv1x : mv0x, second ? mv1y : mv0y));
+        }
+        if (fd.coeffs != nullptr && lane < 16) {
+            const int bx = (lane & 3) * 4, by = (lane >> 2) * 4;
+            const int part = shape == 1 ? (by >= 8) : (shape == 2 ? (bx >= 8) : 0);
+            const int mvx = part ? mv1x : mv0x, mvy = part ? mv1y : mv0y;
+            const int x = lx + bx, y = ly + by;
+            uint32_t sr[4], pr[4];
+#pragma unroll
+            for (int r = 0; r < 4; r++) sr[r] = ld4u(pc.d_src + (long long)(y + r) * pc.cw + x);
+            const int wx = x + pc.pad - scratch[0].wx0 + (mvx >> 2), wy = y + pc.pad - scratch[0].wy0 + (mvy >> 2);
+            if (win_ok && win_covers(wx, wy)) {
+                win_rows(win, wx, wy, mvx & 3, mvy & 3, pr);
+            } else {
+                band_wait_row(bw, &scratch[0].bready, y + (mvy >> 2) + 5);
+                Planes P;
+                P.base = pc.d_planes; P.pw = pw; P.ph = ph; P.pad = pc.pad; P.ps = (long long)pw * ph;
+                P.cg = bw != nullptr;
+                pred_rows(P, x + (mvx >> 2), y + (mvy >> 2), mvx & 3, mvy & 3, pr);
+            }
+            const int qi = (by >= 8 ? 2 : 0) + (bx >= 8 ? 1 : 0), kk = ((by & 4) ? 2 : 0) + ((bx & 4) ? 1 : 0);
+            int16_t* co = fd.coeffs + (long long)m * 256 + qi * 64 + kk * 16;
+            if (REC) {
+                // mb16.rs:3575-3605: the luma reconstruction into the tile
+                int lv[16];
+                tq4x4_store(sr, pr, fd.qff, fd.qmf, co, lv);
+                int any = 0;
+#pragma unroll
+                for (int i = 0; i < 16; i++) any |= lv[i];
+                rec_nz[lane] = any != 0;
+                uint32_t r4[4];
+                rec4x4(lv, pr, rd.qp, r4);
+#pragma unroll
+                for (int r = 0; r < 4; r++)
+                    *reinterpret_cast<uint32_t*>(rec_lt + (4 + by + r) * LT + 4 + bx) = r4[r];
+            } else {
+                tq4x4_store(sr, pr, fd.qff, fd.qmf, co);
+            }
+        }
+        __syncwarp();
+        if (fd.row_count != nullptr && lane == 0 && atom_add_acq_rel(fd.row_count + mby, 1) == fd.mb_w - 1)
+            st_release_sys(fd.row_done + mby, fd.row_token);
+    }
+    if (REC) {
+        const int cx0 = mbx * 8, cy0 = mby * 8;
+        if (w == 1) {
+            // chroma: lanes 0..7 are (plane, block k); lanes 8..31 shadow
+            // them so that the quads' shuffles run over the full warp
+            const int c = (lane >> 2) & 1, kb = lane & 3;
+            const int bx = (kb & 1) * 4, by = (kb >> 1) * 4;
+            const int part = shape == 1 ? (by >= 4) : (shape == 2 ? (bx >= 4) : 0);
+            const int mvx = part ? mv1x : mv0x, mvy = part ? mv1y : mv0y;
+            // the previous reconstruction's chroma rows it reads are final
+            // (pipelined loop: band b complete means MB rows 0..b+1 deblocked)
+            band_wait_row(bw, &scratch[1].bready, 2 * min(cy0 + by + 4 + (mvy >> 3), pc.ch / 2 - 1) + 1);
+            uint32_t r4[4];
+            chroma_tq_rec(rd.src_c[c], rd.ref_c[c], pc.cw / 2, pc.ch / 2, cx0 + bx, cy0 + by, mvx, mvy, kb, rd.qpc,
+                          rd.cff, rd.cmf, lane < 8 ? rd.ccoeffs + (long long)m * 128 + c * 64 + kb * 16 : nullptr,
+                          r4, bw != nullptr);
+            if (lane < 8) {
+#pragma unroll
+                for (int r = 0; r < 4; r++)
+                    *reinterpret_cast<uint32_t*>(&rec_ct[c][(2 + by + r) * CT + 4 + bx]) = r4[r];
+            }
+        }
+        const bool left = mbx > 0, top = mby > 0;
+        const DbStrips strips(lane, rd.rec_y, pc.cw, lx, ly, rd.rec_c, cx0, cy0, rec_lt, rec_ct[0], rec_ct[1], left,
+                              top, true);
+        int nmx = 0, nmy = 0;
+        bool nnz = false;
+        if (w == 2) {
+            // the left and top-right neighbours' deblocking (so the top
+            // neighbour's too), then the strips their edges reach and the
+            // neighbours' blocks on this MB's edges
+            if (lane == 0 && left) wait_flag(dfl + m - 1, epoch, status, 1, spin_limit);
+            if (lane == 1 && top)
+                wait_flag(dfl + m - fd.mb_w + (mbx < fd.mb_w - 1 ? 1 : 0), epoch, status, 1, spin_limit);
+            __syncwarp();
+            strips.load();
+            if (lane < 4 && left) block_state_at(fd.picks, fd.coeffs, m - 1, 3, lane, nmx, nmy, nnz);
+            if (lane >= 16 && lane < 20 && top)
+                block_state_at(fd.picks, fd.coeffs, m - fd.mb_w, lane - 16, 3, nmx, nmy, nnz);
+        }
+        __syncthreads();  // the MB's tiles and coefficient flags are complete
+        if (w == 2) {
+            // bS: lanes 0..15 the vertical edges (edge e, block row sg),
+            // lanes 16..31 the horizontal ones (edge e, block column sg)
+            const int hor = lane >> 4, e = (lane >> 2) & 3, sg = lane & 3;
+            const int qbx = hor ? sg : e, qby = hor ? e : sg;
+            auto own = [&](int bx4, int by4, int& mx, int& my) {
+                const int part = shape == 1 ? (by4 >= 2) : (shape == 2 ? (bx4 >= 2) : 0);
+                mx = part ? mv1x : mv0x;
+                my = part ? mv1y : mv0y;
+            };
+            int bs = 0;
+            if (e > 0 || (hor ? top : left)) {
+                int pmx = nmx, pmy = nmy, qmx, qmy;
+                bool pnz = nnz;
+                if (e > 0) {
+                    const int pbx = hor ? sg : e - 1, pby = hor ? e - 1 : sg;
+                    own(pbx, pby, pmx, pmy);
+                    pnz = rec_nz[pby * 4 + pbx] != 0;
+                }
+                own(qbx, qby, qmx, qmy);
+                bs = bs_of(pnz, rec_nz[qby * 4 + qbx] != 0, pmx, pmy, qmx, qmy);
+            }
+            rec_bs[lane] = bs;
+            __syncwarp();
+            deblock_mb_tiles(lane, rec_lt, rec_ct[0], rec_ct[1], rec_bs, left, top, true, rd.th);
+            db_store_mb(lane, rec_lt, rec_ct[0], rec_ct[1], rd.rec_y, pc.cw, lx, ly, rd.rec_c, cx0, cy0, true);
+            strips.store();
+            __syncwarp();  // every lane's stores ordered before lane 0's release
+            if (lane == 0) st_release(dfl + m, epoch);
+        }
+    }
+}
+
+template <bool BAL, bool LEARN, bool REC>
+__device__ __forceinline__ void me_frames_body_wide(const WideTable& tab, long long total, const MeParamsDev& prm,
+                                                    int* __restrict__ counter, int* __restrict__ flags, int epoch,
+                                                    int* __restrict__ status, int spin_limit) {
+    __shared__ __align__(8) unsigned long long win_bar;
+    __shared__ int ticket;
+    extern __shared__ __align__(128) uint8_t me_win[];
     const uint32_t win = uint32_t(__cvta_generic_to_shared(me_win));
     const uint32_t bar = uint32_t(__cvta_generic_to_shared(&win_bar));
     if (threadIdx.x == 0) {
@@ -1497,9 +1809,9 @@ __device__ __forceinline__ void me_frames_body_wide(const WideTable& tab, long l
     __syncthreads();
     uint32_t parity = 0;
     for (;;) {
-        if (threadIdx.x == 0) mb.t = atomicAdd(counter, 1);
+        if (threadIdx.x == 0) ticket = atomicAdd(counter, 1);
         __syncthreads();
-        const int t = mb.t;
+        const int t = ticket;
         if (t >= total) return;
         int s = 0;
         while (s + 1 < tab.nseg() && tab.seg(s + 1) <= t) s++;
@@ -1511,265 +1823,10 @@ __device__ __forceinline__ void me_frames_body_wide(const WideTable& tab, long l
         const int k = nxt + int(u / (j + 1));
         int mbx, mby;
         wave_mb(fd.mb_w, fd.mb_h, k, mbx, mby);
-        const int m = mby * fd.mb_w + mbx;
-        unsigned long long* const ew = reinterpret_cast<unsigned long long*>(flags) + EW_PER_MB * (fd.flag_base + m);
-        const int lx = mbx * 16, ly = mby * 16;
-        const h264a_picture& pc = fd.pic;
-        const int pw = pc.cw + 2 * pc.pad, ph = pc.ch + 2 * pc.pad;
-        const bool win_ok = ((reinterpret_cast<uintptr_t>(pc.d_planes) | uintptr_t(pw)) & 15) == 0 && pw >= WIN_W &&
-                            ph >= WIN_H;
-        int preds[4] = {0, 0, 0, 0};
-        int fell = 0;
-        // every warp's source rows of its lane's 4x4 block in the 16x16 search
-        // (block lane & 15) and, for the learned search, its proposal (lane
-        // gl holds proposal gl - 1), loaded before the neighbour wait
-        uint32_t src4[4];
-#pragma unroll
-        for (int r = 0; r < 4; r++)
-            src4[r] = ld4u(pc.d_src + (long long)(ly + ((lane >> 2) & 3) * 4 + r) * pc.cw + lx + (lane & 3) * 4);
-        int2 prop = make_int2(0, 0);
-        if (LEARN && lane >= 1 && lane <= N_PROP) {
-            const int32_t* pp = fd.props + 16LL * m + 2 * (lane - 1);
-            prop = make_int2(__ldg(pp), __ldg(pp + 1));
-        }
-        if (w == 0) {
-            // the neighbours' published MVs: lane 0 the left MB's (3,0), lane
-            // 1 the top MB's (0,3), lane 2 the top-right MB's (0,3), lane 3
-            // the top-left MB's (3,3) when there is no top-right
-            const bool aa = mbx > 0, ba = mby > 0, ca = mby > 0 && mbx < fd.mb_w - 1, da = mbx > 0 && mby > 0;
-            int2 nv = make_int2(0, 0);
-            if (lane < 4 && (lane == 0 ? aa : (lane == 1 ? ba : (lane == 2 ? ca : (!ca && da))))) {
-                const int dm = lane == 0 ? -EW_PER_MB
-                                         : EW_PER_MB * (lane == 1 ? -fd.mb_w : (lane == 2 ? 1 - fd.mb_w : -1 - fd.mb_w));
-                nv = wait_mv_word(ew + dm + (lane == 0 ? 0 : (lane == 3 ? 2 : 1)), epoch, status, spin_limit);
-            }
-            __syncwarp();
-            const int2 a = make_int2(__shfl_sync(0xffffffffu, nv.x, 0), __shfl_sync(0xffffffffu, nv.y, 0));
-            const int2 bb = make_int2(__shfl_sync(0xffffffffu, nv.x, 1), __shfl_sync(0xffffffffu, nv.y, 1));
-            const int2 c = make_int2(__shfl_sync(0xffffffffu, nv.x, ca ? 2 : 3), __shfl_sync(0xffffffffu, nv.y, ca ? 2 : 3));
-            const int2 pmv = predict_mv_ref0(aa, a, ba, bb, ca || da, c);
-            if (lane == 0) {
-                mb.pmvx = pmv.x;
-                mb.pmvy = pmv.y;
-                scratch[0].win_ok = win_ok;
-            }
-            if (win_ok) {
-                const int wx0 = min(max((lx + pc.pad + (pmv.x >> 2) - WIN_R) & ~15, 0), pw - WIN_W);
-                const int wy0 = min(max(ly + pc.pad + (pmv.y >> 2) - WIN_R, 0), ph - WIN_H);
-                if (lane == 0) {
-                    scratch[0].wx0 = wx0;
-                    scratch[0].wy0 = wy0;
-                    // every warp's reads of the previous MB's window are
-                    // complete (the CTA barrier at the end of the last MB)
-                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                    if (fd.tmap_ok) {
-                        mbar_expect_tx(bar, uint32_t(WIN_BYTES));
-                        tma_load_3d(win, &fd.tmap, wx0, wy0, 0, bar);
-                    } else {
-                        mbar_expect_tx(bar, uint32_t(4 * WIN_H * WIN_W));
-                    }
-                }
-                __syncwarp();
-                if (!fd.tmap_ok) {
-                    const long long ps = (long long)pw * ph;
-                    for (int i = lane; i < 4 * WIN_H; i += 32) {
-                        const int pl = i / WIN_H, r = i - pl * WIN_H;
-                        bulk_g2s(win + uint32_t(pl * WIN_PLANE + r * WIN_STRIDE),
-                                 pc.d_planes + ps * pl + (long long)(wy0 + r) * pw + wx0, WIN_W, bar);
-                    }
-                }
-            }
-        }
-        __syncthreads();  // the predictor and the window's origin are in shared memory
-        if (lane == 0 && w > 0) {
-            scratch[w].win_ok = scratch[0].win_ok;
-            scratch[w].wx0 = scratch[0].wx0;
-            scratch[w].wy0 = scratch[0].wy0;
-        }
-        __syncwarp();
-        preds[0] = mb.pmvx;
-        preds[1] = mb.pmvy;
-        // the 16x16 search by all warps together (2 * ME_WIDE_WARPS candidates
-        // per pass)
-        int rx16, ry16, ev16;
-        long long c16;
-        {
-            GroupGeom qg;
-            group_geom_init(qg, scratch[w], pc, lx, ly, 0, win, src4);
-            if (win_ok) wait_window(bar, parity, status, 3, spin_limit);
-            if (win_ok) parity ^= 1u;
-            motion_search_group<BAL, LEARN, 2 * ME_WIDE_WARPS, 2 * ME_WIDE_WARPS, ME_WIDE_WARPS>(
-                qg, prm, scratch[w], preds, 1, fd.lambda_me, rx16, ry16, c16, ev16, LEARN, prop, fd.prop_t, &fell,
-                &coop_dist[0][0]);
-        }
-        if (w == 0 && lane == 0) {
-            mb.c16 = c16;
-            mb.mv16x = rx16;
-            mb.mv16y = ry16;
-            mb.ev16 = ev16 << 4;
-        }
-        // every warp holds the same 16x16 result: the gate and the partition
-        // searches' seeds need no barrier
-        const bool gated = fd.split_gate >= 0 && c16 > fd.split_gate;
-        if (gated) {
-            // partition w / ME_PART_TEAM by its team of warps
-            const int part = w / ME_PART_TEAM;
-            preds[2] = rx16;
-            preds[3] = ry16;
-            GroupGeom qg;
-            group_geom_init(qg, scratch[w], pc, lx, ly, 2, win, nullptr, part);
-            int rx, ry, ev;
-            long long rc;
-            motion_search_group<BAL, false, 4 * ME_PART_TEAM, 4 * ME_PART_TEAM, ME_PART_TEAM>(
-                qg, prm, scratch[w], preds, 2, fd.lambda_me, rx, ry, rc, ev, false, make_int2(0, 0), 0, nullptr,
-                &part_dist[part][0][0]);
-            if (lane == 0 && w % ME_PART_TEAM == 0) {
-                mb.px[part] = rx;
-                mb.py[part] = ry;
-                mb.pc[part] = rc;
-                mb.pev[part] = ev << 3;
-            }
-        }
-        __syncthreads();
-        // the shape decision (mb16.rs:8869-8913), taken by every warp from
-        // the shared results
-        int evals = ev16 << 4, shape = 0;
-        int mv0x = rx16, mv0y = ry16, mv1x = rx16, mv1y = ry16;
-        long long best = c16;
-        if (gated) {
-            evals += mb.pev[0] + mb.pev[1] + mb.pev[2] + mb.pev[3];
-            if (mb.pc[0] + mb.pc[1] < best) {  // 16x8 top + bottom
-                best = mb.pc[0] + mb.pc[1]; shape = 1;
-                mv0x = mb.px[0]; mv0y = mb.py[0]; mv1x = mb.px[1]; mv1y = mb.py[1];
-            }
-            if (mb.pc[2] + mb.pc[3] < best) {  // 8x16 left + right
-                best = mb.pc[2] + mb.pc[3]; shape = 2;
-                mv0x = mb.px[2]; mv0y = mb.py[2]; mv1x = mb.px[3]; mv1y = mb.py[3];
-            }
-        }
-        if (w == 0) {
-            if (lane == 0) {
-                int32_t* p = fd.picks + 6 * m;
-                p[0] = shape; p[1] = mv0x; p[2] = mv0y; p[3] = mv1x; p[4] = mv1y; p[5] = evals;
-                fd.costs[2 * m] = best;
-                fd.costs[2 * m + 1] = c16;
-                if (LEARN && fd.fallback) fd.fallback[m] = fell;
-            }
-            // the pick to the wavefront: blocks (3,0), (0,3), (3,3)
-            if (lane < EW_PER_MB) {
-                const bool second = lane == 0 ? shape == 2 : (lane == 1 ? shape == 1 : shape != 0);
-                st_relaxed_u64(ew + lane, mv_word(epoch, second ? mv1x : mv0x, second ? mv1y : mv0y));
-            }
-            if (fd.coeffs != nullptr && lane < 16) {
-                const int bx = (lane & 3) * 4, by = (lane >> 2) * 4;
-                const int part = shape == 1 ? (by >= 8) : (shape == 2 ? (bx >= 8) : 0);
-                const int mvx = part ? mv1x : mv0x, mvy = part ? mv1y : mv0y;
-                const int x = lx + bx, y = ly + by;
-                uint32_t sr[4], pr[4];
-#pragma unroll
-                for (int r = 0; r < 4; r++) sr[r] = ld4u(pc.d_src + (long long)(y + r) * pc.cw + x);
-                const int wx = x + pc.pad - scratch[0].wx0 + (mvx >> 2), wy = y + pc.pad - scratch[0].wy0 + (mvy >> 2);
-                if (win_ok && win_covers(wx, wy)) {
-                    win_rows(win, wx, wy, mvx & 3, mvy & 3, pr);
-                } else {
-                    Planes P;
-                    P.base = pc.d_planes; P.pw = pw; P.ph = ph; P.pad = pc.pad; P.ps = (long long)pw * ph;
-                    pred_rows(P, x + (mvx >> 2), y + (mvy >> 2), mvx & 3, mvy & 3, pr);
-                }
-                const int qi = (by >= 8 ? 2 : 0) + (bx >= 8 ? 1 : 0), kk = ((by & 4) ? 2 : 0) + ((bx & 4) ? 1 : 0);
-                int16_t* co = fd.coeffs + (long long)m * 256 + qi * 64 + kk * 16;
-                if (REC) {
-                    // mb16.rs:3575-3605: the luma reconstruction into the tile
-                    int lv[16];
-                    tq4x4_store(sr, pr, fd.qff, fd.qmf, co, lv);
-                    int any = 0;
-#pragma unroll
-                    for (int i = 0; i < 16; i++) any |= lv[i];
-                    rec_nz[lane] = any != 0;
-                    uint32_t r4[4];
-                    rec4x4(lv, pr, tab.rd(fi).qp, r4);
-#pragma unroll
-                    for (int r = 0; r < 4; r++)
-                        *reinterpret_cast<uint32_t*>(rec_lt + (4 + by + r) * LT + 4 + bx) = r4[r];
-                } else {
-                    tq4x4_store(sr, pr, fd.qff, fd.qmf, co);
-                }
-            }
-            __syncwarp();
-            if (fd.row_count != nullptr && lane == 0 && atom_add_acq_rel(fd.row_count + mby, 1) == fd.mb_w - 1)
-                st_release_sys(fd.row_done + mby, fd.row_token);
-        }
-        if (REC) {
-            const RecDesc& rd = tab.rd(fi);
-            const int cx0 = mbx * 8, cy0 = mby * 8;
-            if (w == 1) {
-                // chroma: lanes 0..7 are (plane, block k); lanes 8..31 shadow
-                // them so that the quads' shuffles run over the full warp
-                const int c = (lane >> 2) & 1, kb = lane & 3;
-                const int bx = (kb & 1) * 4, by = (kb >> 1) * 4;
-                const int part = shape == 1 ? (by >= 4) : (shape == 2 ? (bx >= 4) : 0);
-                const int mvx = part ? mv1x : mv0x, mvy = part ? mv1y : mv0y;
-                uint32_t r4[4];
-                chroma_tq_rec(rd.src_c[c], rd.ref_c[c], pc.cw / 2, pc.ch / 2, cx0 + bx, cy0 + by, mvx, mvy, kb, rd.qpc,
-                              rd.cff, rd.cmf, lane < 8 ? rd.ccoeffs + (long long)m * 128 + c * 64 + kb * 16 : nullptr,
-                              r4);
-                if (lane < 8) {
-#pragma unroll
-                    for (int r = 0; r < 4; r++)
-                        *reinterpret_cast<uint32_t*>(&rec_ct[c][(2 + by + r) * CT + 4 + bx]) = r4[r];
-                }
-            }
-            const bool left = mbx > 0, top = mby > 0;
-            int* dfl = flags + rd.dflag_base;
-            const DbStrips strips(lane, rd.rec_y, pc.cw, lx, ly, rd.rec_c, cx0, cy0, rec_lt, rec_ct[0], rec_ct[1], left,
-                                  top, true);
-            int nmx = 0, nmy = 0;
-            bool nnz = false;
-            if (w == 2) {
-                // the left and top-right neighbours' deblocking (so the top
-                // neighbour's too), then the strips their edges reach and the
-                // neighbours' blocks on this MB's edges
-                if (lane == 0 && left) wait_flag(dfl + m - 1, epoch, status, 1, spin_limit);
-                if (lane == 1 && top)
-                    wait_flag(dfl + m - fd.mb_w + (mbx < fd.mb_w - 1 ? 1 : 0), epoch, status, 1, spin_limit);
-                __syncwarp();
-                strips.load();
-                if (lane < 4 && left) block_state_at(fd.picks, fd.coeffs, m - 1, 3, lane, nmx, nmy, nnz);
-                if (lane >= 16 && lane < 20 && top)
-                    block_state_at(fd.picks, fd.coeffs, m - fd.mb_w, lane - 16, 3, nmx, nmy, nnz);
-            }
-            __syncthreads();  // the MB's tiles and coefficient flags are complete
-            if (w == 2) {
-                // bS: lanes 0..15 the vertical edges (edge e, block row sg),
-                // lanes 16..31 the horizontal ones (edge e, block column sg)
-                const int hor = lane >> 4, e = (lane >> 2) & 3, sg = lane & 3;
-                const int qbx = hor ? sg : e, qby = hor ? e : sg;
-                auto own = [&](int bx4, int by4, int& mx, int& my) {
-                    const int part = shape == 1 ? (by4 >= 2) : (shape == 2 ? (bx4 >= 2) : 0);
-                    mx = part ? mv1x : mv0x;
-                    my = part ? mv1y : mv0y;
-                };
-                int bs = 0;
-                if (e > 0 || (hor ? top : left)) {
-                    int pmx = nmx, pmy = nmy, qmx, qmy;
-                    bool pnz = nnz;
-                    if (e > 0) {
-                        const int pbx = hor ? sg : e - 1, pby = hor ? e - 1 : sg;
-                        own(pbx, pby, pmx, pmy);
-                        pnz = rec_nz[pby * 4 + pbx] != 0;
-                    }
-                    own(qbx, qby, qmx, qmy);
-                    bs = bs_of(pnz, rec_nz[qby * 4 + qbx] != 0, pmx, pmy, qmx, qmy);
-                }
-                rec_bs[lane] = bs;
-                __syncwarp();
-                deblock_mb_tiles(lane, rec_lt, rec_ct[0], rec_ct[1], rec_bs, left, top, true, rd.th);
-                db_store_mb(lane, rec_lt, rec_ct[0], rec_ct[1], rd.rec_y, pc.cw, lx, ly, rd.rec_c, cx0, cy0, true);
-                strips.store();
-                __syncwarp();  // every lane's stores ordered before lane 0's release
-                if (lane == 0) st_release(dfl + m, epoch);
-            }
-        }
+        const RecDesc& rd = tab.rd(fi);
+        wide_mb<BAL, LEARN, REC>(fd, rd, mbx, mby, prm,
+                                 reinterpret_cast<unsigned long long*>(flags) + EW_PER_MB * fd.flag_base,
+                                 flags + rd.dflag_base, nullptr, epoch, status, spin_limit, win, bar, parity);
         __syncthreads();  // the MB's window and shared state are free for the next ticket
     }
 }
@@ -1804,6 +1861,139 @@ __global__ void __launch_bounds__(32 * ME_WARPS, ME_MIN_BLOCKS)
 
 // One warp waits on a flag that nothing sets; the bounded wait must give up
 // after `limit` polls and record status code 2.
+// ---------------------------------------------------------------------------
+// The pipelined closed loop: every P frame of a clip in one launch
+// ---------------------------------------------------------------------------
+// Frame h searches the planes of the deblocked reconstruction of frame h-1,
+// but an MB only reads the reference rows its window (and any candidate off
+// the window) reaches.  So the launch runs the frames' wavefronts overlapped:
+// each frame's tickets are its MBs in wavefront order with, after the last MB
+// of MB row b+1, a band ticket that builds the planes of the frame's
+// reconstruction for picture rows 16b .. 16b+15 (hpel_strip_rows, all four
+// warps) once that row is deblocked.  An MB of frame h waits (bounded) for
+// the bands of frame h-1 its reads need (band_wait_row); a band's flag is
+// published after the previous band's, so it stands for every band up to it.
+// The planes of four consecutive frames live in four buffers (frame h's in
+// buffer h % 4), and a band ticket of frame h first waits until frame h-3,
+// the last reader of the buffer's previous picture, has finished every MB.
+//
+// Deadlock freedom: the CTAs form two pools, the even blocks taking frames 1,
+// 3, 5, ... and the odd ones 2, 4, ..., each pool its frames in order, a CTA
+// moving to the pool's next frame only once the current frame's tickets are
+// all dealt.  A ticket waits only on earlier tickets of its own frame, on
+// frame h-1 (the other pool) and on frame h-3's completion; the oldest
+// unfinished frame therefore depends on nothing unfinished, its tickets are
+// all dealt or held by CTAs of its own pool that are not blocked by a later
+// frame, and it always progresses.  Every wait is still bounded, and after
+// the first timeout the others give up (status 1).
+struct PipeParams {
+    const FrameDesc* fds;  // per frame 0..n-1 (entry 0 unused), in device memory
+    const RecDesc* rds;
+    const int* items;      // a frame's tickets: MB index, or -(band + 1)
+    int nitems, n, mb_w, mb_h, nbands;
+    int* flags;            // per frame fstride ints: MV words, deblocking flags, band flags
+    long long fstride;
+    int ew_off, dfl_off, band_off;
+    int* ctr;              // n ticket counters and n completed-MB counters, zeroed
+    int* done;
+    const uint8_t* rec_y;  // frame h's luma reconstruction at h * fs
+    long long fs;
+    uint8_t* planes;       // four plane buffers, pbytes apart
+    long long pbytes;
+    int cw, ch, pad, word_in, word_out;
+};
+
+// Band b of frame h: the planes of its reconstruction for padded rows
+// [pad + 16b, pad + 16b + 16) (band 0 from row 0, the last band to the end),
+// once MB row b+1 (or the last) is deblocked, into buffer h % 4.
+__device__ __forceinline__ void pipe_band(const PipeParams& pp, int h, int b, int epoch, int* status, int limit) {
+    int* const ff = pp.flags + pp.fstride * h;
+    if (threadIdx.x == 0) {
+        // a row's deblocking runs left to right and waits on the row above:
+        // its last MB done means every MB of rows 0..r is
+        const int r = min(b + 1, pp.mb_h - 1);
+        wait_flag(ff + pp.dfl_off + r * pp.mb_w + pp.mb_w - 1, epoch, status, 1, limit);
+        if (h - 3 >= 1) {
+            const int nmb = pp.mb_w * pp.mb_h;
+            for (int it = 0; ld_acquire(pp.done + h - 3) < nmb; it++) {
+                if (it >= limit || ((it & 255) == 255 && *reinterpret_cast<volatile int*>(status) != 0)) {
+                    atomicCAS(status, 0, 1);
+                    break;
+                }
+                __nanosleep(200);
+            }
+        }
+    }
+    __syncthreads();
+    const int pw = pp.cw + 2 * pp.pad, ph = pp.ch + 2 * pp.pad;
+    const int y0 = b == 0 ? 0 : pp.pad + 16 * b;
+    const int y1 = b == pp.nbands - 1 ? ph : pp.pad + 16 * b + 16;
+    const int strips = (pw + HP_STRIP - 1) / HP_STRIP;
+    for (int st = int(threadIdx.x >> 5); st < strips; st += ME_WIDE_WARPS)
+        hpel_strip_rows(pp.rec_y + pp.fs * h, pp.cw, pp.ch, pp.pad, pp.planes + pp.pbytes * (h & 3), pw, ph, st, y0, y1,
+                        pp.word_in, pp.word_out);
+    // the planes' generic-proxy writes, visible to the readers' bulk copies
+    asm volatile("fence.proxy.async.global;" ::: "memory");
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (b > 0) wait_flag(ff + pp.band_off + b - 1, epoch, status, 1, limit);
+        st_release(ff + pp.band_off + b, epoch);
+    }
+}
+
+template <bool BAL, bool LEARN>
+__global__ void __launch_bounds__(32 * ME_WIDE_WARPS, ME_MIN_BLOCKS)
+    closed_pipe_kernel(const __grid_constant__ PipeParams pp, const __grid_constant__ MeParamsDev prm, int epoch,
+                       int* __restrict__ status, int spin_limit) {
+    __shared__ __align__(8) unsigned long long win_bar;
+    __shared__ int ticket;
+    __shared__ BandWait bwait;
+    extern __shared__ __align__(128) uint8_t me_win[];
+    const uint32_t win = uint32_t(__cvta_generic_to_shared(me_win));
+    const uint32_t bar = uint32_t(__cvta_generic_to_shared(&win_bar));
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    uint32_t parity = 0;
+    int h = 1 + int(blockIdx.x & 1);  // this CTA's pool: frames 1, 3, ... or 2, 4, ...
+    while (h < pp.n) {
+        if (threadIdx.x == 0) ticket = atomicAdd(pp.ctr + h, 1);
+        __syncthreads();
+        const int t = ticket;
+        if (t >= pp.nitems) {
+            h += 2;  // every ticket of frame h is dealt: the pool's next frame
+            __syncthreads();
+            continue;
+        }
+        const int item = __ldg(pp.items + t);
+        int* const ff = pp.flags + pp.fstride * h;
+        if (item >= 0) {
+            if (threadIdx.x == 0) {
+                bwait.flags = pp.flags + pp.fstride * (h - 1) + pp.band_off;
+                bwait.nbands = pp.nbands;
+                bwait.epoch = epoch;
+                bwait.limit = spin_limit;
+                bwait.status = status;
+            }
+            __syncthreads();
+            // frame 1's reference (frame 0) is built before the launch
+            wide_mb<BAL, LEARN, true>(pp.fds[h], pp.rds[h], item % pp.mb_w, item / pp.mb_w, prm,
+                                      reinterpret_cast<unsigned long long*>(ff + pp.ew_off), ff + pp.dfl_off,
+                                      h > 1 ? &bwait : nullptr, epoch, status, spin_limit, win, bar, parity);
+            __syncthreads();  // every read and write of the MB is done
+            if (threadIdx.x == 0) {
+                __threadfence();
+                atomicAdd(pp.done + h, 1);
+            }
+        } else {
+            pipe_band(pp, h, -item - 1, epoch, status, spin_limit);
+        }
+        __syncthreads();  // the window and shared state are free for the next ticket
+    }
+}
+
 __global__ void bounded_wait_selftest_kernel(const int* flag, int* status, int limit) {
     if (threadIdx.x == 0) wait_flag(flag, 1, status, 2, limit);
 }
@@ -2063,6 +2253,35 @@ extern "C" int h264a_me_search(h264a_ctx* ctx, const h264a_picture* d_pics, int 
 
 // Plain-ME of a batch of frames (h264a_me_frames); with `tq`, each frame's
 // MC + luma T/Q is fused in (h264a_me_tq_frames, h264a_pixel_path_host).
+// A frame table's pinned staging buffer (at least `bytes`), then its upload
+// into the device copy on `st`; table_done after the launch that reads it
+// records the event both wait for before they are reused.
+static int table_host(h264a_ctx* ctx, size_t bytes, char** host) {
+    if (!ctx->me_tab_ev) H264A_CUDA(cudaEventCreateWithFlags(&ctx->me_tab_ev, cudaEventDisableTiming));
+    H264A_CUDA(cudaEventSynchronize(ctx->me_tab_ev));
+    if (bytes > ctx->me_tab_cap) {
+        if (ctx->me_tab) cudaFree(ctx->me_tab);
+        if (ctx->me_tab_host) cudaFreeHost(ctx->me_tab_host);
+        ctx->me_tab = ctx->me_tab_host = nullptr;
+        ctx->me_tab_cap = 0;
+        if (cudaMalloc(&ctx->me_tab, bytes) != cudaSuccess || cudaMallocHost(&ctx->me_tab_host, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(H264A_E_NOMEM, "frame table allocation failed");
+        }
+        ctx->me_tab_cap = bytes;
+    }
+    *host = static_cast<char*>(ctx->me_tab_host);
+    return H264A_OK;
+}
+static int table_upload(h264a_ctx* ctx, size_t bytes, cudaStream_t st) {
+    H264A_CUDA(cudaMemcpyAsync(ctx->me_tab, ctx->me_tab_host, bytes, cudaMemcpyHostToDevice, st));
+    return H264A_OK;
+}
+static int table_done(h264a_ctx* ctx, cudaStream_t st) {
+    H264A_CUDA(cudaEventRecord(ctx->me_tab_ev, st));
+    return H264A_OK;
+}
+
 int h264a::me_frames_run(h264a_ctx* ctx, const h264a_me_frame* h_frames, int nframes,
                          const h264a_me_params* params, const MeTqOut* tq, void* stream, const MeLearnIn* learn,
                          const MeRecIn* rec) {
@@ -2201,35 +2420,25 @@ int h264a::me_frames_run(h264a_ctx* ctx, const h264a_me_frame* h_frames, int nfr
                          ctx->d_status, learn != nullptr);
         return check_launch("me_frames_kernel");
     }
-    // the table, its segment starts and j values in one device buffer, uploaded
-    // from a pinned staging buffer (reused once its previous upload is done)
+    // the table, its segment starts and j values in one device buffer
     const size_t b_desc = sizeof(FrameDesc) * nframes, b_seg = sizeof(long long) * (nseg + 1),
                  b_j = sizeof(int) * nseg, bytes = b_desc + b_seg + b_j;
-    if (!ctx->me_tab_ev) H264A_CUDA(cudaEventCreateWithFlags(&ctx->me_tab_ev, cudaEventDisableTiming));
-    H264A_CUDA(cudaEventSynchronize(ctx->me_tab_ev));
-    if (bytes > ctx->me_tab_cap) {
-        if (ctx->me_tab) cudaFree(ctx->me_tab);
-        if (ctx->me_tab_host) cudaFreeHost(ctx->me_tab_host);
-        ctx->me_tab = ctx->me_tab_host = nullptr;
-        ctx->me_tab_cap = 0;
-        if (cudaMalloc(&ctx->me_tab, bytes) != cudaSuccess || cudaMallocHost(&ctx->me_tab_host, bytes) != cudaSuccess) {
-            cudaGetLastError();
-            return fail(H264A_E_NOMEM, "me_frames: frame table allocation failed");
-        }
-        ctx->me_tab_cap = bytes;
-    }
-    char* hst = static_cast<char*>(ctx->me_tab_host);
+    char* hst = nullptr;
+    rc = table_host(ctx, bytes, &hst);
+    if (rc) return rc;
     memcpy(hst, desc.data(), b_desc);
     memcpy(hst + b_desc, seg.data(), b_seg);
     memcpy(hst + b_desc + b_seg, segj.data(), b_j);
-    H264A_CUDA(cudaMemcpyAsync(ctx->me_tab, hst, bytes, cudaMemcpyHostToDevice, st));
-    H264A_CUDA(cudaEventRecord(ctx->me_tab_ev, st));
+    rc = table_upload(ctx, bytes, st);
+    if (rc) return rc;
     char* dv = static_cast<char*>(ctx->me_tab);
     launch_me_frames_dtab(prm, unsigned(blocks), st, reinterpret_cast<const FrameDesc*>(dv),
                           reinterpret_cast<const long long*>(dv + b_desc), reinterpret_cast<const int*>(dv + b_desc + b_seg),
                           nframes, nseg, total, ctx->q[Q_MAIN].d_counter, ctx->q[Q_MAIN].d_flags, epoch, ctx->d_status,
                           learn != nullptr);
-    return check_launch("me_frames_dkernel");
+    rc = check_launch("me_frames_dkernel");
+    if (rc) return rc;
+    return table_done(ctx, st);
 }
 
 extern "C" int h264a_me_frames(h264a_ctx* ctx, const h264a_me_frame* h_frames, int nframes,
@@ -2389,4 +2598,179 @@ extern "C" int h264a_me_frames_noalloc(const h264a_me_frame* h_frames, int nfram
     const MeParamsDev prm = to_dev(*params);
     launch_me_frames(prm, unsigned(blocks), st, fb, total, scratch, scratch + 1, kNoallocFlag, d_status);
     return check_launch("me_frames_kernel (no-alloc)");
+}
+
+// ---------------------------------------------------------------------------
+// The pipelined closed loop's launch
+// ---------------------------------------------------------------------------
+
+static int closed_pipe_setup_once() {
+    const int smem = WIN_BYTES;
+    H264A_CUDA(cudaFuncSetAttribute(closed_pipe_kernel<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    H264A_CUDA(cudaFuncSetAttribute(closed_pipe_kernel<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    H264A_CUDA(cudaFuncSetAttribute(closed_pipe_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    H264A_CUDA(cudaFuncSetAttribute(closed_pipe_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    return H264A_OK;
+}
+
+// The per-device kernel attributes and the CTAs per SM of the pipelined loop.
+static int closed_pipe_setup(int& per_sm) {
+    constexpr int kMaxDev = 64;
+    static int cached[kMaxDev];
+    static std::mutex mu;
+    int dev = 0;
+    H264A_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(mu);
+    if (dev < 0 || dev >= kMaxDev || !cached[dev]) {
+        int rc = closed_pipe_setup_once();
+        if (rc) return rc;
+        int p = 0;
+        H264A_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&p, closed_pipe_kernel<false, true>,
+                                                                 32 * ME_WIDE_WARPS, WIN_BYTES));
+        if (p < 1) p = 1;
+        if (dev < 0 || dev >= kMaxDev) {
+            per_sm = p;
+            return H264A_OK;
+        }
+        cached[dev] = p;
+    }
+    per_sm = cached[dev];
+    return H264A_OK;
+}
+
+int h264a::closed_pipe_run(h264a_ctx* ctx, const ClosedPipeIn& in, const h264a_me_params* params, cudaStream_t st) {
+    const int n = in.n, cw = in.cw, ch = in.ch, pad = in.pad;
+    const int pw = cw + 2 * pad, ph = ch + 2 * pad;
+    if (n < 2) return H264A_OK;
+    if (pw > 8191 || ph > 8191) return fail(H264A_E_ARG, "closed loop: pictures too large for the pipelined loop");
+    const int mb_w = cw / 16, mb_h = ch / 16, nmb = mb_w * mb_h, nbands = mb_h;
+    const long long fs = (long long)cw * ch, cs = fs / 4, pbytes = 4LL * pw * ph;
+    const MeParamsDev prm = to_dev(*params);
+    int per_sm = 0;
+    int rc = closed_pipe_setup(per_sm);
+    if (rc) return rc;
+    // the frame and reconstruction descriptors (entry 0 unused)
+    std::vector<FrameDesc> fds(n);
+    std::vector<RecDesc> rds(n);
+    memset(fds.data(), 0, sizeof(FrameDesc) * n);
+    memset(rds.data(), 0, sizeof(RecDesc) * n);
+    CUtensorMap maps[4];
+    int maps_ok[4];
+    for (int k = 0; k < 4; k++) maps_ok[k] = encode_window_map(&maps[k], in.planes + pbytes * k, pw, ph);
+    for (int h = 1; h < n; h++) {
+        FrameDesc& d = fds[h];
+        const int buf = (h - 1) & 3;
+        d.tmap = maps[buf];
+        d.tmap_ok = maps_ok[buf];
+        d.pic = h264a_picture{in.y + fs * h, in.planes + pbytes * buf, cw, ch, pad};
+        d.lambda_me = in.lambda_me;
+        d.split_gate = in.split_gate;
+        d.picks = in.picks + 6LL * nmb * h;
+        d.costs = in.costs + 2LL * nmb * h;
+        d.mb_w = mb_w;
+        d.mb_h = mb_h;
+        d.coeffs = in.coeffs + 256LL * nmb * h;
+        make_quant_row4(in.qp, in.dz_div, d.qff, d.qmf);
+        if (in.props) {
+            d.props = in.props + 16LL * nmb * h;
+            d.fallback = in.fallback ? in.fallback + (long long)nmb * h : nullptr;
+            d.prop_t = in.prop_t;
+        }
+        RecDesc& r = rds[h];
+        r.src_c[0] = in.u + cs * h;
+        r.src_c[1] = in.v + cs * h;
+        r.ref_c[0] = in.rec_u + cs * (h - 1);
+        r.ref_c[1] = in.rec_v + cs * (h - 1);
+        r.rec_y = in.rec_y + fs * h;
+        r.rec_c[0] = in.rec_u + cs * h;
+        r.rec_c[1] = in.rec_v + cs * h;
+        r.ccoeffs = in.ccoeffs + 128LL * nmb * h;
+        r.qp = in.qp;
+        r.qpc = chroma_qp_of(in.qp);
+        make_quant_row4(r.qpc, 6, r.cff, r.cmf);
+        r.th = db_thresholds(in.qp, 0, 0, 0);
+    }
+    // a frame's tickets: its MBs in wavefront order (anti-diagonals t = x + 2y,
+    // then y), and band b after the last MB of MB row min(b + 1, mb_h - 1)
+    std::vector<int> items;
+    items.reserve(nmb + nbands);
+    for (int t = 0; t <= (mb_w - 1) + 2 * (mb_h - 1); t++) {
+        for (int y = 0; y < mb_h; y++) {
+            const int x = t - 2 * y;
+            if (x < 0 || x >= mb_w) continue;
+            items.push_back(y * mb_w + x);
+            if (x == mb_w - 1)
+                for (int b = 0; b < nbands; b++)
+                    if (std::min(b + 1, mb_h - 1) == y) items.push_back(-(b + 1));
+        }
+    }
+    if ((int)items.size() != nmb + nbands) return fail(H264A_E_ARG, "closed loop: internal ticket layout error");
+    const size_t b_fd = sizeof(FrameDesc) * n, b_rd = (sizeof(RecDesc) * n + 63) & ~size_t(63),
+                 b_it = sizeof(int) * items.size();
+    char* hst = nullptr;
+    rc = table_host(ctx, b_fd + b_rd + b_it, &hst);
+    if (rc) return rc;
+    memcpy(hst, fds.data(), b_fd);
+    memcpy(hst + b_fd, rds.data(), sizeof(RecDesc) * n);
+    memcpy(hst + b_fd + b_rd, items.data(), b_it);
+    rc = table_upload(ctx, b_fd + b_rd + b_it, st);
+    if (rc) return rc;
+    char* dv = static_cast<char*>(ctx->me_tab);
+    // flags: n ticket counters, n completed-MB counters, then per frame its
+    // MV words, deblocking flags and band flags (an even count per frame)
+    PipeParams pp;
+    memset(&pp, 0, sizeof pp);
+    pp.fds = reinterpret_cast<const FrameDesc*>(dv);
+    pp.rds = reinterpret_cast<const RecDesc*>(dv + b_fd);
+    pp.items = reinterpret_cast<const int*>(dv + b_fd + b_rd);
+    pp.nitems = int(items.size());
+    pp.n = n;
+    pp.mb_w = mb_w;
+    pp.mb_h = mb_h;
+    pp.nbands = nbands;
+    pp.ew_off = 0;
+    pp.dfl_off = 2 * EW_PER_MB * nmb;
+    pp.band_off = pp.dfl_off + nmb;
+    pp.fstride = (pp.band_off + nbands + 1) & ~1LL;
+    const long long head = (2LL * n + 1) & ~1LL;
+    const long long need = head + pp.fstride * n;
+    if (need >= (1LL << 31)) return fail(H264A_E_ARG, "closed loop: too many macroblocks for one launch");
+    rc = ensure_me_scratch(ctx, size_t(need));
+    if (rc) return rc;
+    int* fl = ctx->q[Q_MAIN].d_flags;
+    pp.ctr = fl;
+    pp.done = fl + n;
+    pp.flags = fl + head;
+    pp.rec_y = in.rec_y;
+    pp.fs = fs;
+    pp.planes = in.planes;
+    pp.pbytes = pbytes;
+    pp.cw = cw;
+    pp.ch = ch;
+    pp.pad = pad;
+    pp.word_in = (cw % 4 == 0) && (pad % 4 == 0) && ((reinterpret_cast<uintptr_t>(in.rec_y) & 3) == 0);
+    pp.word_out = (pw % 4 == 0) && ((reinterpret_cast<uintptr_t>(in.planes) & 3) == 0) && (pbytes % 4 == 0);
+    H264A_CUDA(cudaMemsetAsync(fl, 0, sizeof(int) * size_t(2 * n), st));
+    const int epoch = next_epoch(ctx, st);
+    if (epoch < 0) return H264A_E_CUDA;
+    long long blocks = (long long)ctx->num_sms * per_sm;
+    blocks &= ~1LL;  // the two pools, even and odd blocks
+    if (blocks < 2) blocks = 2;
+    const bool bal = balanced_preset(prm), learn = in.props != nullptr;
+    const size_t sm = WIN_BYTES;
+    if (learn && bal)
+        closed_pipe_kernel<true, true><<<unsigned(blocks), 32 * ME_WIDE_WARPS, sm, st>>>(pp, prm, epoch, ctx->d_status,
+                                                                                        SPIN_LIMIT);
+    else if (learn)
+        closed_pipe_kernel<false, true><<<unsigned(blocks), 32 * ME_WIDE_WARPS, sm, st>>>(pp, prm, epoch, ctx->d_status,
+                                                                                         SPIN_LIMIT);
+    else if (bal)
+        closed_pipe_kernel<true, false><<<unsigned(blocks), 32 * ME_WIDE_WARPS, sm, st>>>(pp, prm, epoch, ctx->d_status,
+                                                                                         SPIN_LIMIT);
+    else
+        closed_pipe_kernel<false, false><<<unsigned(blocks), 32 * ME_WIDE_WARPS, sm, st>>>(pp, prm, epoch,
+                                                                                          ctx->d_status, SPIN_LIMIT);
+    rc = check_launch("closed_pipe_kernel");
+    if (rc) return rc;
+    return table_done(ctx, st);
 }

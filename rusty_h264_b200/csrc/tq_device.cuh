@@ -148,23 +148,23 @@ static __constant__ int kQuantMfDc[6] = {13107, 11916, 10082, 9362, 8192, 7282};
 // (wa·a + wb·b + wc·c + wd·d + 32) >> 6 over rows y, y+1 of the clamped
 // reference, columns x..x+4.
 __device__ __forceinline__ uint32_t chroma_row(const uint8_t* ref, int w, int h, int x, int y, int wa, int wb, int wc,
-                                               int wd) {
+                                               int wd, bool cg = false) {
     const int ya = clampi(y, 0, h - 1), yb = clampi(y + 1, 0, h - 1);
     const uint8_t* ra = ref + (long long)ya * w;
     const uint8_t* rb = ref + (long long)yb * w;
     int a[5], b[5];
     if (x >= 0 && x + 5 <= w) {
-        const uint32_t a0 = ld4u(ra + x), b0 = ld4u(rb + x);
+        const uint32_t a0 = cg ? ld4u_cg(ra + x) : ld4u(ra + x), b0 = cg ? ld4u_cg(rb + x) : ld4u(rb + x);
 #pragma unroll
         for (int k = 0; k < 4; k++) { a[k] = byte_of(a0, k); b[k] = byte_of(b0, k); }
-        a[4] = __ldg(ra + x + 4);
-        b[4] = __ldg(rb + x + 4);
+        a[4] = ldb(ra + x + 4, cg);
+        b[4] = ldb(rb + x + 4, cg);
     } else {
 #pragma unroll
         for (int k = 0; k < 5; k++) {
             const int xx = clampi(x + k, 0, w - 1);
-            a[k] = __ldg(ra + xx);
-            b[k] = __ldg(rb + xx);
+            a[k] = ldb(ra + xx, cg);
+            b[k] = ldb(rb + xx, cg);
         }
     }
     uint32_t o = 0;
@@ -185,14 +185,14 @@ __device__ __forceinline__ uint32_t chroma_row(const uint8_t* ref, int w, int h,
 // aligned) unless it is null; the reconstructed rows to r4.
 __device__ __forceinline__ void chroma_tq_rec(const uint8_t* src, const uint8_t* ref, int ccw, int cch, int x, int y,
                                               int mvx, int mvy, int k, int q, const int16_t* ff, const int16_t* mf,
-                                              int16_t* co, uint32_t r4[4]) {
+                                              int16_t* co, uint32_t r4[4], bool ref_cg = false) {
     const int fx = mvx & 7, fy = mvy & 7;
     const int wa = (8 - fx) * (8 - fy), wb = fx * (8 - fy), wc = (8 - fx) * fy, wd = fx * fy;
     uint32_t s[4], p[4];
 #pragma unroll
     for (int r = 0; r < 4; r++) {
         s[r] = *reinterpret_cast<const uint32_t*>(src + (long long)(y + r) * ccw + x);
-        p[r] = chroma_row(ref, ccw, cch, x + (mvx >> 3), y + r + (mvy >> 3), wa, wb, wc, wd);
+        p[r] = chroma_row(ref, ccw, cch, x + (mvx >> 3), y + r + (mvy >> 3), wa, wb, wc, wd, ref_cg);
     }
     int mm[16];
 #pragma unroll
