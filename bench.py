@@ -1019,12 +1019,17 @@ def run_ours(args, ws, rank, local):
         # clip (luma + chroma) and downloads picks, costs, levels and the
         # reconstruction
         hy, hu, hv = (torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy() for a in (f, U, V))
+        pinned = lambda shp, dt: torch.zeros(shp, dtype=dt).pin_memory().numpy()
+        r_host = dict(picks=pinned((n, nmb, 6), torch.int32), costs=pinned((n, nmb, 2), torch.int64),
+                      coeffs=pinned((n, nmb, 256), torch.int16), ccoeffs=pinned((n, nmb, 128), torch.int16),
+                      rec_y=pinned(hy.shape, torch.uint8), rec_u=pinned(hu.shape, torch.uint8),
+                      rec_v=pinned(hv.shape, torch.uint8))
         for _ in range(max(1, args.warmup)):
-            r_host = acc.pixel_path_closed(hy, hu, hv, params, lam, gate, qp)
+            acc.pixel_path_closed(hy, hu, hv, params, lam, gate, qp, out=r_host)
         barrier()
         s0 = time.perf_counter()
         for _ in range(args.steps):
-            r_host = acc.pixel_path_closed(hy, hu, hv, params, lam, gate, qp)
+            acc.pixel_path_closed(hy, hu, hv, params, lam, gate, qp, out=r_host)
         ce2e_ms = (time.perf_counter() - s0) * 1e3 / args.steps
         if ws > 1:
             import torch.distributed as dist
@@ -1037,8 +1042,9 @@ def run_ours(args, ws, rank, local):
                        "d2h_bytes_per_step": int(sum(r_host[k].nbytes for k in ("picks", "costs", "coeffs", "ccoeffs",
                                                                                  "rec_y", "rec_u", "rec_v"))),
                        "ms_per_step": round(ce2e_ms, 3),
-                       "timing": "wall clock over synchronous h264a_pixel_path_closed calls (uploads, the loop, "
-                                 "downloads of picks, costs, levels and reconstruction)"}
+                       "timing": "wall clock over synchronous h264a_pixel_path_closed calls from pinned host "
+                                 "buffers (uploads, the loop, downloads of picks, costs, levels and reconstruction; "
+                                 "each frame's downloads start when the kernel reports it final)"}
         # the host entry and the device-resident loop agree
         assert np.array_equal(r_host["rec_y"], cb.ry.cpu().numpy())
         assert np.array_equal(r_host["coeffs"], cb.coeffs.cpu().numpy())

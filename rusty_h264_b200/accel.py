@@ -467,19 +467,27 @@ class Accel:
     # ---- the closed reconstruction loop -------------------------------------------
     def pixel_path_closed(self, y: np.ndarray, u: np.ndarray, v: np.ndarray, params: MeParams, lambda_me: float,
                           split_gate: int, qp: int, dz_div: int = 6, net=None, fallback_t: int = 0,
-                          tab: Optional[np.ndarray] = None):
+                          tab: Optional[np.ndarray] = None, out: Optional[dict] = None):
         """Luma y (n, ch, cw) and chroma u, v (n, ch/2, cw/2) u8 through the
         closed loop; returns picks, costs, coeffs, ccoeffs, rec_y/u/v (and
-        props, fallback with a net)."""
+        props, fallback with a net).  `out`: preallocated C-contiguous output
+        arrays of those names, shapes and dtypes (pinned ones make the
+        per-frame downloads asynchronous)."""
         n, ch, cw = y.shape
         nmb = (cw // 16) * (ch // 16)
         ins = [np.ascontiguousarray(a, np.uint8) for a in (y, u, v)]
-        out = dict(picks=np.zeros((n, nmb, 6), np.int32), costs=np.zeros((n, nmb, 2), np.int64),
-                   coeffs=np.zeros((n, nmb, 256), np.int16), ccoeffs=np.zeros((n, nmb, 128), np.int16),
-                   rec_y=np.zeros_like(ins[0]), rec_u=np.zeros_like(ins[1]), rec_v=np.zeros_like(ins[2]))
+        want = dict(picks=((n, nmb, 6), np.int32), costs=((n, nmb, 2), np.int64),
+                    coeffs=((n, nmb, 256), np.int16), ccoeffs=((n, nmb, 128), np.int16),
+                    rec_y=(ins[0].shape, np.uint8), rec_u=(ins[1].shape, np.uint8), rec_v=(ins[2].shape, np.uint8))
         if net is not None:
-            out["props"] = np.zeros((n, nmb, 16), np.int32)
-            out["fallback"] = np.zeros((n, nmb), np.int32)
+            want["props"] = ((n, nmb, 16), np.int32)
+            want["fallback"] = ((n, nmb), np.int32)
+        if out is None:
+            out = {k: np.zeros(shp, dt) for k, (shp, dt) in want.items()}
+        for k, (shp, dt) in want.items():
+            a = out.get(k)
+            if a is None or a.shape != tuple(shp) or a.dtype != dt or not a.flags.c_contiguous:
+                raise ValueError(f"pixel_path_closed: out[{k!r}] must be a C-contiguous {dt.__name__} array {shp}")
         p = lambda k: out[k].ctypes.data if k in out else None
         job = ClosedJob(ins[0].ctypes.data, ins[1].ctypes.data, ins[2].ctypes.data, n, cw, ch, float(lambda_me),
                         int(split_gate), qp, dz_div, None if net is None else net.h.value, int(fallback_t),

@@ -250,7 +250,7 @@ extern "C" void h264a_build_mv_cost_table(uint16_t* h_out) {
 static size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
 
 // Grows the row-completion buffers of h264a_pixel_path_host to `rows` rows.
-static int ensure_pp_rows(h264a_ctx* ctx, size_t rows) {
+int h264a::ensure_pp_rows(h264a_ctx* ctx, size_t rows) {
     if (rows <= ctx->pp_rows_cap) return H264A_OK;
     if (ctx->pp_row_count) cudaFree(ctx->pp_row_count);
     if (ctx->pp_rows_host) cudaFreeHost(ctx->pp_rows_host);
@@ -267,6 +267,14 @@ static int ensure_pp_rows(h264a_ctx* ctx, size_t rows) {
     ctx->pp_token = 0;
     ctx->pp_rows_cap = rows;
     return H264A_OK;
+}
+
+int32_t h264a::next_pp_token(h264a_ctx* ctx) {
+    if (ctx->pp_token >= 0x7ffffff0) {  // stale words must never equal a new token
+        memset(ctx->pp_rows_host, 0, ctx->pp_rows_cap * sizeof(int32_t));
+        ctx->pp_token = 0;
+    }
+    return ++ctx->pp_token;
 }
 
 // Grows input slot `s` to `bytes`.  Only called for a slot that holds no
@@ -405,11 +413,7 @@ extern "C" int h264a_pixel_path_host(h264a_ctx* ctx, const uint8_t* h_frames, in
     }
     int rc = ensure_pp_rows(ctx, size_t(n > 1 ? n - 1 : 1) * mb_h);
     if (rc) return rc;
-    if (ctx->pp_token >= 0x7ffffff0) {  // stale words must never equal a new token
-        memset(ctx->pp_rows_host, 0, ctx->pp_rows_cap * sizeof(int32_t));
-        ctx->pp_token = 0;
-    }
-    const int32_t token = ++ctx->pp_token;
+    const int32_t token = next_pp_token(ctx);
     H264A_CUDA(cudaMemsetAsync(ctx->pp_row_count, 0, ctx->pp_rows_cap * sizeof(int32_t), st));
     for (int k = 0; k < nk; k++) {
         const int a = int((long long)k * n / nk), b = int((long long)(k + 1) * n / nk);

@@ -14,8 +14,10 @@
 // over the source pairs (f, f-1).  One P frame alone is
 // h264a_closed_step_frame (the planes of rec(f-1) are the caller's).
 // Frame 0 reconstructs to itself (the frame model codes it losslessly).
+#include <chrono>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "h264accel_internal.h"
@@ -44,7 +46,8 @@ int step_run(h264a_ctx* ctx, const h264a_closed_step& s, const h264a_me_params& 
 }
 
 // The per-frame launches of the loop on device buffers (checked by the caller).
-int closed_run(h264a_ctx* ctx, const h264a_closed_dev& j, const h264a_me_params& prm, cudaStream_t st) {
+int closed_run(h264a_ctx* ctx, const h264a_closed_dev& j, const h264a_me_params& prm, cudaStream_t st,
+               int32_t* frame_words = nullptr, int32_t token = 0) {
     const int n = j.n, cw = j.cw, ch = j.ch, pad = 32;
     const int nmb = (cw / 16) * (ch / 16);
     const size_t fs = size_t(cw) * ch, cs = fs / 4;
@@ -88,7 +91,7 @@ int closed_run(h264a_ctx* ctx, const h264a_closed_dev& j, const h264a_me_params&
     in.props = j.net ? j.d_props : nullptr;
     in.fallback = j.net ? j.d_fallback : nullptr;
     in.prop_t = j.fallback_t;
-    rc = closed_pipe_run(ctx, in, &prm, st);
+    rc = closed_pipe_run(ctx, in, &prm, st, frame_words, token);
     if (rc) return rc;
     return H264A_OK;
 }
@@ -137,7 +140,7 @@ extern "C" int h264a_pixel_path_closed(h264a_ctx* ctx, const h264a_closed_job* j
     H264A_CUDA(cudaSetDevice(ctx->device));
     cudaStream_t st = ctx->stream;
     const int pw = cw + 64, ph = ch + 64, nmb = (cw / 16) * (ch / 16);
-    const size_t fs = size_t(cw) * ch, cs = fs / 4;
+    const size_t fs = size_t(cw) * ch, cs = fs / 4, cs_bytes = cs;
     // one cached device buffer, 256-byte aligned parts: src Y|U|V, rec Y|U|V,
     // planes, picks, costs, luma and chroma levels, mv-cost table, and with a
     // net the proposals, fallback flags, half-res frames and lookahead outputs
@@ -206,25 +209,77 @@ extern "C" int h264a_pixel_path_closed(h264a_ctx* ctx, const h264a_closed_job* j
         if (!rc) rc = h264a_lookahead_costs(ctx, j.d_y, half, cw, ch, n, 2, la, la + nmb * n, la + 2 * nmb * n, st);
         if (rc) return rc;
     }
-    rc = closed_run(ctx, j, prm, st);
+    // Each frame's outputs go down on the copy stream as soon as the pipelined
+    // kernel reports the frame final (a mapped word per frame), while later
+    // frames still run; the kernel's completion event covers the rest.
+    rc = ensure_pp_rows(ctx, size_t(n));
     if (rc) {
         cudaStreamSynchronize(st);
         return rc;
     }
-    H264A_CUDA(cudaMemcpyAsync(job->h_picks, j.d_picks, sizeof(int32_t) * 6 * nmb * n, cudaMemcpyDeviceToHost, st));
-    H264A_CUDA(cudaMemcpyAsync(job->h_costs, j.d_costs, sizeof(int64_t) * 2 * nmb * n, cudaMemcpyDeviceToHost, st));
-    if (job->h_coeffs)
-        H264A_CUDA(cudaMemcpyAsync(job->h_coeffs, j.d_coeffs, sizeof(int16_t) * 256 * nmb * n, cudaMemcpyDeviceToHost, st));
-    if (job->h_ccoeffs)
-        H264A_CUDA(cudaMemcpyAsync(job->h_ccoeffs, j.d_ccoeffs, sizeof(int16_t) * 128 * nmb * n, cudaMemcpyDeviceToHost,
-                                   st));
-    if (job->h_rec_y) H264A_CUDA(cudaMemcpyAsync(job->h_rec_y, j.d_rec_y, n * fs, cudaMemcpyDeviceToHost, st));
-    if (job->h_rec_u) H264A_CUDA(cudaMemcpyAsync(job->h_rec_u, j.d_rec_u, n * cs, cudaMemcpyDeviceToHost, st));
-    if (job->h_rec_v) H264A_CUDA(cudaMemcpyAsync(job->h_rec_v, j.d_rec_v, n * cs, cudaMemcpyDeviceToHost, st));
+    const int32_t token = next_pp_token(ctx);
+    rc = closed_run(ctx, j, prm, st, ctx->pp_rows_dev, token);
+    if (rc) {
+        cudaStreamSynchronize(st);
+        return rc;
+    }
+    cudaStream_t copy = ctx->copy_stream;
+    cudaEvent_t done_ev = ctx->pp_ev[PP_EV_TQ];
+    H264A_CUDA(cudaEventRecord(done_ev, st));
+    auto down = [&](int f0, int f1) -> int {  // frames [f0, f1)
+        const size_t k = size_t(f1 - f0), m0 = size_t(f0) * nmb;
+        auto cp = [&](void* h, const void* d, size_t unit) {
+            return cudaMemcpyAsync(static_cast<char*>(h) + unit * m0, static_cast<const char*>(d) + unit * m0,
+                                   unit * k * nmb, cudaMemcpyDeviceToHost, copy);
+        };
+        auto cpf = [&](void* h, const void* d, size_t bytes) {  // per-frame planes
+            return cudaMemcpyAsync(static_cast<char*>(h) + bytes * f0, static_cast<const char*>(d) + bytes * f0,
+                                   bytes * k, cudaMemcpyDeviceToHost, copy);
+        };
+        cudaError_t e = cp(job->h_picks, j.d_picks, sizeof(int32_t) * 6);
+        if (e == cudaSuccess) e = cp(job->h_costs, j.d_costs, sizeof(int64_t) * 2);
+        if (e == cudaSuccess && job->h_coeffs) e = cp(job->h_coeffs, j.d_coeffs, sizeof(int16_t) * 256);
+        if (e == cudaSuccess && job->h_ccoeffs) e = cp(job->h_ccoeffs, j.d_ccoeffs, sizeof(int16_t) * 128);
+        if (e == cudaSuccess && job->h_rec_y) e = cpf(job->h_rec_y, j.d_rec_y, fs);
+        if (e == cudaSuccess && job->h_rec_u) e = cpf(job->h_rec_u, j.d_rec_u, cs_bytes);
+        if (e == cudaSuccess && job->h_rec_v) e = cpf(job->h_rec_v, j.d_rec_v, cs_bytes);
+        return e == cudaSuccess ? H264A_OK : cuda_fail(e, "pixel_path_closed: result downloads");
+    };
+    auto drain = [&](int code) {
+        cudaStreamSynchronize(copy);
+        cudaStreamSynchronize(st);
+        return code;
+    };
+    // frame 0 (final before the kernel starts) goes with frame 1
+    const volatile int32_t* words = ctx->pp_rows_host;
+    int sent = 0;
+    while (sent < n) {
+        const cudaError_t q = cudaEventQuery(done_ev);  // before the words: done means every frame is final
+        if (q != cudaSuccess && q != cudaErrorNotReady) {
+            cudaGetLastError();
+            return drain(cuda_fail(q, "pixel_path_closed: the loop"));
+        }
+        int ready = sent;
+        if (q == cudaSuccess) {
+            ready = n;
+        } else {
+            while (ready < n && (ready == 0 || words[ready] == token)) ready++;
+            if (ready == 1 && n > 1) ready = 0;  // frame 0 waits for frame 1
+        }
+        if (ready > sent) {
+            rc = down(sent, ready);
+            if (rc) return drain(rc);
+            sent = ready;
+        } else {
+            std::this_thread::sleep_for(std::chrono::microseconds(50));
+        }
+    }
     if (job->net && job->h_props)
-        H264A_CUDA(cudaMemcpyAsync(job->h_props, j.d_props, sizeof(int32_t) * 16 * nmb * n, cudaMemcpyDeviceToHost, st));
+        H264A_CUDA(cudaMemcpyAsync(job->h_props, j.d_props, sizeof(int32_t) * 16 * nmb * n, cudaMemcpyDeviceToHost, copy));
     if (job->net && job->h_fallback)
         H264A_CUDA(cudaMemcpyAsync(job->h_fallback, j.d_fallback, sizeof(int32_t) * nmb * n, cudaMemcpyDeviceToHost,
-                                   st));
+                                   copy));
+    const cudaError_t e_cs = cudaStreamSynchronize(copy);
+    if (e_cs != cudaSuccess) return drain(cuda_fail(e_cs, "pixel_path_closed: result downloads"));
     return h264a_sync(ctx, st);
 }

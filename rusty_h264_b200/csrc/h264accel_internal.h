@@ -142,7 +142,16 @@ struct ClosedPipeIn {
     int32_t *fallback;
     int32_t prop_t;
 };
-int closed_pipe_run(h264a_ctx *ctx, const ClosedPipeIn &in, const h264a_me_params *params, cudaStream_t st);
+// frame_words (device view of mapped host words, or null): word h is set to
+// `token` once every MB of frame h is final, for the host to start its
+// downloads while later frames run.
+int closed_pipe_run(h264a_ctx *ctx, const ClosedPipeIn &in, const h264a_me_params *params, cudaStream_t st,
+                    int32_t *frame_words = nullptr, int32_t token = 0);
+// grows the mapped completion words (and their device counters) of the
+// host-buffer entry points to `rows` words
+int ensure_pp_rows(h264a_ctx *ctx, size_t rows);
+// the next token of those words (clearing them when the counter wraps)
+int32_t next_pp_token(h264a_ctx *ctx);
 // plain-ME of frames, with the fused T/Q when tq is given (one entry per
 // frame), the learned-proposal 16x16 search when learn is given, and the
 // fused reconstruction + deblocking when rec is given (tq required, at most

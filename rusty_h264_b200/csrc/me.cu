@@ -1901,6 +1901,8 @@ struct PipeParams {
     uint8_t* planes;       // four plane buffers, pbytes apart
     long long pbytes;
     int cw, ch, pad, word_in, word_out;
+    int32_t* frame_words;  // mapped host words: frame h's set to ftoken when it is final (or null)
+    int32_t ftoken;
 };
 
 // Band b of frame h: the planes of its reconstruction for padded rows
@@ -1984,8 +1986,12 @@ __global__ void __launch_bounds__(32 * ME_WIDE_WARPS, ME_MIN_BLOCKS)
                                       h > 1 ? &bwait : nullptr, epoch, status, spin_limit, win, bar, parity);
             __syncthreads();  // every read and write of the MB is done
             if (threadIdx.x == 0) {
-                __threadfence();
-                atomicAdd(pp.done + h, 1);
+                const int c = atom_add_acq_rel(pp.done + h, 1);
+                if (c == pp.mb_w * pp.mb_h - 1 && pp.frame_words != nullptr) {
+                    // the frame's last MB: its outputs are final, for the host
+                    __threadfence_system();
+                    st_release_sys(pp.frame_words + h, pp.ftoken);
+                }
             }
         } else {
             pipe_band(pp, h, -item - 1, epoch, status, spin_limit);
@@ -2638,7 +2644,8 @@ static int closed_pipe_setup(int& per_sm) {
     return H264A_OK;
 }
 
-int h264a::closed_pipe_run(h264a_ctx* ctx, const ClosedPipeIn& in, const h264a_me_params* params, cudaStream_t st) {
+int h264a::closed_pipe_run(h264a_ctx* ctx, const ClosedPipeIn& in, const h264a_me_params* params, cudaStream_t st,
+                           int32_t* frame_words, int32_t token) {
     const int n = in.n, cw = in.cw, ch = in.ch, pad = in.pad;
     const int pw = cw + 2 * pad, ph = ch + 2 * pad;
     if (n < 2) return H264A_OK;
@@ -2750,6 +2757,8 @@ int h264a::closed_pipe_run(h264a_ctx* ctx, const ClosedPipeIn& in, const h264a_m
     pp.pad = pad;
     pp.word_in = (cw % 4 == 0) && (pad % 4 == 0) && ((reinterpret_cast<uintptr_t>(in.rec_y) & 3) == 0);
     pp.word_out = (pw % 4 == 0) && ((reinterpret_cast<uintptr_t>(in.planes) & 3) == 0) && (pbytes % 4 == 0);
+    pp.frame_words = frame_words;
+    pp.ftoken = token;
     H264A_CUDA(cudaMemsetAsync(fl, 0, sizeof(int) * size_t(2 * n), st));
     const int epoch = next_epoch(ctx, st);
     if (epoch < 0) return H264A_E_CUDA;

@@ -1138,6 +1138,30 @@ def test_closed_loop_learned_matches_oracle(acc):
     net.close()
 
 
+def test_closed_loop_into_pinned_outputs_matches_oracle(acc):
+    """The host entry writing into caller-provided pinned arrays (each frame's
+    downloads queued as the kernel reports it final) gives the oracle's
+    outputs, twice in a row into the same arrays."""
+    torch = acc.torch
+    Y, U, V = _coded_yuv(*synth.cif_clip(12, 8))
+    n, ch, cw = Y.shape
+    nmb = (cw // 16) * (ch // 16)
+    qp = 25
+    lam = float(np.sqrt(A.frame_lambda(qp)) * 1.25)
+    gate = A.split_gate_for_qp(qp)
+    pinned = lambda shp, dt: torch.zeros(shp, dtype=dt).pin_memory().numpy()
+    out = dict(picks=pinned((n, nmb, 6), torch.int32), costs=pinned((n, nmb, 2), torch.int64),
+               coeffs=pinned((n, nmb, 256), torch.int16), ccoeffs=pinned((n, nmb, 128), torch.int16),
+               rec_y=pinned(Y.shape, torch.uint8), rec_u=pinned(U.shape, torch.uint8), rec_v=pinned(V.shape, torch.uint8))
+    want = O.closed_loop_clip(Y, U, V, O.balanced_params(), lam, gate, qp)
+    for _ in range(2):
+        got = acc.pixel_path_closed(Y, U, V, A.default_me_params(), lam, gate, qp, out=out)
+        assert got is out
+        _compare_closed(got, want)
+    with pytest.raises(ValueError):
+        acc.pixel_path_closed(Y, U, V, A.default_me_params(), lam, gate, qp, out=dict(out, picks=out["costs"]))
+
+
 def test_closed_frames_device_path_equals_host_path(acc):
     """h264a_closed_frames on device buffers gives what the host-buffer entry
     gives (which the tests above pin to the oracle)."""
