@@ -405,9 +405,11 @@ H264A_API int h264a_mvnet_propose(h264a_mvnet *net, const h264a_mvnet_frame *h_f
  * (motion_search from its predictors, mb16.rs:2433) and d_fallback[mb] = 1;
  * otherwise the search continues as motion_search with the cheapest of the
  * nine as its start vector (mb16.rs:2445: no full-pel phase, the sub-pel
- * refinement only) and d_fallback[mb] = 0 (d_fallback optional).  Partitions,
- * neighbours, outputs and the queue as h264a_me_frames.  No counterpart in
- * the reference. */
+ * refinement only) and d_fallback[mb] = 0 (d_fallback optional).  The
+ * 16x8/8x16 partitions of an MB that took a proposal refine from its 16x16 MV
+ * in the same way (start vector mv16, mvd centre the predictor); those of a
+ * fallen-back MB, the neighbours, outputs and the queue are as
+ * h264a_me_frames'.  No counterpart in the reference. */
 typedef struct {
     h264a_me_frame me;
     const int32_t *d_props;

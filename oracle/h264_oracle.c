@@ -1049,13 +1049,19 @@ static void mv_neighbors_block(const blk4 *g, int w4, int h4, int pbx, int pby, 
     if (!nb[2].available) nb[2] = nb_get(g, w4, h4, pbx - 1, pby - 1);
 }
 
-/* best_part, mb16.rs:4921-4960, single reference (ref_bits 0). */
-static void best_part1(const or_me_frame *fr, const or_me_params *pr, const or_mv_neighbor nb[3], int rx, int ry, int rw,
-                       int rh, const int32_t *extra, int nextra, double lme, or_me_result *res) {
+/* best_part, mb16.rs:4921-4960, single reference (ref_bits 0); start non-NULL:
+ * a refine-only search from it (the learned search's partitions). */
+static void best_part1s(const or_me_frame *fr, const or_me_params *pr, const or_mv_neighbor nb[3], int rx, int ry,
+                        int rw, int rh, const int32_t *extra, int nextra, double lme, const int32_t *start,
+                        or_me_result *res) {
     int32_t seeds[8];
     or_predict_mv(&nb[0], &nb[1], &nb[2], 0, seeds);
     for (int i = 0; i < nextra; i++) { seeds[2 + 2 * i] = extra[2 * i]; seeds[3 + 2 * i] = extra[2 * i + 1]; }
-    or_motion_search(fr, pr, rx, ry, rw, rh, seeds, 1 + nextra, lme, NULL, res);
+    or_motion_search(fr, pr, rx, ry, rw, rh, seeds, 1 + nextra, lme, start, res);
+}
+static void best_part1(const or_me_frame *fr, const or_me_params *pr, const or_mv_neighbor nb[3], int rx, int ry, int rw,
+                       int rh, const int32_t *extra, int nextra, double lme, or_me_result *res) {
+    best_part1s(fr, pr, nb, rx, ry, rw, rh, extra, nextra, lme, NULL, res);
 }
 
 /* The learned-proposal 16x16 search (no counterpart in the reference): price
@@ -1108,8 +1114,8 @@ void or_me_frame_learned(const or_me_frame *fr, const or_me_params *pr, double l
             or_mv_neighbor nb[3];
             mv_neighbors_block(g, w4, h4, mbx * 4, mby * 4, 4, nb);
             or_me_result r16;
+            int32_t f = 1;
             if (props) {
-                int32_t f = 0;
                 learned_16x16(fr, pr, nb, lx, ly, lambda_me, props + 16 * (mby * mb_w + mbx), prop_t, &r16, &f);
                 if (fell) fell[mby * mb_w + mbx] = f;
             } else {
@@ -1124,11 +1130,14 @@ void or_me_frame_learned(const or_me_frame *fr, const or_me_params *pr, double l
             pk->mv16[0] = r16.mvx; pk->mv16[1] = r16.mvy;
             if (split_gate >= 0 && r16.cost > split_gate) {
                 int32_t e[2] = {r16.mvx, r16.mvy};
+                /* the learned search, when its 16x16 search took a proposal:
+                 * the partitions refine-only from the 16x16 MV */
+                const int32_t *st = props && !f ? e : NULL;
                 or_me_result rt, rb, rl, rr;
-                best_part1(fr, pr, nb, lx, ly, 16, 8, e, 1, lambda_me, &rt);
-                best_part1(fr, pr, nb, lx, ly + 8, 16, 8, e, 1, lambda_me, &rb);
-                best_part1(fr, pr, nb, lx, ly, 8, 16, e, 1, lambda_me, &rl);
-                best_part1(fr, pr, nb, lx + 8, ly, 8, 16, e, 1, lambda_me, &rr);
+                best_part1s(fr, pr, nb, lx, ly, 16, 8, e, 1, lambda_me, st, &rt);
+                best_part1s(fr, pr, nb, lx, ly + 8, 16, 8, e, 1, lambda_me, st, &rb);
+                best_part1s(fr, pr, nb, lx, ly, 8, 16, e, 1, lambda_me, st, &rl);
+                best_part1s(fr, pr, nb, lx + 8, ly, 8, 16, e, 1, lambda_me, st, &rr);
                 int64_t best_c = r16.cost;
                 if (rt.cost + rb.cost < best_c) {
                     best_c = rt.cost + rb.cost;

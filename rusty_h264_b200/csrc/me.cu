@@ -263,7 +263,7 @@ __device__ __forceinline__ long long cand_cost64(const MeParamsDev& pr, const Wa
 }
 
 // Search phases and what an evaluation round's results are for.
-constexpr int PH_SEEDS = 0, PH_PROP = 1, PH_DIA = 2, PH_REPRICE = 3, PH_SUB = 4, PH_DONE = 5;
+constexpr int PH_SEEDS = 0, PH_PROP = 1, PH_DIA = 2, PH_REPRICE = 3, PH_SUB = 4, PH_DONE = 5, PH_START = 6;
 constexpr int EV_START = 0, EV_SEEDS = 1, EV_PROP = 2, EV_FIXED = 3, EV_RING = 4, EV_REPRICE = 5;
 // Candidates of the learned search's proposal round: the median predictor
 // and the network's 8 proposals.
@@ -777,7 +777,8 @@ __device__ __forceinline__ void motion_search_group(const GroupGeom& q, const Me
                                                     const int* preds, int npred, double lambda_me, int& out_x,
                                                     int& out_y, long long& out_c, int& evals, bool use_prop = false,
                                                     int2 prop = make_int2(0, 0), int prop_t = 0, int* fell = nullptr,
-                                                    int* cdist = nullptr) {
+                                                    int* cdist = nullptr, bool use_start = false,
+                                                    int2 start = make_int2(0, 0)) {
     const Knobs<BAL> pr{prm};
     const int gl = q.gl, gb = q.gb;
     const bool sadfp = !pr.fast() && pr.sadfp();
@@ -814,7 +815,7 @@ __device__ __forceinline__ void motion_search_group(const GroupGeom& q, const Me
     evals = 0;
     int bx = 0, by = 0, seed_x = 0, seed_y = 0;
     int best_c = 0, seed_c = 0;  // costs below 2^30 (lane_cost), compared as i32
-    int phase = (LEARN && use_prop) ? PH_PROP : PH_SEEDS;
+    int phase = (LEARN && use_prop) ? PH_PROP : (use_start ? PH_START : PH_SEEDS);
     int si = -1, sk = -1, loops = 0, iter = 0, step = 0;
     bool ring_open = false, ring_improved = false;
     int ring_i = 0, ring_n = 0;
@@ -836,6 +837,9 @@ __device__ __forceinline__ void motion_search_group(const GroupGeom& q, const Me
             } else if (LEARN && phase == PH_PROP) {
                 if (gl <= N_PROP) ws.cand[gb + gl] = gl == 0 ? make_int2(preds[0], preds[1]) : prop;
                 kind = EV_PROP; n = N_PROP + 1; metric = m_main; lam = ws.lam_r;
+            } else if (phase == PH_START) {
+                if (gl == 0) ws.cand[gb] = start;
+                kind = EV_START; n = 1; metric = m_main; lam = ws.lam_r;
             } else if (phase == PH_DIA) {
                 if (ring_open) {
                     kind = EV_RING; n = min(ring_n - ring_i, RR); metric = m_fp; lam = l_fp;
@@ -933,7 +937,7 @@ __device__ __forceinline__ void motion_search_group(const GroupGeom& q, const Me
         // the seed and reprice rounds
         const bool need_min = __any_sync(0xffffffffu, kind == EV_FIXED);
         const bool need_hit = __any_sync(0xffffffffu, kind == EV_RING);
-        const bool need_seed = __any_sync(0xffffffffu, kind == EV_SEEDS || kind == EV_REPRICE);
+        const bool need_seed = __any_sync(0xffffffffu, kind == EV_SEEDS || kind == EV_REPRICE || kind == EV_START);
         if (COOP) {
             // the warp zeroes the slots of the candidates it prices (lane gl
             // < 8: pass gl / cpw, candidate gl % cpw of the warp's share)
@@ -1000,6 +1004,15 @@ __device__ __forceinline__ void motion_search_group(const GroupGeom& q, const Me
                 evals += 1;
             }
             phase = PH_DIA;
+        } else if (kind == EV_START) {
+            // a refine-only search (mb16.rs:2580-2582): the start vector
+            // priced with `cost`, no full-pel phase, the sub-pel steps from it
+            best_c = c_seed[0];
+            bx = start.x;
+            by = start.y;
+            seed_x = bx; seed_y = by; seed_c = best_c;
+            evals += 1;
+            phase = PH_SUB;
         } else if (LEARN && kind == EV_PROP) {
             // the cheapest of the nine (first wins, the predictor first), and
             // the cheapest proposal's distortion against the predictor's
@@ -1350,8 +1363,12 @@ __device__ __forceinline__ void me_frames_body(const TAB& tab, long long total, 
             }
             int rx, ry, ev;
             long long rc;
+            // the learned search's partitions, when its 16x16 search took a
+            // proposal: refine-only from the 16x16 MV
+            const bool lstart = LEARN && mode == 1 && !fell;
             motion_search_group<BAL, LEARN>(qg, prm, scratch[w], preds, mode == 0 ? 1 : 2, fd.lambda_me, rx, ry, rc, ev,
-                                            LEARN && mode == 0, prop, fd.prop_t, &fell);
+                                            LEARN && mode == 0, prop, fd.prop_t, mode == 0 ? &fell : nullptr, nullptr,
+                                            lstart, make_int2(preds[2], preds[3]));
             if (mode == 0) {
                 evals = ev << 4;  // 4x4-block evaluations
                 c16 = rc; best = rc;
@@ -1638,9 +1655,11 @@ __device__ __forceinline__ void wide_mb(const FrameDesc& fd, const RecDesc& rd, 
         group_geom_init(qg, scratch[w], pc, lx, ly, 2, win, nullptr, part, bw, mb.bready);
         int rx, ry, ev;
         long long rc;
+        // the learned search's partitions, when its 16x16 search took a
+        // proposal: refine-only from the 16x16 MV
         motion_search_group<BAL, false, 4 * ME_PART_TEAM, 4 * ME_PART_TEAM, ME_PART_TEAM>(
             qg, prm, scratch[w], preds, 2, fd.lambda_me, rx, ry, rc, ev, false, make_int2(0, 0), 0, nullptr,
-            &part_dist[part][0][0]);
+            &part_dist[part][0][0], LEARN && !fell, make_int2(rx16, ry16));
         if (lane == 0 && w % ME_PART_TEAM == 0) {
             mb.px[part] = rx;
             mb.py[part] = ry;

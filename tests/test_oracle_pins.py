@@ -896,7 +896,8 @@ def np_me_frame(src, ref, lam, gate, props=None, prop_t=0):
     best_part 16x16 seeded [pmv], and when its J exceeds the gate the 16x8 and
     8x16 halves seeded [pmv, mv16], the shape taken on strictly lower summed J
     (mb16.rs:8869-8913).  With props (16 i32 per MB) the 16x16 search is
-    np_learned_16x16; the fallback flags are returned as a third array."""
+    np_learned_16x16, and the halves of an MB that took a proposal search
+    refine-only from mv16; the fallback flags are returned as a third array."""
     ch, cw = src.shape
     mb_w, mb_h = cw // 16, ch // 16
     picks = np.zeros((mb_w * mb_h, 6), np.int32)
@@ -920,8 +921,11 @@ def np_me_frame(src, ref, lam, gate, props=None, prop_t=0):
         shape, mv0, mv1, best = 0, mv16, mv16, c16
         if gate >= 0 and c16 > gate:
             seeds = [pmv, mv16]
-            (mt, ct), (mb_, cb) = (np_motion_search(src, ref, lx, ly + o, 16, 8, seeds, lam) for o in (0, 8))
-            (ml, cl), (mr, cr) = (np_motion_search(src, ref, lx + o, ly, 8, 16, seeds, lam) for o in (0, 8))
+            # the learned search's partitions, when its 16x16 search took a
+            # proposal: refine-only from the 16x16 MV
+            st = mv16 if props is not None and not fell[m] else None
+            (mt, ct), (mb_, cb) = (np_motion_search(src, ref, lx, ly + o, 16, 8, seeds, lam, start=st) for o in (0, 8))
+            (ml, cl), (mr, cr) = (np_motion_search(src, ref, lx + o, ly, 8, 16, seeds, lam, start=st) for o in (0, 8))
             if ct + cb < best:
                 shape, mv0, mv1, best = 1, mt, mb_, ct + cb
             if cl + cr < best:
