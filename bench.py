@@ -180,11 +180,64 @@ def mixed_batch(acc, torch, streams, params, lam: float, gate: int):
     ms = float(np.median(ts))
     px = sum((f.shape[0] - 1) * f.shape[1] * f.shape[2] for f in streams)
     mbs = sum((f.shape[0] - 1) * (f.shape[1] // 16) * (f.shape[2] // 16) for f in streams)
+    ms3 = mixed_batch_3ref(acc, torch, bufs, params, lam, gate)
     return {"streams": "4 x 352x288, 6 x 1280x720, 4 x 1920x1080, 2 x 3840x2160; 30 frames each, 1080p generator",
             "p_frames": len(frames_all), "macroblocks": int(mbs), "me_ms": round(ms, 3),
             "me_mpx_s": round(px / (ms * 1e-3) / 1e6, 1), "launches": 1,
+            "me_3ref_ms": round(ms3, 3), "me_3ref_mpx_s": round(px / (ms3 * 1e-3) / 1e6, 1),
             "batched_equals_alone": True,
-            "note": "plain-ME of all P frames, one reference; not part of value"}
+            "note": "plain-ME of all P frames (one reference, and up to three: the previous three pictures); "
+                    "not part of value"}
+
+
+def mixed_batch_3ref(acc, torch, bufs, params, lam: float, gate: int) -> float:
+    """Plain-ME of every P frame of the mixed batch over up to three
+    references (the previous three source pictures' planes, nearest first) in
+    one h264a_me_frames_multiref launch.  Every stream's picks and costs must
+    equal the same stream run on its own; returns the median CUDA-event time
+    of the batched call in ms (3 warm-up, 5 timed)."""
+    import ctypes as C
+
+    from rusty_h264_b200 import accel as A
+
+    per_stream, outs = [], []
+    for d, planes, _, _ in bufs:
+        n, ch, cw = d.shape
+        nmb = (cw // 16) * (ch // 16)
+        picks = torch.zeros((n, nmb, 8), dtype=torch.int32, device="cuda")
+        costs = torch.zeros((n, nmb, 2), dtype=torch.int64, device="cuda")
+        fr = []
+        for i in range(1, n):
+            nref = min(3, i)
+            refs = [planes[i - 1 - r].data_ptr() for r in range(nref)] + [0] * (4 - nref)
+            fr.append(A.MeMrFrame(d[i].data_ptr(), (C.c_void_p * 4)(*refs), nref, cw, ch, 32, lam, gate,
+                                  picks[i].data_ptr(), costs[i].data_ptr()))
+        per_stream.append(fr)
+        outs.append((picks, costs))
+    alone = []
+    for s, fr in enumerate(per_stream):
+        acc.me_frames_multiref(fr, params)
+        acc.sync()
+        alone.append((outs[s][0].clone(), outs[s][1].clone()))
+    for o in outs:
+        o[0].zero_()
+        o[1].zero_()
+    frames_all = [f for fr in per_stream for f in fr]
+    acc.me_frames_multiref(frames_all, params)
+    acc.sync()
+    for s, o in enumerate(outs):
+        assert torch.equal(o[0], alone[s][0]) and torch.equal(o[1], alone[s][1]), f"stream {s}: 3-ref batched != alone"
+    ts = []
+    for it in range(8):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        acc.me_frames_multiref(frames_all, params)
+        e1.record()
+        torch.cuda.synchronize()
+        if it >= 3:
+            ts.append(e0.elapsed_time(e1))
+    acc.sync()
+    return float(np.median(ts))
 
 
 # Training clips of the learned proposals: the 1080p generator with seeds the

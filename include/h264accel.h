@@ -17,10 +17,13 @@
  *  - `stream` is a cudaStream_t (NULL = the device's default stream, as in the
  *    CUDA runtime).  Calls only enqueue work; results are ready when the
  *    stream is synchronised (h264a_sync).  The persistent wavefront kernels
- *    serialise on a context's work-queue scratch: h264a_me_frames and
- *    h264a_deblock_frames share one queue, h264a_lookahead_costs has a second,
- *    so within one context the lookahead may run on another stream beside
- *    either of them; otherwise use one context per concurrent stream.
+ *    serialise on a context's work-queue scratch: h264a_me_frames (more than
+ *    two frames) and h264a_deblock_frames share one queue,
+ *    h264a_lookahead_costs has a second, and the one- and two-frame searches
+ *    and the closed loop (h264a_me_frames with at most two frames,
+ *    h264a_closed_step_frame, h264a_closed_frames, h264a_pixel_path_closed) a
+ *    third, so within one context the lookahead may run on another stream
+ *    beside any of them; otherwise use one context per concurrent stream.
  *  - Planes: a reference picture's cached planes are one buffer F|H|V|C, each
  *    pw*ph bytes with pw = cw + 2*pad, ph = ch + 2*pad, stride pw: the
  *    HpelPlanes layout of crates/rusty_h264-common/src/inter.rs:707-730.
@@ -418,6 +421,28 @@ typedef struct {
 } h264a_me_learned_frame;
 H264A_API int h264a_me_frames_learned(h264a_ctx *ctx, const h264a_me_learned_frame *h_frames, int nframes,
                                       const h264a_me_params *params, void *stream);
+
+/* ---- plain-ME over several reference pictures ----------------------------------- */
+/* h264a_me_frames with best_part's loop over references (mb16.rs:4921-4960):
+ * each search (16x16, and the 16x8/8x16 partitions when its J exceeds
+ * split_gate) runs on every reference r = 0..nref-1 (d_planes[r]: its F|H|V|C
+ * planes, reference 0 the nearest) seeded [predict_mv against r, extra], its
+ * J plus (lambda_me * ref_bits(r, nref)) truncated to i64 (mb16.rs:5967), the
+ * strictly cheapest reference kept; predictors take only neighbours of the
+ * same reference (inter.rs:36-69).  Picks: 8 i32 per MB (shape, ref0, mv0x,
+ * mv0y, ref1, mv1x, mv1y, 4x4-block evaluations); costs 2 i64 per MB (the
+ * pick's J, the 16x16's).  1 <= nref <= 4.  Queue as h264a_me_frames. */
+typedef struct {
+    const uint8_t *d_src;
+    const uint8_t *d_planes[4];
+    int32_t nref, cw, ch, pad;
+    double lambda_me;
+    int64_t split_gate;
+    int32_t *d_picks;
+    int64_t *d_costs;
+} h264a_me_mr_frame;
+H264A_API int h264a_me_frames_multiref(h264a_ctx *ctx, const h264a_me_mr_frame *h_frames, int nframes,
+                                       const h264a_me_params *params, void *stream);
 
 /* ---- the closed reconstruction loop ------------------------------------------ */
 /* The pixel path as the encoder runs it: every P frame searches, predicts

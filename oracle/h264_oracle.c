@@ -1162,6 +1162,97 @@ void or_me_frame_learned(const or_me_frame *fr, const or_me_params *pr, double l
     free(g);
 }
 
+/* ref_bits (mb16.rs:5967-5981): the bits of ref_idx r among nref references,
+ * te(v): none for one reference, one bit for two, ue(r) beyond. */
+static uint32_t ref_bits(int r, int nref) {
+    if (nref <= 1) return 0;
+    if (nref == 2) return 1;
+    uint32_t n = (uint32_t)r + 1, len = 1;
+    while (n > 1) { n >>= 1; len += 2; }
+    return len;
+}
+
+/* best_part (mb16.rs:4921-4960) over nref references: per reference r the
+ * seeds [predict_mv(a, b, c, r), extra...], motion_search on that reference,
+ * the cost plus (lme * ref_bits) truncated to i64, the lowest cost kept
+ * (strictly lower; references in order). */
+static void best_part_mr(const or_me_frame *frs, int nref, const or_me_params *pr, const or_mv_neighbor nb[3],
+                         int rx, int ry, int rw, int rh, const int32_t *extra, int nextra, double lme, int32_t *ref,
+                         or_me_result *res) {
+    int64_t bc = INT64_MAX;
+    for (int r = 0; r < nref; r++) {
+        int32_t seeds[8];
+        or_predict_mv(&nb[0], &nb[1], &nb[2], r, seeds);
+        for (int i = 0; i < nextra; i++) { seeds[2 + 2 * i] = extra[2 * i]; seeds[3 + 2 * i] = extra[2 * i + 1]; }
+        or_me_result o;
+        or_motion_search(&frs[r], pr, rx, ry, rw, rh, seeds, 1 + nextra, lme, NULL, &o);
+        const int64_t c = o.cost + (int64_t)(lme * (double)ref_bits(r, nref));
+        if (c < bc) {
+            bc = c;
+            *ref = r;
+            *res = o;
+            res->cost = c;
+        }
+    }
+}
+
+/* The plain-ME frame model over nref references (the frame's frs[0..nref),
+ * reference 0 the nearest): as or_me_frame_plain, each partition's search
+ * best_part over the references, the neighbours' reference indices feeding
+ * predict_mv (an MV predicts only from neighbours of the same reference,
+ * inter.rs:36-69).  Picks: shape, ref_idx and MV of each half, costs. */
+void or_me_frame_multiref(const or_me_frame *frs, int nref, const or_me_params *pr, double lambda_me,
+                          int64_t split_gate, or_mb_pick_mr *out) {
+    const or_me_frame *fr = &frs[0];
+    int mb_w = fr->cw / 16, mb_h = fr->ch / 16;
+    int w4 = mb_w * 4, h4 = mb_h * 4;
+    blk4 *g = (blk4 *)calloc((size_t)w4 * h4, sizeof(blk4));
+    for (int mby = 0; mby < mb_h; mby++)
+        for (int mbx = 0; mbx < mb_w; mbx++) {
+            int lx = mbx * 16, ly = mby * 16;
+            or_mv_neighbor nb[3];
+            mv_neighbors_block(g, w4, h4, mbx * 4, mby * 4, 4, nb);
+            or_me_result r16 = {0, 0, 0, 0};
+            int32_t ref16 = 0;
+            best_part_mr(frs, nref, pr, nb, lx, ly, 16, 16, NULL, 0, lambda_me, &ref16, &r16);
+            or_mb_pick_mr *pk = &out[mby * mb_w + mbx];
+            pk->shape = 0;
+            pk->ref[0] = pk->ref[1] = ref16;
+            pk->mv[0][0] = pk->mv[1][0] = r16.mvx;
+            pk->mv[0][1] = pk->mv[1][1] = r16.mvy;
+            pk->cost = pk->cost16 = r16.cost;
+            if (split_gate >= 0 && r16.cost > split_gate) {
+                int32_t e[2] = {r16.mvx, r16.mvy}, rf[4] = {0, 0, 0, 0};
+                or_me_result rp[4] = {{0, 0, 0, 0}, {0, 0, 0, 0}, {0, 0, 0, 0}, {0, 0, 0, 0}};
+                best_part_mr(frs, nref, pr, nb, lx, ly, 16, 8, e, 1, lambda_me, &rf[0], &rp[0]);
+                best_part_mr(frs, nref, pr, nb, lx, ly + 8, 16, 8, e, 1, lambda_me, &rf[1], &rp[1]);
+                best_part_mr(frs, nref, pr, nb, lx, ly, 8, 16, e, 1, lambda_me, &rf[2], &rp[2]);
+                best_part_mr(frs, nref, pr, nb, lx + 8, ly, 8, 16, e, 1, lambda_me, &rf[3], &rp[3]);
+                int64_t best_c = r16.cost;
+                for (int sh = 1; sh <= 2; sh++) {
+                    const int a = sh == 1 ? 0 : 2;
+                    if (rp[a].cost + rp[a + 1].cost < best_c) {
+                        best_c = rp[a].cost + rp[a + 1].cost;
+                        pk->shape = sh;
+                        for (int k = 0; k < 2; k++) {
+                            pk->ref[k] = rf[a + k];
+                            pk->mv[k][0] = rp[a + k].mvx;
+                            pk->mv[k][1] = rp[a + k].mvy;
+                        }
+                    }
+                }
+                pk->cost = best_c;
+            }
+            for (int dy = 0; dy < 4; dy++)
+                for (int dx = 0; dx < 4; dx++) {
+                    int part = pk->shape == 1 ? (dy >= 2) : (pk->shape == 2 ? (dx >= 2) : 0);
+                    blk4 *b = &g[(mby * 4 + dy) * w4 + mbx * 4 + dx];
+                    b->mvx = pk->mv[part][0]; b->mvy = pk->mv[part][1]; b->ref_idx = pk->ref[part]; b->coded = 1;
+                }
+        }
+    free(g);
+}
+
 /* Exhaustive full-pel SAD and SATD over ±R of MB (mbx,mby), values as the ME
  * cost functions return them (mc_sad_hp / mc_satd_hp at full-pel MVs: edge reads
  * clamp).  Grid layout: (dy+R)*(2R+1) + (dx+R). */

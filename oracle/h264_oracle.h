@@ -131,6 +131,11 @@ void or_me_frame_plain(const or_me_frame *fr, const or_me_params *pr, double lam
                        int64_t split_gate, or_mb_pick *out /* mb_w*mb_h */);
 void or_me_frame_learned(const or_me_frame *fr, const or_me_params *pr, double lambda_me, int64_t split_gate,
                          const int32_t *props, int32_t prop_t, or_mb_pick *out, int32_t *fell);
+/* the plain-ME frame model over nref references (frs[r]: the same source, the
+ * planes of reference r; reference 0 the nearest) */
+typedef struct { int32_t shape; int32_t ref[2]; int32_t mv[2][2]; int64_t cost; int64_t cost16; } or_mb_pick_mr;
+void or_me_frame_multiref(const or_me_frame *frs, int nref, const or_me_params *pr, double lambda_me,
+                          int64_t split_gate, or_mb_pick_mr *out);
 /* in-loop deblocking of a plain-ME P picture (h264_oracle_par.c) */
 void or_deblock_frame_plain(uint8_t *y, uint8_t *u, uint8_t *v, int cw, int ch, const int32_t *picks,
                             const int16_t *coeffs, int qp, int offset_a, int offset_b, int chroma_qp_offset);

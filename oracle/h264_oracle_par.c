@@ -130,6 +130,40 @@ void or_me_frame_flat(const uint8_t *src, const uint8_t *ref, const uint8_t *pla
                              NULL);
 }
 
+/* or_me_frame_multiref on flat buffers: nref reference pictures refs
+ * (cw*ch each, contiguous) and their planes (4*pw*ph each); picks 8 i32 per
+ * MB (shape, ref0, mv0x, mv0y, ref1, mv1x, mv1y, 0), costs 2 i64 per MB. */
+void or_me_frame_multiref_flat(const uint8_t *src, const uint8_t *refs, const uint8_t *planes, int nref, int cw,
+                               int ch, int pad, const or_me_params_flat *pf, const uint16_t *tab, double lambda_me,
+                               int64_t split_gate, int32_t *picks, int64_t *costs) {
+    int pw = cw + 2 * pad, ph = ch + 2 * pad;
+    size_t ps = (size_t)pw * ph;
+    or_me_frame frs[8];
+    if (nref < 1 || nref > 8) return;
+    for (int r = 0; r < nref; r++) {
+        const uint8_t *pl = planes + 4 * ps * r;
+        or_me_frame *fr = &frs[r];
+        fr->src = src; fr->ref = refs + (size_t)cw * ch * r; fr->cw = cw; fr->ch = ch;
+        fr->planes.f = pl; fr->planes.h = pl + ps; fr->planes.v = pl + 2 * ps; fr->planes.c = pl + 3 * ps;
+        fr->planes.pw = pw; fr->planes.ph = ph; fr->planes.pad = pad; fr->planes.cw = cw; fr->planes.ch = ch;
+    }
+    or_me_params p;
+    unflatten(pf, tab, &p);
+    int nmb = (cw / 16) * (ch / 16);
+    or_mb_pick_mr *pk = (or_mb_pick_mr *)malloc(sizeof(or_mb_pick_mr) * (size_t)nmb);
+    or_me_frame_multiref(frs, nref, &p, lambda_me, split_gate, pk);
+    for (int m = 0; m < nmb; m++) {
+        int32_t *o = picks + 8 * m;
+        o[0] = pk[m].shape;
+        o[1] = pk[m].ref[0]; o[2] = pk[m].mv[0][0]; o[3] = pk[m].mv[0][1];
+        o[4] = pk[m].ref[1]; o[5] = pk[m].mv[1][0]; o[6] = pk[m].mv[1][1];
+        o[7] = 0;
+        costs[2 * m] = pk[m].cost;
+        costs[2 * m + 1] = pk[m].cost16;
+    }
+    free(pk);
+}
+
 /* or_me_frame_flat with the learned 16x16 search (props: 16 i32 per MB, NULL
  * for the plain search); fell (optional): the fallback flag per MB. */
 void or_me_frame_learned_flat(const uint8_t *src, const uint8_t *ref, const uint8_t *planes4, int cw, int ch, int pad,

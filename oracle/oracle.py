@@ -82,6 +82,8 @@ def lib():
                                        C.c_double, C.c_int64, i32p, i64p]
         L.or_me_frame_learned_flat.argtypes = [u8p, u8p, u8p, C.c_int, C.c_int, C.c_int, C.POINTER(MeParamsFlat),
                                                u16p, C.c_double, C.c_int64, i32p, C.c_int32, i32p, i64p, i32p]
+        L.or_me_frame_multiref_flat.argtypes = [u8p, u8p, u8p, C.c_int, C.c_int, C.c_int, C.c_int,
+                                                C.POINTER(MeParamsFlat), u16p, C.c_double, C.c_int64, i32p, i64p]
         L.or_closed_loop_clip.argtypes = [u8p, u8p, u8p, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(MeParamsFlat),
                                           u16p, C.c_double, C.c_int64, C.c_int, C.c_int, i32p, C.c_int32, i32p, i64p,
                                           i16p, i16p, u8p, u8p, u8p, i32p]
@@ -177,6 +179,24 @@ def me_frame(src, ref, planes4, params, lambda_me, split_gate=-1, tab=None, pad=
     tab = mv_cost_table() if tab is None else tab
     lib().or_me_frame_flat(ptr(src), ptr(ref), ptr(planes4), cw, ch, pad, C.byref(params), ptr(tab, u16p),
                            float(lambda_me), int(split_gate), ptr(picks, i32p), ptr(costs, i64p))
+    return picks, costs
+
+
+def me_frame_multiref(src, refs, planes, params, lambda_me, split_gate=-1, tab=None, pad=32):
+    """The plain-ME frame model over len(refs) references (refs (nref, ch, cw)
+    u8, reference 0 the nearest; planes (nref, 4, ph, pw) their planes):
+    picks (nmb, 8) i32 (shape, ref0, mv0x, mv0y, ref1, mv1x, mv1y, 0) and
+    costs (nmb, 2) i64."""
+    ch, cw = src.shape
+    nmb = (cw // 16) * (ch // 16)
+    refs = np.ascontiguousarray(refs, np.uint8)
+    planes = np.ascontiguousarray(planes, np.uint8)
+    picks = np.zeros((nmb, 8), np.int32)
+    costs = np.zeros((nmb, 2), np.int64)
+    tab = mv_cost_table() if tab is None else tab
+    lib().or_me_frame_multiref_flat(ptr(src), ptr(refs), ptr(planes), len(refs), cw, ch, pad, C.byref(params),
+                                    ptr(tab, u16p), float(lambda_me), int(split_gate), ptr(picks, i32p),
+                                    ptr(costs, i64p))
     return picks, costs
 
 

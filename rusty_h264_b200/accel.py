@@ -128,6 +128,12 @@ class ClosedStep(C.Structure):
                 ("d_props", C.c_void_p), ("d_fallback", C.c_void_p), ("fallback_t", C.c_int32)]
 
 
+class MeMrFrame(C.Structure):
+    _fields_ = [("d_src", C.c_void_p), ("d_planes", C.c_void_p * 4), ("nref", C.c_int32), ("cw", C.c_int32),
+                ("ch", C.c_int32), ("pad", C.c_int32), ("lambda_me", C.c_double), ("split_gate", C.c_int64),
+                ("d_picks", C.c_void_p), ("d_costs", C.c_void_p)]
+
+
 # Every entry point the header declares (checked by tests/test_capi_symbols.py).
 EXPORTS = (
     "h264a_version", "h264a_last_error", "h264a_ctx_create", "h264a_ctx_destroy", "h264a_sync",
@@ -141,7 +147,7 @@ EXPORTS = (
     "h264a_mvnet_create", "h264a_mvnet_destroy", "h264a_mvnet_set_params", "h264a_mvnet_get_params",
     "h264a_mvnet_forward", "h264a_mvnet_grads", "h264a_mvnet_train_step", "h264a_mvnet_propose",
     "h264a_me_frames_learned", "h264a_pixel_path_closed", "h264a_write_stream_cavlc", "h264a_cavlc_table_code",
-    "h264a_closed_frames", "h264a_closed_step_frame",
+    "h264a_closed_frames", "h264a_closed_step_frame", "h264a_me_frames_multiref",
 )
 
 _lib = None
@@ -190,6 +196,7 @@ def load_library() -> C.CDLL:
     L.h264a_pixel_path_closed.argtypes = [vp, C.POINTER(ClosedJob), C.POINTER(MeParams), vp]
     L.h264a_closed_frames.argtypes = [vp, C.POINTER(ClosedDev), C.POINTER(MeParams), vp]
     L.h264a_closed_step_frame.argtypes = [vp, C.POINTER(ClosedStep), C.POINTER(MeParams), vp]
+    L.h264a_me_frames_multiref.argtypes = [vp, vp, C.c_int, C.POINTER(MeParams), vp]
     L.h264a_write_stream_cavlc.argtypes = [C.POINTER(StreamFrames), vp, sz, C.POINTER(sz), vp]
     L.h264a_cavlc_table_code.argtypes = [i32, i32, i32, i32, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L.h264a_mvnet_create.argtypes = [i32, C.c_uint64, C.POINTER(vp)]
@@ -377,6 +384,13 @@ class Accel:
         arr = (MeFrame * len(frames))(*frames)
         self._check(self.L.h264a_me_frames(self.ctx, C.cast(arr, C.c_void_p), len(frames), C.byref(params),
                                            self._stream()))
+
+    def me_frames_multiref(self, frames: Sequence[MeMrFrame], params: MeParams):
+        """Plain-ME of frames over up to 4 reference pictures each
+        (h264a_me_frames_multiref), enqueued on the current stream."""
+        arr = (MeMrFrame * len(frames))(*frames)
+        self._check(self.L.h264a_me_frames_multiref(self.ctx, C.cast(arr, C.c_void_p), len(frames), C.byref(params),
+                                                    self._stream()))
 
     def me_frames_learned(self, frames: Sequence[MeLearnedFrame], params: MeParams):
         """me_frames with the learned proposals in each MB's 16x16 search."""

@@ -19,10 +19,12 @@ struct WorkQueue {
     size_t flags_cap = 0;
     int32_t epoch = 0;
 };
-// Q_MAIN serves plain-ME, deblocking and the bounded-wait self-test;
-// Q_LOOKAHEAD the lookahead, which can therefore run on another stream beside
-// them.  The counters sit 128 bytes apart.
-constexpr int Q_MAIN = 0, Q_LOOKAHEAD = 1, NUM_QUEUES = 2, Q_COUNTER_STRIDE = 32;
+// Q_MAIN serves plain-ME, deblocking and the bounded-wait self-test (flags
+// that only ever hold an epoch); Q_LOOKAHEAD the lookahead, which can
+// therefore run on another stream beside them; Q_WIDE the wide and pipelined
+// closed-loop kernels, whose flag space also holds MV words and counters and
+// is cleared before each of their launches.  The counters sit 128 bytes apart.
+constexpr int Q_MAIN = 0, Q_LOOKAHEAD = 1, Q_WIDE = 2, NUM_QUEUES = 3, Q_COUNTER_STRIDE = 32;
 // h264a_pixel_path_host: PP_CHUNKS upload chunks; its events are the
 // uploads, planes and half-res frames ready, ME + T/Q done, lookahead done.
 constexpr int PP_CHUNKS = 4;

@@ -50,6 +50,10 @@ struct HpelRow {
 
 // Rows [y0, y1) of strip `strip` (plane columns strip * HP_STRIP ..) of the
 // four planes F of picture Y, one warp: see the file comment of hpel.cu.
+// CG: read the picture through L2 rather than the read-only path (a picture
+// written during the launch, whose rows below the strip's may still change:
+// the look-ahead loads past y1 must not leave stale lines in L1).
+template <bool CG = false>
 __device__ __forceinline__ void hpel_strip_rows(const uint8_t* __restrict__ Y, int cw, int ch, int pad,
                                                 uint8_t* __restrict__ F, int pw, int ph, int strip, int y0, int y1,
                                                 int word_in, int word_out) {
@@ -62,9 +66,9 @@ __device__ __forceinline__ void hpel_strip_rows(const uint8_t* __restrict__ Y, i
               c3 = clampi(sx + 3, 0, cw - 1);
     auto ldraw = [&](int yp) {
         const uint8_t* row = Y + (long long)clampi(yp - pad, 0, ch - 1) * cw;
-        return inner ? __ldg(reinterpret_cast<const uint32_t*>(row + sx))
-                     : uint32_t(__ldg(row + c0)) | uint32_t(__ldg(row + c1)) << 8 | uint32_t(__ldg(row + c2)) << 16 |
-                           uint32_t(__ldg(row + c3)) << 24;
+        return inner ? ldw(reinterpret_cast<const uint32_t*>(row + sx), CG)
+                     : uint32_t(ldb(row + c0, CG)) | uint32_t(ldb(row + c1, CG)) << 8 |
+                           uint32_t(ldb(row + c2, CG)) << 16 | uint32_t(ldb(row + c3, CG)) << 24;
     };
     auto mk = [](uint32_t raw) {
         HpelRow r;

@@ -1199,6 +1199,7 @@ struct FrameBatch {
 // The frame table as the kernel body reads it: the launch's parameters
 // (FrameBatch, up to ME_MAXF frames) or arrays in device memory (any count).
 struct ParamTable {
+    static constexpr bool kGlobal = false;  // tensor maps in the kernel's parameters
     const FrameBatch& b;
     __device__ __forceinline__ int n() const { return b.n; }
     __device__ __forceinline__ int nseg() const { return b.nseg; }
@@ -1207,6 +1208,7 @@ struct ParamTable {
     __device__ __forceinline__ const FrameDesc& fr(int i) const { return b.f[i]; }
 };
 struct DeviceTable {
+    static constexpr bool kGlobal = true;  // tensor maps in device memory
     const FrameDesc* f;
     const long long* seg_start;
     const int* seg_j;
@@ -1330,6 +1332,11 @@ __device__ __forceinline__ void me_frames_body(const TAB& tab, long long total, 
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 if (fd.tmap_ok) {  // the whole window in one tensor copy
                     mbar_expect_tx(bar, uint32_t(WIN_BYTES));
+                    // a tensor map written to device memory by the host since an
+                    // earlier launch read that address: acquire it for the copy
+                    if (TAB::kGlobal)
+                        asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&fd.tmap)
+                                     : "memory");
                     tma_load_3d(win, &fd.tmap, wx0, wy0, 0, bar);
                 } else {
                     mbar_expect_tx(bar, uint32_t(4 * WIN_H * WIN_W));
@@ -1528,7 +1535,8 @@ template <bool BAL, bool LEARN, bool REC>
 __device__ __forceinline__ void wide_mb(const FrameDesc& fd, const RecDesc& rd, int mbx, int mby,
                                         const MeParamsDev& prm, unsigned long long* __restrict__ ew_frame,
                                         int* __restrict__ dfl, const BandWait* bw, int epoch, int* __restrict__ status,
-                                        int spin_limit, uint32_t win, uint32_t bar, uint32_t& parity) {
+                                        int spin_limit, uint32_t win, uint32_t bar, uint32_t& parity,
+                                        bool tmap_global = false) {
     __shared__ WarpScratch scratch[ME_WIDE_WARPS];
     __shared__ WideMb mb;
     __shared__ int coop_dist[2][32];     // the team-wide 16x16 search's distortions
@@ -1599,6 +1607,9 @@ __device__ __forceinline__ void wide_mb(const FrameDesc& fd, const RecDesc& rd, 
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 if (fd.tmap_ok) {
                     mbar_expect_tx(bar, uint32_t(WIN_BYTES));
+                    if (tmap_global)  // a tensor map in device memory, as above (once per frame and CTA)
+                        asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&fd.tmap)
+                                     : "memory");
                     tma_load_3d(win, &fd.tmap, wx0, wy0, 0, bar);
                 } else {
                     mbar_expect_tx(bar, uint32_t(4 * WIN_H * WIN_W));
@@ -1951,8 +1962,8 @@ __device__ __forceinline__ void pipe_band(const PipeParams& pp, int h, int b, in
     const int y1 = b == pp.nbands - 1 ? ph : pp.pad + 16 * b + 16;
     const int strips = (pw + HP_STRIP - 1) / HP_STRIP;
     for (int st = int(threadIdx.x >> 5); st < strips; st += ME_WIDE_WARPS)
-        hpel_strip_rows(pp.rec_y + pp.fs * h, pp.cw, pp.ch, pp.pad, pp.planes + pp.pbytes * (h & 3), pw, ph, st, y0, y1,
-                        pp.word_in, pp.word_out);
+        hpel_strip_rows<true>(pp.rec_y + pp.fs * h, pp.cw, pp.ch, pp.pad, pp.planes + pp.pbytes * (h & 3), pw, ph, st,
+                              y0, y1, pp.word_in, pp.word_out);
     // the planes' generic-proxy writes, visible to the readers' bulk copies
     asm volatile("fence.proxy.async.global;" ::: "memory");
     __syncthreads();
@@ -1978,6 +1989,7 @@ __global__ void __launch_bounds__(32 * ME_WIDE_WARPS, ME_MIN_BLOCKS)
     }
     __syncthreads();
     uint32_t parity = 0;
+    int fenced = -1;  // the frame whose tensor maps this CTA has acquired
     int h = 1 + int(blockIdx.x & 1);  // this CTA's pool: frames 1, 3, ... or 2, 4, ...
     while (h < pp.n) {
         if (threadIdx.x == 0) ticket = atomicAdd(pp.ctr + h, 1);
@@ -2002,7 +2014,9 @@ __global__ void __launch_bounds__(32 * ME_WIDE_WARPS, ME_MIN_BLOCKS)
             // frame 1's reference (frame 0) is built before the launch
             wide_mb<BAL, LEARN, true>(pp.fds[h], pp.rds[h], item % pp.mb_w, item / pp.mb_w, prm,
                                       reinterpret_cast<unsigned long long*>(ff + pp.ew_off), ff + pp.dfl_off,
-                                      h > 1 ? &bwait : nullptr, epoch, status, spin_limit, win, bar, parity);
+                                      h > 1 ? &bwait : nullptr, epoch, status, spin_limit, win, bar, parity,
+                                      fenced != h);
+            fenced = h;
             __syncthreads();  // every read and write of the MB is done
             if (threadIdx.x == 0) {
                 const int c = atom_add_acq_rel(pp.done + h, 1);
@@ -2400,22 +2414,23 @@ int h264a::me_frames_run(h264a_ctx* ctx, const h264a_me_frame* h_frames, int nfr
     if (seg[nseg] != total) return fail(H264A_E_ARG, "me_frames: internal queue layout error");
     // The wide kernel (launches of at most ME_WIDE_MAXF frames) publishes MV
     // words (2 * EW_PER_MB ints per MB), then the fused reconstruction's
-    // deblocking flags; its MVs are packed as i16, so the padded pictures must
-    // be at most 8191 samples wide and high.
+    // deblocking flags, in its own queue's flag space (cleared per launch);
+    // its MVs are packed as i16, so the padded pictures must be at most 8191
+    // samples wide and high.
     bool wide = nframes <= ME_WIDE_MAXF;
     for (int k = 0; k < nframes; k++)
         if (desc[k].pic.cw + 2 * desc[k].pic.pad > 8191 || desc[k].pic.ch + 2 * desc[k].pic.pad > 8191) wide = false;
     if (rec && !wide) return fail(H264A_E_ARG, "me_frames: the fused reconstruction needs pictures of at most 8191 - 2 pad samples");
-    int rc = ensure_me_scratch(ctx, size_t(wide ? (2 * EW_PER_MB + (rec ? 1 : 0)) * total : total));
-    if (rc) return rc;
-    H264A_CUDA(cudaMemsetAsync(ctx->q[Q_MAIN].d_counter, 0, sizeof(int32_t), st));
-    const int epoch = next_epoch(ctx, st);
-    if (epoch < 0) return H264A_E_CUDA;
-    long long blocks = (long long)ctx->num_sms * per_sm;
-    const long long need = (total + ME_WARPS - 1) / ME_WARPS;
-    if (blocks > need) blocks = need;
     if (wide) {
-        // few frames: a CTA per MB, the partitions a team of two warps each
+        // few frames: a CTA per MB, the partitions one warp each
+        const size_t nflags = size_t(2 * EW_PER_MB + (rec ? 1 : 0)) * size_t(total);
+        int rc = ensure_me_scratch(ctx, nflags, Q_WIDE);
+        if (rc) return rc;
+        WorkQueue& qw = ctx->q[Q_WIDE];
+        H264A_CUDA(cudaMemsetAsync(qw.d_counter, 0, sizeof(int32_t), st));
+        H264A_CUDA(cudaMemsetAsync(qw.d_flags, 0, sizeof(int32_t) * nflags, st));
+        const int epoch = next_epoch(ctx, st, Q_WIDE);
+        if (epoch < 0) return H264A_E_CUDA;
         int wide_sm = 0;
         rc0 = me_wide_setup(wide_sm);
         if (rc0) return rc0;
@@ -2431,10 +2446,18 @@ int h264a::me_frames_run(h264a_ctx* ctx, const h264a_me_frame* h_frames, int nfr
         }
         wb.nseg = make_segments(wb.f, wb.n, wb.seg_start, wb.seg_j);
         if (wb.seg_start[wb.nseg] != total) return fail(H264A_E_ARG, "me_frames: internal queue layout error");
-        launch_me_frames_wide(prm, unsigned(wblocks), st, wb, total, ctx->q[Q_MAIN].d_counter, ctx->q[Q_MAIN].d_flags,
-                              epoch, ctx->d_status, learn != nullptr, rec != nullptr);
+        launch_me_frames_wide(prm, unsigned(wblocks), st, wb, total, qw.d_counter, qw.d_flags, epoch, ctx->d_status,
+                              learn != nullptr, rec != nullptr);
         return check_launch("me_frames_wide_kernel");
     }
+    int rc = ensure_me_scratch(ctx, size_t(total));
+    if (rc) return rc;
+    H264A_CUDA(cudaMemsetAsync(ctx->q[Q_MAIN].d_counter, 0, sizeof(int32_t), st));
+    const int epoch = next_epoch(ctx, st);
+    if (epoch < 0) return H264A_E_CUDA;
+    long long blocks = (long long)ctx->num_sms * per_sm;
+    const long long need = (total + ME_WARPS - 1) / ME_WARPS;
+    if (blocks > need) blocks = need;
     if (nframes <= ME_MAXF) {
         FrameBatch fb;
         memset(&fb, 0, sizeof fb);
@@ -2761,9 +2784,9 @@ int h264a::closed_pipe_run(h264a_ctx* ctx, const ClosedPipeIn& in, const h264a_m
     const long long head = (2LL * n + 1) & ~1LL;
     const long long need = head + pp.fstride * n;
     if (need >= (1LL << 31)) return fail(H264A_E_ARG, "closed loop: too many macroblocks for one launch");
-    rc = ensure_me_scratch(ctx, size_t(need));
+    rc = ensure_me_scratch(ctx, size_t(need), Q_WIDE);
     if (rc) return rc;
-    int* fl = ctx->q[Q_MAIN].d_flags;
+    int* fl = ctx->q[Q_WIDE].d_flags;
     pp.ctr = fl;
     pp.done = fl + n;
     pp.flags = fl + head;
@@ -2778,8 +2801,10 @@ int h264a::closed_pipe_run(h264a_ctx* ctx, const ClosedPipeIn& in, const h264a_m
     pp.word_out = (pw % 4 == 0) && ((reinterpret_cast<uintptr_t>(in.planes) & 3) == 0) && (pbytes % 4 == 0);
     pp.frame_words = frame_words;
     pp.ftoken = token;
-    H264A_CUDA(cudaMemsetAsync(fl, 0, sizeof(int) * size_t(2 * n), st));
-    const int epoch = next_epoch(ctx, st);
+    // counters zero, and no word of an earlier launch's layout left to be
+    // mistaken for a flag of this one
+    H264A_CUDA(cudaMemsetAsync(fl, 0, sizeof(int) * size_t(need), st));
+    const int epoch = next_epoch(ctx, st, Q_WIDE);
     if (epoch < 0) return H264A_E_CUDA;
     long long blocks = (long long)ctx->num_sms * per_sm;
     blocks &= ~1LL;  // the two pools, even and odd blocks
@@ -2799,6 +2824,320 @@ int h264a::closed_pipe_run(h264a_ctx* ctx, const ClosedPipeIn& in, const h264a_m
         closed_pipe_kernel<false, false><<<unsigned(blocks), 32 * ME_WIDE_WARPS, sm, st>>>(pp, prm, epoch,
                                                                                           ctx->d_status, SPIN_LIMIT);
     rc = check_launch("closed_pipe_kernel");
+    if (rc) return rc;
+    return table_done(ctx, st);
+}
+
+// ---------------------------------------------------------------------------
+// Plain-ME frames over several reference pictures
+// ---------------------------------------------------------------------------
+// best_part's loop over references (mb16.rs:4921-4960) in the frame model:
+// every search (the 16x16, and the four partitions when its J exceeds the
+// gate) runs on each reference r with seeds [predict_mv(a, b, c, r), extra],
+// costs plus (lambda * ref_bits(r, nref)) truncated to i64, the strictly
+// cheapest kept (references in order).  An MV predicts only from neighbours
+// of the same reference (inter.rs:36-69), so a pick carries each half's
+// reference index: 8 i32 per MB (shape, ref0, mv0x, mv0y, ref1, mv1x, mv1y,
+// 4x4-block evaluations).  One warp per MB, the narrow kernel's queue and
+// wavefront; the window is staged again for each reference.
+constexpr int ME_MAXREF = 4;
+struct FrameDescMR {
+    CUtensorMap tmap[ME_MAXREF];  // each reference's planes as the window's 3D tensor
+    const uint8_t* planes[ME_MAXREF];
+    const uint8_t* src;
+    double lambda_me;
+    long long split_gate;
+    int32_t* picks;
+    int64_t* costs;
+    int nref, cw, ch, pad, mb_w, mb_h, flag_base, tmap_ok;
+};
+
+// ref_bits (mb16.rs:5967-5981).
+__device__ __forceinline__ uint32_t ref_bits_of(int r, int nref) {
+    if (nref <= 1) return 0;
+    if (nref == 2) return 1;
+    return 1u + 2u * (31u - uint32_t(__clz(r + 1)));
+}
+
+// predict_mv (inter.rs:36-69) against reference cur: neighbours with their
+// reference indices (available ones are inter, index >= 0).
+__device__ __forceinline__ int2 predict_mv_ref(bool aa, int2 a, int ra, bool ba, int2 b, int rb, bool ca, int2 c, int rc,
+                                               int cur) {
+    int2 mva = aa ? a : make_int2(0, 0), mvb = ba ? b : make_int2(0, 0), mvc = ca ? c : make_int2(0, 0);
+    int qa = aa ? ra : -1, qb = ba ? rb : -1, qc = ca ? rc : -1;
+    if (!ba && !ca && aa) { mvb = mva; qb = qa; mvc = mva; qc = qa; }
+    const int matches = (qa == cur) + (qb == cur) + (qc == cur);
+    if (matches == 1) return qa == cur ? mva : (qb == cur ? mvb : mvc);
+    auto med = [](int x, int y, int z) { return x + y + z - min(min(x, y), z) - max(max(x, y), z); };
+    return make_int2(med(mva.x, mvb.x, mvc.x), med(mva.y, mvb.y, mvc.y));
+}
+
+// The MV and reference of neighbour MB `m`'s 4x4 block (bx4, by4).
+__device__ __forceinline__ int2 pick_mr_at(const int32_t* picks, int m, int bx4, int by4, int& ref) {
+    const int32_t* p = picks + 8 * m;
+    const int shape = __ldcg(p);
+    const int part = shape == 1 ? (by4 >= 2) : (shape == 2 ? (bx4 >= 2) : 0);
+    ref = __ldcg(p + 1 + 3 * part);
+    return make_int2(__ldcg(p + 2 + 3 * part), __ldcg(p + 3 + 3 * part));
+}
+
+template <bool BAL>
+__global__ void __launch_bounds__(32 * ME_WARPS, ME_MIN_BLOCKS)
+    me_frames_mr_kernel(const FrameDescMR* __restrict__ fds, const long long* __restrict__ seg_start,
+                        const int* __restrict__ seg_j, int nf, int ns, long long total,
+                        const __grid_constant__ MeParamsDev prm, int* __restrict__ counter, int* __restrict__ flags,
+                        int epoch, int* __restrict__ status, int spin_limit) {
+    __shared__ WarpScratch scratch[ME_WARPS];
+    __shared__ __align__(8) unsigned long long win_bar[ME_WARPS];
+    extern __shared__ __align__(128) uint8_t me_win[];
+    const int w = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const uint32_t win = uint32_t(__cvta_generic_to_shared(me_win)) + uint32_t(w * WIN_BYTES);
+    const uint32_t bar = uint32_t(__cvta_generic_to_shared(&win_bar[w]));
+    if (lane == 0) {
+        mbar_init(bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncwarp();
+    uint32_t parity = 0;
+    for (;;) {
+        int t = 0;
+        if (lane == 0) t = atomicAdd(counter, 1);
+        t = __shfl_sync(0xffffffffu, t, 0);
+        if (t >= total) return;
+        int s = 0;
+        while (s + 1 < ns && __ldg(seg_start + s + 1) <= t) s++;
+        const int j = __ldg(seg_j + s);
+        const long long u = t - __ldg(seg_start + s);
+        const int nxt = j + 1 < nf ? fds[j + 1].mb_w * fds[j + 1].mb_h : 0;
+        const FrameDescMR& fd = fds[int(u % (j + 1))];
+        const int k = nxt + int(u / (j + 1));
+        int mbx, mby;
+        wave_mb(fd.mb_w, fd.mb_h, k, mbx, mby);
+        const int m = mby * fd.mb_w + mbx;
+        int* fl = flags + fd.flag_base;
+        const int lx = mbx * 16, ly = mby * 16;
+        uint32_t src4[4];
+#pragma unroll
+        for (int r = 0; r < 4; r++)
+            src4[r] = ld4u(fd.src + (long long)(ly + ((lane >> 2) & 3) * 4 + r) * fd.cw + lx + (lane & 3) * 4);
+        if (lane == 0) {
+            if (mbx > 0) wait_flag(fl + m - 1, epoch, status, 1, spin_limit);
+            if (mby > 0) wait_flag(fl + m - fd.mb_w + (mbx < fd.mb_w - 1 ? 1 : 0), epoch, status, 1, spin_limit);
+        }
+        __syncwarp();
+        const bool aa = mbx > 0, ba = mby > 0, ca = mby > 0 && mbx < fd.mb_w - 1, da = mbx > 0 && mby > 0;
+        int ra = -1, rb = -1, rc = -1;
+        const int2 a = aa ? pick_mr_at(fd.picks, m - 1, 3, 0, ra) : make_int2(0, 0);
+        const int2 bb = ba ? pick_mr_at(fd.picks, m - fd.mb_w, 0, 3, rb) : make_int2(0, 0);
+        int2 c = make_int2(0, 0);
+        if (ca) c = pick_mr_at(fd.picks, m - fd.mb_w + 1, 0, 3, rc);
+        else if (da) c = pick_mr_at(fd.picks, m - fd.mb_w - 1, 3, 3, rc);
+        const bool cav = ca || da;
+        const int pw = fd.cw + 2 * fd.pad, ph = fd.ch + 2 * fd.pad;
+        // best_part of the 16x16 over the references, then, J above the gate,
+        // of each partition (lane group g = partition g) over the references
+        int evals = 0, shape = 0;
+        int ref16 = 0, mv16x = 0, mv16y = 0;
+        long long c16 = LLONG_MAX;
+        int pref = 0, pmx = 0, pmy = 0;  // the lane's partition's best (mode 1)
+        long long pcost = LLONG_MAX;
+        for (int mode = 0; mode < 2; mode++) {
+            if (mode == 1 && !(fd.split_gate >= 0 && c16 > fd.split_gate)) break;
+            for (int r = 0; r < fd.nref; r++) {
+                const int2 pmv = predict_mv_ref(aa, a, ra, ba, bb, rb, cav, c, rc, r);
+                h264a_picture pc{fd.src, fd.planes[r], fd.cw, fd.ch, fd.pad};
+                const bool win_ok = ((reinterpret_cast<uintptr_t>(pc.d_planes) | uintptr_t(pw)) & 15) == 0 &&
+                                    pw >= WIN_W && ph >= WIN_H;
+                if (win_ok) {
+                    const int wx0 = min(max((lx + pc.pad + (pmv.x >> 2) - WIN_R) & ~15, 0), pw - WIN_W);
+                    const int wy0 = min(max(ly + pc.pad + (pmv.y >> 2) - WIN_R, 0), ph - WIN_H);
+                    if (lane == 0) {
+                        scratch[w].wx0 = wx0;
+                        scratch[w].wy0 = wy0;
+                        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                        if (fd.tmap_ok) {
+                            mbar_expect_tx(bar, uint32_t(WIN_BYTES));
+                            // a tensor map written to device memory by the host since an
+                            // earlier launch read that address: acquire it for the copy
+                            asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&fd.tmap[r])
+                                         : "memory");
+                            tma_load_3d(win, &fd.tmap[r], wx0, wy0, 0, bar);
+                        } else {
+                            mbar_expect_tx(bar, uint32_t(4 * WIN_H * WIN_W));
+                        }
+                    }
+                    __syncwarp();
+                    if (!fd.tmap_ok) {
+                        const long long ps = (long long)pw * ph;
+                        for (int i = lane; i < 4 * WIN_H; i += 32) {
+                            const int pl = i / WIN_H, rr = i - pl * WIN_H;
+                            bulk_g2s(win + uint32_t(pl * WIN_PLANE + rr * WIN_STRIDE),
+                                     pc.d_planes + ps * pl + (long long)(wy0 + rr) * pw + wx0, WIN_W, bar);
+                        }
+                    }
+                }
+                if (lane == 0) scratch[w].win_ok = win_ok;
+                __syncwarp();
+                GroupGeom qg;
+                group_geom_init(qg, scratch[w], pc, lx, ly, mode, win, mode == 0 ? src4 : nullptr);
+                if (win_ok) {
+                    wait_window(bar, parity, status, 3, spin_limit);
+                    parity ^= 1u;
+                }
+                int preds[4] = {pmv.x, pmv.y, mv16x, mv16y};
+                int rx, ry, ev;
+                long long cst;
+                motion_search_group<BAL>(qg, prm, scratch[w], preds, mode == 0 ? 1 : 2, fd.lambda_me, rx, ry, cst, ev);
+                cst += __double2ll_rz(__dmul_rn(fd.lambda_me, double(ref_bits_of(r, fd.nref))));
+                if (mode == 0) {
+                    evals += ev << 4;
+                    if (cst < c16) { c16 = cst; ref16 = r; mv16x = rx; mv16y = ry; }
+                } else {
+                    // every lane of group g holds partition g's result
+                    evals += (__shfl_sync(0xffffffffu, ev, 0) + __shfl_sync(0xffffffffu, ev, 8) +
+                              __shfl_sync(0xffffffffu, ev, 16) + __shfl_sync(0xffffffffu, ev, 24)) << 3;
+                    if (cst < pcost) { pcost = cst; pref = r; pmx = rx; pmy = ry; }
+                }
+                __syncwarp();  // the window's reads are done before the next copy
+            }
+        }
+        // the shape decision (mb16.rs:8869-8913)
+        int s0r = ref16, s0x = mv16x, s0y = mv16y, s1r = ref16, s1x = mv16x, s1y = mv16y;
+        long long best = c16;
+        if (fd.split_gate >= 0 && c16 > fd.split_gate) {
+            long long pc4[4];
+            int pr4[4], px4[4], py4[4];
+#pragma unroll
+            for (int gi = 0; gi < 4; gi++) {
+                pc4[gi] = __shfl_sync(0xffffffffu, pcost, 8 * gi);
+                pr4[gi] = __shfl_sync(0xffffffffu, pref, 8 * gi);
+                px4[gi] = __shfl_sync(0xffffffffu, pmx, 8 * gi);
+                py4[gi] = __shfl_sync(0xffffffffu, pmy, 8 * gi);
+            }
+            if (pc4[0] + pc4[1] < best) {
+                best = pc4[0] + pc4[1]; shape = 1;
+                s0r = pr4[0]; s0x = px4[0]; s0y = py4[0]; s1r = pr4[1]; s1x = px4[1]; s1y = py4[1];
+            }
+            if (pc4[2] + pc4[3] < best) {
+                best = pc4[2] + pc4[3]; shape = 2;
+                s0r = pr4[2]; s0x = px4[2]; s0y = py4[2]; s1r = pr4[3]; s1x = px4[3]; s1y = py4[3];
+            }
+        }
+        if (lane == 0) {
+            int32_t* p = fd.picks + 8 * m;
+            p[0] = shape; p[1] = s0r; p[2] = s0x; p[3] = s0y; p[4] = s1r; p[5] = s1x; p[6] = s1y; p[7] = evals;
+            fd.costs[2 * m] = best;
+            fd.costs[2 * m + 1] = c16;
+            st_release(fl + m, epoch);  // orders the pick's stores before the flag
+        }
+        __syncwarp();
+    }
+}
+
+static int me_mr_setup_once() {
+    const int smem = ME_WARPS * WIN_BYTES;
+    H264A_CUDA(cudaFuncSetAttribute(me_frames_mr_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    H264A_CUDA(cudaFuncSetAttribute(me_frames_mr_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    return H264A_OK;
+}
+
+extern "C" int h264a_me_frames_multiref(h264a_ctx* ctx, const h264a_me_mr_frame* h_frames, int nframes,
+                                        const h264a_me_params* params, void* stream) {
+    if (!ctx || !h_frames || !params) return fail(H264A_E_ARG, "me_frames_multiref: null pointer");
+    if (nframes < 1) return fail(H264A_E_ARG, "me_frames_multiref: need at least one frame");
+    if ((params->mv_cost_kind == 1 || params->mv_cost_kind == 2) && !params->d_mv_cost_tab)
+        return fail(H264A_E_ARG, "me_frames_multiref: mv cost kinds 1 and 2 need d_mv_cost_tab");
+    for (int i = 0; i < nframes; i++) {
+        const h264a_me_mr_frame& f = h_frames[i];
+        if (f.nref < 1 || f.nref > ME_MAXREF) return fail(H264A_E_ARG, "me_frames_multiref: 1 to 4 references per frame");
+        if (!f.d_src || !f.d_picks || !f.d_costs) return fail(H264A_E_ARG, "me_frames_multiref: null frame pointer");
+        for (int r = 0; r < f.nref; r++)
+            if (!f.d_planes[r]) return fail(H264A_E_ARG, "me_frames_multiref: null reference planes");
+        if (f.cw < 16 || f.ch < 16 || f.cw % 16 || f.ch % 16 || f.pad < 3 || f.pad > 128)
+            return fail(H264A_E_ARG, "me_frames_multiref: frames must be MB-aligned with 3 <= pad <= 128");
+        if ((long long)(f.cw / 16) * (f.ch / 16) > (1 << 24)) return fail(H264A_E_ARG, "me_frames_multiref: frame too large");
+    }
+    static std::once_flag once;
+    static int setup_rc = 0;
+    std::call_once(once, [] { setup_rc = me_mr_setup_once(); });
+    if (setup_rc) return setup_rc;
+    cudaStream_t st = pick_stream(ctx, stream);
+    const MeParamsDev prm = to_dev(*params);
+    std::vector<int> order(nframes);
+    for (int i = 0; i < nframes; i++) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        return (long long)h_frames[a].cw * h_frames[a].ch > (long long)h_frames[b].cw * h_frames[b].ch;
+    });
+    std::vector<FrameDescMR> desc(nframes);
+    memset(desc.data(), 0, sizeof(FrameDescMR) * nframes);
+    std::vector<FrameDesc> segd(nframes);  // the sizes, for the queue's segments
+    memset(segd.data(), 0, sizeof(FrameDesc) * nframes);
+    long long total = 0;
+    for (int k = 0; k < nframes; k++) {
+        const h264a_me_mr_frame& f = h_frames[order[k]];
+        FrameDescMR& d = desc[k];
+        const int pw = f.cw + 2 * f.pad, ph = f.ch + 2 * f.pad;
+        d.tmap_ok = 1;
+        for (int r = 0; r < f.nref; r++) {
+            d.planes[r] = f.d_planes[r];
+            d.tmap_ok &= encode_window_map(&d.tmap[r], f.d_planes[r], pw, ph);
+        }
+        d.src = f.d_src;
+        d.lambda_me = f.lambda_me;
+        d.split_gate = f.split_gate;
+        d.picks = f.d_picks;
+        d.costs = f.d_costs;
+        d.nref = f.nref;
+        d.cw = f.cw; d.ch = f.ch; d.pad = f.pad;
+        d.mb_w = f.cw / 16;
+        d.mb_h = f.ch / 16;
+        d.flag_base = int(total);
+        segd[k].mb_w = d.mb_w;
+        segd[k].mb_h = d.mb_h;
+        total += (long long)d.mb_w * d.mb_h;
+        if (total >= (1LL << 31)) return fail(H264A_E_ARG, "me_frames_multiref: too many macroblocks in one call");
+    }
+    std::vector<long long> seg(nframes + 1);
+    std::vector<int> segj(nframes);
+    const int nseg = make_segments(segd.data(), nframes, seg.data(), segj.data());
+    if (seg[nseg] != total) return fail(H264A_E_ARG, "me_frames_multiref: internal queue layout error");
+    const size_t b_desc = sizeof(FrameDescMR) * nframes, b_seg = sizeof(long long) * (nseg + 1),
+                 b_j = sizeof(int) * nseg, bytes = b_desc + b_seg + b_j;
+    char* hst = nullptr;
+    int rc = table_host(ctx, bytes, &hst);
+    if (rc) return rc;
+    memcpy(hst, desc.data(), b_desc);
+    memcpy(hst + b_desc, seg.data(), b_seg);
+    memcpy(hst + b_desc + b_seg, segj.data(), b_j);
+    rc = table_upload(ctx, bytes, st);
+    if (rc) return rc;
+    rc = ensure_me_scratch(ctx, size_t(total));
+    if (rc) return rc;
+    H264A_CUDA(cudaMemsetAsync(ctx->q[Q_MAIN].d_counter, 0, sizeof(int32_t), st));
+    const int epoch = next_epoch(ctx, st);
+    if (epoch < 0) return H264A_E_CUDA;
+    int per_sm = 0;
+    H264A_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, me_frames_mr_kernel<true>, 32 * ME_WARPS,
+                                                             ME_WARPS * WIN_BYTES));
+    if (per_sm < 1) per_sm = 1;
+    long long blocks = (long long)ctx->num_sms * per_sm;
+    const long long need = (total + ME_WARPS - 1) / ME_WARPS;
+    if (blocks > need) blocks = need;
+    char* dv = static_cast<char*>(ctx->me_tab);
+    const auto* dfd = reinterpret_cast<const FrameDescMR*>(dv);
+    const auto* dseg = reinterpret_cast<const long long*>(dv + b_desc);
+    const auto* dj = reinterpret_cast<const int*>(dv + b_desc + b_seg);
+    const size_t sm = ME_WARPS * WIN_BYTES;
+    if (balanced_preset(prm))
+        me_frames_mr_kernel<true><<<unsigned(blocks), 32 * ME_WARPS, sm, st>>>(
+            dfd, dseg, dj, nframes, nseg, total, prm, ctx->q[Q_MAIN].d_counter, ctx->q[Q_MAIN].d_flags, epoch,
+            ctx->d_status, SPIN_LIMIT);
+    else
+        me_frames_mr_kernel<false><<<unsigned(blocks), 32 * ME_WARPS, sm, st>>>(
+            dfd, dseg, dj, nframes, nseg, total, prm, ctx->q[Q_MAIN].d_counter, ctx->q[Q_MAIN].d_flags, epoch,
+            ctx->d_status, SPIN_LIMIT);
+    rc = check_launch("me_frames_mr_kernel");
     if (rc) return rc;
     return table_done(ctx, st);
 }

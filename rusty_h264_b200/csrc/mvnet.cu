@@ -15,7 +15,8 @@
 // zeros] = 1168 -> FC1 -> 256 -> head -> 296 logits (289 classes: full-pel
 // offsets dx, dy in -8..8, class (dy+8)*17 + dx+8).  ReLU after every layer
 // but the head.  Activations are stored as bf16 (NHWC), every product runs on
-// the tensor cores (mma.sync m16n8k16, bf16 operands, fp32 accumulators).
+// the tensor cores (tcgen05.mma, bf16 operands, fp32 accumulators in tensor
+// memory).
 //
 // Every layer is one implicit GEMM: C[M][N] = sum_k A[m][k] B[k][n], with A
 // and B gathered on the fly by a functor (im2col of a stride-2 3x3 window, a
@@ -29,6 +30,7 @@
 #include <string>
 #include <vector>
 
+#include "h264a_device.cuh"
 #include "h264accel_internal.h"
 
 namespace h264a {
@@ -93,86 +95,161 @@ __device__ __forceinline__ bf16_t mv_feat(const Geo& g, int m, int i) {
     return f2bf(float(v) * (1.f / 64.f));  // exact
 }
 
-// ---- the GEMM kernel --------------------------------------------------------
-constexpr int BM = 64, BK = 32, KW = BK / 2 + 4;  // smem rows of KW words (16 bf16 pairs + 4 pad)
+// ---- the tcgen05 GEMM: 128 x BN tiles, accumulators in tensor memory --------
+// The GEMM of every layer, C[M][N] = sum_k A[m][k] B[k][n] (op.a(m, k) /
+// op.b(k, n) gather the bf16 pair (k, k+1), zero past their tensor; op.store
+// takes each fp32 result; CTA z covers k in [z*kchunk, ...)), on the sm_100
+// tensor cores: per 64-wide K step all 256 threads gather the A (128 x 64)
+// and B (BN x 64) tiles into one of two shared-memory stages, one thread
+// issues four tcgen05.mma (M 128, N BN, K 16, bf16 in, fp32 accumulated in
+// tensor memory) and commits them to the stage's mbarrier, and the gathers of
+// the next step overlap them.  The epilogue reads the accumulator rows with
+// tcgen05.ld: warp w may read tensor-memory lanes 32(w % 4) .. +31 (its tile
+// rows), warps w and w + 4 taking half of the columns each.
+constexpr int TC_BM = 128, TC_BK = 64, TC_THREADS = 256;
 
-__device__ __forceinline__ void mma_bf16(float d[4], const uint32_t a[4], const uint32_t b[2]) {
-    asm volatile(
-        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-        "{%0,%1,%2,%3};\n"
-        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+template <int BN>
+constexpr int tc_cols() {
+    return BN <= 32 ? 32 : (BN <= 64 ? 64 : (BN <= 128 ? 128 : 256));
 }
 
-// C tile BM x BN per CTA of 4 warps (2 x 2, a warp BM/2 x BN/2); CTA z covers
-// k in [z*kchunk, min(K, (z+1)*kchunk)).  K and kchunk are even; op.a(m, k) /
-// op.b(k, n) return the bf16 pair (k, k+1), zero past their tensor.
-template <int BN, class Op>
-__global__ void __launch_bounds__(128) gemm_kernel(const Op op, int M, int N, int K, int kchunk) {
-    static_assert(BN == 16 || BN == 32 || BN == 64, "tile width");
-    constexpr int NT = BN / 16;  // n8 tiles per warp
-    __shared__ uint32_t As[BM][KW];
-    __shared__ uint32_t Bs[BN][KW];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int g = lane >> 2, t = lane & 3;
-    const int wm = warp >> 1, wn = warp & 1;
-    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
-    const int kb = blockIdx.z * kchunk, ke = min(K, kb + kchunk);
-    float acc[2][NT][4];
-#pragma unroll
-    for (int i = 0; i < 2; i++)
-#pragma unroll
-        for (int j = 0; j < NT; j++)
-#pragma unroll
-            for (int r = 0; r < 4; r++) acc[i][j][r] = 0.f;
-    for (int k0 = kb; k0 < ke; k0 += BK) {
-#pragma unroll
-        for (int i = 0; i < BM * (BK / 2) / 128; i++) {
-            const int p = tid + i * 128, row = p >> 4, kp = p & 15;
-            const int m = m0 + row, k = k0 + 2 * kp;
-            As[row][kp] = (m < M && k < ke) ? op.a(m, k) : 0u;
-        }
-#pragma unroll
-        for (int i = 0; i < BN * (BK / 2) / 128; i++) {
-            const int p = tid + i * 128, col = p >> 4, kp = p & 15;
-            const int n = n0 + col, k = k0 + 2 * kp;
-            Bs[col][kp] = (n < N && k < ke) ? op.b(k, n) : 0u;
-        }
-        __syncthreads();
-#pragma unroll
-        for (int ks = 0; ks < BK / 2; ks += 8) {
-            uint32_t a[2][4], b[NT][2];
-#pragma unroll
-            for (int i = 0; i < 2; i++) {
-                const int r = wm * 32 + i * 16 + g;
-                a[i][0] = As[r][ks + t];
-                a[i][1] = As[r + 8][ks + t];
-                a[i][2] = As[r][ks + 4 + t];
-                a[i][3] = As[r + 8][ks + 4 + t];
-            }
-#pragma unroll
-            for (int j = 0; j < NT; j++) {
-                const int c = wn * (BN / 2) + j * 8 + g;
-                b[j][0] = Bs[c][ks + t];
-                b[j][1] = Bs[c][ks + 4 + t];
-            }
-#pragma unroll
-            for (int i = 0; i < 2; i++)
-#pragma unroll
-                for (int j = 0; j < NT; j++) mma_bf16(acc[i][j], a[i], b[j]);
-        }
-        __syncthreads();
+// A K-major operand tile of R rows x 64 k (bf16) in the canonical
+// no-swizzle UMMA layout: 8x8 core matrices of 128 contiguous bytes (8 rows
+// of 16 bytes), the eight k-chunks of an 8-row group 128 bytes apart (the
+// leading byte offset) and the groups 1024 bytes apart (the stride byte
+// offset).  Byte offset of (row, k-chunk):
+__device__ __forceinline__ uint32_t tc_off(int row, int chunk) {
+    return uint32_t(((row >> 3) * 8 + chunk) * 128 + (row & 7) * 16);
+}
+// The shared-memory matrix descriptor of such a tile from shared address a:
+// start >> 4 (bits 0-13), leading byte offset 128 >> 4 (16-29), stride byte
+// offset 1024 >> 4 (32-45), descriptor version 1 (46-47), base offset 0,
+// layout SWIZZLE_NONE (61-63).
+__device__ __forceinline__ uint64_t tc_sdesc(uint32_t a) {
+    return uint64_t((a >> 4) & 0x3fffu) | (uint64_t(128 >> 4) << 16) | (uint64_t(1024 >> 4) << 32) | (1ull << 46);
+}
+// The instruction descriptor of kind::f16: fp32 accumulator (bits 4-5 = 1),
+// A and B bf16 (7-9 = 1, 10-12 = 1), both K-major (15, 16 = 0), N >> 3
+// (17-22), M >> 4 (24-28).
+template <int BN>
+constexpr uint32_t tc_idesc() {
+    return (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(BN >> 3) << 17) | (uint32_t(TC_BM >> 4) << 24);
+}
+
+__device__ __forceinline__ uint32_t tc_smem_u32(const void* p) { return uint32_t(__cvta_generic_to_shared(p)); }
+
+// Waits (bounded) for phase `parity` of an mbarrier; on timeout records 4 in
+// status and keeps waiting up to twice as long, so that no tensor-core work
+// is left reading a stage or writing tensor memory.
+__device__ __forceinline__ void tc_wait(uint32_t bar, uint32_t parity, int* status) {
+    constexpr int kLimit = 1 << 22;
+    for (int it = 0; !mbar_try_wait(bar, parity); it++) {
+        if (it == kLimit && status != nullptr) atomicCAS(status, 0, 4);
+        if (it >= 2 * kLimit) break;
     }
+}
+
+template <int BN, class Op>
+__global__ void __launch_bounds__(TC_THREADS) gemm_tc_kernel(const Op op, int M, int N, int K, int kchunk, int* status) {
+    static_assert(BN % 16 == 0 && BN >= 16 && BN <= 256, "tcgen05 N for M = 128");
+    constexpr int A_BYTES = TC_BM * TC_BK * 2, B_BYTES = BN * TC_BK * 2, STAGE = A_BYTES + B_BYTES;
+    constexpr int NCOL = tc_cols<BN>();
+    constexpr uint32_t IDESC = tc_idesc<BN>();
+    extern __shared__ __align__(128) uint8_t tc_smem[];
+    __shared__ __align__(8) unsigned long long tc_bar[2];
+    __shared__ uint32_t tc_tmem;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int m0 = blockIdx.x * TC_BM, n0 = blockIdx.y * BN;
+    const int kb = blockIdx.z * kchunk, ke = min(K, kb + kchunk);
+    const uint32_t sbase = tc_smem_u32(tc_smem), bar0 = tc_smem_u32(&tc_bar[0]);
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tc_smem_u32(&tc_tmem)),
+                     "r"(NCOL));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) {
+        mbar_init(bar0, 1);
+        mbar_init(bar0 + 8, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tc_tmem;
+    const int nk = ke > kb ? (ke - kb + TC_BK - 1) / TC_BK : 0;
+    for (int it = 0; it < nk; it++) {
+        const int st = it & 1;
+        // the stage's previous MMAs (step it - 2) have read it
+        if (it >= 2) tc_wait(bar0 + 8 * st, uint32_t((it - 2) >> 1) & 1u, status);
+        const int k0 = kb + it * TC_BK;
+        const uint32_t sa = sbase + uint32_t(st * STAGE), sb = sa + A_BYTES;
+        // consecutive threads fill consecutive 16-byte rows of a core
+        // matrix, so a warp's stores meet no bank twice
+        for (int q = tid; q < TC_BM * 8; q += TC_THREADS) {
+            const int row = ((q >> 6) << 3) | (q & 7), c = (q >> 3) & 7, m = m0 + row, k = k0 + 8 * c;
+            uint32_t v[4];
 #pragma unroll
-    for (int i = 0; i < 2; i++)
+            for (int i = 0; i < 4; i++) v[i] = (m < M && k + 2 * i < ke) ? op.a(m, k + 2 * i) : 0u;
+            asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(sa + tc_off(row, c)), "r"(v[0]), "r"(v[1]),
+                         "r"(v[2]), "r"(v[3])
+                         : "memory");
+        }
+        for (int q = tid; q < BN * 8; q += TC_THREADS) {
+            const int row = ((q >> 6) << 3) | (q & 7), c = (q >> 3) & 7, n = n0 + row, k = k0 + 8 * c;
+            uint32_t v[4];
 #pragma unroll
-        for (int j = 0; j < NT; j++)
+            for (int i = 0; i < 4; i++) v[i] = (n < N && k + 2 * i < ke) ? op.b(k + 2 * i, n) : 0u;
+            asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(sb + tc_off(row, c)), "r"(v[0]), "r"(v[1]),
+                         "r"(v[2]), "r"(v[3])
+                         : "memory");
+        }
+        // the tiles' generic-proxy writes, visible to the tensor cores
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 #pragma unroll
-            for (int r = 0; r < 4; r++) {
-                const int m = m0 + wm * 32 + i * 16 + g + ((r & 2) ? 8 : 0);
-                const int n = n0 + wn * (BN / 2) + j * 8 + 2 * t + (r & 1);
-                if (m < M && n < N) op.store(m, n, acc[i][j][r]);
+            for (int j = 0; j < TC_BK / 16; j++) {
+                const uint64_t da = tc_sdesc(sa + 256u * j), db = tc_sdesc(sb + 256u * j);
+                const uint32_t acc = (it > 0 || j > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
+                    "l"(da), "l"(db), "r"(IDESC), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+                    : "memory");
             }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar0 +
+                                                                                                          8 * st)
+                         : "memory");
+        }
+    }
+    if (nk > 0) {
+        // the last step's commit completes after every earlier MMA
+        tc_wait(bar0 + 8 * ((nk - 1) & 1), uint32_t((nk - 1) >> 1) & 1u, status);
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const int row = m0 + (warp & 3) * 32 + lane;
+        const uint32_t taddr = tmem + (uint32_t((warp & 3) * 32) << 16);
+        const int cb = (warp >> 2) * (BN / 2);
+#pragma unroll 1
+        for (int c0 = cb; c0 < cb + BN / 2; c0 += 8) {
+            uint32_t r[8];
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                           "=r"(r[7])
+                         : "r"(taddr + uint32_t(c0)));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (row < M) {
+#pragma unroll
+                for (int i = 0; i < 8; i++) {
+                    const int n = n0 + c0 + i;
+                    if (n < N) op.store(row, n, __uint_as_float(r[i]));
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(NCOL));
 }
 
 // ---- the layers as GEMM operands --------------------------------------------
@@ -514,19 +591,25 @@ __global__ void guide_nmv_kernel(const int32_t* __restrict__ guide, int mb_w, in
 
 template <int BN, class Op>
 static void gemm(const Op& op, int M, int N, int K, cudaStream_t st, int splits = 1) {
+    constexpr int smem = 2 * (TC_BM * TC_BK * 2 + BN * TC_BK * 2);
+    static const bool attr_ok = [] {  // once per instantiation (the dynamic shared memory above 48 KB)
+        return cudaFuncSetAttribute(gemm_tc_kernel<BN, Op>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) ==
+               cudaSuccess;
+    }();
+    (void)attr_ok;
     int kchunk = K;
     if (splits > 1) {
         kchunk = (K + splits - 1) / splits;
-        kchunk = (kchunk + BK - 1) / BK * BK;
+        kchunk = (kchunk + TC_BK - 1) / TC_BK * TC_BK;
         splits = (K + kchunk - 1) / kchunk;
     }
-    dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN, splits);
-    gemm_kernel<BN, Op><<<grid, 128, 0, st>>>(op, M, N, K, kchunk);
+    dim3 grid((M + TC_BM - 1) / TC_BM, (N + BN - 1) / BN, splits);
+    gemm_tc_kernel<BN, Op><<<grid, TC_THREADS, smem, st>>>(op, M, N, K, kchunk, nullptr);
 }
 
 // split count of a weight-gradient GEMM: about 4 waves of CTAs
 static int wsplits(int M, int N, int BN, long long K, int sms) {
-    const long long tiles = (long long)((M + BM - 1) / BM) * ((N + BN - 1) / BN);
+    const long long tiles = (long long)((M + TC_BM - 1) / TC_BM) * ((N + BN - 1) / BN);
     long long s = (4LL * sms + tiles - 1) / tiles;
     const long long maxs = (K + 1023) / 1024;  // at least 1024 rows per CTA
     if (s > maxs) s = maxs;
@@ -654,23 +737,23 @@ void trunk_forward(h264a_mvnet* n, const Geo& g, cudaStream_t st) {
 void head_forward(h264a_mvnet* n, const Geo& g, cudaStream_t st) {
     const Bufs z = bufs(n);
     const int B = g.P * g.nmb;
-    gemm<64>(Fc1Fwd{g, z}, B, HID, FEAT, st);
-    gemm<64>(HeadFwd{z}, B, HEAD_N, HID, st);
+    gemm<256>(Fc1Fwd{g, z}, B, HID, FEAT, st);
+    gemm<160>(HeadFwd{z}, B, HEAD_N, HID, st);
 }
 
 void backward(h264a_mvnet* n, const Geo& g, cudaStream_t st) {
     const Bufs z = bufs(n);
     const int B = g.P * g.nmb, S = n->sms;
     const int K3 = g.P * g.H3 * g.W3, K2 = g.P * g.H2 * g.W2, K1 = g.P * g.H1 * g.W1;
-    gemm<64>(HeadBwdW{z, B}, HEAD_N, HID + 2, B, st, wsplits(HEAD_N, HID + 2, 64, B, S));
-    gemm<64>(HeadBwdData{z}, B, HID, HEAD_N, st);
-    gemm<64>(Fc1BwdW{g, z, B}, HID, FEAT + 2, B, st, wsplits(HID, FEAT + 2, 64, B, S));
-    gemm<64>(Fc1BwdData{z}, B, CONVF, HID, st);
+    gemm<160>(HeadBwdW{z, B}, HEAD_N, HID + 2, B, st, wsplits(HEAD_N, HID + 2, 160, B, S));
+    gemm<256>(HeadBwdData{z}, B, HID, HEAD_N, st);
+    gemm<256>(Fc1BwdW{g, z, B}, HID, FEAT + 2, B, st, wsplits(HID, FEAT + 2, 256, B, S));
+    gemm<256>(Fc1BwdData{z}, B, CONVF, HID, st);
     const long long cells = (long long)K3 * 16;
     uncrop_kernel<<<unsigned((cells + 255) / 256), 256, 0, st>>>(g, n->df, n->a3, n->da3);
-    gemm<64>(Conv3BwdW{g, z, K3}, 32, 9 * 32 + 2, K3, st, wsplits(32, 290, 64, K3, S));
+    gemm<160>(Conv3BwdW{g, z, K3}, 32, 9 * 32 + 2, K3, st, wsplits(32, 290, 160, K3, S));
     gemm<32>(Conv3BwdData{g, z}, K2, 32, 288, st);
-    gemm<64>(Conv2BwdW{g, z, K2}, 32, 9 * 16 + 2, K2, st, wsplits(32, 146, 64, K2, S));
+    gemm<160>(Conv2BwdW{g, z, K2}, 32, 9 * 16 + 2, K2, st, wsplits(32, 146, 160, K2, S));
     gemm<16>(Conv2BwdData{g, z}, K1, 16, 288, st);
     gemm<32>(Conv1BwdW{g, z, K1}, 16, 9 * 2 + 2, K1, st, wsplits(16, 20, 32, K1, S));
 }

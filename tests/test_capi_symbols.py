@@ -70,7 +70,8 @@ def test_struct_layouts_match_header(tmp_path):
                "h264a_tq_chroma_frame": accel.TqChromaFrame, "h264a_deblock_frame": accel.DeblockFrame,
                "h264a_me_learned_frame": accel.MeLearnedFrame, "h264a_closed_job": accel.ClosedJob,
                "h264a_closed_dev": accel.ClosedDev, "h264a_closed_step": accel.ClosedStep,
-               "h264a_stream_frames": accel.StreamFrames, "h264a_mvnet_frame": MvnetFrame}
+               "h264a_stream_frames": accel.StreamFrames, "h264a_mvnet_frame": MvnetFrame,
+               "h264a_me_mr_frame": accel.MeMrFrame}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "h264accel.h"', "int main(void) {"]
     for cname, py in mirrors.items():
         lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')

@@ -375,6 +375,77 @@ def test_me_frames_learned_matches_oracle(acc, prop_t):
         assert fell_total > 0
 
 
+def _mr_case(acc, frames, srcs, refs_of, lam, gate, params):
+    """GPU multi-reference picks for sources srcs (indices into frames) with
+    reference lists refs_of[i] (nearest first), and the oracle's."""
+    torch = acc.torch
+    n, ch, cw = frames.shape
+    nmb = (cw // 16) * (ch // 16)
+    d = dev(acc, frames)
+    planes = acc.hpel_build(d, 32)
+    pk = acc.zeros((len(srcs), nmb, 8), torch.int32)
+    co = acc.zeros((len(srcs), nmb, 2), torch.int64)
+    fr = []
+    for i, (sidx, refs) in enumerate(zip(srcs, refs_of)):
+        f = A.MeMrFrame()
+        f.d_src = d[sidx].data_ptr()
+        for r, ri in enumerate(refs):
+            f.d_planes[r] = planes[ri].data_ptr()
+        f.nref, f.cw, f.ch, f.pad = len(refs), cw, ch, 32
+        f.lambda_me, f.split_gate = lam, gate
+        f.d_picks, f.d_costs = pk[i].data_ptr(), co[i].data_ptr()
+        fr.append(f)
+    acc.me_frames_multiref(fr, params)
+    acc.sync()
+    got_p, got_c = pk.cpu().numpy(), co.cpu().numpy()
+    for i, (sidx, refs) in enumerate(zip(srcs, refs_of)):
+        ro = np.stack([frames[r] for r in refs])
+        po = np.stack([O.build_planes4(frames[r], 32) for r in refs])
+        wp, wc = O.me_frame_multiref(frames[sidx], ro, po, O.balanced_params(), lam, gate)
+        assert np.array_equal(got_p[i, :, :7], wp[:, :7]), (i, np.argwhere(got_p[i, :, :7] != wp[:, :7])[:4])
+        assert np.array_equal(got_c[i], wc), i
+    return got_p, got_c
+
+
+def test_me_frames_multiref_matches_oracle(acc):
+    """best_part over 3, 2 and 1 references (mb16.rs:4921-4960) in one
+    launch: the reference indices, MVs and costs of every pick equal the
+    oracle's, the picks use every reference, and with one reference the
+    picks and costs are those of h264a_me_frames."""
+    torch = acc.torch
+    y, _, _ = synth.cif_clip(6, 13)
+    clip = synth.coded_luma(y)
+    qp = 27
+    lam = float(np.sqrt(A.frame_lambda(qp)) * 1.25)
+    gate = A.split_gate_for_qp(qp)
+    params = A.default_me_params()
+    got_p, got_c = _mr_case(acc, clip, [5, 4, 3, 2], [[4, 3, 2], [3, 2], [2], [1, 0]], lam, gate, params)
+    assert set(np.unique(got_p[0, :, 1])) == {0, 1, 2}
+    assert (got_p[:, :, 0] > 0).any()
+    # one reference: the single-reference frame kernel's picks and costs
+    n, ch, cw = clip.shape
+    nmb = (cw // 16) * (ch // 16)
+    d = dev(acc, clip)
+    planes = acc.hpel_build(d, 32)
+    pk = acc.zeros((nmb, 6), torch.int32)
+    co = acc.zeros((nmb, 2), torch.int64)
+    acc.me_frames([A.MeFrame(A.Picture(d[3].data_ptr(), planes[2].data_ptr(), cw, ch, 32), lam, gate,
+                             pk.data_ptr(), co.data_ptr())], params)
+    acc.sync()
+    p1 = pk.cpu().numpy()
+    assert np.array_equal(got_p[2][:, [0, 2, 3, 5, 6]], p1[:, :5]) and np.array_equal(got_c[2], co.cpu().numpy())
+    assert np.array_equal(got_p[2][:, 7], p1[:, 5])  # the same evaluation counts
+
+
+def test_me_frames_multiref_720p_three_references(acc):
+    """A 1280x720 frame of the textured generator searched over its three
+    previous frames equals the oracle."""
+    y = synth.coded_luma(synth.hd_clip(5, 21, 1280, 720)[0])
+    qp = 30
+    lam = float(np.sqrt(A.frame_lambda(qp)) * 1.25)
+    _mr_case(acc, y, [4], [[3, 2, 1]], lam, A.split_gate_for_qp(qp), A.default_me_params())
+
+
 def test_me_frames_single_mb_and_flat(acc):
     flat = np.full((2, 16, 16), 90, np.uint8)
     rng = np.random.default_rng(3)

@@ -1057,3 +1057,45 @@ def test_mc_tq_oracle_matches_numpy_restatement(qp):
     forced[:, 1:5] = rng.integers(-160, 161, (len(forced), 4))
     for p in (picks, forced):
         assert np.array_equal(O.mc_tq_frame(src, ref, p, qp, 6), np_mc_tq_frame(src, ref, p, qp)), qp
+
+
+# ---------------------------------------------------------------------------
+# best_part over several references (mb16.rs:4921-4960)
+# ---------------------------------------------------------------------------
+
+def test_multiref_oracle_one_reference_is_plain_me():
+    """With one reference the multi-reference frame model is plain-ME: the
+    same shapes, MVs and costs, every reference index 0."""
+    from rusty_h264_b200 import accel as A
+    from rusty_h264_b200 import synth
+
+    y, _, _ = synth.cif_clip(3, 5)
+    c = synth.coded_luma(y)
+    qp = 27
+    lam = float(np.sqrt(A.frame_lambda(qp)) * 1.25)
+    gate = A.split_gate_for_qp(qp)
+    pl = O.build_planes4(c[1], 32)
+    mp, mc = O.me_frame_multiref(c[2], c[1:2], pl[None], O.balanced_params(), lam, gate)
+    wp, wc = O.me_frame(c[2], c[1], pl, O.balanced_params(), lam, gate)
+    assert np.array_equal(mp[:, [0, 2, 3, 5, 6]], wp[:, :5]) and np.array_equal(mc, wc)
+    assert not mp[:, [1, 4]].any()
+
+
+def test_multiref_oracle_identical_references_keep_the_nearest():
+    """Three copies of one reference: every search finds the same MV on each,
+    and ref_bits (te(v): ue(r) = 1, 3, 3 bits for r = 0, 1, 2, mb16.rs:5967)
+    makes reference 0 the strictly cheapest, so every pick uses reference 0
+    and its 16x16 cost is the single-reference one plus floor(lambda * 1)."""
+    from rusty_h264_b200 import accel as A
+    from rusty_h264_b200 import synth
+
+    y, _, _ = synth.cif_clip(3, 6)
+    c = synth.coded_luma(y)
+    qp = 27
+    lam = float(np.sqrt(A.frame_lambda(qp)) * 1.25)
+    pl = O.build_planes4(c[1], 32)
+    mp, mc = O.me_frame_multiref(c[2], np.stack([c[1]] * 3), np.stack([pl] * 3), O.balanced_params(), lam, -1)
+    wp, wc = O.me_frame(c[2], c[1], pl, O.balanced_params(), lam, -1)
+    assert not mp[:, [1, 4]].any()
+    assert np.array_equal(mp[:, [2, 3]], wp[:, [1, 2]])
+    assert np.array_equal(mc[:, 1], wc[:, 1] + int(lam * 1))
