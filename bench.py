@@ -180,64 +180,100 @@ def mixed_batch(acc, torch, streams, params, lam: float, gate: int):
     ms = float(np.median(ts))
     px = sum((f.shape[0] - 1) * f.shape[1] * f.shape[2] for f in streams)
     mbs = sum((f.shape[0] - 1) * (f.shape[1] // 16) * (f.shape[2] // 16) for f in streams)
-    ms3 = mixed_batch_3ref(acc, torch, bufs, params, lam, gate)
+    three = mixed_batch_3ref(acc, torch, bufs, params, lam, gate)
     return {"streams": "4 x 352x288, 6 x 1280x720, 4 x 1920x1080, 2 x 3840x2160; 30 frames each, 1080p generator",
             "p_frames": len(frames_all), "macroblocks": int(mbs), "me_ms": round(ms, 3),
             "me_mpx_s": round(px / (ms * 1e-3) / 1e6, 1), "launches": 1,
-            "me_3ref_ms": round(ms3, 3), "me_3ref_mpx_s": round(px / (ms3 * 1e-3) / 1e6, 1),
+            **three,
             "batched_equals_alone": True,
             "note": "plain-ME of all P frames (one reference, and up to three: the previous three pictures); "
                     "not part of value"}
 
 
-def mixed_batch_3ref(acc, torch, bufs, params, lam: float, gate: int) -> float:
-    """Plain-ME of every P frame of the mixed batch over up to three
-    references (the previous three source pictures' planes, nearest first) in
-    one h264a_me_frames_multiref launch.  Every stream's picks and costs must
-    equal the same stream run on its own; returns the median CUDA-event time
-    of the batched call in ms (3 warm-up, 5 timed)."""
+def mixed_batch_3ref(acc, torch, bufs, params, lam: float, gate: int) -> dict:
+    """The mixed batch through the batched runtime (h264a_batch_*): 8 P frames
+    of every stream per GOP step over up to three references (the previous
+    three source pictures, nearest first), each step one graph launch (the
+    planes of the step's frames, then one persistent launch over all 16
+    streams), in the launch shape the autotuner picked.  Every stream's picks
+    and costs must equal h264a_me_frames_multiref of that stream alone; the
+    four steps of the 29 P frames are timed with CUDA events (3 warm-up
+    passes, median of 5).  The tuner also runs on each resolution alone, to
+    report the shape it picks per resolution."""
     import ctypes as C
 
     from rusty_h264_b200 import accel as A
 
-    per_stream, outs = [], []
-    for d, planes, _, _ in bufs:
+    G, NSLOTS, NREF, PAD = 8, 32, 3, 32
+    rings, streams, alone = [], [], []
+    for d, _, _, _ in bufs:
         n, ch, cw = d.shape
         nmb = (cw // 16) * (ch // 16)
-        picks = torch.zeros((n, nmb, 8), dtype=torch.int32, device="cuda")
-        costs = torch.zeros((n, nmb, 2), dtype=torch.int64, device="cuda")
+        pb = 4 * (cw + 2 * PAD) * (ch + 2 * PAD)
+        src = torch.zeros((NSLOTS, ch, cw), dtype=torch.uint8, device="cuda")
+        src[:n].copy_(d)
+        planes = torch.zeros((NSLOTS, pb), dtype=torch.uint8, device="cuda")
+        picks = torch.zeros((NSLOTS, nmb, 8), dtype=torch.int32, device="cuda")
+        costs = torch.zeros((NSLOTS, nmb, 2), dtype=torch.int64, device="cuda")
+        rings.append((src, planes, picks, costs, n))
+        streams.append(A.BatchStream(cw, ch, PAD, src.data_ptr(), planes.data_ptr(), picks.data_ptr(),
+                                     costs.data_ptr(), lam, gate))
+    # the unbatched path: each stream's P frames in one h264a_me_frames_multiref call
+    for src, planes, picks, costs, n in rings:
+        ch, cw = src.shape[1], src.shape[2]
+        acc.hpel_build(src[: n - 1], PAD, out=planes[: n - 1])
         fr = []
-        for i in range(1, n):
-            nref = min(3, i)
-            refs = [planes[i - 1 - r].data_ptr() for r in range(nref)] + [0] * (4 - nref)
-            fr.append(A.MeMrFrame(d[i].data_ptr(), (C.c_void_p * 4)(*refs), nref, cw, ch, 32, lam, gate,
-                                  picks[i].data_ptr(), costs[i].data_ptr()))
-        per_stream.append(fr)
-        outs.append((picks, costs))
-    alone = []
-    for s, fr in enumerate(per_stream):
+        for f in range(1, n):
+            nref = min(NREF, f)
+            refs = [planes[f - 1 - r].data_ptr() for r in range(nref)] + [0] * (4 - nref)
+            fr.append(A.MeMrFrame(src[f].data_ptr(), (C.c_void_p * 4)(*refs), nref, cw, ch, PAD, lam, gate,
+                                  picks[f].data_ptr(), costs[f].data_ptr()))
         acc.me_frames_multiref(fr, params)
         acc.sync()
-        alone.append((outs[s][0].clone(), outs[s][1].clone()))
-    for o in outs:
-        o[0].zero_()
-        o[1].zero_()
-    frames_all = [f for fr in per_stream for f in fr]
-    acc.me_frames_multiref(frames_all, params)
+        alone.append((picks[1:n].clone(), costs[1:n].clone()))
+        picks.zero_()
+        costs.zero_()
+        planes.zero_()
+    nmax = max(r[4] for r in rings)
+    steps = [(k, min(G, nmax - 1 - k * G)) for k in range((nmax - 2) // G + 1)]
+    b = acc.batch_create(streams, A.BatchConfig(G, NSLOTS, NREF, 1, 0), params)
+    for k, count in steps:
+        b.step(k, count)
     acc.sync()
-    for s, o in enumerate(outs):
-        assert torch.equal(o[0], alone[s][0]) and torch.equal(o[1], alone[s][1]), f"stream {s}: 3-ref batched != alone"
+    for s, (src, planes, picks, costs, n) in enumerate(rings):
+        assert torch.equal(picks[1:n], alone[s][0]) and torch.equal(costs[1:n], alone[s][1]), \
+            f"stream {s}: batched steps != alone"
     ts = []
     for it in range(8):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        acc.me_frames_multiref(frames_all, params)
+        for k, count in steps:
+            b.step(k, count)
         e1.record()
         torch.cuda.synchronize()
         if it >= 3:
             ts.append(e0.elapsed_time(e1))
-    acc.sync()
-    return float(np.median(ts))
+    info = b.info()
+    b.close()
+    # the tuner on each resolution alone (its own signature, so it times again)
+    per_res = {}
+    for w, h, _ in MIXED:
+        sub = [st for st in streams if (st.cw, st.ch) == (w, -(-h // 16) * 16)]
+        bs = acc.batch_create(sub, A.BatchConfig(G, NSLOTS, NREF, 1, 0), params)
+        bs.step(1, G)
+        acc.sync()
+        inf = bs.info()
+        bs.close()
+        shape = A.batch_variant_shape(inf["variant"])
+        per_res[f"{w}x{h}"] = {"variant": inf["variant"], "mbs_per_cta": shape[0], "staged_window": shape[1],
+                               "ms": inf["ms"]}
+    shape = A.batch_variant_shape(info["variant"])
+    ms = float(np.median(ts))
+    px = sum((r[4] - 1) * r[0].shape[1] * r[0].shape[2] for r in rings)
+    return {"me_3ref_ms": round(ms, 3), "me_3ref_mpx_s": round(px / (ms * 1e-3) / 1e6, 1),
+            "gop_step": G, "graph_launches": len(steps), "batched_equals_alone_3ref": True,
+            "autotune": {"variant": info["variant"], "mbs_per_cta": shape[0], "staged_window": shape[1],
+                         "ms_per_variant": info["ms"], "graphs": info["graphs"], "per_resolution": per_res}}
 
 
 # Training clips of the learned proposals: the 1080p generator with seeds the

@@ -444,6 +444,64 @@ typedef struct {
 H264A_API int h264a_me_frames_multiref(h264a_ctx *ctx, const h264a_me_mr_frame *h_frames, int nframes,
                                        const h264a_me_params *params, void *stream);
 
+/* ---- batched plain-ME over many streams, one launch per GOP step ----------------- */
+/* Many streams of uneven resolution advance together, G P frames of every
+ * stream per step, where the reference encodes GOPs on parallel CPU threads
+ * with a fresh encoder each (encoder/src/lib.rs:745-805).  Step k builds the
+ * planes of frames kG..kG+count-1 of every stream (h264a_hpel_build) and then
+ * runs, in one persistent launch over all streams, h264a_me_frames_multiref
+ * of frames kG+1..kG+count (count <= G, the last step may be short), frame f
+ * against frames f-1, .., f-min(nref, f) (nearest first).  Each step runs as
+ * a CUDA graph captured the first time its slot layout occurs and replayed
+ * afterwards (one graph launch per step).  Picks and costs are those of
+ * h264a_me_frames_multiref on the same frames (8 i32 and 2 i64 per MB).
+ * Each stream owns a ring of nslots slots; frame f lives in slot f % nslots
+ * of d_src (cw*ch bytes per slot, 4-byte aligned), d_planes (4*pw*ph bytes
+ * per slot, pw = cw + 2*pad; 16-byte aligned with pw a multiple of 16 for the
+ * TMA-staged shapes), d_picks (8*nmb i32) and d_costs (2*nmb i64).  nslots is
+ * a multiple of G and at least G + nref + 1 (step k reads sources kG..kG+G
+ * and planes from kG-nref+1 on); with 2G + nref + 1 slots the sources of
+ * step k+1 can be uploaded while step k runs.  Launch shape: the autotuner
+ * (autotune = 1) times every variant on the first step, keeps the fastest for
+ * the batch's signature (resolutions, nref, G, preset; cached in the context)
+ * and captures with it; autotune = 0 uses `variant`.  Steps of one batch run
+ * one at a time in stream order (each batch has its own queue; the context's
+ * queues are untouched).  No counterpart of the graphs or the tuner in the
+ * reference. */
+#define H264A_BATCH_VARIANTS 6
+typedef struct {
+    int32_t cw, ch, pad;
+    uint8_t *d_src;
+    uint8_t *d_planes;
+    int32_t *d_picks;
+    int64_t *d_costs;
+    double lambda_me;
+    int64_t split_gate;
+} h264a_batch_stream;
+typedef struct {
+    int32_t gop_step; /* G >= 1 */
+    int32_t nslots;
+    int32_t nref;     /* 1..4 */
+    int32_t autotune;
+    int32_t variant;  /* 0..H264A_BATCH_VARIANTS-1, used when autotune = 0 */
+} h264a_batch_config;
+typedef struct {
+    int32_t variant;                      /* the launch shape the graphs use */
+    int32_t tuned;                        /* 1 when the autotuner chose it (this batch or the cache) */
+    float ms[H264A_BATCH_VARIANTS];       /* the tuner's median ME time per variant (0 if not timed) */
+    int32_t graphs;                       /* graphs captured so far */
+    int64_t steps;                        /* steps run */
+} h264a_batch_info;
+typedef struct h264a_batch h264a_batch;
+H264A_API int h264a_batch_create(h264a_ctx *ctx, const h264a_batch_stream *streams, int nstreams,
+                                 const h264a_batch_config *cfg, const h264a_me_params *params, h264a_batch **out);
+H264A_API int h264a_batch_step(h264a_batch *b, int64_t k, int count, void *stream);
+H264A_API int h264a_batch_get_info(const h264a_batch *b, h264a_batch_info *out);
+H264A_API int h264a_batch_destroy(h264a_batch *b);
+/* Variant v's shape: MBs a CTA holds at once (one warp each) and whether each
+ * search's window is staged in shared memory by TMA (1) or read from L2 (0). */
+H264A_API int h264a_batch_variant_shape(int variant, int *mbs_per_cta, int *staged);
+
 /* ---- the closed reconstruction loop ------------------------------------------ */
 /* The pixel path as the encoder runs it: every P frame searches, predicts
  * from and reconstructs against the deblocked reconstruction of the frame

@@ -134,6 +134,25 @@ class MeMrFrame(C.Structure):
                 ("d_picks", C.c_void_p), ("d_costs", C.c_void_p)]
 
 
+BATCH_VARIANTS = 6  # H264A_BATCH_VARIANTS
+
+
+class BatchStream(C.Structure):
+    _fields_ = [("cw", C.c_int32), ("ch", C.c_int32), ("pad", C.c_int32), ("d_src", C.c_void_p),
+                ("d_planes", C.c_void_p), ("d_picks", C.c_void_p), ("d_costs", C.c_void_p),
+                ("lambda_me", C.c_double), ("split_gate", C.c_int64)]
+
+
+class BatchConfig(C.Structure):
+    _fields_ = [("gop_step", C.c_int32), ("nslots", C.c_int32), ("nref", C.c_int32), ("autotune", C.c_int32),
+                ("variant", C.c_int32)]
+
+
+class BatchInfo(C.Structure):
+    _fields_ = [("variant", C.c_int32), ("tuned", C.c_int32), ("ms", C.c_float * BATCH_VARIANTS),
+                ("graphs", C.c_int32), ("steps", C.c_int64)]
+
+
 # Every entry point the header declares (checked by tests/test_capi_symbols.py).
 EXPORTS = (
     "h264a_version", "h264a_last_error", "h264a_ctx_create", "h264a_ctx_destroy", "h264a_sync",
@@ -148,6 +167,8 @@ EXPORTS = (
     "h264a_mvnet_forward", "h264a_mvnet_grads", "h264a_mvnet_train_step", "h264a_mvnet_propose",
     "h264a_me_frames_learned", "h264a_pixel_path_closed", "h264a_write_stream_cavlc", "h264a_cavlc_table_code",
     "h264a_closed_frames", "h264a_closed_step_frame", "h264a_me_frames_multiref",
+    "h264a_batch_create", "h264a_batch_step", "h264a_batch_get_info", "h264a_batch_destroy",
+    "h264a_batch_variant_shape",
 )
 
 _lib = None
@@ -197,6 +218,11 @@ def load_library() -> C.CDLL:
     L.h264a_closed_frames.argtypes = [vp, C.POINTER(ClosedDev), C.POINTER(MeParams), vp]
     L.h264a_closed_step_frame.argtypes = [vp, C.POINTER(ClosedStep), C.POINTER(MeParams), vp]
     L.h264a_me_frames_multiref.argtypes = [vp, vp, C.c_int, C.POINTER(MeParams), vp]
+    L.h264a_batch_create.argtypes = [vp, vp, i32, C.POINTER(BatchConfig), C.POINTER(MeParams), C.POINTER(vp)]
+    L.h264a_batch_step.argtypes = [vp, i64, i32, vp]
+    L.h264a_batch_get_info.argtypes = [vp, C.POINTER(BatchInfo)]
+    L.h264a_batch_destroy.argtypes = [vp]
+    L.h264a_batch_variant_shape.argtypes = [i32, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L.h264a_write_stream_cavlc.argtypes = [C.POINTER(StreamFrames), vp, sz, C.POINTER(sz), vp]
     L.h264a_cavlc_table_code.argtypes = [i32, i32, i32, i32, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L.h264a_mvnet_create.argtypes = [i32, C.c_uint64, C.POINTER(vp)]
@@ -392,6 +418,14 @@ class Accel:
         self._check(self.L.h264a_me_frames_multiref(self.ctx, C.cast(arr, C.c_void_p), len(frames), C.byref(params),
                                                     self._stream()))
 
+    def batch_create(self, streams: Sequence[BatchStream], cfg: BatchConfig, params: MeParams) -> "Batch":
+        """A batch of streams stepping G P frames per graph launch (h264a_batch_create)."""
+        arr = (BatchStream * len(streams))(*streams)
+        h = C.c_void_p()
+        self._check(self.L.h264a_batch_create(self.ctx, C.cast(arr, C.c_void_p), len(streams), C.byref(cfg),
+                                              C.byref(params), C.byref(h)))
+        return Batch(self, h)
+
     def me_frames_learned(self, frames: Sequence[MeLearnedFrame], params: MeParams):
         """me_frames with the learned proposals in each MB's 16x16 search."""
         arr = (MeLearnedFrame * len(frames))(*frames)
@@ -552,3 +586,42 @@ class Accel:
                 del self._prefetched[i]
                 break
         return out
+
+
+class Batch:
+    """A batch of streams on the device (h264a_batch_*): step(k, count)
+    enqueues step k on the current stream as one graph launch; info() reports
+    the launch shape and the tuner's timings."""
+
+    def __init__(self, acc: Accel, handle: C.c_void_p):
+        self.acc, self.h = acc, handle
+
+    def step(self, k: int, count: int):
+        self.acc._check(self.acc.L.h264a_batch_step(self.h, int(k), int(count), self.acc._stream()))
+
+    def info(self) -> dict:
+        bi = BatchInfo()
+        self.acc._check(self.acc.L.h264a_batch_get_info(self.h, C.byref(bi)))
+        return {"variant": bi.variant, "tuned": bool(bi.tuned), "ms": [round(float(x), 4) for x in bi.ms],
+                "graphs": bi.graphs, "steps": bi.steps}
+
+    def close(self):
+        if self.h:
+            self.acc.L.h264a_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def batch_variant_shape(variant: int):
+    """(MBs per CTA, staged window) of launch shape `variant` (host-only)."""
+    L = load_library()
+    n, st = C.c_int(), C.c_int()
+    rc = L.h264a_batch_variant_shape(int(variant), C.byref(n), C.byref(st))
+    if rc != H264A_OK:
+        raise AccelError(rc, L.h264a_last_error().decode())
+    return n.value, bool(st.value)

@@ -6,7 +6,9 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <map>
 #include <string>
+#include <vector>
 
 #include "../../include/h264accel.h"
 
@@ -82,6 +84,9 @@ struct h264a_ctx {
     PpInput pp_in[PP_SLOTS];
     long long pp_seq = 0;
     cudaStream_t pf_stream = nullptr;
+    // the batch runtime's autotuner: the launch shape found fastest for each
+    // batch signature (resolutions, references, frames per step, preset)
+    std::map<std::string, int> tune_cache;
 };
 
 namespace h264a {
@@ -164,6 +169,23 @@ int me_frames_run(h264a_ctx *ctx, const h264a_me_frame *h_frames, int nframes, c
 // of w*h), box bw x bh x bd, no multicast; 0 when the driver entry point is
 // missing or the layout breaks the TMA rules (the caller then copies without).
 int encode_u8_map_3d(CUtensorMap* map, const uint8_t* base, int w, int h, int d, int bw, int bh, int bd);
+struct MeParamsDev;
+// A multi-reference frame table laid out for the device: the frame
+// descriptors (largest frames first, tensor maps encoded), the queue's
+// segment starts and their frame counts.
+struct MrTable {
+    std::vector<char> bytes;
+    int nframes = 0, nseg = 0;
+    long long total = 0;  // MBs
+    size_t b_desc = 0, b_seg = 0;
+};
+// validates h_frames as h264a_me_frames_multiref does and lays out their table
+int mr_table_build(const h264a_me_mr_frame *h_frames, int nframes, MrTable &t);
+// one launch of the multi-reference kernel in launch shape `variant` over the
+// table at d_table (t's bytes in device memory), on the queue counter/flags
+// (flags of t.total MBs holding no `epoch`)
+int mr_launch(h264a_ctx *ctx, int variant, const MeParamsDev &prm, const void *d_table, const MrTable &t,
+              int32_t *counter, int32_t *flags, int epoch, cudaStream_t st);
 // the flag value of the next persistent launch on `st`
 int next_epoch(h264a_ctx *ctx, cudaStream_t st, int queue = Q_MAIN);
 

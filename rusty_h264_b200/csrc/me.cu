@@ -2881,14 +2881,18 @@ __device__ __forceinline__ int2 pick_mr_at(const int32_t* picks, int m, int bx4,
     return make_int2(__ldcg(p + 2 + 3 * part), __ldcg(p + 3 + 3 * part));
 }
 
-template <bool BAL>
-__global__ void __launch_bounds__(32 * ME_WARPS, ME_MIN_BLOCKS)
+// Launch shapes (the batch runtime's autotuner picks one): NW warps per CTA,
+// one MB each (the MBs a CTA holds at once), and STAGE: each search's window
+// staged in shared memory by TMA, or every candidate read from L2 through the
+// search's global path (no window, no shared memory, the same results).
+template <bool BAL, int NW, bool STAGE>
+__global__ void __launch_bounds__(32 * NW, 16 / NW)
     me_frames_mr_kernel(const FrameDescMR* __restrict__ fds, const long long* __restrict__ seg_start,
                         const int* __restrict__ seg_j, int nf, int ns, long long total,
                         const __grid_constant__ MeParamsDev prm, int* __restrict__ counter, int* __restrict__ flags,
                         int epoch, int* __restrict__ status, int spin_limit) {
-    __shared__ WarpScratch scratch[ME_WARPS];
-    __shared__ __align__(8) unsigned long long win_bar[ME_WARPS];
+    __shared__ WarpScratch scratch[NW];
+    __shared__ __align__(8) unsigned long long win_bar[NW];
     extern __shared__ __align__(128) uint8_t me_win[];
     const int w = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
@@ -2947,7 +2951,7 @@ __global__ void __launch_bounds__(32 * ME_WARPS, ME_MIN_BLOCKS)
             for (int r = 0; r < fd.nref; r++) {
                 const int2 pmv = predict_mv_ref(aa, a, ra, ba, bb, rb, cav, c, rc, r);
                 h264a_picture pc{fd.src, fd.planes[r], fd.cw, fd.ch, fd.pad};
-                const bool win_ok = ((reinterpret_cast<uintptr_t>(pc.d_planes) | uintptr_t(pw)) & 15) == 0 &&
+                const bool win_ok = STAGE && ((reinterpret_cast<uintptr_t>(pc.d_planes) | uintptr_t(pw)) & 15) == 0 &&
                                     pw >= WIN_W && ph >= WIN_H;
                 if (win_ok) {
                     const int wx0 = min(max((lx + pc.pad + (pmv.x >> 2) - WIN_R) & ~15, 0), pw - WIN_W);
@@ -3035,35 +3039,60 @@ __global__ void __launch_bounds__(32 * ME_WARPS, ME_MIN_BLOCKS)
     }
 }
 
-static int me_mr_setup_once() {
-    const int smem = ME_WARPS * WIN_BYTES;
-    H264A_CUDA(cudaFuncSetAttribute(me_frames_mr_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    H264A_CUDA(cudaFuncSetAttribute(me_frames_mr_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+// The launch shapes, variant 0 the default of h264a_me_frames_multiref.
+struct MrShape {
+    int nw;
+    bool stage;
+};
+constexpr MrShape kMrShapes[H264A_BATCH_VARIANTS] = {{4, true}, {2, true}, {8, true}, {4, false}, {2, false}, {8, false}};
+
+template <bool BAL, int NW, bool STAGE>
+static int mr_attr() {
+    if (STAGE)
+        H264A_CUDA(cudaFuncSetAttribute(me_frames_mr_kernel<BAL, NW, STAGE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        NW * WIN_BYTES));
     return H264A_OK;
 }
 
-extern "C" int h264a_me_frames_multiref(h264a_ctx* ctx, const h264a_me_mr_frame* h_frames, int nframes,
-                                        const h264a_me_params* params, void* stream) {
-    if (!ctx || !h_frames || !params) return fail(H264A_E_ARG, "me_frames_multiref: null pointer");
+static int me_mr_setup_once() {
+    int rc = mr_attr<false, 4, true>();
+    if (!rc) rc = mr_attr<true, 4, true>();
+    if (!rc) rc = mr_attr<true, 2, true>();
+    if (!rc) rc = mr_attr<true, 8, true>();
+    return rc;
+}
+
+template <bool BAL, int NW, bool STAGE>
+static int mr_launch_t(h264a_ctx* ctx, const MeParamsDev& prm, const char* dv, const MrTable& t, int32_t* counter,
+                       int32_t* flags, int epoch, cudaStream_t st) {
+    const size_t sm = STAGE ? size_t(NW) * WIN_BYTES : 0;
+    int per_sm = 0;
+    H264A_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, me_frames_mr_kernel<BAL, NW, STAGE>, 32 * NW, sm));
+    if (per_sm < 1) per_sm = 1;
+    long long blocks = (long long)ctx->num_sms * per_sm;
+    const long long need = (t.total + NW - 1) / NW;
+    if (blocks > need) blocks = need;
+    me_frames_mr_kernel<BAL, NW, STAGE><<<unsigned(blocks), 32 * NW, sm, st>>>(
+        reinterpret_cast<const FrameDescMR*>(dv), reinterpret_cast<const long long*>(dv + t.b_desc),
+        reinterpret_cast<const int*>(dv + t.b_desc + t.b_seg), t.nframes, t.nseg, t.total, prm, counter, flags, epoch,
+        ctx->d_status, SPIN_LIMIT);
+    return check_launch("me_frames_mr_kernel");
+}
+
+int h264a::mr_table_build(const h264a_me_mr_frame* h_frames, int nframes, MrTable& t) {
+    if (!h_frames) return fail(H264A_E_ARG, "me_frames_multiref: null pointer");
     if (nframes < 1) return fail(H264A_E_ARG, "me_frames_multiref: need at least one frame");
-    if ((params->mv_cost_kind == 1 || params->mv_cost_kind == 2) && !params->d_mv_cost_tab)
-        return fail(H264A_E_ARG, "me_frames_multiref: mv cost kinds 1 and 2 need d_mv_cost_tab");
     for (int i = 0; i < nframes; i++) {
         const h264a_me_mr_frame& f = h_frames[i];
         if (f.nref < 1 || f.nref > ME_MAXREF) return fail(H264A_E_ARG, "me_frames_multiref: 1 to 4 references per frame");
         if (!f.d_src || !f.d_picks || !f.d_costs) return fail(H264A_E_ARG, "me_frames_multiref: null frame pointer");
+        if (reinterpret_cast<uintptr_t>(f.d_src) & 3) return fail(H264A_E_ARG, "me_frames_multiref: sources must be 4-byte aligned");
         for (int r = 0; r < f.nref; r++)
             if (!f.d_planes[r]) return fail(H264A_E_ARG, "me_frames_multiref: null reference planes");
         if (f.cw < 16 || f.ch < 16 || f.cw % 16 || f.ch % 16 || f.pad < 3 || f.pad > 128)
             return fail(H264A_E_ARG, "me_frames_multiref: frames must be MB-aligned with 3 <= pad <= 128");
         if ((long long)(f.cw / 16) * (f.ch / 16) > (1 << 24)) return fail(H264A_E_ARG, "me_frames_multiref: frame too large");
     }
-    static std::once_flag once;
-    static int setup_rc = 0;
-    std::call_once(once, [] { setup_rc = me_mr_setup_once(); });
-    if (setup_rc) return setup_rc;
-    cudaStream_t st = pick_stream(ctx, stream);
-    const MeParamsDev prm = to_dev(*params);
     std::vector<int> order(nframes);
     for (int i = 0; i < nframes; i++) order[i] = i;
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
@@ -3102,42 +3131,67 @@ extern "C" int h264a_me_frames_multiref(h264a_ctx* ctx, const h264a_me_mr_frame*
     std::vector<int> segj(nframes);
     const int nseg = make_segments(segd.data(), nframes, seg.data(), segj.data());
     if (seg[nseg] != total) return fail(H264A_E_ARG, "me_frames_multiref: internal queue layout error");
-    const size_t b_desc = sizeof(FrameDescMR) * nframes, b_seg = sizeof(long long) * (nseg + 1),
-                 b_j = sizeof(int) * nseg, bytes = b_desc + b_seg + b_j;
+    t.nframes = nframes;
+    t.nseg = nseg;
+    t.total = total;
+    t.b_desc = sizeof(FrameDescMR) * nframes;
+    t.b_seg = sizeof(long long) * (nseg + 1);
+    const size_t b_j = sizeof(int) * nseg;
+    t.bytes.assign(t.b_desc + t.b_seg + b_j, 0);
+    memcpy(t.bytes.data(), desc.data(), t.b_desc);
+    memcpy(t.bytes.data() + t.b_desc, seg.data(), t.b_seg);
+    memcpy(t.bytes.data() + t.b_desc + t.b_seg, segj.data(), b_j);
+    return H264A_OK;
+}
+
+int h264a::mr_launch(h264a_ctx* ctx, int variant, const MeParamsDev& prm, const void* d_table, const MrTable& t,
+                     int32_t* counter, int32_t* flags, int epoch, cudaStream_t st) {
+    if (variant < 0 || variant >= H264A_BATCH_VARIANTS) return fail(H264A_E_ARG, "me_frames_multiref: no such launch shape");
+    static std::once_flag once;
+    static int setup_rc = 0;
+    std::call_once(once, [] { setup_rc = me_mr_setup_once(); });
+    if (setup_rc) return setup_rc;
+    const char* dv = static_cast<const char*>(d_table);
+    if (!balanced_preset(prm)) return mr_launch_t<false, 4, true>(ctx, prm, dv, t, counter, flags, epoch, st);
+    switch (variant) {
+        case 1: return mr_launch_t<true, 2, true>(ctx, prm, dv, t, counter, flags, epoch, st);
+        case 2: return mr_launch_t<true, 8, true>(ctx, prm, dv, t, counter, flags, epoch, st);
+        case 3: return mr_launch_t<true, 4, false>(ctx, prm, dv, t, counter, flags, epoch, st);
+        case 4: return mr_launch_t<true, 2, false>(ctx, prm, dv, t, counter, flags, epoch, st);
+        case 5: return mr_launch_t<true, 8, false>(ctx, prm, dv, t, counter, flags, epoch, st);
+        default: return mr_launch_t<true, 4, true>(ctx, prm, dv, t, counter, flags, epoch, st);
+    }
+}
+
+extern "C" int h264a_batch_variant_shape(int variant, int* mbs_per_cta, int* staged) {
+    if (variant < 0 || variant >= H264A_BATCH_VARIANTS) return fail(H264A_E_ARG, "batch_variant_shape: no such variant");
+    if (mbs_per_cta) *mbs_per_cta = kMrShapes[variant].nw;
+    if (staged) *staged = kMrShapes[variant].stage ? 1 : 0;
+    return H264A_OK;
+}
+
+extern "C" int h264a_me_frames_multiref(h264a_ctx* ctx, const h264a_me_mr_frame* h_frames, int nframes,
+                                        const h264a_me_params* params, void* stream) {
+    if (!ctx || !h_frames || !params) return fail(H264A_E_ARG, "me_frames_multiref: null pointer");
+    if ((params->mv_cost_kind == 1 || params->mv_cost_kind == 2) && !params->d_mv_cost_tab)
+        return fail(H264A_E_ARG, "me_frames_multiref: mv cost kinds 1 and 2 need d_mv_cost_tab");
+    MrTable t;
+    int rc = mr_table_build(h_frames, nframes, t);
+    if (rc) return rc;
+    cudaStream_t st = pick_stream(ctx, stream);
+    const MeParamsDev prm = to_dev(*params);
     char* hst = nullptr;
-    int rc = table_host(ctx, bytes, &hst);
+    rc = table_host(ctx, t.bytes.size(), &hst);
     if (rc) return rc;
-    memcpy(hst, desc.data(), b_desc);
-    memcpy(hst + b_desc, seg.data(), b_seg);
-    memcpy(hst + b_desc + b_seg, segj.data(), b_j);
-    rc = table_upload(ctx, bytes, st);
+    memcpy(hst, t.bytes.data(), t.bytes.size());
+    rc = table_upload(ctx, t.bytes.size(), st);
     if (rc) return rc;
-    rc = ensure_me_scratch(ctx, size_t(total));
+    rc = ensure_me_scratch(ctx, size_t(t.total));
     if (rc) return rc;
     H264A_CUDA(cudaMemsetAsync(ctx->q[Q_MAIN].d_counter, 0, sizeof(int32_t), st));
     const int epoch = next_epoch(ctx, st);
     if (epoch < 0) return H264A_E_CUDA;
-    int per_sm = 0;
-    H264A_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, me_frames_mr_kernel<true>, 32 * ME_WARPS,
-                                                             ME_WARPS * WIN_BYTES));
-    if (per_sm < 1) per_sm = 1;
-    long long blocks = (long long)ctx->num_sms * per_sm;
-    const long long need = (total + ME_WARPS - 1) / ME_WARPS;
-    if (blocks > need) blocks = need;
-    char* dv = static_cast<char*>(ctx->me_tab);
-    const auto* dfd = reinterpret_cast<const FrameDescMR*>(dv);
-    const auto* dseg = reinterpret_cast<const long long*>(dv + b_desc);
-    const auto* dj = reinterpret_cast<const int*>(dv + b_desc + b_seg);
-    const size_t sm = ME_WARPS * WIN_BYTES;
-    if (balanced_preset(prm))
-        me_frames_mr_kernel<true><<<unsigned(blocks), 32 * ME_WARPS, sm, st>>>(
-            dfd, dseg, dj, nframes, nseg, total, prm, ctx->q[Q_MAIN].d_counter, ctx->q[Q_MAIN].d_flags, epoch,
-            ctx->d_status, SPIN_LIMIT);
-    else
-        me_frames_mr_kernel<false><<<unsigned(blocks), 32 * ME_WARPS, sm, st>>>(
-            dfd, dseg, dj, nframes, nseg, total, prm, ctx->q[Q_MAIN].d_counter, ctx->q[Q_MAIN].d_flags, epoch,
-            ctx->d_status, SPIN_LIMIT);
-    rc = check_launch("me_frames_mr_kernel");
+    rc = mr_launch(ctx, 0, prm, ctx->me_tab, t, ctx->q[Q_MAIN].d_counter, ctx->q[Q_MAIN].d_flags, epoch, st);
     if (rc) return rc;
     return table_done(ctx, st);
 }

@@ -71,7 +71,8 @@ def test_struct_layouts_match_header(tmp_path):
                "h264a_me_learned_frame": accel.MeLearnedFrame, "h264a_closed_job": accel.ClosedJob,
                "h264a_closed_dev": accel.ClosedDev, "h264a_closed_step": accel.ClosedStep,
                "h264a_stream_frames": accel.StreamFrames, "h264a_mvnet_frame": MvnetFrame,
-               "h264a_me_mr_frame": accel.MeMrFrame}
+               "h264a_me_mr_frame": accel.MeMrFrame, "h264a_batch_stream": accel.BatchStream,
+               "h264a_batch_config": accel.BatchConfig, "h264a_batch_info": accel.BatchInfo}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "h264accel.h"', "int main(void) {"]
     for cname, py in mirrors.items():
         lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')
@@ -106,3 +107,13 @@ def test_split_gate_and_lambda_helpers():
     # mb16.rs:8885-8887 and :8642
     assert accel.split_gate_for_qp(27) == ((30 * ((14 << 4) + 160)) >> 3) * 2
     assert abs(accel.frame_lambda(12) - 0.85) < 1e-12
+
+
+def test_batch_launch_shapes(lib):
+    """The autotuner's launch shapes: 2, 4 and 8 MBs per CTA, each with the
+    window staged by TMA and read from L2; variant 0 is the default shape."""
+    shapes = [accel.batch_variant_shape(v) for v in range(accel.BATCH_VARIANTS)]
+    assert shapes[0] == (4, True)
+    assert sorted(shapes) == sorted((n, st) for n in (2, 4, 8) for st in (False, True))
+    with pytest.raises(accel.AccelError):
+        accel.batch_variant_shape(accel.BATCH_VARIANTS)
