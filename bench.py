@@ -181,7 +181,7 @@ def mixed_batch(acc, torch, streams, params, lam: float, gate: int):
     px = sum((f.shape[0] - 1) * f.shape[1] * f.shape[2] for f in streams)
     mbs = sum((f.shape[0] - 1) * (f.shape[1] // 16) * (f.shape[2] // 16) for f in streams)
     three = mixed_batch_3ref(acc, torch, bufs, params, lam, gate)
-    return {"streams": "4 x 352x288, 6 x 1280x720, 4 x 1920x1080, 2 x 3840x2160; 30 frames each, 1080p generator",
+    return bufs, {"streams": "4 x 352x288, 6 x 1280x720, 4 x 1920x1080, 2 x 3840x2160; 30 frames each, 1080p generator",
             "p_frames": len(frames_all), "macroblocks": int(mbs), "me_ms": round(ms, 3),
             "me_mpx_s": round(px / (ms * 1e-3) / 1e6, 1), "launches": 1,
             **three,
@@ -274,6 +274,64 @@ def mixed_batch_3ref(acc, torch, bufs, params, lam: float, gate: int) -> dict:
             "gop_step": G, "graph_launches": len(steps), "batched_equals_alone_3ref": True,
             "autotune": {"variant": info["variant"], "mbs_per_cta": shape[0], "staged_window": shape[1],
                          "ms_per_variant": info["ms"], "graphs": info["graphs"], "per_resolution": per_res}}
+
+
+def mixed_learned(acc, torch, bufs, net, params, lam: float, gate: int, plain_ms: float) -> dict:
+    """Learned-proposal ME over the mixed batch (one reference, the source
+    model of mixed_batch): each stream's HalfRes lookahead (the proposals'
+    guide MVs), the proposals of all 464 P frames in one h264a_mvnet_propose
+    call, then one h264a_me_frames_learned launch over all of them.  Timed
+    with CUDA events (median of 5 after 2 warm-ups), against the plain-ME
+    launch of the same frames; J of the picks against plain-ME's."""
+    from rusty_h264_b200 import accel as A
+    from rusty_h264_b200 import mvnet
+
+    T = LEARNED_FALLBACK_T
+    per, pfr, lfr = [], [], []
+    for d, planes, ppicks, pcosts in bufs:
+        n, ch, cw = d.shape
+        nmb = (cw // 16) * (ch // 16)
+        half = torch.empty((n, ch // 2, cw // 2), dtype=torch.uint8, device="cuda")
+        la = torch.zeros((3, n, nmb, 2), dtype=torch.int32, device="cuda")
+        props = torch.zeros((n, nmb, 16), dtype=torch.int32, device="cuda")
+        picks = torch.zeros((n, nmb, 6), dtype=torch.int32, device="cuda")
+        costs = torch.zeros((n, nmb, 2), dtype=torch.int64, device="cuda")
+        fb = torch.zeros((n, nmb), dtype=torch.int32, device="cuda")
+        per.append((d, half, la, props, picks, costs, fb, pcosts))
+        pfr += [mvnet.MvnetFrame(d[i].data_ptr(), d[i - 1].data_ptr(), cw, ch, la[2][i].data_ptr(),
+                                 props[i].data_ptr()) for i in range(1, n)]
+        lfr += [A.MeLearnedFrame(A.MeFrame(A.Picture(d[i].data_ptr(), planes[i - 1].data_ptr(), cw, ch, 32), lam,
+                                           gate, picks[i].data_ptr(), costs[i].data_ptr()), props[i].data_ptr(), T,
+                                 fb[i].data_ptr()) for i in range(1, n)]
+
+    def lookahead():
+        for d, half, la, *_ in per:
+            n, ch, cw = d.shape
+            acc._check(acc.L.h264a_downsample2x(acc.ctx, d.data_ptr(), cw, ch, n, cw * ch, half.data_ptr(),
+                                                acc._stream()))
+            acc._check(acc.L.h264a_lookahead_costs(acc.ctx, d.data_ptr(), half.data_ptr(), cw, ch, n, 2,
+                                                   la[0].data_ptr(), la[1].data_ptr(), la[2].data_ptr(),
+                                                   acc._stream()))
+
+    def step():
+        lookahead()
+        net.propose(pfr)
+        acc.me_frames_learned(lfr, params)
+
+    step_ms = events_ms(torch, step)
+    stage = {"lookahead": events_ms(torch, lookahead), "propose": events_ms(torch, lambda: net.propose(pfr)),
+             "learned_me": events_ms(torch, lambda: acc.me_frames_learned(lfr, params))}
+    acc.sync()
+    px = sum((p[0].shape[0] - 1) * p[0].shape[1] * p[0].shape[2] for p in per)
+    jl = sum(float(p[5][1:, :, 0].sum().item()) for p in per)
+    jp = sum(float(p[7][1:, :, 0].sum().item()) for p in per)
+    fbr = sum(float(p[6][1:].float().sum().item()) for p in per) / sum(p[6][1:].numel() for p in per)
+    return {"value": round(px / (step_ms * 1e-3) / 1e6, 1), "unit": "Mpx/s", "ms_per_step": round(step_ms, 3),
+            "stage_ms": {k: round(v, 3) for k, v in stage.items()},
+            "learned_me_mpx_s": round(px / (stage["learned_me"] * 1e-3) / 1e6, 1),
+            "plain_me_ms": round(plain_ms, 3), "fallback_t": T, "fallback_rate": round(fbr, 4),
+            "J_pick_vs_plain": round(jl / jp - 1, 5),
+            "note": "the mixed batch's 464 P frames, one reference: lookahead + proposals + learned ME per step"}
 
 
 # Training clips of the learned proposals: the 1080p generator with seeds the
@@ -1151,7 +1209,7 @@ def run_ours(args, ws, rank, local):
                                           "(7 P frames) + lookahead, one thread",
                                 "cpu": cpu_model(), "stages": cpu_stages(sample, lam, gate)}
     if args.mixed and rank == 0:
-        line["mixed_batch"] = mixed_batch(acc, torch, mixed_streams, params, lam, gate)
+        mixed_bufs, line["mixed_batch"] = mixed_batch(acc, torch, mixed_streams, params, lam, gate)
     if not args.no_learned and rank == 0:
         from rusty_h264_b200 import bdrate
 
@@ -1163,6 +1221,9 @@ def run_ours(args, ws, rank, local):
             bdrate.psnr(f[1:, :H], cb.ry.cpu().numpy()[1:, :H]), 3)
         if not args.no_closed:
             line["bd_rate"] = bd_rate_record(acc, f, U, V, params, 1.25, net, args.bd_frames)
+        if args.mixed:
+            line["mixed_batch"]["learned"] = mixed_learned(acc, torch, mixed_bufs, net, params, lam, gate,
+                                                           line["mixed_batch"]["me_ms"])
         net.close()
     if rank == 0:
         print(json.dumps(line), flush=True)
