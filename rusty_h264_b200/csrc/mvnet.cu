@@ -28,6 +28,7 @@
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "h264a_device.cuh"
@@ -63,6 +64,15 @@ __device__ __forceinline__ bf16_t f2bf(float f) {  // round to nearest even
 __device__ __forceinline__ float bf2f(bf16_t b) { return __uint_as_float(uint32_t(b) << 16); }
 __device__ __forceinline__ uint32_t pack2(bf16_t lo, bf16_t hi) { return uint32_t(lo) | (uint32_t(hi) << 16); }
 __device__ __forceinline__ uint32_t ld_pair(const bf16_t* p) { return *reinterpret_cast<const uint32_t*>(p); }
+__device__ __forceinline__ uint4 ld8(const bf16_t* p) { return *reinterpret_cast<const uint4*>(p); }
+// 8 values (bias added, ReLU) rounded to bf16 and stored as one 16-byte word
+__device__ __forceinline__ void st8_relu(bf16_t* dst, const float* v, const bf16_t* bias) {
+    uint32_t w[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+        w[i] = pack2(f2bf(fmaxf(v[2 * i] + bf2f(bias[2 * i]), 0.f)), f2bf(fmaxf(v[2 * i + 1] + bf2f(bias[2 * i + 1]), 0.f)));
+    *reinterpret_cast<uint4*>(dst) = make_uint4(w[0], w[1], w[2], w[3]);
+}
 
 // ---- a batch: frame pairs of one geometry, every MB a sample ---------------
 // Trunk maps (NHWC bf16): A1 (ch/2)x(cw/2)x16, A2 (ch/4)x(cw/4)x32, A3
@@ -149,6 +159,15 @@ __device__ __forceinline__ void tc_wait(uint32_t bar, uint32_t parity, int* stat
     }
 }
 
+// An Op with `static constexpr bool kVec = true` also gathers 8 consecutive
+// k at once (op.a8(m, k), op.b8(k, n): 16 bytes, k a multiple of 8, zero past
+// its tensor) and stores 8 consecutive n (op.store8(m, n, v)); the GEMM then
+// moves each 16-byte chunk of a stage with one load (K and N multiples of 8).
+template <class Op, class = void>
+struct VecOp : std::false_type {};
+template <class Op>
+struct VecOp<Op, std::void_t<decltype(Op::kVec)>> : std::bool_constant<Op::kVec> {};
+
 template <int BN, class Op>
 __global__ void __launch_bounds__(TC_THREADS) gemm_tc_kernel(const Op op, int M, int N, int K, int kchunk, int* status) {
     static_assert(BN % 16 == 0 && BN >= 16 && BN <= 256, "tcgen05 N for M = 128");
@@ -188,8 +207,13 @@ __global__ void __launch_bounds__(TC_THREADS) gemm_tc_kernel(const Op op, int M,
         for (int q = tid; q < TC_BM * 8; q += TC_THREADS) {
             const int row = ((q >> 6) << 3) | (q & 7), c = (q >> 3) & 7, m = m0 + row, k = k0 + 8 * c;
             uint32_t v[4];
+            if constexpr (VecOp<Op>::value) {
+                const uint4 w = (m < M && k < ke) ? op.a8(m, k) : make_uint4(0u, 0u, 0u, 0u);
+                v[0] = w.x; v[1] = w.y; v[2] = w.z; v[3] = w.w;
+            } else {
 #pragma unroll
-            for (int i = 0; i < 4; i++) v[i] = (m < M && k + 2 * i < ke) ? op.a(m, k + 2 * i) : 0u;
+                for (int i = 0; i < 4; i++) v[i] = (m < M && k + 2 * i < ke) ? op.a(m, k + 2 * i) : 0u;
+            }
             asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(sa + tc_off(row, c)), "r"(v[0]), "r"(v[1]),
                          "r"(v[2]), "r"(v[3])
                          : "memory");
@@ -197,8 +221,13 @@ __global__ void __launch_bounds__(TC_THREADS) gemm_tc_kernel(const Op op, int M,
         for (int q = tid; q < BN * 8; q += TC_THREADS) {
             const int row = ((q >> 6) << 3) | (q & 7), c = (q >> 3) & 7, n = n0 + row, k = k0 + 8 * c;
             uint32_t v[4];
+            if constexpr (VecOp<Op>::value) {
+                const uint4 w = (n < N && k < ke) ? op.b8(k, n) : make_uint4(0u, 0u, 0u, 0u);
+                v[0] = w.x; v[1] = w.y; v[2] = w.z; v[3] = w.w;
+            } else {
 #pragma unroll
-            for (int i = 0; i < 4; i++) v[i] = (n < N && k + 2 * i < ke) ? op.b(k + 2 * i, n) : 0u;
+                for (int i = 0; i < 4; i++) v[i] = (n < N && k + 2 * i < ke) ? op.b(k + 2 * i, n) : 0u;
+            }
             asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(sb + tc_off(row, c)), "r"(v[0]), "r"(v[1]),
                          "r"(v[2]), "r"(v[3])
                          : "memory");
@@ -238,7 +267,14 @@ __global__ void __launch_bounds__(TC_THREADS) gemm_tc_kernel(const Op op, int M,
                            "=r"(r[7])
                          : "r"(taddr + uint32_t(c0)));
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            if (row < M) {
+            if constexpr (VecOp<Op>::value) {
+                if (row < M && n0 + c0 < N) {
+                    float f[8];
+#pragma unroll
+                    for (int i = 0; i < 8; i++) f[i] = __uint_as_float(r[i]);
+                    op.store8(row, n0 + c0, f);
+                }
+            } else if (row < M) {
 #pragma unroll
                 for (int i = 0; i < 8; i++) {
                     const int n = n0 + c0 + i;
@@ -286,6 +322,25 @@ struct Conv1Fwd {
     __device__ void store(int m, int n, float v) const {
         z.a1[(long long)m * 16 + n] = f2bf(fmaxf(v + bf2f(z.w[O_B1 + n]), 0.f));
     }
+    static constexpr bool kVec = true;
+    __device__ uint4 a8(int m, int k) const {
+        const int OHW = g.H1 * g.W1;
+        const int b = m / OHW, r = m - b * OHW, oy = r / g.W1, ox = r - oy * g.W1;
+        uint32_t v[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const int tap = (k >> 1) + i, ky = tap / 3, kx = tap - ky * 3;
+            v[i] = tap < 9 ? x0_pair(g, b, 2 * oy + ky - 1, 2 * ox + kx - 1) : 0u;
+        }
+        return make_uint4(v[0], v[1], v[2], v[3]);
+    }
+    __device__ uint4 b8(int k, int n) const {
+        uint32_t v[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++) v[i] = b(k + 2 * i, n);
+        return make_uint4(v[0], v[1], v[2], v[3]);
+    }
+    __device__ void store8(int m, int n, const float* v) const { st8_relu(z.a1 + (long long)m * 16 + n, v, z.w + O_B1 + n); }
 };
 // conv2 / conv3 forward: im2col of the previous map
 template <int C, int OW, int OB, int WHICH>
@@ -298,6 +353,17 @@ struct ConvFwd {
     __device__ uint32_t b(int k, int n) const { return ld_pair(z.w + OW + n * 9 * C + k); }
     __device__ void store(int m, int n, float v) const {
         (WHICH == 2 ? z.a2 : z.a3)[(long long)m * 32 + n] = f2bf(fmaxf(v + bf2f(z.w[OB + n]), 0.f));
+    }
+    // k a multiple of 8 (C = 16 or 32): the chunk is 8 channels of one tap,
+    // 16 contiguous bytes of the NHWC map
+    static constexpr bool kVec = true;
+    __device__ uint4 a8(int m, int k) const {
+        const long long o = WHICH == 2 ? im2col_off<C>(g.H1, g.W1, m, k) : im2col_off<C>(g.H2, g.W2, m, k);
+        return o < 0 ? make_uint4(0u, 0u, 0u, 0u) : ld8((WHICH == 2 ? z.a1 : z.a2) + o);
+    }
+    __device__ uint4 b8(int k, int n) const { return ld8(z.w + OW + n * 9 * C + k); }
+    __device__ void store8(int m, int n, const float* v) const {
+        st8_relu((WHICH == 2 ? z.a2 : z.a3) + (long long)m * 32 + n, v, z.w + OB + n);
     }
 };
 using Conv2Fwd = ConvFwd<16, O_W2, O_B2, 2>;
@@ -336,12 +402,36 @@ struct Fc1Fwd {
     __device__ void store(int m, int n, float v) const {
         z.h[(long long)m * HID + n] = f2bf(fmaxf(v + bf2f(z.w[O_B4 + n]), 0.f));
     }
+    // k < 1152, a multiple of 8: 8 channels of one crop cell, 16 contiguous
+    // bytes of A3; then the 6 neighbour-MV features and zeros
+    static constexpr bool kVec = true;
+    __device__ uint4 a8(int m, int k) const {
+        if (k < CONVF) {
+            const long long o = crop_off(g, m, k);
+            return o < 0 ? make_uint4(0u, 0u, 0u, 0u) : ld8(z.a3 + o);
+        }
+        if (k == CONVF)
+            return make_uint4(pack2(mv_feat(g, m, 0), mv_feat(g, m, 1)), pack2(mv_feat(g, m, 2), mv_feat(g, m, 3)),
+                              pack2(mv_feat(g, m, 4), mv_feat(g, m, 5)), 0u);
+        return make_uint4(0u, 0u, 0u, 0u);
+    }
+    __device__ uint4 b8(int k, int n) const { return ld8(z.w + O_W4 + (long long)n * FEAT + k); }
+    __device__ void store8(int m, int n, const float* v) const { st8_relu(z.h + (long long)m * HID + n, v, z.w + O_B4 + n); }
 };
 struct HeadFwd {
     Bufs z;
     __device__ uint32_t a(int m, int k) const { return ld_pair(z.h + (long long)m * HID + k); }
     __device__ uint32_t b(int k, int n) const { return ld_pair(z.w + O_W5 + n * HID + k); }
     __device__ void store(int m, int n, float v) const { z.logits[(long long)m * HEAD_N + n] = v + bf2f(z.w[O_B5 + n]); }
+    static constexpr bool kVec = true;
+    __device__ uint4 a8(int m, int k) const { return ld8(z.h + (long long)m * HID + k); }
+    __device__ uint4 b8(int k, int n) const { return ld8(z.w + O_W5 + n * HID + k); }
+    __device__ void store8(int m, int n, const float* v) const {
+        float4* d = reinterpret_cast<float4*>(z.logits + (long long)m * HEAD_N + n);
+        const bf16_t* bias = z.w + O_B5 + n;
+        d[0] = make_float4(v[0] + bf2f(bias[0]), v[1] + bf2f(bias[1]), v[2] + bf2f(bias[2]), v[3] + bf2f(bias[3]));
+        d[1] = make_float4(v[4] + bf2f(bias[4]), v[5] + bf2f(bias[5]), v[6] + bf2f(bias[6]), v[7] + bf2f(bias[7]));
+    }
 };
 
 // ---- backward -----------------------------------------------------------------
