@@ -163,10 +163,17 @@ __device__ __forceinline__ void tc_wait(uint32_t bar, uint32_t parity, int* stat
 // k at once (op.a8(m, k), op.b8(k, n): 16 bytes, k a multiple of 8, zero past
 // its tensor) and stores 8 consecutive n (op.store8(m, n, v)); the GEMM then
 // moves each 16-byte chunk of a stage with one load (K and N multiples of 8).
+// Such an Op also names a `Row` (what its gathers need of output row m:
+// sample, position, base offset) made once per CTA row by op.row(m), so the
+// per-chunk gather op.a8(row, k) does no division by a runtime size.
 template <class Op, class = void>
-struct VecOp : std::false_type {};
+struct VecOp : std::false_type {
+    using Row = int;
+};
 template <class Op>
-struct VecOp<Op, std::void_t<decltype(Op::kVec)>> : std::bool_constant<Op::kVec> {};
+struct VecOp<Op, std::void_t<decltype(Op::kVec)>> : std::bool_constant<Op::kVec> {
+    using Row = typename Op::Row;
+};
 
 template <int BN, class Op>
 __global__ void __launch_bounds__(TC_THREADS) gemm_tc_kernel(const Op op, int M, int N, int K, int kchunk, int* status) {
@@ -177,8 +184,12 @@ __global__ void __launch_bounds__(TC_THREADS) gemm_tc_kernel(const Op op, int M,
     extern __shared__ __align__(128) uint8_t tc_smem[];
     __shared__ __align__(8) unsigned long long tc_bar[2];
     __shared__ uint32_t tc_tmem;
+    __shared__ typename VecOp<Op>::Row tc_rows[VecOp<Op>::value ? TC_BM : 1];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int m0 = blockIdx.x * TC_BM, n0 = blockIdx.y * BN;
+    if constexpr (VecOp<Op>::value) {
+        for (int i = tid; i < TC_BM; i += TC_THREADS) tc_rows[i] = op.row(min(m0 + i, M - 1));
+    }  // read after the __syncthreads below
     const int kb = blockIdx.z * kchunk, ke = min(K, kb + kchunk);
     const uint32_t sbase = tc_smem_u32(tc_smem), bar0 = tc_smem_u32(&tc_bar[0]);
     if (warp == 0) {
@@ -198,39 +209,65 @@ __global__ void __launch_bounds__(TC_THREADS) gemm_tc_kernel(const Op op, int M,
     const int nk = ke > kb ? (ke - kb + TC_BK - 1) / TC_BK : 0;
     for (int it = 0; it < nk; it++) {
         const int st = it & 1;
-        // the stage's previous MMAs (step it - 2) have read it
-        if (it >= 2) tc_wait(bar0 + 8 * st, uint32_t((it - 2) >> 1) & 1u, status);
         const int k0 = kb + it * TC_BK;
         const uint32_t sa = sbase + uint32_t(st * STAGE), sb = sa + A_BYTES;
         // consecutive threads fill consecutive 16-byte rows of a core
         // matrix, so a warp's stores meet no bank twice
-        for (int q = tid; q < TC_BM * 8; q += TC_THREADS) {
-            const int row = ((q >> 6) << 3) | (q & 7), c = (q >> 3) & 7, m = m0 + row, k = k0 + 8 * c;
-            uint32_t v[4];
-            if constexpr (VecOp<Op>::value) {
-                const uint4 w = (m < M && k < ke) ? op.a8(m, k) : make_uint4(0u, 0u, 0u, 0u);
-                v[0] = w.x; v[1] = w.y; v[2] = w.z; v[3] = w.w;
-            } else {
+        if constexpr (VecOp<Op>::value) {
+            // the step's gathers are issued before waiting for the stage, so
+            // they overlap the MMAs still reading it
+            constexpr int AQ = TC_BM * 8 / TC_THREADS, BQ = (BN * 8 + TC_THREADS - 1) / TC_THREADS;
+            uint4 va[AQ], vb[BQ];
+#pragma unroll
+            for (int j = 0; j < AQ; j++) {
+                const int q = tid + j * TC_THREADS;
+                const int row = ((q >> 6) << 3) | (q & 7), c = (q >> 3) & 7, m = m0 + row, k = k0 + 8 * c;
+                va[j] = (m < M && k < ke) ? op.a8(tc_rows[row], k) : make_uint4(0u, 0u, 0u, 0u);
+            }
+#pragma unroll
+            for (int j = 0; j < BQ; j++) {
+                const int q = tid + j * TC_THREADS;
+                const int row = ((q >> 6) << 3) | (q & 7), c = (q >> 3) & 7, n = n0 + row, k = k0 + 8 * c;
+                vb[j] = (q < BN * 8 && n < N && k < ke) ? op.b8(k, n) : make_uint4(0u, 0u, 0u, 0u);
+            }
+            // the stage's previous MMAs (step it - 2) have read it
+            if (it >= 2) tc_wait(bar0 + 8 * st, uint32_t((it - 2) >> 1) & 1u, status);
+#pragma unroll
+            for (int j = 0; j < AQ; j++) {
+                const int q = tid + j * TC_THREADS, row = ((q >> 6) << 3) | (q & 7), c = (q >> 3) & 7;
+                asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(sa + tc_off(row, c)), "r"(va[j].x),
+                             "r"(va[j].y), "r"(va[j].z), "r"(va[j].w)
+                             : "memory");
+            }
+#pragma unroll
+            for (int j = 0; j < BQ; j++) {
+                const int q = tid + j * TC_THREADS, row = ((q >> 6) << 3) | (q & 7), c = (q >> 3) & 7;
+                if (q < BN * 8)
+                    asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(sb + tc_off(row, c)), "r"(vb[j].x),
+                                 "r"(vb[j].y), "r"(vb[j].z), "r"(vb[j].w)
+                                 : "memory");
+            }
+        } else {
+            // the stage's previous MMAs (step it - 2) have read it
+            if (it >= 2) tc_wait(bar0 + 8 * st, uint32_t((it - 2) >> 1) & 1u, status);
+            for (int q = tid; q < TC_BM * 8; q += TC_THREADS) {
+                const int row = ((q >> 6) << 3) | (q & 7), c = (q >> 3) & 7, m = m0 + row, k = k0 + 8 * c;
+                uint32_t v[4];
 #pragma unroll
                 for (int i = 0; i < 4; i++) v[i] = (m < M && k + 2 * i < ke) ? op.a(m, k + 2 * i) : 0u;
+                asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(sa + tc_off(row, c)), "r"(v[0]),
+                             "r"(v[1]), "r"(v[2]), "r"(v[3])
+                             : "memory");
             }
-            asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(sa + tc_off(row, c)), "r"(v[0]), "r"(v[1]),
-                         "r"(v[2]), "r"(v[3])
-                         : "memory");
-        }
-        for (int q = tid; q < BN * 8; q += TC_THREADS) {
-            const int row = ((q >> 6) << 3) | (q & 7), c = (q >> 3) & 7, n = n0 + row, k = k0 + 8 * c;
-            uint32_t v[4];
-            if constexpr (VecOp<Op>::value) {
-                const uint4 w = (n < N && k < ke) ? op.b8(k, n) : make_uint4(0u, 0u, 0u, 0u);
-                v[0] = w.x; v[1] = w.y; v[2] = w.z; v[3] = w.w;
-            } else {
+            for (int q = tid; q < BN * 8; q += TC_THREADS) {
+                const int row = ((q >> 6) << 3) | (q & 7), c = (q >> 3) & 7, n = n0 + row, k = k0 + 8 * c;
+                uint32_t v[4];
 #pragma unroll
                 for (int i = 0; i < 4; i++) v[i] = (n < N && k + 2 * i < ke) ? op.b(k + 2 * i, n) : 0u;
+                asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(sb + tc_off(row, c)), "r"(v[0]),
+                             "r"(v[1]), "r"(v[2]), "r"(v[3])
+                             : "memory");
             }
-            asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(sb + tc_off(row, c)), "r"(v[0]), "r"(v[1]),
-                         "r"(v[2]), "r"(v[3])
-                         : "memory");
         }
         // the tiles' generic-proxy writes, visible to the tensor cores
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -323,14 +360,20 @@ struct Conv1Fwd {
         z.a1[(long long)m * 16 + n] = f2bf(fmaxf(v + bf2f(z.w[O_B1 + n]), 0.f));
     }
     static constexpr bool kVec = true;
-    __device__ uint4 a8(int m, int k) const {
+    struct Row {
+        int b, y0, x0;  // pair, top-left input pixel of the 3x3 window
+    };
+    __device__ Row row(int m) const {
         const int OHW = g.H1 * g.W1;
         const int b = m / OHW, r = m - b * OHW, oy = r / g.W1, ox = r - oy * g.W1;
+        return Row{b, 2 * oy - 1, 2 * ox - 1};
+    }
+    __device__ uint4 a8(const Row& w, int k) const {
         uint32_t v[4];
 #pragma unroll
         for (int i = 0; i < 4; i++) {
-            const int tap = (k >> 1) + i, ky = tap / 3, kx = tap - ky * 3;
-            v[i] = tap < 9 ? x0_pair(g, b, 2 * oy + ky - 1, 2 * ox + kx - 1) : 0u;
+            const int tap = (k >> 1) + i, ky = (tap * 11) >> 5, kx = tap - ky * 3;  // ky = tap / 3 for tap < 9
+            v[i] = tap < 9 ? x0_pair(g, w.b, w.y0 + ky, w.x0 + kx) : 0u;
         }
         return make_uint4(v[0], v[1], v[2], v[3]);
     }
@@ -357,9 +400,22 @@ struct ConvFwd {
     // k a multiple of 8 (C = 16 or 32): the chunk is 8 channels of one tap,
     // 16 contiguous bytes of the NHWC map
     static constexpr bool kVec = true;
-    __device__ uint4 a8(int m, int k) const {
-        const long long o = WHICH == 2 ? im2col_off<C>(g.H1, g.W1, m, k) : im2col_off<C>(g.H2, g.W2, m, k);
-        return o < 0 ? make_uint4(0u, 0u, 0u, 0u) : ld8((WHICH == 2 ? z.a1 : z.a2) + o);
+    struct Row {
+        long long base;  // element offset of input pixel (y0, x0), channel 0 (may lie outside the map)
+        int y0, x0;
+    };
+    __device__ Row row(int m) const {
+        const int H = WHICH == 2 ? g.H1 : g.H2, W = WHICH == 2 ? g.W1 : g.W2;
+        const int ow = W >> 1, ohw = (H >> 1) * ow;
+        const int b = m / ohw, r = m - b * ohw, oy = r / ow, ox = r - oy * ow;
+        return Row{((long long)(b * H + 2 * oy - 1) * W + 2 * ox - 1) * C, 2 * oy - 1, 2 * ox - 1};
+    }
+    __device__ uint4 a8(const Row& w, int k) const {
+        const int H = WHICH == 2 ? g.H1 : g.H2, W = WHICH == 2 ? g.W1 : g.W2;
+        const int tap = k / C, ci = k - tap * C, ky = (tap * 11) >> 5, kx = tap - ky * 3;
+        const int iy = w.y0 + ky, ix = w.x0 + kx;
+        if (iy < 0 || iy >= H || ix < 0 || ix >= W) return make_uint4(0u, 0u, 0u, 0u);
+        return ld8((WHICH == 2 ? z.a1 : z.a2) + w.base + (long long)(ky * W + kx) * C + ci);
     }
     __device__ uint4 b8(int k, int n) const { return ld8(z.w + OW + n * 9 * C + k); }
     __device__ void store8(int m, int n, const float* v) const {
@@ -405,14 +461,25 @@ struct Fc1Fwd {
     // k < 1152, a multiple of 8: 8 channels of one crop cell, 16 contiguous
     // bytes of A3; then the 6 neighbour-MV features and zeros
     static constexpr bool kVec = true;
-    __device__ uint4 a8(int m, int k) const {
+    struct Row {
+        long long base;  // element offset of the crop's top-left cell (y0, x0), channel 0
+        int m, y0, x0;
+    };
+    __device__ Row row(int m) const {
+        const int b = m / g.nmb, r = m - b * g.nmb, mby = r / g.mb_w, mbx = r - mby * g.mb_w;
+        const int y0 = 2 * mby - 2, x0 = 2 * mbx - 2;
+        return Row{((long long)(b * g.H3 + y0) * g.W3 + x0) * 32, m, y0, x0};
+    }
+    __device__ uint4 a8(const Row& w, int k) const {
         if (k < CONVF) {
-            const long long o = crop_off(g, m, k);
-            return o < 0 ? make_uint4(0u, 0u, 0u, 0u) : ld8(z.a3 + o);
+            const int cy = k / 192, rem = k - cy * 192, cx = rem >> 5, c = rem & 31;
+            const int y = w.y0 + cy, x = w.x0 + cx;
+            if (y < 0 || y >= g.H3 || x < 0 || x >= g.W3) return make_uint4(0u, 0u, 0u, 0u);
+            return ld8(z.a3 + w.base + (long long)(cy * g.W3 + cx) * 32 + c);
         }
         if (k == CONVF)
-            return make_uint4(pack2(mv_feat(g, m, 0), mv_feat(g, m, 1)), pack2(mv_feat(g, m, 2), mv_feat(g, m, 3)),
-                              pack2(mv_feat(g, m, 4), mv_feat(g, m, 5)), 0u);
+            return make_uint4(pack2(mv_feat(g, w.m, 0), mv_feat(g, w.m, 1)), pack2(mv_feat(g, w.m, 2), mv_feat(g, w.m, 3)),
+                              pack2(mv_feat(g, w.m, 4), mv_feat(g, w.m, 5)), 0u);
         return make_uint4(0u, 0u, 0u, 0u);
     }
     __device__ uint4 b8(int k, int n) const { return ld8(z.w + O_W4 + (long long)n * FEAT + k); }
@@ -424,7 +491,9 @@ struct HeadFwd {
     __device__ uint32_t b(int k, int n) const { return ld_pair(z.w + O_W5 + n * HID + k); }
     __device__ void store(int m, int n, float v) const { z.logits[(long long)m * HEAD_N + n] = v + bf2f(z.w[O_B5 + n]); }
     static constexpr bool kVec = true;
-    __device__ uint4 a8(int m, int k) const { return ld8(z.h + (long long)m * HID + k); }
+    using Row = int;
+    __device__ Row row(int m) const { return m; }
+    __device__ uint4 a8(Row m, int k) const { return ld8(z.h + (long long)m * HID + k); }
     __device__ uint4 b8(int k, int n) const { return ld8(z.w + O_W5 + n * HID + k); }
     __device__ void store8(int m, int n, const float* v) const {
         float4* d = reinterpret_cast<float4*>(z.logits + (long long)m * HEAD_N + n);
