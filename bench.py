@@ -64,6 +64,8 @@ def parse():
     ap.add_argument("--learned-epochs", type=float, default=6.0)
     ap.add_argument("--no-closed", action="store_true", help="skip the closed-loop and BD-rate records")
     ap.add_argument("--bd-frames", type=int, default=16)
+    ap.add_argument("--bd-4k", action="store_true",
+                    help="also the BD-rate record on a 3840x2160 clip of the same generator (seed 2)")
     return ap.parse_args()
 
 
@@ -278,8 +280,8 @@ def mixed_batch_3ref(acc, torch, bufs, params, lam: float, gate: int) -> dict:
 
 def mixed_learned(acc, torch, bufs, net, params, lam: float, gate: int, plain_ms: float) -> dict:
     """Learned-proposal ME over the mixed batch (one reference, the source
-    model of mixed_batch): each stream's HalfRes lookahead (the proposals'
-    guide MVs), the proposals of all 464 P frames in one h264a_mvnet_propose
+    model of mixed_batch): the HalfRes lookahead of all 16 streams in one
+    h264a_lookahead_streams launch (the proposals' guide MVs), the proposals of all 464 P frames in one h264a_mvnet_propose
     call, then one h264a_me_frames_learned launch over all of them.  Timed
     with CUDA events (median of 5 after 2 warm-ups), against the plain-ME
     launch of the same frames; J of the picks against plain-ME's."""
@@ -304,14 +306,15 @@ def mixed_learned(acc, torch, bufs, net, params, lam: float, gate: int, plain_ms
                                            gate, picks[i].data_ptr(), costs[i].data_ptr()), props[i].data_ptr(), T,
                                  fb[i].data_ptr()) for i in range(1, n)]
 
-    def lookahead():
+    las = [A.LaStream(d.data_ptr(), half.data_ptr(), d.shape[2], d.shape[1], d.shape[0], la[0].data_ptr(),
+                      la[1].data_ptr(), la[2].data_ptr()) for d, half, la, *_ in per]
+
+    def lookahead():  # each stream's half-res frames, then all 16 lookaheads in one launch
         for d, half, la, *_ in per:
             n, ch, cw = d.shape
             acc._check(acc.L.h264a_downsample2x(acc.ctx, d.data_ptr(), cw, ch, n, cw * ch, half.data_ptr(),
                                                 acc._stream()))
-            acc._check(acc.L.h264a_lookahead_costs(acc.ctx, d.data_ptr(), half.data_ptr(), cw, ch, n, 2,
-                                                   la[0].data_ptr(), la[1].data_ptr(), la[2].data_ptr(),
-                                                   acc._stream()))
+        acc.lookahead_streams(las, 2)
 
     def step():
         lookahead()
@@ -475,7 +478,7 @@ def learned_arm(acc, torch, f, U, V, d_frames, planes, params, lam, gate, qp, pl
     return out, net, rec_y
 
 
-def bd_rate_record(acc, f, U, V, params, lam_scale, net, bd_frames):
+def bd_rate_record(acc, f, U, V, params, lam_scale, net, bd_frames, width=W, height=H):
     """BD-rate of the learned search against plain-ME through the closed loop
     at QP 22/27/32/37 on the clip's first bd_frames frames: rate = the
     Annex-B bytes of the P frames (h264a_write_stream_cavlc), PSNR = luma of
@@ -491,10 +494,11 @@ def bd_rate_record(acc, f, U, V, params, lam_scale, net, bd_frames):
         gq = A.split_gate_for_qp(q)
         for name, nt in (("plain", None), ("learned", net)):
             r = acc.pixel_path_closed(f[:m], U[:m], V[:m], params, lq, gq, q, net=nt, fallback_t=LEARNED_FALLBACK_T)
-            data, fbytes = A.write_stream_cavlc(f[0], U[0], V[0], r["picks"], r["coeffs"], r["ccoeffs"], q, W, H)
-            curves[name].append((float(fbytes[1:].sum()), bdrate.psnr(f[1:m, :H], r["rec_y"][1:m, :H])))
+            data, fbytes = A.write_stream_cavlc(f[0], U[0], V[0], r["picks"], r["coeffs"], r["ccoeffs"], q, width,
+                                                height)
+            curves[name].append((float(fbytes[1:].sum()), bdrate.psnr(f[1:m, :height], r["rec_y"][1:m, :height])))
     return {
-        "qps": list(BD_QPS), "frames": m,
+        "size": f"{width}x{height}", "qps": list(BD_QPS), "frames": m,
         "plain": [(round(r), round(d, 3)) for r, d in curves["plain"]],
         "learned": [(round(r), round(d, 3)) for r, d in curves["learned"]],
         "bd_rate_pct_learned_vs_plain": round(bdrate.bd_rate(curves["plain"], curves["learned"]), 3),
@@ -1221,6 +1225,11 @@ def run_ours(args, ws, rank, local):
             bdrate.psnr(f[1:, :H], cb.ry.cpu().numpy()[1:, :H]), 3)
         if not args.no_closed:
             line["bd_rate"] = bd_rate_record(acc, f, U, V, params, 1.25, net, args.bd_frames)
+            if args.bd_4k:
+                y4, u4, v4 = synth.hd_clip(args.bd_frames, 2, 3840, 2160, with_chroma=True)
+                line["bd_rate_4k"] = bd_rate_record(acc, synth.coded_luma(y4), synth.coded_chroma(u4),
+                                                    synth.coded_chroma(v4), params, 1.25, net, args.bd_frames,
+                                                    3840, 2160)
         if args.mixed:
             line["mixed_batch"]["learned"] = mixed_learned(acc, torch, mixed_bufs, net, params, lam, gate,
                                                            line["mixed_batch"]["me_ms"])

@@ -310,6 +310,18 @@ H264A_API int h264a_downsample2x(h264a_ctx *ctx, const uint8_t *d_frames, int cw
  * inter (i32) and the full-res quarter-pel MV (2 i32). */
 H264A_API int h264a_lookahead_costs(h264a_ctx *ctx, const uint8_t *d_full, const uint8_t *d_half, int cw, int ch, int n,
                           int mode, int32_t *d_intra, int32_t *d_inter, int32_t *d_mvs, void *stream);
+/* h264a_lookahead_costs of several streams (each its own clip of n
+ * consecutive frames, any size) in one persistent launch of the chains (up
+ * to 24 streams per launch), the per-GOP lookahead that encode_all runs for
+ * each GOP (encoder/src/lib.rs:764-770, mbtree::gop_qp_offsets): outputs per
+ * stream exactly as h264a_lookahead_costs gives them. */
+typedef struct {
+    const uint8_t *d_full, *d_half;
+    int32_t cw, ch, n;
+    int32_t *d_intra, *d_inter, *d_mvs;
+} h264a_la_stream;
+H264A_API int h264a_lookahead_streams(h264a_ctx *ctx, const h264a_la_stream *streams, int nstreams, int mode,
+                                      void *stream);
 
 /* ---- the whole pixel path from host memory -------------------------------- */
 /* Copies n coded luma frames (cw x ch, contiguous) to the device, builds the

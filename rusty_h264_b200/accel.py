@@ -134,6 +134,11 @@ class MeMrFrame(C.Structure):
                 ("d_picks", C.c_void_p), ("d_costs", C.c_void_p)]
 
 
+class LaStream(C.Structure):
+    _fields_ = [("d_full", C.c_void_p), ("d_half", C.c_void_p), ("cw", C.c_int32), ("ch", C.c_int32),
+                ("n", C.c_int32), ("d_intra", C.c_void_p), ("d_inter", C.c_void_p), ("d_mvs", C.c_void_p)]
+
+
 BATCH_VARIANTS = 6  # H264A_BATCH_VARIANTS
 
 
@@ -168,7 +173,7 @@ EXPORTS = (
     "h264a_me_frames_learned", "h264a_pixel_path_closed", "h264a_write_stream_cavlc", "h264a_cavlc_table_code",
     "h264a_closed_frames", "h264a_closed_step_frame", "h264a_me_frames_multiref",
     "h264a_batch_create", "h264a_batch_step", "h264a_batch_get_info", "h264a_batch_destroy",
-    "h264a_batch_variant_shape",
+    "h264a_batch_variant_shape", "h264a_lookahead_streams",
 )
 
 _lib = None
@@ -218,6 +223,7 @@ def load_library() -> C.CDLL:
     L.h264a_closed_frames.argtypes = [vp, C.POINTER(ClosedDev), C.POINTER(MeParams), vp]
     L.h264a_closed_step_frame.argtypes = [vp, C.POINTER(ClosedStep), C.POINTER(MeParams), vp]
     L.h264a_me_frames_multiref.argtypes = [vp, vp, C.c_int, C.POINTER(MeParams), vp]
+    L.h264a_lookahead_streams.argtypes = [vp, vp, i32, i32, vp]
     L.h264a_batch_create.argtypes = [vp, vp, i32, C.POINTER(BatchConfig), C.POINTER(MeParams), C.POINTER(vp)]
     L.h264a_batch_step.argtypes = [vp, i64, i32, vp]
     L.h264a_batch_get_info.argtypes = [vp, C.POINTER(BatchInfo)]
@@ -417,6 +423,12 @@ class Accel:
         arr = (MeMrFrame * len(frames))(*frames)
         self._check(self.L.h264a_me_frames_multiref(self.ctx, C.cast(arr, C.c_void_p), len(frames), C.byref(params),
                                                     self._stream()))
+
+    def lookahead_streams(self, streams: Sequence[LaStream], mode: int = 2):
+        """h264a_lookahead_costs of several streams in one launch (h264a_lookahead_streams)."""
+        arr = (LaStream * len(streams))(*streams)
+        self._check(self.L.h264a_lookahead_streams(self.ctx, C.cast(arr, C.c_void_p), len(streams), int(mode),
+                                                   self._stream()))
 
     def batch_create(self, streams: Sequence[BatchStream], cfg: BatchConfig, params: MeParams) -> "Batch":
         """A batch of streams stepping G P frames per graph launch (h264a_batch_create)."""

@@ -19,6 +19,7 @@
 //    TMA one block ahead; candidates outside it, or outside the picture, read
 //    the clamped picture.  The kernel is instantiated per mode.
 #include <cstring>
+#include <vector>
 
 #include "h264a_device.cuh"
 
@@ -330,9 +331,23 @@ constexpr int LA_WARPS = 4;
 // chain's next block window is copied (TMA, lane 0 of the group) while the
 // current block is searched; every copy issued is waited for (bounded,
 // status 3) before the block that reads it.
+// Several streams' lookaheads in one launch: stream s's column tickets are
+// col0[s] .. col0[s+1]-1, all of them before any stream's row tickets
+// (rowt0[s] .. rowt0[s+1]-1 after col0[ns]), so a row ticket's column chain
+// was taken earlier, by a warp that waits for nothing; stream s's flags start
+// at flag0[s].
+constexpr int LA_MAXS = 24;
+struct LaMulti {
+    LaBufs b[LA_MAXS];
+    int col0[LA_MAXS + 1];
+    long long rowt0[LA_MAXS + 1];
+    long long flag0[LA_MAXS];
+    int ns;
+};
+
 template <int MODE>  // b.mode, as a constant
-__global__ void __launch_bounds__(32 * LA_WARPS, 4) la_chains_kernel(const __grid_constant__ LaBufs b,
-                                                                 int* __restrict__ counter, int* __restrict__ flags,
+__global__ void __launch_bounds__(32 * LA_WARPS, 4) la_chains_kernel(const __grid_constant__ LaMulti lm,
+                                                                 int* __restrict__ counter, int* __restrict__ flags0,
                                                                  int epoch, int* __restrict__ status, int spin_limit) {
     __shared__ int2 cs[LA_WARPS][32];
     __shared__ int ds[LA_WARPS][32];
@@ -340,13 +355,10 @@ __global__ void __launch_bounds__(32 * LA_WARPS, 4) la_chains_kernel(const __gri
     const int w = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     const int grp = lane >> 4, gl = lane & 15;
-    const int nf = b.n - 1;
-    const int ncol = (nf + 1) / 2;
-    const long long nrows = (long long)nf * b.mb_h;
     const int buf0 = ((w * 2 + grp) * 2) * LA_WIN_BUF;  // this chain's two buffers in la_win
     const uint32_t win0 = uint32_t(__cvta_generic_to_shared(la_win)) + uint32_t(buf0);
     const uint32_t bar0 = uint32_t(__cvta_generic_to_shared(&la_bar[w][grp][0]));
-    if (b.hmap_ok && gl == 0) {
+    if (gl == 0) {
         mbar_init(bar0, 1);
         mbar_init(bar0 + 8, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -355,7 +367,7 @@ __global__ void __launch_bounds__(32 * LA_WARPS, 4) la_chains_kernel(const __gri
     uint32_t parity = 0;  // bit k: the phase buffer k completes next
     // window of block (mbx, mby) of frame f into buffer k (lane 0 of the group);
     // the group's earlier reads of the buffer are complete (converged warp)
-    auto issue = [&](int k, int f, int mbx, int mby) {
+    auto issue = [&](const LaBufs& b, int k, int f, int mbx, int mby) {
         if (gl == 0) {
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             mbar_expect_tx(bar0 + 8 * k, uint32_t(LA_WIN_BYTES));
@@ -366,19 +378,25 @@ __global__ void __launch_bounds__(32 * LA_WARPS, 4) la_chains_kernel(const __gri
         wait_window(bar0 + 8 * k, (parity >> k) & 1u, status, 3, spin_limit);
         parity ^= 1u << k;
     };
+    const int ns = lm.ns;
     for (;;) {
         int t = 0;
         if (lane == 0) t = atomicAdd(counter, 1);
         t = __shfl_sync(0xffffffffu, t, 0);
-        if (t < ncol) {
-            const int f = 1 + 2 * t + grp;
+        if (t < lm.col0[ns]) {
+            int sidx = 0;
+            while (sidx + 1 < ns && lm.col0[sidx + 1] <= t) sidx++;
+            const LaBufs& b = lm.b[sidx];
+            int* flags = flags0 + lm.flag0[sidx];
+            const int nf = b.n - 1;
+            const int f = 1 + 2 * (t - lm.col0[sidx]) + grp;
             const bool active = f <= nf;
             const bool uw = active && b.hmap_ok;
-            if (uw) issue(0, f, 0, 0);
+            if (uw) issue(b, 0, f, 0, 0);
             int sx = 0, sy = 0;
             for (int mby = 0; mby < b.mb_h; mby++) {
                 const int k = mby & 1;
-                if (uw && mby + 1 < b.mb_h) issue(k ^ 1, f, 0, mby + 1);
+                if (uw && mby + 1 < b.mb_h) issue(b, k ^ 1, f, 0, mby + 1);
                 if (uw) wait(k);
                 int mx, my;
                 la_mb<MODE>(b, active, active ? f : 1, 0, mby, sx, sy, cs[w], ds[w], uw ? buf0 + k * LA_WIN_BUF : -1, mx, my);
@@ -389,19 +407,26 @@ __global__ void __launch_bounds__(32 * LA_WARPS, 4) la_chains_kernel(const __gri
             }
             continue;
         }
-        const long long r = 2 * ((long long)t - ncol) + grp;
-        if (2 * ((long long)t - ncol) >= nrows) return;
+        const long long tr = (long long)t - lm.col0[ns];
+        if (tr >= lm.rowt0[ns]) return;
+        int sidx = 0;
+        while (sidx + 1 < ns && lm.rowt0[sidx + 1] <= tr) sidx++;
+        const LaBufs& b = lm.b[sidx];
+        int* flags = flags0 + lm.flag0[sidx];
+        const int nf = b.n - 1;
+        const long long nrows = (long long)nf * b.mb_h;
+        const long long r = 2 * (tr - lm.rowt0[sidx]) + grp;
         const bool active = r < nrows;
         const bool uw = active && b.hmap_ok && b.mb_w > 1;
         const int mby = active ? int(r / nf) : 0, f = active ? 1 + int(r % nf) : 1;
-        if (uw) issue(0, f, 1, mby);  // the window is an input: no need to wait for column 0
+        if (uw) issue(b, 0, f, 1, mby);  // the window is an input: no need to wait for column 0
         if (active && gl == 0) wait_flag(flags + (f - 1) * b.mb_h + mby, epoch, status, 1, spin_limit);
         __syncwarp();
         const long long gm0 = (long long)b.mb_w * b.mb_h * f + (long long)mby * b.mb_w;
         int sx = active ? __ldcg(b.mvs + 2 * gm0) : 0, sy = active ? __ldcg(b.mvs + 2 * gm0 + 1) : 0;
         for (int mbx = 1; mbx < b.mb_w; mbx++) {
             const int k = (mbx - 1) & 1;
-            if (uw && mbx + 1 < b.mb_w) issue(k ^ 1, f, mbx + 1, mby);
+            if (uw && mbx + 1 < b.mb_w) issue(b, k ^ 1, f, mbx + 1, mby);
             if (uw) wait(k);
             int mx, my;
             la_mb<MODE>(b, active, f, mbx, mby, sx, sy, cs[w], ds[w], uw ? buf0 + k * LA_WIN_BUF : -1, mx, my);
@@ -430,41 +455,103 @@ extern "C" int h264a_downsample2x(h264a_ctx* ctx, const uint8_t* d_frames, int c
     return check_launch("downsample2x_kernel");
 }
 
-extern "C" int h264a_lookahead_costs(h264a_ctx* ctx, const uint8_t* d_full, const uint8_t* d_half, int cw, int ch, int n,
-                                     int mode, int32_t* d_intra, int32_t* d_inter, int32_t* d_mvs, void* stream) {
-    if (!ctx || !d_full || !d_intra || !d_inter || !d_mvs) return fail(H264A_E_ARG, "lookahead_costs: null pointer");
-    if (mode < 0 || mode > 2) return fail(H264A_E_ARG, "lookahead_costs: mode must be 0 (full), 1 (hybrid) or 2 (half)");
-    if (mode != 0 && !d_half) return fail(H264A_E_ARG, "lookahead_costs: modes 1 and 2 need the half-res frames");
-    if (cw < 16 || ch < 16 || cw % 16 || ch % 16 || n < 1) return fail(H264A_E_ARG, "lookahead_costs: bad geometry");
-    cudaStream_t st = pick_stream(ctx, stream);
-    LaBufs b;
+namespace {
+
+// Validates one stream's lookahead and fills its LaBufs (no launch).
+int la_prepare(const h264a_la_stream& q, int mode, LaBufs& b) {
+    if (!q.d_full || !q.d_intra || !q.d_inter || !q.d_mvs) return fail(H264A_E_ARG, "lookahead_costs: null pointer");
+    if (mode != 0 && !q.d_half) return fail(H264A_E_ARG, "lookahead_costs: modes 1 and 2 need the half-res frames");
+    if (q.cw < 16 || q.ch < 16 || q.cw % 16 || q.ch % 16 || q.n < 1)
+        return fail(H264A_E_ARG, "lookahead_costs: bad geometry");
+    if ((long long)(q.n - 1) * (q.ch / 16) > (1 << 24)) return fail(H264A_E_ARG, "lookahead_costs: too many rows");
     memset(&b, 0, sizeof b);
-    b.full = d_full; b.half = d_half; b.cw = cw; b.ch = ch; b.mb_w = cw / 16; b.mb_h = ch / 16; b.n = n; b.mode = mode;
-    b.intra = d_intra; b.inter = d_inter; b.mvs = d_mvs;
-    b.hmap_ok = mode == 2 ? encode_u8_map_3d(&b.hmap, d_half, cw / 2, ch / 2, n, LA_WIN_W, LA_WIN_H, 1) : 0;
-    const LaGeom g = mode == 2 ? LaGeom{8, cw / 2, ch / 2} : LaGeom{16, cw, ch};
-    const size_t fstride = mode == 2 ? (size_t)(cw / 2) * (ch / 2) : (size_t)cw * ch;
-    const long long nmb = (long long)(cw / 16) * (ch / 16);
-    const long long threads = nmb * n * (g.bs == 16 ? 16 : 4);
-    la_intra_kernel<<<unsigned((threads + 255) / 256), 256, 0, st>>>(mode == 2 ? d_half : d_full, fstride, g, cw / 16,
-                                                                    ch / 16, n, d_intra, d_inter, d_mvs);
-    int rc = check_launch("la_intra_kernel");
-    if (rc || n < 2) return rc;
-    const long long chains = ((long long)(n - 1) * (ch / 16) + 1) / 2 + (n - 1 + 1) / 2;  // two chains per warp
-    if ((long long)(n - 1) * (ch / 16) > (1 << 24)) return fail(H264A_E_ARG, "lookahead_costs: too many rows");
-    rc = ensure_me_scratch(ctx, size_t(n - 1) * (ch / 16), Q_LOOKAHEAD);
-    if (rc) return rc;
-    H264A_CUDA(cudaMemsetAsync(ctx->q[Q_LOOKAHEAD].d_counter, 0, sizeof(int32_t), st));
-    const int epoch = next_epoch(ctx, st, Q_LOOKAHEAD);
-    if (epoch < 0) return H264A_E_CUDA;
+    b.full = q.d_full; b.half = q.d_half; b.cw = q.cw; b.ch = q.ch; b.mb_w = q.cw / 16; b.mb_h = q.ch / 16; b.n = q.n;
+    b.mode = mode;
+    b.intra = q.d_intra; b.inter = q.d_inter; b.mvs = q.d_mvs;
+    b.hmap_ok = mode == 2 ? encode_u8_map_3d(&b.hmap, q.d_half, q.cw / 2, q.ch / 2, q.n, LA_WIN_W, LA_WIN_H, 1) : 0;
+    return H264A_OK;
+}
+
+// intra costs of every stream, then their chains in persistent launches of
+// up to LA_MAXS streams each (the queue is the context's lookahead queue).
+int la_run(h264a_ctx* ctx, const h264a_la_stream* qs, int nq, int mode, cudaStream_t st) {
+    if (mode < 0 || mode > 2) return fail(H264A_E_ARG, "lookahead_costs: mode must be 0 (full), 1 (hybrid) or 2 (half)");
+    std::vector<LaBufs> bufs(nq);
+    for (int i = 0; i < nq; i++) {
+        const int rc = la_prepare(qs[i], mode, bufs[i]);
+        if (rc) return rc;
+    }
+    for (int i = 0; i < nq; i++) {
+        const h264a_la_stream& q = qs[i];
+        const int cw = q.cw, ch = q.ch, n = q.n;
+        const LaGeom g = mode == 2 ? LaGeom{8, cw / 2, ch / 2} : LaGeom{16, cw, ch};
+        const size_t fstride = mode == 2 ? (size_t)(cw / 2) * (ch / 2) : (size_t)cw * ch;
+        const long long nmb = (long long)(cw / 16) * (ch / 16);
+        const long long threads = nmb * n * (g.bs == 16 ? 16 : 4);
+        la_intra_kernel<<<unsigned((threads + 255) / 256), 256, 0, st>>>(mode == 2 ? q.d_half : q.d_full, fstride, g,
+                                                                        cw / 16, ch / 16, n, q.d_intra, q.d_inter,
+                                                                        q.d_mvs);
+        const int rc = check_launch("la_intra_kernel");
+        if (rc) return rc;
+    }
     const int smem = LA_WARPS * 2 * 2 * LA_WIN_BUF;  // two window buffers per chain
     auto kern = mode == 0 ? la_chains_kernel<0> : (mode == 1 ? la_chains_kernel<1> : la_chains_kernel<2>);
-    int per_sm = 0;
-    H264A_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * LA_WARPS, smem));
-    long long blocks = (long long)ctx->num_sms * (per_sm > 0 ? per_sm : 1);
-    const long long need = (chains + LA_WARPS - 1) / LA_WARPS;
-    if (blocks > need) blocks = need;
-    kern<<<unsigned(blocks), 32 * LA_WARPS, smem, st>>>(b, ctx->q[Q_LOOKAHEAD].d_counter, ctx->q[Q_LOOKAHEAD].d_flags,
-                                                        epoch, ctx->d_status, SPIN_LIMIT);
-    return check_launch("la_chains_kernel");
+    for (int s0 = 0; s0 < nq; s0 += LA_MAXS) {
+        LaMulti* lm = new LaMulti;
+        memset(lm, 0, sizeof *lm);
+        long long flags = 0;
+        for (int i = s0; i < nq && lm->ns < LA_MAXS; i++) {
+            if (qs[i].n < 2) continue;  // intra only
+            const int k = lm->ns++;
+            const int nf = qs[i].n - 1;
+            const long long nrows = (long long)nf * (qs[i].ch / 16);
+            lm->b[k] = bufs[i];
+            lm->col0[k + 1] = lm->col0[k] + (nf + 1) / 2;
+            lm->rowt0[k + 1] = lm->rowt0[k] + (nrows + 1) / 2;
+            lm->flag0[k] = flags;
+            flags += nrows;
+        }
+        if (lm->ns == 0) {
+            delete lm;
+            continue;
+        }
+        const long long chains = lm->col0[lm->ns] + lm->rowt0[lm->ns];  // two chains per warp
+        int rc = flags > (1LL << 30) ? fail(H264A_E_ARG, "lookahead_costs: too many rows") : H264A_OK;
+        if (!rc) rc = ensure_me_scratch(ctx, size_t(flags), Q_LOOKAHEAD);
+        if (!rc && cudaMemsetAsync(ctx->q[Q_LOOKAHEAD].d_counter, 0, sizeof(int32_t), st) != cudaSuccess)
+            rc = cuda_fail(cudaGetLastError(), "lookahead_costs: counter reset");
+        const int epoch = rc ? -1 : next_epoch(ctx, st, Q_LOOKAHEAD);
+        if (!rc && epoch < 0) rc = H264A_E_CUDA;
+        int per_sm = 0;
+        if (!rc && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * LA_WARPS, smem) != cudaSuccess)
+            rc = cuda_fail(cudaGetLastError(), "lookahead_costs: occupancy");
+        if (!rc) {
+            long long blocks = (long long)ctx->num_sms * (per_sm > 0 ? per_sm : 1);
+            const long long need = (chains + LA_WARPS - 1) / LA_WARPS;
+            if (blocks > need) blocks = need;
+            kern<<<unsigned(blocks), 32 * LA_WARPS, smem, st>>>(*lm, ctx->q[Q_LOOKAHEAD].d_counter,
+                                                                ctx->q[Q_LOOKAHEAD].d_flags, epoch, ctx->d_status,
+                                                                SPIN_LIMIT);
+            rc = check_launch("la_chains_kernel");
+        }
+        delete lm;
+        if (rc) return rc;
+    }
+    return H264A_OK;
+}
+
+}  // namespace
+
+extern "C" int h264a_lookahead_costs(h264a_ctx* ctx, const uint8_t* d_full, const uint8_t* d_half, int cw, int ch, int n,
+                                     int mode, int32_t* d_intra, int32_t* d_inter, int32_t* d_mvs, void* stream) {
+    if (!ctx) return fail(H264A_E_ARG, "lookahead_costs: null pointer");
+    const h264a_la_stream q{d_full, d_half, cw, ch, n, d_intra, d_inter, d_mvs};
+    return la_run(ctx, &q, 1, mode, pick_stream(ctx, stream));
+}
+
+extern "C" int h264a_lookahead_streams(h264a_ctx* ctx, const h264a_la_stream* streams, int nstreams, int mode,
+                                       void* stream) {
+    if (!ctx || !streams) return fail(H264A_E_ARG, "lookahead_streams: null pointer");
+    if (nstreams < 1) return fail(H264A_E_ARG, "lookahead_streams: need at least one stream");
+    return la_run(ctx, streams, nstreams, mode, pick_stream(ctx, stream));
 }

@@ -674,17 +674,30 @@ __global__ void loss_kernel(const float* __restrict__ logits, const int16_t* __r
 // One warp per sample: the 8 largest logits (ties to the lower class) as
 // quarter-pel MVs, 16 i32 per sample; sample i of a batch is MB mb0 + i of
 // the frame whose proposals out points to.
-__global__ void top8_kernel(const float* __restrict__ logits, int B, int32_t* __restrict__ out) {
-    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-    if (w >= B) return;
-    const float* z = logits + (long long)w * HEAD_N;
+// A frame of a propose batch: its guide MVs (may be null) and its proposals.
+struct PropFrame {
+    const int32_t* guide;
+    int32_t* props;
+};
+
+__device__ __forceinline__ void top8_one(const float* __restrict__ z, int32_t* __restrict__ o);
+
+// top8 of every MB of P frames of nmb MBs each, into each frame's proposals
+__global__ void top8_frames_kernel(const float* __restrict__ logits, int P, int nmb, const PropFrame* __restrict__ fr) {
+    const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (w >= (long long)P * nmb) return;
+    const int k = int(w / nmb), m = int(w - (long long)k * nmb);
+    top8_one(logits + w * HEAD_N, fr[k].props + 16LL * m);
+}
+
+__device__ __forceinline__ void top8_one(const float* __restrict__ z, int32_t* __restrict__ o) {
+    const int lane = threadIdx.x & 31;
     float v[10];
 #pragma unroll
     for (int i = 0; i < 10; i++) {
         const int c = lane + 32 * i;
         v[i] = c < NCLS ? z[c] : -INFINITY;
     }
-    int32_t* o = out + 16LL * w;
     for (int r = 0; r < 8; r++) {
         float bv = -INFINITY;
         int bc = 1 << 30;
@@ -727,16 +740,20 @@ __global__ void to_bf16_kernel(const float* __restrict__ src, bf16_t* __restrict
     if (i < n) dst[i] = f2bf(src[i]);
 }
 
-// The neighbour MV features of every MB of one frame from its guide MVs
-// (2 i32 per MB): left, top, top-right MB, zero outside the frame or when
-// the frame has no guide MVs; written for MBs [0, nmb) at nmv + 6 * (base + m).
-__global__ void guide_nmv_kernel(const int32_t* __restrict__ guide, int mb_w, int mb_h, long long base,
-                                 int16_t* __restrict__ nmv) {
-    const int m = blockIdx.x * blockDim.x + threadIdx.x;
-    if (m >= mb_w * mb_h) return;
+// The neighbour MV features of every MB of the P frames of a propose batch
+// (frame k's MBs at samples k * nmb ..) from their guide MVs (2 i32 per MB):
+// left, top, top-right MB, zero outside the frame or when the frame has no
+// guide MVs.
+__global__ void guide_frames_kernel(const PropFrame* __restrict__ fr, int P, int mb_w, int mb_h,
+                                    int16_t* __restrict__ nmv) {
+    const int nmb = mb_w * mb_h;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)P * nmb) return;
+    const int k = int(t / nmb), m = int(t - (long long)k * nmb);
+    const int32_t* guide = fr[k].guide;
     const int mbx = m % mb_w, mby = m / mb_w;
     const int nb[3] = {mbx > 0 ? m - 1 : -1, mby > 0 ? m - mb_w : -1, (mby > 0 && mbx + 1 < mb_w) ? m - mb_w + 1 : -1};
-    int16_t* o = nmv + 6 * (base + m);
+    int16_t* o = nmv + 6 * t;
     for (int j = 0; j < 3; j++) {
         int vx = 0, vy = 0;
         if (guide && nb[j] >= 0) {
@@ -797,6 +814,7 @@ struct h264a_mvnet {
     float* loss = nullptr;
     // inference: the batch's pair table and neighbour features
     h264a_mvnet_pair* ipairs = nullptr;
+    PropFrame* iprop = nullptr;  // a propose batch's frames: guide MVs and proposals
     int16_t* inmv = nullptr;
 };
 
@@ -813,7 +831,7 @@ int dmalloc(T** p, size_t n) {
 
 void free_net(h264a_mvnet* n) {
     void* ps[] = {n->master, n->w, n->grad, n->m1, n->m2, n->a1, n->a2, n->a3, n->h, n->dl, n->dh, n->df,
-                  n->da3, n->da2, n->da1, n->logits, n->loss, n->ipairs, n->inmv};
+                  n->da3, n->da2, n->da1, n->logits, n->loss, n->ipairs, n->inmv, n->iprop};
     for (void* p : ps)
         if (p) cudaFree(p);
     delete n;
@@ -946,6 +964,7 @@ extern "C" int h264a_mvnet_create(int device, uint64_t seed, h264a_mvnet** out) 
     if (!rc) rc = dmalloc(&n->loss, 1);
     if (!rc) rc = dmalloc(&n->inmv, size_t(MAXS * 6));
     if (!rc) rc = dmalloc(&n->ipairs, size_t(MAXPIX / 256));
+    if (!rc) rc = dmalloc(&n->iprop, size_t(MAXPIX / 256));
     if (rc) {
         free_net(n);
         return rc;
@@ -1055,29 +1074,30 @@ extern "C" int h264a_mvnet_propose(h264a_mvnet* n, const h264a_mvnet_frame* h_fr
     // their trunk maps in one pass, then FC1 + head over their MBs, then each
     // frame's top-8 into its own d_props
     std::vector<h264a_mvnet_pair> pr;
+    std::vector<PropFrame> pf;
     int i = 0;
     while (i < nframes) {
         const int cw = h_frames[i].cw, ch = h_frames[i].ch;
         int j = i;
         pr.clear();
+        pf.clear();
         while (j < nframes && h_frames[j].cw == cw && h_frames[j].ch == ch && (long long)(j - i + 1) * cw * ch <= MAXPIX) {
             pr.push_back(h264a_mvnet_pair{h_frames[j].d_cur, h_frames[j].d_ref});
+            pf.push_back(PropFrame{h_frames[j].d_guide_mvs, h_frames[j].d_props});
             j++;
         }
         const int P = j - i;
-        // the previous batch's kernels read the pair table on this stream, so
-        // the upload is stream-ordered after them (pageable source: the copy
-        // is staged before the call returns)
+        // the previous batch's kernels read the tables on this stream, so the
+        // uploads are stream-ordered after them (pageable sources: the copies
+        // are staged before the call returns)
         H264A_CUDA(cudaMemcpyAsync(n->ipairs, pr.data(), sizeof(h264a_mvnet_pair) * P, cudaMemcpyHostToDevice, st));
+        H264A_CUDA(cudaMemcpyAsync(n->iprop, pf.data(), sizeof(PropFrame) * P, cudaMemcpyHostToDevice, st));
         const Geo g = make_geo(n->ipairs, P, cw, ch, n->inmv, nullptr);
-        for (int k = 0; k < P; k++)
-            guide_nmv_kernel<<<(g.nmb + 255) / 256, 256, 0, st>>>(h_frames[i + k].d_guide_mvs, g.mb_w, g.mb_h,
-                                                                  (long long)k * g.nmb, n->inmv);
+        const long long samples = (long long)P * g.nmb;
+        guide_frames_kernel<<<unsigned((samples + 255) / 256), 256, 0, st>>>(n->iprop, P, g.mb_w, g.mb_h, n->inmv);
         trunk_forward(n, g, st);
         head_forward(n, g, st);
-        for (int k = 0; k < P; k++)
-            top8_kernel<<<(g.nmb * 32 + 255) / 256, 256, 0, st>>>(n->logits + (long long)k * g.nmb * HEAD_N, g.nmb,
-                                                                  h_frames[i + k].d_props);
+        top8_frames_kernel<<<unsigned((samples * 32 + 255) / 256), 256, 0, st>>>(n->logits, P, g.nmb, n->iprop);
         i = j;
     }
     return check_launch("mvnet propose");

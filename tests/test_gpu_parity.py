@@ -917,6 +917,41 @@ def test_lookahead_window_misses_and_no_window(acc, cw, ch, pan):
         assert (np.abs(wm[1:, :, 0]) >= 32).mean() > 0.25  # the search follows the pan past the window
 
 
+@pytest.mark.parametrize("mode", [2, 0])
+def test_lookahead_streams_one_launch(acc, mode):
+    """h264a_lookahead_streams over four clips of three sizes and lengths
+    (CIF x 5, 208x144 x 3 without windows, 384x272 x 6, and a one-frame clip,
+    intra only) gives, stream by stream, what h264a_lookahead_costs gives each
+    alone, and the CIF stream equals the oracle."""
+    torch = acc.torch
+    cif = synth.coded_luma(synth.cif_clip(5, 3)[0])
+    hd = synth.coded_luma(synth.hd_clip(6, 4, 384, 272)[0])
+    rng = np.random.default_rng(9)
+    small = rng.integers(0, 256, (3, 144, 208)).astype(np.uint8)
+    one = rng.integers(0, 256, (1, 64, 96)).astype(np.uint8)
+    clips, keep, streams, alone = [cif, small, hd, one], [], [], []
+    for c in clips:
+        n, ch, cw = c.shape
+        nmb = (cw // 16) * (ch // 16)
+        full = dev(acc, c)
+        half = acc.downsample2x(full)
+        outs = [acc.zeros((n, nmb), torch.int32), acc.zeros((n, nmb), torch.int32), acc.zeros((n, nmb, 2), torch.int32)]
+        keep.append((full, half, outs))
+        streams.append(A.LaStream(full.data_ptr(), half.data_ptr(), cw, ch, n, outs[0].data_ptr(), outs[1].data_ptr(),
+                                  outs[2].data_ptr()))
+        i1, n1, m1 = acc.lookahead_costs(full, half, mode)
+        acc.sync()
+        alone.append((i1.cpu().numpy(), n1.cpu().numpy(), m1.cpu().numpy()))
+    acc.lookahead_streams(streams, mode)
+    acc.sync()
+    for k, (_, _, outs) in enumerate(keep):
+        got = [o.cpu().numpy() for o in outs]
+        for g, a in zip(got, alone[k]):
+            assert np.array_equal(g, a), (mode, k)
+    wi, wn, wm = O.lookahead_clip(cif, mode)
+    assert np.array_equal(alone[0][0], wi) and np.array_equal(alone[0][1], wn) and np.array_equal(alone[0][2], wm)
+
+
 def test_lookahead_flat_and_static(acc):
     flat = np.full((3, 32, 32), 77, np.uint8)
     full = dev(acc, flat)
