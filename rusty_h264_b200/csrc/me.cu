@@ -1575,26 +1575,29 @@ __device__ __forceinline__ void wide_mb(const FrameDesc& fd, const RecDesc& rd, 
         // 1 the top MB's (0,3), lane 2 the top-right MB's (0,3), lane 3
         // the top-left MB's (3,3) when there is no top-right
         const bool aa = mbx > 0, ba = mby > 0, ca = mby > 0 && mbx < fd.mb_w - 1, da = mbx > 0 && mby > 0;
+        const bool need = lane < 4 && (lane == 0 ? aa : (lane == 1 ? ba : (lane == 2 ? ca : (!ca && da))));
+        const int dm = lane == 0 ? -EW_PER_MB
+                                 : EW_PER_MB * (lane == 1 ? -fd.mb_w : (lane == 2 ? 1 - fd.mb_w : -1 - fd.mb_w));
+        const unsigned long long* word = ew + dm + (lane == 0 ? 0 : (lane == 3 ? 2 : 1));
+        // The neighbours above were published a row earlier, so the window's
+        // origin is guessed from the top MB's MV and its copy overlaps the
+        // wait for the left MB (on the wavefront's path).  Any origin gives
+        // the same results: candidates the window misses read the planes.
         int2 nv = make_int2(0, 0);
-        if (lane < 4 && (lane == 0 ? aa : (lane == 1 ? ba : (lane == 2 ? ca : (!ca && da))))) {
-            const int dm = lane == 0 ? -EW_PER_MB
-                                     : EW_PER_MB * (lane == 1 ? -fd.mb_w : (lane == 2 ? 1 - fd.mb_w : -1 - fd.mb_w));
-            nv = wait_mv_word(ew + dm + (lane == 0 ? 0 : (lane == 3 ? 2 : 1)), epoch, status, spin_limit);
-        }
+        if (need && (lane > 0 || !ba)) nv = wait_mv_word(word, epoch, status, spin_limit);
         __syncwarp();
-        const int2 a = make_int2(__shfl_sync(0xffffffffu, nv.x, 0), __shfl_sync(0xffffffffu, nv.y, 0));
         const int2 bb = make_int2(__shfl_sync(0xffffffffu, nv.x, 1), __shfl_sync(0xffffffffu, nv.y, 1));
         const int2 c = make_int2(__shfl_sync(0xffffffffu, nv.x, ca ? 2 : 3), __shfl_sync(0xffffffffu, nv.y, ca ? 2 : 3));
-        const int2 pmv = predict_mv_ref0(aa, a, ba, bb, ca || da, c);
+        const int2 guess = ba ? bb : predict_mv_ref0(aa, make_int2(__shfl_sync(0xffffffffu, nv.x, 0),
+                                                                   __shfl_sync(0xffffffffu, nv.y, 0)),
+                                                     false, bb, false, c);
         if (lane == 0) {
-            mb.pmvx = pmv.x;
-            mb.pmvy = pmv.y;
             mb.bready = -1;
             scratch[0].win_ok = win_ok;
         }
         if (win_ok) {
-            const int wx0 = min(max((lx + pc.pad + (pmv.x >> 2) - WIN_R) & ~15, 0), pw - WIN_W);
-            const int wy0 = min(max(ly + pc.pad + (pmv.y >> 2) - WIN_R, 0), ph - WIN_H);
+            const int wx0 = min(max((lx + pc.pad + (guess.x >> 2) - WIN_R) & ~15, 0), pw - WIN_W);
+            const int wy0 = min(max(ly + pc.pad + (guess.y >> 2) - WIN_R, 0), ph - WIN_H);
             if (lane == 0) {
                 scratch[0].wx0 = wx0;
                 scratch[0].wy0 = wy0;
@@ -1624,6 +1627,14 @@ __device__ __forceinline__ void wide_mb(const FrameDesc& fd, const RecDesc& rd, 
                              pc.d_planes + ps * pl + (long long)(wy0 + r) * pw + wx0, WIN_W, bar);
                 }
             }
+        }
+        if (need && lane == 0 && ba) nv = wait_mv_word(word, epoch, status, spin_limit);
+        __syncwarp();
+        const int2 a = make_int2(__shfl_sync(0xffffffffu, nv.x, 0), __shfl_sync(0xffffffffu, nv.y, 0));
+        const int2 pmv = predict_mv_ref0(aa, a, ba, bb, ca || da, c);
+        if (lane == 0) {
+            mb.pmvx = pmv.x;
+            mb.pmvy = pmv.y;
         }
     }
     __syncthreads();  // the predictor and the window's origin are in shared memory
