@@ -144,3 +144,24 @@ def test_batch_tuning_cached_per_signature(acc):
     with pytest.raises(A.AccelError):
         b.step(0, G + 1)
     b.close()
+
+
+def test_batch_one_reference_one_frame_steps(acc):
+    """G = 1, one reference, the smallest ring (3 slots): every step is one
+    frame of each stream and equals h264a_me_frames_multiref's one-reference
+    search (the oracle) frame by frame, across ring wrap-arounds."""
+    global NREF, G, NSLOTS
+    saved = (NREF, G, NSLOTS)
+    NREF, G, NSLOTS = 1, 1, 3
+    try:
+        clips = _clips(7)
+        lam, gate, params = _setup(30)
+        out, info = _run(acc, clips, lam, gate, params, autotune=0, variant=3)
+        assert info["steps"] == 6 and info["graphs"] == 4  # slots 0, 1, 2 (+ the warm-up layout of step 0)
+        for f, res in sorted(out.items()):
+            for s, (clip, (gp, gc)) in enumerate(zip(clips, res)):
+                wp, wc = _oracle(clip, f, lam, gate)
+                assert np.array_equal(gp[:, :7], wp[:, :7]) and np.array_equal(gc, wc), (f, s)
+                assert (gp[:, 1] == 0).all() and (gp[:, 4] == 0).all()  # one reference: index 0 throughout
+    finally:
+        NREF, G, NSLOTS = saved

@@ -952,6 +952,33 @@ def test_lookahead_streams_one_launch(acc, mode):
     assert np.array_equal(alone[0][0], wi) and np.array_equal(alone[0][1], wn) and np.array_equal(alone[0][2], wm)
 
 
+def test_lookahead_streams_more_than_one_launch(acc):
+    """26 small clips (more than the 24 streams one launch takes) of 2 to 4
+    frames: two chains launches, each stream equal to the oracle."""
+    torch = acc.torch
+    rng = np.random.default_rng(21)
+    keep, streams, clips = [], [], []
+    for k in range(26):
+        n, ch, cw = 2 + k % 3, 32 + 16 * (k % 2), 48 + 16 * (k % 3)
+        base = rng.integers(0, 256, (ch + 8, cw + 8)).astype(np.uint8)
+        c = np.ascontiguousarray(np.stack([base[f % 3: f % 3 + ch, f: f + cw] for f in range(n)]))
+        nmb = (cw // 16) * (ch // 16)
+        full = dev(acc, c)
+        half = acc.downsample2x(full)
+        outs = [acc.zeros((n, nmb), torch.int32), acc.zeros((n, nmb), torch.int32), acc.zeros((n, nmb, 2), torch.int32)]
+        keep.append(outs)
+        keep.append((full, half))
+        clips.append((c, outs))
+        streams.append(A.LaStream(full.data_ptr(), half.data_ptr(), cw, ch, n, outs[0].data_ptr(), outs[1].data_ptr(),
+                                  outs[2].data_ptr()))
+    acc.lookahead_streams(streams, 2)
+    acc.sync()
+    for k, (c, outs) in enumerate(clips):
+        wi, wn, wm = O.lookahead_clip(c, 2)
+        got = [o.cpu().numpy() for o in outs]
+        assert np.array_equal(got[0], wi) and np.array_equal(got[1], wn) and np.array_equal(got[2], wm), k
+
+
 def test_lookahead_flat_and_static(acc):
     flat = np.full((3, 32, 32), 77, np.uint8)
     full = dev(acc, flat)
