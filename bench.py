@@ -519,7 +519,9 @@ class ClosedBufs:
         self.u = torch.from_numpy(np.ascontiguousarray(U)).to(dev)
         self.v = torch.from_numpy(np.ascontiguousarray(V)).to(dev)
         self.ry, self.ru, self.rv = torch.empty_like(self.y), torch.empty_like(self.u), torch.empty_like(self.v)
-        self.planes = torch.empty((16 * (cw + 64) * (ch + 64),), dtype=torch.uint8, device=dev)
+        from rusty_h264_b200 import accel as A
+
+        self.planes = torch.empty((A.closed_plane_bytes(n, cw, ch),), dtype=torch.uint8, device=dev)
         self.picks = torch.zeros((n, nmb, 6), dtype=torch.int32, device=dev)
         self.costs = torch.zeros((n, nmb, 2), dtype=torch.int64, device=dev)
         self.coeffs = torch.zeros((n, nmb, 256), dtype=torch.int16, device=dev)

@@ -553,13 +553,15 @@ H264A_API int h264a_pixel_path_closed(h264a_ctx *ctx, const h264a_closed_job *jo
                                       const uint16_t *h_mv_cost_tab);
 /* The same loop on device buffers, enqueued on `stream` (no allocation, no
  * host copy): the caller passes the n source frames, room for their
- * reconstruction (frame 0 is copied from the source), four pictures' planes
- * as scratch (16*(cw+64)*(ch+64) bytes: the loop overlaps consecutive frames,
- * each building its reconstruction's planes band by band while the next
- * frame searches the finished bands), the outputs (levels 16-byte aligned,
+ * reconstruction (frame 0 is copied from the source), the planes of
+ * min(n, H264A_CLOSED_PLANE_PICTURES) pictures as scratch (4*(cw+64)*(ch+64)
+ * bytes each: the loop overlaps many consecutive frames, each building its
+ * reconstruction's planes segment by segment while later frames search the
+ * finished segments), the outputs (levels 16-byte aligned,
  * chroma 4-byte aligned), and with a net the proposals buffer (16 i32/MB per
  * frame), optional fallback flags and the guide MVs (2 i32/MB per frame, the
  * lookahead's, or NULL). */
+#define H264A_CLOSED_PLANE_PICTURES 16
 typedef struct {
     const uint8_t *d_y, *d_u, *d_v;
     uint8_t *d_rec_y, *d_rec_u, *d_rec_v;

@@ -140,6 +140,12 @@ class LaStream(C.Structure):
 
 
 BATCH_VARIANTS = 6  # H264A_BATCH_VARIANTS
+CLOSED_PLANE_PICTURES = 16  # H264A_CLOSED_PLANE_PICTURES
+
+
+def closed_plane_bytes(n: int, cw: int, ch: int, pad: int = 32) -> int:
+    """Plane scratch of h264a_closed_frames: min(n, 16) pictures' F|H|V|C planes."""
+    return 4 * min(n, CLOSED_PLANE_PICTURES) * (cw + 2 * pad) * (ch + 2 * pad)
 
 
 class BatchStream(C.Structure):

@@ -14,6 +14,7 @@
 // over the source pairs (f, f-1).  One P frame alone is
 // h264a_closed_step_frame (the planes of rec(f-1) are the caller's).
 // Frame 0 reconstructs to itself (the frame model codes it losslessly).
+#include <algorithm>
 #include <chrono>
 #include <cstring>
 #include <string>
@@ -75,8 +76,8 @@ int closed_run(h264a_ctx* ctx, const h264a_closed_dev& j, const h264a_me_params&
         const int rc = h264a_mvnet_propose(j.net, nf.data(), n - 1, st);
         if (rc) return rc;
     }
-    // the planes of rec(0) in the first of the four plane buffers, then every
-    // P frame in one pipelined launch
+    // the planes of rec(0) in the first plane buffer, then every P frame in
+    // one pipelined launch
     int rc = h264a_hpel_build(ctx, j.d_rec_y, cw, ch, pad, 1, fs, j.d_planes, st);
     if (rc) return rc;
     ClosedPipeIn in;
@@ -152,7 +153,7 @@ extern "C" int h264a_pixel_path_closed(h264a_ctx* ctx, const h264a_closed_job* j
     };
     const size_t o_sy = part(n * fs), o_su = part(n * cs), o_sv = part(n * cs);
     const size_t o_ry = part(n * fs), o_ru = part(n * cs), o_rv = part(n * cs);
-    const size_t o_pl = part(size_t(16) * pw * ph), o_pk = part(sizeof(int32_t) * 6 * nmb * n);
+    const size_t o_pl = part(size_t(4) * std::min(n, H264A_CLOSED_PLANE_PICTURES) * pw * ph), o_pk = part(sizeof(int32_t) * 6 * nmb * n);
     const size_t o_co = part(sizeof(int64_t) * 2 * nmb * n), o_lv = part(sizeof(int16_t) * 256 * nmb * n);
     const size_t o_cl = part(sizeof(int16_t) * 128 * nmb * n), o_tab = part(sizeof(uint16_t) * 4096);
     size_t o_pr = 0, o_fb = 0, o_half = 0, o_la = 0;

@@ -50,13 +50,16 @@ struct HpelRow {
 
 // Rows [y0, y1) of strip `strip` (plane columns strip * HP_STRIP ..) of the
 // four planes F of picture Y, one warp: see the file comment of hpel.cu.
+// Only the 4-byte words whose plane column lies in [xlo, xhi) are written
+// (xlo, xhi multiples of 4): a strip shared by two column segments is
+// written by each for its own columns.
 // CG: read the picture through L2 rather than the read-only path (a picture
 // written during the launch, whose rows below the strip's may still change:
 // the look-ahead loads past y1 must not leave stale lines in L1).
 template <bool CG = false>
 __device__ __forceinline__ void hpel_strip_rows(const uint8_t* __restrict__ Y, int cw, int ch, int pad,
                                                 uint8_t* __restrict__ F, int pw, int ph, int strip, int y0, int y1,
-                                                int word_in, int word_out) {
+                                                int word_in, int word_out, int xlo = 0, int xhi = 1 << 30) {
     const int lane = threadIdx.x & 31;
     const long long ps = (long long)pw * ph;
     const int X = strip * HP_STRIP + 4 * (lane - 1);  // plane column of the lane's word
@@ -78,7 +81,7 @@ __device__ __forceinline__ void hpel_strip_rows(const uint8_t* __restrict__ Y, i
         return r;
     };
     auto load = [&](int yp) { return mk(ldraw(yp)); };
-    const bool owner = lane >= 1 && lane <= 30 && X < pw;
+    const bool owner = lane >= 1 && lane <= 30 && X < pw && X >= xlo && X < xhi;
     // the four planes' words of row y from the rows y-2 .. y+3
     auto emit = [&](int y, const HpelRow& a, const HpelRow& b, const HpelRow& c, const HpelRow& d, const HpelRow& e,
                     const HpelRow& f) {

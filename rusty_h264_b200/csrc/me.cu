@@ -47,21 +47,26 @@ constexpr int ME_PART_TEAM = ME_WIDE_WARPS / 4;  // warps per partition search
 // means bands 0..b are complete), and a search waits (bounded) for the band
 // of every row it reads.
 struct BandWait {
-    const int* flags;
-    int nbands, epoch, limit;
+    const int* flags;  // nbands x nseg readiness flags, band-major
+    int nbands, nseg, segw, epoch, limit;
     int* status;
 };
 
-// Waits until the band holding picture row `row` of the reference is built
-// (nothing when the search has no BandWait); `ready` caches the highest band
-// seen complete.
-__device__ __forceinline__ void band_wait_row(const BandWait* bw, int* ready, int row) {
+// Waits until the reference's planes (and reconstruction) are final at
+// picture pixel (row, col), clamped into the picture: the flag of the band
+// (16 rows) and column segment (segw columns) holding it.  Segment (b, s) is
+// published after (b-1, s) and (b, s-1), so it stands for every segment up
+// and left of it.  `ready` caches a segment seen ready, packed b << 12 | s
+// (-1: none); any value stored there was seen ready, so a torn update between
+// lanes only loses a shortcut.  Nothing when the search has no BandWait.
+__device__ __forceinline__ void band_wait_px(const BandWait* bw, int* ready, int row, int col) {
     if (bw == nullptr) return;
-    int b = row < 16 ? 0 : row >> 4;
-    if (b >= bw->nbands) b = bw->nbands - 1;
-    if (b <= *reinterpret_cast<volatile int*>(ready)) return;
-    wait_flag(bw->flags + b, bw->epoch, bw->status, 1, bw->limit);
-    atomicMax(ready, b);
+    const int b = min(max(row, 0) >> 4, bw->nbands - 1);
+    const int sg = min(max(col, 0) / bw->segw, bw->nseg - 1);
+    const int c = *reinterpret_cast<volatile int*>(ready);
+    if (c >= 0 && b <= (c >> 12) && sg <= (c & 4095)) return;
+    wait_flag(bw->flags + b * bw->nseg + sg, bw->epoch, bw->status, 1, bw->limit);
+    if (c < 0 || (b >= (c >> 12) && sg >= (c & 4095))) *reinterpret_cast<volatile int*>(ready) = (b << 12) | sg;
 }
 
 // Per-warp shared state: the round's candidates and distortions, and the
@@ -79,7 +84,7 @@ struct WarpScratch {
     int win_ok;           // the MB's reference window is staged in shared memory
     int wx0, wy0;         // its origin in padded-plane coordinates
     const BandWait* bw;   // the reference's band readiness, or nullptr (complete)
-    int bready;           // the highest band seen complete
+    int bready;           // a reference segment seen complete (band_wait_px)
 };
 
 // ---------------------------------------------------------------------------
@@ -693,7 +698,7 @@ __device__ __forceinline__ void eval_round_group(const GroupGeom& q, WarpScratch
                 if (win_covers(wx, wy)) {
                     win_rows(g.win, wx, wy, mv.x & 3, mv.y & 3, pr4[kk]);
                 } else {
-                    band_wait_row(ws.bw, &ws.bready, g.ly + g.byo + dy + 5);
+                    band_wait_px(ws.bw, &ws.bready, g.ly + g.byo + dy + 5, g.lx + g.bxo + dx + 5);
                     Planes P;
                     P.base = ws.base; P.pw = ws.pw; P.ph = ws.ph; P.pad = ws.pad; P.ps = (long long)ws.pw * ws.ph;
                     P.cg = ws.bw != nullptr;
@@ -1190,6 +1195,9 @@ constexpr int ME_MAXF = 96;
 // one frame's wavefront has at most a few dozen ready MBs, far fewer than the
 // resident warps, so each MB's own latency is what counts.
 constexpr int ME_WIDE_MAXF = 2;
+// The pipelined closed loop: the width of a band's column segments in MBs,
+// and the number of CTA pools (frames dealt round-robin to them).
+constexpr int PIPE_SEGW = 8, PIPE_POOLS = 8;
 struct FrameBatch {
     FrameDesc f[ME_MAXF];
     long long seg_start[ME_MAXF + 1];
@@ -1517,7 +1525,7 @@ __device__ __forceinline__ int2 wait_mv_word(const unsigned long long* p, int ep
 
 struct WideMb {
     int pmvx, pmvy;         // the median predictor
-    int bready;             // the reference's highest band seen complete (pipelined loop)
+    int bready;             // a reference segment seen complete (pipelined loop, band_wait_px)
     long long c16;          // 16x16 J
     int mv16x, mv16y, ev16;
     int px[4], py[4], pev[4];
@@ -1603,7 +1611,7 @@ __device__ __forceinline__ void wide_mb(const FrameDesc& fd, const RecDesc& rd, 
                 scratch[0].wy0 = wy0;
                 // the window's reference rows are built (pipelined loop), and
                 // the generic-proxy writes of them are visible to the copy
-                band_wait_row(bw, &mb.bready, wy0 - pc.pad + WIN_H - 1);
+                band_wait_px(bw, &mb.bready, wy0 - pc.pad + WIN_H - 1, wx0 - pc.pad + WIN_W - 1);
                 if (bw != nullptr) asm volatile("fence.proxy.async.global;" ::: "memory");
                 // every warp's reads of the previous MB's window are
                 // complete (the CTA barrier at the end of the last MB)
@@ -1731,7 +1739,7 @@ __device__ __forceinline__ void wide_mb(const FrameDesc& fd, const RecDesc& rd, 
             if (win_ok && win_covers(wx, wy)) {
                 win_rows(win, wx, wy, mvx & 3, mvy & 3, pr);
             } else {
-                band_wait_row(bw, &scratch[0].bready, y + (mvy >> 2) + 5);
+                band_wait_px(bw, &scratch[0].bready, y + (mvy >> 2) + 5, x + (mvx >> 2) + 5);
                 Planes P;
                 P.base = pc.d_planes; P.pw = pw; P.ph = ph; P.pad = pc.pad; P.ps = (long long)pw * ph;
                 P.cg = bw != nullptr;
@@ -1771,7 +1779,8 @@ __device__ __forceinline__ void wide_mb(const FrameDesc& fd, const RecDesc& rd, 
             const int mvx = part ? mv1x : mv0x, mvy = part ? mv1y : mv0y;
             // the previous reconstruction's chroma rows it reads are final
             // (pipelined loop: band b complete means MB rows 0..b+1 deblocked)
-            band_wait_row(bw, &scratch[1].bready, 2 * min(cy0 + by + 4 + (mvy >> 3), pc.ch / 2 - 1) + 1);
+            band_wait_px(bw, &scratch[1].bready, 2 * min(cy0 + by + 4 + (mvy >> 3), pc.ch / 2 - 1) + 1,
+                         2 * min(cx0 + bx + 4 + (mvx >> 3), pc.cw / 2 - 1) + 1);
             uint32_t r4[4];
             chroma_tq_rec(rd.src_c[c], rd.ref_c[c], pc.cw / 2, pc.ch / 2, cx0 + bx, cy0 + by, mvx, mvy, kb, rd.qpc,
                           rd.cff, rd.cmf, lane < 8 ? rd.ccoeffs + (long long)m * 128 + c * 64 + kb * 16 : nullptr,
@@ -1906,59 +1915,66 @@ __global__ void __launch_bounds__(32 * ME_WARPS, ME_MIN_BLOCKS)
 // The pipelined closed loop: every P frame of a clip in one launch
 // ---------------------------------------------------------------------------
 // Frame h searches the planes of the deblocked reconstruction of frame h-1,
-// but an MB only reads the reference rows its window (and any candidate off
-// the window) reaches.  So the launch runs the frames' wavefronts overlapped:
-// each frame's tickets are its MBs in wavefront order with, after the last MB
-// of MB row b+1, a band ticket that builds the planes of the frame's
-// reconstruction for picture rows 16b .. 16b+15 (hpel_strip_rows, all four
-// warps) once that row is deblocked.  An MB of frame h waits (bounded) for
-// the bands of frame h-1 its reads need (band_wait_row); a band's flag is
-// published after the previous band's, so it stands for every band up to it.
-// The planes of four consecutive frames live in four buffers (frame h's in
-// buffer h % 4), and a band ticket of frame h first waits until frame h-3,
-// the last reader of the buffer's previous picture, has finished every MB.
+// but an MB only reads the reference pixels its window (and any candidate
+// off the window) reaches.  So the launch runs the frames' wavefronts
+// overlapped: each frame's tickets are its MBs in wavefront order with
+// segment tickets among them.  Segment (b, s) covers picture rows
+// 16b .. 16b+15 (band b) and columns 16*segw*s .. (segment s, the first and
+// last segments reaching into the padding); its ticket comes after the MB
+// whose deblocking makes those reconstruction pixels final, MB
+// (min(segw*(s+1), mb_w-1), min(b+1, mb_h-1)) (deblocking runs as a
+// wavefront too, so that MB done means every MB up and left of it is), and
+// builds the planes of the segment (hpel_strip_rows, its own columns only).
+// An MB of frame h waits (bounded) for the segments of frame h-1 its reads
+// need (band_wait_px); a segment's flag is published after the flags of the
+// segments above and left of it, so one flag stands for all of those.  The
+// next frame can therefore start a few MB columns and rows behind the
+// previous one instead of a whole frame width behind.  The planes of nbuf
+// consecutive frames live in nbuf buffers (frame h's in buffer h % nbuf),
+// and a segment ticket of frame h first waits until frame h-nbuf+1, the last
+// reader of the buffer's previous picture, has finished every MB.
 //
-// Deadlock freedom: the CTAs form two pools, the even blocks taking frames 1,
-// 3, 5, ... and the odd ones 2, 4, ..., each pool its frames in order, a CTA
-// moving to the pool's next frame only once the current frame's tickets are
-// all dealt.  A ticket waits only on earlier tickets of its own frame, on
-// frame h-1 (the other pool) and on frame h-3's completion; the oldest
-// unfinished frame therefore depends on nothing unfinished, its tickets are
-// all dealt or held by CTAs of its own pool that are not blocked by a later
-// frame, and it always progresses.  Every wait is still bounded, and after
-// the first timeout the others give up (status 1).
+// Deadlock freedom: the CTAs form `pools` pools, block i taking frames
+// 1 + i % pools, 1 + i % pools + pools, ..., each pool its frames in order, a
+// CTA moving to the pool's next frame only once the current frame's tickets
+// are all dealt.  A ticket waits only on earlier tickets of its own frame, on
+// frame h-1 and on frame h-nbuf+1's completion; the oldest unfinished frame
+// therefore depends on nothing unfinished, its tickets are all dealt or held
+// by CTAs of its own pool that are not blocked by a later frame, and it
+// always progresses.  Every wait is still bounded, and after the first
+// timeout the others give up (status 1).
 struct PipeParams {
     const FrameDesc* fds;  // per frame 0..n-1 (entry 0 unused), in device memory
     const RecDesc* rds;
-    const int* items;      // a frame's tickets: MB index, or -(band + 1)
-    int nitems, n, mb_w, mb_h, nbands;
-    int* flags;            // per frame fstride ints: MV words, deblocking flags, band flags
+    const int* items;      // a frame's tickets: MB index, or -(1 + b * nseg + s)
+    int nitems, n, mb_w, mb_h, nbands, nseg, segw, nbuf, pools;
+    int* flags;            // per frame fstride ints: MV words, deblocking flags, segment flags
     long long fstride;
     int ew_off, dfl_off, band_off;
     int* ctr;              // n ticket counters and n completed-MB counters, zeroed
     int* done;
     const uint8_t* rec_y;  // frame h's luma reconstruction at h * fs
     long long fs;
-    uint8_t* planes;       // four plane buffers, pbytes apart
+    uint8_t* planes;       // nbuf plane buffers, pbytes apart
     long long pbytes;
     int cw, ch, pad, word_in, word_out;
     int32_t* frame_words;  // mapped host words: frame h's set to ftoken when it is final (or null)
     int32_t ftoken;
 };
 
-// Band b of frame h: the planes of its reconstruction for padded rows
-// [pad + 16b, pad + 16b + 16) (band 0 from row 0, the last band to the end),
-// once MB row b+1 (or the last) is deblocked, into buffer h % 4.
-__device__ __forceinline__ void pipe_band(const PipeParams& pp, int h, int b, int epoch, int* status, int limit) {
+// Segment (b, s) of frame h: the planes of its reconstruction for padded rows
+// [pad + 16b, pad + 16b + 16) (band 0 from row 0, the last band to the end)
+// and padded columns [pad + 16*segw*s, pad + 16*segw*(s+1)) (segment 0 from
+// column 0, the last segment to the end), into buffer h % nbuf.
+__device__ __forceinline__ void pipe_band(const PipeParams& pp, int h, int b, int sg, int epoch, int* status,
+                                          int limit) {
     int* const ff = pp.flags + pp.fstride * h;
     if (threadIdx.x == 0) {
-        // a row's deblocking runs left to right and waits on the row above:
-        // its last MB done means every MB of rows 0..r is
-        const int r = min(b + 1, pp.mb_h - 1);
-        wait_flag(ff + pp.dfl_off + r * pp.mb_w + pp.mb_w - 1, epoch, status, 1, limit);
-        if (h - 3 >= 1) {
+        const int r = min(b + 1, pp.mb_h - 1), x = min(pp.segw * (sg + 1), pp.mb_w - 1);
+        wait_flag(ff + pp.dfl_off + r * pp.mb_w + x, epoch, status, 1, limit);
+        if (h - pp.nbuf + 1 >= 1) {
             const int nmb = pp.mb_w * pp.mb_h;
-            for (int it = 0; ld_acquire(pp.done + h - 3) < nmb; it++) {
+            for (int it = 0; ld_acquire(pp.done + h - pp.nbuf + 1) < nmb; it++) {
                 if (it >= limit || ((it & 255) == 255 && *reinterpret_cast<volatile int*>(status) != 0)) {
                     atomicCAS(status, 0, 1);
                     break;
@@ -1971,16 +1987,19 @@ __device__ __forceinline__ void pipe_band(const PipeParams& pp, int h, int b, in
     const int pw = pp.cw + 2 * pp.pad, ph = pp.ch + 2 * pp.pad;
     const int y0 = b == 0 ? 0 : pp.pad + 16 * b;
     const int y1 = b == pp.nbands - 1 ? ph : pp.pad + 16 * b + 16;
-    const int strips = (pw + HP_STRIP - 1) / HP_STRIP;
-    for (int st = int(threadIdx.x >> 5); st < strips; st += ME_WIDE_WARPS)
-        hpel_strip_rows<true>(pp.rec_y + pp.fs * h, pp.cw, pp.ch, pp.pad, pp.planes + pp.pbytes * (h & 3), pw, ph, st,
-                              y0, y1, pp.word_in, pp.word_out);
+    const int x0 = sg == 0 ? 0 : pp.pad + 16 * pp.segw * sg;
+    const int x1 = sg == pp.nseg - 1 ? pw : pp.pad + 16 * pp.segw * (sg + 1);
+    for (int st = x0 / HP_STRIP + int(threadIdx.x >> 5); st * HP_STRIP < x1; st += ME_WIDE_WARPS)
+        hpel_strip_rows<true>(pp.rec_y + pp.fs * h, pp.cw, pp.ch, pp.pad, pp.planes + pp.pbytes * (h % pp.nbuf), pw,
+                              ph, st, y0, y1, pp.word_in, pp.word_out, x0, x1);
     // the planes' generic-proxy writes, visible to the readers' bulk copies
     asm volatile("fence.proxy.async.global;" ::: "memory");
     __syncthreads();
     if (threadIdx.x == 0) {
-        if (b > 0) wait_flag(ff + pp.band_off + b - 1, epoch, status, 1, limit);
-        st_release(ff + pp.band_off + b, epoch);
+        int* const sf = ff + pp.band_off + b * pp.nseg + sg;
+        if (b > 0) wait_flag(sf - pp.nseg, epoch, status, 1, limit);
+        if (sg > 0) wait_flag(sf - 1, epoch, status, 1, limit);
+        st_release(sf, epoch);
     }
 }
 
@@ -2001,13 +2020,13 @@ __global__ void __launch_bounds__(32 * ME_WIDE_WARPS, ME_MIN_BLOCKS)
     __syncthreads();
     uint32_t parity = 0;
     int fenced = -1;  // the frame whose tensor maps this CTA has acquired
-    int h = 1 + int(blockIdx.x & 1);  // this CTA's pool: frames 1, 3, ... or 2, 4, ...
+    int h = 1 + int(blockIdx.x % unsigned(pp.pools));  // this CTA's pool: frames h, h + pools, ...
     while (h < pp.n) {
         if (threadIdx.x == 0) ticket = atomicAdd(pp.ctr + h, 1);
         __syncthreads();
         const int t = ticket;
         if (t >= pp.nitems) {
-            h += 2;  // every ticket of frame h is dealt: the pool's next frame
+            h += pp.pools;  // every ticket of frame h is dealt: the pool's next frame
             __syncthreads();
             continue;
         }
@@ -2017,6 +2036,8 @@ __global__ void __launch_bounds__(32 * ME_WIDE_WARPS, ME_MIN_BLOCKS)
             if (threadIdx.x == 0) {
                 bwait.flags = pp.flags + pp.fstride * (h - 1) + pp.band_off;
                 bwait.nbands = pp.nbands;
+                bwait.nseg = pp.nseg;
+                bwait.segw = 16 * pp.segw;
                 bwait.epoch = epoch;
                 bwait.limit = spin_limit;
                 bwait.status = status;
@@ -2038,7 +2059,7 @@ __global__ void __launch_bounds__(32 * ME_WIDE_WARPS, ME_MIN_BLOCKS)
                 }
             }
         } else {
-            pipe_band(pp, h, -item - 1, epoch, status, spin_limit);
+            pipe_band(pp, h, (-item - 1) / pp.nseg, (-item - 1) % pp.nseg, epoch, status, spin_limit);
         }
         __syncthreads();  // the window and shared state are free for the next ticket
     }
@@ -2714,12 +2735,18 @@ int h264a::closed_pipe_run(h264a_ctx* ctx, const ClosedPipeIn& in, const h264a_m
     std::vector<RecDesc> rds(n);
     memset(fds.data(), 0, sizeof(FrameDesc) * n);
     memset(rds.data(), 0, sizeof(RecDesc) * n);
-    CUtensorMap maps[4];
-    int maps_ok[4];
-    for (int k = 0; k < 4; k++) maps_ok[k] = encode_window_map(&maps[k], in.planes + pbytes * k, pw, ph);
+    // the plane buffers (frame h's planes in buffer h % nbuf), the column
+    // segments of the bands, the CTA pools
+    const int nbuf = std::min(n, H264A_CLOSED_PLANE_PICTURES);
+    const int segw = PIPE_SEGW, nseg = (mb_w + segw - 1) / segw;
+    const int pools = std::min(PIPE_POOLS, n - 1);
+    if (pad % 4) return fail(H264A_E_ARG, "closed loop: the plane padding must be a multiple of 4");
+    std::vector<CUtensorMap> maps(nbuf);
+    std::vector<int> maps_ok(nbuf);
+    for (int k = 0; k < nbuf; k++) maps_ok[k] = encode_window_map(&maps[k], in.planes + pbytes * k, pw, ph);
     for (int h = 1; h < n; h++) {
         FrameDesc& d = fds[h];
-        const int buf = (h - 1) & 3;
+        const int buf = (h - 1) % nbuf;
         d.tmap = maps[buf];
         d.tmap_ok = maps_ok[buf];
         d.pic = h264a_picture{in.y + fs * h, in.planes + pbytes * buf, cw, ch, pad};
@@ -2751,20 +2778,23 @@ int h264a::closed_pipe_run(h264a_ctx* ctx, const ClosedPipeIn& in, const h264a_m
         r.th = db_thresholds(in.qp, 0, 0, 0);
     }
     // a frame's tickets: its MBs in wavefront order (anti-diagonals t = x + 2y,
-    // then y), and band b after the last MB of MB row min(b + 1, mb_h - 1)
+    // then y), and segment (b, s) right after MB (min(segw*(s+1), mb_w-1),
+    // min(b+1, mb_h-1)), segments of one MB in (b, s) order
+    std::vector<std::vector<int>> trig(nmb);
+    for (int b = 0; b < nbands; b++)
+        for (int sg = 0; sg < nseg; sg++)
+            trig[std::min(b + 1, mb_h - 1) * mb_w + std::min(segw * (sg + 1), mb_w - 1)].push_back(-(1 + b * nseg + sg));
     std::vector<int> items;
-    items.reserve(nmb + nbands);
+    items.reserve(nmb + nbands * nseg);
     for (int t = 0; t <= (mb_w - 1) + 2 * (mb_h - 1); t++) {
         for (int y = 0; y < mb_h; y++) {
             const int x = t - 2 * y;
             if (x < 0 || x >= mb_w) continue;
             items.push_back(y * mb_w + x);
-            if (x == mb_w - 1)
-                for (int b = 0; b < nbands; b++)
-                    if (std::min(b + 1, mb_h - 1) == y) items.push_back(-(b + 1));
+            for (int it : trig[y * mb_w + x]) items.push_back(it);
         }
     }
-    if ((int)items.size() != nmb + nbands) return fail(H264A_E_ARG, "closed loop: internal ticket layout error");
+    if ((int)items.size() != nmb + nbands * nseg) return fail(H264A_E_ARG, "closed loop: internal ticket layout error");
     const size_t b_fd = sizeof(FrameDesc) * n, b_rd = (sizeof(RecDesc) * n + 63) & ~size_t(63),
                  b_it = sizeof(int) * items.size();
     char* hst = nullptr;
@@ -2788,10 +2818,14 @@ int h264a::closed_pipe_run(h264a_ctx* ctx, const ClosedPipeIn& in, const h264a_m
     pp.mb_w = mb_w;
     pp.mb_h = mb_h;
     pp.nbands = nbands;
+    pp.nseg = nseg;
+    pp.segw = segw;
+    pp.nbuf = nbuf;
+    pp.pools = pools;
     pp.ew_off = 0;
     pp.dfl_off = 2 * EW_PER_MB * nmb;
     pp.band_off = pp.dfl_off + nmb;
-    pp.fstride = (pp.band_off + nbands + 1) & ~1LL;
+    pp.fstride = (pp.band_off + (long long)nbands * nseg + 1) & ~1LL;
     const long long head = (2LL * n + 1) & ~1LL;
     const long long need = head + pp.fstride * n;
     if (need >= (1LL << 31)) return fail(H264A_E_ARG, "closed loop: too many macroblocks for one launch");
@@ -2818,8 +2852,8 @@ int h264a::closed_pipe_run(h264a_ctx* ctx, const ClosedPipeIn& in, const h264a_m
     const int epoch = next_epoch(ctx, st, Q_WIDE);
     if (epoch < 0) return H264A_E_CUDA;
     long long blocks = (long long)ctx->num_sms * per_sm;
-    blocks &= ~1LL;  // the two pools, even and odd blocks
-    if (blocks < 2) blocks = 2;
+    blocks -= blocks % pools;  // an equal share of CTAs per pool
+    if (blocks < pools) blocks = pools;
     const bool bal = balanced_preset(prm), learn = in.props != nullptr;
     const size_t sm = WIN_BYTES;
     if (learn && bal)

@@ -1309,7 +1309,7 @@ def test_closed_frames_device_path_equals_host_path(acc):
     want = acc.pixel_path_closed(Y, U, V, params, lam, gate, qp)
     dy, du, dv = dev(acc, Y), dev(acc, U), dev(acc, V)
     ry, ru, rv = torch.empty_like(dy), torch.empty_like(du), torch.empty_like(dv)
-    planes = acc.empty((16 * (cw + 64) * (ch + 64),), torch.uint8)
+    planes = acc.empty((A.closed_plane_bytes(n, cw, ch),), torch.uint8)
     pk = acc.empty((n, nmb, 6), torch.int32)
     co = acc.empty((n, nmb, 2), torch.int64)
     lv = acc.empty((n, nmb, 256), torch.int16)
