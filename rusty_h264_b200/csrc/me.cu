@@ -1197,7 +1197,13 @@ constexpr int ME_MAXF = 96;
 constexpr int ME_WIDE_MAXF = 2;
 // The pipelined closed loop: the width of a band's column segments in MBs,
 // and the number of CTA pools (frames dealt round-robin to them).
-constexpr int PIPE_SEGW = 8, PIPE_POOLS = 8;
+#ifndef PIPE_SEGW_MBS
+#define PIPE_SEGW_MBS 8
+#endif
+#ifndef PIPE_POOL_COUNT
+#define PIPE_POOL_COUNT 8
+#endif
+constexpr int PIPE_SEGW = PIPE_SEGW_MBS, PIPE_POOLS = PIPE_POOL_COUNT;
 struct FrameBatch {
     FrameDesc f[ME_MAXF];
     long long seg_start[ME_MAXF + 1];
