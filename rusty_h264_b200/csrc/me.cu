@@ -777,6 +777,20 @@ struct Knobs {
 // (eval_round_group) into the team's shared distortions cdist[2][32], one
 // named barrier (1 + the team's index) per round, the two halves alternating
 // by round.
+// Named barrier `id` (1..4) over a team of TW warps.  The barrier index is
+// an immediate in each branch, so the compiler reserves barriers 1..4 only
+// (an index in a register reserves all 16, and the barrier count then caps
+// the CTAs per SM).
+template <int TW>
+__device__ __forceinline__ void team_sync(int id) {
+    switch (id) {
+        case 1: asm volatile("bar.sync 1, %0;" ::"n"(32 * TW) : "memory"); break;
+        case 2: asm volatile("bar.sync 2, %0;" ::"n"(32 * TW) : "memory"); break;
+        case 3: asm volatile("bar.sync 3, %0;" ::"n"(32 * TW) : "memory"); break;
+        default: asm volatile("bar.sync 4, %0;" ::"n"(32 * TW) : "memory"); break;
+    }
+}
+
 template <bool BAL, bool LEARN = false, int RF = RING_FIRST, int RR = RING_REST, int TW = 1>
 __device__ __forceinline__ void motion_search_group(const GroupGeom& q, const MeParamsDev& prm, WarpScratch& ws,
                                                     const int* preds, int npred, double lambda_me, int& out_x,
@@ -957,7 +971,7 @@ __device__ __forceinline__ void motion_search_group(const GroupGeom& q, const Me
 
         // ---------- price ----------
         eval_round_group<BAL, TW>(q, ws, n, metric, dist);
-        if (COOP) asm volatile("bar.sync %0, %1;" ::"r"(team_bar), "r"(32 * TW) : "memory");
+        if (COOP) team_sync<TW>(team_bar);
         int cc = INT_MAX;  // dist + λ·rate of slot gb + gl, as lane_cost prices it
         if (gl < n) {
             const int2 mv = ws.cand[gb + gl];
@@ -2009,8 +2023,11 @@ __device__ __forceinline__ void pipe_band(const PipeParams& pp, int h, int b, in
     }
 }
 
+#ifndef PIPE_MIN_BLOCKS
+#define PIPE_MIN_BLOCKS ME_MIN_BLOCKS
+#endif
 template <bool BAL, bool LEARN>
-__global__ void __launch_bounds__(32 * ME_WIDE_WARPS, ME_MIN_BLOCKS)
+__global__ void __launch_bounds__(32 * ME_WIDE_WARPS, PIPE_MIN_BLOCKS)
     closed_pipe_kernel(const __grid_constant__ PipeParams pp, const __grid_constant__ MeParamsDev prm, int epoch,
                        int* __restrict__ status, int spin_limit) {
     __shared__ __align__(8) unsigned long long win_bar;
