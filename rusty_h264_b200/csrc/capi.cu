@@ -148,6 +148,7 @@ extern "C" int h264a_ctx_destroy(h264a_ctx* ctx) {
     if (ctx->me_tab_ev) cudaEventDestroy(ctx->me_tab_ev);
     if (ctx->pp_row_count) cudaFree(ctx->pp_row_count);
     if (ctx->pp_rows_host) cudaFreeHost(ctx->pp_rows_host);
+    if (ctx->upl_tok) cudaFreeHost(ctx->upl_tok);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
     if (ctx->la_stream) cudaStreamDestroy(ctx->la_stream);

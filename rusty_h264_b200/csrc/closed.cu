@@ -27,6 +27,8 @@ using namespace h264a;
 
 namespace {
 
+constexpr int UPL_CHUNK = 4;  // frames per source upload of h264a_pixel_path_closed
+
 int check_geometry(int n, int cw, int ch, int qp, int dz_div) {
     if (n < 1 || cw < 16 || ch < 16 || cw % 16 || ch % 16 || (long long)cw * ch > (1LL << 26))
         return fail(H264A_E_ARG, "closed loop: frames must be MB-aligned and at least one");
@@ -48,7 +50,7 @@ int step_run(h264a_ctx* ctx, const h264a_closed_step& s, const h264a_me_params& 
 
 // The per-frame launches of the loop on device buffers (checked by the caller).
 int closed_run(h264a_ctx* ctx, const h264a_closed_dev& j, const h264a_me_params& prm, cudaStream_t st,
-               int32_t* frame_words = nullptr, int32_t token = 0) {
+               int32_t* frame_words = nullptr, int32_t token = 0, const int32_t* arrive = nullptr) {
     const int n = j.n, cw = j.cw, ch = j.ch, pad = 32;
     const int nmb = (cw / 16) * (ch / 16);
     const size_t fs = size_t(cw) * ch, cs = fs / 4;
@@ -92,6 +94,8 @@ int closed_run(h264a_ctx* ctx, const h264a_closed_dev& j, const h264a_me_params&
     in.props = j.net ? j.d_props : nullptr;
     in.fallback = j.net ? j.d_fallback : nullptr;
     in.prop_t = j.fallback_t;
+    in.arrive = arrive;
+    in.atoken = token;
     rc = closed_pipe_run(ctx, in, &prm, st, frame_words, token);
     if (rc) return rc;
     return H264A_OK;
@@ -156,6 +160,7 @@ extern "C" int h264a_pixel_path_closed(h264a_ctx* ctx, const h264a_closed_job* j
     const size_t o_pl = part(size_t(4) * std::min(n, H264A_CLOSED_PLANE_PICTURES) * pw * ph), o_pk = part(sizeof(int32_t) * 6 * nmb * n);
     const size_t o_co = part(sizeof(int64_t) * 2 * nmb * n), o_lv = part(sizeof(int16_t) * 256 * nmb * n);
     const size_t o_cl = part(sizeof(int16_t) * 128 * nmb * n), o_tab = part(sizeof(uint16_t) * 4096);
+    const size_t o_arr = part(sizeof(int32_t) * n);
     size_t o_pr = 0, o_fb = 0, o_half = 0, o_la = 0;
     if (job->net) {
         o_pr = part(sizeof(int32_t) * 16 * nmb * n);
@@ -190,9 +195,16 @@ extern "C" int h264a_pixel_path_closed(h264a_ctx* ctx, const h264a_closed_job* j
     j.d_costs = reinterpret_cast<int64_t*>(b + o_co);
     j.d_coeffs = reinterpret_cast<int16_t*>(b + o_lv);
     j.d_ccoeffs = reinterpret_cast<int16_t*>(b + o_cl);
-    H264A_CUDA(cudaMemcpyAsync(const_cast<uint8_t*>(j.d_y), job->h_y, n * fs, cudaMemcpyHostToDevice, st));
-    H264A_CUDA(cudaMemcpyAsync(const_cast<uint8_t*>(j.d_u), job->h_u, n * cs, cudaMemcpyHostToDevice, st));
-    H264A_CUDA(cudaMemcpyAsync(const_cast<uint8_t*>(j.d_v), job->h_v, n * cs, cudaMemcpyHostToDevice, st));
+    // The sources: with a net, all of them before anything runs (the
+    // proposals of every frame come first); without, frame 0 before the
+    // loop and the others on the upload stream beside it, in chunks of
+    // UPL_CHUNK frames, each chunk followed by its frames' arrival words
+    // (copied from pinned host words holding the call's token), which the
+    // pipelined kernel waits for before it reads a frame's sources.
+    const int up_n = job->net ? n : 1;
+    H264A_CUDA(cudaMemcpyAsync(const_cast<uint8_t*>(j.d_y), job->h_y, up_n * fs, cudaMemcpyHostToDevice, st));
+    H264A_CUDA(cudaMemcpyAsync(const_cast<uint8_t*>(j.d_u), job->h_u, up_n * cs, cudaMemcpyHostToDevice, st));
+    H264A_CUDA(cudaMemcpyAsync(const_cast<uint8_t*>(j.d_v), job->h_v, up_n * cs, cudaMemcpyHostToDevice, st));
     h264a_me_params prm = *params;
     if (h_mv_cost_tab) {
         H264A_CUDA(cudaMemcpyAsync(b + o_tab, h_mv_cost_tab, sizeof(uint16_t) * 4096, cudaMemcpyHostToDevice, st));
@@ -219,8 +231,44 @@ extern "C" int h264a_pixel_path_closed(h264a_ctx* ctx, const h264a_closed_job* j
         return rc;
     }
     const int32_t token = next_pp_token(ctx);
-    rc = closed_run(ctx, j, prm, st, ctx->pp_rows_dev, token);
+    int32_t* arrive = job->net || n < 2 ? nullptr : reinterpret_cast<int32_t*>(b + o_arr);
+    cudaStream_t up = ctx->pf_stream;
+    if (arrive) {
+        if (ctx->upl_cap < size_t(n)) {
+            if (ctx->upl_tok) cudaFreeHost(ctx->upl_tok);
+            ctx->upl_tok = nullptr;
+            ctx->upl_cap = 0;
+            if (cudaHostAlloc(reinterpret_cast<void**>(&ctx->upl_tok), sizeof(int32_t) * n, cudaHostAllocDefault) !=
+                cudaSuccess) {
+                cudaGetLastError();
+                cudaStreamSynchronize(st);
+                return fail(H264A_E_NOMEM, "pixel_path_closed: cudaHostAlloc failed");
+            }
+            ctx->upl_cap = size_t(n);
+        }
+        for (int f = 0; f < n; f++) ctx->upl_tok[f] = token;  // the upload stream is idle: nothing reads them now
+        for (int f0 = 1; f0 < n; f0 += UPL_CHUNK) {
+            const int k = std::min(UPL_CHUNK, n - f0);
+            cudaError_t e = cudaMemcpyAsync(const_cast<uint8_t*>(j.d_y) + fs * f0, job->h_y + fs * f0, fs * k,
+                                            cudaMemcpyHostToDevice, up);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(const_cast<uint8_t*>(j.d_u) + cs * f0, job->h_u + cs * f0, cs * k,
+                                    cudaMemcpyHostToDevice, up);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(const_cast<uint8_t*>(j.d_v) + cs * f0, job->h_v + cs * f0, cs * k,
+                                    cudaMemcpyHostToDevice, up);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(arrive + f0, ctx->upl_tok + f0, sizeof(int32_t) * k, cudaMemcpyHostToDevice, up);
+            if (e != cudaSuccess) {
+                cudaStreamSynchronize(up);
+                cudaStreamSynchronize(st);
+                return cuda_fail(e, "pixel_path_closed: source uploads");
+            }
+        }
+    }
+    rc = closed_run(ctx, j, prm, st, ctx->pp_rows_dev, token, arrive);
     if (rc) {
+        cudaStreamSynchronize(up);
         cudaStreamSynchronize(st);
         return rc;
     }
@@ -249,6 +297,7 @@ extern "C" int h264a_pixel_path_closed(h264a_ctx* ctx, const h264a_closed_job* j
     auto drain = [&](int code) {
         cudaStreamSynchronize(copy);
         cudaStreamSynchronize(st);
+        cudaStreamSynchronize(up);
         return code;
     };
     // frame 0 (final before the kernel starts) goes with frame 1
@@ -282,5 +331,7 @@ extern "C" int h264a_pixel_path_closed(h264a_ctx* ctx, const h264a_closed_job* j
                                    copy));
     const cudaError_t e_cs = cudaStreamSynchronize(copy);
     if (e_cs != cudaSuccess) return drain(cuda_fail(e_cs, "pixel_path_closed: result downloads"));
+    const cudaError_t e_up = cudaStreamSynchronize(up);
+    if (e_up != cudaSuccess) return drain(cuda_fail(e_up, "pixel_path_closed: source uploads"));
     return h264a_sync(ctx, st);
 }

@@ -84,6 +84,10 @@ struct h264a_ctx {
     PpInput pp_in[PP_SLOTS];
     long long pp_seq = 0;
     cudaStream_t pf_stream = nullptr;
+    // pinned host words holding the current token, the source of the arrival
+    // words that h264a_pixel_path_closed's uploads write after each chunk
+    int32_t *upl_tok = nullptr;
+    size_t upl_cap = 0;
     // the batch runtime's autotuner: the launch shape found fastest for each
     // batch signature (resolutions, references, frames per step, preset)
     std::map<std::string, int> tune_cache;
@@ -148,6 +152,10 @@ struct ClosedPipeIn {
     const int32_t *props;
     int32_t *fallback;
     int32_t prop_t;
+    // arrival words (or null): frame h's sources are in device memory once
+    // arrive[h] == atoken (written by the host's upload stream after them)
+    const int32_t *arrive = nullptr;
+    int32_t atoken = 0;
 };
 // frame_words (device view of mapped host words, or null): word h is set to
 // `token` once every MB of frame h is final, for the host to start its

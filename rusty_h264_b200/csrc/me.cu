@@ -1980,6 +1980,8 @@ struct PipeParams {
     int cw, ch, pad, word_in, word_out;
     int32_t* frame_words;  // mapped host words: frame h's set to ftoken when it is final (or null)
     int32_t ftoken;
+    const int32_t* arrive;  // frame h's sources uploaded once arrive[h] == atoken (or null: all resident)
+    int32_t atoken;
 };
 
 // Segment (b, s) of frame h: the planes of its reconstruction for padded rows
@@ -2042,7 +2044,8 @@ __global__ void __launch_bounds__(32 * ME_WIDE_WARPS, PIPE_MIN_BLOCKS)
     }
     __syncthreads();
     uint32_t parity = 0;
-    int fenced = -1;  // the frame whose tensor maps this CTA has acquired
+    int fenced = -1;   // the frame whose tensor maps this CTA has acquired
+    int arrived = -1;  // the frame whose sources this CTA has seen uploaded
     int h = 1 + int(blockIdx.x % unsigned(pp.pools));  // this CTA's pool: frames h, h + pools, ...
     while (h < pp.n) {
         if (threadIdx.x == 0) ticket = atomicAdd(pp.ctr + h, 1);
@@ -2057,6 +2060,17 @@ __global__ void __launch_bounds__(32 * ME_WIDE_WARPS, PIPE_MIN_BLOCKS)
         int* const ff = pp.flags + pp.fstride * h;
         if (item >= 0) {
             if (threadIdx.x == 0) {
+                if (pp.arrive != nullptr && arrived != h) {
+                    // the frame's sources are still being uploaded beside the launch
+                    for (int it = 0; ld_acquire(pp.arrive + h) != pp.atoken; it++) {
+                        if (it >= spin_limit ||
+                            ((it & 255) == 255 && *reinterpret_cast<volatile int*>(status) != 0)) {
+                            atomicCAS(status, 0, 1);
+                            break;
+                        }
+                        __nanosleep(200);
+                    }
+                }
                 bwait.flags = pp.flags + pp.fstride * (h - 1) + pp.band_off;
                 bwait.nbands = pp.nbands;
                 bwait.nseg = pp.nseg;
@@ -2072,6 +2086,7 @@ __global__ void __launch_bounds__(32 * ME_WIDE_WARPS, PIPE_MIN_BLOCKS)
                                       h > 1 ? &bwait : nullptr, epoch, status, spin_limit, win, bar, parity,
                                       fenced != h);
             fenced = h;
+            arrived = h;
             __syncthreads();  // every read and write of the MB is done
             if (threadIdx.x == 0) {
                 const int c = atom_add_acq_rel(pp.done + h, 1);
@@ -2869,6 +2884,8 @@ int h264a::closed_pipe_run(h264a_ctx* ctx, const ClosedPipeIn& in, const h264a_m
     pp.word_out = (pw % 4 == 0) && ((reinterpret_cast<uintptr_t>(in.planes) & 3) == 0) && (pbytes % 4 == 0);
     pp.frame_words = frame_words;
     pp.ftoken = token;
+    pp.arrive = in.arrive;
+    pp.atoken = in.atoken;
     // counters zero, and no word of an earlier launch's layout left to be
     // mistaken for a flag of this one
     H264A_CUDA(cudaMemsetAsync(fl, 0, sizeof(int) * size_t(need), st));
