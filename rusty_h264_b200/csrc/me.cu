@@ -1212,7 +1212,7 @@ constexpr int ME_WIDE_MAXF = 2;
 // The pipelined closed loop: the width of a band's column segments in MBs,
 // and the number of CTA pools (frames dealt round-robin to them).
 #ifndef PIPE_SEGW_MBS
-#define PIPE_SEGW_MBS 8
+#define PIPE_SEGW_MBS 16
 #endif
 #ifndef PIPE_POOL_COUNT
 #define PIPE_POOL_COUNT 8
