@@ -7,9 +7,9 @@
 // every P frame in one launch of the pipelined kernel (closed_pipe_kernel,
 // me.cu): each MB's search (the wide kernel's), its MC + T/Q and
 // reconstruction of luma and chroma and its in-loop deblocking in the same
-// CTA, and the planes of each reconstruction built band by band as its MB
-// rows are deblocked, so that frame f's wavefront runs while frame f-1's is
-// still finishing the rows below the ones f reads.  With a proposal net the
+// CTA, and the planes of each reconstruction built segment by segment
+// (16 picture rows by 16 MB columns) as its MBs are deblocked, so that about
+// ten frames' wavefronts run at once, each a few MBs behind the one before.  With a proposal net the
 // proposals of all frames come first, in one batched h264a_mvnet_propose pass
 // over the source pairs (f, f-1).  One P frame alone is
 // h264a_closed_step_frame (the planes of rec(f-1) are the caller's).

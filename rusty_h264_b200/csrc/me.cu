@@ -43,9 +43,10 @@ constexpr int ME_WIDE_WARPS = 4;
 constexpr int ME_PART_TEAM = ME_WIDE_WARPS / 4;  // warps per partition search
 
 // The reference picture's readiness in the pipelined closed loop: its planes
-// are built band by band (MB rows of 16 picture rows; band b's flag == epoch
-// means bands 0..b are complete), and a search waits (bounded) for the band
-// of every row it reads.
+// are built segment by segment (16 picture rows by segw picture columns;
+// segment (b, s)'s flag == epoch means every segment up and left of it is
+// complete), and a search waits (bounded) for the segment of every pixel it
+// reads.
 struct BandWait {
     const int* flags;  // nbands x nseg readiness flags, band-major
     int nbands, nseg, segw, epoch, limit;
