@@ -527,8 +527,11 @@ H264A_API int h264a_batch_variant_shape(int variant, int *mbs_per_cta, int *stag
  * the search prices them on the reconstruction),
  * MC + T/Q and reconstruction of luma and chroma, and deblocking.  Each
  * frame's MBs run as a wavefront, and consecutive frames overlap in one
- * launch: an MB of frame f waits only for the bands (MB rows) of rec(f-1)
- * its search reads, whose planes are built as those rows are deblocked.
+ * launch: an MB of frame f waits only for the segments (16 rows by 16 MB
+ * columns) of rec(f-1) its search reads, whose planes are built as those
+ * MBs are deblocked, so about ten frames run at once.  From host buffers the
+ * sources of frames 1.. are uploaded beside the launch and each frame's
+ * outputs come down as it becomes final.
  * Inputs: n frames of luma
  * (cw x ch) and chroma (cw/2 x ch/2), contiguous, host memory.  Outputs per
  * frame (frame 0 rows zero): picks 6 i32/MB, costs 2 i64/MB, luma levels 256
