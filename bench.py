@@ -64,6 +64,8 @@ def parse():
     ap.add_argument("--learned-epochs", type=float, default=6.0)
     ap.add_argument("--no-closed", action="store_true", help="skip the closed-loop and BD-rate records")
     ap.add_argument("--bd-frames", type=int, default=16)
+    ap.add_argument("--gop-step", type=int, default=29,
+                    help="P frames of every stream per batched step (--mixed; 29: the clip's whole GOP)")
     ap.add_argument("--bd-4k", action="store_true",
                     help="also the BD-rate record on a 3840x2160 clip of the same generator (seed 2)")
     return ap.parse_args()
@@ -135,7 +137,7 @@ def mixed_inputs():
         return list(ex.map(mixed_stream, jobs))
 
 
-def mixed_batch(acc, torch, streams, params, lam: float, gate: int):
+def mixed_batch(acc, torch, streams, params, lam: float, gate: int, gop_step: int = 29):
     """Plain-ME (one reference) of every P frame of the mixed batch in one
     h264a_me_frames call: one persistent wavefront launch over all 464 frames,
     largest first (the frame table in device memory).  Every stream's
@@ -182,7 +184,7 @@ def mixed_batch(acc, torch, streams, params, lam: float, gate: int):
     ms = float(np.median(ts))
     px = sum((f.shape[0] - 1) * f.shape[1] * f.shape[2] for f in streams)
     mbs = sum((f.shape[0] - 1) * (f.shape[1] // 16) * (f.shape[2] // 16) for f in streams)
-    three = mixed_batch_3ref(acc, torch, bufs, params, lam, gate)
+    three = mixed_batch_3ref(acc, torch, bufs, params, lam, gate, gop_step)
     return bufs, {"streams": "4 x 352x288, 6 x 1280x720, 4 x 1920x1080, 2 x 3840x2160; 30 frames each, 1080p generator",
             "p_frames": len(frames_all), "macroblocks": int(mbs), "me_ms": round(ms, 3),
             "me_mpx_s": round(px / (ms * 1e-3) / 1e6, 1), "launches": 1,
@@ -192,21 +194,24 @@ def mixed_batch(acc, torch, streams, params, lam: float, gate: int):
                     "not part of value"}
 
 
-def mixed_batch_3ref(acc, torch, bufs, params, lam: float, gate: int) -> dict:
-    """The mixed batch through the batched runtime (h264a_batch_*): 8 P frames
-    of every stream per GOP step over up to three references (the previous
-    three source pictures, nearest first), each step one graph launch (the
-    planes of the step's frames, then one persistent launch over all 16
-    streams), in the launch shape the autotuner picked.  Every stream's picks
-    and costs must equal h264a_me_frames_multiref of that stream alone; the
-    four steps of the 29 P frames are timed with CUDA events (3 warm-up
-    passes, median of 5).  The tuner also runs on each resolution alone, to
-    report the shape it picks per resolution."""
+def mixed_batch_3ref(acc, torch, bufs, params, lam: float, gate: int, gop_step: int = 29) -> dict:
+    """The mixed batch through the batched runtime (h264a_batch_*): gop_step P
+    frames of every stream per step (29 by default: each stream's whole GOP,
+    one step) over up to three references (the previous three source
+    pictures, nearest first), each step one graph launch (the planes of the
+    step's frames, then one persistent launch over all 16 streams), in the
+    launch shape the autotuner picked.  Every stream's picks and costs must
+    equal h264a_me_frames_multiref of that stream alone; the steps of the 29 P
+    frames are timed with CUDA events (3 warm-up passes, median of 5).  The
+    tuner also runs on each resolution alone, to report the shape it picks
+    per resolution."""
     import ctypes as C
 
     from rusty_h264_b200 import accel as A
 
-    G, NSLOTS, NREF, PAD = 8, 32, 3, 32
+    NREF, PAD = 3, 32
+    G = gop_step
+    NSLOTS = -(-max(32, G + NREF + 1) // G) * G  # a multiple of G with room for a step and its references
     rings, streams, alone = [], [], []
     for d, _, _, _ in bufs:
         n, ch, cw = d.shape
@@ -262,7 +267,7 @@ def mixed_batch_3ref(acc, torch, bufs, params, lam: float, gate: int) -> dict:
     for w, h, _ in MIXED:
         sub = [st for st in streams if (st.cw, st.ch) == (w, -(-h // 16) * 16)]
         bs = acc.batch_create(sub, A.BatchConfig(G, NSLOTS, NREF, 1, 0), params)
-        bs.step(1, G)
+        bs.step(0, min(G, nmax - 1))
         acc.sync()
         inf = bs.info()
         bs.close()
@@ -1215,7 +1220,7 @@ def run_ours(args, ws, rank, local):
                                           "(7 P frames) + lookahead, one thread",
                                 "cpu": cpu_model(), "stages": cpu_stages(sample, lam, gate)}
     if args.mixed and rank == 0:
-        mixed_bufs, line["mixed_batch"] = mixed_batch(acc, torch, mixed_streams, params, lam, gate)
+        mixed_bufs, line["mixed_batch"] = mixed_batch(acc, torch, mixed_streams, params, lam, gate, args.gop_step)
     if not args.no_learned and rank == 0:
         from rusty_h264_b200 import bdrate
 
