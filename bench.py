@@ -195,13 +195,14 @@ def mixed_batch(acc, torch, streams, params, lam: float, gate: int, gop_step: in
 
 
 def mixed_batch_3ref(acc, torch, bufs, params, lam: float, gate: int, gop_step: int = 29) -> dict:
-    """The mixed batch through the batched runtime (h264a_batch_*): gop_step P
-    frames of every stream per step (29 by default: each stream's whole GOP,
+    """The mixed batch through the batched runtime (h264a_batch_*), search and
+    MC + luma T/Q at QP 27: gop_step P frames of every stream per step (29 by default: each stream's whole GOP,
     one step) over up to three references (the previous three source
     pictures, nearest first), each step one graph launch (the planes of the
     step's frames, then one persistent launch over all 16 streams), in the
-    launch shape the autotuner picked.  Every stream's picks and costs must
-    equal h264a_me_frames_multiref of that stream alone; the steps of the 29 P
+    launch shape the autotuner picked.  Every stream's picks, costs and levels
+    must equal h264a_me_frames_multiref + h264a_mc_tq_frames_multiref of that
+    stream alone; the steps of the 29 P
     frames are timed with CUDA events (3 warm-up passes, median of 5).  The
     tuner also runs on each resolution alone, to report the shape it picks
     per resolution."""
@@ -209,7 +210,7 @@ def mixed_batch_3ref(acc, torch, bufs, params, lam: float, gate: int, gop_step: 
 
     from rusty_h264_b200 import accel as A
 
-    NREF, PAD = 3, 32
+    NREF, PAD, QP = 3, 32, 27
     G = gop_step
     NSLOTS = -(-max(32, G + NREF + 1) // G) * G  # a multiple of G with room for a step and its references
     rings, streams, alone = [], [], []
@@ -222,11 +223,12 @@ def mixed_batch_3ref(acc, torch, bufs, params, lam: float, gate: int, gop_step: 
         planes = torch.zeros((NSLOTS, pb), dtype=torch.uint8, device="cuda")
         picks = torch.zeros((NSLOTS, nmb, 8), dtype=torch.int32, device="cuda")
         costs = torch.zeros((NSLOTS, nmb, 2), dtype=torch.int64, device="cuda")
-        rings.append((src, planes, picks, costs, n))
+        levels = torch.zeros((NSLOTS, nmb, 256), dtype=torch.int16, device="cuda")
+        rings.append((src, planes, picks, costs, n, levels))
         streams.append(A.BatchStream(cw, ch, PAD, src.data_ptr(), planes.data_ptr(), picks.data_ptr(),
-                                     costs.data_ptr(), lam, gate))
+                                     costs.data_ptr(), lam, gate, levels.data_ptr(), QP, 6))
     # the unbatched path: each stream's P frames in one h264a_me_frames_multiref call
-    for src, planes, picks, costs, n in rings:
+    for src, planes, picks, costs, n, levels in rings:
         ch, cw = src.shape[1], src.shape[2]
         acc.hpel_build(src[: n - 1], PAD, out=planes[: n - 1])
         fr = []
@@ -236,9 +238,13 @@ def mixed_batch_3ref(acc, torch, bufs, params, lam: float, gate: int, gop_step: 
             fr.append(A.MeMrFrame(src[f].data_ptr(), (C.c_void_p * 4)(*refs), nref, cw, ch, PAD, lam, gate,
                                   picks[f].data_ptr(), costs[f].data_ptr()))
         acc.me_frames_multiref(fr, params)
+        tq = [A.McTqMrFrame(m.d_src, m.d_planes, m.nref, cw, ch, PAD, m.d_picks, QP, 6, levels[f].data_ptr())
+              for f, m in zip(range(1, n), fr)]
+        acc.mc_tq_frames_multiref(tq)
         acc.sync()
-        alone.append((picks[1:n].clone(), costs[1:n].clone()))
+        alone.append((picks[1:n].clone(), costs[1:n].clone(), levels[1:n].clone()))
         picks.zero_()
+        levels.zero_()
         costs.zero_()
         planes.zero_()
     nmax = max(r[4] for r in rings)
@@ -247,7 +253,8 @@ def mixed_batch_3ref(acc, torch, bufs, params, lam: float, gate: int, gop_step: 
     for k, count in steps:
         b.step(k, count)
     acc.sync()
-    for s, (src, planes, picks, costs, n) in enumerate(rings):
+    for s, (src, planes, picks, costs, n, levels) in enumerate(rings):
+        assert torch.equal(levels[1:n], alone[s][2]), f"stream {s}: batched levels != alone"
         assert torch.equal(picks[1:n], alone[s][0]) and torch.equal(costs[1:n], alone[s][1]), \
             f"stream {s}: batched steps != alone"
     ts = []
@@ -279,6 +286,7 @@ def mixed_batch_3ref(acc, torch, bufs, params, lam: float, gate: int, gop_step: 
     px = sum((r[4] - 1) * r[0].shape[1] * r[0].shape[2] for r in rings)
     return {"me_3ref_ms": round(ms, 3), "me_3ref_mpx_s": round(px / (ms * 1e-3) / 1e6, 1),
             "gop_step": G, "graph_launches": len(steps), "batched_equals_alone_3ref": True,
+            "with_mc_tq": "each step also runs the MC + luma T/Q (QP 27) of its frames, levels checked too",
             "autotune": {"variant": info["variant"], "mbs_per_cta": shape[0], "staged_window": shape[1],
                          "ms_per_variant": info["ms"], "graphs": info["graphs"], "per_resolution": per_res}}
 

@@ -455,6 +455,20 @@ typedef struct {
 } h264a_me_mr_frame;
 H264A_API int h264a_me_frames_multiref(h264a_ctx *ctx, const h264a_me_mr_frame *h_frames, int nframes,
                                        const h264a_me_params *params, void *stream);
+/* h264a_mc_tq_frames for multi-reference picks (8 i32 per MB, as
+ * h264a_me_frames_multiref writes them): each half of an MB is predicted
+ * from the planes of its own reference (mb16.rs:3436-3450 with best_part's
+ * reference, mb16.rs:4921-4960), then the luma T/Q; 256 i16 per MB. */
+typedef struct {
+    const uint8_t *d_src;
+    const uint8_t *d_planes[4];
+    int32_t nref, cw, ch, pad;
+    const int32_t *d_picks;
+    int32_t qp, dz_div;
+    int16_t *d_coeffs;
+} h264a_mc_tq_mr_frame;
+H264A_API int h264a_mc_tq_frames_multiref(h264a_ctx *ctx, const h264a_mc_tq_mr_frame *h_frames, int nframes,
+                                          void *stream);
 
 /* ---- batched plain-ME over many streams, one launch per GOP step ----------------- */
 /* Many streams of uneven resolution advance together, G P frames of every
@@ -467,6 +481,9 @@ H264A_API int h264a_me_frames_multiref(h264a_ctx *ctx, const h264a_me_mr_frame *
  * a CUDA graph captured the first time its slot layout occurs and replayed
  * afterwards (one graph launch per step).  Picks and costs are those of
  * h264a_me_frames_multiref on the same frames (8 i32 and 2 i64 per MB).
+ * Streams with d_coeffs (a ring of nslots x nmb x 256 i16, 16-byte aligned)
+ * also get each frame's MC + luma T/Q at qp (h264a_mc_tq_frames_multiref,
+ * one launch in the same graph after the search; one dz_div per batch).
  * Each stream owns a ring of nslots slots; frame f lives in slot f % nslots
  * of d_src (cw*ch bytes per slot, 4-byte aligned), d_planes (4*pw*ph bytes
  * per slot, pw = cw + 2*pad; 16-byte aligned with pw a multiple of 16 for the
@@ -489,6 +506,8 @@ typedef struct {
     int64_t *d_costs;
     double lambda_me;
     int64_t split_gate;
+    int16_t *d_coeffs; /* NULL: search only */
+    int32_t qp, dz_div;
 } h264a_batch_stream;
 typedef struct {
     int32_t gop_step; /* G >= 1 */

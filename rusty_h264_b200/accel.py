@@ -151,7 +151,14 @@ def closed_plane_bytes(n: int, cw: int, ch: int, pad: int = 32) -> int:
 class BatchStream(C.Structure):
     _fields_ = [("cw", C.c_int32), ("ch", C.c_int32), ("pad", C.c_int32), ("d_src", C.c_void_p),
                 ("d_planes", C.c_void_p), ("d_picks", C.c_void_p), ("d_costs", C.c_void_p),
-                ("lambda_me", C.c_double), ("split_gate", C.c_int64)]
+                ("lambda_me", C.c_double), ("split_gate", C.c_int64), ("d_coeffs", C.c_void_p),
+                ("qp", C.c_int32), ("dz_div", C.c_int32)]
+
+
+class McTqMrFrame(C.Structure):
+    _fields_ = [("d_src", C.c_void_p), ("d_planes", C.c_void_p * 4), ("nref", C.c_int32), ("cw", C.c_int32),
+                ("ch", C.c_int32), ("pad", C.c_int32), ("d_picks", C.c_void_p), ("qp", C.c_int32),
+                ("dz_div", C.c_int32), ("d_coeffs", C.c_void_p)]
 
 
 class BatchConfig(C.Structure):
@@ -179,7 +186,7 @@ EXPORTS = (
     "h264a_me_frames_learned", "h264a_pixel_path_closed", "h264a_write_stream_cavlc", "h264a_cavlc_table_code",
     "h264a_closed_frames", "h264a_closed_step_frame", "h264a_me_frames_multiref",
     "h264a_batch_create", "h264a_batch_step", "h264a_batch_get_info", "h264a_batch_destroy",
-    "h264a_batch_variant_shape", "h264a_lookahead_streams",
+    "h264a_batch_variant_shape", "h264a_lookahead_streams", "h264a_mc_tq_frames_multiref",
 )
 
 _lib = None
@@ -230,6 +237,7 @@ def load_library() -> C.CDLL:
     L.h264a_closed_step_frame.argtypes = [vp, C.POINTER(ClosedStep), C.POINTER(MeParams), vp]
     L.h264a_me_frames_multiref.argtypes = [vp, vp, C.c_int, C.POINTER(MeParams), vp]
     L.h264a_lookahead_streams.argtypes = [vp, vp, i32, i32, vp]
+    L.h264a_mc_tq_frames_multiref.argtypes = [vp, vp, i32, vp]
     L.h264a_batch_create.argtypes = [vp, vp, i32, C.POINTER(BatchConfig), C.POINTER(MeParams), C.POINTER(vp)]
     L.h264a_batch_step.argtypes = [vp, i64, i32, vp]
     L.h264a_batch_get_info.argtypes = [vp, C.POINTER(BatchInfo)]
@@ -429,6 +437,12 @@ class Accel:
         arr = (MeMrFrame * len(frames))(*frames)
         self._check(self.L.h264a_me_frames_multiref(self.ctx, C.cast(arr, C.c_void_p), len(frames), C.byref(params),
                                                     self._stream()))
+
+    def mc_tq_frames_multiref(self, frames: Sequence[McTqMrFrame]):
+        """MC + luma T/Q of multi-reference picks (h264a_mc_tq_frames_multiref)."""
+        arr = (McTqMrFrame * len(frames))(*frames)
+        self._check(self.L.h264a_mc_tq_frames_multiref(self.ctx, C.cast(arr, C.c_void_p), len(frames),
+                                                       self._stream()))
 
     def lookahead_streams(self, streams: Sequence[LaStream], mode: int = 2):
         """h264a_lookahead_costs of several streams in one launch (h264a_lookahead_streams)."""

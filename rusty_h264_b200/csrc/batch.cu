@@ -9,7 +9,9 @@
 // stream) and then one launch of the multi-reference frame kernel (me.cu,
 // me_frames_mr_kernel) over frames kG+1..kG+count of all streams, largest
 // frames first in one work queue, so the small streams' MBs fill the SMs the
-// large frames' wavefronts leave idle.
+// large frames' wavefronts leave idle; for the streams that ask for it, the
+// MC + luma T/Q of those frames follows in the same graph (one launch of
+// tq.cu's MC kernel, each half predicted from its own reference).
 //
 // Every stream keeps its frames in a ring of nslots slots (frame f in slot
 // f % nslots), so the frame table of a step depends only on the slot of
@@ -121,6 +123,34 @@ int step_search(h264a_batch* b, int variant, const MrTable& t, const void* d_tab
     return mr_launch(b->ctx, variant, prm, d_table, t, b->d_q, b->d_q + BQ_COUNTER_INTS, 1, st);
 }
 
+// The MC + luma T/Q of frames kG+1..kG+count of the streams with
+// coefficient rings, from the picks the search just wrote.
+int step_tq(h264a_batch* b, int64_t k, int count, cudaStream_t st) {
+    const int G = b->cfg.gop_step, ns = b->cfg.nslots;
+    std::vector<h264a_mc_tq_mr_frame> fr;
+    for (const h264a_batch_stream& s : b->s) {
+        if (!s.d_coeffs) continue;
+        const size_t fs = size_t(s.cw) * s.ch, pb = plane_bytes(s), nmb = size_t(nmb_of(s));
+        for (int i = 1; i <= count; i++) {
+            const int64_t f = k * G + i;
+            h264a_mc_tq_mr_frame m;
+            memset(&m, 0, sizeof m);
+            const size_t slot = size_t(f % ns);
+            m.d_src = s.d_src + slot * fs;
+            m.nref = int(std::min<int64_t>(b->cfg.nref, f));
+            for (int r = 0; r < m.nref; r++) m.d_planes[r] = s.d_planes + size_t((f - 1 - r) % ns) * pb;
+            m.cw = s.cw; m.ch = s.ch; m.pad = s.pad;
+            m.d_picks = s.d_picks + slot * 8 * nmb;
+            m.qp = s.qp;
+            m.dz_div = s.dz_div;
+            m.d_coeffs = s.d_coeffs + slot * 256 * nmb;
+            fr.push_back(m);
+        }
+    }
+    if (fr.empty()) return H264A_OK;
+    return mc_tq_mr_run(b->ctx, fr.data(), int(fr.size()), st);
+}
+
 int upload_table(StepGraph& g) {
     if (cudaMalloc(&g.d_table, g.table.bytes.size()) != cudaSuccess) {
         cudaGetLastError();
@@ -180,6 +210,7 @@ int capture(h264a_batch* b, int64_t k, int count, StepGraph& g) {
     H264A_CUDA(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeRelaxed));
     int rc = step_planes(b, k, count, b->cap);
     if (!rc) rc = step_search(b, b->variant, g.table, g.d_table, b->cap);
+    if (!rc) rc = step_tq(b, k, count, b->cap);
     cudaGraph_t graph = nullptr;
     const cudaError_t e = cudaStreamEndCapture(b->cap, &graph);
     if (rc) {
@@ -223,6 +254,9 @@ extern "C" int h264a_batch_create(h264a_ctx* ctx, const h264a_batch_stream* stre
             return fail(H264A_E_ARG, "batch_create: streams must be MB-aligned with 3 <= pad <= 128");
         if (reinterpret_cast<uintptr_t>(s.d_src) & 3)
             return fail(H264A_E_ARG, "batch_create: source rings must be 4-byte aligned");
+        if (s.d_coeffs && ((reinterpret_cast<uintptr_t>(s.d_coeffs) & 15) || s.qp < 0 || s.qp > 51 || s.dz_div < 1 ||
+                           s.dz_div != streams[0].dz_div))
+            return fail(H264A_E_ARG, "batch_create: coefficient rings 16-byte aligned, qp 0..51, one dz_div >= 1");
         total += (long long)nmb_of(s) * G;
         char buf[48];
         snprintf(buf, sizeof buf, "%dx%d", s.cw, s.ch);

@@ -187,6 +187,8 @@ struct MrTable {
     long long total = 0;  // MBs
     size_t b_desc = 0, b_seg = 0;
 };
+// h264a_mc_tq_frames_multiref on stream st (checks its arguments)
+int mc_tq_mr_run(h264a_ctx *ctx, const h264a_mc_tq_mr_frame *h_frames, int nframes, cudaStream_t st);
 // validates h_frames as h264a_me_frames_multiref does and lays out their table
 int mr_table_build(const h264a_me_mr_frame *h_frames, int nframes, MrTable &t);
 // one launch of the multi-reference kernel in launch shape `variant` over the

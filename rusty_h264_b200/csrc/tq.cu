@@ -133,6 +133,11 @@ struct TqFrameDesc {
     int mb_w;
     int nmb;
     uint8_t* rec;  // cw x ch luma reconstruction, or nullptr
+    // multi-reference picks (8 i32 per MB: shape, then reference index and
+    // MV of each half) predict each half from rplanes[its reference];
+    // stride 6: single-reference picks, pic.d_planes
+    const uint8_t* rplanes[4];
+    int stride;
 };
 
 constexpr int TQ_MAXF = 96;
@@ -156,11 +161,20 @@ __global__ void mc_tq_frames_kernel(const __grid_constant__ TqBatch batch, long 
     const int blk = int(t & 15);
     const int bx = (blk & 3) * 4, by = (blk >> 2) * 4;  // 4x4 block inside the MB
     const int mbx = m % fd.mb_w, mby = m / fd.mb_w;
-    const int32_t* pk = fd.picks + 6 * m;
+    const int32_t* pk = fd.picks + fd.stride * m;
     const int shape = pk[0];
     const int part = shape == 1 ? (by >= 8) : (shape == 2 ? (bx >= 8) : 0);
-    const int mvx = pk[1 + 2 * part], mvy = pk[2 + 2 * part];
-    Planes P{fd.pic.d_planes, fd.pic.cw + 2 * fd.pic.pad, fd.pic.ch + 2 * fd.pic.pad, fd.pic.pad, 0};
+    int mvx, mvy;
+    const uint8_t* planes = fd.pic.d_planes;
+    if (fd.stride == 8) {
+        planes = fd.rplanes[pk[1 + 3 * part] & 3];
+        mvx = pk[2 + 3 * part];
+        mvy = pk[3 + 3 * part];
+    } else {
+        mvx = pk[1 + 2 * part];
+        mvy = pk[2 + 2 * part];
+    }
+    Planes P{planes, fd.pic.cw + 2 * fd.pic.pad, fd.pic.ch + 2 * fd.pic.pad, fd.pic.pad, 0};
     P.ps = (long long)P.pw * P.ph;
     const int x = mbx * 16 + bx, y = mby * 16 + by;
     uint32_t s[4], p[4];
@@ -299,7 +313,7 @@ static int mc_tq_launch(h264a_ctx* ctx, const h264a_tq_frame* h_frames, uint8_t*
         for (int k = 0; k < gn; k++) {
             const h264a_tq_frame& f = h_frames[g0 + k];
             b.f[k] = {f.pic, f.d_picks, f.qp, f.d_coeffs, f.pic.cw / 16, (f.pic.cw / 16) * (f.pic.ch / 16),
-                      recs ? recs[g0 + k] : nullptr};
+                      recs ? recs[g0 + k] : nullptr, {nullptr, nullptr, nullptr, nullptr}, 6};
             b.mb_base[k] = int(total);
             total += b.f[k].nmb;
         }
@@ -309,6 +323,58 @@ static int mc_tq_launch(h264a_ctx* ctx, const h264a_tq_frame* h_frames, uint8_t*
         if (rc) return rc;
     }
     return H264A_OK;
+}
+
+int h264a::mc_tq_mr_run(h264a_ctx* ctx, const h264a_mc_tq_mr_frame* h_frames, int nframes, cudaStream_t st) {
+    if (!ctx || !h_frames || nframes < 1) return fail(H264A_E_ARG, "mc_tq_frames_multiref: bad arguments");
+    const int dz = h_frames[0].dz_div;
+    for (int i = 0; i < nframes; i++) {
+        const h264a_mc_tq_mr_frame& f = h_frames[i];
+        if (!f.d_src || !f.d_picks || !f.d_coeffs) return fail(H264A_E_ARG, "mc_tq_frames_multiref: null frame pointer");
+        if (f.nref < 1 || f.nref > 4) return fail(H264A_E_ARG, "mc_tq_frames_multiref: 1 to 4 references per frame");
+        for (int r = 0; r < f.nref; r++)
+            if (!f.d_planes[r]) return fail(H264A_E_ARG, "mc_tq_frames_multiref: null reference planes");
+        if (f.cw < 16 || f.ch < 16 || f.cw % 16 || f.ch % 16 || f.pad < 3 || f.pad > 128)
+            return fail(H264A_E_ARG, "mc_tq_frames_multiref: frames must be MB-aligned with 3 <= pad <= 128");
+        if (f.dz_div != dz || dz < 1) return fail(H264A_E_ARG, "mc_tq_frames_multiref: one dz_div >= 1 per call");
+        if (((reinterpret_cast<uintptr_t>(f.d_coeffs) & 15) | (reinterpret_cast<uintptr_t>(f.d_src) & 3)) != 0)
+            return fail(H264A_E_ARG, "mc_tq_frames_multiref: coefficients 16-byte and sources 4-byte aligned");
+        if ((long long)(f.cw / 16) * (f.ch / 16) > (1 << 24)) return fail(H264A_E_ARG, "mc_tq_frames_multiref: frame too large");
+    }
+    const QuantTables4 qt = make_tables4(dz);
+    for (int g0 = 0; g0 < nframes; g0 += TQ_MAXF) {
+        const int gn = nframes - g0 < TQ_MAXF ? nframes - g0 : TQ_MAXF;
+        TqBatch b;
+        memset(&b, 0, sizeof b);
+        b.n = gn;
+        long long total = 0;
+        for (int k = 0; k < gn; k++) {
+            const h264a_mc_tq_mr_frame& f = h_frames[g0 + k];
+            TqFrameDesc& d = b.f[k];
+            d.pic = h264a_picture{f.d_src, f.d_planes[0], f.cw, f.ch, f.pad};
+            d.picks = f.d_picks;
+            d.qp = f.qp;
+            d.coeffs = f.d_coeffs;
+            d.mb_w = f.cw / 16;
+            d.nmb = (f.cw / 16) * (f.ch / 16);
+            d.rec = nullptr;
+            for (int r = 0; r < 4; r++) d.rplanes[r] = f.d_planes[r < f.nref ? r : 0];
+            d.stride = 8;
+            b.mb_base[k] = int(total);
+            total += d.nmb;
+        }
+        if (total >= (1LL << 31)) return fail(H264A_E_ARG, "mc_tq_frames_multiref: too many macroblocks in one call");
+        const long long threads = total * 16;
+        mc_tq_frames_kernel<<<unsigned((threads + 255) / 256), 256, 0, st>>>(b, total, qt);
+        const int rc = check_launch("mc_tq_frames_kernel");
+        if (rc) return rc;
+    }
+    return H264A_OK;
+}
+
+extern "C" int h264a_mc_tq_frames_multiref(h264a_ctx* ctx, const h264a_mc_tq_mr_frame* h_frames, int nframes,
+                                           void* stream) {
+    return mc_tq_mr_run(ctx, h_frames, nframes, pick_stream(ctx, stream));
 }
 
 extern "C" int h264a_mc_tq_frames(h264a_ctx* ctx, const h264a_tq_frame* h_frames, int nframes, void* stream) {

@@ -73,7 +73,7 @@ def test_struct_layouts_match_header(tmp_path):
                "h264a_stream_frames": accel.StreamFrames, "h264a_mvnet_frame": MvnetFrame,
                "h264a_me_mr_frame": accel.MeMrFrame, "h264a_batch_stream": accel.BatchStream,
                "h264a_batch_config": accel.BatchConfig, "h264a_batch_info": accel.BatchInfo,
-               "h264a_la_stream": accel.LaStream}
+               "h264a_la_stream": accel.LaStream, "h264a_mc_tq_mr_frame": accel.McTqMrFrame}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "h264accel.h"', "int main(void) {"]
     for cname, py in mirrors.items():
         lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')

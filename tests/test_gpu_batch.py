@@ -39,9 +39,9 @@ def _clips(nframes: int):
 class _Rings:
     """Each stream's device rings (sources, planes, picks, costs)."""
 
-    def __init__(self, acc, clips, lam, gate):
+    def __init__(self, acc, clips, lam, gate, qp=None):
         torch = acc.torch
-        self.clips, self.rings, self.streams = clips, [], []
+        self.clips, self.rings, self.streams, self.coeffs = clips, [], [], []
         for c in clips:
             _, ch, cw = c.shape
             nmb = (cw // 16) * (ch // 16)
@@ -50,9 +50,12 @@ class _Rings:
             planes = acc.zeros((NSLOTS, pb), torch.uint8)
             picks = acc.zeros((NSLOTS, nmb, 8), torch.int32)
             costs = acc.zeros((NSLOTS, nmb, 2), torch.int64)
+            co = acc.zeros((NSLOTS, nmb, 256), torch.int16) if qp is not None else None
             self.rings.append((src, planes, picks, costs))
+            self.coeffs.append(co)
             self.streams.append(A.BatchStream(cw, ch, PAD, src.data_ptr(), planes.data_ptr(), picks.data_ptr(),
-                                              costs.data_ptr(), lam, gate))
+                                              costs.data_ptr(), lam, gate, 0 if co is None else co.data_ptr(),
+                                              qp or 0, 6))
 
     def upload(self, acc, frames):
         for c, (src, _, _, _) in zip(self.clips, self.rings):
@@ -62,11 +65,15 @@ class _Rings:
     def results(self, f):
         return [(r[2][f % NSLOTS].cpu().numpy(), r[3][f % NSLOTS].cpu().numpy()) for r in self.rings]
 
+    def levels(self, f):
+        return [co[f % NSLOTS].cpu().numpy() for co in self.coeffs]
 
-def _run(acc, clips, lam, gate, params, autotune=1, variant=0):
-    """Steps the batch over every P frame; returns {frame: [(picks, costs) per stream]} and the batch info."""
+
+def _run(acc, clips, lam, gate, params, autotune=1, variant=0, qp=None, levels=None):
+    """Steps the batch over every P frame; returns {frame: [(picks, costs) per stream]} and the batch info
+    (with qp, the luma levels of every frame go to levels[frame] too)."""
     n = clips[0].shape[0]
-    rings = _Rings(acc, clips, lam, gate)
+    rings = _Rings(acc, clips, lam, gate, qp)
     b = acc.batch_create(rings.streams, A.BatchConfig(G, NSLOTS, NREF, autotune, variant), params)
     out, k = {}, 0
     while k * G + 1 < n:
@@ -76,6 +83,8 @@ def _run(acc, clips, lam, gate, params, autotune=1, variant=0):
         acc.sync()
         for f in range(k * G + 1, k * G + count + 1):
             out[f] = rings.results(f)
+            if qp is not None:
+                levels[f] = rings.levels(f)
         k += 1
     info = b.info()
     b.close()
@@ -165,3 +174,42 @@ def test_batch_one_reference_one_frame_steps(acc):
                 assert (gp[:, 1] == 0).all() and (gp[:, 4] == 0).all()  # one reference: index 0 throughout
     finally:
         NREF, G, NSLOTS = saved
+
+
+def _oracle_levels(src, refs, picks8, qp):
+    """MC + luma T/Q of multi-reference picks from the single-reference
+    oracle, each 4x4 block from the reference of its half."""
+    nmb = picks8.shape[0]
+    p6 = np.zeros((nmb, 6), np.int32)
+    p6[:, 0], p6[:, 1:3], p6[:, 3:5] = picks8[:, 0], picks8[:, 2:4], picks8[:, 5:7]
+    out = np.zeros((nmb, 256), np.int16)
+    for r, ref in enumerate(refs):
+        c = O.mc_tq_frame(src, ref, p6, qp)
+        for by in range(0, 16, 4):
+            for bx in range(0, 16, 4):
+                part = np.where(picks8[:, 0] == 1, by >= 8, np.where(picks8[:, 0] == 2, bx >= 8, 0)).astype(int)
+                sel = picks8[np.arange(nmb), 1 + 3 * part] == r
+                off = ((2 if by >= 8 else 0) + (1 if bx >= 8 else 0)) * 64 + ((2 if by & 4 else 0) + (1 if bx & 4 else 0)) * 16
+                out[sel, off:off + 16] = c[sel, off:off + 16]
+    return out
+
+
+def test_batch_steps_with_mc_tq(acc):
+    """Streams with coefficient rings: each step's graph also runs the MC +
+    luma T/Q of the step's frames from the picks, each half from its own
+    reference; every frame's levels equal the oracle's and the picks still
+    equal the oracle's search."""
+    clips = _clips(8)
+    qp = 28
+    lam, gate, params = _setup(qp)
+    levels = {}
+    out, info = _run(acc, clips, lam, gate, params, qp=qp, levels=levels)
+    assert info["graphs"] >= 3
+    for f, res in sorted(out.items()):
+        refs_idx = [f - 1 - r for r in range(min(NREF, f))]
+        for s, (clip, (gp, gc)) in enumerate(zip(clips, res)):
+            wp, wc = _oracle(clip, f, lam, gate)
+            assert np.array_equal(gp[:, :7], wp[:, :7]) and np.array_equal(gc, wc), (f, s)
+            want = _oracle_levels(clip[f], [clip[r] for r in refs_idx], gp, qp)
+            assert np.array_equal(levels[f][s], want), (f, s)
+    assert any((lv != 0).any() for lvs in levels.values() for lv in lvs)

@@ -437,6 +437,64 @@ def test_me_frames_multiref_matches_oracle(acc):
     assert np.array_equal(got_p[2][:, 7], p1[:, 5])  # the same evaluation counts
 
 
+def oracle_mc_tq_multiref(src, refs, picks8, qp, dz_div=6):
+    """MC + luma T/Q of multi-reference picks from the single-reference
+    oracle: each 4x4 block's levels depend only on its source, its reference
+    picture and its MV, so every MB is priced once per reference and each
+    block taken from the reference of its half."""
+    nmb = picks8.shape[0]
+    p6 = np.zeros((nmb, 6), np.int32)
+    p6[:, 0] = picks8[:, 0]
+    p6[:, 1:3] = picks8[:, 2:4]
+    p6[:, 3:5] = picks8[:, 5:7]
+    out = np.zeros((nmb, 256), np.int16)
+    shape = picks8[:, 0]
+    for r, ref in enumerate(refs):
+        c = O.mc_tq_frame(src, ref, p6, qp, dz_div)
+        for by in range(0, 16, 4):
+            for bx in range(0, 16, 4):
+                part = np.where(shape == 1, by >= 8, np.where(shape == 2, bx >= 8, 0)).astype(int)
+                ref_of = picks8[np.arange(nmb), 1 + 3 * part]
+                off = ((2 if by >= 8 else 0) + (1 if bx >= 8 else 0)) * 64 + ((2 if by & 4 else 0) + (1 if bx & 4 else 0)) * 16
+                sel = ref_of == r
+                out[sel, off:off + 16] = c[sel, off:off + 16]
+    return out
+
+
+def test_mc_tq_frames_multiref_matches_oracle(acc):
+    """MC + luma T/Q of multi-reference picks (each half from its own
+    reference, the picks of a three-reference search) equals the
+    single-reference oracle block by block."""
+    torch = acc.torch
+    y, _, _ = synth.cif_clip(6, 17)
+    clip = synth.coded_luma(y)
+    qp = 26
+    lam = float(np.sqrt(A.frame_lambda(qp)) * 1.25)
+    got_p, _ = _mr_case(acc, clip, [5, 3], [[4, 3, 2], [2, 1]], lam, A.split_gate_for_qp(qp), A.default_me_params())
+    n, ch, cw = clip.shape
+    nmb = (cw // 16) * (ch // 16)
+    d = dev(acc, clip)
+    planes = acc.hpel_build(d, 32)
+    pk = dev(acc, got_p)
+    co = acc.zeros((2, nmb, 256), torch.int16)
+    fr = []
+    for i, (sidx, refs) in enumerate(zip([5, 3], [[4, 3, 2], [2, 1]])):
+        f = A.McTqMrFrame()
+        f.d_src = d[sidx].data_ptr()
+        for r, ri in enumerate(refs):
+            f.d_planes[r] = planes[ri].data_ptr()
+        f.nref, f.cw, f.ch, f.pad = len(refs), cw, ch, 32
+        f.d_picks, f.qp, f.dz_div, f.d_coeffs = pk[i].data_ptr(), qp, 6, co[i].data_ptr()
+        fr.append(f)
+    acc.mc_tq_frames_multiref(fr)
+    acc.sync()
+    got = co.cpu().numpy()
+    for i, (sidx, refs) in enumerate(zip([5, 3], [[4, 3, 2], [2, 1]])):
+        want = oracle_mc_tq_multiref(clip[sidx], [clip[r] for r in refs], got_p[i], qp)
+        assert np.array_equal(got[i], want), i
+    assert (got != 0).any()
+
+
 def test_me_frames_multiref_720p_three_references(acc):
     """A 1280x720 frame of the textured generator searched over its three
     previous frames equals the oracle."""
